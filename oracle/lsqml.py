@@ -1,0 +1,177 @@
+"""pty-chi LSQML in float64 (oracle restatement, test infrastructure only).
+
+Follows physwkim/ptyrs `ptyrs/src/engine/lsqml.rs` for one object slice, no probe variation
+(`ProbeVariation::none`) and no position features: `LsqmlBatch::new` (lsqml.rs:102-179),
+`obj_directions`, `frame_probe_directions`, `probe_direction` (lsqml.rs:194-229),
+`step_sizes` (lsqml.rs:286-350), `trim_mean` (lsqml.rs:392-398), `Lsqml::step`
+(lsqml.rs:581-643) and `Lsqml::epoch` (lsqml.rs:663-714).
+"""
+import math
+
+import numpy as np
+
+from . import ops
+from .base import fftshift2, random_batches
+
+EPS_AMPLITUDE = 1e-9
+EPS_POISSON = 1e-6
+EPS_XI = 1e-5
+LAMBDA0 = 1.2e-7
+
+
+def trim_mean(x):
+    """MATLAB `trimmean(x, 10)` (engine/lsqml.rs:392-398)."""
+    s = sorted(float(v) for v in x)
+    k = int(math.ceil(len(s) * 0.1 / 2.0 - 0.5))
+    kept = s[k:len(s) - k]
+    total = 0.0
+    for v in kept:
+        total += v
+    return total / len(kept)
+
+
+class Lsqml:
+    """LSQML state across epochs (engine/lsqml.rs:415-430). cost: "poisson" or "amplitude"."""
+
+    def __init__(self, batch_size, cost="poisson", seed=7):
+        if batch_size == 0:
+            raise ValueError("LSQML batch_size must be >= 1")
+        self.batch_size, self.cost, self.seed = batch_size, cost, seed
+        self.epochs = 0
+        self.preconditioner = None
+        self.a_far_all = {}
+
+    def a_far(self, f):
+        return self.a_far_all.get(f, 0.5)
+
+    def batch(self, views, obs, optics, obj, probe):
+        """`LsqmlBatch::new` (engine/lsqml.rs:102-179) for one slice without probe
+        variation: returns `(frames, nmode, psi, chi, a_far)`."""
+        nmode = 1
+        while nmode < len(views) and views[nmode]["frame"] == views[0]["frame"]:
+            nmode += 1
+        frames = [int(views[b * nmode]["frame"]) for b in range(len(views) // nmode)]
+        ny, nx = probe.shape[-2:]
+        psi = ops.obj_probe_to_psi(views, obj, probe, optics.quad)
+        chi = optics.exit_forward(psi)
+        sh = (len(frames), nmode, ny, nx)
+        icalc = (np.abs(chi.reshape(sh)) ** 2).sum(axis=1)
+        iobs, mask = obs.iobs[frames], obs.mask[frames]
+        keep = ~mask
+        if self.cost == "poisson":
+            a_far = [self.a_far(f) for f in frames]
+            for _ in range(2):
+                prev = sum(a_far) / len(a_far)
+                for b in range(len(frames)):
+                    yt, yp = iobs[b][keep[b]], icalc[b][keep[b]]
+                    xi = 1.0 - yt / (yp + EPS_XI)
+                    num = float((xi * (yp - yt / (1.0 - prev * xi))).sum())
+                    den = float((xi * xi * yp).sum())
+                    ratio = num / den if den > 0.0 else 0.0
+                    a_far[b] = min(max(0.5 * prev + 0.5 * ratio, 0.0), 1.0)
+            c = np.where(mask, 0.0, 1.0 - iobs / (icalc + EPS_POISSON))
+        else:
+            a_far = [0.5] * len(frames)
+            c = np.where(mask, 0.0,
+                         2.0 * (1.0 - np.sqrt(np.maximum(iobs, 0.0))
+                                / (np.sqrt(icalc) + EPS_AMPLITUDE)))
+        fac = 1.0 - np.asarray(a_far)[:, None, None] * c
+        chi = (chi.reshape(sh) * fac[:, None]).reshape(chi.shape)
+        chi = optics.exit_adjoint(chi) - psi
+        return frames, nmode, psi, chi, a_far
+
+    def step(self, views, obs, optics, obj, probe):
+        """`Lsqml::step` (engine/lsqml.rs:581-643); returns the new object and probe and the
+        step record."""
+        pre = self.preconditioner
+        floor = (0.1 * pre.max()) ** 2
+        frames, nmode, psi, chi, a_far = self.batch(views, obs, optics, obj, probe)
+        q = optics.quad
+        ny, nx = probe.shape[-2:]
+        np_ = probe.shape[0]
+        nb = len(frames)
+        # obj_directions: accumulate_obj over the views at each frame's own probe
+        d_obj = ops.accumulate_obj(views, obj.shape, probe, q, chi)[0]
+        d_obj = d_obj / np.sqrt(pre * pre + floor)
+        # frame_probe_directions: per-frame planes b·np + m
+        uviews = views.copy()
+        uviews["probe"] = np.repeat(np.arange(nb) * np_, nmode) + views["probe"]
+        d, _ = ops.accumulate_probe(uviews, obj, (nb * np_, ny, nx), q, chi)
+        d_probe = np.zeros_like(probe)
+        for b in range(nb):
+            for m in range(np_):
+                d_probe[m] += d[b * np_ + m]
+        d_probe = d_probe / float(nb)
+        a_obj, a_probe = self.step_sizes(views, nmode, optics, obj, probe, chi, d_obj, d_probe)
+        for f, a in zip(frames, a_far):
+            self.a_far_all[f] = a
+        so = trim_mean(a_obj)
+        new_obj = obj + so * d_obj
+        sp = sum(a_probe) / len(a_probe)
+        new_probe = probe + sp * d_probe
+        return new_obj, new_probe, dict(frames=frames, a_far=a_far, a_obj=a_obj,
+                                        a_probe=a_probe)
+
+    def step_sizes(self, views, nmode, optics, obj, probe, chi, d_obj, d_probe):
+        """pty-chi Eq. 22 per frame (engine/lsqml.rs:286-350), one slice."""
+        ny, nx = probe.shape[-2:]
+        n = ny * nx
+        q = optics.quad
+        scale = float(1 * nmode)
+        dpo = ops.obj_probe_to_psi(views, obj, d_probe, q)
+        dop = ops.obj_probe_to_psi(views, d_obj, probe, q)
+        lambda0 = LAMBDA0 * optics.intensity_scale() / n
+        nb = len(views) // nmode
+        sh = (nb, nmode * n)
+        u, v, c = dop.reshape(sh), dpo.reshape(sh), chi.reshape(sh)
+        a12 = u * np.conj(v)
+        s = np.stack([(np.abs(u) ** 2 + lambda0).sum(axis=1),
+                      (np.abs(v) ** 2 + lambda0).sum(axis=1),
+                      a12.real.sum(axis=1), a12.imag.sum(axis=1),
+                      (np.conj(u) * c).real.sum(axis=1),
+                      (np.conj(v) * c).real.sum(axis=1)], axis=1)
+        reg11, reg22 = 0.1 * (s[:, 0].sum() / nb), 0.1 * (s[:, 1].sum() / nb)
+        a_obj, a_probe = [], []
+        for r in s:
+            a11, a22 = r[0] + reg11, r[1] + reg22
+            det = a11 * a22 - (r[2] * r[2] + r[3] * r[3])
+            x0 = (a22 * r[4] - r[2] * r[5]) / det
+            x1 = (a11 * r[5] - r[2] * r[4]) / det
+            a_obj.append(0.9 * max(x0, 0.0) / scale)
+            a_probe.append(0.9 * max(x1, 0.0))
+        return a_obj, a_probe
+
+    def epoch(self, addr, obs, optics, obj, probe):
+        """`Lsqml::epoch` (engine/lsqml.rs:663-714): preconditioner on pty-chi's schedule, then
+        `step` over the epoch's seeded batches. Returns `(obj, probe, steps)`."""
+        nframe, nmode = addr.nframe, addr.nmode
+        if self.epochs < 10 or self.epochs % 10 == 0:
+            illum = ops.illumination(addr.views, obj.shape, probe)
+            pre = self.preconditioner
+            if pre is None:
+                n = float(probe.shape[-1] * probe.shape[-2])
+                k = optics.intensity_scale()
+                power = 0.0
+                for f in range(nframe):
+                    power = max(power, float(obs.iobs[f][~obs.mask[f]].sum()))
+                pre = illum * (power / (4.0 * n * k))
+            self.preconditioner = (pre + illum) / 2.0
+        epoch = self.epochs
+        self.epochs += 1
+        size = min(self.batch_size, nframe)
+        steps = []
+        for frames in random_batches(nframe, size, self.seed, epoch):
+            views = np.concatenate([addr.frame_views(f) for f in frames])
+            obj, probe, st = self.step(views, obs, optics, obj, probe)
+            steps.append(st)
+        return obj, probe, steps
+
+    @staticmethod
+    def llk(addr, obs, optics, obj, probe):
+        """Normalised LLK of the model the steps update (engine/lsqml.rs:537-551)."""
+        psi = optics.exit_forward(ops.obj_probe_to_psi(addr.views, obj, probe, optics.quad))
+        return ops.llk(obs, slice(0, addr.nframe), addr.nmode, psi).normalised(obs.nb_obs)
+
+
+def fftshift_planes(a):
+    return fftshift2(a)

@@ -1,0 +1,267 @@
+"""rPIE and ML (Poisson conjugate gradient) in float64 (oracle restatement, test
+infrastructure only).
+
+Follows physwkim/ptyrs `ptyrs/src/engine/ptycho.rs` (`Ptycho`) for the far-field and
+planar near-field optics of a single object slice, without position features.
+"""
+import numpy as np
+
+from . import ops
+from .base import AddrTable, Observed, fftshift2, pynx_preprocess, random_batches
+
+
+def llk_due(calc_llk, ic, ncycle):
+    """engine/ptycho.rs:44-46."""
+    return calc_llk > 0 and (ic % calc_llk == 0 or ic + 1 == ncycle)
+
+
+class Ptycho:
+    """Reconstruction state of one scan (engine/ptycho.rs:198-285).
+
+    counts: `[nframe, ny, nx]` detector order (u16 with MASKED, or float with negative masked);
+    y, x: positions in metres; object `[nobj, nyo, nxo]`, probe `[nprobe, ny, nx]` complex.
+    """
+
+    def __init__(self, counts, y, x, optics, obj, probe):
+        counts = np.asarray(counts)
+        frame = list(counts.shape[1:])
+        if list(probe.shape[1:]) != frame:
+            raise ValueError("probe plane differs from frame")
+        self.optics = optics
+        py, px = pynx_preprocess(y, x, optics.pixel)
+        self.addr = AddrTable(py, px, optics.pixel, frame, list(obj.shape[1:]),
+                              probe.shape[0], obj.shape[0])
+        self.obs = Observed(counts)
+        self.object = np.array(obj, np.complex128)
+        self.probe = np.array(probe, np.complex128)
+        self.cycle = 0
+        self.history = []
+
+    # exit waves -------------------------------------------------------------------------
+    def calc_psi(self, views=None, obj=None, probe=None):
+        views = self.addr.views if views is None else views
+        obj = self.object if obj is None else obj
+        probe = self.probe if probe is None else probe
+        return ops.obj_probe_to_psi(views, obj, probe, self.optics.quad)
+
+    def llk(self):
+        """Normalised LLK of the current estimate (engine/ptycho.rs:454-466)."""
+        psi = self.optics.exit_forward(self.calc_psi())
+        return ops.llk(self.obs, slice(0, self.addr.nframe), self.addr.nmode,
+                       psi).normalised(self.obs.nb_obs)
+
+    def record(self, algorithm, l):
+        self.history.append(dict(cycle=self.cycle, algorithm=algorithm, **l.as_dict()))
+
+    # ML ---------------------------------------------------------------------------------
+    def grad_psi(self):
+        """Object-plane `2·∂L/∂psi*` (engine/ptycho.rs:548-561)."""
+        psi = self.optics.exit_forward(self.calc_psi())
+        psi = ops.poisson_grad(self.obs, slice(0, self.addr.nframe), self.addr.nmode, psi)
+        return self.optics.exit_adjoint(psi)
+
+    def grads(self, obj=True, probe=True):
+        """Numerators of the back-projections of `grad_psi` (engine/ptycho.rs:429-450,
+        511-513)."""
+        g = self.grad_psi()
+        views, q = self.addr.views, self.optics.quad
+        go = (ops.accumulate_obj(views, self.object.shape, self.probe, q, g)[0] if obj
+              else np.zeros_like(self.object))
+        gp = (ops.accumulate_probe(views, self.object, self.probe.shape, q, g)[0] if probe
+              else np.zeros_like(self.probe))
+        return go, gp
+
+    def cg_gamma(self, d_obj, d_probe):
+        """engine/ptycho.rs:517-545 without position features."""
+        views, q = self.addr.views, self.optics.quad
+        po = self.calc_psi()
+        a = (ops.obj_probe_to_psi(views, d_obj, self.probe, q)
+             + ops.obj_probe_to_psi(views, self.object, d_probe, q))
+        b = ops.obj_probe_to_psi(views, d_obj, d_probe, q)
+        po, a, b = (self.optics.exit_forward(x) for x in (po, a, b))
+        return ops.cg_poisson_gamma(self.obs, slice(0, self.addr.nframe), self.addr.nmode,
+                                    po, a, b)
+
+    def scale_obj_probe(self):
+        """PyNX ScaleObjProbe(absolute=True) without background (engine/ptycho.rs:577-591)."""
+        calc = self.llk().nb_photons_calc
+        s = np.sqrt(self.obs.total() / calc)
+        os_ = float(np.abs(self.object).sum())
+        ps = float(np.abs(self.probe).sum())
+        fp, fo = np.sqrt(os_ / ps * s), np.sqrt(ps / os_ * s)
+        self.probe = self.probe * fp
+        self.object = self.object * fo
+
+    def ml(self, ncycle, update_object=True, update_probe=False, calc_llk=0,
+           zero_phase_ramp=True):
+        """PyNX ML Poisson CG (engine/ptycho.rs:775-842)."""
+        self.scale_obj_probe()
+        last = None
+        d_obj = np.zeros_like(self.object)
+        d_probe = np.zeros_like(self.probe)
+        for ic in range(ncycle):
+            l = self.llk() if llk_due(calc_llk, ic, ncycle) else None
+            go, gp = self.grads(update_object, update_probe)
+            if last is None:
+                beta = 0.0
+            else:
+                num = ((np.conj(go) * (go - last[0])).real.sum()
+                       + (np.conj(gp) * (gp - last[1])).real.sum())
+                den = (np.abs(last[0]) ** 2).sum() + (np.abs(last[1]) ** 2).sum()
+                with np.errstate(divide="ignore", invalid="ignore"):
+                    beta = num / den
+                if not (np.isfinite(beta) and beta >= 0.0):
+                    beta = 0.0
+            d_obj = d_obj * beta - go
+            d_probe = d_probe * beta - gp
+            num, den = self.cg_gamma(d_obj, d_probe)
+            with np.errstate(divide="ignore", invalid="ignore"):
+                gamma = np.float64(num) / np.float64(den)
+            if np.isfinite(gamma):
+                self.object = self.object + d_obj * gamma
+                self.probe = self.probe + d_probe * gamma
+            else:
+                d_obj, d_probe = -go, -gp
+            last = (go, gp)
+            if l is not None:
+                self.record("ml", l)
+            self.cycle += 1
+        if zero_phase_ramp:
+            self.zero_phase_ramp()
+
+    def zero_phase_ramp(self):
+        """PyNX ZeroPhaseRamp (engine/ptycho.rs:1134-1170)."""
+        self.object, self.probe = zero_phase_ramp(self.object, self.probe)
+
+    # AP (only as the warm-up of the reference's golden ML run) ----------------------------
+    def ap(self, ncycle, obj_inertia=0.01, probe_inertia=None, calc_llk=0,
+           zero_phase_ramp=True):
+        """PyNX AP without features (engine/ptycho.rs:609-641, ops.rs:352-381)."""
+        nframe, nmode = self.addr.nframe, self.addr.nmode
+        views, q = self.addr.views, self.optics.quad
+        for ic in range(ncycle):
+            psi = self.optics.exit_forward(self.calc_psi())
+            l = None
+            if llk_due(calc_llk, ic, ncycle):
+                l = ops.llk(self.obs, slice(0, nframe), nmode, psi).normalised(self.obs.nb_obs)
+            psi = ops.apply_amplitude(self.obs, slice(0, nframe), nmode, psi)
+            psi = self.optics.exit_adjoint(psi)
+            acc = (ops.accumulate_obj(views, self.object.shape, self.probe, q, psi)
+                   if obj_inertia is not None else None)
+            if probe_inertia is not None:
+                num, norm = ops.accumulate_probe(views, self.object, self.probe.shape, q, psi)
+                self.probe = _blend(self.probe, num, norm, probe_inertia)
+            if acc is not None:
+                self.object = _blend(self.object, acc[0], acc[1], obj_inertia)
+            if l is not None:
+                self.record("ap", l)
+            self.cycle += 1
+        if zero_phase_ramp:
+            self.zero_phase_ramp()
+
+    # rPIE -------------------------------------------------------------------------------
+    def rpie(self, nepoch, obj_step=1.0, probe_step=1.0, obj_alpha=0.1, probe_alpha=0.1,
+             batch_size=100, calc_llk=0, seed=7):
+        """pty-chi rPIE on seeded mini-batches (engine/ptycho.rs:874-902)."""
+        if self.addr.nobj != 1:
+            raise ValueError("rPIE needs exactly one object mode")
+        if batch_size == 0:
+            raise ValueError("rPIE batch_size must be >= 1")
+        nframe = self.addr.nframe
+        for ic in range(nepoch):
+            for frames in random_batches(nframe, batch_size, seed, self.cycle):
+                self.rpie_batch(frames, obj_step, probe_step, obj_alpha, probe_alpha)
+            if llk_due(calc_llk, ic, nepoch):
+                self.record("rpie", self.llk())
+            self.cycle += 1
+
+    def rpie_batch(self, frames, obj_step, probe_step, obj_alpha, probe_alpha):
+        """One rPIE batch from the batch-start object and probe (engine/ptycho.rs:904-1085),
+        Patch sampling without offsets."""
+        ny, nx = self.probe.shape[-2:]
+        nmode = self.addr.nmode
+        nbatch = len(frames)
+        views = np.concatenate([self.addr.frame_views(f) for f in frames])
+        q = self.optics.quad
+        psi = ops.obj_probe_to_psi(views, self.object, self.probe, q)
+        delta = self.optics.exit_forward(psi)
+        sh = (nbatch, nmode, ny, nx)
+        d4 = delta.reshape(sh)
+        calc = np.sqrt((np.abs(d4) ** 2).sum(axis=1))
+        iobs, mask = self.obs.iobs[frames], self.obs.mask[frames]
+        r = np.where(mask, 1.0, np.sqrt(iobs + 1e-7) / (calc + 1e-7))
+        delta = (d4 * r[:, None]).reshape(psi.shape)
+        delta = self.optics.exit_adjoint(delta) - psi
+
+        pidx = views["probe"].astype(np.int64)
+        wave = fftshift2(self.probe[pidx] * q)            # shifted, per view
+        w2 = fftshift2(np.abs(self.probe[pidx]) ** 2)       # shifted, per view
+        nyo, nxo = self.object.shape[-2:]
+        new_obj = new_probe = None
+        if obj_step is not None:
+            # overlap D_m placed on the object per probe mode, read back per view
+            # (engine/ptycho.rs:1094-1130)
+            dplanes = np.zeros((self.addr.nprobe, nyo, nxo))
+            w2n = fftshift2(w2)
+            for k, v in enumerate(views):
+                oy, ox = int(v["oy"]), int(v["ox"])
+                dplanes[pidx[k], oy:oy + ny, ox:ox + nx] += w2n[k]
+            dens = np.empty_like(w2)
+            for k, v in enumerate(views):
+                oy, ox = int(v["oy"]), int(v["ox"])
+                dens[k] = fftshift2(dplanes[pidx[k], oy:oy + ny, ox:ox + nx])
+            pmax = dens.reshape(sh).sum(axis=1).max()
+            a = obj_alpha
+            steps = np.conj(wave) / ((1.0 - a) * dens + a * pmax) * delta
+            stepn = fftshift2(steps)
+            d = np.zeros((nyo, nxo), np.complex128)
+            for k, v in enumerate(views):
+                oy, ox = int(v["oy"]), int(v["ox"])
+                d[oy:oy + ny, ox:ox + nx] += stepn[k]
+            new_obj = d
+        if probe_step is not None:
+            a = probe_alpha
+            dp = np.zeros_like(self.probe)
+            deltan = fftshift2(delta)
+            ob = self.object[0]
+            for b in range(nbatch):
+                fv = views[b * nmode:(b + 1) * nmode]
+                oy, ox = int(fv[0]["oy"]), int(fv[0]["ox"])
+                win = ob[oy:oy + ny, ox:ox + nx]
+                omax = (np.abs(win) ** 2).max()
+                w = np.conj(win * q) / ((1.0 - a) * np.abs(win) ** 2 + a * omax)
+                for m, v in enumerate(fv):
+                    dp[int(v["probe"])] += w * deltan[b * nmode + m]
+            new_probe = dp
+        if obj_step is not None:
+            self.object = self.object + new_obj[None] * obj_step
+        if probe_step is not None:
+            self.probe = self.probe + new_probe * (probe_step / nbatch)
+
+
+def zero_phase_ramp(obj, probe):
+    """engine/ptycho.rs:1134-1170."""
+    ny, nx = probe.shape[-2:]
+    far = ops.fft2(fftshift2(probe))
+    v = (np.abs(fftshift2(far)) ** 2).sum(axis=0)
+    w = v.sum()
+    iy, ix = np.mgrid[:ny, :nx]
+    dy = (v * iy).sum() / w - (ny // 2)
+    dx = (v * ix).sum() / w - (nx // 2)
+
+    def ramp(length, half, scale, d, sign):
+        return sign * 2.0 * np.pi * d * (np.arange(length) - half) / scale
+
+    ry, rx = ramp(ny, ny // 2, ny, dy, -1.0), ramp(nx, nx // 2, nx, dx, -1.0)
+    probe = probe * np.exp(1j * (ry[:, None] + rx[None, :]))
+    nyo, nxo = obj.shape[-2:]
+    ry, rx = ramp(nyo, nyo // 2, ny, dy, 1.0), ramp(nxo, nxo // 2, nx, dx, 1.0)
+    obj = obj * np.exp(1j * (ry[:, None] + rx[None, :]))
+    return obj, probe
+
+
+def _blend(old, num, norm, inertia):
+    """`(num + reg·old) / max(norm + reg, 1e-12)`, `reg = max(norm)·inertia`
+    (engine/ops.rs:371-381)."""
+    reg = max(0.0, float(norm.max())) * inertia
+    return (num + old * reg) / np.maximum(norm + reg, 1e-12)

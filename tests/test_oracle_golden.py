@@ -1,0 +1,192 @@
+"""The f64 oracle against the reference's golden vectors (pty-chi runs in float64 saved by the
+reference, converted by `tests/golden/make_golden.py`), to the reference's own bounds:
+`ptyrs/tests/engine_rpie_near.rs` (rPIE, LLK trace and changes to 1e-12) and
+`ptyrs/tests/engine_lsqml_near.rs` (LSQML forward model, one step, and the epochs)."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import ops
+from oracle.base import AddrTable, Observed, counts_from_f64, fftshift2
+from oracle.lsqml import Lsqml
+from oracle.ptycho import Ptycho
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SHAPE, OBJ, NPROBE = (24, 24), (40, 40), 2
+
+
+def golden(name):
+    return dict(np.load(os.path.join(HERE, "golden", f"{name}.npz")))
+
+
+def max_rel(a, b):
+    a, b = np.asarray(a, float).ravel(), np.asarray(b, float).ravel()
+    return np.abs(a - b).max() / np.abs(b).max()
+
+
+def stack(dims, rows, lead):
+    return (rows[:, lead] + 1j * rows[:, lead + 1]).reshape(dims)
+
+
+def change(a, b):
+    d = (a - b).ravel()
+    return np.stack([d.real, d.imag], axis=1).ravel()
+
+
+def of_run(rows, run, lead):
+    r = rows[rows[:, 0] == run]
+    return np.stack([r[:, lead], r[:, lead + 1]], axis=1).ravel()
+
+
+def near_case(g, c, pixel):
+    """Positions from the golden corners (`corner = (OBJ − SHAPE)/2 + position/pixel`), the
+    counts of case `c` and its free-space optics."""
+    corners = g["corners"]
+    ys = (corners[:, 1] - (OBJ[0] - SHAPE[0]) // 2) * pixel
+    xs = (corners[:, 2] - (OBJ[1] - SHAPE[1]) // 2) * pixel
+    rows = g["counts"][g["counts"][:, 0] == c[0]]
+    counts = counts_from_f64(rows[:, 2:].reshape(len(corners), *SHAPE))
+    w = ops.Wavefield(SHAPE, c[1], [pixel, pixel], c[3])
+    optics = ops.Optics.free_space(w)
+    kind = {"fourier": 0, "angular": 1, "fresnel": 2}[optics.propagator.kind]
+    assert kind == int(c[4])
+    obj = stack((1,) + OBJ, g["obj"], 2)
+    probe = stack((NPROBE,) + SHAPE, g["probe"], 3)
+    return corners, counts, ys, xs, optics, obj, probe
+
+
+def test_rpie_matches_ptychi_near_field():
+    """engine_rpie_near.rs:92-170: 3 propagators × batches 1/4/16 over 30 epochs."""
+    g = golden("rpie_near")
+    runs, trace = g["runs"], g["llk"]
+    for r in runs:
+        c = g["cases"][int(r[1])]
+        corners, counts, ys, xs, optics, obj, probe = near_case(g, c, c[2])
+        p = Ptycho(counts, ys, xs, optics, obj, probe)
+        for f in range(len(corners)):
+            v = p.addr.frame_views(f)[0]
+            assert [v["oy"], v["ox"]] == [corners[f, 1], corners[f, 2]]
+        o0, p0 = p.object.copy(), p.probe.copy()
+        llks = [p.llk().poisson]
+        p.rpie(int(r[3]), obj_step=r[4], probe_step=r[5], obj_alpha=r[6], probe_alpha=r[7],
+               batch_size=int(r[2]), calc_llk=1, seed=7)
+        llks += [h["poisson"] for h in p.history]
+        want = trace[trace[:, 0] == r[0]][:, 2]
+        assert max_rel(llks, want) < 1e-12, f"run {r[0]} LLK trace"
+        assert max_rel(change(p.object, o0), of_run(g["run_obj"], r[0], 3)) < 1e-12
+        assert max_rel(change(p.probe, p0), of_run(g["run_probe"], r[0], 4)) < 1e-12
+
+
+def lsqml_state():
+    g = golden("lsqml_near")
+    corners = g["corners"]
+    ys = corners[:, 1] - (OBJ[0] - SHAPE[0]) // 2
+    xs = corners[:, 2] - (OBJ[1] - SHAPE[1]) // 2
+    addr = AddrTable(ys, xs, [1.0, 1.0], SHAPE, OBJ, NPROBE, 1)
+    for f in range(len(corners)):
+        v = addr.frame_views(f)[0]
+        assert [v["oy"], v["ox"]] == [corners[f, 1], corners[f, 2]]
+    obj = stack((1,) + OBJ, g["obj"], 2)
+    probe = stack((NPROBE,) + SHAPE, g["probe"], 3)
+    cases = []
+    for c in g["cases"]:
+        w = ops.Wavefield(SHAPE, c[1], [c[2], c[2]], c[3])
+        optics = ops.Optics.free_space(w)
+        assert abs(optics.intensity_scale() - c[5]) <= 1e-15 * abs(c[5])
+        rows = g["counts"][g["counts"][:, 0] == c[0]]
+        obs = Observed(counts_from_f64(rows[:, 2:].reshape(len(corners), *SHAPE)))
+        cases.append((optics, obs, c[6]))
+    return g, addr, obj, probe, cases
+
+
+def test_lsqml_forward_matches_ptychi():
+    """engine_lsqml_near.rs:154-171: pty-chi's `y_pred` of frames 0..4."""
+    g, addr, obj, probe, cases = lsqml_state()
+    for r in g["icalc"]:
+        optics, obs, _ = cases[int(r[0])]
+        f = int(r[1])
+        psi = optics.exit_forward(ops.obj_probe_to_psi(addr.frame_views(f), obj, probe,
+                                                       optics.quad))
+        got = (np.abs(psi) ** 2).sum(axis=0)
+        want = fftshift2(r[2:].reshape(SHAPE))
+        assert max_rel(got, want) < 1e-14
+
+
+def assert_step(st, rows, col):
+    assert st["frames"] == [int(v) for v in rows[:, col]]
+    assert max_rel(st["a_far"], rows[:, col + 1]) < 1e-13
+    assert max_rel(st["a_obj"], rows[:, col + 2]) < 1e-12
+    assert max_rel(st["a_probe"], rows[:, col + 3]) < 1e-12
+
+
+def test_lsqml_step_matches_ptychi():
+    """engine_lsqml_near.rs:300-340: one step on frames 0..8, every case."""
+    g, addr, obj, probe, cases = lsqml_state()
+    views = addr.views[:8 * addr.nmode]
+    for k, (optics, obs, _) in enumerate(cases):
+        run = Lsqml(8, "poisson", 0)
+        run.preconditioner = ops.illumination(addr.views, obj.shape, probe)
+        o, p, st = run.step(views, obs, optics, obj, probe)
+        assert_step(st, g["step_steps"][g["step_steps"][:, 0] == k], 1)
+        assert max_rel(change(o, obj), of_run(g["step_obj"], k, 3)) < 1e-12
+        assert max_rel(change(p, probe), of_run(g["step_probe"], k, 4)) < 1e-12
+
+
+def test_lsqml_epochs_match_ptychi():
+    """engine_lsqml_near.rs:450-510: batches of 8 (seed 7) over the saved epochs."""
+    g, addr, obj0, probe0, cases = lsqml_state()
+    steps, trace = g["epochs_steps"], g["llk"]
+    for k, (optics, obs, truth) in enumerate(cases):
+        obj, probe = obj0.copy(), probe0.copy()
+        run = Lsqml(8, "poisson", 7)
+        want = trace[trace[:, 0] == k]
+        rows = steps[steps[:, 0] == k]
+        llks = [Lsqml.llk(addr, obs, optics, obj, probe).poisson]
+        nxt = 0
+        for e in range(len(want) - 1):
+            obj, probe, sts = run.epoch(addr, obs, optics, obj, probe)
+            for st in sts:
+                w = rows[nxt:nxt + len(st["frames"])]
+                nxt += len(st["frames"])
+                assert (w[:, 1] == e).all()
+                assert_step(st, w, 2)
+            llks.append(Lsqml.llk(addr, obs, optics, obj, probe).poisson)
+        assert nxt == len(rows)
+        assert max_rel(llks, want[:, 2]) < 1e-12
+        assert max_rel(change(obj, obj0), of_run(g["epochs_obj"], k, 3)) < 1e-12
+        assert max_rel(change(probe, probe0), of_run(g["epochs_probe"], k, 4)) < 1e-12
+
+
+def test_ml_matches_pynx_near_field():
+    """engine_pynx_near.rs:107-205, the exact-kernel ML run (run 7): 10 AP cycles with probe
+    inertia 0.001, then 30 ML cycles updating object and probe; every LLK column per record
+    and the final arrays to the reference's 5e-12."""
+    g = golden("pynx_near")
+    c = g["case"][0]
+    pixel = c[1]
+    corners = g["corners"]
+    ys = (corners[:, 1] - (OBJ[0] - SHAPE[0]) // 2) * pixel
+    xs = (corners[:, 2] - (OBJ[1] - SHAPE[1]) // 2) * pixel
+    counts = counts_from_f64(g["counts"][:, 1:].reshape(len(corners), *SHAPE))
+    optics = ops.Optics.free_space(ops.Wavefield(SHAPE, c[0], [pixel, pixel], c[2]))
+    assert optics.propagator.kind == "angular"
+    obj = stack((1,) + OBJ, g["obj"], 2)
+    probe = stack((NPROBE,) + SHAPE, g["probe"], 3)
+    run = g["runs"][7]
+    assert run[1] == 1 and run[2] == 3
+    p = Ptycho(counts, ys, xs, optics, obj, probe)
+    p.ap(10, probe_inertia=0.001, calc_llk=0, zero_phase_ramp=False)
+    p.ml(int(run[3]), update_probe=True, calc_llk=1, zero_phase_ramp=False)
+    cols = ["poisson", "gaussian", "euclidian", "nb_photons_calc"]
+    got = [[h[k] for k in cols] for h in p.history][1:]
+    got.append([p.llk().as_dict()[k] for k in cols])
+    got = np.asarray(got)
+    want = g["llk"][g["llk"][:, 0] == run[0]][:, 2:6]
+    err = (np.abs(got - want) / np.abs(want)).max()
+    assert err < 5e-12, err
+    for arr, rows, lead in [(p.object, g["run_obj"], 3), (p.probe, g["run_probe"], 4)]:
+        r = rows[rows[:, 0] == run[0]]
+        want = r[:, lead] + 1j * r[:, lead + 1]
+        got = arr.ravel()
+        assert max_rel(np.stack([got.real, got.imag], 1), np.stack([want.real, want.imag], 1)) < 5e-12
