@@ -1,0 +1,338 @@
+"""Throughput of the reconstruction hot path on B200: diffraction patterns·iterations per second.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload lsqml128|rpie64]
+
+Workload `lsqml128` (default): the LSQML configuration — a 1024² smooth-noise object, a
+128² probe with 3 incoherent modes (powers 0.8/0.15/0.05), a 4096-position Fermat scan at
+6 px, Poisson counts at 1e6 photons per pattern, batches of 256 frames, Poisson cost, FP32.
+A step is one epoch: every one of the 4096 patterns once (16 batch updates). Inputs live in
+HBM before the timed region; the counts (268 MB) are larger than the 126 MB L2, so no flush
+is needed between steps. `rpie64`: the rPIE configuration (256² object, 64² probe, 20×20
+raster, batch 100), a step again one epoch.
+
+The timed region is bracketed by CUDA events on the engine's own stream (its device time of
+the K epochs) with a synchronize and, for N > 1, a barrier on both sides; N > 1 runs N
+independent replicas (one scan per GPU; the path has no exchange step), the time is the max
+over ranks and the value the patterns of all ranks over it.
+
+`--impl reference` times the reference's CPU path on the host cores: the reference engine is
+Rust and cannot be built in this image, so its numpy float64 restatement (`oracle/`) runs, one
+LSQML batch of 256 frames per step, its FFTs on every host thread.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+
+WORKLOADS = {
+    "lsqml128": dict(kind="lsqml128", algorithm="lsqml", batch=256, cost="poisson",
+                     desc="LSQML, 1024^2 object, 128^2 probe x3 modes, Fermat 4096 @ 6 px, "
+                          "1e6 photons, batch 256, Poisson"),
+    "rpie64": dict(kind="rpie64", algorithm="rpie", batch=100,
+                   desc="rPIE, 256^2 object, 64^2 probe, 20x20 raster 8 px +-1 px, "
+                        "1e5 photons, batch 100, alpha=beta=0.1"),
+}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    return int(os.environ.get("RANK", "0")), ws, int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f), "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.seek(0)
+        rows = [r.split(",") for r in self.file.read().strip().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for name, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_inputs(workload, seed):
+    from ptyrs_b200 import sim
+    return sim.make_scan(WORKLOADS[workload]["kind"], seed=seed)
+
+
+def run_algorithm(g, wl, nepoch):
+    if wl["algorithm"] == "lsqml":
+        g.lsqml(nepoch, batch_size=wl["batch"], cost=wl["cost"], seed=7)
+    else:
+        g.rpie(nepoch, batch_size=wl["batch"], obj_alpha=0.1, probe_alpha=0.1, seed=7)
+
+
+def algorithmic_bytes(kind, s, wl):
+    """Bytes each launch of `kind` must move from HBM (the unique inputs it reads and outputs
+    it writes), per frame of the launch; probe, phase and twiddle reads are L2-resident."""
+    n2 = s["n"] ** 2
+    K = s["probe"].shape[0]
+    table = {
+        "frame_store": 8 * n2 + 8 * K * n2 + 4 * n2,
+        "frame_from_store": 8 * K * n2 + 4 * n2 + 8 * n2 + 8 * K * n2,
+        "frame_rpie": 8 * n2 + 4 * n2 + 8 * K * n2,
+        "frame_lsqml": 8 * n2 + 4 * n2 + 8 * K * n2,
+        "frame_llk": 8 * n2 + 4 * n2,
+        "probe_partial": 8 * K * n2 + 8 * n2,
+        "lsqml_dots": 8 * K * n2 + 16 * n2,
+        "object_lsqml": 8 * K * n2,
+        "object_rpie": 8 * K * n2,
+    }
+    return table.get(kind)
+
+
+def cpu_baseline(s, wl, seconds=15.0, threads=None):
+    """The oracle (numpy float64 restatement of the reference's CPU engine) on a bounded sample
+    of the workload: successive batch updates of `wl["batch"]` frames from the same start until
+    `seconds` pass; patterns·iter/s = frames processed / time."""
+    from oracle import ops
+    from oracle.lsqml import Lsqml
+    from oracle.ptycho import Ptycho
+    from ptyrs_b200 import sim
+    ops.FFT_WORKERS = threads
+    n = s["n"]
+    optics = ops.Optics.far_field(sim.WAVELENGTH, sim.DISTANCE, sim.DETECTOR_PIXEL, [n, n])
+    p = Ptycho(s["counts"], s["y"], s["x"], optics, s["object"], s["probe"])
+    from oracle.base import random_batches
+    batches = random_batches(p.addr.nframe, wl["batch"], 7, 0)
+    done, t0 = 0, time.perf_counter()
+    obj, probe = p.object, p.probe
+    if wl["algorithm"] == "lsqml":
+        run = Lsqml(wl["batch"], wl["cost"], 7)
+        run.preconditioner = ops.illumination(p.addr.views, obj.shape, probe)
+    for frames in batches:
+        views = np.concatenate([p.addr.frame_views(f) for f in frames])
+        if wl["algorithm"] == "lsqml":
+            obj, probe, _ = run.step(views, p.obs, optics, obj, probe)
+        else:
+            p.rpie_batch(frames, 1.0, 1.0, 0.1, 0.1)
+        done += len(frames)
+        if time.perf_counter() - t0 > seconds:
+            break
+    dt = time.perf_counter() - t0
+    ops.FFT_WORKERS = None
+    return done / dt, done, dt
+
+
+def reference_arm(args, wl):
+    rank, ws, _ = dist_env()
+    if rank != 0:
+        return
+    s = make_inputs(args.workload, 0)
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_baseline(s, wl, seconds=0.0, threads=threads)
+    vals, frames, secs = [], 0, 0.0
+    for _ in range(args.steps):
+        v, d, t = cpu_baseline(s, wl, seconds=0.0, threads=threads)
+        vals.append(v)
+        frames += d
+        secs += t
+    value = frames / secs
+    sample = (f"{args.steps} steps of one {wl['algorithm']} batch update of {wl['batch']} frames "
+              f"of the {args.workload} scan ({frames} pattern-iterations in {secs:.1f} s)")
+    line = {
+        "impl": "reference", "metric": "diffraction patterns*iter/sec", "value": value,
+        "unit": "patterns*iter/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * secs / max(args.steps, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "description": wl["desc"]},
+        "cpu_baseline": {"value": value, "unit": "patterns*iter/s", "cores": threads,
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "patterns*iter/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="lsqml128", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return reference_arm(args, wl)
+
+    rank, ws, local = dist_env()
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import torch
+
+    from ptyrs_b200 import GpuPtycho, Scan, build, sim
+    build.build()
+    s = make_inputs(args.workload, seed=rank)
+    P = len(s["counts"])
+    scan = Scan(s["counts"], s["y"], s["x"], s["wavelength"], s["distance"], s["detector_pixel"])
+    g = GpuPtycho(scan, s["object"], s["probe"], device=local)
+    run_algorithm(g, wl, args.warmup)
+    g.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # Timed region: K epochs, device time from events on the engine's stream.
+    g.set_timing(True)
+    barrier()
+    g.synchronize()
+    launches0 = g.launches()
+    clocks = Clocks(local)
+    run_algorithm(g, wl, args.steps)
+    g.synchronize()
+    clk = clocks.stop()
+    barrier()
+    ms = g.last_call_ms()
+    launches = g.launches() - launches0
+    times = g.kernel_times()
+    g.set_timing(False)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = P * ws * args.steps / (ms / 1e3)
+
+    # Dominant kernel and its roofline (algorithmic bytes per launch / mean launch time).
+    pk, pk_kind = peaks()
+    top = max(times.items(), key=lambda kv: kv[1][0])
+    kname, (kms, kn) = top
+    per_frame = algorithmic_bytes(kname, s, wl)
+    frames_per_launch = wl["batch"]
+    roofline = None
+    if per_frame:
+        bytes_launch = per_frame * frames_per_launch
+        achieved = bytes_launch / (kms / kn / 1e3) / 1e9
+        roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved,
+                    "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
+                    "peak_source": pk_kind, "traffic": None,
+                    "bytes_per_launch": bytes_launch, "mean_launch_ms": kms / kn,
+                    "share": kms / sum(v[0] for v in times.values())}
+
+    # End to end through the public API from pinned host buffers: per step, a fresh state
+    # (counts, positions, object and probe uploaded), one epoch, the object and probe read back.
+    e2e = None
+    if args.e2e_steps > 0:
+        pinned = torch.empty(s["counts"].shape, dtype=torch.float32, pin_memory=True)
+        pinned.numpy()[...] = s["counts"]
+        escan = Scan(pinned.numpy(), s["y"], s["x"], s["wavelength"], s["distance"],
+                     s["detector_pixel"])
+        with GpuPtycho(escan, s["object"], s["probe"], device=local) as w:  # warm-up
+            run_algorithm(w, wl, 1)
+            w.object()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            with GpuPtycho(escan, s["object"], s["probe"], device=local) as w:
+                run_algorithm(w, wl, 1)
+                w.object()
+                w.probe()
+        dt = time.perf_counter() - t0
+        if dist is not None:
+            t = torch.tensor([dt], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dt = float(t.item())
+        n = s["n"]
+        h2d = (s["counts"].nbytes + 8 * s["object"].size + 8 * s["probe"].size + 8 * P)
+        d2h = 8 * s["object"].size + 8 * s["probe"].size
+        e2e = {"value": P * ws * args.e2e_steps / dt, "unit": "patterns*iter/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "what": "per step: create from pinned host counts, one epoch, object and probe "
+                       "read back"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        v, done, secs = cpu_baseline(s, wl, seconds=15.0, threads=threads)
+        cpu = {"value": v, "unit": "patterns*iter/s", "cores": threads, "kind": "port",
+               "sample": f"{done} pattern-iterations ({done // wl['batch']} batch updates of "
+                         f"{wl['batch']} frames) of the same scan in {secs:.1f} s, numpy float64, "
+                         f"FFTs on {threads} threads"}
+    g.close()
+    if rank == 0:
+        line = {
+            "metric": "diffraction patterns*iter/sec", "value": value,
+            "unit": "patterns*iter/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "description": wl["desc"],
+                       "patterns_per_step_per_gpu": P, "parallelism": f"replicas{ws}",
+                       "l2": "inputs larger than L2 (counts "
+                             f"{s['counts'].nbytes / 1e6:.0f} MB)"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": int(launches), "clocks": clk,
+            "kernels_ms": {k: round(v[0], 3) for k, v in sorted(times.items())},
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

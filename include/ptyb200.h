@@ -1,0 +1,180 @@
+/* ptyb200 — B200-native ptychography reconstruction hot path behind a C ABI.
+ *
+ * One handle is one reconstruction state of one scan on one CUDA device, as the reference
+ * engine's `GpuPtycho` (physwkim/ptyrs, ptyrs/src/engine/gpu/mod.rs:533-881) is; the handle
+ * owns every device buffer. Inputs are copied (and rounded to single precision) at create;
+ * outputs are copied out on request as complex128 (interleaved re, im doubles).
+ *
+ * Errors follow the reference's `EngineError` (ptyrs/src/engine/mod.rs:106-123): every call
+ * returns a status; PTYB_INVALID leaves the state unchanged; a device failure part-way
+ * through an algorithm poisons the handle (PTYB_ABORTED for every later call that would
+ * enqueue work, while downloads still work, the reference's abort gate,
+ * ptyrs/src/engine/gpu/gate.rs:8-71). `ptyb_last_error` gives the message. A handle is not
+ * thread-safe; several handles may coexist.
+ */
+#ifndef PTYB200_H
+#define PTYB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum ptyb_status {
+  PTYB_OK = 0,
+  PTYB_INVALID = 1, /* bad shape or parameter; nothing changed */
+  PTYB_GPU = 2,     /* CUDA failure; the handle is poisoned */
+  PTYB_ABORTED = 3, /* an earlier call failed part-way; enqueueing calls are refused */
+};
+
+/* Counts encodings of `ptyb_scan.counts`. */
+enum ptyb_counts_kind {
+  PTYB_COUNTS_U16 = 0, /* uint16, 65535 masked (reference `Counts`, base/counts.rs:377-379) */
+  PTYB_COUNTS_F32 = 1, /* float32, negative masked (counts past 65534 photons) */
+  PTYB_COUNTS_F64 = 2, /* float64, negative masked */
+};
+
+/* A far-field scan (reference `Scan` + `Geometry`, ptyrs-py/src/lib.rs:435-463): counts
+ * [nframe][ny][nx] in detector order (zero frequency at the centre), positions in metres. */
+typedef struct ptyb_scan {
+  int32_t nframe, ny, nx;
+  int32_t counts_kind;
+  const void* counts;
+  const double* pos_y;
+  const double* pos_x;
+  double wavelength, distance, detector_pixel;
+} ptyb_scan;
+
+/* Reference `GpuOptions` (engine/gpu/mod.rs:63-112): frames per launch of the passes over the
+ * whole scan (LLK, ML), 0 for the default. */
+typedef struct ptyb_options {
+  int32_t device;
+  int32_t stack_size;
+} ptyb_options;
+
+/* Reference `RpieParams` (engine/ptycho.rs:148-186). A step flag of 0 holds that array. */
+typedef struct ptyb_rpie_params {
+  int32_t update_object, update_probe;
+  double obj_step, probe_step, obj_alpha, probe_alpha;
+  int32_t batch_size, calc_llk;
+  uint64_t seed;
+} ptyb_rpie_params;
+
+enum ptyb_cost { PTYB_COST_POISSON = 0, PTYB_COST_AMPLITUDE = 1 };
+
+/* Reference `LsqmlParams` (engine/lsqml.rs:34-53). */
+typedef struct ptyb_lsqml_params {
+  int32_t batch_size, cost;
+  uint64_t seed;
+} ptyb_lsqml_params;
+
+/* Reference `MlParams` (engine/ptycho.rs:123-143). */
+typedef struct ptyb_ml_params {
+  int32_t update_object, update_probe, calc_llk, zero_phase_ramp;
+} ptyb_ml_params;
+
+/* Reference `Llk` (engine/ops.rs:257-277), normalised by the unmasked pixel count. */
+typedef struct ptyb_llk {
+  double poisson, gaussian, euclidian, nb_photons_calc;
+} ptyb_llk;
+
+/* Reference `LlkRecord` (engine/ptycho.rs:36-41); algorithm 3 = rPIE, 4 = ML, 6 = LSQML
+ * (the reference's `Algorithm` order Ap, Dm, Raar, Rpie, Ml, Bh, Lsqml). */
+typedef struct ptyb_llk_record {
+  int64_t cycle;
+  int32_t algorithm;
+  int32_t pad_;
+  ptyb_llk llk;
+} ptyb_llk_record;
+
+/* One frame's LSQML step sizes (reference `LsqmlStep`, engine/lsqml.rs:56-66). */
+typedef struct ptyb_lsqml_step {
+  int32_t batch, frame;
+  double a_far, a_obj, a_probe;
+} ptyb_lsqml_step;
+
+typedef struct ptyb_handle ptyb_handle;
+
+/* Reference `GpuPtycho::new` (engine/gpu/mod.rs:601-617): object complex128 [nobj][nyo][nxo],
+ * probe complex128 [nprobe][ny][nx]. Positions go through PyNX's preprocessing and every
+ * window must lie inside the object (PTYB_INVALID otherwise). */
+int ptyb_create(const ptyb_scan* scan, const double* object, int32_t nobj, int32_t nyo,
+                int32_t nxo, const double* probe, int32_t nprobe, const ptyb_options* options,
+                ptyb_handle** out);
+
+/* Reference `GpuPtycho::rpie` (engine/gpu/rpie.rs:31-63). */
+int ptyb_rpie(ptyb_handle* h, const ptyb_rpie_params* params, int32_t nepoch);
+
+/* Reference `GpuPtycho::lsqml` with `ProbeVariation::none` (engine/gpu/lsqml.rs:75-121). */
+int ptyb_lsqml(ptyb_handle* h, const ptyb_lsqml_params* params, int32_t nepoch,
+               int32_t calc_llk);
+
+/* Reference `GpuPtycho::ml` (engine/gpu/ml.rs:38-83). */
+int ptyb_ml(ptyb_handle* h, const ptyb_ml_params* params, int32_t ncycle);
+
+/* Reference `GpuPtycho::llk` (engine/gpu/mod.rs:871-881): normalised LLK of the estimate. */
+int ptyb_get_llk(ptyb_handle* h, ptyb_llk* out);
+
+/* The model intensity Σ_modes |Ψ|² of the current estimate for frames[0..n) into out[n][ny][nx]
+ * in the FFT-shifted detector layout (zero frequency at [0, 0]), the far-field forward model of
+ * the reference binding's `forward` (ptyrs-py/src/cpu.rs) summed over modes. */
+int ptyb_forward_intensity(ptyb_handle* h, const int32_t* frames, int32_t n, float* out);
+
+/* Reference `GpuPtycho::{object, probe, set_object}` (engine/gpu/mod.rs:763-817). */
+int ptyb_get_object(ptyb_handle* h, double* dst);
+int ptyb_get_probe(ptyb_handle* h, double* dst);
+int ptyb_set_object(ptyb_handle* h, const double* src);
+int ptyb_set_probe(ptyb_handle* h, const double* src);
+
+/* Window corners [nframe][2] (oy, ox) of the address table (reference `AddrTable`,
+ * base/addr.rs:35-81). */
+int ptyb_corners(ptyb_handle* h, int32_t* dst);
+
+/* Reference `GpuPtycho::history` / `cycle` (engine/gpu/mod.rs:818-864). */
+int ptyb_history_len(ptyb_handle* h);
+int ptyb_history(ptyb_handle* h, ptyb_llk_record* dst, int32_t cap);
+int64_t ptyb_cycle(ptyb_handle* h);
+
+/* Reference `GpuPtycho::lsqml_steps`: the steps of the last LSQML epoch, one per frame in
+ * batch order. */
+int ptyb_lsqml_steps_len(ptyb_handle* h);
+int ptyb_lsqml_steps(ptyb_handle* h, ptyb_lsqml_step* dst, int32_t cap);
+
+/* Reference `GpuPtycho::synchronize` (engine/gpu/mod.rs:865-870). */
+int ptyb_synchronize(ptyb_handle* h);
+
+/* Host-only (no device needed): reference `random_batches` (engine/batch.rs:18-38), the
+ * frames of `epoch` in seeded sorted batches of `size`, concatenated into order[nframe]. */
+int ptyb_random_batches(int32_t nframe, int32_t size, uint64_t seed, uint64_t epoch,
+                        int32_t* order);
+
+/* Host-only: PyNX position preprocessing and the window corners [nframe][2] (oy, ox) of
+ * positions in metres on an object pixel (pixel_y, pixel_x) (reference
+ * `Positions::pynx_preprocess` + `AddrTable::new`, base/positions.rs:274-315,
+ * base/addr.rs:35-127); PTYB_INVALID when a window leaves the object. */
+int ptyb_view_corners(const double* y, const double* x, int32_t nframe, double pixel_y,
+                      double pixel_x, int32_t ny, int32_t nx, int32_t nyo, int32_t nxo,
+                      int32_t* corners);
+
+/* Per-kernel device timing: `on` resets the totals and brackets every later launch of this
+ * handle with CUDA events on its stream (kernel names by ptyb_kernel_name). */
+int ptyb_set_timing(ptyb_handle* h, int32_t on);
+int32_t ptyb_kernel_kinds(void);
+const char* ptyb_kernel_name(int32_t kind);
+int ptyb_kernel_times(ptyb_handle* h, double* ms, int64_t* launches, int32_t cap);
+
+/* Device time (ms, CUDA events on the handle's stream) of the last rPIE / LSQML / ML call. */
+double ptyb_last_call_ms(ptyb_handle* h);
+
+/* Device-side launch count of this handle's own kernels since create (observability). */
+int64_t ptyb_launches(ptyb_handle* h);
+
+const char* ptyb_last_error(ptyb_handle* h);
+void ptyb_destroy(ptyb_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PTYB200_H */

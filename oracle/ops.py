@@ -9,13 +9,23 @@ from .base import fftshift2
 
 
 # --------------------------------------------------------------------------------------
-# Unitary FFT (engine/fft.rs:155-234): numpy's `norm="ortho"`, no shift.
+# Unitary FFT (engine/fft.rs:155-234): numpy's `norm="ortho"`, no shift. With FFT_WORKERS set,
+# scipy's pocketfft splits a batch of planes over that many threads (same transforms).
+
+FFT_WORKERS = None
+
 
 def fft2(a):
+    if FFT_WORKERS:
+        import scipy.fft
+        return scipy.fft.fft2(a, axes=(-2, -1), norm="ortho", workers=FFT_WORKERS)
     return np.fft.fft2(a, axes=(-2, -1), norm="ortho")
 
 
 def ifft2(a):
+    if FFT_WORKERS:
+        import scipy.fft
+        return scipy.fft.ifft2(a, axes=(-2, -1), norm="ortho", workers=FFT_WORKERS)
     return np.fft.ifft2(a, axes=(-2, -1), norm="ortho")
 
 

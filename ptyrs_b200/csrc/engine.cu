@@ -1,0 +1,1061 @@
+// The reconstruction engine behind the C ABI (include/ptyb200.h): the device state of one
+// scan and the launch sequences of rPIE, LSQML and the LLK pass on one CUDA stream.
+//
+// Reference engine (physwkim/ptyrs): `GpuPtycho` (ptyrs/src/engine/gpu/mod.rs:533-881), rPIE
+// (engine/gpu/rpie.rs:31-63, 198-529), LSQML (engine/gpu/lsqml.rs:75-126), the LLK pass
+// (engine/gpu/device.rs:3379-3395).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/ptyb200.h"
+#include "frame.cuh"
+#include "gather.cuh"
+#include "lsqml.cuh"
+#include "scan.h"
+
+using namespace ptyb;
+
+namespace ptyb {
+
+// Counts of one frame per block, detector order in, FFT-shifted float out (engine/obs.rs:61-76):
+// masked (u16 65535, or negative) becomes -1; per-frame photon sum and unmasked count; `bad`
+// is set by a non-finite unmasked value.
+template <typename T>
+__global__ void __launch_bounds__(256) counts_kernel(const T* raw, int u16, float* iobs,
+                                                     double* power, int* nobs, int* bad, int N) {
+  __shared__ double shp[8];
+  __shared__ int shc[8];
+  const int f = blockIdx.x;
+  const size_t plane = (size_t)N * N;
+  double p = 0.0;
+  int c = 0;
+  for (int j = threadIdx.x; j < N * N; j += 256) {
+    const int jy = j / N, jx = j % N;
+    const double v = (double)raw[f * plane + (size_t)((jy + N / 2) % N) * N + (jx + N / 2) % N];
+    const bool masked = u16 ? v == 65535.0 : v < 0.0;
+    if (!masked && !isfinite(v)) *bad = 1;
+    iobs[f * plane + j] = masked ? -1.f : (float)v;
+    if (!masked) {
+      p += v;
+      ++c;
+    }
+  }
+  p = warp_sum(p);
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if (threadIdx.x % 32 == 0) {
+    shp[threadIdx.x / 32] = p;
+    shc[threadIdx.x / 32] = c;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sp = 0.0;
+    int sc = 0;
+    for (int w = 0; w < 8; ++w) {
+      sp += shp[w];
+      sc += shc[w];
+    }
+    power[f] = sp;
+    nobs[f] = sc;
+  }
+}
+
+__global__ void fill_kernel(float* x, float v, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] = v;
+}
+
+}  // namespace ptyb
+
+namespace {
+
+constexpr int kAlgRpie = 3, kAlgLsqml = 6;
+
+// One device allocation, freed with the handle.
+struct Buf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct ptyb_handle {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int P = 0, N = 0, nprobe = 0, nobj = 0, K = 0, nyo = 0, nxo = 0, C = 1, stack = 0;
+  double nb_obs = 0, obs_total = 0, max_power = 0, pixel[2] = {0, 0};
+  std::vector<int32_t> corners_h;
+  // Resident state.
+  float* iobs = nullptr;      // [P][N][N] shifted, < 0 masked
+  int2* corners = nullptr;    // [P] (oy, ox)
+  float2* object = nullptr;   // [nobj][nyo][nxo]
+  float2* probe = nullptr;    // [nprobe][N][N]
+  float2* quad = nullptr;     // [N][N]
+  float2* tw = nullptr;       // [N]
+  int* iota = nullptr;        // [P] 0..P-1
+  int* order = nullptr;       // [P] frames of one launch (forward_intensity)
+  int* order_all = nullptr;   // [order_cap] the call's epoch orders, concatenated
+  size_t order_cap = 0;
+  float* afar_all = nullptr;  // [P]
+  // Scratch, sized for `slots` frames per launch.
+  int slots = 0;
+  float2* upd = nullptr;      // [slots][K][N][N]
+  float2* field = nullptr;    // [slots][K][N][N]
+  float* icalc = nullptr;     // [slots][N][N]
+  float* omax = nullptr;      // [slots]
+  double* llk = nullptr;      // [P][4]
+  float* afar1 = nullptr;     // [slots]
+  float* afar2 = nullptr;     // [slots]
+  float2* partial = nullptr;  // [nchunk][K][N][N]
+  int max_chunks = 0;
+  float* scal = nullptr;      // [8]: pmax, pre max, object step, probe step
+  float* pre = nullptr;       // [nyo][nxo]
+  float2* d_obj = nullptr;    // [nyo][nxo]
+  float2* d_probe = nullptr;  // [K][N][N]
+  double* sums = nullptr;     // [slots][6]
+  double* steplog = nullptr;  // [P][3]
+  std::vector<Buf> bufs;
+  // Per-kernel device timing (CUDA events on the engine's stream), when enabled.
+  bool timing = false;
+  std::vector<cudaEvent_t> event_pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+  double kind_ms[32] = {0};
+  int64_t kind_n[32] = {0};
+  cudaEvent_t call_ev[2] = {nullptr, nullptr};
+  float last_call_ms = 0.f;
+  // Host state.
+  int64_t cycle = 0;
+  int64_t launches = 0;
+  std::vector<ptyb_llk_record> history;
+  std::vector<ptyb_lsqml_step> steps;
+  bool aborted = false;
+  std::string err;
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct Fail {
+  int code;
+};
+
+void check(ptyb_handle* h, cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    h->err = std::string(what) + ": " + cudaGetErrorString(e);
+    h->aborted = true;
+    throw Fail{PTYB_GPU};
+  }
+}
+
+template <typename T>
+T* alloc(ptyb_handle* h, size_t count) {
+  void* p = nullptr;
+  check(h, cudaMalloc(&p, count * sizeof(T) + 16), "cudaMalloc");
+  h->bufs.push_back({p, count * sizeof(T)});
+  return static_cast<T*>(p);
+}
+
+void launched(ptyb_handle* h, const char* what) {
+  ++h->launches;
+  check(h, cudaGetLastError(), what);
+}
+
+// Kernel kinds for the per-kernel timing (ptyb_kernel_name).
+enum Kind : int {
+  kKFrameRpie = 0, kKFrameLsqml, kKFrameMl, kKFrameLlk, kKFrameStore, kKFrameFromStore,
+  kKObjRpie, kKObjOverlap, kKObjLsqml, kKObjMl, kKIllum, kKProbePartial, kKProbeFinal,
+  kKAfar, kKDots, kKSolve, kKAxpy, kKMax, kKCounts, kKMisc, kNumKinds
+};
+const char* const kKindNames[kNumKinds] = {
+    "frame_rpie", "frame_lsqml", "frame_ml_grad", "frame_llk", "frame_store",
+    "frame_from_store", "object_rpie", "object_overlap", "object_lsqml", "object_ml",
+    "illumination", "probe_partial", "probe_finalize", "lsqml_afar", "lsqml_dots",
+    "lsqml_solve", "axpy", "max", "counts", "misc"};
+
+cudaEvent_t take_event(ptyb_handle* h) {
+  if (!h->event_pool.empty()) {
+    cudaEvent_t e = h->event_pool.back();
+    h->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  check(h, cudaEventCreate(&e), "event");
+  return e;
+}
+
+// Runs `launch` (which enqueues one kernel on the engine's stream), bracketed by events when
+// timing is on.
+template <typename F>
+void timed(ptyb_handle* h, int kind, F&& launch) {
+  if (!h->timing) {
+    launch();
+    return;
+  }
+  cudaEvent_t a = take_event(h), b = take_event(h);
+  check(h, cudaEventRecord(a, h->stream), "event");
+  launch();
+  check(h, cudaEventRecord(b, h->stream), "event");
+  h->pending.push_back({kind, {a, b}});
+}
+
+// Folds the finished launches' times into the per-kind totals (after a stream sync).
+void harvest(ptyb_handle* h) {
+  for (auto& p : h->pending) {
+    float ms = 0.f;
+    check(h, cudaEventElapsedTime(&ms, p.second.first, p.second.second), "event time");
+    h->kind_ms[p.first] += ms;
+    h->kind_n[p.first] += 1;
+    h->event_pool.push_back(p.second.first);
+    h->event_pool.push_back(p.second.second);
+  }
+  h->pending.clear();
+}
+
+// Brackets a whole algorithm call with events; `end_call` syncs and stores its device time.
+void begin_call(ptyb_handle* h) {
+  if (!h->call_ev[0]) {
+    check(h, cudaEventCreate(&h->call_ev[0]), "event");
+    check(h, cudaEventCreate(&h->call_ev[1]), "event");
+  }
+  check(h, cudaEventRecord(h->call_ev[0], h->stream), "event");
+}
+
+void end_call(ptyb_handle* h, const char* what) {
+  check(h, cudaEventRecord(h->call_ev[1], h->stream), "event");
+  check(h, cudaStreamSynchronize(h->stream), what);
+  check(h, cudaEventElapsedTime(&h->last_call_ms, h->call_ev[0], h->call_ev[1]), "event time");
+  harvest(h);
+}
+
+// Cluster size for frames of side N with K modes: the smallest that fits shared memory.
+int cluster_for(int N, int K) {
+  const size_t lim = 227 * 1024;
+  if (N == 64) return frame_smem_bytes<64, 1>(K) <= lim ? 1 : 0;
+  if (N == 128) {
+    if (frame_smem_bytes<128, 2>(K) <= lim) return 2;
+    if (frame_smem_bytes<128, 4>(K) <= lim) return 4;
+    return 0;
+  }
+  if (N == 256) return frame_smem_bytes<256, 8>(K) <= lim ? 8 : 0;
+  return 0;
+}
+
+template <int N, int C, int MODE>
+cudaError_t launch_frame_nc(const FrameArgs& a, int nslot, int K, cudaStream_t s) {
+  auto kern = frame_kernel<N, C, MODE>;
+  const size_t smem = frame_smem_bytes<N, C>(K);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nslot * C);
+  cfg.blockDim = dim3(FrameShape<N, C>::T);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = C > 1 ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kern, a);
+}
+
+template <int MODE>
+cudaError_t launch_frame_raw(ptyb_handle* h, const FrameArgs& a, int nslot) {
+  if (nslot <= 0) return cudaSuccess;
+  switch (h->N * 100 + h->C) {
+    case 6401: return launch_frame_nc<64, 1, MODE>(a, nslot, h->K, h->stream);
+    case 12802: return launch_frame_nc<128, 2, MODE>(a, nslot, h->K, h->stream);
+    case 12804: return launch_frame_nc<128, 4, MODE>(a, nslot, h->K, h->stream);
+    case 25608: return launch_frame_nc<256, 8, MODE>(a, nslot, h->K, h->stream);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <int MODE>
+cudaError_t launch_frame(ptyb_handle* h, const FrameArgs& a, int nslot) {
+  constexpr int kind = MODE == kRpie ? kKFrameRpie
+                       : MODE == kLsqmlFused ? kKFrameLsqml
+                       : MODE == kMlGrad ? kKFrameMl
+                       : MODE == kLlk ? kKFrameLlk
+                       : MODE == kStore ? kKFrameStore
+                                        : kKFrameFromStore;
+  cudaError_t e = cudaSuccess;
+  timed(h, kind, [&] { e = launch_frame_raw<MODE>(h, a, nslot); });
+  return e;
+}
+
+FrameArgs frame_args(ptyb_handle* h, const int* frames) {
+  FrameArgs a = {};
+  a.object = h->object;
+  a.probe = h->probe;
+  a.quad = h->quad;
+  a.tw = h->tw;
+  a.iobs = h->iobs;
+  a.frames = frames;
+  a.corners = h->corners;
+  a.out = h->upd;
+  a.field = h->field;
+  a.icalc = h->icalc;
+  a.omax = h->omax;
+  a.llk = h->llk;
+  a.a_far = h->afar2;
+  a.nyo = h->nyo;
+  a.nxo = h->nxo;
+  a.nprobe = h->nprobe;
+  a.nobj = h->nobj;
+  a.cost = kCostPoisson;
+  return a;
+}
+
+GatherArgs gather_args(ptyb_handle* h, const int* frames, int nslot) {
+  GatherArgs g = {};
+  g.object = h->object;
+  g.probe = h->probe;
+  g.quad = h->quad;
+  g.upd = h->upd;
+  g.frames = frames;
+  g.corners = h->corners;
+  g.pmax = h->scal + 0;
+  g.pre = h->pre;
+  g.pre_max = h->scal + 1;
+  g.out = h->d_obj;
+  g.nslot = nslot;
+  g.nyo = h->nyo;
+  g.nxo = h->nxo;
+  g.nprobe = h->nprobe;
+  g.N = h->N;
+  return g;
+}
+
+int ntiles(ptyb_handle* h) {
+  return ((h->nyo + kTile - 1) / kTile) * ((h->nxo + kTile - 1) / kTile);
+}
+
+// Scratch for `n` frames per launch.
+void ensure_slots(ptyb_handle* h, int n) {
+  if (n <= h->slots) return;
+  const size_t plane = (size_t)h->N * h->N;
+  h->upd = alloc<float2>(h, (size_t)n * h->K * plane);
+  h->field = alloc<float2>(h, (size_t)n * h->K * plane);
+  h->icalc = alloc<float>(h, (size_t)n * plane);
+  h->omax = alloc<float>(h, n);
+  h->afar1 = alloc<float>(h, n);
+  h->afar2 = alloc<float>(h, n);
+  h->sums = alloc<double>(h, (size_t)n * 6);
+  h->slots = n;
+}
+
+// Probe-pass chunking: about 2 CTAs per SM over the probe pixels.
+int probe_chunk(ptyb_handle* h, int nslot, int* nchunk) {
+  const int pixblocks = (h->N * h->N + 255) / 256;
+  int want = std::max(1, 296 / pixblocks);
+  int chunk = std::max(1, (nslot + want - 1) / want);
+  *nchunk = (nslot + chunk - 1) / chunk;
+  if (*nchunk > h->max_chunks) {
+    h->partial = alloc<float2>(h, (size_t)(*nchunk) * h->K * h->N * h->N);
+    h->max_chunks = *nchunk;
+  }
+  return chunk;
+}
+
+// Σ_frames (w·upd) into the probe (mode 0: P += coef·Σ with the rPIE weight; 1: d_probe =
+// coef·Σ conj(q·O)·upd).
+void probe_pass(ptyb_handle* h, const int* frames, int nslot, int mode, float alpha, float coef) {
+  int nchunk = 0;
+  const int chunk = probe_chunk(h, nslot, &nchunk);
+  ProbeArgs p = {};
+  p.object = h->object;
+  p.quad = h->quad;
+  p.upd = h->upd;
+  p.frames = frames;
+  p.corners = h->corners;
+  p.omax = h->omax;
+  p.partial = h->partial;
+  p.alpha = alpha;
+  p.nslot = nslot;
+  p.chunk = chunk;
+  p.nxo = h->nxo;
+  p.K = h->K;
+  p.N = h->N;
+  p.mode = mode == 0 ? 0 : 1;
+  dim3 grid((h->N * h->N + 255) / 256, nchunk);
+  timed(h, kKProbePartial, [&] { probe_partial_kernel<<<grid, 256, 0, h->stream>>>(p); });
+  launched(h, "probe_partial");
+  const int count = h->K * h->N * h->N;
+  timed(h, kKProbeFinal, [&] {
+  probe_finalize_kernel<<<(count + 255) / 256, 256, 0, h->stream>>>(
+      h->partial, nchunk, count, h->probe, h->d_probe, nullptr, coef, mode);
+  });
+  launched(h, "probe_finalize");
+}
+
+// The LLK of the current estimate over every frame: per-frame sums in frame order.
+ptyb_llk llk_pass(ptyb_handle* h) {
+  const int stack = std::min(h->P, h->stack);
+  ensure_slots(h, stack);
+  for (int s0 = 0; s0 < h->P; s0 += stack) {
+    const int n = std::min(stack, h->P - s0);
+    FrameArgs a = frame_args(h, h->iota + s0);
+    a.llk = h->llk + (size_t)s0 * 4;
+    check(h, launch_frame<kLlk>(h, a, n), "llk pass");
+    ++h->launches;
+  }
+  std::vector<double> v((size_t)h->P * 4);
+  check(h, cudaMemcpyAsync(v.data(), h->llk, v.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                           h->stream),
+        "llk download");
+  check(h, cudaStreamSynchronize(h->stream), "llk pass");
+  double s[4] = {0, 0, 0, 0};
+  for (int f = 0; f < h->P; ++f)
+    for (int k = 0; k < 4; ++k) s[k] += v[(size_t)f * 4 + k];
+  ptyb_llk l;
+  l.poisson = s[0] / h->nb_obs;
+  l.gaussian = s[1] / h->nb_obs;
+  l.euclidian = s[2] / h->nb_obs;
+  l.nb_photons_calc = s[3];
+  return l;
+}
+
+void record(ptyb_handle* h, int algorithm, const ptyb_llk& l) {
+  ptyb_llk_record r = {};
+  r.cycle = h->cycle;
+  r.algorithm = algorithm;
+  r.llk = l;
+  h->history.push_back(r);
+}
+
+bool llk_due(int calc_llk, int ic, int ncycle) {
+  return calc_llk > 0 && (ic % calc_llk == 0 || ic + 1 == ncycle);
+}
+
+// Every epoch's batch order of a call, computed on the host and uploaded once before the
+// call's first launch; sizes[e] holds epoch e's batch lengths.
+void upload_orders(ptyb_handle* h, int nepoch, int size, uint64_t seed, int64_t epoch0,
+                   std::vector<std::vector<int32_t>>* sizes, std::vector<int32_t>* last) {
+  std::vector<int32_t> all, order, sz;
+  all.reserve((size_t)nepoch * h->P);
+  sizes->clear();
+  for (int e = 0; e < nepoch; ++e) {
+    random_batches(h->P, size, seed, (uint64_t)(epoch0 + e), &order, &sz);
+    all.insert(all.end(), order.begin(), order.end());
+    sizes->push_back(sz);
+  }
+  if (last) *last = order;
+  if (all.size() > h->order_cap) {
+    h->order_all = alloc<int>(h, all.size());
+    h->order_cap = all.size();
+  }
+  if (!all.empty())
+    check(h, cudaMemcpy(h->order_all, all.data(), all.size() * sizeof(int32_t),
+                        cudaMemcpyHostToDevice),
+          "order upload");
+}
+
+// One rPIE batch (engine/ptycho.rs:904-1085; GPU launch sequence engine/gpu/rpie.rs:239-345).
+void rpie_batch(ptyb_handle* h, const ptyb_rpie_params& p, const int* frames, int nslot) {
+  FrameArgs a = frame_args(h, frames);
+  check(h, launch_frame<kRpie>(h, a, nslot), "rpie frame pass");
+  ++h->launches;
+  GatherArgs g = gather_args(h, frames, nslot);
+  if (p.update_object) {
+    check(h, cudaMemsetAsync(h->scal, 0, sizeof(float), h->stream), "memset");
+    timed(h, kKObjOverlap, [&] { object_tile_kernel<kGatherOverlap><<<ntiles(h), 1024, 0, h->stream>>>(g); });
+    launched(h, "overlap max");
+  }
+  if (p.update_probe) {
+    // Reads the batch-start object, so it runs before the object update.
+    int nchunk = 0;
+    const int chunk = probe_chunk(h, nslot, &nchunk);
+    ProbeArgs pa = {};
+    pa.object = h->object;
+    pa.quad = h->quad;
+    pa.upd = h->upd;
+    pa.frames = frames;
+    pa.corners = h->corners;
+    pa.omax = h->omax;
+    pa.partial = h->partial;
+    pa.alpha = (float)p.probe_alpha;
+    pa.nslot = nslot;
+    pa.chunk = chunk;
+    pa.nxo = h->nxo;
+    pa.K = h->K;
+    pa.N = h->N;
+    pa.mode = 0;
+    dim3 grid((h->N * h->N + 255) / 256, nchunk);
+    timed(h, kKProbePartial, [&] { probe_partial_kernel<<<grid, 256, 0, h->stream>>>(pa); });
+    launched(h, "probe partial");
+    if (p.update_object) {
+      g.alpha = (float)p.obj_alpha;
+      g.step = (float)p.obj_step;
+      timed(h, kKObjRpie, [&] { object_tile_kernel<kGatherRpie><<<ntiles(h), 1024, 0, h->stream>>>(g); });
+      launched(h, "object update");
+    }
+    const int count = h->K * h->N * h->N;
+    timed(h, kKProbeFinal, [&] {
+    probe_finalize_kernel<<<(count + 255) / 256, 256, 0, h->stream>>>(
+        h->partial, nchunk, count, h->probe, nullptr, nullptr,
+        (float)(p.probe_step / nslot), 0);
+    });
+    launched(h, "probe update");
+  } else if (p.update_object) {
+    g.alpha = (float)p.obj_alpha;
+    g.step = (float)p.obj_step;
+    timed(h, kKObjRpie, [&] { object_tile_kernel<kGatherRpie><<<ntiles(h), 1024, 0, h->stream>>>(g); });
+    launched(h, "object update");
+  }
+}
+
+// The preconditioner over every view on pty-chi's schedule (engine/lsqml.rs:676-700).
+void lsqml_preconditioner(ptyb_handle* h, bool init) {
+  GatherArgs g = gather_args(h, h->iota, h->P);
+  g.pre_scale = init ? (float)(h->max_power / (4.0 * h->N * h->N * ((double)h->N * h->N))) : -1.f;
+  timed(h, kKIllum, [&] { object_tile_kernel<kGatherIllum><<<ntiles(h), 1024, 0, h->stream>>>(g); });
+  launched(h, "illumination");
+  check(h, cudaMemsetAsync(h->scal + 1, 0, sizeof(float), h->stream), "memset");
+  const size_t n = (size_t)h->nyo * h->nxo;
+  timed(h, kKMax, [&] { max_kernel<<<296, 256, 0, h->stream>>>(h->pre, n, h->scal + 1); });
+  launched(h, "pre max");
+}
+
+// One LSQML step on a batch (engine/lsqml.rs:581-643).
+void lsqml_batch(ptyb_handle* h, const ptyb_lsqml_params& p, const int* frames, int nslot,
+                 double* log) {
+  FrameArgs a = frame_args(h, frames);
+  a.cost = p.cost;
+  if (p.cost == PTYB_COST_POISSON) {
+    check(h, launch_frame<kStore>(h, a, nslot), "lsqml forward");
+    ++h->launches;
+    timed(h, kKAfar, [&] {
+    afar_kernel<<<nslot, 256, 0, h->stream>>>(h->icalc, h->iobs, frames, h->afar_all, 1, h->afar1,
+                                               nslot, h->N * h->N);
+    });
+    launched(h, "a_far pass 1");
+    timed(h, kKAfar, [&] {
+    afar_kernel<<<nslot, 256, 0, h->stream>>>(h->icalc, h->iobs, frames, h->afar1, 0, h->afar2,
+                                               nslot, h->N * h->N);
+    });
+    launched(h, "a_far pass 2");
+    check(h, launch_frame<kFromStore>(h, a, nslot), "lsqml backward");
+    ++h->launches;
+  } else {
+    timed(h, kKMisc, [&] {
+      fill_kernel<<<(nslot + 255) / 256, 256, 0, h->stream>>>(h->afar2, 0.5f, nslot);
+    });
+    launched(h, "a_far");
+    check(h, launch_frame<kLsqmlFused>(h, a, nslot), "lsqml pass");
+    ++h->launches;
+  }
+  GatherArgs g = gather_args(h, frames, nslot);
+  timed(h, kKObjLsqml, [&] { object_tile_kernel<kGatherLsqml><<<ntiles(h), 1024, 0, h->stream>>>(g); });
+  launched(h, "object direction");
+  probe_pass(h, frames, nslot, 1, 0.f, 1.0f / nslot);
+  const double lambda0 = 1.2e-7 * ((double)h->N * h->N) / ((double)h->N * h->N);
+  timed(h, kKDots, [&] {
+  lsqml_dots_kernel<<<nslot, 256, 0, h->stream>>>(h->object, h->d_obj, h->probe, h->d_probe,
+                                                   h->quad, h->upd, frames, h->corners, h->nxo,
+                                                   h->K, h->N, lambda0, h->sums);
+  });
+  launched(h, "step sums");
+  timed(h, kKSolve, [&] {
+  lsqml_solve_kernel<<<1, 1024, 0, h->stream>>>(h->sums, nslot, (double)(1 * h->K), h->afar2,
+                                                 frames, h->afar_all, log, h->scal + 2);
+  });
+  launched(h, "step solve");
+  const size_t no = (size_t)h->nyo * h->nxo, np = (size_t)h->K * h->N * h->N;
+  timed(h, kKAxpy, [&] {
+  axpy_scal_kernel<<<(unsigned)((no + 255) / 256), 256, 0, h->stream>>>(h->object, h->d_obj,
+                                                                       h->scal + 2, 0, no);
+  });
+  launched(h, "object step");
+  timed(h, kKAxpy, [&] {
+  axpy_scal_kernel<<<(unsigned)((np + 255) / 256), 256, 0, h->stream>>>(h->probe, h->d_probe,
+                                                                       h->scal + 2, 1, np);
+  });
+  launched(h, "probe step");
+}
+
+void to_c64(const float2* src, double* dst, size_t n) {
+  for (size_t i = 0; i < n; ++i) {
+    dst[2 * i] = src[i].x;
+    dst[2 * i + 1] = src[i].y;
+  }
+}
+
+std::vector<float2> from_c64(const double* src, size_t n) {
+  std::vector<float2> v(n);
+  for (size_t i = 0; i < n; ++i) v[i] = make_float2((float)src[2 * i], (float)src[2 * i + 1]);
+  return v;
+}
+
+template <typename F>
+int guarded(ptyb_handle* h, bool enqueues, F&& body) {
+  if (!h) return PTYB_INVALID;
+  if (enqueues && h->aborted) {
+    h->err = "an earlier call failed part-way; the state is poisoned";
+    return PTYB_ABORTED;
+  }
+  try {
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e != cudaSuccess) {
+      h->err = std::string("cudaSetDevice: ") + cudaGetErrorString(e);
+      if (enqueues) h->aborted = true;
+      return PTYB_GPU;
+    }
+    return body();
+  } catch (const Fail& f) {
+    return f.code;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int ptyb_create(const ptyb_scan* scan, const double* object, int32_t nobj, int32_t nyo,
+                int32_t nxo, const double* probe, int32_t nprobe, const ptyb_options* options,
+                ptyb_handle** out) {
+  if (!out) return PTYB_INVALID;
+  *out = nullptr;
+  if (!scan || !object || !probe || !scan->counts || !scan->pos_y || !scan->pos_x)
+    return PTYB_INVALID;
+  const int N = scan->ny;
+  g_create_error.clear();
+  if (scan->nx != N || !(N == 64 || N == 128 || N == 256)) {
+    g_create_error = "frames must be square with a side of 64, 128 or 256";
+    return PTYB_INVALID;
+  }
+  if (scan->nframe <= 0 || nprobe <= 0 || nprobe > kMaxModes || nobj != 1 || nyo < N || nxo < N) {
+    g_create_error = "need frames, 1-4 probe modes, one object mode and an object >= the frame";
+    return PTYB_INVALID;
+  }
+  if (!(scan->wavelength > 0 && scan->distance > 0 && scan->detector_pixel > 0)) {
+    g_create_error = "wavelength, distance and detector pixel must be > 0";
+    return PTYB_INVALID;
+  }
+  const int K = nprobe * nobj;
+  const int C = cluster_for(N, K);
+  if (C == 0) {
+    g_create_error = "the frame's modes do not fit one cluster's shared memory";
+    return PTYB_INVALID;
+  }
+  auto* h = new ptyb_handle();
+  h->device = options ? options->device : 0;
+  h->P = scan->nframe;
+  h->N = N;
+  h->nprobe = nprobe;
+  h->nobj = nobj;
+  h->K = K;
+  h->nyo = nyo;
+  h->nxo = nxo;
+  h->C = C;
+  h->stack = options && options->stack_size > 0 ? options->stack_size : 64;
+  // Positions: PyNX preprocessing and window corners (base/positions.rs, base/addr.rs).
+  const double lz = scan->wavelength * scan->distance;
+  h->pixel[0] = lz / (N * scan->detector_pixel);
+  h->pixel[1] = lz / (N * scan->detector_pixel);
+  std::vector<double> y(scan->pos_y, scan->pos_y + h->P), x(scan->pos_x, scan->pos_x + h->P);
+  for (int f = 0; f < h->P; ++f)
+    if (!std::isfinite(y[f]) || !std::isfinite(x[f]) || std::fabs(y[f]) > 1e10 ||
+        std::fabs(x[f]) > 1e10) {
+      g_create_error = "positions must be finite with |pos| <= 1e10";
+      delete h;
+      return PTYB_INVALID;
+    }
+  const std::vector<double> py = pynx_axis(y, h->pixel[0]), px = pynx_axis(x, h->pixel[1]);
+  if (!corners_of(py, px, h->pixel, N, N, nyo, nxo, &h->corners_h, &g_create_error)) {
+    delete h;
+    return PTYB_INVALID;
+  }
+  int rc = guarded(h, true, [&]() -> int {
+    check(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
+    // Observed intensities in the FFT-shifted layout (engine/obs.rs:61-76), converted on the
+    // device from the raw counts.
+    const size_t plane = (size_t)N * N, nval = (size_t)h->P * plane;
+    const size_t esize = scan->counts_kind == PTYB_COUNTS_U16   ? 2
+                         : scan->counts_kind == PTYB_COUNTS_F32 ? 4
+                                                                : 8;
+    h->iobs = alloc<float>(h, nval);
+    void* raw = nullptr;
+    check(h, cudaMalloc(&raw, nval * esize), "cudaMalloc");
+    double* power = alloc<double>(h, h->P);
+    int* nobs = alloc<int>(h, h->P + 1);
+    check(h, cudaMemset(nobs, 0, (h->P + 1) * sizeof(int)), "memset");
+    cudaError_t e = cudaMemcpy(raw, scan->counts, nval * esize, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+      if (scan->counts_kind == PTYB_COUNTS_U16)
+        counts_kernel<<<h->P, 256, 0, h->stream>>>(static_cast<const uint16_t*>(raw), 1, h->iobs,
+                                                   power, nobs, nobs + h->P, N);
+      else if (scan->counts_kind == PTYB_COUNTS_F32)
+        counts_kernel<<<h->P, 256, 0, h->stream>>>(static_cast<const float*>(raw), 0, h->iobs,
+                                                   power, nobs, nobs + h->P, N);
+      else
+        counts_kernel<<<h->P, 256, 0, h->stream>>>(static_cast<const double*>(raw), 0, h->iobs,
+                                                   power, nobs, nobs + h->P, N);
+      e = cudaGetLastError();
+      ++h->launches;
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(raw);
+    check(h, e, "counts upload");
+    std::vector<double> pw(h->P);
+    std::vector<int> nb(h->P + 1);
+    check(h, cudaMemcpy(pw.data(), power, h->P * sizeof(double), cudaMemcpyDeviceToHost), "counts");
+    check(h, cudaMemcpy(nb.data(), nobs, (h->P + 1) * sizeof(int), cudaMemcpyDeviceToHost), "counts");
+    if (nb[h->P]) {
+      h->err = "counts must be finite";
+      return PTYB_INVALID;
+    }
+    for (int f = 0; f < h->P; ++f) {
+      h->obs_total += pw[f];
+      h->max_power = std::max(h->max_power, pw[f]);
+      h->nb_obs += nb[f];
+    }
+    h->corners = alloc<int2>(h, h->P);
+    check(h, cudaMemcpy(h->corners, h->corners_h.data(), h->P * sizeof(int2), cudaMemcpyHostToDevice),
+          "corners upload");
+    h->object = alloc<float2>(h, (size_t)nobj * nyo * nxo);
+    auto o = from_c64(object, (size_t)nobj * nyo * nxo);
+    check(h, cudaMemcpy(h->object, o.data(), o.size() * sizeof(float2), cudaMemcpyHostToDevice),
+          "object upload");
+    h->probe = alloc<float2>(h, (size_t)nprobe * plane);
+    auto pr = from_c64(probe, (size_t)nprobe * plane);
+    check(h, cudaMemcpy(h->probe, pr.data(), pr.size() * sizeof(float2), cudaMemcpyHostToDevice),
+          "probe upload");
+    // Far-field plane phase (engine/ops.rs:17-33) and the FFT twiddles, in double.
+    std::vector<float2> q(plane), tw(N);
+    const double fq = M_PI / (scan->wavelength * scan->distance);
+    for (int yy = 0; yy < N; ++yy)
+      for (int xx = 0; xx < N; ++xx) {
+        const double dy = (double)yy - (double)(N / 2), dx = (double)xx - (double)(N / 2);
+        const double ph =
+            fq * (dx * dx * h->pixel[1] * h->pixel[1] + dy * dy * h->pixel[0] * h->pixel[0]);
+        q[(size_t)yy * N + xx] = make_float2((float)std::cos(ph), (float)std::sin(ph));
+      }
+    for (int t = 0; t < N; ++t)
+      tw[t] = make_float2((float)std::cos(2.0 * M_PI * t / N), (float)-std::sin(2.0 * M_PI * t / N));
+    h->quad = alloc<float2>(h, plane);
+    check(h, cudaMemcpy(h->quad, q.data(), plane * sizeof(float2), cudaMemcpyHostToDevice), "quad");
+    h->tw = alloc<float2>(h, N);
+    check(h, cudaMemcpy(h->tw, tw.data(), N * sizeof(float2), cudaMemcpyHostToDevice), "tw");
+    std::vector<int> iota(h->P);
+    for (int f = 0; f < h->P; ++f) iota[f] = f;
+    h->iota = alloc<int>(h, h->P);
+    check(h, cudaMemcpy(h->iota, iota.data(), h->P * sizeof(int), cudaMemcpyHostToDevice), "iota");
+    h->order = alloc<int>(h, h->P);
+    h->afar_all = alloc<float>(h, h->P);
+    h->llk = alloc<double>(h, (size_t)h->P * 4);
+    h->scal = alloc<float>(h, 8);
+    h->pre = alloc<float>(h, (size_t)nyo * nxo);
+    h->d_obj = alloc<float2>(h, (size_t)nyo * nxo);
+    h->d_probe = alloc<float2>(h, (size_t)K * plane);
+    h->steplog = alloc<double>(h, (size_t)h->P * 3);
+    check(h, cudaMemset(h->scal, 0, 8 * sizeof(float)), "memset");
+    return PTYB_OK;
+  });
+  if (rc != PTYB_OK) {
+    g_create_error = h->err;
+    ptyb_destroy(h);
+    return rc;
+  }
+  *out = h;
+  return PTYB_OK;
+}
+
+int ptyb_rpie(ptyb_handle* h, const ptyb_rpie_params* p, int32_t nepoch) {
+  if (!h || !p) return PTYB_INVALID;
+  if (p->batch_size <= 0 || nepoch < 0) {
+    h->err = "rPIE batch_size must be >= 1";
+    return PTYB_INVALID;
+  }
+  if (h->nobj != 1) {
+    h->err = "rPIE needs exactly one object mode";
+    return PTYB_INVALID;
+  }
+  return guarded(h, true, [&]() -> int {
+    const int bs = std::min(p->batch_size, h->P);
+    ensure_slots(h, std::max(bs, std::min(h->P, h->stack)));
+    std::vector<std::vector<int32_t>> sizes;
+    upload_orders(h, nepoch, p->batch_size, p->seed, h->cycle, &sizes, nullptr);
+    begin_call(h);
+    for (int ic = 0; ic < nepoch; ++ic) {
+      const int* order = h->order_all + (size_t)ic * h->P;
+      int off = 0;
+      for (int n : sizes[ic]) {
+        rpie_batch(h, *p, order + off, n);
+        off += n;
+      }
+      if (llk_due(p->calc_llk, ic, nepoch)) record(h, kAlgRpie, llk_pass(h));
+      ++h->cycle;
+    }
+    end_call(h, "rpie");
+    return PTYB_OK;
+  });
+}
+
+int ptyb_lsqml(ptyb_handle* h, const ptyb_lsqml_params* p, int32_t nepoch, int32_t calc_llk) {
+  if (!h || !p) return PTYB_INVALID;
+  if (p->batch_size <= 0 || nepoch < 0 ||
+      !(p->cost == PTYB_COST_POISSON || p->cost == PTYB_COST_AMPLITUDE)) {
+    h->err = "LSQML batch_size must be >= 1 and cost poisson or amplitude";
+    return PTYB_INVALID;
+  }
+  if (std::min(p->batch_size, h->P) > 1024) {
+    h->err = "LSQML batches of more than 1024 frames are not supported";
+    return PTYB_INVALID;
+  }
+  return guarded(h, true, [&]() -> int {
+    const int size = std::min(p->batch_size, h->P);
+    ensure_slots(h, std::max(size, std::min(h->P, h->stack)));
+    std::vector<std::vector<int32_t>> sizes;
+    std::vector<int32_t> last;
+    // A fresh run: epochs from 0 (engine/gpu/lsqml.rs:97-105).
+    upload_orders(h, nepoch, size, p->seed, 0, &sizes, &last);
+    begin_call(h);
+    timed(h, kKMisc, [&] {
+      fill_kernel<<<(h->P + 255) / 256, 256, 0, h->stream>>>(h->afar_all, 0.5f, h->P);
+    });
+    launched(h, "a_far");
+    for (int ic = 0; ic < nepoch; ++ic) {
+      if (ic < 10 || ic % 10 == 0) lsqml_preconditioner(h, ic == 0);
+      const int* order = h->order_all + (size_t)ic * h->P;
+      int off = 0;
+      for (int n : sizes[ic]) {
+        lsqml_batch(h, *p, order + off, n, h->steplog + (size_t)off * 3);
+        off += n;
+      }
+      if (llk_due(calc_llk, ic, nepoch)) record(h, kAlgLsqml, llk_pass(h));
+      ++h->cycle;
+    }
+    end_call(h, "lsqml");
+    // The last epoch's steps, for `ptyb_lsqml_steps`.
+    h->steps.clear();
+    if (nepoch > 0) {
+      std::vector<double> log((size_t)h->P * 3);
+      check(h, cudaMemcpy(log.data(), h->steplog, log.size() * sizeof(double),
+                          cudaMemcpyDeviceToHost),
+            "steps");
+      int b = 0, o = 0;
+      for (int n : sizes.back()) {
+        for (int i = 0; i < n; ++i) {
+          ptyb_lsqml_step st;
+          st.batch = b;
+          st.frame = last[o + i];
+          st.a_far = log[(size_t)(o + i) * 3];
+          st.a_obj = log[(size_t)(o + i) * 3 + 1];
+          st.a_probe = log[(size_t)(o + i) * 3 + 2];
+          h->steps.push_back(st);
+        }
+        o += n;
+        ++b;
+      }
+    }
+    return PTYB_OK;
+  });
+}
+
+int ptyb_ml(ptyb_handle* h, const ptyb_ml_params* p, int32_t ncycle) {
+  if (!h || !p) return PTYB_INVALID;
+  h->err = "ML is not built in this library version";
+  return PTYB_INVALID;
+}
+
+int ptyb_get_llk(ptyb_handle* h, ptyb_llk* out) {
+  if (!h || !out) return PTYB_INVALID;
+  return guarded(h, true, [&]() -> int {
+    *out = llk_pass(h);
+    return PTYB_OK;
+  });
+}
+
+int ptyb_forward_intensity(ptyb_handle* h, const int32_t* frames, int32_t n, float* out) {
+  if (!h || !frames || !out || n < 0) return PTYB_INVALID;
+  for (int i = 0; i < n; ++i)
+    if (frames[i] < 0 || frames[i] >= h->P) {
+      h->err = "frame index out of range";
+      return PTYB_INVALID;
+    }
+  return guarded(h, true, [&]() -> int {
+    const int stack = std::min(h->P, h->stack);
+    ensure_slots(h, stack);
+    const size_t plane = (size_t)h->N * h->N;
+    for (int s0 = 0; s0 < n; s0 += stack) {
+      const int m = std::min(stack, n - s0);
+      check(h, cudaMemcpyAsync(h->order, frames + s0, m * sizeof(int32_t), cudaMemcpyHostToDevice,
+                               h->stream),
+            "frames");
+      FrameArgs a = frame_args(h, h->order);
+      check(h, launch_frame<kStore>(h, a, m), "forward");
+      ++h->launches;
+      check(h, cudaMemcpyAsync(out + (size_t)s0 * plane, h->icalc, m * plane * sizeof(float),
+                               cudaMemcpyDeviceToHost, h->stream),
+            "intensity");
+      check(h, cudaStreamSynchronize(h->stream), "forward");
+    }
+    return PTYB_OK;
+  });
+}
+
+int ptyb_get_object(ptyb_handle* h, double* dst) {
+  if (!h || !dst) return PTYB_INVALID;
+  return guarded(h, false, [&]() -> int {
+    const size_t n = (size_t)h->nobj * h->nyo * h->nxo;
+    std::vector<float2> v(n);
+    check(h, cudaStreamSynchronize(h->stream), "sync");
+    check(h, cudaMemcpy(v.data(), h->object, n * sizeof(float2), cudaMemcpyDeviceToHost), "object");
+    to_c64(v.data(), dst, n);
+    return PTYB_OK;
+  });
+}
+
+int ptyb_get_probe(ptyb_handle* h, double* dst) {
+  if (!h || !dst) return PTYB_INVALID;
+  return guarded(h, false, [&]() -> int {
+    const size_t n = (size_t)h->nprobe * h->N * h->N;
+    std::vector<float2> v(n);
+    check(h, cudaStreamSynchronize(h->stream), "sync");
+    check(h, cudaMemcpy(v.data(), h->probe, n * sizeof(float2), cudaMemcpyDeviceToHost), "probe");
+    to_c64(v.data(), dst, n);
+    return PTYB_OK;
+  });
+}
+
+int ptyb_set_object(ptyb_handle* h, const double* src) {
+  if (!h || !src) return PTYB_INVALID;
+  return guarded(h, true, [&]() -> int {
+    const size_t n = (size_t)h->nobj * h->nyo * h->nxo;
+    auto v = from_c64(src, n);
+    check(h, cudaStreamSynchronize(h->stream), "sync");
+    check(h, cudaMemcpy(h->object, v.data(), n * sizeof(float2), cudaMemcpyHostToDevice), "object");
+    return PTYB_OK;
+  });
+}
+
+int ptyb_set_probe(ptyb_handle* h, const double* src) {
+  if (!h || !src) return PTYB_INVALID;
+  return guarded(h, true, [&]() -> int {
+    const size_t n = (size_t)h->nprobe * h->N * h->N;
+    auto v = from_c64(src, n);
+    check(h, cudaStreamSynchronize(h->stream), "sync");
+    check(h, cudaMemcpy(h->probe, v.data(), n * sizeof(float2), cudaMemcpyHostToDevice), "probe");
+    return PTYB_OK;
+  });
+}
+
+int ptyb_corners(ptyb_handle* h, int32_t* dst) {
+  if (!h || !dst) return PTYB_INVALID;
+  std::memcpy(dst, h->corners_h.data(), h->corners_h.size() * sizeof(int32_t));
+  return PTYB_OK;
+}
+
+int ptyb_history_len(ptyb_handle* h) { return h ? (int)h->history.size() : 0; }
+
+int ptyb_history(ptyb_handle* h, ptyb_llk_record* dst, int32_t cap) {
+  if (!h || (!dst && cap > 0)) return PTYB_INVALID;
+  const int n = std::min<int>(cap, (int)h->history.size());
+  for (int i = 0; i < n; ++i) dst[i] = h->history[i];
+  return PTYB_OK;
+}
+
+int64_t ptyb_cycle(ptyb_handle* h) { return h ? h->cycle : 0; }
+
+int ptyb_lsqml_steps_len(ptyb_handle* h) { return h ? (int)h->steps.size() : 0; }
+
+int ptyb_lsqml_steps(ptyb_handle* h, ptyb_lsqml_step* dst, int32_t cap) {
+  if (!h || (!dst && cap > 0)) return PTYB_INVALID;
+  const int n = std::min<int>(cap, (int)h->steps.size());
+  for (int i = 0; i < n; ++i) dst[i] = h->steps[i];
+  return PTYB_OK;
+}
+
+int ptyb_synchronize(ptyb_handle* h) {
+  if (!h) return PTYB_INVALID;
+  return guarded(h, false, [&]() -> int {
+    check(h, cudaStreamSynchronize(h->stream), "synchronize");
+    return PTYB_OK;
+  });
+}
+
+int64_t ptyb_launches(ptyb_handle* h) { return h ? h->launches : 0; }
+
+int ptyb_set_timing(ptyb_handle* h, int32_t on) {
+  if (!h) return PTYB_INVALID;
+  return guarded(h, false, [&]() -> int {
+    check(h, cudaStreamSynchronize(h->stream), "sync");
+    harvest(h);
+    h->timing = on != 0;
+    for (int k = 0; k < kNumKinds; ++k) {
+      h->kind_ms[k] = 0.0;
+      h->kind_n[k] = 0;
+    }
+    return PTYB_OK;
+  });
+}
+
+int32_t ptyb_kernel_kinds(void) { return kNumKinds; }
+
+const char* ptyb_kernel_name(int32_t kind) {
+  return kind >= 0 && kind < kNumKinds ? kKindNames[kind] : "";
+}
+
+int ptyb_kernel_times(ptyb_handle* h, double* ms, int64_t* launches, int32_t cap) {
+  if (!h || !ms || !launches) return PTYB_INVALID;
+  for (int k = 0; k < std::min<int>(cap, kNumKinds); ++k) {
+    ms[k] = h->kind_ms[k];
+    launches[k] = h->kind_n[k];
+  }
+  return PTYB_OK;
+}
+
+double ptyb_last_call_ms(ptyb_handle* h) { return h ? h->last_call_ms : 0.0; }
+
+int ptyb_random_batches(int32_t nframe, int32_t size, uint64_t seed, uint64_t epoch,
+                        int32_t* order) {
+  if (nframe < 0 || size <= 0 || (!order && nframe > 0)) return PTYB_INVALID;
+  std::vector<int32_t> o, sizes;
+  random_batches(nframe, size, seed, epoch, &o, &sizes);
+  std::memcpy(order, o.data(), o.size() * sizeof(int32_t));
+  return PTYB_OK;
+}
+
+int ptyb_view_corners(const double* y, const double* x, int32_t nframe, double pixel_y,
+                      double pixel_x, int32_t ny, int32_t nx, int32_t nyo, int32_t nxo,
+                      int32_t* corners) {
+  if (nframe < 0 || !y || !x || !corners) return PTYB_INVALID;
+  const double pixel[2] = {pixel_y, pixel_x};
+  std::vector<double> yy(y, y + nframe), xx(x, x + nframe);
+  std::vector<int32_t> c;
+  std::string err;
+  if (!corners_of(pynx_axis(yy, pixel_y), pynx_axis(xx, pixel_x), pixel, ny, nx, nyo, nxo, &c,
+                  &err)) {
+    g_create_error = err;
+    return PTYB_INVALID;
+  }
+  std::memcpy(corners, c.data(), c.size() * sizeof(int32_t));
+  return PTYB_OK;
+}
+
+const char* ptyb_last_error(ptyb_handle* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+void ptyb_destroy(ptyb_handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (auto& b : h->bufs) cudaFree(b.p);
+  for (auto e : h->event_pool) cudaEventDestroy(e);
+  for (auto& p : h->pending) {
+    cudaEventDestroy(p.second.first);
+    cudaEventDestroy(p.second.second);
+  }
+  for (auto e : h->call_ev)
+    if (e) cudaEventDestroy(e);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+}  // extern "C"

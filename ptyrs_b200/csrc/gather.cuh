@@ -1,0 +1,232 @@
+// Deterministic scatter-adds of the per-view updates onto the object and the probe.
+//
+// Object: one CTA owns a 32×32 object tile, lists the launch's views that overlap it in
+// ascending slot order (the reference's view order) and accumulates every pixel of the tile
+// over that list with Kahan-compensated float sums, so no atomics touch the object and the
+// result does not depend on scheduling (the reference's tile-owned gather,
+// ptyrs-kernels/src/lib.rs:388-437; operator engine/ops.rs:282-310). Probe: the slots are cut
+// into chunks, each CTA sums one chunk in slot order for 256 probe pixels, and a second pass
+// adds the chunk sums in chunk order (engine/ops.rs:315-345).
+#pragma once
+#include "common.cuh"
+
+namespace ptyb {
+
+constexpr int kTile = 32;
+constexpr int kMaxModes = 4;
+
+enum GatherMode : int {
+  kGatherRpie = 0,   // O += step·Σ_m num_m / ((1−α)·D_m + α·pmax)
+  kGatherLsqml = 1,  // d_obj = Σ conj(q·P)·χ / √(pre² + floor²)
+  kGatherMl = 2,     // grad += Σ conj(q·P)·g (compensated across launches)
+  kGatherOverlap = 3,  // pmax = max over pixels of Σ_m D_m
+  kGatherIllum = 4,    // pre = (pre + I)/2 with I = Σ|P|² over every view
+};
+
+struct GatherArgs {
+  float2* object;          // [nyo][nxo] object mode 0 (rPIE updates it)
+  const float2* probe;     // [nprobe][N][N]
+  const float2* quad;      // [N][N]
+  const float2* upd;       // [slot][K][N][N] natural: Δ, χ or g
+  const int* frames;       // [nslot]
+  const int2* corners;     // [nframe]
+  float* pmax;             // rPIE overlap max (device scalar)
+  float* pre;              // LSQML preconditioner [nyo][nxo]
+  const float* pre_max;    // LSQML: max of pre (device scalar)
+  float2* out;             // LSQML d_obj / ML gradient sum [nyo][nxo]
+  float2* comp;            // ML gradient compensation [nyo][nxo]
+  float alpha, step, pre_scale;
+  int nslot, nyo, nxo, nprobe, N;
+};
+
+// The launch's slots whose window overlaps the tile [ty0, ty0+32) × [tx0, tx0+32), in
+// ascending order, for slots [s0, s1): list built by warp 0 with ballots.
+PTYB_D int tile_list(const GatherArgs& a, int s0, int s1, int ty0, int tx0, int* list) {
+  __shared__ int count;
+  if (threadIdx.x < 32) {
+    int n = 0;
+    const int lane = threadIdx.x;
+    for (int base = s0; base < s1; base += 32) {
+      const int s = base + lane;
+      bool hit = false;
+      if (s < s1) {
+        const int2 c = a.corners[a.frames[s]];
+        hit = c.x < ty0 + kTile && c.x + a.N > ty0 && c.y < tx0 + kTile && c.y + a.N > tx0;
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, hit);
+      if (hit) list[n + __popc(m & ((1u << lane) - 1u))] = s;
+      n += __popc(m);
+    }
+    if (lane == 0) count = n;
+  }
+  __syncthreads();
+  const int n = count;
+  __syncthreads();
+  return n;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(1024) object_tile_kernel(GatherArgs a) {
+  constexpr int kChunk = 1024;
+  __shared__ int list[kChunk];
+  __shared__ float red[32];
+  const int tiles_x = (a.nxo + kTile - 1) / kTile;
+  const int tx0 = (blockIdx.x % tiles_x) * kTile, ty0 = (blockIdx.x / tiles_x) * kTile;
+  const int x = tx0 + threadIdx.x % kTile, y = ty0 + threadIdx.x / kTile;
+  const bool inside = x < a.nxo && y < a.nyo;
+  const int K = a.nprobe;
+  const int N = a.N;
+  const size_t plane = (size_t)N * N;
+  KahanC num[kMaxModes];
+  Kahan den[kMaxModes];
+#pragma unroll
+  for (int m = 0; m < kMaxModes; ++m) {
+    num[m].init();
+    den[m].init();
+  }
+  bool covered = false, any = false;
+  for (int s0 = 0; s0 < a.nslot; s0 += kChunk) {
+    const int s1 = min(a.nslot, s0 + kChunk);
+    const int n = tile_list(a, s0, s1, ty0, tx0, list);
+    any |= n > 0;
+    for (int i = 0; i < n; ++i) {
+      const int s = list[i];
+      const int2 c = a.corners[a.frames[s]];
+      const int yy = y - c.x, xx = x - c.y;
+      if (!inside || yy < 0 || yy >= N || xx < 0 || xx >= N) continue;
+      covered = true;
+      const int pix = yy * N + xx;
+      const float2 q = a.quad[pix];
+#pragma unroll
+      for (int m = 0; m < kMaxModes; ++m) {
+        if (m >= K) break;
+        const float2 p = a.probe[m * plane + pix];
+        if (MODE == kGatherOverlap || MODE == kGatherIllum || MODE == kGatherRpie)
+          den[m].add(cnorm2(p));
+        if (MODE == kGatherRpie || MODE == kGatherLsqml || MODE == kGatherMl) {
+          const float2 u = a.upd[((size_t)s * K + m) * plane + pix];
+          const float2 t = cmulc(cmul(p, q), u);  // conj(P·q)·u
+          if (MODE == kGatherRpie)
+            num[m].add(t);
+          else
+            num[0].add(t);
+        }
+      }
+    }
+  }
+  const size_t o = (size_t)y * a.nxo + x;
+  if (MODE == kGatherOverlap) {
+    float d = 0.f;
+#pragma unroll
+    for (int m = 0; m < kMaxModes; ++m)
+      if (m < K) d += den[m].s;
+    d = warp_max(inside ? d : 0.f);
+    if (threadIdx.x % 32 == 0) red[threadIdx.x / 32] = d;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      float mx = 0.f;
+      for (int w = 0; w < 32; ++w) mx = fmaxf(mx, red[w]);
+      atomic_max_nonneg(a.pmax, mx);
+    }
+    return;
+  }
+  if (!inside) return;
+  if (MODE == kGatherRpie) {
+    if (!covered) return;
+    const float pmax = *a.pmax;
+    float2 d = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int m = 0; m < kMaxModes; ++m) {
+      if (m >= K) break;
+      const float w = (1.f - a.alpha) * den[m].s + a.alpha * pmax;
+      d = cadd(d, cscale(num[m].value(), 1.f / w));
+    }
+    a.object[o] = cadd(a.object[o], cscale(d, a.step));
+  } else if (MODE == kGatherLsqml) {
+    const float p = a.pre[o];
+    const float fl = 0.1f * (*a.pre_max);
+    a.out[o] = cscale(num[0].value(), rsqrtf(p * p + fl * fl));
+  } else if (MODE == kGatherMl) {
+    if (!any) return;
+    // out += num with the running compensation in comp.
+    const float2 v = num[0].value();
+    float2 g = a.out[o], cc = a.comp[o];
+    const float yr = v.x - cc.x, yi = v.y - cc.y;
+    const float tr = g.x + yr, ti = g.y + yi;
+    cc = make_float2((tr - g.x) - yr, (ti - g.y) - yi);
+    a.out[o] = make_float2(tr, ti);
+    a.comp[o] = cc;
+  } else if (MODE == kGatherIllum) {
+    float d = 0.f;
+#pragma unroll
+    for (int m = 0; m < kMaxModes; ++m)
+      if (m < K) d += den[m].s;
+    // pty-chi's schedule: (pre + I)/2, the first from pre = I·pre_scale.
+    a.pre[o] = a.pre_scale >= 0.f ? 0.5f * (d * a.pre_scale + d) : 0.5f * (a.pre[o] + d);
+  }
+}
+
+struct ProbeArgs {
+  const float2* object;   // [nyo][nxo] object mode 0
+  const float2* quad;     // [N][N]
+  const float2* upd;      // [slot][K][N][N]
+  const int* frames;
+  const int2* corners;
+  const float* omax;      // rPIE [slot]
+  float2* partial;        // [nchunk][K][N][N]
+  float alpha;
+  int nslot, chunk, nxo, K, N, mode;  // mode 0 rPIE weight, 1 plain conj(q·O)
+};
+
+// Chunk `blockIdx.y` of slots, 256 probe pixels per CTA: Σ_slots w·upd in slot order.
+__global__ void __launch_bounds__(256) probe_partial_kernel(ProbeArgs a) {
+  const int N = a.N;
+  const size_t plane = (size_t)N * N;
+  const int pix = blockIdx.x * 256 + threadIdx.x;
+  if (pix >= N * N) return;
+  const int yy = pix / N, xx = pix % N;
+  const int s0 = blockIdx.y * a.chunk, s1 = min(a.nslot, s0 + a.chunk);
+  const float2 q = a.quad[pix];
+  KahanC acc[kMaxModes];
+#pragma unroll
+  for (int m = 0; m < kMaxModes; ++m) acc[m].init();
+  for (int s = s0; s < s1; ++s) {
+    const int2 c = a.corners[a.frames[s]];
+    const float2 o = a.object[(size_t)(c.x + yy) * a.nxo + c.y + xx];
+    float2 w = cconj(cmul(o, q));
+    if (a.mode == 0) w = cscale(w, 1.f / ((1.f - a.alpha) * cnorm2(o) + a.alpha * a.omax[s]));
+#pragma unroll
+    for (int m = 0; m < kMaxModes; ++m) {
+      if (m >= a.K) break;
+      acc[m].add(cmul(w, a.upd[((size_t)s * a.K + m) * plane + pix]));
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < kMaxModes; ++m)
+    if (m < a.K) a.partial[((size_t)blockIdx.y * a.K + m) * plane + pix] = acc[m].value();
+}
+
+// Σ over chunks in order; mode 0: P += coef·Σ; 1: out = coef·Σ; 2: out += Σ compensated.
+__global__ void probe_finalize_kernel(const float2* partial, int nchunk, int count,
+                                      float2* probe, float2* out, float2* comp, float coef,
+                                      int mode) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  KahanC acc;
+  acc.init();
+  for (int ch = 0; ch < nchunk; ++ch) acc.add(partial[(size_t)ch * count + i]);
+  const float2 v = acc.value();
+  if (mode == 0) {
+    probe[i] = cadd(probe[i], cscale(v, coef));
+  } else if (mode == 1) {
+    out[i] = cscale(v, coef);
+  } else {
+    float2 g = out[i], cc = comp[i];
+    const float yr = v.x - cc.x, yi = v.y - cc.y;
+    const float tr = g.x + yr, ti = g.y + yi;
+    comp[i] = make_float2((tr - g.x) - yr, (ti - g.y) - yi);
+    out[i] = make_float2(tr, ti);
+  }
+}
+
+}  // namespace ptyb

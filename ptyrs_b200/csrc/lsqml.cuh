@@ -1,0 +1,160 @@
+// LSQML's batch reductions: the Poisson far-field step, the per-frame 2×2 step-size systems
+// (solved in double), the trimmed mean and the update (physwkim/ptyrs engine/lsqml.rs:102-179,
+// 286-350, 392-398, 581-643).
+#pragma once
+#include "common.cuh"
+
+namespace ptyb {
+
+// Block sum in double of one value per thread (T = 256), result in every thread.
+template <int T>
+PTYB_D double block_sum1(double v, double* sh) {
+  v = warp_sum(v);
+  if (threadIdx.x % 32 == 0) sh[threadIdx.x / 32] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int w = 0; w < T / 32; ++w) s += sh[w];
+  __syncthreads();
+  return s;
+}
+
+// One pass of PtychoShelves' Poisson `xi` solver per slot: with `prev` the slot-order mean of
+// `a_in` (indexed by frame when `by_frame`), a = clip(prev/2 + Σ xi·(Ĩ − I/(1 − prev·xi)) /
+// Σ xi²·Ĩ / 2, 0, 1), xi = 1 − I/(Ĩ + 1e-5), over unmasked pixels.
+__global__ void __launch_bounds__(256) afar_kernel(const float* icalc, const float* iobs,
+                                                   const int* frames, const float* a_in,
+                                                   int by_frame, float* a_out, int nslot,
+                                                   int npix) {
+  __shared__ double sh[8];
+  __shared__ double prev_s;
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int i = 0; i < nslot; ++i) s += a_in[by_frame ? frames[i] : i];
+    prev_s = s / nslot;
+  }
+  __syncthreads();
+  const double prev = prev_s;
+  const int slot = blockIdx.x;
+  const float* ic = icalc + (size_t)slot * npix;
+  const float* io = iobs + (size_t)frames[slot] * npix;
+  double num = 0.0, den = 0.0;
+  for (int j = threadIdx.x; j < npix; j += 256) {
+    const double yt = io[j];
+    if (yt < 0.0) continue;
+    const double yp = ic[j];
+    const double xi = 1.0 - yt / (yp + 1e-5);
+    num += xi * (yp - yt / (1.0 - prev * xi));
+    den += xi * xi * yp;
+  }
+  num = block_sum1<256>(num, sh);
+  den = block_sum1<256>(den, sh);
+  if (threadIdx.x == 0) {
+    const double ratio = den > 0.0 ? num / den : 0.0;
+    a_out[slot] = (float)fmin(fmax(0.5 * prev + 0.5 * ratio, 0.0), 1.0);
+  }
+}
+
+// Per slot, the six sums of the step-size system over its modes and pixels (natural layout):
+// u = P·dO·q (dop), v = dP·O·q (dpo), c = χ: Σ|u|²+λ0, Σ|v|²+λ0, Σ Re u·v̄, Σ Im u·v̄,
+// Σ Re ū·c, Σ Re v̄·c.
+__global__ void __launch_bounds__(256) lsqml_dots_kernel(
+    const float2* object, const float2* d_obj, const float2* probe, const float2* d_probe,
+    const float2* quad, const float2* chi, const int* frames, const int2* corners, int nxo,
+    int K, int N, double lambda0, double* sums) {
+  __shared__ double sh[8];
+  const int slot = blockIdx.x;
+  const int2 c = corners[frames[slot]];
+  const size_t plane = (size_t)N * N;
+  double s[6] = {0, 0, 0, 0, 0, 0};
+  for (int idx = threadIdx.x; idx < K * N * N; idx += 256) {
+    const int m = idx / (N * N), pix = idx % (N * N);
+    const int yy = pix / N, xx = pix % N;
+    const size_t o = (size_t)(c.x + yy) * nxo + c.y + xx;
+    const float2 q = quad[pix];
+    const float2 u = cmul(cmul(probe[m * plane + pix], d_obj[o]), q);
+    const float2 v = cmul(cmul(d_probe[m * plane + pix], object[o]), q);
+    const float2 x = chi[((size_t)slot * K + m) * plane + pix];
+    s[0] += (double)cnorm2(u) + lambda0;
+    s[1] += (double)cnorm2(v) + lambda0;
+    s[2] += (double)u.x * v.x + (double)u.y * v.y;
+    s[3] += (double)u.y * v.x - (double)u.x * v.y;
+    s[4] += (double)u.x * x.x + (double)u.y * x.y;
+    s[5] += (double)v.x * x.x + (double)v.y * x.y;
+  }
+  for (int k = 0; k < 6; ++k) {
+    const double t = block_sum1<256>(s[k], sh);
+    if (threadIdx.x == 0) sums[(size_t)slot * 6 + k] = t;
+  }
+}
+
+// One block: the per-frame 2×2 solves in double, trimmed mean of a_obj, mean of a_probe;
+// scal[0] = object step, scal[1] = probe step. Records a_far / a_obj / a_probe per slot in
+// `log` ([slot][3]) and the frames' a_far in `a_far_all`.
+__global__ void __launch_bounds__(1024) lsqml_solve_kernel(const double* sums, int nslot,
+                                                           double scale, const float* a_far,
+                                                           const int* frames, float* a_far_all,
+                                                           double* log, float* scal) {
+  __shared__ double aobj[1024], aprb[1024], sorted[1024];
+  __shared__ double means[2];
+  const int t = threadIdx.x;
+  if (t == 0) {
+    double m0 = 0.0, m1 = 0.0;
+    for (int i = 0; i < nslot; ++i) {
+      m0 += sums[i * 6 + 0];
+      m1 += sums[i * 6 + 1];
+    }
+    means[0] = 0.1 * (m0 / nslot);
+    means[1] = 0.1 * (m1 / nslot);
+  }
+  __syncthreads();
+  if (t < nslot) {
+    const double* s = sums + (size_t)t * 6;
+    const double a11 = s[0] + means[0], a22 = s[1] + means[1];
+    const double det = a11 * a22 - (s[2] * s[2] + s[3] * s[3]);
+    const double x0 = (a22 * s[4] - s[2] * s[5]) / det;
+    const double x1 = (a11 * s[5] - s[2] * s[4]) / det;
+    aobj[t] = 0.9 * fmax(x0, 0.0) / scale;
+    aprb[t] = 0.9 * fmax(x1, 0.0);
+    a_far_all[frames[t]] = a_far[t];
+    log[t * 3 + 0] = a_far[t];
+    log[t * 3 + 1] = aobj[t];
+    log[t * 3 + 2] = aprb[t];
+  }
+  __syncthreads();
+  if (t < nslot) {
+    int rank = 0;
+    const double v = aobj[t];
+    for (int j = 0; j < nslot; ++j) rank += (aobj[j] < v) || (aobj[j] == v && j < t);
+    sorted[rank] = v;
+  }
+  __syncthreads();
+  if (t == 0) {
+    const int k = (int)ceil(nslot * 0.1 / 2.0 - 0.5);
+    double s = 0.0;
+    for (int i = k; i < nslot - k; ++i) s += sorted[i];
+    double p = 0.0;
+    for (int i = 0; i < nslot; ++i) p += aprb[i];
+    scal[0] = (float)(s / (nslot - 2 * k));
+    scal[1] = (float)(p / nslot);
+  }
+}
+
+// x += scal[which]·d over n values.
+__global__ void axpy_scal_kernel(float2* x, const float2* d, const float* scal, int which,
+                                 size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  x[i] = cadd(x[i], cscale(d[i], scal[which]));
+}
+
+// Max of a non-negative float array into *out (which starts at 0).
+__global__ void max_kernel(const float* v, size_t n, float* out) {
+  float m = 0.f;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    m = fmaxf(m, v[i]);
+  m = warp_max(m);
+  if (threadIdx.x % 32 == 0) atomic_max_nonneg(out, m);
+}
+
+}  // namespace ptyb

@@ -1,0 +1,237 @@
+"""Python face of the B200 engine, mirroring the reference binding `ptyrs.Scan` and
+`ptyrs.GpuPtycho` (physwkim/ptyrs ptyrs-py/src/lib.rs:435-463, ptyrs-py/src/gpu.rs:28-267):
+numpy arrays in and out, every call through the C ABI of `libptyb200.so`."""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+STATUS = {0: "ok", 1: "invalid", 2: "gpu", 3: "aborted"}
+ALGORITHMS = {0: "ap", 1: "dm", 2: "raar", 3: "rpie", 4: "ml", 5: "bh", 6: "lsqml"}
+COSTS = {"poisson": 0, "amplitude": 1, "gaussian": 1}
+
+
+class PtybError(RuntimeError):
+    """A refused or failed engine call: `status` is "invalid", "gpu" or "aborted"."""
+
+    def __init__(self, status, message):
+        super().__init__(f"{status}: {message}")
+        self.status = status
+
+
+def _dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Scan:
+    """A far-field scan: counts `[nframe, ny, nx]` in detector order (uint16 with 65535 masked,
+    or float32/float64 with negative values masked), positions `y`, `x` in metres, geometry in
+    metres."""
+
+    def __init__(self, counts, y, x, wavelength, distance, detector_pixel):
+        counts = np.asarray(counts)
+        if counts.ndim != 3:
+            raise ValueError("counts must be [nframe, ny, nx]")
+        if counts.dtype == np.uint16:
+            kind = 0
+        elif counts.dtype == np.float32:
+            kind = 1
+        else:
+            counts, kind = counts.astype(np.float64), 2
+        self.counts = np.ascontiguousarray(counts)
+        self.kind = kind
+        self.y = np.ascontiguousarray(y, dtype=np.float64)
+        self.x = np.ascontiguousarray(x, dtype=np.float64)
+        if self.y.shape != (counts.shape[0],) or self.x.shape != (counts.shape[0],):
+            raise ValueError("one y and one x position per frame")
+        self.wavelength, self.distance, self.detector_pixel = wavelength, distance, detector_pixel
+
+    def _struct(self):
+        n, ny, nx = self.counts.shape
+        return _lib.Scan(n, ny, nx, self.kind, self.counts.ctypes.data_as(ctypes.c_void_p),
+                         _dptr(self.y), _dptr(self.x), self.wavelength, self.distance,
+                         self.detector_pixel)
+
+
+class GpuPtycho:
+    """The GPU reconstruction state of a scan on CUDA device `device`: `object` complex
+    `[1, nyo, nxo]`, `probe` complex `[nprobe, ny, nx]`."""
+
+    def __init__(self, scan, obj, probe, device=0, stack_size=0):
+        self._lib = _lib.load()
+        obj = np.ascontiguousarray(obj, dtype=np.complex128)
+        probe = np.ascontiguousarray(probe, dtype=np.complex128)
+        if obj.ndim != 3 or probe.ndim != 3:
+            raise ValueError("object must be [nobj, nyo, nxo] and probe [nprobe, ny, nx]")
+        self._obj_shape, self._probe_shape = obj.shape, probe.shape
+        self._nframe = scan.counts.shape[0]
+        st = scan._struct()
+        opts = _lib.Options(device, stack_size)
+        h = ctypes.c_void_p()
+        rc = self._lib.ptyb_create(ctypes.byref(st), _dptr(obj.view(np.float64)), obj.shape[0],
+                                   obj.shape[1], obj.shape[2], _dptr(probe.view(np.float64)),
+                                   probe.shape[0], ctypes.byref(opts), ctypes.byref(h))
+        if rc != 0:
+            raise PtybError(STATUS.get(rc, rc), self._lib.ptyb_last_error(None).decode())
+        self._h = h
+
+    def _check(self, rc):
+        if rc != 0:
+            raise PtybError(STATUS.get(rc, rc), self._lib.ptyb_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.ptyb_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # Algorithms ---------------------------------------------------------------------------
+    def rpie(self, nepoch, obj_step=1.0, probe_step=1.0, obj_alpha=0.1, probe_alpha=0.1,
+             batch_size=100, calc_llk=0, seed=7):
+        """rPIE epochs (reference `RpieParams` keywords; a step of None holds that array)."""
+        p = _lib.RpieParams(obj_step is not None, probe_step is not None,
+                            0.0 if obj_step is None else obj_step,
+                            0.0 if probe_step is None else probe_step, obj_alpha, probe_alpha,
+                            batch_size, calc_llk, seed)
+        self._check(self._lib.ptyb_rpie(self._h, ctypes.byref(p), nepoch))
+
+    def lsqml(self, nepoch, calc_llk=0, batch_size=256, cost="poisson", seed=7):
+        """LSQML epochs without probe variation, fresh preconditioner per call."""
+        p = _lib.LsqmlParams(batch_size, COSTS[cost], seed)
+        self._check(self._lib.ptyb_lsqml(self._h, ctypes.byref(p), nepoch, calc_llk))
+
+    def ml(self, ncycle, update_object=True, update_probe=False, calc_llk=0,
+           zero_phase_ramp=True):
+        """Poisson ML conjugate-gradient cycles (reference `MlParams`)."""
+        p = _lib.MlParams(update_object, update_probe, calc_llk, zero_phase_ramp)
+        self._check(self._lib.ptyb_ml(self._h, ctypes.byref(p), ncycle))
+
+    # State --------------------------------------------------------------------------------
+    def llk(self):
+        out = _lib.Llk()
+        self._check(self._lib.ptyb_get_llk(self._h, ctypes.byref(out)))
+        return dict(poisson=out.poisson, gaussian=out.gaussian, euclidian=out.euclidian,
+                    nb_photons_calc=out.nb_photons_calc)
+
+    def forward_intensity(self, frames=None):
+        """Model intensity `Σ_modes |Ψ|²` `[len(frames), ny, nx]` of the current estimate, in the
+        FFT-shifted detector layout (zero frequency at [0, 0])."""
+        frames = np.arange(self._nframe, dtype=np.int32) if frames is None else np.ascontiguousarray(frames, np.int32)
+        n = self._probe_shape[-1]
+        out = np.empty((len(frames), n, n), np.float32)
+        self._check(self._lib.ptyb_forward_intensity(
+            self._h, frames.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), len(frames),
+            out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return out
+
+    def object(self):
+        out = np.empty(self._obj_shape, np.complex128)
+        self._check(self._lib.ptyb_get_object(self._h, _dptr(out.view(np.float64))))
+        return out
+
+    def probe(self):
+        out = np.empty(self._probe_shape, np.complex128)
+        self._check(self._lib.ptyb_get_probe(self._h, _dptr(out.view(np.float64))))
+        return out
+
+    def set_object(self, obj):
+        obj = np.ascontiguousarray(obj, dtype=np.complex128).reshape(self._obj_shape)
+        self._check(self._lib.ptyb_set_object(self._h, _dptr(obj.view(np.float64))))
+
+    def set_probe(self, probe):
+        probe = np.ascontiguousarray(probe, dtype=np.complex128).reshape(self._probe_shape)
+        self._check(self._lib.ptyb_set_probe(self._h, _dptr(probe.view(np.float64))))
+
+    def corners(self):
+        out = np.empty((self._nframe, 2), np.int32)
+        self._check(self._lib.ptyb_corners(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))))
+        return out
+
+    def history(self):
+        n = self._lib.ptyb_history_len(self._h)
+        recs = (_lib.LlkRecord * max(n, 1))()
+        self._check(self._lib.ptyb_history(self._h, recs, n))
+        recs = recs[:n]
+        return dict(cycle=np.array([r.cycle for r in recs], np.int64),
+                    algorithm=[ALGORITHMS[r.algorithm] for r in recs],
+                    poisson=np.array([r.llk.poisson for r in recs]),
+                    gaussian=np.array([r.llk.gaussian for r in recs]),
+                    euclidian=np.array([r.llk.euclidian for r in recs]),
+                    nb_photons_calc=np.array([r.llk.nb_photons_calc for r in recs]))
+
+    def cycle(self):
+        return int(self._lib.ptyb_cycle(self._h))
+
+    def lsqml_steps(self):
+        """The last LSQML epoch's steps: per batch, its frames and their a_far, a_obj, a_probe."""
+        n = self._lib.ptyb_lsqml_steps_len(self._h)
+        buf = (_lib.LsqmlStep * max(n, 1))()
+        self._check(self._lib.ptyb_lsqml_steps(self._h, buf, n))
+        steps = []
+        for s in buf[:n]:
+            if not steps or steps[-1]["batch"] != s.batch:
+                steps.append(dict(batch=s.batch, frames=[], a_far=[], a_obj=[], a_probe=[]))
+            st = steps[-1]
+            st["frames"].append(s.frame)
+            st["a_far"].append(s.a_far)
+            st["a_obj"].append(s.a_obj)
+            st["a_probe"].append(s.a_probe)
+        return steps
+
+    def synchronize(self):
+        self._check(self._lib.ptyb_synchronize(self._h))
+
+    def set_timing(self, on=True):
+        """Per-kernel device timing of every later launch (resets the totals)."""
+        self._check(self._lib.ptyb_set_timing(self._h, int(on)))
+
+    def kernel_times(self):
+        """`{kernel: (total ms, launches)}` of the launches timed since `set_timing`."""
+        k = self._lib.ptyb_kernel_kinds()
+        ms = (ctypes.c_double * k)()
+        n = (ctypes.c_int64 * k)()
+        self._check(self._lib.ptyb_kernel_times(self._h, ms, n, k))
+        return {self._lib.ptyb_kernel_name(i).decode(): (ms[i], n[i]) for i in range(k) if n[i]}
+
+    def last_call_ms(self):
+        """Device time of the last algorithm call (CUDA events on the engine's stream)."""
+        return float(self._lib.ptyb_last_call_ms(self._h))
+
+    def launches(self):
+        """Kernels this handle has launched since it was made."""
+        return int(self._lib.ptyb_launches(self._h))
+
+
+def random_batches(nframe, size, seed, epoch):
+    """The reference's seeded mini-batches of one epoch from the native host code, as a list of
+    sorted frame lists."""
+    lib = _lib.load()
+    order = np.empty(nframe, np.int32)
+    rc = lib.ptyb_random_batches(nframe, size, seed, epoch,
+                                 order.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+    if rc != 0:
+        raise PtybError(STATUS.get(rc, rc), "random_batches")
+    return [order[s:s + size].tolist() for s in range(0, nframe, size)]
+
+
+def view_corners(y, x, pixel, frame, obj):
+    """Window corners `[P, 2]` (oy, ox) of positions in metres from the native host code."""
+    lib = _lib.load()
+    y = np.ascontiguousarray(y, np.float64)
+    x = np.ascontiguousarray(x, np.float64)
+    out = np.empty((len(y), 2), np.int32)
+    rc = lib.ptyb_view_corners(_dptr(y), _dptr(x), len(y), pixel[0], pixel[1], frame[0],
+                               frame[1], obj[0], obj[1],
+                               out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+    if rc != 0:
+        raise PtybError(STATUS.get(rc, rc), lib.ptyb_last_error(None).decode())
+    return out

@@ -1,0 +1,132 @@
+"""Seeded synthetic scans of the shapes the benchmarks and tests use: smooth-noise objects,
+defocused-aperture probes (with Hermite-Gauss modes), raster / Fermat scans and Poisson
+far-field counts, all in numpy float64 (data generation, not part of the reconstruction path).
+
+The far-field forward model here is the reference's (`obj_probe_to_psi` then the unitary FFT,
+physwkim/ptyrs engine/ops.rs:47-71, engine/fft.rs:155-234) on the integer windows that PyNX's
+position convention gives (base/addr.rs:123-127): positions are centred on their mean and the
+window corner is `round_half_even((nobj − n)//2 + position/pixel)`.
+"""
+import numpy as np
+from scipy.ndimage import gaussian_filter
+
+WAVELENGTH, DISTANCE, DETECTOR_PIXEL = 1.5e-10, 1.0, 75e-6
+GOLDEN_ANGLE = np.pi * (3.0 - np.sqrt(5.0))
+
+
+def object_pixel(n):
+    """Object pixel in metres of an n×n far-field frame at the default geometry."""
+    return WAVELENGTH * DISTANCE / (n * DETECTOR_PIXEL)
+
+
+def smooth_object(side, seed, phase_scale=np.pi / 2):
+    """`amp = 1 − 0.2·g`, `phase = phase_scale·g`, `g` uniform noise smoothed by a σ = 3 px
+    Gaussian (periodic) and normalised to [0, 1]; `[1, side, side]` complex128."""
+    rng = np.random.default_rng(seed)
+    g = gaussian_filter(rng.uniform(size=(side, side)), 3.0, mode="wrap")
+    g = (g - g.min()) / (g.max() - g.min())
+    return ((1.0 - 0.2 * g) * np.exp(1j * phase_scale * g))[None]
+
+
+def aperture_probe(n, radius, edge_phase=2.0):
+    """A circular aperture of `radius` px with a quadratic defocus phase reaching `edge_phase`
+    rad at the edge (slightly softened edge), `[n, n]` complex128."""
+    y, x = np.mgrid[:n, :n] - n / 2.0
+    r = np.hypot(y, x)
+    amp = np.clip(radius + 0.5 - r, 0.0, 1.0)
+    return amp * np.exp(1j * edge_phase * (r / radius) ** 2)
+
+
+def hermite_probe(n, radius, powers, edge_phase=2.0):
+    """Incoherent probe modes: the defocused aperture times Hermite-Gauss factors of orders
+    (0,0), (1,0), (0,1), (1,1), … of width radius/2, mode k scaled to power `powers[k]` of a
+    total of 1e4 (arbitrary units), `[len(powers), n, n]`."""
+    base = aperture_probe(n, radius, edge_phase)
+    y, x = (np.mgrid[:n, :n] - n / 2.0) / (radius / 2.0)
+    herm = [lambda t: np.ones_like(t), lambda t: 2 * t, lambda t: 4 * t * t - 2]
+    orders = [(0, 0), (1, 0), (0, 1), (1, 1), (2, 0), (0, 2)]
+    modes = []
+    for k, p in enumerate(powers):
+        a, b = orders[k]
+        m = base * herm[a](x) * herm[b](y) * np.exp(-(x * x + y * y) / 4.0)
+        if k == 0:
+            m = base
+        modes.append(m * np.sqrt(p * 1e4) / np.linalg.norm(m))
+    return np.array(modes)
+
+
+def raster_positions(ny, nx, step, jitter, seed):
+    """`ny × nx` raster of `step` px with uniform ±`jitter` px noise, in pixels `[P, 2]`."""
+    rng = np.random.default_rng(seed)
+    gy, gx = np.mgrid[:ny, :nx] * float(step)
+    p = np.stack([gy.ravel(), gx.ravel()], 1)
+    return p + rng.uniform(-jitter, jitter, size=p.shape)
+
+
+def fermat_positions(count, step):
+    """Fermat spiral of `count` points with about `step` px between neighbours, `[P, 2]`."""
+    k = np.arange(count, dtype=np.float64)
+    c = step / np.sqrt(np.pi)
+    r, t = c * np.sqrt(k), k * GOLDEN_ANGLE
+    return np.stack([r * np.sin(t), r * np.cos(t)], 1)
+
+
+def corners(pos_px, n, nobj):
+    """Window corners `[P, 2]` of positions in pixels under PyNX's convention (centred on the
+    mean, rounded half to even, relative to the object centre)."""
+    p = pos_px - pos_px.mean(axis=0)
+    c = np.round((nobj - n) // 2 + p).astype(np.int64)
+    if (c < 0).any() or (c > nobj - n).any():
+        raise ValueError("a window leaves the object")
+    return c
+
+
+def far_field_counts(obj, probe, corner, photons, seed, chunk=64):
+    """Poisson counts `[P, n, n]` (float32, detector order: zero frequency at the centre) of
+    `Σ_modes |FFT_ortho(P·O_window)|²`, scaled so the mean pattern holds `photons`."""
+    n = probe.shape[-1]
+    P = len(corner)
+    inten = np.empty((P, n, n), np.float64)
+    for s in range(0, P, chunk):
+        cs = corner[s:s + chunk]
+        win = np.stack([obj[0, y:y + n, x:x + n] for y, x in cs])
+        psi = probe[None] * win[:, None]
+        far = np.fft.fft2(psi, norm="ortho")
+        inten[s:s + chunk] = np.fft.fftshift((np.abs(far) ** 2).sum(axis=1), axes=(-2, -1))
+    inten *= photons / inten.sum(axis=(1, 2)).mean()
+    rng = np.random.default_rng(seed)
+    return rng.poisson(inten).astype(np.float32)
+
+
+def make_scan(kind, seed=0, scale=1.0):
+    """Seeded synthetic inputs of a benchmark configuration: returns a dict with counts
+    (float32), y, x (metres), object start, probe start, truth object and sizes.
+
+    kind "rpie64": 256² object, 64² aperture probe, 20×20 raster of 8 px ±1 px, 1e5 photons.
+    kind "lsqml128": 1024² object, 128² probe with 3 modes (0.8/0.15/0.05), Fermat 4096 at
+    6 px, 1e6 photons. kind "ml256": 2048² object, 256² probe with 2 modes, Fermat 10000 at
+    12 px, 1e7 photons. `scale` < 1 keeps that fraction of the positions (the same first ones)
+    for small cases.
+    """
+    if kind == "rpie64":
+        n, side, modes, photons = 64, 256, [1.0], 1e5
+        pos = raster_positions(20, 20, 8, 1.0, seed + 1)
+    elif kind == "lsqml128":
+        n, side, modes, photons = 128, 1024, [0.8, 0.15, 0.05], 1e6
+        pos = fermat_positions(4096, 6.0)
+    elif kind == "ml256":
+        n, side, modes, photons = 256, 2048, [0.8, 0.2], 1e7
+        pos = fermat_positions(10000, 12.0)
+    else:
+        raise ValueError(kind)
+    if scale < 1.0:
+        pos = pos[:max(2, int(len(pos) * scale))]
+    truth = smooth_object(side, seed + 2)
+    probe = hermite_probe(n, n / 4.0, modes) if len(modes) > 1 else aperture_probe(n, n / 4.0)[None] * 30.0
+    c = corners(pos, n, side)
+    counts = far_field_counts(truth, probe, c, photons, seed + 3)
+    px = object_pixel(n)
+    start = np.ones_like(truth)
+    return dict(counts=counts, y=pos[:, 0] * px, x=pos[:, 1] * px, object=start, probe=probe,
+                truth=truth, corners=c, n=n, side=side, wavelength=WAVELENGTH,
+                distance=DISTANCE, detector_pixel=DETECTOR_PIXEL)

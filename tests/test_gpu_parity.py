@@ -1,0 +1,159 @@
+"""The CUDA path through the C ABI against the f64 oracle on the same seeded far-field scans,
+as the reference holds its GPU engine to its CPU oracle (ptyrs/tests/engine_gpu.rs:160-165,
+298-322: relative error < 1e-4 on the LLK records and the final object and probe). One epoch
+of one batch is held to 1e-5 (FP32 against FP64 for one update); several epochs to 1e-4.
+Frame sides 64, 128 and 256 run the cluster sizes 1, 2 and 8."""
+import numpy as np
+import pytest
+
+from oracle.lsqml import Lsqml
+from ptyrs_b200 import GpuPtycho, PtybError, Scan, sim
+from scenarios import far_field, oracle_state, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+ONE_STEP_TOL = 1e-5
+RUN_TOL = 1e-4
+# LSQML's Poisson far-field step (PtychoShelves' xi solver, engine/lsqml.rs:133-150) weighs
+# pixels by xi = 1 − I/(Ĩ + 1e-5): at the far-field zeros of a hard-edged aperture Ĩ is set by
+# the FP32 FFT's absolute rounding, so over several epochs a_far holds to 3e-4 of its largest.
+AFAR_RUN_TOL = 3e-4
+
+# (frame side, probe modes, frames, object side)
+SHAPES = [(64, 1, 40, 192), (64, 2, 40, 192), (128, 3, 24, 320), (256, 2, 10, 448)]
+
+
+def gpu_of(s, **kw):
+    scan = Scan(s["counts"], s["y"], s["x"], sim.WAVELENGTH, sim.DISTANCE, sim.DETECTOR_PIXEL)
+    return GpuPtycho(scan, s["object"], s["probe"], **kw)
+
+
+@pytest.fixture(scope="module", params=SHAPES, ids=lambda p: f"n{p[0]}k{p[1]}")
+def case(request):
+    n, k, nframe, side = request.param
+    return far_field(n, k, nframe, side, masked=True, seed=n + k)
+
+
+def test_corners_and_start_llk(case):
+    cpu = oracle_state(case)
+    with gpu_of(case) as g:
+        want = np.stack([cpu.addr.views["oy"], cpu.addr.views["ox"]], 1)[::cpu.addr.nmode]
+        assert (g.corners() == want).all()
+        got, ref = g.llk(), cpu.llk()
+        for key in ("poisson", "gaussian", "euclidian", "nb_photons_calc"):
+            assert abs(got[key] - getattr(ref, key)) <= ONE_STEP_TOL * abs(getattr(ref, key)), key
+
+
+def test_rpie_one_batch(case):
+    cpu = oracle_state(case)
+    nframe = len(case["counts"])
+    cpu.rpie(1, obj_alpha=0.1, probe_alpha=0.1, batch_size=nframe, seed=7)
+    with gpu_of(case) as g:
+        g.rpie(1, obj_alpha=0.1, probe_alpha=0.1, batch_size=nframe, seed=7)
+        assert g.launches() > 0
+        assert rel_l2(g.object() - case["object"], cpu.object - case["object"]) < ONE_STEP_TOL
+        assert rel_l2(g.probe() - case["probe"], cpu.probe - case["probe"]) < ONE_STEP_TOL
+
+
+@pytest.mark.parametrize("batch", [7, 13])
+def test_rpie_epochs(case, batch):
+    cpu = oracle_state(case)
+    cpu.rpie(3, obj_alpha=0.1, probe_alpha=0.1, batch_size=batch, calc_llk=1, seed=7)
+    with gpu_of(case) as g:
+        g.rpie(3, obj_alpha=0.1, probe_alpha=0.1, batch_size=batch, calc_llk=1, seed=7)
+        assert rel_l2(g.object(), cpu.object) < RUN_TOL
+        assert rel_l2(g.probe(), cpu.probe) < RUN_TOL
+        h = g.history()
+        want = np.array([r["poisson"] for r in cpu.history])
+        assert list(h["cycle"]) == [r["cycle"] for r in cpu.history]
+        assert np.abs(h["poisson"] - want).max() <= RUN_TOL * np.abs(want).max()
+        assert g.cycle() == 3
+
+
+def test_rpie_single_frame_batches():
+    """Batches of one frame (pty-chi's per-frame rPIE) on a scan whose f64 run moves by < 1e-5
+    under a 1e-7 change of the start: the single-mode aperture scans amplify such a change to
+    1e-2 in three epochs in f64 alone, so no FP32 run can be held to them."""
+    s = far_field(64, 2, 40, 192, masked=True, seed=66)
+    cpu = oracle_state(s)
+    cpu.rpie(2, batch_size=1, seed=7)
+    with gpu_of(s) as g:
+        g.rpie(2, batch_size=1, seed=7)
+        assert rel_l2(g.object(), cpu.object) < RUN_TOL
+        assert rel_l2(g.probe(), cpu.probe) < RUN_TOL
+
+
+def test_rpie_holds_an_array_without_its_step(case):
+    cpu = oracle_state(case)
+    cpu.rpie(1, obj_step=None, batch_size=7, seed=3)
+    with gpu_of(case) as g:
+        g.rpie(1, obj_step=None, batch_size=7, seed=3)
+        assert np.array_equal(g.object(), case["object"].astype(np.complex64).astype(complex))
+        assert rel_l2(g.probe(), cpu.probe) < RUN_TOL
+
+
+def lsqml_cpu(case, nepoch, batch, cost):
+    cpu = oracle_state(case)
+    run = Lsqml(batch, cost, 7)
+    obj, probe, steps = cpu.object, cpu.probe, None
+    for _ in range(nepoch):
+        obj, probe, steps = run.epoch(cpu.addr, cpu.obs, cpu.optics, obj, probe)
+    return obj, probe, steps
+
+
+@pytest.mark.parametrize("cost", ["poisson", "amplitude"])
+def test_lsqml_one_batch(case, cost):
+    nframe = len(case["counts"])
+    obj, probe, steps = lsqml_cpu(case, 1, nframe, cost)
+    with gpu_of(case) as g:
+        g.lsqml(1, batch_size=nframe, cost=cost, seed=7)
+        got = g.lsqml_steps()
+        assert len(got) == 1 and got[0]["frames"] == steps[0]["frames"]
+        for key in ("a_far", "a_obj", "a_probe"):
+            a, b = np.array(got[0][key]), np.array(steps[0][key])
+            assert np.abs(a - b).max() <= ONE_STEP_TOL * 10 * np.abs(b).max(), key
+        assert rel_l2(g.object() - case["object"], obj - case["object"]) < ONE_STEP_TOL * 10
+        assert rel_l2(g.probe() - case["probe"], probe - case["probe"]) < ONE_STEP_TOL * 10
+
+
+@pytest.mark.parametrize("cost", ["poisson", "amplitude"])
+def test_lsqml_epochs(case, cost):
+    obj, probe, steps = lsqml_cpu(case, 3, 8, cost)
+    with gpu_of(case) as g:
+        g.lsqml(3, batch_size=8, cost=cost, seed=7)
+        got = g.lsqml_steps()
+        assert [s["frames"] for s in got] == [s["frames"] for s in steps]
+        for gs, cs in zip(got, steps):
+            for key in ("a_far", "a_obj", "a_probe"):
+                a, b = np.array(gs[key]), np.array(cs[key])
+                tol = AFAR_RUN_TOL if key == "a_far" else RUN_TOL
+                assert np.abs(a - b).max() <= tol * np.abs(b).max() + 1e-30, key
+        assert rel_l2(g.object(), obj) < RUN_TOL
+        assert rel_l2(g.probe(), probe) < RUN_TOL
+
+
+def test_runs_are_deterministic(case):
+    outs = []
+    for _ in range(2):
+        with gpu_of(case) as g:
+            g.rpie(2, batch_size=6, seed=11)
+            g.lsqml(2, batch_size=6, seed=5)
+            outs.append((g.object(), g.probe()))
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+
+
+def test_invalid_calls_leave_the_state():
+    s = far_field(64, 1, 12, 160, seed=1)
+    with gpu_of(s) as g:
+        before = g.object()
+        with pytest.raises(PtybError) as e:
+            g.rpie(1, batch_size=0)
+        assert e.value.status == "invalid"
+        assert np.array_equal(g.object(), before)
+        g.rpie(1, batch_size=4)  # still usable
+    bad = dict(s, y=s["y"] * 100.0)
+    with pytest.raises(PtybError) as e:
+        gpu_of(bad)
+    assert e.value.status == "invalid"
+    with pytest.raises(PtybError):
+        gpu_of(dict(s, object=np.ones((2, 160, 160), complex)))
