@@ -121,6 +121,19 @@ int ptyb_get_llk(ptyb_handle* h, ptyb_llk* out);
  * the reference binding's `forward` (ptyrs-py/src/cpu.rs) summed over modes. */
 int ptyb_forward_intensity(ptyb_handle* h, const int32_t* frames, int32_t n, float* out);
 
+/* No counterpart in the reference. `ptyb_forward_intensity` without any device allocation,
+ * for callers that cannot call cudaMalloc at that point (a host runtime whose device memory
+ * is fixed once the handle exists, or a memory-capped service that must not grow its
+ * footprint per request): the same model intensity, computed with the same kernel, its
+ * scratch (frame list, detector field, intensities) in one fixed 32 MiB device array that
+ * every GPU loading this library holds until exit. Frames are processed in chunks that fit it;
+ * PTYB_INVALID when a single frame (K field planes and one intensity plane) does not. The
+ * first call on a device looks the array's address up (cudaGetSymbolAddress); make that call
+ * before any stream capture. Every call shares the array and leaves its last contents there:
+ * every byte a call reads it writes first, and calls that overlap on the GPU (other handles or
+ * threads at the same time) race on it. */
+int ptyb_forward_intensity_noalloc(ptyb_handle* h, const int32_t* frames, int32_t n, float* out);
+
 /* Reference `GpuPtycho::{object, probe, set_object}` (engine/gpu/mod.rs:763-817). */
 int ptyb_get_object(ptyb_handle* h, double* dst);
 int ptyb_get_probe(ptyb_handle* h, double* dst);

@@ -58,6 +58,8 @@ SIGNATURES = {
     "ptyb_ml": (c_int32, [c_void_p, P(MlParams), c_int32]),
     "ptyb_get_llk": (c_int32, [c_void_p, P(Llk)]),
     "ptyb_forward_intensity": (c_int32, [c_void_p, P(c_int32), c_int32, P(ctypes.c_float)]),
+    "ptyb_forward_intensity_noalloc": (c_int32, [c_void_p, P(c_int32), c_int32,
+                                                 P(ctypes.c_float)]),
     "ptyb_get_object": (c_int32, [c_void_p, P(c_double)]),
     "ptyb_get_probe": (c_int32, [c_void_p, P(c_double)]),
     "ptyb_set_object": (c_int32, [c_void_p, P(c_double)]),

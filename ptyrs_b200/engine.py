@@ -133,6 +133,18 @@ class GpuPtycho:
             out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
         return out
 
+    def forward_intensity_noalloc(self, frames=None):
+        """`forward_intensity` through the entry point that allocates no device memory (its
+        scratch is a fixed 32 MiB device array shared by every call in the process; calls that
+        run on the GPU at the same time race on it)."""
+        frames = np.arange(self._nframe, dtype=np.int32) if frames is None else np.ascontiguousarray(frames, np.int32)
+        n = self._probe_shape[-1]
+        out = np.empty((len(frames), n, n), np.float32)
+        self._check(self._lib.ptyb_forward_intensity_noalloc(
+            self._h, frames.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), len(frames),
+            out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return out
+
     def object(self):
         out = np.empty(self._obj_shape, np.complex128)
         self._check(self._lib.ptyb_get_object(self._h, _dptr(out.view(np.float64))))
