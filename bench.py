@@ -105,9 +105,9 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def make_inputs(workload, seed):
+def make_inputs(workload, seed, scale=1.0):
     from ptyrs_b200 import sim
-    return sim.make_scan(WORKLOADS[workload]["kind"], seed=seed)
+    return sim.make_scan(WORKLOADS[workload]["kind"], seed=seed, scale=scale)
 
 
 def run_algorithm(g, wl, nepoch):
@@ -209,6 +209,10 @@ def main():
     ap.add_argument("--workload", default="lsqml128", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cluster", type=int, default=0,
+                    help="CTAs per frame of the frame kernel (0: the engine chooses)")
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="keep this fraction of the scan's positions (small profiling cases)")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
@@ -227,10 +231,10 @@ def main():
 
     from ptyrs_b200 import GpuPtycho, Scan, build, sim
     build.build()
-    s = make_inputs(args.workload, seed=rank)
+    s = make_inputs(args.workload, seed=rank, scale=args.scale)
     P = len(s["counts"])
     scan = Scan(s["counts"], s["y"], s["x"], s["wavelength"], s["distance"], s["detector_pixel"])
-    g = GpuPtycho(scan, s["object"], s["probe"], device=local)
+    g = GpuPtycho(scan, s["object"], s["probe"], device=local, cluster=args.cluster)
     run_algorithm(g, wl, args.warmup)
     g.synchronize()
 
@@ -321,6 +325,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": args.workload, "description": wl["desc"],
+                       "scale": args.scale,
                        "patterns_per_step_per_gpu": P, "parallelism": f"replicas{ws}",
                        "l2": "inputs larger than L2 (counts "
                              f"{s['counts'].nbytes / 1e6:.0f} MB)"},

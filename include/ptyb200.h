@@ -47,10 +47,12 @@ typedef struct ptyb_scan {
 } ptyb_scan;
 
 /* Reference `GpuOptions` (engine/gpu/mod.rs:63-112): frames per launch of the passes over the
- * whole scan (LLK, ML), 0 for the default. */
+ * whole scan (LLK, ML), 0 for the default; `cluster` the CTAs per frame of the frame kernel
+ * (1 at frame side 64; 2 or 4 at 128; 8 or 16 at 256), 0 to let the engine choose. */
 typedef struct ptyb_options {
   int32_t device;
   int32_t stack_size;
+  int32_t cluster;
 } ptyb_options;
 
 /* Reference `RpieParams` (engine/ptycho.rs:148-186). A step flag of 0 holds that array. */

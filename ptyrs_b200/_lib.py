@@ -17,7 +17,7 @@ class Scan(ctypes.Structure):
 
 
 class Options(ctypes.Structure):
-    _fields_ = [("device", c_int32), ("stack_size", c_int32)]
+    _fields_ = [("device", c_int32), ("stack_size", c_int32), ("cluster", c_int32)]
 
 
 class RpieParams(ctypes.Structure):

@@ -16,6 +16,7 @@
 #include "frame.cuh"
 #include "gather.cuh"
 #include "lsqml.cuh"
+#include "ml.cuh"
 #include "scan.h"
 
 using namespace ptyb;
@@ -80,7 +81,7 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratch
 
 namespace {
 
-constexpr int kAlgRpie = 3, kAlgLsqml = 6;
+constexpr int kAlgRpie = 3, kAlgMl = 4, kAlgLsqml = 6;
 
 // One device allocation, freed with the handle.
 struct Buf {
@@ -125,6 +126,12 @@ struct ptyb_handle {
   float2* d_probe = nullptr;  // [K][N][N]
   double* sums = nullptr;     // [slots][6]
   double* steplog = nullptr;  // [P][3]
+  // ML: gradients (with compensation), the previous gradients, the CG directions, the line
+  // search's per-frame sums and reduction partials.
+  float2 *g_obj = nullptr, *g_obj_c = nullptr, *g_probe = nullptr, *g_probe_c = nullptr;
+  float2 *last_obj = nullptr, *last_probe = nullptr, *dir_obj = nullptr, *dir_probe = nullptr;
+  double* gamma_sums = nullptr;  // [P][2]
+  double* partials = nullptr;    // [kPartialBlocks][2]
   std::vector<Buf> bufs;
   // Per-kernel device timing (CUDA events on the engine's stream), when enabled.
   bool timing = false;
@@ -191,17 +198,19 @@ void launched(ptyb_handle* h, const char* what) {
   check(h, cudaGetLastError(), what);
 }
 
+constexpr int kPartialBlocks = 296;
+
 // Kernel kinds for the per-kernel timing (ptyb_kernel_name).
 enum Kind : int {
   kKFrameRpie = 0, kKFrameLsqml, kKFrameMl, kKFrameLlk, kKFrameStore, kKFrameFromStore,
   kKObjRpie, kKObjOverlap, kKObjLsqml, kKObjMl, kKIllum, kKProbePartial, kKProbeFinal,
-  kKAfar, kKDots, kKSolve, kKAxpy, kKMax, kKCounts, kKMisc, kNumKinds
+  kKAfar, kKDots, kKSolve, kKAxpy, kKMax, kKCounts, kKMisc, kKGamma, kKArraySums, kNumKinds
 };
 const char* const kKindNames[kNumKinds] = {
     "frame_rpie", "frame_lsqml", "frame_ml_grad", "frame_llk", "frame_store",
     "frame_from_store", "object_rpie", "object_overlap", "object_lsqml", "object_ml",
     "illumination", "probe_partial", "probe_finalize", "lsqml_afar", "lsqml_dots",
-    "lsqml_solve", "axpy", "max", "counts", "misc"};
+    "lsqml_solve", "axpy", "max", "counts", "misc", "ml_gamma", "array_sums"};
 
 cudaEvent_t take_event(ptyb_handle* h) {
   if (!h->event_pool.empty()) {
@@ -258,16 +267,24 @@ void end_call(ptyb_handle* h, const char* what) {
   harvest(h);
 }
 
-// Cluster size for frames of side N with K modes: the smallest that fits shared memory.
-int cluster_for(int N, int K) {
-  const size_t lim = 227 * 1024;
-  if (N == 64) return frame_smem_bytes<64, 1>(K) <= lim ? 1 : 0;
-  if (N == 128) {
-    if (frame_smem_bytes<128, 2>(K) <= lim) return 2;
-    if (frame_smem_bytes<128, 4>(K) <= lim) return 4;
-    return 0;
-  }
-  if (N == 256) return frame_smem_bytes<256, 8>(K) <= lim ? 8 : 0;
+// Cluster size for frames of side N with K modes: `want` if it is built and fits shared
+// memory, else the smallest that fits with at least two CTAs per SM, else the smallest that
+// fits; 0 when none does.
+int cluster_for(int N, int K, int want) {
+  const size_t lim = 227 * 1024, two = 113 * 1024;
+  struct Opt {
+    int n, c;
+    size_t bytes;
+  };
+  const Opt opts[] = {{64, 1, frame_smem_bytes<64, 1>(K)},   {128, 2, frame_smem_bytes<128, 2>(K)},
+                      {128, 4, frame_smem_bytes<128, 4>(K)}, {256, 8, frame_smem_bytes<256, 8>(K)},
+                      {256, 16, frame_smem_bytes<256, 16>(K)}};
+  for (const Opt& o : opts)
+    if (o.n == N && o.c == want && o.bytes <= lim) return o.c;
+  for (const Opt& o : opts)
+    if (o.n == N && o.bytes <= two) return o.c;
+  for (const Opt& o : opts)
+    if (o.n == N && o.bytes <= lim) return o.c;
   return 0;
 }
 
@@ -277,6 +294,10 @@ cudaError_t launch_frame_nc(const FrameArgs& a, int nslot, int K, cudaStream_t s
   const size_t smem = frame_smem_bytes<N, C>(K);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
+  if (C > 8) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return e;
+  }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(nslot * C);
   cfg.blockDim = dim3(FrameShape<N, C>::T);
@@ -300,6 +321,7 @@ cudaError_t launch_frame_raw(ptyb_handle* h, const FrameArgs& a, int nslot) {
     case 12802: return launch_frame_nc<128, 2, MODE>(a, nslot, h->K, h->stream);
     case 12804: return launch_frame_nc<128, 4, MODE>(a, nslot, h->K, h->stream);
     case 25608: return launch_frame_nc<256, 8, MODE>(a, nslot, h->K, h->stream);
+    case 25616: return launch_frame_nc<256, 16, MODE>(a, nslot, h->K, h->stream);
   }
   return cudaErrorInvalidValue;
 }
@@ -378,11 +400,11 @@ void ensure_slots(ptyb_handle* h, int n) {
   h->slots = n;
 }
 
-// Probe-pass chunking: about 2 CTAs per SM over the probe pixels.
+// Probe-pass chunking: about 8 CTAs per SM over the probe pixels.
 int probe_chunk(ptyb_handle* h, int nslot, int* nchunk) {
   const int pixblocks = (h->N * h->N + 255) / 256;
-  int want = std::max(1, 296 / pixblocks);
-  int chunk = std::max(1, (nslot + want - 1) / want);
+  int want = std::max(1, 148 * 8 / pixblocks);
+  int chunk = std::min(kMaxProbeChunk, std::max(1, (nslot + want - 1) / want));
   *nchunk = (nslot + chunk - 1) / chunk;
   if (*nchunk > h->max_chunks) {
     h->partial = alloc<float2>(h, (size_t)(*nchunk) * h->K * h->N * h->N);
@@ -556,18 +578,16 @@ void lsqml_batch(ptyb_handle* h, const ptyb_lsqml_params& p, const int* frames, 
   FrameArgs a = frame_args(h, frames);
   a.cost = p.cost;
   if (p.cost == PTYB_COST_POISSON) {
+    // Forward pass with the xi solver's first pass, backward pass with its second.
+    a.nslot = nslot;
+    a.icalc = nullptr;
+    a.a_prev = h->afar_all;
+    a.a_prev_by_frame = 1;
+    a.a_out = h->afar1;
     check(h, launch_frame<kStore>(h, a, nslot), "lsqml forward");
     ++h->launches;
-    timed(h, kKAfar, [&] {
-    afar_kernel<<<nslot, 256, 0, h->stream>>>(h->icalc, h->iobs, frames, h->afar_all, 1, h->afar1,
-                                               nslot, h->N * h->N);
-    });
-    launched(h, "a_far pass 1");
-    timed(h, kKAfar, [&] {
-    afar_kernel<<<nslot, 256, 0, h->stream>>>(h->icalc, h->iobs, frames, h->afar1, 0, h->afar2,
-                                               nslot, h->N * h->N);
-    });
-    launched(h, "a_far pass 2");
+    a.a_mid = h->afar1;
+    a.a_out = h->afar2;
     check(h, launch_frame<kFromStore>(h, a, nslot), "lsqml backward");
     ++h->launches;
   } else {
@@ -584,7 +604,7 @@ void lsqml_batch(ptyb_handle* h, const ptyb_lsqml_params& p, const int* frames, 
   probe_pass(h, frames, nslot, 1, 0.f, 1.0f / nslot);
   const double lambda0 = 1.2e-7 * ((double)h->N * h->N) / ((double)h->N * h->N);
   timed(h, kKDots, [&] {
-  lsqml_dots_kernel<<<nslot, 256, 0, h->stream>>>(h->object, h->d_obj, h->probe, h->d_probe,
+  lsqml_dots_kernel<<<nslot, 512, 0, h->stream>>>(h->object, h->d_obj, h->probe, h->d_probe,
                                                    h->quad, h->upd, frames, h->corners, h->nxo,
                                                    h->K, h->N, lambda0, h->sums);
   });
@@ -605,6 +625,272 @@ void lsqml_batch(ptyb_handle* h, const ptyb_lsqml_params& p, const int* frames, 
                                                                        h->scal + 2, 1, np);
   });
   launched(h, "probe step");
+}
+
+
+template <int N, int C>
+cudaError_t launch_gamma_nc(const GammaArgs& a, int nslot, cudaStream_t s) {
+  auto kern = gamma_kernel<N, C>;
+  const size_t smem = gamma_smem_bytes<N, C>();
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  if (C > 8) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return e;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nslot * C);
+  cfg.blockDim = dim3(FrameShape<N, C>::T);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = C > 1 ? 1 : 0;
+  if (C > 1) {
+    int clusters = 0;
+    e = cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg);
+    if (e != cudaSuccess) return e;
+    if (clusters < 1) return cudaErrorLaunchOutOfResources;
+  }
+  return cudaLaunchKernelEx(&cfg, kern, a);
+}
+
+cudaError_t launch_gamma(ptyb_handle* h, const GammaArgs& a, int nslot) {
+  if (nslot <= 0) return cudaSuccess;
+  cudaError_t e = cudaErrorInvalidValue;
+  timed(h, kKGamma, [&] {
+    switch (h->N) {
+      case 64: e = launch_gamma_nc<64, 1>(a, nslot, h->stream); break;
+      case 128: e = launch_gamma_nc<128, 4>(a, nslot, h->stream); break;
+      case 256: e = launch_gamma_nc<256, 16>(a, nslot, h->stream); break;
+    }
+  });
+  return e;
+}
+
+void ensure_ml(ptyb_handle* h) {
+  if (h->g_obj) return;
+  const size_t no = (size_t)h->nobj * h->nyo * h->nxo, np = (size_t)h->K * h->N * h->N;
+  h->g_obj = alloc<float2>(h, no);
+  h->g_obj_c = alloc<float2>(h, no);
+  h->last_obj = alloc<float2>(h, no);
+  h->dir_obj = alloc<float2>(h, no);
+  h->g_probe = alloc<float2>(h, np);
+  h->g_probe_c = alloc<float2>(h, np);
+  h->last_probe = alloc<float2>(h, np);
+  h->dir_probe = alloc<float2>(h, np);
+  h->gamma_sums = alloc<double>(h, (size_t)h->P * 2);
+  h->partials = alloc<double>(h, kPartialBlocks * 2);
+}
+
+// Two double sums of an array (mode 0: Polak–Ribière numerator and |h|²; 1: Σ|g|), the block
+// partials added in block order on the host.
+void array_sums(ptyb_handle* h, const float2* g, const float2* hh, size_t n, int mode, double out[2]) {
+  timed(h, kKArraySums, [&] {
+    array_sums_kernel<<<kPartialBlocks, 256, 0, h->stream>>>(g, hh, n, mode, h->partials);
+  });
+  launched(h, "array sums");
+  std::vector<double> v(kPartialBlocks * 2);
+  check(h, cudaMemcpyAsync(v.data(), h->partials, v.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                           h->stream),
+        "sums");
+  check(h, cudaStreamSynchronize(h->stream), "sums");
+  out[0] = out[1] = 0.0;
+  for (int b = 0; b < kPartialBlocks; ++b) {
+    out[0] += v[b * 2];
+    out[1] += v[b * 2 + 1];
+  }
+}
+
+unsigned blocks_for(size_t n) { return (unsigned)((n + 255) / 256); }
+
+// The Poisson gradient numerators of object and probe over every frame, by stacks in frame
+// order (engine/ptycho.rs:497-561).
+void ml_gradients(ptyb_handle* h, bool uo, bool up) {
+  const size_t no = (size_t)h->nyo * h->nxo, np = (size_t)h->K * h->N * h->N;
+  check(h, cudaMemsetAsync(h->g_obj, 0, no * sizeof(float2), h->stream), "memset");
+  check(h, cudaMemsetAsync(h->g_obj_c, 0, no * sizeof(float2), h->stream), "memset");
+  check(h, cudaMemsetAsync(h->g_probe, 0, np * sizeof(float2), h->stream), "memset");
+  check(h, cudaMemsetAsync(h->g_probe_c, 0, np * sizeof(float2), h->stream), "memset");
+  if (!uo && !up) return;
+  const int stack = std::min(h->P, h->stack);
+  for (int s0 = 0; s0 < h->P; s0 += stack) {
+    const int n = std::min(stack, h->P - s0);
+    const int* frames = h->iota + s0;
+    FrameArgs a = frame_args(h, frames);
+    check(h, launch_frame<kMlGrad>(h, a, n), "ml gradient pass");
+    ++h->launches;
+    if (uo) {
+      GatherArgs g = gather_args(h, frames, n);
+      g.out = h->g_obj;
+      g.comp = h->g_obj_c;
+      timed(h, kKObjMl, [&] { object_tile_kernel<kGatherMl><<<ntiles(h), 1024, 0, h->stream>>>(g); });
+      launched(h, "object gradient");
+    }
+    if (up) {
+      int nchunk = 0;
+      const int chunk = probe_chunk(h, n, &nchunk);
+      ProbeArgs pa = {};
+      pa.object = h->object;
+      pa.quad = h->quad;
+      pa.upd = h->upd;
+      pa.frames = frames;
+      pa.corners = h->corners;
+      pa.omax = h->omax;
+      pa.partial = h->partial;
+      pa.nslot = n;
+      pa.chunk = chunk;
+      pa.nxo = h->nxo;
+      pa.K = h->K;
+      pa.N = h->N;
+      pa.mode = 1;
+      dim3 grid((h->N * h->N + 255) / 256, nchunk);
+      timed(h, kKProbePartial, [&] { probe_partial_kernel<<<grid, 256, 0, h->stream>>>(pa); });
+      launched(h, "probe gradient");
+      const int count = h->K * h->N * h->N;
+      timed(h, kKProbeFinal, [&] {
+        probe_finalize_kernel<<<(count + 255) / 256, 256, 0, h->stream>>>(
+            h->partial, nchunk, count, nullptr, h->g_probe, h->g_probe_c, 1.f, 2);
+      });
+      launched(h, "probe gradient sum");
+    }
+  }
+}
+
+// num and den of the Poisson line search along (dir_obj, dir_probe), frames summed in order.
+void ml_gamma(ptyb_handle* h, double* num, double* den) {
+  const int stack = std::min(h->P, h->stack);
+  GammaArgs a = {};
+  a.object = h->object;
+  a.d_obj = h->dir_obj;
+  a.probe = h->probe;
+  a.d_probe = h->dir_probe;
+  a.quad = h->quad;
+  a.tw = h->tw;
+  a.iobs = h->iobs;
+  a.corners = h->corners;
+  a.nyo = h->nyo;
+  a.nxo = h->nxo;
+  a.nprobe = h->nprobe;
+  a.nobj = h->nobj;
+  for (int s0 = 0; s0 < h->P; s0 += stack) {
+    const int n = std::min(stack, h->P - s0);
+    a.frames = h->iota + s0;
+    a.out = h->gamma_sums + (size_t)s0 * 2;
+    check(h, launch_gamma(h, a, n), "ml line search");
+    ++h->launches;
+  }
+  std::vector<double> v((size_t)h->P * 2);
+  check(h, cudaMemcpyAsync(v.data(), h->gamma_sums, v.size() * sizeof(double),
+                           cudaMemcpyDeviceToHost, h->stream),
+        "gamma");
+  check(h, cudaStreamSynchronize(h->stream), "gamma");
+  *num = *den = 0.0;
+  for (int f = 0; f < h->P; ++f) {
+    *num += v[(size_t)f * 2];
+    *den += v[(size_t)f * 2 + 1];
+  }
+}
+
+// In-place radix-2 FFT of n (a power of 2) complex doubles, forward, unscaled.
+void host_fft(std::vector<double>& re, std::vector<double>& im, size_t off, size_t stride, int n) {
+  std::vector<double> r(n), i(n);
+  for (int k = 0; k < n; ++k) {
+    r[k] = re[off + k * stride];
+    i[k] = im[off + k * stride];
+  }
+  for (int a = 1, j = 0; a < n; ++a) {
+    int bit = n >> 1;
+    for (; j & bit; bit >>= 1) j ^= bit;
+    j ^= bit;
+    if (a < j) {
+      std::swap(r[a], r[j]);
+      std::swap(i[a], i[j]);
+    }
+  }
+  for (int len = 2; len <= n; len <<= 1) {
+    const double ang = -2.0 * M_PI / len;
+    for (int s0 = 0; s0 < n; s0 += len)
+      for (int k = 0; k < len / 2; ++k) {
+        const double wr = std::cos(ang * k), wi = std::sin(ang * k);
+        const int u = s0 + k, v = s0 + k + len / 2;
+        const double tr = r[v] * wr - i[v] * wi, ti = r[v] * wi + i[v] * wr;
+        r[v] = r[u] - tr;
+        i[v] = i[u] - ti;
+        r[u] += tr;
+        i[u] += ti;
+      }
+  }
+  for (int k = 0; k < n; ++k) {
+    re[off + k * stride] = r[k];
+    im[off + k * stride] = i[k];
+  }
+}
+
+// PyNX ZeroPhaseRamp (engine/ptycho.rs:1134-1170): the centroid of the probe modes' summed
+// far-field intensity on the host, then the probe's and the object's phase ramps on the device.
+void zero_phase_ramp(ptyb_handle* h) {
+  const int N = h->N;
+  const size_t plane = (size_t)N * N;
+  std::vector<float2> pr((size_t)h->K * plane);
+  check(h, cudaMemcpyAsync(pr.data(), h->probe, pr.size() * sizeof(float2), cudaMemcpyDeviceToHost,
+                           h->stream),
+        "probe");
+  check(h, cudaStreamSynchronize(h->stream), "probe");
+  std::vector<double> v(plane, 0.0), re(plane), im(plane);
+  for (int m = 0; m < h->K; ++m) {
+    // far = FFT of the probe in the shifted layout
+    for (int jy = 0; jy < N; ++jy)
+      for (int jx = 0; jx < N; ++jx) {
+        const float2 p = pr[m * plane + (size_t)((jy + N / 2) % N) * N + (jx + N / 2) % N];
+        re[(size_t)jy * N + jx] = p.x;
+        im[(size_t)jy * N + jx] = p.y;
+      }
+    for (int y = 0; y < N; ++y) host_fft(re, im, (size_t)y * N, 1, N);
+    for (int x = 0; x < N; ++x) host_fft(re, im, x, N, N);
+    // v at natural i = |far[shift(i)]|²
+    for (int iy = 0; iy < N; ++iy)
+      for (int ix = 0; ix < N; ++ix) {
+        const size_t j = (size_t)((iy + N / 2) % N) * N + (ix + N / 2) % N;
+        v[(size_t)iy * N + ix] += re[j] * re[j] + im[j] * im[j];
+      }
+  }
+  double w = 0.0, wy = 0.0, wx = 0.0;
+  for (size_t i = 0; i < plane; ++i) {
+    w += v[i];
+    wy += v[i] * (double)(i / N);
+    wx += v[i] * (double)(i % N);
+  }
+  const double dy = wy / w - (double)(N / 2), dx = wx / w - (double)(N / 2);
+  const size_t np = (size_t)h->K * plane, no = (size_t)h->nobj * h->nyo * h->nxo;
+  timed(h, kKMisc, [&] {
+    ramp_kernel<<<blocks_for(np), 256, 0, h->stream>>>(h->probe, h->K, N, N, dy, dx, N, N, -1.0);
+  });
+  launched(h, "probe ramp");
+  timed(h, kKMisc, [&] {
+    ramp_kernel<<<blocks_for(no), 256, 0, h->stream>>>(h->object, h->nobj, h->nyo, h->nxo, dy, dx,
+                                                      N, N, 1.0);
+  });
+  launched(h, "object ramp");
+}
+
+// PyNX ScaleObjProbe(absolute=True) without background (engine/ptycho.rs:577-591).
+void scale_obj_probe(ptyb_handle* h) {
+  const ptyb_llk l = llk_pass(h);
+  const double s = std::sqrt(h->obs_total / l.nb_photons_calc);
+  const size_t no = (size_t)h->nobj * h->nyo * h->nxo, np = (size_t)h->K * h->N * h->N;
+  double so[2], sp[2];
+  array_sums(h, h->object, nullptr, no, 1, so);
+  array_sums(h, h->probe, nullptr, np, 1, sp);
+  const double fp = std::sqrt(so[0] / sp[0] * s), fo = std::sqrt(sp[0] / so[0] * s);
+  timed(h, kKAxpy, [&] { scale_kernel<<<blocks_for(np), 256, 0, h->stream>>>(h->probe, (float)fp, np); });
+  launched(h, "scale");
+  timed(h, kKAxpy, [&] { scale_kernel<<<blocks_for(no), 256, 0, h->stream>>>(h->object, (float)fo, no); });
+  launched(h, "scale");
 }
 
 void to_c64(const float2* src, double* dst, size_t n) {
@@ -666,7 +952,7 @@ int ptyb_create(const ptyb_scan* scan, const double* object, int32_t nobj, int32
     return PTYB_INVALID;
   }
   const int K = nprobe * nobj;
-  const int C = cluster_for(N, K);
+  const int C = cluster_for(N, K, options ? options->cluster : 0);
   if (C == 0) {
     g_create_error = "the frame's modes do not fit one cluster's shared memory";
     return PTYB_INVALID;
@@ -888,8 +1174,74 @@ int ptyb_lsqml(ptyb_handle* h, const ptyb_lsqml_params* p, int32_t nepoch, int32
 
 int ptyb_ml(ptyb_handle* h, const ptyb_ml_params* p, int32_t ncycle) {
   if (!h || !p) return PTYB_INVALID;
-  h->err = "ML is not built in this library version";
-  return PTYB_INVALID;
+  if (ncycle < 0) {
+    h->err = "ncycle must be >= 0";
+    return PTYB_INVALID;
+  }
+  return guarded(h, true, [&]() -> int {
+    ensure_slots(h, std::min(h->P, h->stack));
+    ensure_ml(h);
+    const bool uo = p->update_object != 0, up = p->update_probe != 0;
+    const size_t no = (size_t)h->nyo * h->nxo, np = (size_t)h->K * h->N * h->N;
+    begin_call(h);
+    scale_obj_probe(h);
+    check(h, cudaMemsetAsync(h->dir_obj, 0, no * sizeof(float2), h->stream), "memset");
+    check(h, cudaMemsetAsync(h->dir_probe, 0, np * sizeof(float2), h->stream), "memset");
+    bool have_last = false;
+    for (int ic = 0; ic < ncycle; ++ic) {
+      const bool due = llk_due(p->calc_llk, ic, ncycle);
+      ptyb_llk l = {};
+      if (due) l = llk_pass(h);
+      ml_gradients(h, uo, up);
+      double beta = 0.0;
+      if (have_last) {
+        double a[2], b[2];
+        array_sums(h, h->g_obj, h->last_obj, no, 0, a);
+        array_sums(h, h->g_probe, h->last_probe, np, 0, b);
+        beta = (a[0] + b[0]) / (a[1] + b[1]);
+        if (!(std::isfinite(beta) && beta >= 0.0)) beta = 0.0;
+      }
+      timed(h, kKAxpy, [&] {
+        cg_direction_kernel<<<blocks_for(no), 256, 0, h->stream>>>(h->dir_obj, h->g_obj, (float)beta, no);
+      });
+      launched(h, "direction");
+      timed(h, kKAxpy, [&] {
+        cg_direction_kernel<<<blocks_for(np), 256, 0, h->stream>>>(h->dir_probe, h->g_probe, (float)beta, np);
+      });
+      launched(h, "direction");
+      double num = 0.0, den = 0.0;
+      ml_gamma(h, &num, &den);
+      const double gamma = num / den;
+      if (std::isfinite(gamma)) {
+        timed(h, kKAxpy, [&] {
+          axpy_kernel<<<blocks_for(no), 256, 0, h->stream>>>(h->object, h->dir_obj, (float)gamma, no);
+        });
+        launched(h, "step");
+        timed(h, kKAxpy, [&] {
+          axpy_kernel<<<blocks_for(np), 256, 0, h->stream>>>(h->probe, h->dir_probe, (float)gamma, np);
+        });
+        launched(h, "step");
+      } else {
+        // No update; the direction restarts from the gradient.
+        timed(h, kKAxpy, [&] {
+          cg_direction_kernel<<<blocks_for(no), 256, 0, h->stream>>>(h->dir_obj, h->g_obj, 0.f, no);
+        });
+        launched(h, "direction");
+        timed(h, kKAxpy, [&] {
+          cg_direction_kernel<<<blocks_for(np), 256, 0, h->stream>>>(h->dir_probe, h->g_probe, 0.f, np);
+        });
+        launched(h, "direction");
+      }
+      std::swap(h->g_obj, h->last_obj);
+      std::swap(h->g_probe, h->last_probe);
+      have_last = true;
+      if (due) record(h, kAlgMl, l);
+      ++h->cycle;
+    }
+    if (p->zero_phase_ramp) zero_phase_ramp(h);
+    end_call(h, "ml");
+    return PTYB_OK;
+  });
 }
 
 int ptyb_get_llk(ptyb_handle* h, ptyb_llk* out) {

@@ -97,31 +97,45 @@ struct LineShape<256> {
   static constexpr int N1 = 16, N2 = 16;
 };
 
-// In-place FFT of one shared-memory line by the G = N2 threads t = 0..G-1 of a warp (the
-// whole warp calls it together). `tw` holds e^{-2πi·t/N} for t = 0..N-1.
+// Bank swizzle of a shared-memory line: element e of line `l` sits at l·N + (e ^ swz(l)).
+// Consecutive lines differ in bit 3 and any 16 consecutive lines take 16 distinct values, so
+// the line FFT's accesses (two to four lines per warp) and the column accesses across lines
+// each hit 16 distinct 8-byte bank pairs per half-warp.
+PTYB_HD int swz(int l) { return ((l & 1) << 3) | ((l >> 1) & 7); }
+
+// The step-1 twiddles ω_N^{t·k1}, k1 = 1..N1-1, of a thread's fixed line offset t (forward
+// sign; the inverse conjugates them), loaded once per thread.
+template <int N>
+struct LineTwiddles {
+  float2 w[LineShape<N>::N1];
+  PTYB_D void load(const float2* tw, int t) {
+#pragma unroll
+    for (int k1 = 1; k1 < LineShape<N>::N1; ++k1) w[k1] = tw[(t * k1) & (N - 1)];
+  }
+};
+
+// In-place FFT of one shared-memory line (swizzled by `sw`) by the G = N2 threads
+// t = 0..G-1 of a warp (the whole warp calls it together).
 template <int N, int DIR>
-PTYB_D void line_fft(float2* line, int t, const float2* tw) {
+PTYB_D void line_fft(float2* line, int t, const LineTwiddles<N>& tw, int sw) {
   constexpr int N1 = LineShape<N>::N1, N2 = LineShape<N>::N2;
   constexpr int P = N1 / N2;
   float2 v[N1];
 #pragma unroll
-  for (int n1 = 0; n1 < N1; ++n1) v[n1] = line[N2 * n1 + t];
+  for (int n1 = 0; n1 < N1; ++n1) v[n1] = line[(N2 * n1 + t) ^ sw];
   dft<N1, DIR>(v);
 #pragma unroll
-  for (int k1 = 1; k1 < N1; ++k1) {
-    const float2 w = tw[(t * k1) & (N - 1)];
-    v[k1] = cmul(v[k1], DIR < 0 ? w : cconj(w));
-  }
+  for (int k1 = 1; k1 < N1; ++k1) v[k1] = cmul(v[k1], DIR < 0 ? tw.w[k1] : cconj(tw.w[k1]));
   __syncwarp();
 #pragma unroll
-  for (int k1 = 0; k1 < N1; ++k1) line[k1 * N2 + ((t + k1) & (N2 - 1))] = v[k1];
+  for (int k1 = 0; k1 < N1; ++k1) line[(k1 * N2 + ((t + k1) & (N2 - 1))) ^ sw] = v[k1];
   __syncwarp();
 #pragma unroll
   for (int p = 0; p < P; ++p) {
     const int k1 = t + N2 * p;
     float2 u[N2];
 #pragma unroll
-    for (int n2 = 0; n2 < N2; ++n2) u[n2] = line[k1 * N2 + ((n2 + k1) & (N2 - 1))];
+    for (int n2 = 0; n2 < N2; ++n2) u[n2] = line[(k1 * N2 + ((n2 + k1) & (N2 - 1))) ^ sw];
     dft<N2, DIR>(u);
 #pragma unroll
     for (int k2 = 0; k2 < N2; ++k2) v[p * N2 + k2] = u[k2];
@@ -131,7 +145,7 @@ PTYB_D void line_fft(float2* line, int t, const float2* tw) {
   for (int p = 0; p < P; ++p) {
     const int k1 = t + N2 * p;
 #pragma unroll
-    for (int k2 = 0; k2 < N2; ++k2) line[k1 + N1 * k2] = v[p * N2 + k2];
+    for (int k2 = 0; k2 < N2; ++k2) line[(k1 + N1 * k2) ^ sw] = v[p * N2 + k2];
   }
   __syncwarp();
 }

@@ -2,8 +2,9 @@
 // inverse 2-D FFT → exit-wave update, for every probe mode of one diffraction frame, on one
 // thread-block cluster whose distributed shared memory holds the frame's K planes.
 //
-// Cluster of C CTAs, CTA rank r owning H = N/C rows. Shared memory holds K·H lines of
-// L = N+1 float2 (the pad keeps transposed accesses off one bank). The row FFTs run on rows; a
+// Cluster of C CTAs, CTA rank r owning H = N/C rows. Shared memory holds K·H lines of N
+// float2, each XOR-swizzled (`swz`) so no access pattern conflicts on banks. The row FFTs run
+// on rows; a
 // cluster-wide transpose through DSMEM turns the rows into H columns per CTA, stored as lines,
 // so the column FFTs, the per-pixel projection (which needs every mode at a pixel) and the
 // inverse column FFTs run on local lines; a second transpose brings the rows back for the
@@ -48,7 +49,14 @@ struct FrameArgs {
   float* icalc;          // [slot][N][N] Σ_modes |Ψ|², detector layout
   float* omax;           // [slot] max |O|² over the window (object mode 0)
   double* llk;           // [slot][4] Poisson, Gaussian, Euclidian, photons
-  const float* a_far;    // [slot] LSQML far-field step
+  const float* a_far;    // [slot] LSQML far-field step (kLsqmlFused)
+  // LSQML Poisson far-field step, PtychoShelves' xi solver in two passes
+  // (engine/lsqml.rs:133-150): kStore runs pass 1 from `a_prev` (by frame when
+  // `a_prev_by_frame`), kFromStore pass 2 from `a_mid`; each writes its result to `a_out`.
+  const float* a_prev;
+  const float* a_mid;
+  float* a_out;
+  int a_prev_by_frame, nslot;
   int nyo, nxo, nprobe, nobj, cost;
 };
 
@@ -56,7 +64,7 @@ template <int N, int C>
 struct FrameShape {
   static constexpr int H = N / C;           // rows (then columns) per CTA
   static constexpr int T = H * N / 16;      // threads: 16 transposed values each per mode
-  static constexpr int L = N + 1;           // line stride in float2
+  static constexpr int L = N;               // line stride in float2 (lines are swizzled)
   static constexpr int G = LineShape<N>::N2; // threads per line FFT
   static constexpr int E = H * N / T;       // = 16
 };
@@ -79,10 +87,11 @@ PTYB_D void csync(cg::cluster_group& cluster) {
 // Every local line through a forward (DIR = -1) or inverse (+1) line FFT; the block barrier at
 // the end publishes every line to every thread of the CTA.
 template <int N, int C, int DIR>
-PTYB_D void all_lines(float2* S, int nlines, const float2* tw) {
+PTYB_D void all_lines(float2* S, int nlines, const LineTwiddles<N>& tw) {
   using F = FrameShape<N, C>;
   const int g = threadIdx.x / F::G, t = threadIdx.x % F::G;
-  for (int line = g; line < nlines; line += F::T / F::G) line_fft<N, DIR>(S + line * F::L, t, tw);
+  for (int line = g; line < nlines; line += F::T / F::G)
+    line_fft<N, DIR>(S + line * F::L, t, tw, swz(line));
   __syncthreads();
 }
 
@@ -100,14 +109,16 @@ PTYB_D void transpose(float2* S, int K, cg::cluster_group& cluster) {
       const int e = threadIdx.x + i * F::T;
       const int c = e % F::H, j = e / F::H;
       const float2* src = C > 1 ? cluster.map_shared_rank(S, j / F::H) : S;
-      v[i] = src[(m * F::H + j % F::H) * F::L + r * F::H + c];
+      const int sl = m * F::H + j % F::H;
+      v[i] = src[sl * F::L + ((r * F::H + c) ^ swz(sl))];
     }
     csync<C>(cluster);
 #pragma unroll
     for (int i = 0; i < F::E; ++i) {
       const int e = threadIdx.x + i * F::T;
       const int c = e % F::H, j = e / F::H;
-      S[(m * F::H + c) * F::L + j] = v[i];
+      const int dl = m * F::H + c;
+      S[dl * F::L + (j ^ swz(dl))] = v[i];
     }
   }
   __syncthreads();
@@ -133,6 +144,39 @@ PTYB_D void block_sum(double (&v)[4], int n, double* red) {
   __syncthreads();
 }
 
+// Mean of the launch's far-field steps, summed by warp 0 in a fixed order (lane-strided
+// partial sums, then a fixed butterfly), so every CTA gets the same value; broadcast through
+// `slot` in shared memory (block barrier inside).
+PTYB_D double batch_mean(const float* v, const int* frames, int by_frame, int nslot,
+                         double* slot) {
+  if (threadIdx.x < 32) {
+    double s = 0.0;
+    for (int i = threadIdx.x; i < nslot; i += 32) s += v[by_frame ? frames[i] : i];
+    s = warp_sum(s);
+    if (threadIdx.x == 0) *slot = s / nslot;
+  }
+  __syncthreads();
+  return *slot;
+}
+
+// Cluster-wide sums of two doubles (every CTA gets the totals, added in rank order).
+template <int N, int C>
+PTYB_D void cluster_sum2(double& x, double& y, double* red, cg::cluster_group& cluster) {
+  using F = FrameShape<N, C>;
+  double v[4] = {x, y, 0.0, 0.0};
+  block_sum<F::T>(v, 2, red);
+  csync<C>(cluster);
+  double sx = 0.0, sy = 0.0;
+  for (int q = 0; q < C; ++q) {
+    const double* rq = C > 1 ? cluster.map_shared_rank(red, q) : red;
+    sx += rq[0];
+    sy += rq[1];
+  }
+  csync<C>(cluster);
+  x = sx;
+  y = sy;
+}
+
 template <int N, int C, int MODE>
 __global__ void __launch_bounds__(FrameShape<N, C>::T)
     frame_kernel(FrameArgs a) {
@@ -149,27 +193,36 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T)
   const int f = a.frames[slot];
   const int2 corner = a.corners[f];
   const int tid = threadIdx.x;
-  for (int i = tid; i < N; i += T) tw[i] = a.tw[i];
+  LineTwiddles<N> ltw;
+  ltw.load(a.tw, tid % F::G);
+  (void)tw;
 
   float omax = 0.f;
   if (MODE == kFromStore) {
     const float2* src = a.field + ((size_t)slot * C + r) * K * H * N;
+#pragma unroll 8
     for (int idx = tid; idx < K * H * N; idx += T) {
       const int line = idx / N, e = idx % N;
-      S[line * L + e] = src[idx];
+      S[line * L + (e ^ swz(line))] = src[idx];
     }
   } else {
-    // Exit waves ψ = P·O·q of shifted rows r·H .. r·H+H-1, every mode.
-    for (int idx = tid; idx < K * H * N; idx += T) {
-      const int m = idx / (H * N), rem = idx % (H * N);
-      const int yl = rem / N, jx = rem % N;
+    // Exit waves ψ = P·O·q of shifted rows r·H .. r·H+H-1, every mode; the object window and
+    // the phase are read once per pixel.
+#pragma unroll 2
+    for (int idx = tid; idx < H * N; idx += T) {
+      const int yl = idx / N, jx = idx % N;
       const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
-      const int pm = m % a.nprobe, om = m / a.nprobe;
-      const float2 p = a.probe[((size_t)pm * N + ny) * N + nx];
-      const float2 o = a.object[((size_t)om * a.nyo + corner.x + ny) * a.nxo + corner.y + nx];
       const float2 q = a.quad[ny * N + nx];
-      S[(m * H + yl) * L + jx] = cmul(cmul(p, o), q);
-      if (MODE == kRpie && om == 0) omax = fmaxf(omax, cnorm2(o));
+      for (int om = 0; om < a.nobj; ++om) {
+        const float2 o = a.object[((size_t)om * a.nyo + corner.x + ny) * a.nxo + corner.y + nx];
+        const float2 oq = cmul(o, q);
+        if (MODE == kRpie && om == 0) omax = fmaxf(omax, cnorm2(o));
+        for (int pm = 0; pm < a.nprobe; ++pm) {
+          const int line = (om * a.nprobe + pm) * H + yl;
+          // (P·O)·q as P·(O·q): the reference's product up to rounding
+          S[line * L + (jx ^ swz(line))] = cmul(a.probe[((size_t)pm * N + ny) * N + nx], oq);
+        }
+      }
     }
   }
   __syncthreads();
@@ -188,7 +241,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T)
   }
 
   if (MODE != kFromStore) {
-    all_lines<N, C, -1>(S, K * H, tw);
+    all_lines<N, C, -1>(S, K * H, ltw);
     transpose<N, C>(S, K, cluster);  // its first cluster barrier publishes red[0]
     if (MODE == kRpie && r == 0 && tid == 0) {
       float mx = 0.f;
@@ -196,7 +249,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T)
         mx = fmaxf(mx, *reinterpret_cast<float*>(C > 1 ? cluster.map_shared_rank(red, q) : red));
       a.omax[slot] = mx;
     }
-    all_lines<N, C, -1>(S, K * H, tw);
+    all_lines<N, C, -1>(S, K * H, ltw);
   }
 
   // Detector plane: CTA r holds columns r·H .. r·H+H-1 as lines (m·H + c), elements ky.
@@ -205,17 +258,42 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T)
   constexpr float inv_n2 = 1.0f / ((float)N * (float)N);
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
   const float* iobs = a.iobs + (size_t)f * N * N;
-  const float afar = (MODE == kLsqmlFused || MODE == kFromStore) ? a.a_far[slot] : 0.f;
+  float afar = MODE == kLsqmlFused ? a.a_far[slot] : 0.f;
+  if ((MODE == kStore || MODE == kFromStore) && a.cost == kCostPoisson && a.a_out) {
+    // One pass of the Poisson xi solver over this frame: with prev the batch mean of the
+    // previous pass, a = clip(prev/2 + Σ xi·(Ĩ − I/(1 − prev·xi)) / Σ xi²·Ĩ / 2, 0, 1).
+    const double prev = MODE == kStore
+                            ? batch_mean(a.a_prev, a.frames, a.a_prev_by_frame, a.nslot, red + 7)
+                            : batch_mean(a.a_mid, a.frames, 0, a.nslot, red + 7);
+    double num = 0.0, den = 0.0;
+#pragma unroll 4
+    for (int idx = tid; idx < H * N; idx += T) {
+      const int c = idx % H, ky = idx / H;
+      const float yo = iobs[ky * N + r * H + c];
+      if (yo < 0.f) continue;
+      float ic = 0.f;
+      for (int m = 0; m < K; ++m) ic += cnorm2(S[(m * H + c) * L + (ky ^ swz(m * H + c))]);
+      const double yp = (double)(ic * inv_n2), yt = yo;
+      const double xi = 1.0 - yt / (yp + 1e-5);
+      num += xi * (yp - yt / (1.0 - prev * xi));
+      den += xi * xi * yp;
+    }
+    cluster_sum2<N, C>(num, den, red, cluster);
+    const double ratio = den > 0.0 ? num / den : 0.0;
+    afar = (float)fmin(fmax(0.5 * prev + 0.5 * ratio, 0.0), 1.0);
+    if (r == 0 && tid == 0) a.a_out[slot] = afar;
+  }
+#pragma unroll 4
   for (int idx = tid; idx < H * N; idx += T) {
     const int c = idx % H, ky = idx / H;
     const int kx = r * H + c;
     float ic = 0.f;
-    for (int m = 0; m < K; ++m) ic += cnorm2(S[(m * H + c) * L + ky]);
+    for (int m = 0; m < K; ++m) ic += cnorm2(S[(m * H + c) * L + (ky ^ swz(m * H + c))]);
     ic *= inv_n2;
     const float yo = iobs[ky * N + kx];
     const bool masked = yo < 0.f;
     if (MODE == kStore) {
-      a.icalc[((size_t)slot * N + ky) * N + kx] = ic;
+      if (a.icalc) a.icalc[((size_t)slot * N + ky) * N + kx] = ic;
       continue;
     }
     if (MODE == kLlk) {
@@ -243,7 +321,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T)
     }
     fac *= inv_n2;
     for (int m = 0; m < K; ++m) {
-      float2& v = S[(m * H + c) * L + ky];
+      float2& v = S[(m * H + c) * L + (ky ^ swz(m * H + c))];
       v = cscale(v, fac);
     }
   }
@@ -265,32 +343,39 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T)
   if (MODE == kStore) {
     __syncthreads();
     float2* dst = a.field + ((size_t)slot * C + r) * K * H * N;
+#pragma unroll 8
     for (int idx = tid; idx < K * H * N; idx += T) {
       const int line = idx / N, e = idx % N;
-      dst[idx] = S[line * L + e];
+      dst[idx] = S[line * L + (e ^ swz(line))];
     }
     return;
   }
   __syncthreads();
-  all_lines<N, C, +1>(S, K * H, tw);
+  all_lines<N, C, +1>(S, K * H, ltw);
   transpose<N, C>(S, K, cluster);
-  all_lines<N, C, +1>(S, K * H, tw);
+  all_lines<N, C, +1>(S, K * H, ltw);
 
-  // Epilogue on shifted rows: out = ψ' − ψ (or ψ'), natural layout.
+  // Epilogue on shifted rows: out = ψ' − ψ (or ψ'), natural layout; the object window and the
+  // phase are read once per pixel.
   float2* out = a.out + (size_t)slot * K * N * N;
-  for (int idx = tid; idx < K * H * N; idx += T) {
-    const int m = idx / (H * N), rem = idx % (H * N);
-    const int yl = rem / N, jx = rem % N;
+#pragma unroll 2
+  for (int idx = tid; idx < H * N; idx += T) {
+    const int yl = idx / N, jx = idx % N;
     const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
-    float2 v = S[(m * H + yl) * L + jx];
-    if (MODE != kMlGrad) {
-      const int pm = m % a.nprobe, om = m / a.nprobe;
-      const float2 p = a.probe[((size_t)pm * N + ny) * N + nx];
-      const float2 o = a.object[((size_t)om * a.nyo + corner.x + ny) * a.nxo + corner.y + nx];
-      const float2 q = a.quad[ny * N + nx];
-      v = csub(v, cmul(cmul(p, o), q));
+    float2 q = make_float2(0.f, 0.f);
+    if (MODE != kMlGrad) q = a.quad[ny * N + nx];
+    for (int om = 0; om < a.nobj; ++om) {
+      float2 oq = make_float2(0.f, 0.f);
+      if (MODE != kMlGrad)
+        oq = cmul(a.object[((size_t)om * a.nyo + corner.x + ny) * a.nxo + corner.y + nx], q);
+      for (int pm = 0; pm < a.nprobe; ++pm) {
+        const int m = om * a.nprobe + pm;
+        const int line = m * H + yl;
+        float2 v = S[line * L + (jx ^ swz(line))];
+        if (MODE != kMlGrad) v = csub(v, cmul(a.probe[((size_t)pm * N + ny) * N + nx], oq));
+        out[((size_t)m * N + ny) * N + nx] = v;
+      }
     }
-    out[((size_t)m * N + ny) * N + nx] = v;
   }
 }
 

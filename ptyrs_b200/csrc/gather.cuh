@@ -1,10 +1,11 @@
 // Deterministic scatter-adds of the per-view updates onto the object and the probe.
 //
-// Object: one CTA owns a 32×32 object tile, lists the launch's views that overlap it in
-// ascending slot order (the reference's view order) and accumulates every pixel of the tile
-// over that list with Kahan-compensated float sums, so no atomics touch the object and the
-// result does not depend on scheduling (the reference's tile-owned gather,
-// ptyrs-kernels/src/lib.rs:388-437; operator engine/ops.rs:282-310). Probe: the slots are cut
+// Object: one CTA owns a 16×16 object tile and lists the launch's views that overlap it in
+// ascending slot order (the reference's view order); four thread groups per pixel take every
+// fourth view of that list, each with Kahan-compensated float sums, and the groups' sums are
+// added in group order. No atomics touch the object and the result does not depend on
+// scheduling (the reference's tile-owned gather, ptyrs-kernels/src/lib.rs:388-437; operator
+// engine/ops.rs:282-310). Probe: the slots are cut
 // into chunks, each CTA sums one chunk in slot order for 256 probe pixels, and a second pass
 // adds the chunk sums in chunk order (engine/ops.rs:315-345).
 #pragma once
@@ -12,7 +13,8 @@
 
 namespace ptyb {
 
-constexpr int kTile = 32;
+constexpr int kTile = 16;      // object tile side
+constexpr int kGroups = 4;     // view groups per pixel
 constexpr int kMaxModes = 4;
 
 enum GatherMode : int {
@@ -39,40 +41,67 @@ struct GatherArgs {
   int nslot, nyo, nxo, nprobe, N;
 };
 
-// The launch's slots whose window overlaps the tile [ty0, ty0+32) × [tx0, tx0+32), in
-// ascending order, for slots [s0, s1): list built by warp 0 with ballots.
-PTYB_D int tile_list(const GatherArgs& a, int s0, int s1, int ty0, int tx0, int* list) {
-  __shared__ int count;
-  if (threadIdx.x < 32) {
-    int n = 0;
-    const int lane = threadIdx.x;
-    for (int base = s0; base < s1; base += 32) {
-      const int s = base + lane;
-      bool hit = false;
-      if (s < s1) {
-        const int2 c = a.corners[a.frames[s]];
-        hit = c.x < ty0 + kTile && c.x + a.N > ty0 && c.y < tx0 + kTile && c.y + a.N > tx0;
-      }
-      const unsigned m = __ballot_sync(0xffffffffu, hit);
-      if (hit) list[n + __popc(m & ((1u << lane) - 1u))] = s;
-      n += __popc(m);
+// The launch's slots in [s0, s1) (at most 1024) whose window overlaps the tile
+// [ty0, ty0+16) × [tx0, tx0+16), in ascending order with their corners: an ordered
+// compaction by all 1024 threads (warp ballots, then a prefix over the warps).
+PTYB_D int tile_list(const GatherArgs& a, int s0, int s1, int ty0, int tx0, int* list,
+                     int2* corner) {
+  __shared__ int wbase[32];
+  __shared__ int total;
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const int s = s0 + t;
+  bool hit = false;
+  int2 c = make_int2(0, 0);
+  if (s < s1) {
+    c = a.corners[a.frames[s]];
+    hit = c.x < ty0 + kTile && c.x + a.N > ty0 && c.y < tx0 + kTile && c.y + a.N > tx0;
+  }
+  const unsigned m = __ballot_sync(0xffffffffu, hit);
+  if (lane == 0) wbase[w] = __popc(m);
+  __syncthreads();
+  if (w == 0) {
+    const int v = wbase[lane];
+    int incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += u;
     }
-    if (lane == 0) count = n;
+    wbase[lane] = incl - v;
+    if (lane == 31) total = incl;
   }
   __syncthreads();
-  const int n = count;
+  if (hit) {
+    const int pos = wbase[w] + __popc(m & ((1u << lane) - 1u));
+    list[pos] = s;
+    corner[pos] = c;
+  }
+  __syncthreads();
+  const int n = total;
   __syncthreads();
   return n;
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(1024) object_tile_kernel(GatherArgs a) {
+__global__ void __launch_bounds__(1024, MODE == kGatherRpie ? 1 : 2) object_tile_kernel(GatherArgs a) {
   constexpr int kChunk = 1024;
-  __shared__ int list[kChunk];
+  constexpr int kPix = kTile * kTile;  // 256 pixels, kGroups threads each
+  // The view list (during the walk), then the groups' partial sums (after it).
+  constexpr int kListBytes = kChunk * (sizeof(int) + sizeof(int2));
+  constexpr int kNumBytes = (kGroups - 1) * kMaxModes * kPix * sizeof(float2);
+  constexpr int kDenBytes = (kGroups - 1) * kMaxModes * kPix * sizeof(float);
+  constexpr int kPartBytes = kNumBytes + kDenBytes + (kGroups - 1) * kPix * sizeof(int);
+  __shared__ __align__(16) unsigned char sm[kListBytes > kPartBytes ? kListBytes : kPartBytes];
   __shared__ float red[32];
+  int* list = reinterpret_cast<int*>(sm);
+  int2* lcorner = reinterpret_cast<int2*>(sm + kChunk * sizeof(int));
+  float2(*part_num)[kMaxModes][kPix] = reinterpret_cast<float2(*)[kMaxModes][kPix]>(sm);
+  float(*part_den)[kMaxModes][kPix] = reinterpret_cast<float(*)[kMaxModes][kPix]>(sm + kNumBytes);
+  int(*part_cov)[kPix] = reinterpret_cast<int(*)[kPix]>(sm + kNumBytes + kDenBytes);
   const int tiles_x = (a.nxo + kTile - 1) / kTile;
   const int tx0 = (blockIdx.x % tiles_x) * kTile, ty0 = (blockIdx.x / tiles_x) * kTile;
-  const int x = tx0 + threadIdx.x % kTile, y = ty0 + threadIdx.x / kTile;
+  const int px = threadIdx.x % kPix, grp = threadIdx.x / kPix;
+  const int x = tx0 + px % kTile, y = ty0 + px / kTile;
   const bool inside = x < a.nxo && y < a.nyo;
   const int K = a.nprobe;
   const int N = a.N;
@@ -87,16 +116,22 @@ __global__ void __launch_bounds__(1024) object_tile_kernel(GatherArgs a) {
   bool covered = false, any = false;
   for (int s0 = 0; s0 < a.nslot; s0 += kChunk) {
     const int s1 = min(a.nslot, s0 + kChunk);
-    const int n = tile_list(a, s0, s1, ty0, tx0, list);
+    const int n = tile_list(a, s0, s1, ty0, tx0, list, lcorner);
     any |= n > 0;
-    for (int i = 0; i < n; ++i) {
+#pragma unroll 2
+    for (int i = grp; i < n; i += kGroups) {
       const int s = list[i];
-      const int2 c = a.corners[a.frames[s]];
+      const int2 c = lcorner[i];
       const int yy = y - c.x, xx = x - c.y;
       if (!inside || yy < 0 || yy >= N || xx < 0 || xx >= N) continue;
       covered = true;
       const int pix = yy * N + xx;
       const float2 q = a.quad[pix];
+      float2 u[kMaxModes];
+#pragma unroll
+      for (int m = 0; m < kMaxModes; ++m)
+        if (m < K && (MODE == kGatherRpie || MODE == kGatherLsqml || MODE == kGatherMl))
+          u[m] = a.upd[((size_t)s * K + m) * plane + pix];
 #pragma unroll
       for (int m = 0; m < kMaxModes; ++m) {
         if (m >= K) break;
@@ -104,8 +139,7 @@ __global__ void __launch_bounds__(1024) object_tile_kernel(GatherArgs a) {
         if (MODE == kGatherOverlap || MODE == kGatherIllum || MODE == kGatherRpie)
           den[m].add(cnorm2(p));
         if (MODE == kGatherRpie || MODE == kGatherLsqml || MODE == kGatherMl) {
-          const float2 u = a.upd[((size_t)s * K + m) * plane + pix];
-          const float2 t = cmulc(cmul(p, q), u);  // conj(P·q)·u
+          const float2 t = cmulc(cmul(p, q), u[m]);  // conj(P·q)·u
           if (MODE == kGatherRpie)
             num[m].add(t);
           else
@@ -114,13 +148,35 @@ __global__ void __launch_bounds__(1024) object_tile_kernel(GatherArgs a) {
       }
     }
   }
+  // Groups 1..3 hand their compensated sums to group 0, which adds them in group order.
+  __syncthreads();  // the list's space becomes the partial sums'
+  if (grp > 0) {
+#pragma unroll
+    for (int m = 0; m < kMaxModes; ++m) {
+      part_num[grp - 1][m][px] = make_float2(num[m].re.s - num[m].re.c, num[m].im.s - num[m].im.c);
+      part_den[grp - 1][m][px] = den[m].s - den[m].c;
+    }
+    part_cov[grp - 1][px] = covered;
+  }
+  __syncthreads();
+  if (grp == 0) {
+#pragma unroll
+    for (int g = 0; g < kGroups - 1; ++g) {
+#pragma unroll
+      for (int m = 0; m < kMaxModes; ++m) {
+        num[m].add(part_num[g][m][px]);
+        den[m].add(part_den[g][m][px]);
+      }
+      covered |= part_cov[g][px] != 0;
+    }
+  }
   const size_t o = (size_t)y * a.nxo + x;
   if (MODE == kGatherOverlap) {
     float d = 0.f;
 #pragma unroll
     for (int m = 0; m < kMaxModes; ++m)
       if (m < K) d += den[m].s;
-    d = warp_max(inside ? d : 0.f);
+    d = warp_max(inside && grp == 0 ? d : 0.f);
     if (threadIdx.x % 32 == 0) red[threadIdx.x / 32] = d;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -130,7 +186,7 @@ __global__ void __launch_bounds__(1024) object_tile_kernel(GatherArgs a) {
     }
     return;
   }
-  if (!inside) return;
+  if (!inside || grp != 0) return;
   if (MODE == kGatherRpie) {
     if (!covered) return;
     const float pmax = *a.pmax;
@@ -178,23 +234,34 @@ struct ProbeArgs {
   int nslot, chunk, nxo, K, N, mode;  // mode 0 rPIE weight, 1 plain conj(q·O)
 };
 
-// Chunk `blockIdx.y` of slots, 256 probe pixels per CTA: Σ_slots w·upd in slot order.
+constexpr int kMaxProbeChunk = 256;
+
+// Chunk `blockIdx.y` of slots (at most kMaxProbeChunk), 256 probe pixels per CTA:
+// Σ_slots w·upd in slot order.
 __global__ void __launch_bounds__(256) probe_partial_kernel(ProbeArgs a) {
+  __shared__ int2 cs[kMaxProbeChunk];
+  __shared__ float om[kMaxProbeChunk];
   const int N = a.N;
   const size_t plane = (size_t)N * N;
+  const int s0 = blockIdx.y * a.chunk, s1 = min(a.nslot, s0 + a.chunk);
+  for (int i = threadIdx.x; i < s1 - s0; i += 256) {
+    cs[i] = a.corners[a.frames[s0 + i]];
+    om[i] = a.mode == 0 ? a.omax[s0 + i] : 0.f;
+  }
+  __syncthreads();
   const int pix = blockIdx.x * 256 + threadIdx.x;
   if (pix >= N * N) return;
   const int yy = pix / N, xx = pix % N;
-  const int s0 = blockIdx.y * a.chunk, s1 = min(a.nslot, s0 + a.chunk);
   const float2 q = a.quad[pix];
   KahanC acc[kMaxModes];
 #pragma unroll
   for (int m = 0; m < kMaxModes; ++m) acc[m].init();
+#pragma unroll 4
   for (int s = s0; s < s1; ++s) {
-    const int2 c = a.corners[a.frames[s]];
+    const int2 c = cs[s - s0];
     const float2 o = a.object[(size_t)(c.x + yy) * a.nxo + c.y + xx];
     float2 w = cconj(cmul(o, q));
-    if (a.mode == 0) w = cscale(w, 1.f / ((1.f - a.alpha) * cnorm2(o) + a.alpha * a.omax[s]));
+    if (a.mode == 0) w = cscale(w, 1.f / ((1.f - a.alpha) * cnorm2(o) + a.alpha * om[s - s0]));
 #pragma unroll
     for (int m = 0; m < kMaxModes; ++m) {
       if (m >= a.K) break;

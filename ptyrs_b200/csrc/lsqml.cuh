@@ -18,55 +18,21 @@ PTYB_D double block_sum1(double v, double* sh) {
   return s;
 }
 
-// One pass of PtychoShelves' Poisson `xi` solver per slot: with `prev` the slot-order mean of
-// `a_in` (indexed by frame when `by_frame`), a = clip(prev/2 + Σ xi·(Ĩ − I/(1 − prev·xi)) /
-// Σ xi²·Ĩ / 2, 0, 1), xi = 1 − I/(Ĩ + 1e-5), over unmasked pixels.
-__global__ void __launch_bounds__(256) afar_kernel(const float* icalc, const float* iobs,
-                                                   const int* frames, const float* a_in,
-                                                   int by_frame, float* a_out, int nslot,
-                                                   int npix) {
-  __shared__ double sh[8];
-  __shared__ double prev_s;
-  if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int i = 0; i < nslot; ++i) s += a_in[by_frame ? frames[i] : i];
-    prev_s = s / nslot;
-  }
-  __syncthreads();
-  const double prev = prev_s;
-  const int slot = blockIdx.x;
-  const float* ic = icalc + (size_t)slot * npix;
-  const float* io = iobs + (size_t)frames[slot] * npix;
-  double num = 0.0, den = 0.0;
-  for (int j = threadIdx.x; j < npix; j += 256) {
-    const double yt = io[j];
-    if (yt < 0.0) continue;
-    const double yp = ic[j];
-    const double xi = 1.0 - yt / (yp + 1e-5);
-    num += xi * (yp - yt / (1.0 - prev * xi));
-    den += xi * xi * yp;
-  }
-  num = block_sum1<256>(num, sh);
-  den = block_sum1<256>(den, sh);
-  if (threadIdx.x == 0) {
-    const double ratio = den > 0.0 ? num / den : 0.0;
-    a_out[slot] = (float)fmin(fmax(0.5 * prev + 0.5 * ratio, 0.0), 1.0);
-  }
-}
-
 // Per slot, the six sums of the step-size system over its modes and pixels (natural layout):
 // u = P·dO·q (dop), v = dP·O·q (dpo), c = χ: Σ|u|²+λ0, Σ|v|²+λ0, Σ Re u·v̄, Σ Im u·v̄,
-// Σ Re ū·c, Σ Re v̄·c.
-__global__ void __launch_bounds__(256) lsqml_dots_kernel(
+// Σ Re ū·c, Σ Re v̄·c (engine/lsqml.rs:302-323). Each thread sums its pixels in float, the
+// block adds the threads' sums in double; λ0 joins once per pixel and mode.
+__global__ void __launch_bounds__(512) lsqml_dots_kernel(
     const float2* object, const float2* d_obj, const float2* probe, const float2* d_probe,
     const float2* quad, const float2* chi, const int* frames, const int2* corners, int nxo,
     int K, int N, double lambda0, double* sums) {
-  __shared__ double sh[8];
+  __shared__ double sh[16];
   const int slot = blockIdx.x;
   const int2 c = corners[frames[slot]];
   const size_t plane = (size_t)N * N;
-  double s[6] = {0, 0, 0, 0, 0, 0};
-  for (int idx = threadIdx.x; idx < K * N * N; idx += 256) {
+  float s[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll 4
+  for (int idx = threadIdx.x; idx < K * N * N; idx += 512) {
     const int m = idx / (N * N), pix = idx % (N * N);
     const int yy = pix / N, xx = pix % N;
     const size_t o = (size_t)(c.x + yy) * nxo + c.y + xx;
@@ -74,16 +40,17 @@ __global__ void __launch_bounds__(256) lsqml_dots_kernel(
     const float2 u = cmul(cmul(probe[m * plane + pix], d_obj[o]), q);
     const float2 v = cmul(cmul(d_probe[m * plane + pix], object[o]), q);
     const float2 x = chi[((size_t)slot * K + m) * plane + pix];
-    s[0] += (double)cnorm2(u) + lambda0;
-    s[1] += (double)cnorm2(v) + lambda0;
-    s[2] += (double)u.x * v.x + (double)u.y * v.y;
-    s[3] += (double)u.y * v.x - (double)u.x * v.y;
-    s[4] += (double)u.x * x.x + (double)u.y * x.y;
-    s[5] += (double)v.x * x.x + (double)v.y * x.y;
+    s[0] += cnorm2(u);
+    s[1] += cnorm2(v);
+    s[2] += u.x * v.x + u.y * v.y;
+    s[3] += u.y * v.x - u.x * v.y;
+    s[4] += u.x * x.x + u.y * x.y;
+    s[5] += v.x * x.x + v.y * x.y;
   }
+  const double reg = lambda0 * (double)K * (double)plane;
   for (int k = 0; k < 6; ++k) {
-    const double t = block_sum1<256>(s[k], sh);
-    if (threadIdx.x == 0) sums[(size_t)slot * 6 + k] = t;
+    const double t = block_sum1<512>((double)s[k], sh);
+    if (threadIdx.x == 0) sums[(size_t)slot * 6 + k] = t + (k < 2 ? reg : 0.0);
   }
 }
 

@@ -1,0 +1,207 @@
+// Poisson maximum-likelihood conjugate gradient on the device (physwkim/ptyrs
+// engine/ptycho.rs:775-842): the line-search numerator and denominator of
+// `cg_poisson_gamma` (engine/ops.rs:206-253) per frame, and the array reductions of the
+// Polak–Ribière β and of `scale_obj_probe` (engine/ptycho.rs:577-591).
+#pragma once
+#include "frame.cuh"
+
+namespace ptyb {
+
+// Per frame: po = F(P·O·q), a = F(P·dO·q + dP·O·q), b = F(dP·dO·q) mode by mode, with
+// per-pixel accumulators calc = Σ|po|², r = Σ Re(p̄o·a), s = Σ |a|² + 2·Re(p̄o·b); then over
+// unmasked pixels, d = 1 − I/max(calc, 1e-32): num = −Σ 2·r·d, den = Σ 2·s·d + I·(2r/calc)².
+// Shared memory: two planes (po, then a / b) of H lines and the three accumulators.
+struct GammaArgs {
+  const float2* object;
+  const float2* d_obj;
+  const float2* probe;
+  const float2* d_probe;
+  const float2* quad;
+  const float2* tw;
+  const float* iobs;
+  const int* frames;
+  const int2* corners;
+  double* out;  // [slot][2]: num, den
+  int nyo, nxo, nprobe, nobj;
+};
+
+template <int N, int C>
+__host__ __device__ constexpr size_t gamma_smem_bytes() {
+  using F = FrameShape<N, C>;
+  return 2 * (size_t)F::H * F::L * sizeof(float2) + 3 * (size_t)F::H * N * sizeof(float) +
+         N * sizeof(float2) + 160 * sizeof(double);
+}
+
+template <int N, int C>
+__global__ void __launch_bounds__(FrameShape<N, C>::T) gamma_kernel(GammaArgs a) {
+  using F = FrameShape<N, C>;
+  constexpr int H = F::H, T = F::T, L = F::L;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float2* S0 = reinterpret_cast<float2*>(smem_raw);  // po
+  float2* S1 = S0 + (size_t)H * L;                   // a, then b
+  float* acc = reinterpret_cast<float*>(S1 + (size_t)H * L);  // [3][H·N]
+  float2* tw = reinterpret_cast<float2*>(acc + 3 * H * N);
+  double* red = reinterpret_cast<double*>(tw + N);
+  cg::cluster_group cluster = cg::this_cluster();
+  const int r = C > 1 ? (int)cluster.block_rank() : 0;
+  const int slot = blockIdx.x / C;
+  const int f = a.frames[slot];
+  const int2 corner = a.corners[f];
+  const int tid = threadIdx.x;
+  const int K = a.nprobe * a.nobj;
+  constexpr float inv_n2 = 1.0f / ((float)N * (float)N);
+  LineTwiddles<N> ltw;
+  ltw.load(a.tw, tid % F::G);
+  (void)tw;
+  for (int i = tid; i < 3 * H * N; i += T) acc[i] = 0.f;
+
+  for (int m = 0; m < K; ++m) {
+    const int pm = m % a.nprobe, om = m / a.nprobe;
+    // Exit-plane rows of po and a.
+#pragma unroll 4
+    for (int idx = tid; idx < H * N; idx += T) {
+      const int yl = idx / N, jx = idx % N;
+      const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
+      const size_t pi = ((size_t)pm * N + ny) * N + nx;
+      const size_t oi = ((size_t)om * a.nyo + corner.x + ny) * a.nxo + corner.y + nx;
+      const float2 p = a.probe[pi], dp = a.d_probe[pi];
+      const float2 o = a.object[oi], dob = a.d_obj[oi];
+      const float2 q = a.quad[ny * N + nx];
+      S0[yl * L + (jx ^ swz(yl))] = cmul(cmul(p, o), q);
+      S1[yl * L + (jx ^ swz(yl))] = cmul(cadd(cmul(p, dob), cmul(dp, o)), q);
+    }
+    __syncthreads();
+    all_lines<N, C, -1>(S0, 2 * H, ltw);  // both planes: lines 0..2H-1 (S1 follows S0)
+    transpose<N, C>(S0, 2, cluster);
+    all_lines<N, C, -1>(S0, 2 * H, ltw);
+#pragma unroll 4
+    for (int idx = tid; idx < H * N; idx += T) {
+      const int c = idx % H, ky = idx / H;
+      const float2 po = S0[c * L + (ky ^ swz(c))], av = S1[c * L + (ky ^ swz(c))];
+      acc[idx] += cnorm2(po) * inv_n2;
+      acc[H * N + idx] += (po.x * av.x + po.y * av.y) * inv_n2;
+      acc[2 * H * N + idx] += cnorm2(av) * inv_n2;
+    }
+    __syncthreads();
+    // b into the second plane, through the same transform; po stays in column layout.
+#pragma unroll 4
+    for (int idx = tid; idx < H * N; idx += T) {
+      const int yl = idx / N, jx = idx % N;
+      const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
+      const size_t pi = ((size_t)pm * N + ny) * N + nx;
+      const size_t oi = ((size_t)om * a.nyo + corner.x + ny) * a.nxo + corner.y + nx;
+      S1[yl * L + (jx ^ swz(yl))] = cmul(cmul(a.d_probe[pi], a.d_obj[oi]), a.quad[ny * N + nx]);
+    }
+    __syncthreads();
+    all_lines<N, C, -1>(S1, H, ltw);
+    transpose<N, C>(S1, 1, cluster);
+    all_lines<N, C, -1>(S1, H, ltw);
+#pragma unroll 4
+    for (int idx = tid; idx < H * N; idx += T) {
+      const int c = idx % H, ky = idx / H;
+      const float2 po = S0[c * L + (ky ^ swz(c))], bv = S1[c * L + (ky ^ swz(c))];
+      acc[2 * H * N + idx] += 2.f * (po.x * bv.x + po.y * bv.y) * inv_n2;
+    }
+    __syncthreads();
+  }
+  const float* iobs = a.iobs + (size_t)f * N * N;
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int idx = tid; idx < H * N; idx += T) {
+    const int c = idx % H, ky = idx / H;
+    const float yo = iobs[ky * N + r * H + c];
+    if (yo < 0.f) continue;
+    const double calc = fmax((double)acc[idx], 1e-32);
+    const double rr = acc[H * N + idx], ss = acc[2 * H * N + idx];
+    const double d = 1.0 - (double)yo / calc;
+    v[0] -= 2.0 * rr * d;
+    const double t = 2.0 * rr / calc;
+    v[1] += 2.0 * ss * d + (double)yo * t * t;
+  }
+  block_sum<T>(v, 2, red);
+  csync<C>(cluster);
+  if (r == 0 && tid == 0) {
+    double num = 0.0, den = 0.0;
+    for (int q = 0; q < C; ++q) {
+      const double* rq = C > 1 ? cluster.map_shared_rank(red, q) : red;
+      num += rq[0];
+      den += rq[1];
+    }
+    a.out[slot * 2] = num;
+    a.out[slot * 2 + 1] = den;
+  }
+  csync<C>(cluster);
+}
+
+// Per block, in double: mode 0 Σ Re(conj(g)·(g − h)) and Σ |h|² (Polak–Ribière);
+// mode 1 Σ |g| (the modulus sum of scale_obj_probe). Partial sums [block][2].
+__global__ void __launch_bounds__(256) array_sums_kernel(const float2* g, const float2* h,
+                                                         size_t n, int mode, double* partial) {
+  __shared__ double sh[16];
+  double s0 = 0.0, s1 = 0.0;
+  for (size_t i = (size_t)blockIdx.x * 256 + threadIdx.x; i < n; i += (size_t)gridDim.x * 256) {
+    const float2 a = g[i];
+    if (mode == 0) {
+      const float2 b = h[i];
+      s0 += (double)a.x * ((double)a.x - b.x) + (double)a.y * ((double)a.y - b.y);
+      s1 += (double)b.x * b.x + (double)b.y * b.y;
+    } else {
+      s0 += sqrt((double)a.x * a.x + (double)a.y * a.y);
+    }
+  }
+  s0 = warp_sum(s0);
+  s1 = warp_sum(s1);
+  if (threadIdx.x % 32 == 0) {
+    sh[threadIdx.x / 32] = s0;
+    sh[8 + threadIdx.x / 32] = s1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a0 = 0.0, a1 = 0.0;
+    for (int w = 0; w < 8; ++w) {
+      a0 += sh[w];
+      a1 += sh[8 + w];
+    }
+    partial[blockIdx.x * 2] = a0;
+    partial[blockIdx.x * 2 + 1] = a1;
+  }
+}
+
+// d = beta·d − g.
+__global__ void cg_direction_kernel(float2* d, const float2* g, float beta, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float2 a = d[i], b = g[i];
+  d[i] = make_float2(a.x * beta - b.x, a.y * beta - b.y);
+}
+
+// x += gamma·d (gamma in double, applied in float).
+__global__ void axpy_kernel(float2* x, const float2* d, float gamma, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  x[i] = cadd(x[i], cscale(d[i], gamma));
+}
+
+// x *= s.
+__global__ void scale_kernel(float2* x, float s, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  x[i] = cscale(x[i], s);
+}
+
+// x[k][y][x] *= exp(i·2π·sign·(dy·(y − hy)/sy + dx·(x − hx)/sx)) for every plane k
+// (the ramps of `zero_phase_ramp`, engine/ptycho.rs:1153-1170), phase in double.
+__global__ void ramp_kernel(float2* x, int nplanes, int ny, int nx, double dy, double dx,
+                            double sy, double sx, double sign) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t n = (size_t)nplanes * ny * nx;
+  if (i >= n) return;
+  const int yy = (int)((i / nx) % ny), xx = (int)(i % nx);
+  const double ph = sign * 2.0 * 3.14159265358979323846 *
+                    (dy * (yy - ny / 2) / sy + dx * (xx - nx / 2) / sx);
+  double sn, cs;
+  sincos(ph, &sn, &cs);
+  const float2 v = x[i];
+  x[i] = make_float2((float)(v.x * cs - v.y * sn), (float)(v.x * sn + v.y * cs));
+}
+
+}  // namespace ptyb

@@ -58,7 +58,7 @@ class GpuPtycho:
     """The GPU reconstruction state of a scan on CUDA device `device`: `object` complex
     `[1, nyo, nxo]`, `probe` complex `[nprobe, ny, nx]`."""
 
-    def __init__(self, scan, obj, probe, device=0, stack_size=0):
+    def __init__(self, scan, obj, probe, device=0, stack_size=0, cluster=0):
         self._lib = _lib.load()
         obj = np.ascontiguousarray(obj, dtype=np.complex128)
         probe = np.ascontiguousarray(probe, dtype=np.complex128)
@@ -67,7 +67,7 @@ class GpuPtycho:
         self._obj_shape, self._probe_shape = obj.shape, probe.shape
         self._nframe = scan.counts.shape[0]
         st = scan._struct()
-        opts = _lib.Options(device, stack_size)
+        opts = _lib.Options(device, stack_size, cluster)
         h = ctypes.c_void_p()
         rc = self._lib.ptyb_create(ctypes.byref(st), _dptr(obj.view(np.float64)), obj.shape[0],
                                    obj.shape[1], obj.shape[2], _dptr(probe.view(np.float64)),

@@ -161,3 +161,21 @@ def test_invalid_calls_leave_the_state():
     assert e.value.status == "invalid"
     with pytest.raises(PtybError):
         gpu_of(dict(s, object=np.ones((2, 160, 160), complex)))
+
+
+@pytest.mark.parametrize("update_probe", [False, True])
+@pytest.mark.parametrize("ramp", [False, True])
+def test_ml_cycles(case, update_probe, ramp):
+    """Poisson ML conjugate gradient (scale, gradients, Polak–Ribière, Newton step) over four
+    cycles against the oracle's `Ptycho::ml`, with and without the probe and the final phase
+    ramp removal."""
+    cpu = oracle_state(case)
+    cpu.ml(4, update_probe=update_probe, calc_llk=1, zero_phase_ramp=ramp)
+    with gpu_of(case) as g:
+        g.ml(4, update_probe=update_probe, calc_llk=1, zero_phase_ramp=ramp)
+        assert rel_l2(g.object(), cpu.object) < RUN_TOL
+        assert rel_l2(g.probe(), cpu.probe) < RUN_TOL
+        h = g.history()
+        want = np.array([r["poisson"] for r in cpu.history])
+        assert list(h["algorithm"]) == ["ml"] * 4
+        assert np.abs(h["poisson"] - want).max() <= RUN_TOL * np.abs(want).max()
