@@ -136,6 +136,14 @@ int ptyb_forward_intensity(ptyb_handle* h, const int32_t* frames, int32_t n, flo
  * threads at the same time) race on it. */
 int ptyb_forward_intensity_noalloc(ptyb_handle* h, const int32_t* frames, int32_t n, float* out);
 
+/* Reference `GpuPtycho::set_features` with `Features::position` (engine/gpu/mod.rs:848-859,
+ * engine/features.rs:20-130): per-frame sub-pixel offsets [nframe][2] (dy, dx) in object pixels
+ * on top of the views' corners, modelled under Patch sampling (each frame's probe moved by its
+ * offset), refined by LSQML when `refine` is set; NULL clears them. Read back with
+ * ptyb_get_positions. */
+int ptyb_set_positions(ptyb_handle* h, const double* offsets, int32_t refine);
+int ptyb_get_positions(ptyb_handle* h, double* dst);
+
 /* Reference `GpuPtycho::{object, probe, set_object}` (engine/gpu/mod.rs:763-817). */
 int ptyb_get_object(ptyb_handle* h, double* dst);
 int ptyb_get_probe(ptyb_handle* h, double* dst);

@@ -33,13 +33,33 @@ def trim_mean(x):
 class Lsqml:
     """LSQML state across epochs (engine/lsqml.rs:415-430). cost: "poisson" or "amplitude"."""
 
-    def __init__(self, batch_size, cost="poisson", seed=7):
+    def __init__(self, batch_size, cost="poisson", seed=7, offsets=None, refine=False):
         if batch_size == 0:
             raise ValueError("LSQML batch_size must be >= 1")
         self.batch_size, self.cost, self.seed = batch_size, cost, seed
         self.epochs = 0
         self.preconditioner = None
         self.a_far_all = {}
+        # Features::position under Patch sampling: per-frame offsets [P, 2] in object pixels
+        self.offsets = None if offsets is None else np.array(offsets, np.float64)
+        self.refine = refine
+
+    def frame_probes(self, frames, probe, quad):
+        """`ProbeVariation::unique` planes moved by each frame's offset (engine/lsqml.rs:
+        474-499): `[len(frames)·nprobe, ny, nx]`."""
+        planes = np.concatenate([probe] * len(frames))
+        if self.offsets is None:
+            return planes
+        np_ = probe.shape[0]
+        for b, f in enumerate(frames):
+            planes[b * np_:(b + 1) * np_] = ops.move_planes(probe, quad, self.offsets[f])
+        return planes
+
+    @staticmethod
+    def unique_views(views, nb, np_, nmode):
+        uv = views.copy()
+        uv["probe"] = np.repeat(np.arange(nb) * np_, nmode) + views["probe"]
+        return uv
 
     def a_far(self, f):
         return self.a_far_all.get(f, 0.5)
@@ -52,7 +72,9 @@ class Lsqml:
             nmode += 1
         frames = [int(views[b * nmode]["frame"]) for b in range(len(views) // nmode)]
         ny, nx = probe.shape[-2:]
-        psi = ops.obj_probe_to_psi(views, obj, probe, optics.quad)
+        uprobe = self.frame_probes(frames, probe, optics.quad)
+        uviews = self.unique_views(views, len(frames), probe.shape[0], nmode)
+        psi = ops.obj_probe_to_psi(uviews, obj, uprobe, optics.quad)
         chi = optics.exit_forward(psi)
         sh = (len(frames), nmode, ny, nx)
         icalc = (np.abs(chi.reshape(sh)) ** 2).sum(axis=1)
@@ -78,48 +100,77 @@ class Lsqml:
         fac = 1.0 - np.asarray(a_far)[:, None, None] * c
         chi = (chi.reshape(sh) * fac[:, None]).reshape(chi.shape)
         chi = optics.exit_adjoint(chi) - psi
-        return frames, nmode, psi, chi, a_far
+        return frames, nmode, psi, chi, a_far, uprobe, uviews
 
     def step(self, views, obs, optics, obj, probe):
         """`Lsqml::step` (engine/lsqml.rs:581-643); returns the new object and probe and the
         step record."""
         pre = self.preconditioner
         floor = (0.1 * pre.max()) ** 2
-        frames, nmode, psi, chi, a_far = self.batch(views, obs, optics, obj, probe)
+        frames, nmode, psi, chi, a_far, uprobe, uviews = self.batch(views, obs, optics, obj,
+                                                                     probe)
         q = optics.quad
         ny, nx = probe.shape[-2:]
         np_ = probe.shape[0]
         nb = len(frames)
         # obj_directions: accumulate_obj over the views at each frame's own probe
-        d_obj = ops.accumulate_obj(views, obj.shape, probe, q, chi)[0]
+        d_obj = ops.accumulate_obj(uviews, obj.shape, uprobe, q, chi)[0]
         d_obj = d_obj / np.sqrt(pre * pre + floor)
-        # frame_probe_directions: per-frame planes b·np + m
-        uviews = views.copy()
-        uviews["probe"] = np.repeat(np.arange(nb) * np_, nmode) + views["probe"]
+        # frame_probe_directions: per-frame planes b·np + m, moved back by −offset
         d, _ = ops.accumulate_probe(uviews, obj, (nb * np_, ny, nx), q, chi)
+        if self.offsets is not None:
+            for b, f in enumerate(frames):
+                d[b * np_:(b + 1) * np_] = ops.move_planes(d[b * np_:(b + 1) * np_], q,
+                                                           -self.offsets[f])
         d_probe = np.zeros_like(probe)
         for b in range(nb):
             for m in range(np_):
                 d_probe[m] += d[b * np_ + m]
         d_probe = d_probe / float(nb)
-        a_obj, a_probe = self.step_sizes(views, nmode, optics, obj, probe, chi, d_obj, d_probe)
+        a_obj, a_probe = self.step_sizes(views, nmode, optics, obj, probe, chi, d_obj, d_probe,
+                                         uprobe, uviews)
+        d_pos = None
+        if self.refine and self.offsets is not None:
+            d_pos = self.position_directions(frames, nmode, optics, obj, uprobe, uviews, chi)
         for f, a in zip(frames, a_far):
             self.a_far_all[f] = a
         so = trim_mean(a_obj)
         new_obj = obj + so * d_obj
         sp = sum(a_probe) / len(a_probe)
         new_probe = probe + sp * d_probe
+        if d_pos is not None:
+            ops.batch_position_step(self.offsets, frames, d_pos)
         return new_obj, new_probe, dict(frames=frames, a_far=a_far, a_obj=a_obj,
                                         a_probe=a_probe)
 
-    def step_sizes(self, views, nmode, optics, obj, probe, chi, d_obj, d_probe):
-        """pty-chi Eq. 22 per frame (engine/lsqml.rs:286-350), one slice."""
+    def position_directions(self, frames, nmode, optics, obj, uprobe, uviews, chi):
+        """pty-chi LSQML's gradient position direction per frame, from the frame's mode-0
+        wave and chi and its object window (engine/lsqml.rs:237-270), single slice."""
+        ny, nx = uprobe.shape[-2:]
+        sums = []
+        for b in range(len(frames)):
+            k = b * nmode
+            v = uviews[k]
+            w = fftshift2(uprobe[int(v["probe"])] * optics.quad)
+            oy, ox = int(v["oy"]), int(v["ox"])
+            patch = obj[int(v["obj"]), oy:oy + ny, ox:ox + nx]
+            sums.append(ops.gradient_sums(patch, w, chi[k]))
+        eps = ops.EPS_POSITION * optics.intensity_scale()
+        return ops.gradient_directions(sums, eps)
+
+    def step_sizes(self, views, nmode, optics, obj, probe, chi, d_obj, d_probe, uprobe=None,
+                   uviews=None):
+        """pty-chi Eq. 22 per frame (engine/lsqml.rs:286-350), one slice: `dop` at each
+        frame's own probe, `dpo` from the shared probe direction."""
         ny, nx = probe.shape[-2:]
         n = ny * nx
         q = optics.quad
         scale = float(1 * nmode)
         dpo = ops.obj_probe_to_psi(views, obj, d_probe, q)
-        dop = ops.obj_probe_to_psi(views, d_obj, probe, q)
+        if uprobe is None:
+            dop = ops.obj_probe_to_psi(views, d_obj, probe, q)
+        else:
+            dop = ops.obj_probe_to_psi(uviews, d_obj, uprobe, q)
         lambda0 = LAMBDA0 * optics.intensity_scale() / n
         nb = len(views) // nmode
         sh = (nb, nmode * n)
@@ -166,10 +217,13 @@ class Lsqml:
             steps.append(st)
         return obj, probe, steps
 
-    @staticmethod
-    def llk(addr, obs, optics, obj, probe):
-        """Normalised LLK of the model the steps update (engine/lsqml.rs:537-551)."""
-        psi = optics.exit_forward(ops.obj_probe_to_psi(addr.views, obj, probe, optics.quad))
+    def llk(self, addr, obs, optics, obj, probe):
+        """Normalised LLK of the model the steps update, each frame's own (moved) probe
+        (engine/lsqml.rs:537-551)."""
+        frames = list(range(addr.nframe))
+        uprobe = self.frame_probes(frames, probe, optics.quad)
+        uviews = self.unique_views(addr.views, addr.nframe, probe.shape[0], addr.nmode)
+        psi = optics.exit_forward(ops.obj_probe_to_psi(uviews, obj, uprobe, optics.quad))
         return ops.llk(obs, slice(0, addr.nframe), addr.nmode, psi).normalised(obs.nb_obs)
 
 

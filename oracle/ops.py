@@ -344,6 +344,79 @@ def accumulate_probe(views, obj, probe_shape, quad, psi):
     return num, norm
 
 
+# --------------------------------------------------------------------------------------
+# The position model under Patch sampling (engine/features.rs:337-527).
+
+POSITION_STEP = 0.3
+POSITION_LIMIT = 0.1
+EPS_POSITION = 1e-6
+
+
+def _freqs(n):
+    return np.array([freq(k, n) for k in range(n)])
+
+
+def translation(shape, offset):
+    """`exp(−2πi f·offset)` on the unshifted DFT grid (engine/features.rs:364-369)."""
+    ny, nx = shape
+    fy, fx = _freqs(ny), _freqs(nx)
+    ph = -2.0 * np.pi * (fy[:, None] * offset[0] + fx[None, :] * offset[1])
+    return np.cos(ph) + 1j * np.sin(ph), (fy, fx)
+
+
+def move_planes(planes, quad, offset, axes=()):
+    """Natural-layout planes moved by `offset` as pty-chi moves its probe, `conj(q)·T(q·p)`,
+    with the derivative over the listed offset components (engine/features.rs:393-441)."""
+    shape = planes.shape[-2:]
+    e, (fy, fx) = translation(shape, offset)
+    for a in axes:
+        f = fy[:, None] if a == 0 else fx[None, :]
+        e = e * (-2j * np.pi * f)
+    q = 1.0 if quad is None else quad
+    out = ifft2(fft2(planes * q) * e)
+    return out * (np.conj(quad) if quad is not None else 1.0)
+
+
+def gradient_sums(patch, w, chi):
+    """Per axis `num = Σ Re(conj(∂O·w)·chi)`, `den = Σ |∂O·w|²` with ∂O the periodic Fourier
+    derivative of the natural-layout window (engine/features.rs:459-492); `w`, `chi` shifted."""
+    ny, nx = patch.shape
+    fy, fx = _freqs(ny), _freqs(nx)
+    g = fft2(patch)
+    grads = [ifft2(g * (2j * np.pi * fy[:, None])), ifft2(g * (2j * np.pi * fx[None, :]))]
+    num, den = [0.0, 0.0], [0.0, 0.0]
+    for axis in range(2):
+        u = fftshift2(grads[axis]) * w
+        num[axis] = float((np.conj(u) * chi).real.sum())
+        den[axis] = float((np.abs(u) ** 2).sum())
+    return [num, den]
+
+
+def gradient_directions(sums, eps):
+    """`num / (den + max(max_batch den, eps))` per axis (engine/features.rs:496-501)."""
+    mx = [max([eps] + [s[1][a] for s in sums]) for a in range(2)]
+    return [[s[0][a] / (s[1][a] + mx[a]) for a in range(2)] for s in sums]
+
+
+def batch_position_step(d, frames, delta):
+    """pty-chi's SGD position step with the per-axis clip `min(10·MAD, 0.1)` over every frame
+    (engine/features.rs:507-521); `d` `[P, 2]` is updated in place."""
+    dx = np.zeros_like(d)
+    for f, dl in zip(frames, delta):
+        dx[f] = [POSITION_STEP * dl[0], POSITION_STEP * dl[1]]
+    n = float(len(d))
+    for axis in range(2):
+        s = 0.0
+        for v in dx[:, axis]:
+            s += v
+        mean = s / n
+        s = 0.0
+        for v in dx[:, axis]:
+            s += abs(v - mean)
+        limit = min(10.0 * (s / n), POSITION_LIMIT)
+        d[:, axis] += np.clip(dx[:, axis], -limit, limit)
+
+
 def illumination(views, obj_shape, probe):
     """pty-chi illumination map `Σ|P[probe_k]|²` on each window (engine/lsqml.rs:374-388)."""
     ny, nx = probe.shape[-2:]

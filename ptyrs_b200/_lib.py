@@ -60,6 +60,8 @@ SIGNATURES = {
     "ptyb_forward_intensity": (c_int32, [c_void_p, P(c_int32), c_int32, P(ctypes.c_float)]),
     "ptyb_forward_intensity_noalloc": (c_int32, [c_void_p, P(c_int32), c_int32,
                                                  P(ctypes.c_float)]),
+    "ptyb_set_positions": (c_int32, [c_void_p, P(c_double), c_int32]),
+    "ptyb_get_positions": (c_int32, [c_void_p, P(c_double)]),
     "ptyb_get_object": (c_int32, [c_void_p, P(c_double)]),
     "ptyb_get_probe": (c_int32, [c_void_p, P(c_double)]),
     "ptyb_set_object": (c_int32, [c_void_p, P(c_double)]),

@@ -17,6 +17,7 @@
 #include "gather.cuh"
 #include "lsqml.cuh"
 #include "ml.cuh"
+#include "position.cuh"
 #include "scan.h"
 
 using namespace ptyb;
@@ -131,6 +132,12 @@ struct ptyb_handle {
   float2 *g_obj = nullptr, *g_obj_c = nullptr, *g_probe = nullptr, *g_probe_c = nullptr;
   float2 *last_obj = nullptr, *last_probe = nullptr, *dir_obj = nullptr, *dir_probe = nullptr;
   double* gamma_sums = nullptr;  // [P][2]
+  // Position model (Patch sampling): per-frame offsets [P][2] (dy, dx object pixels) on the
+  // device, whether they are refined, the batch's moved probes and its position sums.
+  double* offsets = nullptr;
+  bool have_offsets = false, refine_offsets = false;
+  float2* wave = nullptr;        // [slots][K][N][N]
+  double* pos_sums = nullptr;    // [slots][4]
   double* partials = nullptr;    // [kPartialBlocks][2]
   std::vector<Buf> bufs;
   // Per-kernel device timing (CUDA events on the engine's stream), when enabled.
@@ -204,13 +211,15 @@ constexpr int kPartialBlocks = 296;
 enum Kind : int {
   kKFrameRpie = 0, kKFrameLsqml, kKFrameMl, kKFrameLlk, kKFrameStore, kKFrameFromStore,
   kKObjRpie, kKObjOverlap, kKObjLsqml, kKObjMl, kKIllum, kKProbePartial, kKProbeFinal,
-  kKAfar, kKDots, kKSolve, kKAxpy, kKMax, kKCounts, kKMisc, kKGamma, kKArraySums, kNumKinds
+  kKAfar, kKDots, kKSolve, kKAxpy, kKMax, kKCounts, kKMisc, kKGamma, kKArraySums, kKMove,
+  kKPositionSums, kNumKinds
 };
 const char* const kKindNames[kNumKinds] = {
     "frame_rpie", "frame_lsqml", "frame_ml_grad", "frame_llk", "frame_store",
     "frame_from_store", "object_rpie", "object_overlap", "object_lsqml", "object_ml",
     "illumination", "probe_partial", "probe_finalize", "lsqml_afar", "lsqml_dots",
-    "lsqml_solve", "axpy", "max", "counts", "misc", "ml_gamma", "array_sums"};
+    "lsqml_solve", "axpy", "max", "counts", "misc", "ml_gamma", "array_sums", "move",
+    "position_sums"};
 
 cudaEvent_t take_event(ptyb_handle* h) {
   if (!h->event_pool.empty()) {
@@ -339,6 +348,65 @@ cudaError_t launch_frame(ptyb_handle* h, const FrameArgs& a, int nslot) {
   return e;
 }
 
+template <int N, int C, int MODE>
+cudaError_t launch_move_nc(const MoveArgs& a, int nslot, int K, cudaStream_t s) {
+  auto kern = move_kernel<N, C, MODE>;
+  const size_t smem = move_smem_bytes<N, C>(K);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  if (C > 8) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return e;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nslot * C);
+  cfg.blockDim = dim3(FrameShape<N, C>::T);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = C > 1 ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kern, a);
+}
+
+// Plane transforms of the position model over `nslot` frames (the frame kernel's cluster
+// shape; window derivatives carry two planes).
+template <int MODE>
+cudaError_t launch_move(ptyb_handle* h, const MoveArgs& a, int nslot) {
+  if (nslot <= 0) return cudaSuccess;
+  const int K = MODE == kDerivWindow ? 2 : h->K;
+  cudaError_t e = cudaErrorInvalidValue;
+  timed(h, kKMove, [&] {
+    switch (h->N * 100 + h->C) {
+      case 6401: e = launch_move_nc<64, 1, MODE>(a, nslot, K, h->stream); break;
+      case 12802: e = launch_move_nc<128, 2, MODE>(a, nslot, K, h->stream); break;
+      case 12804: e = launch_move_nc<128, 4, MODE>(a, nslot, K, h->stream); break;
+      case 25608: e = launch_move_nc<256, 8, MODE>(a, nslot, K, h->stream); break;
+      case 25616: e = launch_move_nc<256, 16, MODE>(a, nslot, K, h->stream); break;
+    }
+  });
+  return e;
+}
+
+MoveArgs move_args(ptyb_handle* h, const int* frames, float2* planes) {
+  MoveArgs m = {};
+  m.probe = h->probe;
+  m.quad = h->quad;
+  m.tw = h->tw;
+  m.object = h->object;
+  m.frames = frames;
+  m.corners = h->corners;
+  m.offsets = h->offsets;
+  m.planes = planes;
+  m.nxo = h->nxo;
+  m.K = h->K;
+  return m;
+}
+
 FrameArgs frame_args(ptyb_handle* h, const int* frames) {
   FrameArgs a = {};
   a.object = h->object;
@@ -397,6 +465,10 @@ void ensure_slots(ptyb_handle* h, int n) {
   h->afar1 = alloc<float>(h, n);
   h->afar2 = alloc<float>(h, n);
   h->sums = alloc<double>(h, (size_t)n * 6);
+  if (h->have_offsets) {
+    h->wave = alloc<float2>(h, (size_t)n * h->K * plane);
+    h->pos_sums = alloc<double>(h, (size_t)n * 4);
+  }
   h->slots = n;
 }
 
@@ -452,6 +524,13 @@ ptyb_llk llk_pass(ptyb_handle* h) {
     const int n = std::min(stack, h->P - s0);
     FrameArgs a = frame_args(h, h->iota + s0);
     a.llk = h->llk + (size_t)s0 * 4;
+    if (h->have_offsets) {
+      // each frame's own moved probe (engine/lsqml.rs:537-551)
+      check(h, launch_move<kMoveProbe>(h, move_args(h, h->iota + s0, h->wave), n), "probe move");
+      ++h->launches;
+      a.probe = h->wave;
+      a.probe_stride = h->K * h->N * h->N;
+    }
     check(h, launch_frame<kLlk>(h, a, n), "llk pass");
     ++h->launches;
   }
@@ -572,11 +651,20 @@ void lsqml_preconditioner(ptyb_handle* h, bool init) {
   launched(h, "pre max");
 }
 
-// One LSQML step on a batch (engine/lsqml.rs:581-643).
+// One LSQML step on a batch (engine/lsqml.rs:581-643), with the position model when offsets
+// are set: each frame's probe moved by its offset, the probe directions moved back before
+// their frame mean, and with refinement pty-chi's position step after the update.
 void lsqml_batch(ptyb_handle* h, const ptyb_lsqml_params& p, const int* frames, int nslot,
                  double* log) {
+  const int pstride = h->K * h->N * h->N;
   FrameArgs a = frame_args(h, frames);
   a.cost = p.cost;
+  if (h->have_offsets) {
+    check(h, launch_move<kMoveProbe>(h, move_args(h, frames, h->wave), nslot), "probe move");
+    ++h->launches;
+    a.probe = h->wave;
+    a.probe_stride = pstride;
+  }
   if (p.cost == PTYB_COST_POISSON) {
     // Forward pass with the xi solver's first pass, backward pass with its second.
     a.nslot = nslot;
@@ -599,34 +687,87 @@ void lsqml_batch(ptyb_handle* h, const ptyb_lsqml_params& p, const int* frames, 
     ++h->launches;
   }
   GatherArgs g = gather_args(h, frames, nslot);
+  if (h->have_offsets) {
+    g.probe = h->wave;
+    g.probe_stride = pstride;
+  }
   timed(h, kKObjLsqml, [&] { object_tile_kernel<kGatherLsqml><<<ntiles(h), 1024, 0, h->stream>>>(g); });
   launched(h, "object direction");
-  probe_pass(h, frames, nslot, 1, 0.f, 1.0f / nslot);
+  if (h->have_offsets) {
+    timed(h, kKProbePartial, [&] {
+      probe_terms_kernel<<<dim3((h->N * h->N + 255) / 256, nslot), 256, 0, h->stream>>>(
+          h->object, h->quad, h->upd, frames, h->corners, h->nxo, h->K, h->N, h->field);
+    });
+    launched(h, "probe terms");
+    check(h, launch_move<kMoveBack>(h, move_args(h, frames, h->field), nslot), "probe move back");
+    ++h->launches;
+    timed(h, kKProbeFinal, [&] {
+      probe_finalize_kernel<<<(pstride + 255) / 256, 256, 0, h->stream>>>(
+          h->field, nslot, pstride, h->probe, h->d_probe, nullptr, 1.0f / nslot, 1);
+    });
+    launched(h, "probe direction");
+  } else {
+    probe_pass(h, frames, nslot, 1, 0.f, 1.0f / nslot);
+  }
   const double lambda0 = 1.2e-7 * ((double)h->N * h->N) / ((double)h->N * h->N);
+  const float2* fprobe = h->have_offsets ? h->wave : h->probe;
+  const int fstride = h->have_offsets ? pstride : 0;
   timed(h, kKDots, [&] {
-  lsqml_dots_kernel<<<nslot, 512, 0, h->stream>>>(h->object, h->d_obj, h->probe, h->d_probe,
-                                                   h->quad, h->upd, frames, h->corners, h->nxo,
-                                                   h->K, h->N, lambda0, h->sums);
+    lsqml_dots_kernel<<<nslot, 512, 0, h->stream>>>(h->object, h->d_obj, fprobe, h->d_probe,
+                                                     h->quad, h->upd, frames, h->corners,
+                                                     h->nxo, h->K, h->N, lambda0, h->sums,
+                                                     fstride);
   });
   launched(h, "step sums");
+  const bool refine = h->have_offsets && h->refine_offsets;
+  if (refine) {
+    // position directions from the state on entry (engine/lsqml.rs:237-270)
+    check(h, launch_move<kDerivWindow>(h, move_args(h, frames, h->field), nslot), "window derivative");
+    ++h->launches;
+    timed(h, kKPositionSums, [&] {
+      position_sums_kernel<<<nslot, 256, 0, h->stream>>>(h->field, h->wave, pstride, h->quad,
+                                                          h->upd, h->K, h->N, h->pos_sums);
+    });
+    launched(h, "position sums");
+  }
   timed(h, kKSolve, [&] {
-  lsqml_solve_kernel<<<1, 1024, 0, h->stream>>>(h->sums, nslot, (double)(1 * h->K), h->afar2,
-                                                 frames, h->afar_all, log, h->scal + 2);
+    lsqml_solve_kernel<<<1, 1024, 0, h->stream>>>(h->sums, nslot, (double)(1 * h->K), h->afar2,
+                                                   frames, h->afar_all, log, h->scal + 2);
   });
   launched(h, "step solve");
   const size_t no = (size_t)h->nyo * h->nxo, np = (size_t)h->K * h->N * h->N;
   timed(h, kKAxpy, [&] {
-  axpy_scal_kernel<<<(unsigned)((no + 255) / 256), 256, 0, h->stream>>>(h->object, h->d_obj,
-                                                                       h->scal + 2, 0, no);
+    axpy_scal_kernel<<<(unsigned)((no + 255) / 256), 256, 0, h->stream>>>(h->object, h->d_obj,
+                                                                         h->scal + 2, 0, no);
   });
   launched(h, "object step");
   timed(h, kKAxpy, [&] {
-  axpy_scal_kernel<<<(unsigned)((np + 255) / 256), 256, 0, h->stream>>>(h->probe, h->d_probe,
-                                                                       h->scal + 2, 1, np);
+    axpy_scal_kernel<<<(unsigned)((np + 255) / 256), 256, 0, h->stream>>>(h->probe, h->d_probe,
+                                                                         h->scal + 2, 1, np);
   });
   launched(h, "probe step");
+  if (refine) {
+    const double eps = 1e-6 * ((double)h->N * h->N);
+    timed(h, kKSolve, [&] {
+      position_step_kernel<<<1, 32, 0, h->stream>>>(h->pos_sums, nslot, h->P, eps, frames,
+                                                    h->offsets);
+    });
+    launched(h, "position step");
+  }
 }
 
+void to_c64(const float2* src, double* dst, size_t n) {
+  for (size_t i = 0; i < n; ++i) {
+    dst[2 * i] = src[i].x;
+    dst[2 * i + 1] = src[i].y;
+  }
+}
+
+std::vector<float2> from_c64(const double* src, size_t n) {
+  std::vector<float2> v(n);
+  for (size_t i = 0; i < n; ++i) v[i] = make_float2((float)src[2 * i], (float)src[2 * i + 1]);
+  return v;
+}
 
 template <int N, int C>
 cudaError_t launch_gamma_nc(const GammaArgs& a, int nslot, cudaStream_t s) {
@@ -893,19 +1034,6 @@ void scale_obj_probe(ptyb_handle* h) {
   launched(h, "scale");
 }
 
-void to_c64(const float2* src, double* dst, size_t n) {
-  for (size_t i = 0; i < n; ++i) {
-    dst[2 * i] = src[i].x;
-    dst[2 * i + 1] = src[i].y;
-  }
-}
-
-std::vector<float2> from_c64(const double* src, size_t n) {
-  std::vector<float2> v(n);
-  for (size_t i = 0; i < n; ++i) v[i] = make_float2((float)src[2 * i], (float)src[2 * i + 1]);
-  return v;
-}
-
 template <typename F>
 int guarded(ptyb_handle* h, bool enqueues, F&& body) {
   if (!h) return PTYB_INVALID;
@@ -1090,6 +1218,10 @@ int ptyb_rpie(ptyb_handle* h, const ptyb_rpie_params* p, int32_t nepoch) {
     h->err = "rPIE needs exactly one object mode";
     return PTYB_INVALID;
   }
+  if (h->have_offsets) {
+    h->err = "rPIE does not model position offsets in this version";
+    return PTYB_INVALID;
+  }
   return guarded(h, true, [&]() -> int {
     const int bs = std::min(p->batch_size, h->P);
     ensure_slots(h, std::max(bs, std::min(h->P, h->stack)));
@@ -1176,6 +1308,10 @@ int ptyb_ml(ptyb_handle* h, const ptyb_ml_params* p, int32_t ncycle) {
   if (!h || !p) return PTYB_INVALID;
   if (ncycle < 0) {
     h->err = "ncycle must be >= 0";
+    return PTYB_INVALID;
+  }
+  if (h->have_offsets) {
+    h->err = "ML does not model position offsets in this version";
     return PTYB_INVALID;
   }
   return guarded(h, true, [&]() -> int {
@@ -1318,6 +1454,49 @@ int ptyb_forward_intensity_noalloc(ptyb_handle* h, const int32_t* frames, int32_
             "intensity");
       check(h, cudaStreamSynchronize(h->stream), "forward");
     }
+    return PTYB_OK;
+  });
+}
+
+int ptyb_set_positions(ptyb_handle* h, const double* offsets, int32_t refine) {
+  if (!h) return PTYB_INVALID;
+  if (offsets)
+    for (int i = 0; i < 2 * h->P; ++i)
+      if (!std::isfinite(offsets[i])) {
+        h->err = "position offsets must be finite";
+        return PTYB_INVALID;
+      }
+  return guarded(h, true, [&]() -> int {
+    check(h, cudaStreamSynchronize(h->stream), "sync");
+    if (!offsets) {
+      h->have_offsets = h->refine_offsets = false;
+      return PTYB_OK;
+    }
+    if (!h->offsets) h->offsets = alloc<double>(h, (size_t)h->P * 2);
+    check(h, cudaMemcpy(h->offsets, offsets, (size_t)h->P * 2 * sizeof(double),
+                        cudaMemcpyHostToDevice),
+          "offsets");
+    if (!h->have_offsets && h->slots > 0) {
+      const size_t plane = (size_t)h->N * h->N;
+      h->wave = alloc<float2>(h, (size_t)h->slots * h->K * plane);
+      h->pos_sums = alloc<double>(h, (size_t)h->slots * 4);
+    }
+    h->have_offsets = true;
+    h->refine_offsets = refine != 0;
+    return PTYB_OK;
+  });
+}
+
+int ptyb_get_positions(ptyb_handle* h, double* dst) {
+  if (!h || !dst) return PTYB_INVALID;
+  return guarded(h, false, [&]() -> int {
+    check(h, cudaStreamSynchronize(h->stream), "sync");
+    if (!h->have_offsets) {
+      std::fill(dst, dst + 2 * h->P, 0.0);
+      return PTYB_OK;
+    }
+    check(h, cudaMemcpy(dst, h->offsets, (size_t)h->P * 2 * sizeof(double), cudaMemcpyDeviceToHost),
+          "offsets");
     return PTYB_OK;
   });
 }

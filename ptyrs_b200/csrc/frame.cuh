@@ -58,6 +58,9 @@ struct FrameArgs {
   float* a_out;
   int a_prev_by_frame, nslot;
   int nyo, nxo, nprobe, nobj, cost;
+  // Elements between consecutive slots' probes: 0 for the shared probe, K·N·N for the
+  // per-frame (moved) probes of the position model.
+  int probe_stride;
 };
 
 template <int N, int C>
@@ -220,7 +223,8 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T)
         for (int pm = 0; pm < a.nprobe; ++pm) {
           const int line = (om * a.nprobe + pm) * H + yl;
           // (P·O)·q as P·(O·q): the reference's product up to rounding
-          S[line * L + (jx ^ swz(line))] = cmul(a.probe[((size_t)pm * N + ny) * N + nx], oq);
+          S[line * L + (jx ^ swz(line))] =
+              cmul(a.probe[(size_t)slot * a.probe_stride + ((size_t)pm * N + ny) * N + nx], oq);
         }
       }
     }
@@ -372,7 +376,9 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T)
         const int m = om * a.nprobe + pm;
         const int line = m * H + yl;
         float2 v = S[line * L + (jx ^ swz(line))];
-        if (MODE != kMlGrad) v = csub(v, cmul(a.probe[((size_t)pm * N + ny) * N + nx], oq));
+        if (MODE != kMlGrad)
+          v = csub(v, cmul(a.probe[(size_t)slot * a.probe_stride + ((size_t)pm * N + ny) * N + nx],
+                           oq));
         out[((size_t)m * N + ny) * N + nx] = v;
       }
     }

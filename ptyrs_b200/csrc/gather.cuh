@@ -39,6 +39,7 @@ struct GatherArgs {
   float2* comp;            // ML gradient compensation [nyo][nxo]
   float alpha, step, pre_scale;
   int nslot, nyo, nxo, nprobe, N;
+  int probe_stride;        // elements between slots' probes (0: the shared probe)
 };
 
 // The launch's slots in [s0, s1) (at most 1024) whose window overlaps the tile
@@ -135,7 +136,7 @@ __global__ void __launch_bounds__(1024, MODE == kGatherRpie ? 1 : 2) object_tile
 #pragma unroll
       for (int m = 0; m < kMaxModes; ++m) {
         if (m >= K) break;
-        const float2 p = a.probe[m * plane + pix];
+        const float2 p = a.probe[(size_t)s * a.probe_stride + m * plane + pix];
         if (MODE == kGatherOverlap || MODE == kGatherIllum || MODE == kGatherRpie)
           den[m].add(cnorm2(p));
         if (MODE == kGatherRpie || MODE == kGatherLsqml || MODE == kGatherMl) {

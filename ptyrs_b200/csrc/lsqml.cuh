@@ -25,7 +25,7 @@ PTYB_D double block_sum1(double v, double* sh) {
 __global__ void __launch_bounds__(512) lsqml_dots_kernel(
     const float2* object, const float2* d_obj, const float2* probe, const float2* d_probe,
     const float2* quad, const float2* chi, const int* frames, const int2* corners, int nxo,
-    int K, int N, double lambda0, double* sums) {
+    int K, int N, double lambda0, double* sums, int probe_stride) {
   __shared__ double sh[16];
   const int slot = blockIdx.x;
   const int2 c = corners[frames[slot]];
@@ -37,7 +37,7 @@ __global__ void __launch_bounds__(512) lsqml_dots_kernel(
     const int yy = pix / N, xx = pix % N;
     const size_t o = (size_t)(c.x + yy) * nxo + c.y + xx;
     const float2 q = quad[pix];
-    const float2 u = cmul(cmul(probe[m * plane + pix], d_obj[o]), q);
+    const float2 u = cmul(cmul(probe[(size_t)slot * probe_stride + m * plane + pix], d_obj[o]), q);
     const float2 v = cmul(cmul(d_probe[m * plane + pix], object[o]), q);
     const float2 x = chi[((size_t)slot * K + m) * plane + pix];
     s[0] += cnorm2(u);

@@ -1,0 +1,197 @@
+// The position model under Patch sampling (physwkim/ptyrs engine/features.rs:337-527,
+// engine/lsqml.rs:237-270): each frame's probe moved by its sub-pixel offset on the periodic
+// grid, the adjoint move of the probe directions, the Fourier derivative of the object window,
+// pty-chi's gradient position sums and its clipped SGD step (in double).
+#pragma once
+#include "frame.cuh"
+
+namespace ptyb {
+
+enum MoveMode : int {
+  kMoveProbe = 0,  // planes[slot][m] = conj(q)·T_d(q·P_m)       (probe of frame f moved by d_f)
+  kMoveBack = 1,   // planes[slot][m] = conj(q)·T_{−d}(q·planes)  (the adjoint move, in place)
+  kDerivWindow = 2 // planes[slot][a] = ∂_a O_window (periodic Fourier derivative), a = y, x
+};
+
+struct MoveArgs {
+  const float2* probe;    // [K][N][N] shared probe (kMoveProbe)
+  const float2* quad;     // [N][N]
+  const float2* tw;       // [N]
+  const float2* object;   // [nyo][nxo] (kDerivWindow)
+  const int* frames;
+  const int2* corners;
+  const double* offsets;  // [nframe][2] (dy, dx) in object pixels
+  float2* planes;         // [slot][K][N][N] natural layout
+  int nxo, K;
+};
+
+// numpy fftfreq of index k of n points (engine/features.rs:337-344).
+PTYB_D float fft_freq(int k, int n) { return (float)(k < (n + 1) / 2 ? k : k - n) / (float)n; }
+
+template <int N, int C, int MODE>
+__global__ void __launch_bounds__(FrameShape<N, C>::T) move_kernel(MoveArgs a) {
+  using F = FrameShape<N, C>;
+  constexpr int H = F::H, T = F::T, L = F::L;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int K = MODE == kDerivWindow ? 2 : a.K;
+  float2* S = reinterpret_cast<float2*>(smem_raw);
+  cg::cluster_group cluster = cg::this_cluster();
+  const int r = C > 1 ? (int)cluster.block_rank() : 0;
+  const int slot = blockIdx.x / C;
+  const int f = a.frames[slot];
+  const int2 corner = a.corners[f];
+  const int tid = threadIdx.x;
+  LineTwiddles<N> ltw;
+  ltw.load(a.tw, tid % F::G);
+  const size_t plane = (size_t)N * N;
+  float2* out = a.planes + (size_t)slot * K * plane;
+
+  // Natural-layout rows r·H .. r·H+H-1 of every plane.
+#pragma unroll 2
+  for (int idx = tid; idx < H * N; idx += T) {
+    const int yl = idx / N, x = idx % N, y = r * H + yl;
+    const float2 q = a.quad[y * N + x];
+    for (int m = 0; m < K; ++m) {
+      float2 v;
+      if (MODE == kMoveProbe)
+        v = cmul(q, a.probe[m * plane + y * N + x]);
+      else if (MODE == kMoveBack)
+        v = cmul(q, out[m * plane + y * N + x]);
+      else
+        v = a.object[(size_t)(corner.x + y) * a.nxo + corner.y + x];
+      const int line = m * H + yl;
+      S[line * L + (x ^ swz(line))] = v;
+    }
+  }
+  __syncthreads();
+  all_lines<N, C, -1>(S, K * H, ltw);
+  transpose<N, C>(S, K, cluster);
+  all_lines<N, C, -1>(S, K * H, ltw);
+
+  // Spectrum: column kx = r·H + c as line (m·H + c), element ky.
+  constexpr float inv_n2 = 1.0f / ((float)N * (float)N);
+  float dy = 0.f, dx = 0.f;
+  if (MODE != kDerivWindow) {
+    const float sgn = MODE == kMoveProbe ? 1.f : -1.f;
+    dy = sgn * (float)a.offsets[2 * f];
+    dx = sgn * (float)a.offsets[2 * f + 1];
+  }
+#pragma unroll 2
+  for (int idx = tid; idx < H * N; idx += T) {
+    const int c = idx % H, ky = idx / H;
+    const float fy = fft_freq(ky, N), fx = fft_freq(r * H + c, N);
+    float2 e;
+    if (MODE != kDerivWindow) {
+      float sn, cs;
+      sincospif(-2.f * (fy * dy + fx * dx), &sn, &cs);  // exp(−2πi f·d)
+      e = make_float2(cs * inv_n2, sn * inv_n2);
+    }
+    for (int m = 0; m < K; ++m) {
+      float2& v = S[(m * H + c) * L + (ky ^ swz(m * H + c))];
+      if (MODE == kDerivWindow) {
+        const float w = 2.f * 3.14159265358979f * (m == 0 ? fy : fx) * inv_n2;
+        v = make_float2(-w * v.y, w * v.x);  // × 2πi·f_axis
+      } else {
+        v = cmul(v, e);
+      }
+    }
+  }
+  __syncthreads();
+  all_lines<N, C, +1>(S, K * H, ltw);
+  transpose<N, C>(S, K, cluster);
+  all_lines<N, C, +1>(S, K * H, ltw);
+
+#pragma unroll 2
+  for (int idx = tid; idx < H * N; idx += T) {
+    const int yl = idx / N, x = idx % N, y = r * H + yl;
+    const float2 cq = MODE == kDerivWindow ? make_float2(1.f, 0.f) : cconj(a.quad[y * N + x]);
+    for (int m = 0; m < K; ++m) {
+      const int line = m * H + yl;
+      const float2 v = S[line * L + (x ^ swz(line))];
+      out[m * plane + y * N + x] = MODE == kDerivWindow ? v : cmul(cq, v);
+    }
+  }
+}
+
+template <int N, int C>
+__host__ __device__ constexpr size_t move_smem_bytes(int K) {
+  return frame_smem_bytes<N, C>(K);
+}
+
+// planes[slot][m] = conj(q·O_window)·χ_m per natural pixel: each frame's probe direction
+// before its adjoint move (engine/lsqml.rs:200-207).
+__global__ void probe_terms_kernel(const float2* object, const float2* quad, const float2* chi,
+                                   const int* frames, const int2* corners, int nxo, int K, int N,
+                                   float2* planes) {
+  const int slot = blockIdx.y;
+  const size_t plane = (size_t)N * N;
+  const int2 c = corners[frames[slot]];
+  for (int pix = blockIdx.x * blockDim.x + threadIdx.x; pix < N * N;
+       pix += gridDim.x * blockDim.x) {
+    const int y = pix / N, x = pix % N;
+    const float2 w = cconj(cmul(quad[pix], object[(size_t)(c.x + y) * nxo + c.y + x]));
+    for (int m = 0; m < K; ++m) {
+      const size_t i = ((size_t)slot * K + m) * plane + pix;
+      planes[i] = cmul(w, chi[i]);
+    }
+  }
+}
+
+// Per slot, pty-chi's position sums on mode 0 (engine/features.rs:459-492): with w the
+// frame's moved probe times q, per axis num = Σ Re(conj(∂O·w)·χ), den = Σ |∂O·w|²;
+// sums[slot] = (num_y, num_x, den_y, den_x) in double.
+__global__ void __launch_bounds__(256) position_sums_kernel(const float2* dwin,
+                                                           const float2* wave, int wave_stride,
+                                                           const float2* quad,
+                                                           const float2* chi, int K, int N,
+                                                           double* sums) {
+  __shared__ double sh[8];
+  const int slot = blockIdx.x;
+  const size_t plane = (size_t)N * N;
+  double s[4] = {0, 0, 0, 0};
+  for (int pix = threadIdx.x; pix < N * N; pix += 256) {
+    const float2 w = cmul(wave[(size_t)slot * wave_stride + pix], quad[pix]);
+    const float2 c = chi[(size_t)slot * K * plane + pix];
+    for (int a = 0; a < 2; ++a) {
+      const float2 u = cmul(dwin[((size_t)slot * 2 + a) * plane + pix], w);
+      s[a] += (double)u.x * c.x + (double)u.y * c.y;
+      s[2 + a] += (double)u.x * u.x + (double)u.y * u.y;
+    }
+  }
+  for (int k = 0; k < 4; ++k) {
+    double v = warp_sum(s[k]);
+    if (threadIdx.x % 32 == 0) sh[threadIdx.x / 32] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < 8; ++w) t += sh[w];
+      sums[(size_t)slot * 4 + k] = t;
+    }
+    __syncthreads();
+  }
+}
+
+// pty-chi's gradient position step on the batch (engine/features.rs:496-521), one thread in
+// double: delta = num/(den + max(max_batch den, eps)), dx = 0.3·delta at the batch's frames
+// (0 elsewhere), each axis clipped to min(10·mean|dx − mean dx|, 0.1) over every frame.
+__global__ void position_step_kernel(const double* sums, int nslot, int nframe, double eps,
+                                     const int* frames, double* offsets) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  for (int a = 0; a < 2; ++a) {
+    double mx = eps;
+    for (int s = 0; s < nslot; ++s) mx = fmax(mx, sums[s * 4 + 2 + a]);
+    double total = 0.0;
+    for (int s = 0; s < nslot; ++s) total += 0.3 * (sums[s * 4 + a] / (sums[s * 4 + 2 + a] + mx));
+    const double mean = total / nframe;
+    double dev = (double)(nframe - nslot) * fabs(mean);
+    for (int s = 0; s < nslot; ++s)
+      dev += fabs(0.3 * (sums[s * 4 + a] / (sums[s * 4 + 2 + a] + mx)) - mean);
+    const double limit = fmin(10.0 * (dev / nframe), 0.1);
+    for (int s = 0; s < nslot; ++s) {
+      const double dx = 0.3 * (sums[s * 4 + a] / (sums[s * 4 + 2 + a] + mx));
+      offsets[2 * frames[s] + a] += fmin(fmax(dx, -limit), limit);
+    }
+  }
+}
+
+}  // namespace ptyb

@@ -163,6 +163,21 @@ class GpuPtycho:
         probe = np.ascontiguousarray(probe, dtype=np.complex128).reshape(self._probe_shape)
         self._check(self._lib.ptyb_set_probe(self._h, _dptr(probe.view(np.float64))))
 
+    def set_positions(self, offsets=None, refine=True):
+        """Per-frame sub-pixel offsets `[nframe, 2]` (dy, dx) in object pixels, modelled by
+        moving each frame's probe and refined by LSQML when `refine`; None clears them."""
+        if offsets is None:
+            self._check(self._lib.ptyb_set_positions(self._h, None, 0))
+            return
+        d = np.ascontiguousarray(offsets, np.float64).reshape(self._nframe, 2)
+        self._check(self._lib.ptyb_set_positions(self._h, _dptr(d), int(refine)))
+
+    def positions(self):
+        """The offsets `[nframe, 2]` as the last step left them (zeros when none are set)."""
+        out = np.empty((self._nframe, 2), np.float64)
+        self._check(self._lib.ptyb_get_positions(self._h, _dptr(out)))
+        return out
+
     def corners(self):
         out = np.empty((self._nframe, 2), np.int32)
         self._check(self._lib.ptyb_corners(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))))

@@ -179,3 +179,45 @@ def test_ml_cycles(case, update_probe, ramp):
         want = np.array([r["poisson"] for r in cpu.history])
         assert list(h["algorithm"]) == ["ml"] * 4
         assert np.abs(h["poisson"] - want).max() <= RUN_TOL * np.abs(want).max()
+
+
+@pytest.mark.parametrize("refine", [False, True])
+def test_lsqml_with_positions(case, refine):
+    """LSQML with per-frame sub-pixel offsets under Patch sampling (each frame's probe moved by
+    its offset, the probe directions moved back, and with `refine` pty-chi's position step)
+    against the oracle, which is pinned to pty-chi's golden step: the step sizes, the arrays,
+    the offset changes and the LLK of the moved-probe model. The single hard-edged aperture
+    runs the amplitude cost: under the Poisson cost its step sizes are FP32-limited at the
+    aperture's far-field zeros (see test_lsqml_epochs)."""
+    nframe = len(case["counts"])
+    d0 = np.random.default_rng(5).uniform(-0.6, 0.6, (nframe, 2))
+    single = case["probe"].shape[0] == 1
+    nepoch = 1 if single else 2
+    cost = "amplitude" if single else "poisson"
+    cpu = oracle_state(case)
+    run = Lsqml(8, cost, 7, offsets=d0, refine=refine)
+    obj, probe, steps = cpu.object, cpu.probe, None
+    for _ in range(nepoch):
+        obj, probe, steps = run.epoch(cpu.addr, cpu.obs, cpu.optics, obj, probe)
+    with gpu_of(case) as g:
+        g.set_positions(d0, refine=refine)
+        g.lsqml(nepoch, batch_size=8, cost=cost, seed=7)
+        got = g.lsqml_steps()
+        assert [s["frames"] for s in got] == [s["frames"] for s in steps]
+        for gs, cs in zip(got, steps):
+            for key in ("a_far", "a_obj", "a_probe"):
+                a, b = np.array(gs[key]), np.array(cs[key])
+                tol = AFAR_RUN_TOL if key == "a_far" else RUN_TOL
+                assert np.abs(a - b).max() <= tol * np.abs(b).max(), key
+        assert rel_l2(g.object(), obj) < RUN_TOL
+        assert rel_l2(g.probe(), probe) < RUN_TOL
+        d = g.positions()
+        if refine:
+            moved = run.offsets - d0
+            assert np.abs(moved).max() > 0
+            assert np.abs((d - d0) - moved).max() <= RUN_TOL * 10 * np.abs(moved).max()
+        else:
+            assert np.array_equal(d, d0)
+        cpu.object, cpu.probe = obj, probe
+        want = run.llk(cpu.addr, cpu.obs, cpu.optics, obj, probe).poisson
+        assert abs(g.llk()["poisson"] - want) <= RUN_TOL * abs(want)

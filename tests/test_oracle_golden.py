@@ -142,7 +142,7 @@ def test_lsqml_epochs_match_ptychi():
         run = Lsqml(8, "poisson", 7)
         want = trace[trace[:, 0] == k]
         rows = steps[steps[:, 0] == k]
-        llks = [Lsqml.llk(addr, obs, optics, obj, probe).poisson]
+        llks = [run.llk(addr, obs, optics, obj, probe).poisson]
         nxt = 0
         for e in range(len(want) - 1):
             obj, probe, sts = run.epoch(addr, obs, optics, obj, probe)
@@ -151,7 +151,7 @@ def test_lsqml_epochs_match_ptychi():
                 nxt += len(st["frames"])
                 assert (w[:, 1] == e).all()
                 assert_step(st, w, 2)
-            llks.append(Lsqml.llk(addr, obs, optics, obj, probe).poisson)
+            llks.append(run.llk(addr, obs, optics, obj, probe).poisson)
         assert nxt == len(rows)
         assert max_rel(llks, want[:, 2]) < 1e-12
         assert max_rel(change(obj, obj0), of_run(g["epochs_obj"], k, 3)) < 1e-12
@@ -190,3 +190,28 @@ def test_ml_matches_pynx_near_field():
         want = r[:, lead] + 1j * r[:, lead + 1]
         got = arr.ravel()
         assert max_rel(np.stack([got.real, got.imag], 1), np.stack([want.real, want.imag], 1)) < 5e-12
+
+
+def test_lsqml_step_with_positions_matches_ptychi():
+    """engine_lsqml_near.rs:386-440 under PATCH: from the truth object, every frame moved by
+    its offset and the positions refined, one step on frames 0..8 of each case the files hold:
+    the step sizes, the object and probe changes, and the offset changes (1e-11)."""
+    g, addr, obj0, probe, cases = lsqml_state()
+    p = golden("lsqml_near_pos")
+    start = stack((1,) + OBJ, p["start"], 2)
+    views = addr.views[:8 * addr.nmode]
+    checked = 0
+    for k, (optics, obs, _) in enumerate(cases):
+        rows = p["offsets"][p["offsets"][:, 0] == k]
+        if len(rows) == 0:
+            continue
+        checked += 1
+        d0, want = rows[:, 2:4], rows[:, 4:6]
+        run = Lsqml(8, "poisson", 0, offsets=d0, refine=True)
+        run.preconditioner = ops.illumination(addr.views, start.shape, probe)
+        o, pr, st = run.step(views, obs, optics, start, probe)
+        assert_step(st, p["steps"][p["steps"][:, 0] == k], 1)
+        assert max_rel(change(o, start), of_run(p["obj"], k, 3)) < 1e-12
+        assert max_rel(change(pr, probe), of_run(p["probe"], k, 4)) < 1e-12
+        assert max_rel(run.offsets - d0, want - d0) < 1e-11
+    assert checked == 2
