@@ -464,7 +464,7 @@ void ensure_slots(ptyb_handle* h, int n) {
   h->omax = alloc<float>(h, n);
   h->afar1 = alloc<float>(h, n);
   h->afar2 = alloc<float>(h, n);
-  h->sums = alloc<double>(h, (size_t)n * 6);
+  h->sums = alloc<double>(h, (size_t)n * 6 * kDotParts);
   if (h->have_offsets) {
     h->wave = alloc<float2>(h, (size_t)n * h->K * plane);
     h->pos_sums = alloc<double>(h, (size_t)n * 4);
@@ -713,7 +713,7 @@ void lsqml_batch(ptyb_handle* h, const ptyb_lsqml_params& p, const int* frames, 
   const float2* fprobe = h->have_offsets ? h->wave : h->probe;
   const int fstride = h->have_offsets ? pstride : 0;
   timed(h, kKDots, [&] {
-    lsqml_dots_kernel<<<nslot, 512, 0, h->stream>>>(h->object, h->d_obj, fprobe, h->d_probe,
+    lsqml_dots_kernel<<<nslot * kDotParts, 512, 0, h->stream>>>(h->object, h->d_obj, fprobe, h->d_probe,
                                                      h->quad, h->upd, frames, h->corners,
                                                      h->nxo, h->K, h->N, lambda0, h->sums,
                                                      fstride);

@@ -263,6 +263,18 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T)
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
   const float* iobs = a.iobs + (size_t)f * N * N;
   float afar = MODE == kLsqmlFused ? a.a_far[slot] : 0.f;
+  // Each thread's 16 pixels (idx = tid + i·T): their counts and model intensity, read once.
+  constexpr int kPixPerThread = H * N / T;
+  float yo_r[kPixPerThread], ic_r[kPixPerThread];
+#pragma unroll
+  for (int i = 0; i < kPixPerThread; ++i) {
+    const int idx = tid + i * T;
+    const int c = idx % H, ky = idx / H;
+    yo_r[i] = iobs[ky * N + r * H + c];
+    float ic = 0.f;
+    for (int m = 0; m < K; ++m) ic += cnorm2(S[(m * H + c) * L + (ky ^ swz(m * H + c))]);
+    ic_r[i] = ic * inv_n2;
+  }
   if ((MODE == kStore || MODE == kFromStore) && a.cost == kCostPoisson && a.a_out) {
     // One pass of the Poisson xi solver over this frame: with prev the batch mean of the
     // previous pass, a = clip(prev/2 + Σ xi·(Ĩ − I/(1 − prev·xi)) / Σ xi²·Ĩ / 2, 0, 1).
@@ -270,14 +282,11 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T)
                             ? batch_mean(a.a_prev, a.frames, a.a_prev_by_frame, a.nslot, red + 7)
                             : batch_mean(a.a_mid, a.frames, 0, a.nslot, red + 7);
     double num = 0.0, den = 0.0;
-#pragma unroll 4
-    for (int idx = tid; idx < H * N; idx += T) {
-      const int c = idx % H, ky = idx / H;
-      const float yo = iobs[ky * N + r * H + c];
+#pragma unroll
+    for (int i = 0; i < kPixPerThread; ++i) {
+      const float yo = yo_r[i];
       if (yo < 0.f) continue;
-      float ic = 0.f;
-      for (int m = 0; m < K; ++m) ic += cnorm2(S[(m * H + c) * L + (ky ^ swz(m * H + c))]);
-      const double yp = (double)(ic * inv_n2), yt = yo;
+      const double yp = (double)ic_r[i], yt = yo;
       const double xi = 1.0 - yt / (yp + 1e-5);
       num += xi * (yp - yt / (1.0 - prev * xi));
       den += xi * xi * yp;
@@ -287,17 +296,17 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T)
     afar = (float)fmin(fmax(0.5 * prev + 0.5 * ratio, 0.0), 1.0);
     if (r == 0 && tid == 0) a.a_out[slot] = afar;
   }
-#pragma unroll 4
-  for (int idx = tid; idx < H * N; idx += T) {
+#pragma unroll
+  for (int i = 0; i < kPixPerThread; ++i) {
+    if (MODE == kStore && !a.icalc) break;
+    const int idx = tid + i * T;
     const int c = idx % H, ky = idx / H;
     const int kx = r * H + c;
-    float ic = 0.f;
-    for (int m = 0; m < K; ++m) ic += cnorm2(S[(m * H + c) * L + (ky ^ swz(m * H + c))]);
-    ic *= inv_n2;
-    const float yo = iobs[ky * N + kx];
+    const float ic = ic_r[i];
+    const float yo = yo_r[i];
     const bool masked = yo < 0.f;
     if (MODE == kStore) {
-      if (a.icalc) a.icalc[((size_t)slot * N + ky) * N + kx] = ic;
+      a.icalc[((size_t)slot * N + ky) * N + kx] = ic;
       continue;
     }
     if (MODE == kLlk) {

@@ -22,17 +22,21 @@ PTYB_D double block_sum1(double v, double* sh) {
 // u = P·dO·q (dop), v = dP·O·q (dpo), c = χ: Σ|u|²+λ0, Σ|v|²+λ0, Σ Re u·v̄, Σ Im u·v̄,
 // Σ Re ū·c, Σ Re v̄·c (engine/lsqml.rs:302-323). Each thread sums its pixels in float, the
 // block adds the threads' sums in double; λ0 joins once per pixel and mode.
+constexpr int kDotParts = 4;  // blocks per frame; their sums are added in block order
+
 __global__ void __launch_bounds__(512) lsqml_dots_kernel(
     const float2* object, const float2* d_obj, const float2* probe, const float2* d_probe,
     const float2* quad, const float2* chi, const int* frames, const int2* corners, int nxo,
     int K, int N, double lambda0, double* sums, int probe_stride) {
   __shared__ double sh[16];
-  const int slot = blockIdx.x;
+  const int slot = blockIdx.x / kDotParts, part = blockIdx.x % kDotParts;
   const int2 c = corners[frames[slot]];
   const size_t plane = (size_t)N * N;
+  const int span = (K * N * N + kDotParts - 1) / kDotParts;
+  const int i0 = part * span, i1 = min(K * N * N, i0 + span);
   float s[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll 4
-  for (int idx = threadIdx.x; idx < K * N * N; idx += 512) {
+  for (int idx = i0 + threadIdx.x; idx < i1; idx += 512) {
     const int m = idx / (N * N), pix = idx % (N * N);
     const int yy = pix / N, xx = pix % N;
     const size_t o = (size_t)(c.x + yy) * nxo + c.y + xx;
@@ -47,10 +51,10 @@ __global__ void __launch_bounds__(512) lsqml_dots_kernel(
     s[4] += u.x * x.x + u.y * x.y;
     s[5] += v.x * x.x + v.y * x.y;
   }
-  const double reg = lambda0 * (double)K * (double)plane;
+  const double reg = part == 0 ? lambda0 * (double)K * (double)plane : 0.0;
   for (int k = 0; k < 6; ++k) {
     const double t = block_sum1<512>((double)s[k], sh);
-    if (threadIdx.x == 0) sums[(size_t)slot * 6 + k] = t + (k < 2 ? reg : 0.0);
+    if (threadIdx.x == 0) sums[((size_t)slot * kDotParts + part) * 6 + k] = t + (k < 2 ? reg : 0.0);
   }
 }
 
@@ -62,20 +66,28 @@ __global__ void __launch_bounds__(1024) lsqml_solve_kernel(const double* sums, i
                                                            const int* frames, float* a_far_all,
                                                            double* log, float* scal) {
   __shared__ double aobj[1024], aprb[1024], sorted[1024];
+  __shared__ double frame_sums[1024][2];
   __shared__ double means[2];
   const int t = threadIdx.x;
+  double s[6] = {0, 0, 0, 0, 0, 0};
+  if (t < nslot) {
+    for (int p = 0; p < kDotParts; ++p)
+      for (int k = 0; k < 6; ++k) s[k] += sums[((size_t)t * kDotParts + p) * 6 + k];
+    frame_sums[t][0] = s[0];
+    frame_sums[t][1] = s[1];
+  }
+  __syncthreads();
   if (t == 0) {
     double m0 = 0.0, m1 = 0.0;
     for (int i = 0; i < nslot; ++i) {
-      m0 += sums[i * 6 + 0];
-      m1 += sums[i * 6 + 1];
+      m0 += frame_sums[i][0];
+      m1 += frame_sums[i][1];
     }
     means[0] = 0.1 * (m0 / nslot);
     means[1] = 0.1 * (m1 / nslot);
   }
   __syncthreads();
   if (t < nslot) {
-    const double* s = sums + (size_t)t * 6;
     const double a11 = s[0] + means[0], a22 = s[1] + means[1];
     const double det = a11 * a22 - (s[2] * s[2] + s[3] * s[3]);
     const double x0 = (a22 * s[4] - s[2] * s[5]) / det;
