@@ -105,6 +105,24 @@ int ptyb_create(const ptyb_scan* scan, const double* object, int32_t nobj, int32
                 int32_t nxo, const double* probe, int32_t nprobe, const ptyb_options* options,
                 ptyb_handle** out);
 
+/* Reference `GpuPtycho::with_slices` (engine/gpu/mod.rs:629-660) on `Optics::with_slices`
+ * (engine/propagate.rs:81-99): pty-chi's multislice object, `objects` complex128
+ * [nslice][nyo][nxo] in the order the wave crosses them, `gaps` the nslice - 1 slice spacings in
+ * metres, each gap an angular-spectrum propagation at the object pixel; the exit is the scan's
+ * far field with its phase on the last slice. 1 <= nslice <= 16. A handle of more than one
+ * slice runs LSQML alone (ptyb_rpie, ptyb_ml, ptyb_set_positions and the forward-intensity
+ * calls return PTYB_INVALID on it); ptyb_get_object / ptyb_set_object read and replace slice 0
+ * as the reference's `object` / `set_object` do. */
+int ptyb_create_slices(const ptyb_scan* scan, const double* objects, int32_t nslice,
+                       const double* gaps, int32_t nyo, int32_t nxo, const double* probe,
+                       int32_t nprobe, const ptyb_options* options, ptyb_handle** out);
+
+/* The handle's object slices (1 for ptyb_create). */
+int ptyb_nslice(const ptyb_handle* h);
+
+/* Reference `GpuPtycho::objects` (engine/gpu/mod.rs:772-779): every slice, [nslice][nyo][nxo]. */
+int ptyb_get_objects(ptyb_handle* h, double* dst);
+
 /* Reference `GpuPtycho::rpie` (engine/gpu/rpie.rs:31-63). */
 int ptyb_rpie(ptyb_handle* h, const ptyb_rpie_params* params, int32_t nepoch);
 
@@ -163,6 +181,9 @@ int64_t ptyb_cycle(ptyb_handle* h);
  * batch order. */
 int ptyb_lsqml_steps_len(ptyb_handle* h);
 int ptyb_lsqml_steps(ptyb_handle* h, ptyb_lsqml_step* dst, int32_t cap);
+/* Of a multislice handle, the object steps of slices 1.. for the same frames,
+ * [ptyb_lsqml_steps_len][nslice - 1] (the reference `LsqmlStep::a_obj` of those slices). */
+int ptyb_lsqml_slice_steps(ptyb_handle* h, double* dst);
 
 /* Reference `GpuPtycho::synchronize` (engine/gpu/mod.rs:865-870). */
 int ptyb_synchronize(ptyb_handle* h);

@@ -1,7 +1,8 @@
 """pty-chi LSQML in float64 (oracle restatement, test infrastructure only).
 
-Follows physwkim/ptyrs `ptyrs/src/engine/lsqml.rs` for one object slice, no probe variation
-(`ProbeVariation::none`) and no position features: `LsqmlBatch::new` (lsqml.rs:102-179),
+Follows physwkim/ptyrs `ptyrs/src/engine/lsqml.rs` without probe variation
+(`ProbeVariation::none`), with the position feature under Patch sampling and pty-chi's
+multislice object (`SliceWaves`, engine/multislice.rs:87-438): `LsqmlBatch::new` (lsqml.rs:102-179),
 `obj_directions`, `frame_probe_directions`, `probe_direction` (lsqml.rs:194-229),
 `step_sizes` (lsqml.rs:286-350), `trim_mean` (lsqml.rs:392-398), `Lsqml::step`
 (lsqml.rs:581-643) and `Lsqml::epoch` (lsqml.rs:663-714).
@@ -28,6 +29,57 @@ def trim_mean(x):
     for v in kept:
         total += v
     return total / len(kept)
+
+
+def _unit(shape):
+    return np.ones(shape, np.complex128)
+
+
+class SliceWaves:
+    """The waves of `views` (each with its own probe plane, natural layout `planes[k]`)
+    through the slices of `optics` (engine/multislice.rs:87-173): `incident[s]` the wave
+    entering slice s (natural, one plane per view), `psi` the exit waves (shifted)."""
+
+    def __init__(self, optics, views, objects, planes):
+        self.optics, self.views, self.objects = optics, views, objects
+        ny, nx = planes.shape[-2:]
+        self.own = views.copy()
+        self.own["probe"] = np.arange(len(views))
+        self.incident = [planes]
+        for s, gap in enumerate(optics.gaps):
+            psi = ops.obj_probe_to_psi(self.own, objects[s], self.incident[s], _unit((ny, nx)))
+            psi = gap.forward(psi)
+            self.incident.append(fftshift2(psi))
+        last = len(objects) - 1
+        self.psi = ops.obj_probe_to_psi(self.own, objects[last], self.incident[last],
+                                        self.shared(last))
+
+    def shared(self, s):
+        q = self.optics.slice_quad(s)
+        return q if q is not None else _unit(self.optics.quad.shape)
+
+    def back_propagate(self, chi):
+        """Per slice, its change of psi_s (engine/multislice.rs:266-286)."""
+        out = [chi]
+        n = len(self.objects)
+        dims = self.incident[0].shape
+        for s in range(n - 2, -1, -1):
+            up = out[-1]
+            h, _ = ops.accumulate_probe(self.own, self.objects[s + 1], dims, self.shared(s + 1),
+                                        up)
+            g = self.optics.gaps[s].adjoint(fftshift2(h))
+            out.append(g)
+        out.reverse()
+        return out
+
+    def obj_adjoint(self, s, chi_s):
+        """Σ conj(q_s·in_s)·chi_s on the slice (engine/multislice.rs:399-428)."""
+        return ops.accumulate_obj(self.own, self.objects[s].shape, self.incident[s],
+                                  self.shared(s), chi_s)[0]
+
+    def obj_tangent(self, s, d):
+        """q_s·d·in_s per view, the change of psi_s along d (engine/multislice.rs:375-392)."""
+        return ops.obj_probe_to_psi(self.own, d, self.incident[s], self.shared(s))
 
 
 class Lsqml:
@@ -64,17 +116,19 @@ class Lsqml:
     def a_far(self, f):
         return self.a_far_all.get(f, 0.5)
 
-    def batch(self, views, obs, optics, obj, probe):
-        """`LsqmlBatch::new` (engine/lsqml.rs:102-179) for one slice without probe
-        variation: returns `(frames, nmode, psi, chi, a_far)`."""
+    def batch(self, views, obs, optics, objs, probe):
+        """`LsqmlBatch::new` (engine/lsqml.rs:102-179) without probe variation: returns
+        `(frames, nmode, waves, chis, a_far, uprobe, uviews)` with `chis` one per slice."""
         nmode = 1
         while nmode < len(views) and views[nmode]["frame"] == views[0]["frame"]:
             nmode += 1
         frames = [int(views[b * nmode]["frame"]) for b in range(len(views) // nmode)]
         ny, nx = probe.shape[-2:]
-        uprobe = self.frame_probes(frames, probe, optics.quad)
+        uprobe = self.frame_probes(frames, probe, optics.slice_quad(0))
         uviews = self.unique_views(views, len(frames), probe.shape[0], nmode)
-        psi = ops.obj_probe_to_psi(uviews, obj, uprobe, optics.quad)
+        planes = uprobe[uviews["probe"].astype(np.int64)]
+        waves = SliceWaves(optics, uviews, objs, planes)
+        psi = waves.psi
         chi = optics.exit_forward(psi)
         sh = (len(frames), nmode, ny, nx)
         icalc = (np.abs(chi.reshape(sh)) ** 2).sum(axis=1)
@@ -100,81 +154,81 @@ class Lsqml:
         fac = 1.0 - np.asarray(a_far)[:, None, None] * c
         chi = (chi.reshape(sh) * fac[:, None]).reshape(chi.shape)
         chi = optics.exit_adjoint(chi) - psi
-        return frames, nmode, psi, chi, a_far, uprobe, uviews
+        chis = waves.back_propagate(chi)
+        return frames, nmode, waves, chis, a_far, uprobe, uviews
 
     def step(self, views, obs, optics, obj, probe):
-        """`Lsqml::step` (engine/lsqml.rs:581-643); returns the new object and probe and the
-        step record."""
+        """`Lsqml::step` (engine/lsqml.rs:581-643); `obj` is one slice's array or a list of
+        slices. Returns the new object(s) and probe and the step record."""
+        single = not isinstance(obj, (list, tuple))
+        objs = [obj] if single else list(obj)
         pre = self.preconditioner
         floor = (0.1 * pre.max()) ** 2
-        frames, nmode, psi, chi, a_far, uprobe, uviews = self.batch(views, obs, optics, obj,
-                                                                     probe)
-        q = optics.quad
+        frames, nmode, waves, chis, a_far, uprobe, uviews = self.batch(views, obs, optics, objs,
+                                                                       probe)
         ny, nx = probe.shape[-2:]
         np_ = probe.shape[0]
         nb = len(frames)
-        # obj_directions: accumulate_obj over the views at each frame's own probe
-        d_obj = ops.accumulate_obj(uviews, obj.shape, uprobe, q, chi)[0]
-        d_obj = d_obj / np.sqrt(pre * pre + floor)
-        # frame_probe_directions: per-frame planes b·np + m, moved back by −offset
-        d, _ = ops.accumulate_probe(uviews, obj, (nb * np_, ny, nx), q, chi)
+        d_obj = [waves.obj_adjoint(s, chis[s]) / np.sqrt(pre * pre + floor)
+                 for s in range(len(objs))]
+        # frame_probe_directions on slice 0, moved back by −offset
+        d, _ = ops.accumulate_probe(uviews, objs[0], (nb * np_, ny, nx), waves.shared(0),
+                                    chis[0])
         if self.offsets is not None:
             for b, f in enumerate(frames):
-                d[b * np_:(b + 1) * np_] = ops.move_planes(d[b * np_:(b + 1) * np_], q,
+                d[b * np_:(b + 1) * np_] = ops.move_planes(d[b * np_:(b + 1) * np_],
+                                                           optics.slice_quad(0),
                                                            -self.offsets[f])
         d_probe = np.zeros_like(probe)
         for b in range(nb):
             for m in range(np_):
                 d_probe[m] += d[b * np_ + m]
         d_probe = d_probe / float(nb)
-        a_obj, a_probe = self.step_sizes(views, nmode, optics, obj, probe, chi, d_obj, d_probe,
-                                         uprobe, uviews)
+        a_obj, a_probe = self.step_sizes(views, nmode, optics, objs, waves, chis, d_obj,
+                                         d_probe)
         d_pos = None
         if self.refine and self.offsets is not None:
-            d_pos = self.position_directions(frames, nmode, optics, obj, uprobe, uviews, chi)
+            d_pos = self.position_directions(frames, nmode, optics, objs, waves, chis, uviews)
         for f, a in zip(frames, a_far):
             self.a_far_all[f] = a
-        so = trim_mean(a_obj)
-        new_obj = obj + so * d_obj
+        new_objs = [o + trim_mean(a) * dd for o, a, dd in zip(objs, a_obj, d_obj)]
         sp = sum(a_probe) / len(a_probe)
         new_probe = probe + sp * d_probe
         if d_pos is not None:
             ops.batch_position_step(self.offsets, frames, d_pos)
-        return new_obj, new_probe, dict(frames=frames, a_far=a_far, a_obj=a_obj,
-                                        a_probe=a_probe)
+        rec = dict(frames=frames, a_far=a_far, a_obj=a_obj[0] if single else a_obj,
+                   a_probe=a_probe)
+        return (new_objs[0] if single else new_objs), new_probe, rec
 
-    def position_directions(self, frames, nmode, optics, obj, uprobe, uviews, chi):
-        """pty-chi LSQML's gradient position direction per frame, from the frame's mode-0
-        wave and chi and its object window (engine/lsqml.rs:237-270), single slice."""
-        ny, nx = uprobe.shape[-2:]
+    def position_directions(self, frames, nmode, optics, objs, waves, chis, uviews):
+        """pty-chi LSQML's gradient position direction per frame on slice nslice/2, from the
+        wave entering it at the frame's first view times the slice's phase, its chi and the
+        slice's window (engine/lsqml.rs:237-270)."""
+        s = len(objs) // 2
+        ny, nx = waves.incident[0].shape[-2:]
         sums = []
         for b in range(len(frames)):
             k = b * nmode
             v = uviews[k]
-            w = fftshift2(uprobe[int(v["probe"])] * optics.quad)
+            w = fftshift2(waves.incident[s][k] * waves.shared(s))
             oy, ox = int(v["oy"]), int(v["ox"])
-            patch = obj[int(v["obj"]), oy:oy + ny, ox:ox + nx]
-            sums.append(ops.gradient_sums(patch, w, chi[k]))
+            patch = objs[s][int(v["obj"]), oy:oy + ny, ox:ox + nx]
+            sums.append(ops.gradient_sums(patch, w, chis[s][k]))
         eps = ops.EPS_POSITION * optics.intensity_scale()
         return ops.gradient_directions(sums, eps)
 
-    def step_sizes(self, views, nmode, optics, obj, probe, chi, d_obj, d_probe, uprobe=None,
-                   uviews=None):
-        """pty-chi Eq. 22 per frame (engine/lsqml.rs:286-350), one slice: `dop` at each
-        frame's own probe, `dpo` from the shared probe direction."""
-        ny, nx = probe.shape[-2:]
+    def step_sizes(self, views, nmode, optics, objs, waves, chis, d_obj, d_probe):
+        """pty-chi Eq. 22 on slice 0 jointly with the probe, Eq. 23b on the other slices
+        (engine/lsqml.rs:286-350)."""
+        ny, nx = d_probe.shape[-2:]
         n = ny * nx
-        q = optics.quad
-        scale = float(1 * nmode)
-        dpo = ops.obj_probe_to_psi(views, obj, d_probe, q)
-        if uprobe is None:
-            dop = ops.obj_probe_to_psi(views, d_obj, probe, q)
-        else:
-            dop = ops.obj_probe_to_psi(uviews, d_obj, uprobe, q)
+        scale = float(len(objs) * nmode)
+        dpo = ops.obj_probe_to_psi(views, objs[0], d_probe, waves.shared(0))
+        dop = waves.obj_tangent(0, d_obj[0])
         lambda0 = LAMBDA0 * optics.intensity_scale() / n
         nb = len(views) // nmode
         sh = (nb, nmode * n)
-        u, v, c = dop.reshape(sh), dpo.reshape(sh), chi.reshape(sh)
+        u, v, c = dop.reshape(sh), dpo.reshape(sh), chis[0].reshape(sh)
         a12 = u * np.conj(v)
         s = np.stack([(np.abs(u) ** 2 + lambda0).sum(axis=1),
                       (np.abs(v) ** 2 + lambda0).sum(axis=1),
@@ -182,22 +236,30 @@ class Lsqml:
                       (np.conj(u) * c).real.sum(axis=1),
                       (np.conj(v) * c).real.sum(axis=1)], axis=1)
         reg11, reg22 = 0.1 * (s[:, 0].sum() / nb), 0.1 * (s[:, 1].sum() / nb)
-        a_obj, a_probe = [], []
+        a_obj0, a_probe = [], []
         for r in s:
             a11, a22 = r[0] + reg11, r[1] + reg22
             det = a11 * a22 - (r[2] * r[2] + r[3] * r[3])
             x0 = (a22 * r[4] - r[2] * r[5]) / det
             x1 = (a11 * r[5] - r[2] * r[4]) / det
-            a_obj.append(0.9 * max(x0, 0.0) / scale)
+            a_obj0.append(0.9 * max(x0, 0.0) / scale)
             a_probe.append(0.9 * max(x1, 0.0))
+        a_obj = [a_obj0]
+        for sl in range(1, len(objs)):
+            du = waves.obj_tangent(sl, d_obj[sl]).reshape(sh)
+            cs = chis[sl].reshape(sh)
+            num = (np.conj(du) * cs).real.sum(axis=1)
+            den = (np.abs(du) ** 2).sum(axis=1)
+            a_obj.append([max(0.5 * nu / de * 0.9 / scale, 0.0) for nu, de in zip(num, den)])
         return a_obj, a_probe
 
     def epoch(self, addr, obs, optics, obj, probe):
         """`Lsqml::epoch` (engine/lsqml.rs:663-714): preconditioner on pty-chi's schedule, then
         `step` over the epoch's seeded batches. Returns `(obj, probe, steps)`."""
-        nframe, nmode = addr.nframe, addr.nmode
+        nframe = addr.nframe
+        o0 = obj if not isinstance(obj, (list, tuple)) else obj[0]
         if self.epochs < 10 or self.epochs % 10 == 0:
-            illum = ops.illumination(addr.views, obj.shape, probe)
+            illum = ops.illumination(addr.views, o0.shape, probe)
             pre = self.preconditioner
             if pre is None:
                 n = float(probe.shape[-1] * probe.shape[-2])
@@ -218,12 +280,14 @@ class Lsqml:
         return obj, probe, steps
 
     def llk(self, addr, obs, optics, obj, probe):
-        """Normalised LLK of the model the steps update, each frame's own (moved) probe
-        (engine/lsqml.rs:537-551)."""
+        """Normalised LLK of the model the steps update, each frame's own (moved) probe,
+        through every slice (engine/lsqml.rs:537-551)."""
+        objs = [obj] if not isinstance(obj, (list, tuple)) else list(obj)
         frames = list(range(addr.nframe))
-        uprobe = self.frame_probes(frames, probe, optics.quad)
+        uprobe = self.frame_probes(frames, probe, optics.slice_quad(0))
         uviews = self.unique_views(addr.views, addr.nframe, probe.shape[0], addr.nmode)
-        psi = optics.exit_forward(ops.obj_probe_to_psi(uviews, obj, uprobe, optics.quad))
+        waves = SliceWaves(optics, uviews, objs, uprobe[uviews["probe"].astype(np.int64)])
+        psi = optics.exit_forward(waves.psi)
         return ops.llk(obs, slice(0, addr.nframe), addr.nmode, psi).normalised(obs.nb_obs)
 
 

@@ -176,12 +176,28 @@ class Propagator:
 
 
 class Optics:
-    """Exit-wave model `psi = E(P·O·q)` (engine/propagate.rs:24-207), single slice."""
+    """Exit-wave model `psi = E(P·O·q)` (engine/propagate.rs:24-207); with `gaps`, the
+    angular-spectrum propagators between consecutive object slices (propagate.rs:84-99)."""
 
-    def __init__(self, pixel, quad, propagator):
+    def __init__(self, pixel, quad, propagator, gaps=()):
         self.pixel = list(pixel)
         self.quad = quad  # natural layout [ny, nx]
         self.propagator = propagator
+        self.gaps = list(gaps)
+
+    def with_slices(self, gap_wavefields):
+        """This model through len(gaps) + 1 slices, each gap angular spectrum
+        (propagate.rs:84-99)."""
+        return Optics(self.pixel, self.quad, self.propagator,
+                      [Propagator._angular(w) for w in gap_wavefields])
+
+    def nslice(self):
+        return len(self.gaps) + 1
+
+    def slice_quad(self, s):
+        """The plane phase slice `s` applies: `quad` on the last slice, none before
+        (propagate.rs:143-148)."""
+        return self.quad if s + 1 == self.nslice() else None
 
     @staticmethod
     def far_field(wavelength, distance, detector_pixel, frame):

@@ -53,6 +53,10 @@ class LsqmlStep(ctypes.Structure):
 SIGNATURES = {
     "ptyb_create": (c_int32, [P(Scan), P(c_double), c_int32, c_int32, c_int32, P(c_double),
                               c_int32, P(Options), P(c_void_p)]),
+    "ptyb_create_slices": (c_int32, [P(Scan), P(c_double), c_int32, P(c_double), c_int32,
+                                     c_int32, P(c_double), c_int32, P(Options), P(c_void_p)]),
+    "ptyb_nslice": (c_int32, [c_void_p]),
+    "ptyb_get_objects": (c_int32, [c_void_p, P(c_double)]),
     "ptyb_rpie": (c_int32, [c_void_p, P(RpieParams), c_int32]),
     "ptyb_lsqml": (c_int32, [c_void_p, P(LsqmlParams), c_int32, c_int32]),
     "ptyb_ml": (c_int32, [c_void_p, P(MlParams), c_int32]),
@@ -72,6 +76,7 @@ SIGNATURES = {
     "ptyb_cycle": (c_int64, [c_void_p]),
     "ptyb_lsqml_steps_len": (c_int32, [c_void_p]),
     "ptyb_lsqml_steps": (c_int32, [c_void_p, P(LsqmlStep), c_int32]),
+    "ptyb_lsqml_slice_steps": (c_int32, [c_void_p, P(c_double)]),
     "ptyb_synchronize": (c_int32, [c_void_p]),
     "ptyb_launches": (c_int64, [c_void_p]),
     "ptyb_random_batches": (c_int32, [c_int32, c_int32, ctypes.c_uint64, ctypes.c_uint64,

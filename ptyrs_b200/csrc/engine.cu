@@ -18,6 +18,7 @@
 #include "lsqml.cuh"
 #include "ml.cuh"
 #include "position.cuh"
+#include "multislice.cuh"
 #include "scan.h"
 
 using namespace ptyb;
@@ -78,6 +79,10 @@ __global__ void fill_kernel(float* x, float v, int n) {
 // to a kernel (on the host it names a stand-in, not the device array): it takes the device
 // address from `noalloc_scratch()`.
 constexpr size_t kNoallocScratchBytes = size_t(32) << 20;
+// Object slices of a multislice handle, and the float scalars on the device (maxima, the
+// batch's object and probe steps, one step per further slice).
+constexpr int kMaxSlices = 16;
+constexpr int kScalars = 8 + kMaxSlices;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];
 
 namespace {
@@ -138,6 +143,14 @@ struct ptyb_handle {
   bool have_offsets = false, refine_offsets = false;
   float2* wave = nullptr;        // [slots][K][N][N]
   double* pos_sums = nullptr;    // [slots][4]
+  // Multislice (pty-chi's multislice object, LSQML only): slices, gap transfer functions, the
+  // incident waves of slices 1.., every slice's χ, a plane of ones (slices without a phase).
+  int nslice = 1;
+  float2* tf = nullptr;          // [nslice-1][N][N]
+  float2* incident = nullptr;    // [nslice-1][slots][K][N][N]
+  float2* chi_slices = nullptr;  // [nslice][slots][K][N][N]
+  float2* ones = nullptr;        // [N][N]
+  double* slice_sums = nullptr;  // [slots][2]
   double* partials = nullptr;    // [kPartialBlocks][2]
   std::vector<Buf> bufs;
   // Per-kernel device timing (CUDA events on the engine's stream), when enabled.
@@ -153,6 +166,8 @@ struct ptyb_handle {
   int64_t launches = 0;
   std::vector<ptyb_llk_record> history;
   std::vector<ptyb_lsqml_step> steps;
+  std::vector<double> slice_steps;  // [frame of the last epoch][slice 1..]: a_obj
+  int log_stride = 3;
   bool aborted = false;
   std::string err;
 };
@@ -212,14 +227,14 @@ enum Kind : int {
   kKFrameRpie = 0, kKFrameLsqml, kKFrameMl, kKFrameLlk, kKFrameStore, kKFrameFromStore,
   kKObjRpie, kKObjOverlap, kKObjLsqml, kKObjMl, kKIllum, kKProbePartial, kKProbeFinal,
   kKAfar, kKDots, kKSolve, kKAxpy, kKMax, kKCounts, kKMisc, kKGamma, kKArraySums, kKMove,
-  kKPositionSums, kNumKinds
+  kKPositionSums, kKSliceForward, kKSliceBackward, kKSliceLlk, kNumKinds
 };
 const char* const kKindNames[kNumKinds] = {
     "frame_rpie", "frame_lsqml", "frame_ml_grad", "frame_llk", "frame_store",
     "frame_from_store", "object_rpie", "object_overlap", "object_lsqml", "object_ml",
     "illumination", "probe_partial", "probe_finalize", "lsqml_afar", "lsqml_dots",
     "lsqml_solve", "axpy", "max", "counts", "misc", "ml_gamma", "array_sums", "move",
-    "position_sums"};
+    "position_sums", "slice_forward", "slice_backward", "slice_llk"};
 
 cudaEvent_t take_event(ptyb_handle* h) {
   if (!h->event_pool.empty()) {
@@ -392,6 +407,50 @@ cudaError_t launch_move(ptyb_handle* h, const MoveArgs& a, int nslot) {
   return e;
 }
 
+template <int N, int C, int MODE>
+cudaError_t launch_slice_nc(const SliceArgs& a, int nslot, int K, cudaStream_t s) {
+  auto kern = slice_kernel<N, C, MODE>;
+  const size_t smem = frame_smem_bytes<N, C>(K);
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  if (C > 8) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return e;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nslot * C);
+  cfg.blockDim = dim3(FrameShape<N, C>::T);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = C > 1 ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kern, a);
+}
+
+template <int MODE>
+cudaError_t launch_slice(ptyb_handle* h, const SliceArgs& a, int nslot) {
+  if (nslot <= 0) return cudaSuccess;
+  constexpr int kind = MODE == kSliceForward ? kKSliceForward
+                       : MODE == kSliceBackward ? kKSliceBackward
+                                                : kKSliceLlk;
+  cudaError_t e = cudaErrorInvalidValue;
+  timed(h, kind, [&] {
+    switch (h->N * 100 + h->C) {
+      case 6401: e = launch_slice_nc<64, 1, MODE>(a, nslot, h->K, h->stream); break;
+      case 12802: e = launch_slice_nc<128, 2, MODE>(a, nslot, h->K, h->stream); break;
+      case 12804: e = launch_slice_nc<128, 4, MODE>(a, nslot, h->K, h->stream); break;
+      case 25608: e = launch_slice_nc<256, 8, MODE>(a, nslot, h->K, h->stream); break;
+      case 25616: e = launch_slice_nc<256, 16, MODE>(a, nslot, h->K, h->stream); break;
+    }
+  });
+  return e;
+}
+
 MoveArgs move_args(ptyb_handle* h, const int* frames, float2* planes) {
   MoveArgs m = {};
   m.probe = h->probe;
@@ -469,6 +528,11 @@ void ensure_slots(ptyb_handle* h, int n) {
     h->wave = alloc<float2>(h, (size_t)n * h->K * plane);
     h->pos_sums = alloc<double>(h, (size_t)n * 4);
   }
+  if (h->nslice > 1) {
+    h->incident = alloc<float2>(h, (size_t)(h->nslice - 1) * n * h->K * plane);
+    h->chi_slices = alloc<float2>(h, (size_t)h->nslice * n * h->K * plane);
+    h->slice_sums = alloc<double>(h, (size_t)n * 2);
+  }
   h->slots = n;
 }
 
@@ -487,13 +551,16 @@ int probe_chunk(ptyb_handle* h, int nslot, int* nchunk) {
 
 // Σ_frames (w·upd) into the probe (mode 0: P += coef·Σ with the rPIE weight; 1: d_probe =
 // coef·Σ conj(q·O)·upd).
-void probe_pass(ptyb_handle* h, const int* frames, int nslot, int mode, float alpha, float coef) {
+// Probe direction Σ w·upd over the batch; `quad` and `upd` default to the exit phase and the
+// frame kernel's update planes.
+void probe_pass(ptyb_handle* h, const int* frames, int nslot, int mode, float alpha, float coef,
+                const float2* quad = nullptr, const float2* upd = nullptr) {
   int nchunk = 0;
   const int chunk = probe_chunk(h, nslot, &nchunk);
   ProbeArgs p = {};
   p.object = h->object;
-  p.quad = h->quad;
-  p.upd = h->upd;
+  p.quad = quad ? quad : h->quad;
+  p.upd = upd ? upd : h->upd;
   p.frames = frames;
   p.corners = h->corners;
   p.omax = h->omax;
@@ -524,6 +591,17 @@ ptyb_llk llk_pass(ptyb_handle* h) {
     const int n = std::min(stack, h->P - s0);
     FrameArgs a = frame_args(h, h->iota + s0);
     a.llk = h->llk + (size_t)s0 * 4;
+    if (h->nslice > 1) {
+      SliceArgs sa = {};
+      sa.f = a;
+      sa.f.nslot = n;
+      sa.tf = h->tf;
+      sa.nslice = h->nslice;
+      sa.obj_plane = (size_t)h->nyo * h->nxo;
+      check(h, launch_slice<kSliceLlk>(h, sa, n), "llk pass");
+      ++h->launches;
+      continue;
+    }
     if (h->have_offsets) {
       // each frame's own moved probe (engine/lsqml.rs:537-551)
       check(h, launch_move<kMoveProbe>(h, move_args(h, h->iota + s0, h->wave), n), "probe move");
@@ -651,6 +729,89 @@ void lsqml_preconditioner(ptyb_handle* h, bool init) {
   launched(h, "pre max");
 }
 
+// One LSQML step through pty-chi's multislice object (engine/lsqml.rs:581-643 with
+// SliceWaves, engine/multislice.rs): forward through the slices, backward χ per slice, every
+// slice's object direction from its incident wave, the probe direction from χ of slice 0,
+// slice 0's step sizes jointly with the probe and Eq. 23b on the others.
+void lsqml_batch_slices(ptyb_handle* h, const ptyb_lsqml_params& p, const int* frames, int nslot,
+                        double* log, int log_stride) {
+  const int S = h->nslice;
+  const size_t plane = (size_t)h->N * h->N, fplanes = (size_t)h->K * plane;
+  const size_t slice_stride = (size_t)nslot * fplanes, no = (size_t)h->nyo * h->nxo;
+  SliceArgs sa = {};
+  sa.f = frame_args(h, frames);
+  sa.f.cost = p.cost;
+  sa.f.nslot = nslot;
+  sa.f.a_prev = h->afar_all;
+  sa.f.a_prev_by_frame = 1;
+  sa.f.a_out = h->afar1;
+  sa.tf = h->tf;
+  sa.incident = h->incident;
+  sa.chi = h->chi_slices;
+  sa.nslice = S;
+  sa.obj_plane = no;
+  check(h, launch_slice<kSliceForward>(h, sa, nslot), "multislice forward");
+  ++h->launches;
+  sa.f.a_mid = h->afar1;
+  sa.f.a_out = h->afar2;
+  check(h, launch_slice<kSliceBackward>(h, sa, nslot), "multislice backward");
+  ++h->launches;
+  for (int s = 0; s < S; ++s) {
+    GatherArgs g = gather_args(h, frames, nslot);
+    g.upd = h->chi_slices + s * slice_stride;
+    g.out = h->d_obj + s * no;
+    g.quad = s + 1 == S ? h->quad : h->ones;
+    if (s > 0) {
+      g.probe = h->incident + (s - 1) * slice_stride;
+      g.probe_stride = (int)fplanes;
+    }
+    timed(h, kKObjLsqml, [&] { object_tile_kernel<kGatherLsqml><<<ntiles(h), 1024, 0, h->stream>>>(g); });
+    launched(h, "slice object direction");
+  }
+  // probe direction from χ of slice 0 through slice 0's windows (no phase when S > 1)
+  probe_pass(h, frames, nslot, 1, 0.f, 1.0f / nslot, h->ones, h->chi_slices);
+  const double lambda0 = 1.2e-7 * ((double)h->N * h->N) / ((double)h->N * h->N);
+  timed(h, kKDots, [&] {
+    lsqml_dots_kernel<<<nslot * kDotParts, 512, 0, h->stream>>>(
+        h->object, h->d_obj, h->probe, h->d_probe, h->ones, h->chi_slices, frames, h->corners,
+        h->nxo, h->K, h->N, lambda0, h->sums, 0);
+  });
+  launched(h, "step sums");
+  const double scale = (double)(S * h->K);
+  for (int s = 1; s < S; ++s) {
+    timed(h, kKDots, [&] {
+      slice_dots_kernel<<<nslot, 512, 0, h->stream>>>(
+          h->d_obj + s * no, h->incident + (s - 1) * slice_stride,
+          s + 1 == S ? h->quad : nullptr, h->chi_slices + s * slice_stride, frames, h->corners,
+          h->nxo, h->K, h->N, h->slice_sums);
+    });
+    launched(h, "slice sums");
+    timed(h, kKSolve, [&] {
+      slice_solve_kernel<<<1, 1024, 0, h->stream>>>(h->slice_sums, nslot, scale, log + 2 + s,
+                                                    log_stride, h->scal + 3 + s);
+    });
+    launched(h, "slice solve");
+  }
+  timed(h, kKSolve, [&] {
+    lsqml_solve_kernel<<<1, 1024, 0, h->stream>>>(h->sums, nslot, scale, h->afar2, frames,
+                                                   h->afar_all, log, h->scal + 2, log_stride);
+  });
+  launched(h, "step solve");
+  for (int s = 0; s < S; ++s) {
+    const int which = s == 0 ? 0 : 1 + s;  // relative to scal + 2: so_0, sp, so_1, so_2, …
+    timed(h, kKAxpy, [&] {
+      axpy_scal_kernel<<<(unsigned)((no + 255) / 256), 256, 0, h->stream>>>(
+          h->object + s * no, h->d_obj + s * no, h->scal + 2, which, no);
+    });
+    launched(h, "slice step");
+  }
+  timed(h, kKAxpy, [&] {
+    axpy_scal_kernel<<<(unsigned)((fplanes + 255) / 256), 256, 0, h->stream>>>(
+        h->probe, h->d_probe, h->scal + 2, 1, fplanes);
+  });
+  launched(h, "probe step");
+}
+
 // One LSQML step on a batch (engine/lsqml.rs:581-643), with the position model when offsets
 // are set: each frame's probe moved by its offset, the probe directions moved back before
 // their frame mean, and with refinement pty-chi's position step after the update.
@@ -732,7 +893,7 @@ void lsqml_batch(ptyb_handle* h, const ptyb_lsqml_params& p, const int* frames, 
   }
   timed(h, kKSolve, [&] {
     lsqml_solve_kernel<<<1, 1024, 0, h->stream>>>(h->sums, nslot, (double)(1 * h->K), h->afar2,
-                                                   frames, h->afar_all, log, h->scal + 2);
+                                                   frames, h->afar_all, log, h->scal + 2, 3);
   });
   launched(h, "step solve");
   const size_t no = (size_t)h->nyo * h->nxo, np = (size_t)h->K * h->N * h->N;
@@ -1058,15 +1219,30 @@ int guarded(ptyb_handle* h, bool enqueues, F&& body) {
 
 extern "C" {
 
-int ptyb_create(const ptyb_scan* scan, const double* object, int32_t nobj, int32_t nyo,
-                int32_t nxo, const double* probe, int32_t nprobe, const ptyb_options* options,
-                ptyb_handle** out) {
+}  // extern "C"
+
+namespace {
+
+// A handle over `nslice` object slices (each one object mode) with the angular-spectrum gaps
+// `gaps` (metres) between them; one slice is the plain object of ptyb_create.
+int create_handle(const ptyb_scan* scan, const double* object, int32_t nobj, int32_t nslice,
+                  const double* gaps, int32_t nyo, int32_t nxo, const double* probe,
+                  int32_t nprobe, const ptyb_options* options, ptyb_handle** out) {
   if (!out) return PTYB_INVALID;
   *out = nullptr;
   if (!scan || !object || !probe || !scan->counts || !scan->pos_y || !scan->pos_x)
     return PTYB_INVALID;
   const int N = scan->ny;
   g_create_error.clear();
+  if (nslice < 1 || nslice > kMaxSlices || (nslice > 1 && !gaps)) {
+    g_create_error = "need 1 to " + std::to_string(kMaxSlices) + " slices and their gaps";
+    return PTYB_INVALID;
+  }
+  for (int s = 0; s + 1 < nslice; ++s)
+    if (!std::isfinite(gaps[s])) {
+      g_create_error = "slice gaps must be finite";
+      return PTYB_INVALID;
+    }
   if (scan->nx != N || !(N == 64 || N == 128 || N == 256)) {
     g_create_error = "frames must be square with a side of 64, 128 or 256";
     return PTYB_INVALID;
@@ -1096,6 +1272,8 @@ int ptyb_create(const ptyb_scan* scan, const double* object, int32_t nobj, int32
   h->nxo = nxo;
   h->C = C;
   h->stack = options && options->stack_size > 0 ? options->stack_size : 64;
+  h->nslice = nslice;
+  h->log_stride = 2 + nslice;
   // Positions: PyNX preprocessing and window corners (base/positions.rs, base/addr.rs).
   const double lz = scan->wavelength * scan->distance;
   h->pixel[0] = lz / (N * scan->detector_pixel);
@@ -1160,8 +1338,8 @@ int ptyb_create(const ptyb_scan* scan, const double* object, int32_t nobj, int32
     h->corners = alloc<int2>(h, h->P);
     check(h, cudaMemcpy(h->corners, h->corners_h.data(), h->P * sizeof(int2), cudaMemcpyHostToDevice),
           "corners upload");
-    h->object = alloc<float2>(h, (size_t)nobj * nyo * nxo);
-    auto o = from_c64(object, (size_t)nobj * nyo * nxo);
+    h->object = alloc<float2>(h, (size_t)nslice * nobj * nyo * nxo);
+    auto o = from_c64(object, (size_t)nslice * nobj * nyo * nxo);
     check(h, cudaMemcpy(h->object, o.data(), o.size() * sizeof(float2), cudaMemcpyHostToDevice),
           "object upload");
     h->probe = alloc<float2>(h, (size_t)nprobe * plane);
@@ -1191,12 +1369,39 @@ int ptyb_create(const ptyb_scan* scan, const double* object, int32_t nobj, int32
     h->order = alloc<int>(h, h->P);
     h->afar_all = alloc<float>(h, h->P);
     h->llk = alloc<double>(h, (size_t)h->P * 4);
-    h->scal = alloc<float>(h, 8);
+    h->scal = alloc<float>(h, kScalars);
     h->pre = alloc<float>(h, (size_t)nyo * nxo);
-    h->d_obj = alloc<float2>(h, (size_t)nyo * nxo);
+    h->d_obj = alloc<float2>(h, (size_t)nslice * nyo * nxo);
     h->d_probe = alloc<float2>(h, (size_t)K * plane);
-    h->steplog = alloc<double>(h, (size_t)h->P * 3);
-    check(h, cudaMemset(h->scal, 0, 8 * sizeof(float)), "memset");
+    h->steplog = alloc<double>(h, (size_t)h->P * h->log_stride);
+    check(h, cudaMemset(h->scal, 0, kScalars * sizeof(float)), "memset");
+    if (nslice > 1) {
+      // Angular-spectrum transfer functions exp(2πi z √(1 − r)) of the gaps in DFT order, 0 on
+      // the evanescent band (engine/propagate.rs:505-531), in double; the plane of ones is the
+      // phase of every slice but the last.
+      const double width = h->pixel[1] / scan->wavelength, ar = h->pixel[1] / h->pixel[0];
+      std::vector<float2> t((size_t)(nslice - 1) * plane), ones(plane, make_float2(1.f, 0.f));
+      for (int g = 0; g + 1 < nslice; ++g) {
+        const double i2piz = 2.0 * M_PI * (gaps[g] / scan->wavelength);
+        for (int yy = 0; yy < N; ++yy)
+          for (int xx = 0; xx < N; ++xx) {
+            const double fy = (double)(yy < N / 2 ? yy : yy - N) / N;
+            const double fx = (double)(xx < N / 2 ? xx : xx - N) / N;
+            const double ratio = (fx * fx + (ar * fy) * (ar * fy)) / (width * width);
+            float2 v = make_float2(0.f, 0.f);
+            if (ratio < 1.0) {
+              const double ph = i2piz * std::sqrt(1.0 - ratio);
+              v = make_float2((float)std::cos(ph), (float)std::sin(ph));
+            }
+            t[(size_t)g * plane + (size_t)yy * N + xx] = v;
+          }
+      }
+      h->tf = alloc<float2>(h, t.size());
+      check(h, cudaMemcpy(h->tf, t.data(), t.size() * sizeof(float2), cudaMemcpyHostToDevice), "tf");
+      h->ones = alloc<float2>(h, plane);
+      check(h, cudaMemcpy(h->ones, ones.data(), plane * sizeof(float2), cudaMemcpyHostToDevice),
+            "ones");
+    }
     return PTYB_OK;
   });
   if (rc != PTYB_OK) {
@@ -1205,6 +1410,30 @@ int ptyb_create(const ptyb_scan* scan, const double* object, int32_t nobj, int32
     return rc;
   }
   *out = h;
+  return PTYB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ptyb_create(const ptyb_scan* scan, const double* object, int32_t nobj, int32_t nyo,
+                int32_t nxo, const double* probe, int32_t nprobe, const ptyb_options* options,
+                ptyb_handle** out) {
+  return create_handle(scan, object, nobj, 1, nullptr, nyo, nxo, probe, nprobe, options, out);
+}
+
+int ptyb_create_slices(const ptyb_scan* scan, const double* objects, int32_t nslice,
+                       const double* gaps, int32_t nyo, int32_t nxo, const double* probe,
+                       int32_t nprobe, const ptyb_options* options, ptyb_handle** out) {
+  return create_handle(scan, objects, 1, nslice, gaps, nyo, nxo, probe, nprobe, options, out);
+}
+
+int ptyb_nslice(const ptyb_handle* h) { return h ? h->nslice : 0; }
+
+int ptyb_lsqml_slice_steps(ptyb_handle* h, double* dst) {
+  if (!h || !dst) return PTYB_INVALID;
+  std::copy(h->slice_steps.begin(), h->slice_steps.end(), dst);
   return PTYB_OK;
 }
 
@@ -1220,6 +1449,10 @@ int ptyb_rpie(ptyb_handle* h, const ptyb_rpie_params* p, int32_t nepoch) {
   }
   if (h->have_offsets) {
     h->err = "rPIE does not model position offsets in this version";
+    return PTYB_INVALID;
+  }
+  if (h->nslice > 1) {
+    h->err = "rPIE runs on a single-slice object";
     return PTYB_INVALID;
   }
   return guarded(h, true, [&]() -> int {
@@ -1270,8 +1503,12 @@ int ptyb_lsqml(ptyb_handle* h, const ptyb_lsqml_params* p, int32_t nepoch, int32
       if (ic < 10 || ic % 10 == 0) lsqml_preconditioner(h, ic == 0);
       const int* order = h->order_all + (size_t)ic * h->P;
       int off = 0;
+      const int stride = h->log_stride;
       for (int n : sizes[ic]) {
-        lsqml_batch(h, *p, order + off, n, h->steplog + (size_t)off * 3);
+        if (h->nslice > 1)
+          lsqml_batch_slices(h, *p, order + off, n, h->steplog + (size_t)off * stride, stride);
+        else
+          lsqml_batch(h, *p, order + off, n, h->steplog + (size_t)off * stride);
         off += n;
       }
       if (llk_due(calc_llk, ic, nepoch)) record(h, kAlgLsqml, llk_pass(h));
@@ -1280,21 +1517,25 @@ int ptyb_lsqml(ptyb_handle* h, const ptyb_lsqml_params* p, int32_t nepoch, int32
     end_call(h, "lsqml");
     // The last epoch's steps, for `ptyb_lsqml_steps`.
     h->steps.clear();
+    h->slice_steps.clear();
     if (nepoch > 0) {
-      std::vector<double> log((size_t)h->P * 3);
+      const int stride = h->log_stride;
+      std::vector<double> log((size_t)h->P * stride);
       check(h, cudaMemcpy(log.data(), h->steplog, log.size() * sizeof(double),
                           cudaMemcpyDeviceToHost),
             "steps");
       int b = 0, o = 0;
       for (int n : sizes.back()) {
         for (int i = 0; i < n; ++i) {
+          const double* row = log.data() + (size_t)(o + i) * stride;
           ptyb_lsqml_step st;
           st.batch = b;
           st.frame = last[o + i];
-          st.a_far = log[(size_t)(o + i) * 3];
-          st.a_obj = log[(size_t)(o + i) * 3 + 1];
-          st.a_probe = log[(size_t)(o + i) * 3 + 2];
+          st.a_far = row[0];
+          st.a_obj = row[1];
+          st.a_probe = row[2];
           h->steps.push_back(st);
+          for (int sl = 1; sl < h->nslice; ++sl) h->slice_steps.push_back(row[2 + sl]);
         }
         o += n;
         ++b;
@@ -1312,6 +1553,10 @@ int ptyb_ml(ptyb_handle* h, const ptyb_ml_params* p, int32_t ncycle) {
   }
   if (h->have_offsets) {
     h->err = "ML does not model position offsets in this version";
+    return PTYB_INVALID;
+  }
+  if (h->nslice > 1) {
+    h->err = "ML runs on a single-slice object";
     return PTYB_INVALID;
   }
   return guarded(h, true, [&]() -> int {
@@ -1390,6 +1635,10 @@ int ptyb_get_llk(ptyb_handle* h, ptyb_llk* out) {
 
 int ptyb_forward_intensity(ptyb_handle* h, const int32_t* frames, int32_t n, float* out) {
   if (!h || !frames || !out || n < 0) return PTYB_INVALID;
+  if (h->nslice > 1) {
+    h->err = "forward intensity runs on a single-slice object";
+    return PTYB_INVALID;
+  }
   for (int i = 0; i < n; ++i)
     if (frames[i] < 0 || frames[i] >= h->P) {
       h->err = "frame index out of range";
@@ -1419,6 +1668,10 @@ int ptyb_forward_intensity(ptyb_handle* h, const int32_t* frames, int32_t n, flo
 int ptyb_forward_intensity_noalloc(ptyb_handle* h, const int32_t* frames, int32_t n,
                                    float* out) {
   if (!h || !frames || !out || n < 0) return PTYB_INVALID;
+  if (h->nslice > 1) {
+    h->err = "forward intensity runs on a single-slice object";
+    return PTYB_INVALID;
+  }
   for (int i = 0; i < n; ++i)
     if (frames[i] < 0 || frames[i] >= h->P) {
       h->err = "frame index out of range";
@@ -1460,6 +1713,10 @@ int ptyb_forward_intensity_noalloc(ptyb_handle* h, const int32_t* frames, int32_
 
 int ptyb_set_positions(ptyb_handle* h, const double* offsets, int32_t refine) {
   if (!h) return PTYB_INVALID;
+  if (h->nslice > 1 && offsets) {
+    h->err = "the position model runs on a single-slice object in this version";
+    return PTYB_INVALID;
+  }
   if (offsets)
     for (int i = 0; i < 2 * h->P; ++i)
       if (!std::isfinite(offsets[i])) {
@@ -1508,6 +1765,18 @@ int ptyb_get_object(ptyb_handle* h, double* dst) {
     std::vector<float2> v(n);
     check(h, cudaStreamSynchronize(h->stream), "sync");
     check(h, cudaMemcpy(v.data(), h->object, n * sizeof(float2), cudaMemcpyDeviceToHost), "object");
+    to_c64(v.data(), dst, n);
+    return PTYB_OK;
+  });
+}
+
+int ptyb_get_objects(ptyb_handle* h, double* dst) {
+  if (!h || !dst) return PTYB_INVALID;
+  return guarded(h, false, [&]() -> int {
+    const size_t n = (size_t)h->nslice * h->nobj * h->nyo * h->nxo;
+    std::vector<float2> v(n);
+    check(h, cudaStreamSynchronize(h->stream), "sync");
+    check(h, cudaMemcpy(v.data(), h->object, n * sizeof(float2), cudaMemcpyDeviceToHost), "objects");
     to_c64(v.data(), dst, n);
     return PTYB_OK;
   });

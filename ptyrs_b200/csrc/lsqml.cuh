@@ -64,7 +64,8 @@ __global__ void __launch_bounds__(512) lsqml_dots_kernel(
 __global__ void __launch_bounds__(1024) lsqml_solve_kernel(const double* sums, int nslot,
                                                            double scale, const float* a_far,
                                                            const int* frames, float* a_far_all,
-                                                           double* log, float* scal) {
+                                                           double* log, float* scal,
+                                                           int log_stride) {
   __shared__ double aobj[1024], aprb[1024], sorted[1024];
   __shared__ double frame_sums[1024][2];
   __shared__ double means[2];
@@ -95,9 +96,9 @@ __global__ void __launch_bounds__(1024) lsqml_solve_kernel(const double* sums, i
     aobj[t] = 0.9 * fmax(x0, 0.0) / scale;
     aprb[t] = 0.9 * fmax(x1, 0.0);
     a_far_all[frames[t]] = a_far[t];
-    log[t * 3 + 0] = a_far[t];
-    log[t * 3 + 1] = aobj[t];
-    log[t * 3 + 2] = aprb[t];
+    log[t * log_stride + 0] = a_far[t];
+    log[t * log_stride + 1] = aobj[t];
+    log[t * log_stride + 2] = aprb[t];
   }
   __syncthreads();
   if (t < nslot) {

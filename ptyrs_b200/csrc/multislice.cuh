@@ -1,0 +1,336 @@
+// pty-chi's multislice exit wave and its adjoint on the device (physwkim/ptyrs
+// engine/multislice.rs:87-173 forward, 266-286 back-propagation; gaps are angular spectrum,
+// engine/propagate.rs:505-531), for LSQML with the Poisson or Gaussian cost.
+//
+// One cluster per frame holds the frame's K planes, as the frame kernel does. Forward: the
+// probe times slice 0's window, then per gap an FFT pair with the transfer function between
+// them and the next slice's window (the last also the exit phase q), each incident wave stored
+// for the gathers; then the far-field FFT, the xi solver's first pass and the detector field.
+// Backward: the field, the second xi pass, the residual, the inverse FFT and χ of the last
+// slice, then per gap back through conj(q·O) and the conjugate transfer function.
+#pragma once
+#include "frame.cuh"
+
+namespace ptyb {
+
+struct SliceArgs {
+  FrameArgs f;           // object = slice 0, probe, quad, counts, field, χ out (`out`) …
+  const float2* tf;      // [nslice-1][N][N] transfer functions, unshifted DFT order
+  float2* incident;      // [nslice-1][slot][K][N][N]: the waves entering slices 1.. (natural)
+  float2* chi;           // [nslice][slot][K][N][N]: χ of every slice (natural)
+  int nslice;
+  size_t obj_plane;      // nyo·nxo: slice s's object at object + s·obj_plane
+};
+
+enum SliceMode : int { kSliceForward = 0, kSliceBackward = 1, kSliceLlk = 2 };
+
+// Window of slice s times `v` for every plane's rows of this CTA (shifted layout); the last
+// slice also takes q. `conj_mode` multiplies by conj(q·O) instead.
+template <int N, int C>
+PTYB_D void apply_window(float2* S, const SliceArgs& a, int s, int2 corner, int r, int K,
+                         bool conj_mode) {
+  using F = FrameShape<N, C>;
+  constexpr int H = F::H, T = F::T, L = F::L;
+  const bool last = s + 1 == a.nslice;
+  const float2* obj = a.f.object + (size_t)s * a.obj_plane;
+#pragma unroll 2
+  for (int idx = threadIdx.x; idx < H * N; idx += T) {
+    const int yl = idx / N, jx = idx % N;
+    const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
+    float2 w = obj[(size_t)(corner.x + ny) * a.f.nxo + corner.y + nx];
+    if (last) w = cmul(w, a.f.quad[ny * N + nx]);
+    if (conj_mode) w = cconj(w);
+    for (int m = 0; m < K; ++m) {
+      const int line = m * H + yl;
+      float2& v = S[line * L + (jx ^ swz(line))];
+      v = cmul(v, w);
+    }
+  }
+  __syncthreads();
+}
+
+// The planes through gap s in place: FFT, × tf (or its conjugate) / N², inverse FFT.
+template <int N, int C>
+PTYB_D void through_gap(float2* S, const float2* tf, int K, bool adjoint, const LineTwiddles<N>& ltw,
+                        cg::cluster_group& cluster, int r) {
+  using F = FrameShape<N, C>;
+  constexpr int H = F::H, T = F::T, L = F::L;
+  constexpr float inv_n2 = 1.0f / ((float)N * (float)N);
+  all_lines<N, C, -1>(S, K * H, ltw);
+  transpose<N, C>(S, K, cluster);
+  all_lines<N, C, -1>(S, K * H, ltw);
+#pragma unroll 2
+  for (int idx = threadIdx.x; idx < H * N; idx += T) {
+    const int c = idx % H, ky = idx / H;
+    float2 t = tf[ky * N + r * H + c];
+    if (adjoint) t = cconj(t);
+    t = cscale(t, inv_n2);
+    for (int m = 0; m < K; ++m) {
+      float2& v = S[(m * H + c) * L + (ky ^ swz(m * H + c))];
+      v = cmul(v, t);
+    }
+  }
+  __syncthreads();
+  all_lines<N, C, +1>(S, K * H, ltw);
+  transpose<N, C>(S, K, cluster);
+  all_lines<N, C, +1>(S, K * H, ltw);
+}
+
+// This CTA's rows of every plane to `dst` ([K][N][N] natural layout), or loaded from it.
+template <int N, int C>
+PTYB_D void rows_io(float2* S, float2* dst, int r, int K, bool store) {
+  using F = FrameShape<N, C>;
+  constexpr int H = F::H, T = F::T, L = F::L;
+#pragma unroll 2
+  for (int idx = threadIdx.x; idx < H * N; idx += T) {
+    const int yl = idx / N, jx = idx % N;
+    const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
+    for (int m = 0; m < K; ++m) {
+      const int line = m * H + yl;
+      float2& v = S[line * L + (jx ^ swz(line))];
+      float2* g = dst + ((size_t)m * N + ny) * N + nx;
+      if (store)
+        *g = v;
+      else
+        v = *g;
+    }
+  }
+  __syncthreads();
+}
+
+template <int N, int C, int MODE>
+__global__ void __launch_bounds__(FrameShape<N, C>::T) slice_kernel(SliceArgs sa) {
+  using F = FrameShape<N, C>;
+  constexpr int H = F::H, T = F::T, L = F::L;
+  const FrameArgs& a = sa.f;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int K = a.nprobe;
+  float2* S = reinterpret_cast<float2*>(smem_raw);
+  float2* twb = S + (size_t)K * H * L;
+  double* red = reinterpret_cast<double*>(twb + N);
+  cg::cluster_group cluster = cg::this_cluster();
+  const int r = C > 1 ? (int)cluster.block_rank() : 0;
+  const int slot = blockIdx.x / C;
+  const int f = a.frames[slot];
+  const int2 corner = a.corners[f];
+  const int tid = threadIdx.x;
+  LineTwiddles<N> ltw;
+  ltw.load(a.tw, tid % F::G);
+  const size_t frame_planes = (size_t)K * N * N;
+  const size_t slice_stride = (size_t)a.nslot * frame_planes;  // one slice's [slot][K][N][N]
+  constexpr float inv_n2 = 1.0f / ((float)N * (float)N);
+
+  if (MODE != kSliceBackward) {
+    // Slice 0's exit wave: probe (natural) times the window, in the shifted layout.
+#pragma unroll 2
+    for (int idx = tid; idx < H * N; idx += T) {
+      const int yl = idx / N, jx = idx % N;
+      const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
+      for (int m = 0; m < K; ++m) {
+        const int line = m * H + yl;
+        S[line * L + (jx ^ swz(line))] = a.probe[((size_t)m * N + ny) * N + nx];
+      }
+    }
+    __syncthreads();
+    apply_window<N, C>(S, sa, 0, corner, r, K, false);
+    for (int s = 0; s + 1 < sa.nslice; ++s) {
+      through_gap<N, C>(S, sa.tf + (size_t)s * N * N, K, false, ltw, cluster, r);
+      if (MODE == kSliceForward)
+        rows_io<N, C>(S, sa.incident + s * slice_stride + slot * frame_planes, r, K, true);
+      apply_window<N, C>(S, sa, s + 1, corner, r, K, false);
+    }
+    all_lines<N, C, -1>(S, K * H, ltw);
+    transpose<N, C>(S, K, cluster);
+    all_lines<N, C, -1>(S, K * H, ltw);
+  } else {
+    const float2* src = a.field + ((size_t)slot * C + r) * K * H * N;
+#pragma unroll 8
+    for (int idx = tid; idx < K * H * N; idx += T) {
+      const int line = idx / N, e = idx % N;
+      S[line * L + (e ^ swz(line))] = src[idx];
+    }
+    __syncthreads();
+  }
+
+  // Detector plane (column strips): xi pass, LLK, projection, as the frame kernel.
+  constexpr int kPix = H * N / T;
+  const float* iobs = a.iobs + (size_t)f * N * N;
+  float yo_r[kPix], ic_r[kPix];
+#pragma unroll
+  for (int i = 0; i < kPix; ++i) {
+    const int idx = tid + i * T;
+    const int c = idx % H, ky = idx / H;
+    yo_r[i] = iobs[ky * N + r * H + c];
+    float ic = 0.f;
+    for (int m = 0; m < K; ++m) ic += cnorm2(S[(m * H + c) * L + (ky ^ swz(m * H + c))]);
+    ic_r[i] = ic * inv_n2;
+  }
+  if (MODE == kSliceLlk) {
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int i = 0; i < kPix; ++i) {
+      const float yo = yo_r[i], ic = ic_r[i];
+      if (yo < 0.f) continue;
+      acc[0] += yo > 0.f ? (double)ic - yo + (double)yo * log((double)yo / ic) : (double)ic;
+      const double dg = (double)yo - ic;
+      acc[1] += dg * dg / ((double)yo + 1.0);
+      const double de = sqrt((double)yo) - sqrt((double)ic);
+      acc[2] += 4.0 * de * de;
+      acc[3] += ic;
+    }
+    block_sum<T>(acc, 4, red);
+    csync<C>(cluster);
+    if (r == 0 && tid == 0) {
+      for (int k = 0; k < 4; ++k) {
+        double s = 0.0;
+        for (int q = 0; q < C; ++q) s += (C > 1 ? cluster.map_shared_rank(red, q) : red)[k];
+        a.llk[(size_t)slot * 4 + k] = s;
+      }
+    }
+    csync<C>(cluster);
+    return;
+  }
+  float afar = 0.5f;
+  if (a.cost == kCostPoisson) {
+    const double prev = MODE == kSliceForward
+                            ? batch_mean(a.a_prev, a.frames, a.a_prev_by_frame, a.nslot, red + 7)
+                            : batch_mean(a.a_mid, a.frames, 0, a.nslot, red + 7);
+    double num = 0.0, den = 0.0;
+#pragma unroll
+    for (int i = 0; i < kPix; ++i) {
+      const float yo = yo_r[i];
+      if (yo < 0.f) continue;
+      const double yp = (double)ic_r[i], yt = yo;
+      const double xi = 1.0 - yt / (yp + 1e-5);
+      num += xi * (yp - yt / (1.0 - prev * xi));
+      den += xi * xi * yp;
+    }
+    cluster_sum2<N, C>(num, den, red, cluster);
+    const double ratio = den > 0.0 ? num / den : 0.0;
+    afar = (float)fmin(fmax(0.5 * prev + 0.5 * ratio, 0.0), 1.0);
+    if (r == 0 && tid == 0) a.a_out[slot] = afar;
+  } else if (MODE == kSliceBackward && r == 0 && tid == 0) {
+    a.a_out[slot] = afar;
+  }
+  if (MODE == kSliceForward) {
+    float2* dst = a.field + ((size_t)slot * C + r) * K * H * N;
+#pragma unroll 8
+    for (int idx = tid; idx < K * H * N; idx += T) {
+      const int line = idx / N, e = idx % N;
+      dst[idx] = S[line * L + (e ^ swz(line))];
+    }
+    return;
+  }
+#pragma unroll
+  for (int i = 0; i < kPix; ++i) {
+    const int idx = tid + i * T;
+    const int c = idx % H, ky = idx / H;
+    const float yo = yo_r[i], ic = ic_r[i];
+    float cres = 0.f;
+    if (yo >= 0.f)
+      cres = a.cost == kCostPoisson ? 1.f - yo / (ic + 1e-6f)
+                                    : 2.f * (1.f - sqrtf(fmaxf(yo, 0.f)) / (sqrtf(ic) + 1e-9f));
+    const float fac = (1.f - afar * cres) * inv_n2;
+    for (int m = 0; m < K; ++m) {
+      float2& v = S[(m * H + c) * L + (ky ^ swz(m * H + c))];
+      v = cscale(v, fac);
+    }
+  }
+  __syncthreads();
+  all_lines<N, C, +1>(S, K * H, ltw);
+  transpose<N, C>(S, K, cluster);
+  all_lines<N, C, +1>(S, K * H, ltw);
+  // χ of the last slice: ψ' − q·O_last·in_last.
+  const int last = sa.nslice - 1;
+  const float2* in_last = last == 0 ? nullptr : sa.incident + (last - 1) * slice_stride + slot * frame_planes;
+  const float2* obj_last = a.object + (size_t)last * sa.obj_plane;
+#pragma unroll 2
+  for (int idx = tid; idx < H * N; idx += T) {
+    const int yl = idx / N, jx = idx % N;
+    const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
+    const float2 oq =
+        cmul(obj_last[(size_t)(corner.x + ny) * a.nxo + corner.y + nx], a.quad[ny * N + nx]);
+    for (int m = 0; m < K; ++m) {
+      const int line = m * H + yl;
+      const size_t pi = ((size_t)m * N + ny) * N + nx;
+      const float2 in = in_last ? in_last[pi] : a.probe[pi];
+      float2& v = S[line * L + (jx ^ swz(line))];
+      v = csub(v, cmul(in, oq));
+    }
+  }
+  __syncthreads();
+  rows_io<N, C>(S, sa.chi + last * slice_stride + slot * frame_planes, r, K, true);
+  for (int s = last - 1; s >= 0; --s) {
+    apply_window<N, C>(S, sa, s + 1, corner, r, K, true);
+    through_gap<N, C>(S, sa.tf + (size_t)s * N * N, K, true, ltw, cluster, r);
+    rows_io<N, C>(S, sa.chi + s * slice_stride + slot * frame_planes, r, K, true);
+  }
+}
+
+// Per slot, slice s ≥ 1's Eq. 23b sums (engine/lsqml.rs:327-347): with dop = q_s·dO_s·in_s,
+// num = Σ Re(conj(dop)·χ_s), den = Σ |dop|² over modes and pixels; sums [slot][2] in double.
+__global__ void __launch_bounds__(512) slice_dots_kernel(const float2* d_obj,
+                                                        const float2* incident,
+                                                        const float2* quad, const float2* chi,
+                                                        const int* frames, const int2* corners,
+                                                        int nxo, int K, int N, double* sums) {
+  __shared__ double sh[16];
+  const int slot = blockIdx.x;
+  const int2 c = corners[frames[slot]];
+  const size_t plane = (size_t)N * N;
+  float s0 = 0.f, s1 = 0.f;
+  for (int idx = threadIdx.x; idx < K * N * N; idx += 512) {
+    const int m = idx / (N * N), pix = idx % (N * N);
+    const int yy = pix / N, xx = pix % N;
+    float2 u = cmul(incident[((size_t)slot * K + m) * plane + pix],
+                    d_obj[(size_t)(c.x + yy) * nxo + c.y + xx]);
+    if (quad) u = cmul(u, quad[pix]);
+    const float2 x = chi[((size_t)slot * K + m) * plane + pix];
+    s0 += u.x * x.x + u.y * x.y;
+    s1 += cnorm2(u);
+  }
+  auto bsum = [&](float v) {
+    double d = warp_sum((double)v);
+    if (threadIdx.x % 32 == 0) sh[threadIdx.x / 32] = d;
+    __syncthreads();
+    double t = 0.0;
+    for (int w = 0; w < 16; ++w) t += sh[w];
+    __syncthreads();
+    return t;
+  };
+  const double num = bsum(s0), den = bsum(s1);
+  if (threadIdx.x == 0) {
+    sums[(size_t)slot * 2] = num;
+    sums[(size_t)slot * 2 + 1] = den;
+  }
+}
+
+// One block: a_obj_s = max(0.5·num/den·0.9/scale, 0) per frame, their trimmed mean into
+// *step (engine/lsqml.rs:327-347, 392-398).
+__global__ void __launch_bounds__(1024) slice_solve_kernel(const double* sums, int nslot,
+                                                           double scale, double* log,
+                                                           int log_stride, float* step) {
+  __shared__ double a[1024], sorted[1024];
+  const int t = threadIdx.x;
+  if (t < nslot) {
+    const double num = sums[t * 2], den = sums[t * 2 + 1];
+    a[t] = fmax(0.5 * num / den * 0.9 / scale, 0.0);
+    log[(size_t)t * log_stride] = a[t];
+  }
+  __syncthreads();
+  if (t < nslot) {
+    int rank = 0;
+    const double v = a[t];
+    for (int j = 0; j < nslot; ++j) rank += (a[j] < v) || (a[j] == v && j < t);
+    sorted[rank] = v;
+  }
+  __syncthreads();
+  if (t == 0) {
+    const int k = (int)ceil(nslot * 0.1 / 2.0 - 0.5);
+    double s = 0.0;
+    for (int i = k; i < nslot - k; ++i) s += sorted[i];
+    *step = (float)(s / (nslot - 2 * k));
+  }
+}
+
+}  // namespace ptyb

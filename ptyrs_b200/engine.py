@@ -56,22 +56,40 @@ class Scan:
 
 class GpuPtycho:
     """The GPU reconstruction state of a scan on CUDA device `device`: `object` complex
-    `[1, nyo, nxo]`, `probe` complex `[nprobe, ny, nx]`."""
+    `[1, nyo, nxo]`, `probe` complex `[nprobe, ny, nx]`.
 
-    def __init__(self, scan, obj, probe, device=0, stack_size=0, cluster=0):
+    With `gaps` (the nslice - 1 slice spacings in metres, reference `Optics::with_slices`),
+    `obj` is pty-chi's multislice object `[nslice, nyo, nxo]` in the order the wave crosses the
+    slices; `object()` / `set_object()` then read and replace slice 0 and `objects()` returns
+    every slice, as the reference's `GpuPtycho::with_slices` does."""
+
+    def __init__(self, scan, obj, probe, device=0, stack_size=0, cluster=0, gaps=None):
         self._lib = _lib.load()
         obj = np.ascontiguousarray(obj, dtype=np.complex128)
         probe = np.ascontiguousarray(probe, dtype=np.complex128)
         if obj.ndim != 3 or probe.ndim != 3:
             raise ValueError("object must be [nobj, nyo, nxo] and probe [nprobe, ny, nx]")
-        self._obj_shape, self._probe_shape = obj.shape, probe.shape
+        self._nslice = 1 if gaps is None else obj.shape[0]
+        if gaps is not None and len(gaps) != self._nslice - 1:
+            raise ValueError(f"{obj.shape[0]} slices need {obj.shape[0] - 1} gaps, got {len(gaps)}")
+        self._obj_shape = (1,) + obj.shape[1:] if gaps is not None else obj.shape
+        self._probe_shape = probe.shape
         self._nframe = scan.counts.shape[0]
         st = scan._struct()
         opts = _lib.Options(device, stack_size, cluster)
         h = ctypes.c_void_p()
-        rc = self._lib.ptyb_create(ctypes.byref(st), _dptr(obj.view(np.float64)), obj.shape[0],
-                                   obj.shape[1], obj.shape[2], _dptr(probe.view(np.float64)),
-                                   probe.shape[0], ctypes.byref(opts), ctypes.byref(h))
+        if gaps is None:
+            rc = self._lib.ptyb_create(ctypes.byref(st), _dptr(obj.view(np.float64)),
+                                       obj.shape[0], obj.shape[1], obj.shape[2],
+                                       _dptr(probe.view(np.float64)), probe.shape[0],
+                                       ctypes.byref(opts), ctypes.byref(h))
+        else:
+            g = np.ascontiguousarray(gaps, dtype=np.float64).reshape(-1)
+            rc = self._lib.ptyb_create_slices(ctypes.byref(st), _dptr(obj.view(np.float64)),
+                                              obj.shape[0], _dptr(g) if len(g) else None,
+                                              obj.shape[1], obj.shape[2],
+                                              _dptr(probe.view(np.float64)), probe.shape[0],
+                                              ctypes.byref(opts), ctypes.byref(h))
         if rc != 0:
             raise PtybError(STATUS.get(rc, rc), self._lib.ptyb_last_error(None).decode())
         self._h = h
@@ -150,6 +168,16 @@ class GpuPtycho:
         self._check(self._lib.ptyb_get_object(self._h, _dptr(out.view(np.float64))))
         return out
 
+    def nslice(self):
+        """The handle's object slices."""
+        return self._lib.ptyb_nslice(self._h)
+
+    def objects(self):
+        """Every object slice `[nslice, nyo, nxo]` (reference `GpuPtycho::objects`)."""
+        out = np.empty((self._nslice,) + tuple(self._obj_shape[1:]), np.complex128)
+        self._check(self._lib.ptyb_get_objects(self._h, _dptr(out.view(np.float64))))
+        return out
+
     def probe(self):
         out = np.empty(self._probe_shape, np.complex128)
         self._check(self._lib.ptyb_get_probe(self._h, _dptr(out.view(np.float64))))
@@ -203,15 +231,25 @@ class GpuPtycho:
         n = self._lib.ptyb_lsqml_steps_len(self._h)
         buf = (_lib.LsqmlStep * max(n, 1))()
         self._check(self._lib.ptyb_lsqml_steps(self._h, buf, n))
+        extra = np.zeros((n, self._nslice - 1))
+        if self._nslice > 1 and n:
+            self._check(self._lib.ptyb_lsqml_slice_steps(self._h, _dptr(extra)))
         steps = []
-        for s in buf[:n]:
+        for i, s in enumerate(buf[:n]):
             if not steps or steps[-1]["batch"] != s.batch:
-                steps.append(dict(batch=s.batch, frames=[], a_far=[], a_obj=[], a_probe=[]))
+                steps.append(dict(batch=s.batch, frames=[], a_far=[], a_probe=[],
+                                  a_obj=[] if self._nslice == 1 else
+                                  [[] for _ in range(self._nslice)]))
             st = steps[-1]
             st["frames"].append(s.frame)
             st["a_far"].append(s.a_far)
-            st["a_obj"].append(s.a_obj)
             st["a_probe"].append(s.a_probe)
+            if self._nslice == 1:
+                st["a_obj"].append(s.a_obj)
+            else:
+                st["a_obj"][0].append(s.a_obj)
+                for k in range(1, self._nslice):
+                    st["a_obj"][k].append(extra[i, k - 1])
         return steps
 
     def synchronize(self):

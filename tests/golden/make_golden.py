@@ -6,7 +6,9 @@ Sources (physwkim/ptyrs, `ptyrs/tests/engine/data/`): the rPIE near-field set
 `refs/f64/rpie_near.py`) and the LSQML near-field set `lsqml_near_*_f64.txt` (pty-chi LSQML in
 float64, `refs/f64/lsqml_near.py`), and the PyNX set `pynx_near_*_f64.txt` (PyNX `cpu_operator` promoted
 to float64, `refs/f64/pynx_near.py`) whose ML run pins the Poisson conjugate gradient, and `lsqml_near_pos_*_f64.txt` (one pty-chi
-LSQML step refining the positions under PATCH, `refs/f64/lsqml_near_pos.py`). Each text table becomes one float64 array of the same
+LSQML step refining the positions under PATCH, `refs/f64/lsqml_near_pos.py`) and
+`lsqml_multislice_*_f64.txt` (pty-chi LSQML through three slices with angular-spectrum, Fresnel
+and far-field exits, `refs/f64/lsqml_multislice.py`). Each text table becomes one float64 array of the same
 rows and columns under its stem in `rpie_near.npz`, `lsqml_near.npz` and `pynx_near.npz`.
 
     python tests/golden/make_golden.py [REFERENCE_ROOT]
@@ -25,6 +27,9 @@ GROUPS = {
     "pynx_near": ["case", "corners", "counts", "obj", "probe", "runs", "llk", "run_obj",
                   "run_probe"],
     "lsqml_near_pos": ["start", "steps", "offsets", "obj", "probe"],
+    "lsqml_multislice": ["cases", "corners", "counts", "obj", "probe", "icalc", "llk",
+                         "step_steps", "step_obj", "step_probe", "epochs_steps", "epochs_obj",
+                         "epochs_probe"],
 }
 
 

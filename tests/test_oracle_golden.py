@@ -215,3 +215,97 @@ def test_lsqml_step_with_positions_matches_ptychi():
         assert max_rel(change(pr, probe), of_run(p["probe"], k, 4)) < 1e-12
         assert max_rel(run.offsets - d0, want - d0) < 1e-11
     assert checked == 2
+
+
+NSLICE = 3
+
+
+def multislice_state():
+    """engine_lsqml_multislice.rs:63-145: three slices with unequal angular-spectrum gaps; case
+    kind 0 is the far field of a geometry (its q on the last slice), 1 angular spectrum, 2 a
+    Fresnel transform."""
+    g = golden("lsqml_multislice")
+    corners = g["corners"]
+    ys = corners[:, 1] - (OBJ[0] - SHAPE[0]) // 2
+    xs = corners[:, 2] - (OBJ[1] - SHAPE[1]) // 2
+    addr = AddrTable(ys, xs, [1.0, 1.0], SHAPE, OBJ, NPROBE, 1)
+    objs = [stack((1,) + OBJ, g["obj"][g["obj"][:, 0] == s], 3) for s in range(NSLICE)]
+    probe = stack((NPROBE,) + SHAPE, g["probe"], 3)
+    cases = []
+    for c in g["cases"]:
+        if c[4] == 0.0:
+            lz = c[1] * c[3]
+            optics = ops.Optics.far_field(c[1], c[3], lz / (SHAPE[0] * c[2]), list(SHAPE))
+            pixel = optics.pixel
+        else:
+            pixel = [c[2], c[2]]
+            optics = ops.Optics.free_space(ops.Wavefield(SHAPE, c[1], pixel, c[3]))
+        gaps = [ops.Wavefield(SHAPE, c[1], pixel, d) for d in c[7:]]
+        optics = optics.with_slices(gaps)
+        assert abs(optics.intensity_scale() - c[5]) <= 1e-15 * abs(c[5])
+        rows = g["counts"][g["counts"][:, 0] == c[0]]
+        obs = Observed(counts_from_f64(rows[:, 2:].reshape(len(corners), *SHAPE)))
+        cases.append((optics, obs, c[6]))
+    return g, addr, objs, probe, cases
+
+
+def multislice_changes(objs, objs0):
+    return np.concatenate([change(o, o0) for o, o0 in zip(objs, objs0)])
+
+
+def of_case(rows, k):
+    r = rows[rows[:, 0] == k]
+    return np.stack([r[:, 4], r[:, 5]], axis=1).ravel()
+
+
+def assert_ms_step(st, rows, col):
+    assert st["frames"] == [int(v) for v in rows[:, col]]
+    assert max_rel(st["a_far"], rows[:, col + 1]) < 1e-13
+    for i in range(NSLICE):
+        assert max_rel(st["a_obj"][i], rows[:, col + 2 + i]) < 1e-12
+    assert max_rel(st["a_probe"], rows[:, col + 2 + NSLICE]) < 1e-12
+
+
+def test_multislice_forward_and_step_match_ptychi():
+    """engine_lsqml_multislice.rs:163-181 and 343-372: pty-chi's y_pred through three slices,
+    and one LSQML step on frames 0..8 with the joint slice-0 step sizes."""
+    g, addr, objs, probe, cases = multislice_state()
+    from oracle.lsqml import SliceWaves
+    for r in g["icalc"]:
+        optics, obs, _ = cases[int(r[0])]
+        v = addr.frame_views(int(r[1]))
+        w = SliceWaves(optics, v, objs, probe[v["probe"].astype(np.int64)])
+        got = (np.abs(optics.exit_forward(w.psi)) ** 2).sum(axis=0)
+        assert max_rel(got, fftshift2(r[2:].reshape(SHAPE))) < 1e-14
+    views = addr.views[:8 * addr.nmode]
+    for k, (optics, obs, _) in enumerate(cases):
+        run = Lsqml(8, "poisson", 0)
+        run.preconditioner = ops.illumination(addr.views, objs[0].shape, probe)
+        o, pr, st = run.step(views, obs, optics, objs, probe)
+        assert_ms_step(st, g["step_steps"][g["step_steps"][:, 0] == k], 1)
+        assert max_rel(multislice_changes(o, objs), of_case(g["step_obj"], k)) < 1e-12
+        assert max_rel(change(pr, probe), of_case(g["step_probe"], k)) < 1e-12
+
+
+def test_multislice_epochs_match_ptychi():
+    """engine_lsqml_multislice.rs:481-540: the epochs (seed 7), every step and the LLK trace."""
+    g, addr, objs0, probe0, cases = multislice_state()
+    steps, trace = g["epochs_steps"], g["llk"]
+    for k, (optics, obs, truth) in enumerate(cases):
+        objs, probe = list(objs0), probe0.copy()
+        run = Lsqml(8, "poisson", 7)
+        want = trace[trace[:, 0] == k]
+        rows = steps[steps[:, 0] == k]
+        llks = [run.llk(addr, obs, optics, objs, probe).poisson]
+        nxt = 0
+        for e in range(len(want) - 1):
+            objs, probe, sts = run.epoch(addr, obs, optics, objs, probe)
+            for st in sts:
+                w = rows[nxt:nxt + len(st["frames"])]
+                nxt += len(st["frames"])
+                assert_ms_step(st, w, 2)
+            llks.append(run.llk(addr, obs, optics, objs, probe).poisson)
+        assert nxt == len(rows)
+        assert max_rel(llks, want[:, 2]) < 1e-12
+        assert max_rel(multislice_changes(objs, objs0), of_case(g["epochs_obj"], k)) < 1e-12
+        assert max_rel(change(probe, probe0), of_case(g["epochs_probe"], k)) < 1e-12
