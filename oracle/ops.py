@@ -433,6 +433,29 @@ def batch_position_step(d, frames, delta):
         d[:, axis] += np.clip(dx[:, axis], -limit, limit)
 
 
+def position_step(d, sums):
+    """The position step of AP, DM and ML (engine/features.rs:1028-1047): per axis, with `max`
+    the largest `den` over every frame, `step = clip(0.3·num / (den + max), ±0.1)` (0 where the
+    denominator is not positive), then `d += step − mean(step)` over every frame. `sums`
+    `[P][2][2]` holds each frame's `[num, den]`; `d` `[P, 2]` is updated in place."""
+    n = len(d)
+    for axis in range(2):
+        mx = 0.0
+        for s in sums:
+            mx = max(mx, float(s[1][axis]))
+        step = []
+        for s in sums:
+            den = float(s[1][axis]) + mx
+            step.append(min(max(POSITION_STEP * float(s[0][axis]) / den, -POSITION_LIMIT),
+                            POSITION_LIMIT) if den > 0.0 else 0.0)
+        total = 0.0
+        for v in step:
+            total += v
+        mean = total / n
+        for f in range(n):
+            d[f, axis] += step[f] - mean
+
+
 def illumination(views, obj_shape, probe):
     """pty-chi illumination map `Σ|P[probe_k]|²` on each window (engine/lsqml.rs:374-388)."""
     ny, nx = probe.shape[-2:]

@@ -2,12 +2,106 @@
 infrastructure only).
 
 Follows physwkim/ptyrs `ptyrs/src/engine/ptycho.rs` (`Ptycho`) for the far-field and
-planar near-field optics of a single object slice, without position features.
+planar near-field optics of a single object slice; ML also under `Features::position`'s
+sub-pixel offsets with Patch sampling (`engine/features.rs`, `Shifted`).
 """
 import numpy as np
 
 from . import ops
 from .base import AddrTable, Observed, fftshift2, pynx_preprocess, random_batches
+
+
+class Shifted:
+    """`Features::position`'s model of `probe` on `views` under Patch sampling
+    (engine/features.rs:558-1025): every view's wave `W = T_d(q·P)`, its probe mode with the
+    exit phase moved by its frame's offset `d` on the periodic grid, takes the place of `q·P`,
+    and the window is the integer one. Planes are kept in the natural layout here; the
+    reference's shifted layout commutes with the move."""
+
+    def __init__(self, views, probe, quad, offsets):
+        self.views = views
+        self.quad = np.ones(probe.shape[-2:]) if quad is None else quad
+        self.offsets = np.asarray(offsets, np.float64)
+        self.probe = probe
+        self.pidx = views["probe"].astype(np.int64)
+        self.frames = views["frame"].astype(np.int64)
+        moved = {}
+        waves = np.empty((len(views),) + probe.shape[-2:], np.complex128)
+        for k, (p, f) in enumerate(zip(self.pidx, self.frames)):
+            if f not in moved:
+                moved[f] = self.quad * ops.move_planes(probe, self.quad, self.offsets[f])
+            waves[k] = moved[f][p]
+        self.waves = waves
+
+    def _windows(self, obj):
+        ny, nx = self.waves.shape[-2:]
+        return ops.windows(self.views, obj, ny, nx)
+
+    def to_psi(self, obj):
+        """`psi[k] = W[k]·O[win_k]` in the shifted exit layout (features.rs:803-818)."""
+        return fftshift2(self.waves * self._windows(obj))
+
+    def derivatives(self, obj, axis):
+        """`O[win]·∂W/∂d[axis]` per view, shifted layout (features.rs:964-990)."""
+        win = self._windows(obj)
+        out = np.empty_like(self.waves)
+        cache = {}
+        for k, (p, f) in enumerate(zip(self.pidx, self.frames)):
+            if f not in cache:
+                cache[f] = self.quad * ops.move_planes(self.probe, self.quad, self.offsets[f],
+                                                       axes=(axis,))
+            out[k] = win[k] * cache[f][p]
+        return fftshift2(out)
+
+    def accumulate_obj(self, obj_shape, psi):
+        """`num += psi·conj(W)`, `norm += |W|²` on each window in view order
+        (features.rs:855-890)."""
+        ny, nx = self.waves.shape[-2:]
+        num = np.zeros(obj_shape, np.complex128)
+        norm = np.zeros(obj_shape, np.float64)
+        w = fftshift2(psi)
+        for k, v in enumerate(self.views):
+            oy, ox, o = int(v["oy"]), int(v["ox"]), int(v["obj"])
+            num[o, oy:oy + ny, ox:ox + nx] += w[k] * np.conj(self.waves[k])
+            norm[o, oy:oy + ny, ox:ox + nx] += np.abs(self.waves[k]) ** 2
+        return num, norm
+
+    def accumulate_probe(self, obj, probe_shape, psi):
+        """Through the move's adjoint (features.rs:897-957): per probe mode
+        `num = conj(q)·Σ_f IDFT(DFT(Y_f)·conj(exp(−2πi f·d_f)))`, `Y_f = Σ conj(O[win])·psi`
+        over frame f's views of that mode, the spectra summed frame by frame;
+        `norm = Σ|O[win]|²`."""
+        w = fftshift2(psi)
+        win = self._windows(obj)
+        spectrum = np.zeros(probe_shape, np.complex128)
+        norm = np.zeros(probe_shape, np.float64)
+        k = 0
+        nv = len(self.views)
+        while k < nv:
+            f = self.frames[k]
+            y = np.zeros(probe_shape, np.complex128)
+            while k < nv and self.frames[k] == f:
+                p = self.pidx[k]
+                y[p] += np.conj(win[k]) * w[k]
+                norm[p] += np.abs(win[k]) ** 2
+                k += 1
+            e, _ = ops.translation(probe_shape[-2:], self.offsets[f])
+            spectrum += ops.fft2(y) * np.conj(e)
+        return np.conj(self.quad) * ops.ifft2(spectrum), norm
+
+    def position_sums(self, obj, psi, nframe):
+        """Per frame `[num, den]` (features.rs:992-1025): `num[a] = Re Σ conj(x − O·W)·∂psi_a`,
+        `den[a] = Σ|∂psi_a|²` over the frame's views and pixels, `x` the new exit waves."""
+        c = psi - self.to_psi(obj)
+        sums = np.zeros((nframe, 2, 2))
+        for axis in range(2):
+            dpsi = self.derivatives(obj, axis)
+            num = (np.conj(c) * dpsi).real.sum(axis=(1, 2))
+            den = (np.abs(dpsi) ** 2).sum(axis=(1, 2))
+            for k, f in enumerate(self.frames):
+                sums[f, 0, axis] += num[k]
+                sums[f, 1, axis] += den[k]
+        return sums
 
 
 def llk_due(calc_llk, ic, ncycle):
@@ -36,9 +130,27 @@ class Ptycho:
         self.probe = np.array(probe, np.complex128)
         self.cycle = 0
         self.history = []
+        self.offsets = None
+        self.refine = False
+
+    def set_positions(self, offsets, refine=False):
+        """`Features::position` with Patch sampling: per-frame offsets `[P, 2]` (dy, dx) in
+        object pixels, refined by ML when `refine` (engine/features.rs:20-130)."""
+        self.offsets = None if offsets is None else np.array(offsets, np.float64)
+        self.refine = bool(refine) and offsets is not None
+
+    def shifted(self, probe=None):
+        """`Ptycho::shifted` (engine/ptycho.rs:373-386): the position model of every view, or
+        None without offsets."""
+        if self.offsets is None:
+            return None
+        return Shifted(self.addr.views, self.probe if probe is None else probe,
+                       self.optics.quad, self.offsets)
 
     # exit waves -------------------------------------------------------------------------
     def calc_psi(self, views=None, obj=None, probe=None):
+        if views is None and obj is None and probe is None and self.offsets is not None:
+            return self.shifted().to_psi(self.object)
         views = self.addr.views if views is None else views
         obj = self.object if obj is None else obj
         probe = self.probe if probe is None else probe
@@ -65,6 +177,13 @@ class Ptycho:
         511-513)."""
         g = self.grad_psi()
         views, q = self.addr.views, self.optics.quad
+        s = self.shifted()
+        if s is not None:
+            go = (s.accumulate_obj(self.object.shape, g)[0] if obj
+                  else np.zeros_like(self.object))
+            gp = (s.accumulate_probe(self.object, self.probe.shape, g)[0] if probe
+                  else np.zeros_like(self.probe))
+            return go, gp
         go = (ops.accumulate_obj(views, self.object.shape, self.probe, q, g)[0] if obj
               else np.zeros_like(self.object))
         gp = (ops.accumulate_probe(views, self.object, self.probe.shape, q, g)[0] if probe
@@ -72,12 +191,17 @@ class Ptycho:
         return go, gp
 
     def cg_gamma(self, d_obj, d_probe):
-        """engine/ptycho.rs:517-545 without position features."""
+        """engine/ptycho.rs:517-545, under the position model when offsets are set."""
         views, q = self.addr.views, self.optics.quad
         po = self.calc_psi()
-        a = (ops.obj_probe_to_psi(views, d_obj, self.probe, q)
-             + ops.obj_probe_to_psi(views, self.object, d_probe, q))
-        b = ops.obj_probe_to_psi(views, d_obj, d_probe, q)
+        if self.offsets is not None:
+            sp, sd = self.shifted(), self.shifted(d_probe)
+            a = sp.to_psi(d_obj) + sd.to_psi(self.object)
+            b = sd.to_psi(d_obj)
+        else:
+            a = (ops.obj_probe_to_psi(views, d_obj, self.probe, q)
+                 + ops.obj_probe_to_psi(views, self.object, d_probe, q))
+            b = ops.obj_probe_to_psi(views, d_obj, d_probe, q)
         po, a, b = (self.optics.exit_forward(x) for x in (po, a, b))
         return ops.cg_poisson_gamma(self.obs, slice(0, self.addr.nframe), self.addr.nmode,
                                     po, a, b)
@@ -92,15 +216,26 @@ class Ptycho:
         self.probe = self.probe * fp
         self.object = self.object * fo
 
+    def projected_position_sums(self, s):
+        """`Shifted::position_sums` of the magnitude projection of the current estimate's
+        exit waves (engine/ptycho.rs:470-480)."""
+        nframe, nmode = self.addr.nframe, self.addr.nmode
+        psi = self.optics.exit_forward(s.to_psi(self.object))
+        psi = ops.apply_amplitude(self.obs, slice(0, nframe), nmode, psi)
+        psi = self.optics.exit_adjoint(psi)
+        return s.position_sums(self.object, psi, nframe)
+
     def ml(self, ncycle, update_object=True, update_probe=False, calc_llk=0,
            zero_phase_ramp=True):
-        """PyNX ML Poisson CG (engine/ptycho.rs:775-842)."""
+        """PyNX ML Poisson CG (engine/ptycho.rs:775-842); refined offsets take AP's and DM's
+        position step from the estimate each cycle starts from, after the update."""
         self.scale_obj_probe()
         last = None
         d_obj = np.zeros_like(self.object)
         d_probe = np.zeros_like(self.probe)
         for ic in range(ncycle):
             l = self.llk() if llk_due(calc_llk, ic, ncycle) else None
+            sums = self.projected_position_sums(self.shifted()) if self.refine else None
             go, gp = self.grads(update_object, update_probe)
             if last is None:
                 beta = 0.0
@@ -123,6 +258,8 @@ class Ptycho:
             else:
                 d_obj, d_probe = -go, -gp
             last = (go, gp)
+            if sums is not None:
+                ops.position_step(self.offsets, sums)
             if l is not None:
                 self.record("ml", l)
             self.cycle += 1

@@ -151,6 +151,11 @@ struct ptyb_handle {
   float2* chi_slices = nullptr;  // [nslice][slots][K][N][N]
   float2* ones = nullptr;        // [N][N]
   double* slice_sums = nullptr;  // [slots][2]
+  // ML under the position model: the moved probe direction per slot, each frame's position
+  // sums (num_y, num_x, den_y, den_x).
+  float2* wave2 = nullptr;       // [wave2_slots][K][N][N]
+  int wave2_slots = 0;
+  double* ml_pos_sums = nullptr; // [P][4]
   double* partials = nullptr;    // [kPartialBlocks][2]
   std::vector<Buf> bufs;
   // Per-kernel device timing (CUDA events on the engine's stream), when enabled.
@@ -227,14 +232,14 @@ enum Kind : int {
   kKFrameRpie = 0, kKFrameLsqml, kKFrameMl, kKFrameLlk, kKFrameStore, kKFrameFromStore,
   kKObjRpie, kKObjOverlap, kKObjLsqml, kKObjMl, kKIllum, kKProbePartial, kKProbeFinal,
   kKAfar, kKDots, kKSolve, kKAxpy, kKMax, kKCounts, kKMisc, kKGamma, kKArraySums, kKMove,
-  kKPositionSums, kKSliceForward, kKSliceBackward, kKSliceLlk, kNumKinds
+  kKPositionSums, kKSliceForward, kKSliceBackward, kKSliceLlk, kKFrameProject, kNumKinds
 };
 const char* const kKindNames[kNumKinds] = {
     "frame_rpie", "frame_lsqml", "frame_ml_grad", "frame_llk", "frame_store",
     "frame_from_store", "object_rpie", "object_overlap", "object_lsqml", "object_ml",
     "illumination", "probe_partial", "probe_finalize", "lsqml_afar", "lsqml_dots",
     "lsqml_solve", "axpy", "max", "counts", "misc", "ml_gamma", "array_sums", "move",
-    "position_sums", "slice_forward", "slice_backward", "slice_llk"};
+    "position_sums", "slice_forward", "slice_backward", "slice_llk", "frame_project"};
 
 cudaEvent_t take_event(ptyb_handle* h) {
   if (!h->event_pool.empty()) {
@@ -357,6 +362,7 @@ cudaError_t launch_frame(ptyb_handle* h, const FrameArgs& a, int nslot) {
                        : MODE == kMlGrad ? kKFrameMl
                        : MODE == kLlk ? kKFrameLlk
                        : MODE == kStore ? kKFrameStore
+                       : MODE == kProject ? kKFrameProject
                                         : kKFrameFromStore;
   cudaError_t e = cudaSuccess;
   timed(h, kind, [&] { e = launch_frame_raw<MODE>(h, a, nslot); });
@@ -1020,20 +1026,47 @@ void ml_gradients(ptyb_handle* h, bool uo, bool up) {
   check(h, cudaMemsetAsync(h->g_probe_c, 0, np * sizeof(float2), h->stream), "memset");
   if (!uo && !up) return;
   const int stack = std::min(h->P, h->stack);
+  const int pstride = h->K * h->N * h->N;
   for (int s0 = 0; s0 < h->P; s0 += stack) {
     const int n = std::min(stack, h->P - s0);
     const int* frames = h->iota + s0;
     FrameArgs a = frame_args(h, frames);
+    if (h->have_offsets) {
+      // each frame's moved probe W = T_d(q·P) in place of q·P (engine/ptycho.rs:373-450)
+      check(h, launch_move<kMoveProbe>(h, move_args(h, frames, h->wave), n), "probe move");
+      ++h->launches;
+      a.probe = h->wave;
+      a.probe_stride = pstride;
+    }
     check(h, launch_frame<kMlGrad>(h, a, n), "ml gradient pass");
     ++h->launches;
     if (uo) {
       GatherArgs g = gather_args(h, frames, n);
       g.out = h->g_obj;
       g.comp = h->g_obj_c;
+      if (h->have_offsets) {
+        g.probe = h->wave;
+        g.probe_stride = pstride;
+      }
       timed(h, kKObjMl, [&] { object_tile_kernel<kGatherMl><<<ntiles(h), 1024, 0, h->stream>>>(g); });
       launched(h, "object gradient");
     }
-    if (up) {
+    if (up && h->have_offsets) {
+      // conj(q·O_win)·g per frame, moved back by −d, summed in frame order
+      // (engine/features.rs:897-957)
+      timed(h, kKProbePartial, [&] {
+        probe_terms_kernel<<<dim3((h->N * h->N + 255) / 256, n), 256, 0, h->stream>>>(
+            h->object, h->quad, h->upd, frames, h->corners, h->nxo, h->K, h->N, h->field);
+      });
+      launched(h, "probe gradient terms");
+      check(h, launch_move<kMoveBack>(h, move_args(h, frames, h->field), n), "probe move back");
+      ++h->launches;
+      timed(h, kKProbeFinal, [&] {
+        probe_finalize_kernel<<<(pstride + 255) / 256, 256, 0, h->stream>>>(
+            h->field, n, pstride, nullptr, h->g_probe, h->g_probe_c, 1.f, 2);
+      });
+      launched(h, "probe gradient sum");
+    } else if (up) {
       int nchunk = 0;
       const int chunk = probe_chunk(h, n, &nchunk);
       ProbeArgs pa = {};
@@ -1063,6 +1096,36 @@ void ml_gradients(ptyb_handle* h, bool uo, bool up) {
   }
 }
 
+// Every frame's position sums from the magnitude projection of the current estimate under
+// the position model (engine/ptycho.rs:470-480, engine/features.rs:992-1025).
+void ml_position_sums(ptyb_handle* h) {
+  const int stack = std::min(h->P, h->stack);
+  const int pstride = h->K * h->N * h->N;
+  for (int s0 = 0; s0 < h->P; s0 += stack) {
+    const int n = std::min(stack, h->P - s0);
+    const int* frames = h->iota + s0;
+    check(h, launch_move<kMoveProbe>(h, move_args(h, frames, h->wave), n), "probe move");
+    ++h->launches;
+    FrameArgs a = frame_args(h, frames);
+    a.probe = h->wave;
+    a.probe_stride = pstride;
+    check(h, launch_frame<kProject>(h, a, n), "magnitude projection");
+    ++h->launches;
+    for (int axis = 0; axis < 2; ++axis) {
+      MoveArgs md = move_args(h, frames, h->field);
+      md.axis = axis;
+      check(h, launch_move<kDerivProbe>(h, md, n), "wave derivative");
+      ++h->launches;
+      timed(h, kKPositionSums, [&] {
+        ml_position_sums_kernel<<<n, 256, 0, h->stream>>>(h->field, h->upd, h->object, frames,
+                                                           h->corners, h->nxo, h->K, h->N, axis,
+                                                           h->ml_pos_sums);
+      });
+      launched(h, "position sums");
+    }
+  }
+}
+
 // num and den of the Poisson line search along (dir_obj, dir_probe), frames summed in order.
 void ml_gamma(ptyb_handle* h, double* num, double* den) {
   const int stack = std::min(h->P, h->stack);
@@ -1083,6 +1146,18 @@ void ml_gamma(ptyb_handle* h, double* num, double* den) {
     const int n = std::min(stack, h->P - s0);
     a.frames = h->iota + s0;
     a.out = h->gamma_sums + (size_t)s0 * 2;
+    if (h->have_offsets) {
+      // the probe and its direction, each moved by the frame's offset (engine/ptycho.rs:527-534)
+      check(h, launch_move<kMoveProbe>(h, move_args(h, a.frames, h->wave), n), "probe move");
+      ++h->launches;
+      MoveArgs md = move_args(h, a.frames, h->wave2);
+      md.probe = h->dir_probe;
+      check(h, launch_move<kMoveProbe>(h, md, n), "direction move");
+      ++h->launches;
+      a.probe = h->wave;
+      a.d_probe = h->wave2;
+      a.probe_stride = h->K * h->N * h->N;
+    }
     check(h, launch_gamma(h, a, n), "ml line search");
     ++h->launches;
   }
@@ -1551,10 +1626,6 @@ int ptyb_ml(ptyb_handle* h, const ptyb_ml_params* p, int32_t ncycle) {
     h->err = "ncycle must be >= 0";
     return PTYB_INVALID;
   }
-  if (h->have_offsets) {
-    h->err = "ML does not model position offsets in this version";
-    return PTYB_INVALID;
-  }
   if (h->nslice > 1) {
     h->err = "ML runs on a single-slice object";
     return PTYB_INVALID;
@@ -1562,6 +1633,12 @@ int ptyb_ml(ptyb_handle* h, const ptyb_ml_params* p, int32_t ncycle) {
   return guarded(h, true, [&]() -> int {
     ensure_slots(h, std::min(h->P, h->stack));
     ensure_ml(h);
+    const bool refine = h->have_offsets && h->refine_offsets;
+    if (h->have_offsets && h->wave2_slots < h->slots) {
+      h->wave2 = alloc<float2>(h, (size_t)h->slots * h->K * h->N * h->N);
+      h->wave2_slots = h->slots;
+    }
+    if (refine && !h->ml_pos_sums) h->ml_pos_sums = alloc<double>(h, (size_t)h->P * 4);
     const bool uo = p->update_object != 0, up = p->update_probe != 0;
     const size_t no = (size_t)h->nyo * h->nxo, np = (size_t)h->K * h->N * h->N;
     begin_call(h);
@@ -1573,6 +1650,7 @@ int ptyb_ml(ptyb_handle* h, const ptyb_ml_params* p, int32_t ncycle) {
       const bool due = llk_due(p->calc_llk, ic, ncycle);
       ptyb_llk l = {};
       if (due) l = llk_pass(h);
+      if (refine) ml_position_sums(h);
       ml_gradients(h, uo, up);
       double beta = 0.0;
       if (have_last) {
@@ -1616,6 +1694,12 @@ int ptyb_ml(ptyb_handle* h, const ptyb_ml_params* p, int32_t ncycle) {
       std::swap(h->g_obj, h->last_obj);
       std::swap(h->g_probe, h->last_probe);
       have_last = true;
+      if (refine) {
+        timed(h, kKSolve, [&] {
+          ml_position_step_kernel<<<1, 1024, 0, h->stream>>>(h->ml_pos_sums, h->P, h->offsets);
+        });
+        launched(h, "position step");
+      }
       if (due) record(h, kAlgMl, l);
       ++h->cycle;
     }

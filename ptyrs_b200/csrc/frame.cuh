@@ -32,6 +32,7 @@ enum FrameMode : int {
   kLlk = 3,        // forward only; per-frame LLK sums
   kStore = 4,      // forward only; detector field and Σ_modes |Ψ|² to global
   kFromStore = 5,  // detector field from global; LSQML residual; out = χ
+  kProject = 6,    // magnitude projection √I/max(√Ĩ, 1e-12), masked kept; out = ψ' − ψ
 };
 
 enum Cost : int { kCostPoisson = 0, kCostAmplitude = 1 };
@@ -323,6 +324,9 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T)
     float fac;
     if (MODE == kRpie) {
       fac = masked ? 1.f : sqrtf(yo + 1e-7f) / (sqrtf(ic) + 1e-7f);
+    } else if (MODE == kProject) {
+      // ApplyAmplitude (engine/ops.rs:83-107)
+      fac = masked ? 1.f : sqrtf(yo) / fmaxf(sqrtf(ic), 1e-12f);
     } else if (MODE == kMlGrad) {
       fac = masked ? 0.f : 2.f * (1.f - yo / fmaxf(ic, 1e-12f));
     } else {

@@ -23,6 +23,9 @@ struct GammaArgs {
   const int2* corners;
   double* out;  // [slot][2]: num, den
   int nyo, nxo, nprobe, nobj;
+  // Elements between consecutive slots' probe and probe direction: 0 for the shared ones,
+  // K·N·N for the per-frame moved ones of the position model.
+  int probe_stride;
 };
 
 template <int N, int C>
@@ -62,7 +65,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T) gamma_kernel(GammaArgs a)
     for (int idx = tid; idx < H * N; idx += T) {
       const int yl = idx / N, jx = idx % N;
       const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
-      const size_t pi = ((size_t)pm * N + ny) * N + nx;
+      const size_t pi = (size_t)slot * a.probe_stride + ((size_t)pm * N + ny) * N + nx;
       const size_t oi = ((size_t)om * a.nyo + corner.x + ny) * a.nxo + corner.y + nx;
       const float2 p = a.probe[pi], dp = a.d_probe[pi];
       const float2 o = a.object[oi], dob = a.d_obj[oi];
@@ -88,7 +91,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T) gamma_kernel(GammaArgs a)
     for (int idx = tid; idx < H * N; idx += T) {
       const int yl = idx / N, jx = idx % N;
       const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
-      const size_t pi = ((size_t)pm * N + ny) * N + nx;
+      const size_t pi = (size_t)slot * a.probe_stride + ((size_t)pm * N + ny) * N + nx;
       const size_t oi = ((size_t)om * a.nyo + corner.x + ny) * a.nxo + corner.y + nx;
       S1[yl * L + (jx ^ swz(yl))] = cmul(cmul(a.d_probe[pi], a.d_obj[oi]), a.quad[ny * N + nx]);
     }

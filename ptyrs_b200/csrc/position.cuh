@@ -10,7 +10,8 @@ namespace ptyb {
 enum MoveMode : int {
   kMoveProbe = 0,  // planes[slot][m] = conj(q)·T_d(q·P_m)       (probe of frame f moved by d_f)
   kMoveBack = 1,   // planes[slot][m] = conj(q)·T_{−d}(q·planes)  (the adjoint move, in place)
-  kDerivWindow = 2 // planes[slot][a] = ∂_a O_window (periodic Fourier derivative), a = y, x
+  kDerivWindow = 2, // planes[slot][a] = ∂_a O_window (periodic Fourier derivative), a = y, x
+  kDerivProbe = 3   // planes[slot][m] = ∂T_d(q·P_m)/∂d[axis]: the moved wave's derivative
 };
 
 struct MoveArgs {
@@ -23,6 +24,7 @@ struct MoveArgs {
   const double* offsets;  // [nframe][2] (dy, dx) in object pixels
   float2* planes;         // [slot][K][N][N] natural layout
   int nxo, K;
+  int axis;               // kDerivProbe: 0 = dy, 1 = dx
 };
 
 // numpy fftfreq of index k of n points (engine/features.rs:337-344).
@@ -53,7 +55,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T) move_kernel(MoveArgs a) {
     const float2 q = a.quad[y * N + x];
     for (int m = 0; m < K; ++m) {
       float2 v;
-      if (MODE == kMoveProbe)
+      if (MODE == kMoveProbe || MODE == kDerivProbe)
         v = cmul(q, a.probe[m * plane + y * N + x]);
       else if (MODE == kMoveBack)
         v = cmul(q, out[m * plane + y * N + x]);
@@ -72,7 +74,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T) move_kernel(MoveArgs a) {
   constexpr float inv_n2 = 1.0f / ((float)N * (float)N);
   float dy = 0.f, dx = 0.f;
   if (MODE != kDerivWindow) {
-    const float sgn = MODE == kMoveProbe ? 1.f : -1.f;
+    const float sgn = MODE == kMoveBack ? -1.f : 1.f;
     dy = sgn * (float)a.offsets[2 * f];
     dx = sgn * (float)a.offsets[2 * f + 1];
   }
@@ -85,6 +87,11 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T) move_kernel(MoveArgs a) {
       float sn, cs;
       sincospif(-2.f * (fy * dy + fx * dx), &sn, &cs);  // exp(−2πi f·d)
       e = make_float2(cs * inv_n2, sn * inv_n2);
+      if (MODE == kDerivProbe) {
+        // × (−2πi·f_axis): the derivative of the translation phase (engine/features.rs:372-387)
+        const float w = 2.f * 3.14159265358979f * (a.axis == 0 ? fy : fx);
+        e = make_float2(w * e.y, -w * e.x);
+      }
     }
     for (int m = 0; m < K; ++m) {
       float2& v = S[(m * H + c) * L + (ky ^ swz(m * H + c))];
@@ -104,11 +111,12 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T) move_kernel(MoveArgs a) {
 #pragma unroll 2
   for (int idx = tid; idx < H * N; idx += T) {
     const int yl = idx / N, x = idx % N, y = r * H + yl;
-    const float2 cq = MODE == kDerivWindow ? make_float2(1.f, 0.f) : cconj(a.quad[y * N + x]);
+    constexpr bool bare = MODE == kDerivWindow || MODE == kDerivProbe;
+    const float2 cq = bare ? make_float2(1.f, 0.f) : cconj(a.quad[y * N + x]);
     for (int m = 0; m < K; ++m) {
       const int line = m * H + yl;
       const float2 v = S[line * L + (x ^ swz(line))];
-      out[m * plane + y * N + x] = MODE == kDerivWindow ? v : cmul(cq, v);
+      out[m * plane + y * N + x] = bare ? v : cmul(cq, v);
     }
   }
 }
@@ -191,6 +199,91 @@ __global__ void position_step_kernel(const double* sums, int nslot, int nframe, 
       const double dx = 0.3 * (sums[s * 4 + a] / (sums[s * 4 + 2 + a] + mx));
       offsets[2 * frames[s] + a] += fmin(fmax(dx, -limit), limit);
     }
+  }
+}
+
+// Per slot, one axis of the position sums of AP, DM and ML (engine/features.rs:992-1025):
+// with c = x − O·W the magnitude projection's change of the exit wave and dψ = O·∂W/∂d[axis],
+// num = Σ Re(conj(c)·dψ), den = Σ |dψ|² over the frame's modes and pixels, in double, into
+// sums[frame][axis] (num) and sums[frame][2 + axis] (den).
+__global__ void __launch_bounds__(256) ml_position_sums_kernel(const float2* dwave,
+                                                              const float2* c,
+                                                              const float2* object,
+                                                              const int* frames,
+                                                              const int2* corners, int nxo,
+                                                              int K, int N, int axis,
+                                                              double* sums) {
+  __shared__ double sh[16];
+  const int slot = blockIdx.x;
+  const int f = frames[slot];
+  const int2 cn = corners[f];
+  const size_t plane = (size_t)N * N;
+  double num = 0.0, den = 0.0;
+  for (int pix = threadIdx.x; pix < N * N; pix += 256) {
+    const int y = pix / N, x = pix % N;
+    const float2 o = object[(size_t)(cn.x + y) * nxo + cn.y + x];
+    for (int m = 0; m < K; ++m) {
+      const size_t i = ((size_t)slot * K + m) * plane + pix;
+      const float2 d = cmul(o, dwave[i]), v = c[i];
+      num += (double)v.x * d.x + (double)v.y * d.y;
+      den += (double)d.x * d.x + (double)d.y * d.y;
+    }
+  }
+  num = warp_sum(num);
+  den = warp_sum(den);
+  if (threadIdx.x % 32 == 0) {
+    sh[threadIdx.x / 32] = num;
+    sh[8 + threadIdx.x / 32] = den;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int w = 0; w < 8; ++w) {
+      a += sh[w];
+      b += sh[8 + w];
+    }
+    sums[(size_t)f * 4 + axis] = a;
+    sums[(size_t)f * 4 + 2 + axis] = b;
+  }
+}
+
+// Block sum of one double per thread in a fixed order (lane trees, then warps in order).
+template <int T>
+PTYB_D double fixed_block_sum(double v, double* sh) {
+  v = warp_sum(v);
+  __syncthreads();
+  if (threadIdx.x % 32 == 0) sh[threadIdx.x / 32] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int w = 0; w < T / 32; ++w) s += sh[w];
+  return s;
+}
+
+// The position step of AP, DM and ML on every frame (engine/features.rs:1028-1047), one block:
+// per axis, with max the largest den, step = clip(0.3·num / (den + max), ±0.1) (0 where that
+// denominator is not positive) and d += step − mean(step) over every frame.
+__global__ void __launch_bounds__(1024) ml_position_step_kernel(const double* sums, int nframe,
+                                                               double* offsets) {
+  __shared__ double sh[32];
+  const int t = threadIdx.x;
+  for (int a = 0; a < 2; ++a) {
+    double mx = 0.0;
+    for (int f = t; f < nframe; f += 1024) mx = fmax(mx, sums[(size_t)f * 4 + 2 + a]);
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    __syncthreads();
+    if (t % 32 == 0) sh[t / 32] = mx;
+    __syncthreads();
+    mx = 0.0;
+    for (int w = 0; w < 32; ++w) mx = fmax(mx, sh[w]);
+    auto step = [&](int f) {
+      const double den = sums[(size_t)f * 4 + 2 + a] + mx;
+      return den > 0.0 ? fmin(fmax(0.3 * sums[(size_t)f * 4 + a] / den, -0.1), 0.1) : 0.0;
+    };
+    double part = 0.0;
+    for (int f = t; f < nframe; f += 1024) part += step(f);
+    const double mean = fixed_block_sum<1024>(part, sh) / nframe;
+    for (int f = t; f < nframe; f += 1024) offsets[2 * f + a] += step(f) - mean;
+    __syncthreads();
   }
 }
 

@@ -29,7 +29,7 @@ def far_field(n, nmode, nframe, side, photons=1e5, seed=0, masked=False, step=No
     start_probe = probe * 0.9 * np.exp(0.2j)
     start_obj = np.ones((1, side, side), np.complex128)
     return dict(counts=counts, y=pos[:, 0] * px, x=pos[:, 1] * px, object=start_obj,
-                probe=start_probe, corners=corner, n=n)
+                probe=start_probe, corners=corner, n=n, truth=truth)
 
 
 def oracle_state(s):

@@ -221,3 +221,38 @@ def test_lsqml_with_positions(case, refine):
         cpu.object, cpu.probe = obj, probe
         want = run.llk(cpu.addr, cpu.obs, cpu.optics, obj, probe).poisson
         assert abs(g.llk()["poisson"] - want) <= RUN_TOL * abs(want)
+
+
+@pytest.mark.parametrize("refine", [False, True])
+def test_ml_with_positions(case, refine):
+    """Poisson ML under per-frame sub-pixel offsets (Patch sampling: every view's probe moved by
+    its frame's offset in the LLK, the gradients and the line search, the probe gradient moved
+    back), with `refine` AP's position step from the magnitude projection of the estimate each
+    cycle starts from, against the oracle's `Ptycho::ml`: the arrays, the LLK records and the
+    offsets' changes. The start object is the perturbed truth: under a flat object the
+    intensities do not depend on the offsets, so their step would be rounding. The single
+    hard-edged aperture runs one cycle: its moved copies ring over the whole frame, and at
+    the far-field zeros, where the Poisson gradient 2(1 − I/Ĩ) is led by Ĩ, FP32 rounding of
+    the moves grows over the CG cycles."""
+    nframe = len(case["counts"])
+    ncycle = 1 if case["probe"].shape[0] == 1 else 4
+    d0 = np.random.default_rng(6).uniform(-0.6, 0.6, (nframe, 2))
+    start = dict(case, object=case["truth"] * 0.9 * np.exp(0.1j))
+    cpu = oracle_state(start)
+    cpu.set_positions(d0, refine=refine)
+    cpu.ml(ncycle, update_probe=True, calc_llk=1, zero_phase_ramp=False)
+    with gpu_of(start) as g:
+        g.set_positions(d0, refine=refine)
+        g.ml(ncycle, update_probe=True, calc_llk=1, zero_phase_ramp=False)
+        assert rel_l2(g.object(), cpu.object) < RUN_TOL
+        assert rel_l2(g.probe(), cpu.probe) < RUN_TOL
+        h = g.history()
+        want = np.array([r["poisson"] for r in cpu.history])
+        assert np.abs(h["poisson"] - want).max() <= RUN_TOL * np.abs(want).max()
+        d = g.positions()
+        if refine:
+            moved = cpu.offsets - d0
+            assert np.abs(moved).max() > 0
+            assert np.abs((d - d0) - moved).max() <= RUN_TOL * 10 * np.abs(moved).max()
+        else:
+            assert np.array_equal(d, d0)
