@@ -1,24 +1,31 @@
 """Throughput of the reconstruction hot path on B200: diffraction patterns·iterations per second.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload lsqml128|rpie64]
+                    [--workload ml256|lsqml128|rpie64]
 
-Workload `lsqml128` (default): the LSQML configuration — a 1024² smooth-noise object, a
-128² probe with 3 incoherent modes (powers 0.8/0.15/0.05), a 4096-position Fermat scan at
-6 px, Poisson counts at 1e6 photons per pattern, batches of 256 frames, Poisson cost, FP32.
-A step is one epoch: every one of the 4096 patterns once (16 batch updates). Inputs live in
-HBM before the timed region; the counts (268 MB) are larger than the 126 MB L2, so no flush
-is needed between steps. `rpie64`: the rPIE configuration (256² object, 64² probe, 20×20
-raster, batch 100), a step again one epoch.
+Workload `ml256` (default; the configuration the metric names, a 256² probe): Poisson
+maximum-likelihood conjugate gradient with position refinement — a 2048² smooth-noise object,
+a 256² probe with 2 incoherent modes (powers 0.8/0.2), a 10000-position Fermat scan at 12 px
+whose frames were taken at true positions off the nominal ones by seeded N(0, 1.5 px)
+offsets (the solver gets the nominal positions and refines sub-pixel offsets under the Patch
+model), Poisson counts at 1e7 photons per pattern, FP32. A step is one ML cycle over all 10000
+patterns: the position sums from the magnitude projection, the object and probe gradients,
+the Polak–Ribière direction, the Poisson line search, the update and the position step.
+`lsqml128`: the LSQML configuration (1024² object, 128² probe × 3 modes, Fermat 4096 at 6 px,
+1e6 photons, batches of 256, Poisson cost), a step one epoch. `rpie64`: the rPIE
+configuration (256² object, 64² probe, 20×20 raster, batch 100), a step one epoch. Inputs
+live in HBM before the timed region; the counts of `ml256` (2.6 GB) and `lsqml128` (268 MB)
+are larger than the 126 MB L2, so no flush is needed between steps.
 
 The timed region is bracketed by CUDA events on the engine's own stream (its device time of
-the K epochs) with a synchronize and, for N > 1, a barrier on both sides; N > 1 runs N
+the K steps) with a synchronize and, for N > 1, a barrier on both sides; N > 1 runs N
 independent replicas (one scan per GPU; the path has no exchange step), the time is the max
 over ranks and the value the patterns of all ranks over it.
 
 `--impl reference` times the reference's CPU path on the host cores: the reference engine is
-Rust and cannot be built in this image, so its numpy float64 restatement (`oracle/`) runs, one
-LSQML batch of 256 frames per step, its FFTs on every host thread.
+Rust and cannot be built in this image, so its numpy float64 restatement (`oracle/`) runs on a
+bounded sample of the workload (one ML cycle over the first frames of the scan, or one batch
+update of LSQML / rPIE per step), its FFTs on every host thread.
 """
 import argparse
 import json
@@ -37,6 +44,10 @@ sys.path.insert(0, ROOT)
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 
 WORKLOADS = {
+    "ml256": dict(kind="ml256", algorithm="ml", refine=True, sample_frames=48,
+                  desc="ML (Poisson CG) with position refinement, 2048^2 object, 256^2 probe x2 "
+                       "modes, Fermat 10000 @ 12 px, true positions off the nominal by "
+                       "N(0, 1.5 px), 1e7 photons"),
     "lsqml128": dict(kind="lsqml128", algorithm="lsqml", batch=256, cost="poisson",
                      desc="LSQML, 1024^2 object, 128^2 probe x3 modes, Fermat 4096 @ 6 px, "
                           "1e6 photons, batch 256, Poisson"),
@@ -110,36 +121,61 @@ def make_inputs(workload, seed, scale=1.0):
     return sim.make_scan(WORKLOADS[workload]["kind"], seed=seed, scale=scale)
 
 
+def prepare(g, s, wl):
+    """The workload's features on a fresh state: ML starts at the nominal positions with the
+    sub-pixel offsets refined."""
+    if wl["algorithm"] == "ml":
+        g.set_positions(np.zeros((len(s["counts"]), 2)), refine=wl["refine"])
+
+
 def run_algorithm(g, wl, nepoch):
-    if wl["algorithm"] == "lsqml":
+    if wl["algorithm"] == "ml":
+        g.ml(nepoch, update_object=True, update_probe=True, calc_llk=0, zero_phase_ramp=False)
+    elif wl["algorithm"] == "lsqml":
         g.lsqml(nepoch, batch_size=wl["batch"], cost=wl["cost"], seed=7)
     else:
         g.rpie(nepoch, batch_size=wl["batch"], obj_alpha=0.1, probe_alpha=0.1, seed=7)
 
 
 def algorithmic_bytes(kind, s, wl):
-    """Bytes each launch of `kind` must move from HBM (the unique inputs it reads and outputs
-    it writes), per frame of the launch; probe, phase and twiddle reads are L2-resident."""
+    """Bytes a launch of `kind` must move from HBM per frame it processes: the unique inputs it
+    reads and the outputs it writes (object window 8·N², counts 4·N², per-mode planes 8·K·N²);
+    the shared probe, phase and twiddles are L2-resident, the moved per-frame probes of the
+    position model are not."""
     n2 = s["n"] ** 2
     K = s["probe"].shape[0]
+    moved = 8 * K * n2 if wl.get("refine") else 0
     table = {
         "frame_store": 8 * n2 + 8 * K * n2 + 4 * n2,
         "frame_from_store": 8 * K * n2 + 4 * n2 + 8 * n2 + 8 * K * n2,
         "frame_rpie": 8 * n2 + 4 * n2 + 8 * K * n2,
         "frame_lsqml": 8 * n2 + 4 * n2 + 8 * K * n2,
-        "frame_llk": 8 * n2 + 4 * n2,
+        "frame_llk": 8 * n2 + 4 * n2 + moved,
+        "frame_ml": 8 * n2 + 4 * n2 + 8 * K * n2 + moved,
+        "frame_project": 8 * n2 + 4 * n2 + 8 * K * n2 + moved,
+        "ml_gamma": 16 * n2 + 4 * n2 + 2 * moved,
+        "move": 8 * K * n2,
+        "position_sums": 16 * K * n2 + 8 * n2,
         "probe_partial": 8 * K * n2 + 8 * n2,
         "lsqml_dots": 8 * K * n2 + 16 * n2,
         "object_lsqml": 8 * K * n2,
         "object_rpie": 8 * K * n2,
+        "object_ml": 8 * K * n2 + moved,
     }
     return table.get(kind)
 
 
-def cpu_baseline(s, wl, seconds=15.0, threads=None):
+def sample_scan(s, m):
+    """The first `m` frames of the scan, its object and probe starts (a bounded sample)."""
+    return dict(s, counts=s["counts"][:m], y=s["y"][:m], x=s["x"][:m])
+
+
+def cpu_baseline(s, wl, seconds=15.0, threads=None, cycles=2):
     """The oracle (numpy float64 restatement of the reference's CPU engine) on a bounded sample
-    of the workload: successive batch updates of `wl["batch"]` frames from the same start until
-    `seconds` pass; patterns·iter/s = frames processed / time."""
+    of the workload. ML: `cycles` cycles (one call, as the GPU step) over the first
+    `wl["sample_frames"]` frames of the scan. LSQML / rPIE: successive batch updates of
+    `wl["batch"]` frames from the same start until `seconds` pass. Returns patterns·iter/s,
+    the pattern-iterations done, the seconds and the oracle state."""
     from oracle import ops
     from oracle.lsqml import Lsqml
     from oracle.ptycho import Ptycho
@@ -147,6 +183,15 @@ def cpu_baseline(s, wl, seconds=15.0, threads=None):
     ops.FFT_WORKERS = threads
     n = s["n"]
     optics = ops.Optics.far_field(sim.WAVELENGTH, sim.DISTANCE, sim.DETECTOR_PIXEL, [n, n])
+    if wl["algorithm"] == "ml":
+        t = sample_scan(s, min(wl["sample_frames"], len(s["counts"])))
+        p = Ptycho(t["counts"], t["y"], t["x"], optics, t["object"], t["probe"])
+        p.set_positions(np.zeros((p.addr.nframe, 2)), refine=wl["refine"])
+        t0 = time.perf_counter()
+        p.ml(cycles, update_object=True, update_probe=True, calc_llk=0, zero_phase_ramp=False)
+        dt = time.perf_counter() - t0
+        ops.FFT_WORKERS = None
+        return p.addr.nframe * cycles / dt, p.addr.nframe * cycles, dt, p
     p = Ptycho(s["counts"], s["y"], s["x"], optics, s["object"], s["probe"])
     from oracle.base import random_batches
     batches = random_batches(p.addr.nframe, wl["batch"], 7, 0)
@@ -166,26 +211,61 @@ def cpu_baseline(s, wl, seconds=15.0, threads=None):
             break
     dt = time.perf_counter() - t0
     ops.FFT_WORKERS = None
-    return done / dt, done, dt
+    return done / dt, done, dt, p
+
+
+def object_nrmse(a, b, weight):
+    """‖a − c·b‖/‖c·b‖ over the pixels where `weight` > 0, c the least-squares complex scalar
+    that removes the global phase (and scale) between them."""
+    a, b = a[weight > 0], b[weight > 0]
+    c = np.vdot(b, a) / np.vdot(b, b)
+    return float(np.linalg.norm(a - c * b) / np.linalg.norm(c * b))
+
+
+def accuracy(s, wl, oracle_state, device, cycles=2):
+    """The FP32 GPU path against the float64 oracle on the bounded ML sample: object NRMSE
+    after the global phase, over the illuminated pixels (illumination ≥ 1e-3 of its max)."""
+    from oracle import ops
+    from ptyrs_b200 import GpuPtycho, Scan
+    t = sample_scan(s, oracle_state.addr.nframe)
+    scan = Scan(t["counts"], t["y"], t["x"], t["wavelength"], t["distance"], t["detector_pixel"])
+    with GpuPtycho(scan, t["object"], t["probe"], device=device) as g:
+        prepare(g, t, wl)
+        run_algorithm(g, wl, cycles)
+        obj = g.object()
+        d = g.positions()
+    illum = ops.illumination(oracle_state.addr.views, oracle_state.object.shape,
+                             oracle_state.probe)
+    w = (illum >= 1e-3 * illum.max()).astype(float)
+    moved = oracle_state.offsets
+    return {"object_nrmse_vs_f64": object_nrmse(obj, oracle_state.object, w),
+            "offsets_max_abs_diff_px": float(np.abs(d - moved).max()),
+            "sample": f"{cycles} ML cycles over the first {t['counts'].shape[0]} frames, GPU "
+                      "FP32 vs the float64 oracle from the same start"}
 
 
 def reference_arm(args, wl):
     rank, ws, _ = dist_env()
     if rank != 0:
         return
-    s = make_inputs(args.workload, 0)
+    s = make_inputs(args.workload, 0, scale=args.scale)
     threads = os.cpu_count() or 1
     for _ in range(args.warmup):
-        cpu_baseline(s, wl, seconds=0.0, threads=threads)
+        cpu_baseline(s, wl, seconds=0.0, threads=threads, cycles=1)
     vals, frames, secs = [], 0, 0.0
     for _ in range(args.steps):
-        v, d, t = cpu_baseline(s, wl, seconds=0.0, threads=threads)
+        v, d, t, _ = cpu_baseline(s, wl, seconds=0.0, threads=threads, cycles=1)
         vals.append(v)
         frames += d
         secs += t
     value = frames / secs
-    sample = (f"{args.steps} steps of one {wl['algorithm']} batch update of {wl['batch']} frames "
-              f"of the {args.workload} scan ({frames} pattern-iterations in {secs:.1f} s)")
+    if wl["algorithm"] == "ml":
+        what = (f"one ML cycle (with position refinement) over the first "
+                f"{wl['sample_frames']} frames")
+    else:
+        what = f"one {wl['algorithm']} batch update of {wl['batch']} frames"
+    sample = (f"{args.steps} steps of {what} of the {args.workload} scan ({frames} "
+              f"pattern-iterations in {secs:.1f} s)")
     line = {
         "impl": "reference", "metric": "diffraction patterns*iter/sec", "value": value,
         "unit": "patterns*iter/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
@@ -206,11 +286,13 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="lsqml128", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="ml256", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cluster", type=int, default=0,
                     help="CTAs per frame of the frame kernel (0: the engine chooses)")
+    ap.add_argument("--stack", type=int, default=0,
+                    help="frames per launch of the whole-scan passes (0: the engine's default)")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="keep this fraction of the scan's positions (small profiling cases)")
     args = ap.parse_args()
@@ -234,7 +316,9 @@ def main():
     s = make_inputs(args.workload, seed=rank, scale=args.scale)
     P = len(s["counts"])
     scan = Scan(s["counts"], s["y"], s["x"], s["wavelength"], s["distance"], s["detector_pixel"])
-    g = GpuPtycho(scan, s["object"], s["probe"], device=local, cluster=args.cluster)
+    g = GpuPtycho(scan, s["object"], s["probe"], device=local, cluster=args.cluster,
+                  stack_size=args.stack)
+    prepare(g, s, wl)
     run_algorithm(g, wl, args.warmup)
     g.synchronize()
 
@@ -255,6 +339,7 @@ def main():
     ms = g.last_call_ms()
     launches = g.launches() - launches0
     times = g.kernel_times()
+    kframes = g.kernel_frames()
     g.set_timing(False)
     if dist is not None:
         t = torch.tensor([ms], device="cuda")
@@ -267,10 +352,9 @@ def main():
     top = max(times.items(), key=lambda kv: kv[1][0])
     kname, (kms, kn) = top
     per_frame = algorithmic_bytes(kname, s, wl)
-    frames_per_launch = wl["batch"]
     roofline = None
-    if per_frame:
-        bytes_launch = per_frame * frames_per_launch
+    if per_frame and kframes.get(kname):
+        bytes_launch = per_frame * kframes[kname] / kn
         achieved = bytes_launch / (kms / kn / 1e3) / 1e9
         roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved,
                     "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
@@ -286,36 +370,50 @@ def main():
         pinned.numpy()[...] = s["counts"]
         escan = Scan(pinned.numpy(), s["y"], s["x"], s["wavelength"], s["distance"],
                      s["detector_pixel"])
-        with GpuPtycho(escan, s["object"], s["probe"], device=local) as w:  # warm-up
+        ekw = dict(device=local, cluster=args.cluster, stack_size=args.stack)
+        with GpuPtycho(escan, s["object"], s["probe"], **ekw) as w:  # warm-up
+            prepare(w, s, wl)
             run_algorithm(w, wl, 1)
             w.object()
         barrier()
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
-            with GpuPtycho(escan, s["object"], s["probe"], device=local) as w:
+            with GpuPtycho(escan, s["object"], s["probe"], **ekw) as w:
+                prepare(w, s, wl)
                 run_algorithm(w, wl, 1)
                 w.object()
                 w.probe()
+                if wl["algorithm"] == "ml":
+                    w.positions()
         dt = time.perf_counter() - t0
         if dist is not None:
             t = torch.tensor([dt], device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             dt = float(t.item())
         n = s["n"]
-        h2d = (s["counts"].nbytes + 8 * s["object"].size + 8 * s["probe"].size + 8 * P)
-        d2h = 8 * s["object"].size + 8 * s["probe"].size
+        # counts (f32), object and probe (complex64 on the device), positions (y, x and the
+        # ML offsets in f64)
+        pos_bytes = 16 * P + (16 * P if wl["algorithm"] == "ml" else 0)
+        h2d = s["counts"].nbytes + 8 * s["object"].size + 8 * s["probe"].size + pos_bytes
+        d2h = (8 * s["object"].size + 8 * s["probe"].size
+               + (16 * P if wl["algorithm"] == "ml" else 0))
         e2e = {"value": P * ws * args.e2e_steps / dt, "unit": "patterns*iter/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-               "what": "per step: create from pinned host counts, one epoch, object and probe "
-                       "read back"}
+               "what": "per step: create from pinned host counts (and the start offsets), one "
+                       "epoch or ML cycle, the object, probe (and offsets) read back"}
 
-    cpu = None
+    cpu, acc = None, None
     if rank == 0 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        v, done, secs = cpu_baseline(s, wl, seconds=15.0, threads=threads)
+        v, done, secs, state = cpu_baseline(s, wl, seconds=15.0, threads=threads)
+        if wl["algorithm"] == "ml":
+            what = (f"2 ML cycles with position refinement over the first "
+                    f"{state.addr.nframe} frames of the scan")
+            acc = accuracy(s, wl, state, local)
+        else:
+            what = f"{done // wl['batch']} batch updates of {wl['batch']} frames of the scan"
         cpu = {"value": v, "unit": "patterns*iter/s", "cores": threads, "kind": "port",
-               "sample": f"{done} pattern-iterations ({done // wl['batch']} batch updates of "
-                         f"{wl['batch']} frames) of the same scan in {secs:.1f} s, numpy float64, "
+               "sample": f"{done} pattern-iterations ({what}) in {secs:.1f} s, numpy float64, "
                          f"FFTs on {threads} threads"}
     g.close()
     if rank == 0:
@@ -329,7 +427,7 @@ def main():
                        "patterns_per_step_per_gpu": P, "parallelism": f"replicas{ws}",
                        "l2": "inputs larger than L2 (counts "
                              f"{s['counts'].nbytes / 1e6:.0f} MB)"},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "accuracy": acc,
             "gpu_launches": int(launches), "clocks": clk,
             "kernels_ms": {k: round(v[0], 3) for k, v in sorted(times.items())},
         }

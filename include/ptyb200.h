@@ -209,6 +209,8 @@ int ptyb_set_timing(ptyb_handle* h, int32_t on);
 int32_t ptyb_kernel_kinds(void);
 const char* ptyb_kernel_name(int32_t kind);
 int ptyb_kernel_times(ptyb_handle* h, double* ms, int64_t* launches, int32_t cap);
+/* The frames the timed launches of each kind processed (0 for kinds not per frame). */
+int ptyb_kernel_frames(ptyb_handle* h, int64_t* frames, int32_t cap);
 
 /* Device time (ms, CUDA events on the handle's stream) of the last rPIE / LSQML / ML call. */
 double ptyb_last_call_ms(ptyb_handle* h);

@@ -87,6 +87,7 @@ SIGNATURES = {
     "ptyb_kernel_kinds": (c_int32, []),
     "ptyb_kernel_name": (ctypes.c_char_p, [c_int32]),
     "ptyb_kernel_times": (c_int32, [c_void_p, P(c_double), P(c_int64), c_int32]),
+    "ptyb_kernel_frames": (c_int32, [c_void_p, P(c_int64), c_int32]),
     "ptyb_last_call_ms": (c_double, [c_void_p]),
     "ptyb_last_error": (ctypes.c_char_p, [c_void_p]),
     "ptyb_destroy": (None, [c_void_p]),

@@ -156,14 +156,25 @@ struct ptyb_handle {
   float2* wave2 = nullptr;       // [wave2_slots][K][N][N]
   int wave2_slots = 0;
   double* ml_pos_sums = nullptr; // [P][4]
+  // The position model's spectra DFT(q·P) of the probe and of the ML probe direction, and
+  // every frame's moved probe for one ML cycle.
+  float2* spec = nullptr;        // [K][N][N]
+  float2* spec_d = nullptr;      // [K][N][N]
+  float2* wave_all = nullptr;    // [P][K][N][N]
   double* partials = nullptr;    // [kPartialBlocks][2]
   std::vector<Buf> bufs;
   // Per-kernel device timing (CUDA events on the engine's stream), when enabled.
   bool timing = false;
   std::vector<cudaEvent_t> event_pool;
-  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+  struct Pending {
+    int kind;
+    int64_t frames;
+    cudaEvent_t a, b;
+  };
+  std::vector<Pending> pending;
   double kind_ms[32] = {0};
   int64_t kind_n[32] = {0};
+  int64_t kind_frames[32] = {0};  // frames the launches of each kind processed
   cudaEvent_t call_ev[2] = {nullptr, nullptr};
   float last_call_ms = 0.f;
   // Host state.
@@ -232,14 +243,16 @@ enum Kind : int {
   kKFrameRpie = 0, kKFrameLsqml, kKFrameMl, kKFrameLlk, kKFrameStore, kKFrameFromStore,
   kKObjRpie, kKObjOverlap, kKObjLsqml, kKObjMl, kKIllum, kKProbePartial, kKProbeFinal,
   kKAfar, kKDots, kKSolve, kKAxpy, kKMax, kKCounts, kKMisc, kKGamma, kKArraySums, kKMove,
-  kKPositionSums, kKSliceForward, kKSliceBackward, kKSliceLlk, kKFrameProject, kNumKinds
+  kKPositionSums, kKSliceForward, kKSliceBackward, kKSliceLlk, kKFrameProject, kKSpectrum,
+  kKDerivSums, kNumKinds
 };
 const char* const kKindNames[kNumKinds] = {
     "frame_rpie", "frame_lsqml", "frame_ml_grad", "frame_llk", "frame_store",
     "frame_from_store", "object_rpie", "object_overlap", "object_lsqml", "object_ml",
     "illumination", "probe_partial", "probe_finalize", "lsqml_afar", "lsqml_dots",
     "lsqml_solve", "axpy", "max", "counts", "misc", "ml_gamma", "array_sums", "move",
-    "position_sums", "slice_forward", "slice_backward", "slice_llk", "frame_project"};
+    "position_sums", "slice_forward", "slice_backward", "slice_llk", "frame_project", "spectrum",
+    "deriv_sums"};
 
 cudaEvent_t take_event(ptyb_handle* h) {
   if (!h->event_pool.empty()) {
@@ -255,7 +268,7 @@ cudaEvent_t take_event(ptyb_handle* h) {
 // Runs `launch` (which enqueues one kernel on the engine's stream), bracketed by events when
 // timing is on.
 template <typename F>
-void timed(ptyb_handle* h, int kind, F&& launch) {
+void timed(ptyb_handle* h, int kind, F&& launch, int64_t frames = 0) {
   if (!h->timing) {
     launch();
     return;
@@ -264,18 +277,19 @@ void timed(ptyb_handle* h, int kind, F&& launch) {
   check(h, cudaEventRecord(a, h->stream), "event");
   launch();
   check(h, cudaEventRecord(b, h->stream), "event");
-  h->pending.push_back({kind, {a, b}});
+  h->pending.push_back({kind, frames, a, b});
 }
 
 // Folds the finished launches' times into the per-kind totals (after a stream sync).
 void harvest(ptyb_handle* h) {
   for (auto& p : h->pending) {
     float ms = 0.f;
-    check(h, cudaEventElapsedTime(&ms, p.second.first, p.second.second), "event time");
-    h->kind_ms[p.first] += ms;
-    h->kind_n[p.first] += 1;
-    h->event_pool.push_back(p.second.first);
-    h->event_pool.push_back(p.second.second);
+    check(h, cudaEventElapsedTime(&ms, p.a, p.b), "event time");
+    h->kind_ms[p.kind] += ms;
+    h->kind_n[p.kind] += 1;
+    h->kind_frames[p.kind] += p.frames;
+    h->event_pool.push_back(p.a);
+    h->event_pool.push_back(p.b);
   }
   h->pending.clear();
 }
@@ -365,7 +379,7 @@ cudaError_t launch_frame(ptyb_handle* h, const FrameArgs& a, int nslot) {
                        : MODE == kProject ? kKFrameProject
                                         : kKFrameFromStore;
   cudaError_t e = cudaSuccess;
-  timed(h, kind, [&] { e = launch_frame_raw<MODE>(h, a, nslot); });
+  timed(h, kind, [&] { e = launch_frame_raw<MODE>(h, a, nslot); }, nslot);
   return e;
 }
 
@@ -400,8 +414,9 @@ template <int MODE>
 cudaError_t launch_move(ptyb_handle* h, const MoveArgs& a, int nslot) {
   if (nslot <= 0) return cudaSuccess;
   const int K = MODE == kDerivWindow ? 2 : h->K;
+  constexpr int kind = MODE == kDerivSums ? kKDerivSums : MODE == kSpectrum ? kKSpectrum : kKMove;
   cudaError_t e = cudaErrorInvalidValue;
-  timed(h, kKMove, [&] {
+  timed(h, kind, [&] {
     switch (h->N * 100 + h->C) {
       case 6401: e = launch_move_nc<64, 1, MODE>(a, nslot, K, h->stream); break;
       case 12802: e = launch_move_nc<128, 2, MODE>(a, nslot, K, h->stream); break;
@@ -409,7 +424,7 @@ cudaError_t launch_move(ptyb_handle* h, const MoveArgs& a, int nslot) {
       case 25608: e = launch_move_nc<256, 8, MODE>(a, nslot, K, h->stream); break;
       case 25616: e = launch_move_nc<256, 16, MODE>(a, nslot, K, h->stream); break;
     }
-  });
+ }, nslot);
   return e;
 }
 
@@ -453,7 +468,7 @@ cudaError_t launch_slice(ptyb_handle* h, const SliceArgs& a, int nslot) {
       case 25608: e = launch_slice_nc<256, 8, MODE>(a, nslot, h->K, h->stream); break;
       case 25616: e = launch_slice_nc<256, 16, MODE>(a, nslot, h->K, h->stream); break;
     }
-  });
+ }, nslot);
   return e;
 }
 
@@ -470,6 +485,31 @@ MoveArgs move_args(ptyb_handle* h, const int* frames, float2* planes) {
   m.nxo = h->nxo;
   m.K = h->K;
   return m;
+}
+
+// DFT(q·P) of the K planes `probe` into `spec` (the probe spectra the moves start from,
+// engine/features.rs:347-360).
+void spectrum_of(ptyb_handle* h, const float2* probe, float2* spec) {
+  MoveArgs m = move_args(h, h->iota, spec);
+  m.probe = probe;
+  check(h, launch_move<kSpectrum>(h, m, 1), "probe spectrum");
+  ++h->launches;
+}
+
+// Each of `n` frames' moved probe conj(q)·T_d(q·P) from the spectrum `spec` into `out`
+// ([slot][K][N][N]).
+void move_frames(ptyb_handle* h, const int* frames, int n, const float2* spec, float2* out) {
+  MoveArgs m = move_args(h, frames, out);
+  m.spec = spec;
+  check(h, launch_move<kFromSpectrum>(h, m, n), "probe move");
+  ++h->launches;
+}
+
+void ensure_spec(ptyb_handle* h) {
+  if (h->spec) return;
+  const size_t np = (size_t)h->K * h->N * h->N;
+  h->spec = alloc<float2>(h, np);
+  h->spec_d = alloc<float2>(h, np);
 }
 
 FrameArgs frame_args(ptyb_handle* h, const int* frames) {
@@ -579,7 +619,7 @@ void probe_pass(ptyb_handle* h, const int* frames, int nslot, int mode, float al
   p.N = h->N;
   p.mode = mode == 0 ? 0 : 1;
   dim3 grid((h->N * h->N + 255) / 256, nchunk);
-  timed(h, kKProbePartial, [&] { probe_partial_kernel<<<grid, 256, 0, h->stream>>>(p); });
+  timed(h, kKProbePartial, [&] { probe_partial_kernel<<<grid, 256, 0, h->stream>>>(p); }, nslot);
   launched(h, "probe_partial");
   const int count = h->K * h->N * h->N;
   timed(h, kKProbeFinal, [&] {
@@ -590,9 +630,15 @@ void probe_pass(ptyb_handle* h, const int* frames, int nslot, int mode, float al
 }
 
 // The LLK of the current estimate over every frame: per-frame sums in frame order.
-ptyb_llk llk_pass(ptyb_handle* h) {
+// `waves` (optional): every frame's moved probe, [P][K][N][N], when the caller has them.
+ptyb_llk llk_pass(ptyb_handle* h, const float2* waves = nullptr) {
   const int stack = std::min(h->P, h->stack);
+  const size_t pstride = (size_t)h->K * h->N * h->N;
   ensure_slots(h, stack);
+  if (h->have_offsets && !waves && h->nslice == 1) {
+    ensure_spec(h);
+    spectrum_of(h, h->probe, h->spec);
+  }
   for (int s0 = 0; s0 < h->P; s0 += stack) {
     const int n = std::min(stack, h->P - s0);
     FrameArgs a = frame_args(h, h->iota + s0);
@@ -610,10 +656,13 @@ ptyb_llk llk_pass(ptyb_handle* h) {
     }
     if (h->have_offsets) {
       // each frame's own moved probe (engine/lsqml.rs:537-551)
-      check(h, launch_move<kMoveProbe>(h, move_args(h, h->iota + s0, h->wave), n), "probe move");
-      ++h->launches;
-      a.probe = h->wave;
-      a.probe_stride = h->K * h->N * h->N;
+      if (waves) {
+        a.probe = waves + s0 * pstride;
+      } else {
+        move_frames(h, h->iota + s0, n, h->spec, h->wave);
+        a.probe = h->wave;
+      }
+      a.probe_stride = (int)pstride;
     }
     check(h, launch_frame<kLlk>(h, a, n), "llk pass");
     ++h->launches;
@@ -677,7 +726,7 @@ void rpie_batch(ptyb_handle* h, const ptyb_rpie_params& p, const int* frames, in
   GatherArgs g = gather_args(h, frames, nslot);
   if (p.update_object) {
     check(h, cudaMemsetAsync(h->scal, 0, sizeof(float), h->stream), "memset");
-    timed(h, kKObjOverlap, [&] { object_tile_kernel<kGatherOverlap><<<ntiles(h), 1024, 0, h->stream>>>(g); });
+    timed(h, kKObjOverlap, [&] { object_tile_kernel<kGatherOverlap><<<ntiles(h), 1024, 0, h->stream>>>(g); }, nslot);
     launched(h, "overlap max");
   }
   if (p.update_probe) {
@@ -700,12 +749,12 @@ void rpie_batch(ptyb_handle* h, const ptyb_rpie_params& p, const int* frames, in
     pa.N = h->N;
     pa.mode = 0;
     dim3 grid((h->N * h->N + 255) / 256, nchunk);
-    timed(h, kKProbePartial, [&] { probe_partial_kernel<<<grid, 256, 0, h->stream>>>(pa); });
+    timed(h, kKProbePartial, [&] { probe_partial_kernel<<<grid, 256, 0, h->stream>>>(pa); }, pa.nslot);
     launched(h, "probe partial");
     if (p.update_object) {
       g.alpha = (float)p.obj_alpha;
       g.step = (float)p.obj_step;
-      timed(h, kKObjRpie, [&] { object_tile_kernel<kGatherRpie><<<ntiles(h), 1024, 0, h->stream>>>(g); });
+      timed(h, kKObjRpie, [&] { object_tile_kernel<kGatherRpie><<<ntiles(h), 1024, 0, h->stream>>>(g); }, g.nslot);
       launched(h, "object update");
     }
     const int count = h->K * h->N * h->N;
@@ -718,7 +767,7 @@ void rpie_batch(ptyb_handle* h, const ptyb_rpie_params& p, const int* frames, in
   } else if (p.update_object) {
     g.alpha = (float)p.obj_alpha;
     g.step = (float)p.obj_step;
-    timed(h, kKObjRpie, [&] { object_tile_kernel<kGatherRpie><<<ntiles(h), 1024, 0, h->stream>>>(g); });
+    timed(h, kKObjRpie, [&] { object_tile_kernel<kGatherRpie><<<ntiles(h), 1024, 0, h->stream>>>(g); }, g.nslot);
     launched(h, "object update");
   }
 }
@@ -771,7 +820,7 @@ void lsqml_batch_slices(ptyb_handle* h, const ptyb_lsqml_params& p, const int* f
       g.probe = h->incident + (s - 1) * slice_stride;
       g.probe_stride = (int)fplanes;
     }
-    timed(h, kKObjLsqml, [&] { object_tile_kernel<kGatherLsqml><<<ntiles(h), 1024, 0, h->stream>>>(g); });
+    timed(h, kKObjLsqml, [&] { object_tile_kernel<kGatherLsqml><<<ntiles(h), 1024, 0, h->stream>>>(g); }, nslot);
     launched(h, "slice object direction");
   }
   // probe direction from χ of slice 0 through slice 0's windows (no phase when S > 1)
@@ -781,7 +830,7 @@ void lsqml_batch_slices(ptyb_handle* h, const ptyb_lsqml_params& p, const int* f
     lsqml_dots_kernel<<<nslot * kDotParts, 512, 0, h->stream>>>(
         h->object, h->d_obj, h->probe, h->d_probe, h->ones, h->chi_slices, frames, h->corners,
         h->nxo, h->K, h->N, lambda0, h->sums, 0);
-  });
+  }, nslot);
   launched(h, "step sums");
   const double scale = (double)(S * h->K);
   for (int s = 1; s < S; ++s) {
@@ -790,7 +839,7 @@ void lsqml_batch_slices(ptyb_handle* h, const ptyb_lsqml_params& p, const int* f
           h->d_obj + s * no, h->incident + (s - 1) * slice_stride,
           s + 1 == S ? h->quad : nullptr, h->chi_slices + s * slice_stride, frames, h->corners,
           h->nxo, h->K, h->N, h->slice_sums);
-    });
+    }, nslot);
     launched(h, "slice sums");
     timed(h, kKSolve, [&] {
       slice_solve_kernel<<<1, 1024, 0, h->stream>>>(h->slice_sums, nslot, scale, log + 2 + s,
@@ -827,8 +876,9 @@ void lsqml_batch(ptyb_handle* h, const ptyb_lsqml_params& p, const int* frames, 
   FrameArgs a = frame_args(h, frames);
   a.cost = p.cost;
   if (h->have_offsets) {
-    check(h, launch_move<kMoveProbe>(h, move_args(h, frames, h->wave), nslot), "probe move");
-    ++h->launches;
+    ensure_spec(h);
+    spectrum_of(h, h->probe, h->spec);
+    move_frames(h, frames, nslot, h->spec, h->wave);
     a.probe = h->wave;
     a.probe_stride = pstride;
   }
@@ -858,7 +908,7 @@ void lsqml_batch(ptyb_handle* h, const ptyb_lsqml_params& p, const int* frames, 
     g.probe = h->wave;
     g.probe_stride = pstride;
   }
-  timed(h, kKObjLsqml, [&] { object_tile_kernel<kGatherLsqml><<<ntiles(h), 1024, 0, h->stream>>>(g); });
+  timed(h, kKObjLsqml, [&] { object_tile_kernel<kGatherLsqml><<<ntiles(h), 1024, 0, h->stream>>>(g); }, nslot);
   launched(h, "object direction");
   if (h->have_offsets) {
     timed(h, kKProbePartial, [&] {
@@ -884,7 +934,7 @@ void lsqml_batch(ptyb_handle* h, const ptyb_lsqml_params& p, const int* frames, 
                                                      h->quad, h->upd, frames, h->corners,
                                                      h->nxo, h->K, h->N, lambda0, h->sums,
                                                      fstride);
-  });
+  }, nslot);
   launched(h, "step sums");
   const bool refine = h->have_offsets && h->refine_offsets;
   if (refine) {
@@ -894,7 +944,7 @@ void lsqml_batch(ptyb_handle* h, const ptyb_lsqml_params& p, const int* frames, 
     timed(h, kKPositionSums, [&] {
       position_sums_kernel<<<nslot, 256, 0, h->stream>>>(h->field, h->wave, pstride, h->quad,
                                                           h->upd, h->K, h->N, h->pos_sums);
-    });
+    }, nslot);
     launched(h, "position sums");
   }
   timed(h, kKSolve, [&] {
@@ -976,7 +1026,7 @@ cudaError_t launch_gamma(ptyb_handle* h, const GammaArgs& a, int nslot) {
       case 128: e = launch_gamma_nc<128, 4>(a, nslot, h->stream); break;
       case 256: e = launch_gamma_nc<256, 16>(a, nslot, h->stream); break;
     }
-  });
+  }, nslot);
   return e;
 }
 
@@ -1031,11 +1081,10 @@ void ml_gradients(ptyb_handle* h, bool uo, bool up) {
     const int n = std::min(stack, h->P - s0);
     const int* frames = h->iota + s0;
     FrameArgs a = frame_args(h, frames);
-    if (h->have_offsets) {
-      // each frame's moved probe W = T_d(q·P) in place of q·P (engine/ptycho.rs:373-450)
-      check(h, launch_move<kMoveProbe>(h, move_args(h, frames, h->wave), n), "probe move");
-      ++h->launches;
-      a.probe = h->wave;
+    const float2* waves = h->have_offsets ? h->wave_all + (size_t)s0 * pstride : nullptr;
+    if (waves) {
+      // each frame's moved probe conj(q)·T_d(q·P) in place of P (engine/ptycho.rs:373-450)
+      a.probe = waves;
       a.probe_stride = pstride;
     }
     check(h, launch_frame<kMlGrad>(h, a, n), "ml gradient pass");
@@ -1044,11 +1093,11 @@ void ml_gradients(ptyb_handle* h, bool uo, bool up) {
       GatherArgs g = gather_args(h, frames, n);
       g.out = h->g_obj;
       g.comp = h->g_obj_c;
-      if (h->have_offsets) {
-        g.probe = h->wave;
+      if (waves) {
+        g.probe = waves;
         g.probe_stride = pstride;
       }
-      timed(h, kKObjMl, [&] { object_tile_kernel<kGatherMl><<<ntiles(h), 1024, 0, h->stream>>>(g); });
+      timed(h, kKObjMl, [&] { object_tile_kernel<kGatherMl><<<ntiles(h), 1024, 0, h->stream>>>(g); }, n);
       launched(h, "object gradient");
     }
     if (up && h->have_offsets) {
@@ -1084,7 +1133,7 @@ void ml_gradients(ptyb_handle* h, bool uo, bool up) {
       pa.N = h->N;
       pa.mode = 1;
       dim3 grid((h->N * h->N + 255) / 256, nchunk);
-      timed(h, kKProbePartial, [&] { probe_partial_kernel<<<grid, 256, 0, h->stream>>>(pa); });
+      timed(h, kKProbePartial, [&] { probe_partial_kernel<<<grid, 256, 0, h->stream>>>(pa); }, pa.nslot);
       launched(h, "probe gradient");
       const int count = h->K * h->N * h->N;
       timed(h, kKProbeFinal, [&] {
@@ -1104,31 +1153,26 @@ void ml_position_sums(ptyb_handle* h) {
   for (int s0 = 0; s0 < h->P; s0 += stack) {
     const int n = std::min(stack, h->P - s0);
     const int* frames = h->iota + s0;
-    check(h, launch_move<kMoveProbe>(h, move_args(h, frames, h->wave), n), "probe move");
-    ++h->launches;
     FrameArgs a = frame_args(h, frames);
-    a.probe = h->wave;
+    a.probe = h->wave_all + (size_t)s0 * pstride;
     a.probe_stride = pstride;
     check(h, launch_frame<kProject>(h, a, n), "magnitude projection");
     ++h->launches;
-    for (int axis = 0; axis < 2; ++axis) {
-      MoveArgs md = move_args(h, frames, h->field);
-      md.axis = axis;
-      check(h, launch_move<kDerivProbe>(h, md, n), "wave derivative");
-      ++h->launches;
-      timed(h, kKPositionSums, [&] {
-        ml_position_sums_kernel<<<n, 256, 0, h->stream>>>(h->field, h->upd, h->object, frames,
-                                                           h->corners, h->nxo, h->K, h->N, axis,
-                                                           h->ml_pos_sums);
-      });
-      launched(h, "position sums");
-    }
+    // the moved wave's derivatives from the probe spectra, dotted with the change of the exit
+    // wave on chip
+    MoveArgs md = move_args(h, frames, nullptr);
+    md.spec = h->spec;
+    md.c = h->upd;
+    md.sums = h->ml_pos_sums;
+    check(h, launch_move<kDerivSums>(h, md, n), "position sums");
+    ++h->launches;
   }
 }
 
 // num and den of the Poisson line search along (dir_obj, dir_probe), frames summed in order.
 void ml_gamma(ptyb_handle* h, double* num, double* den) {
   const int stack = std::min(h->P, h->stack);
+  if (h->have_offsets) spectrum_of(h, h->dir_probe, h->spec_d);
   GammaArgs a = {};
   a.object = h->object;
   a.d_obj = h->dir_obj;
@@ -1148,13 +1192,8 @@ void ml_gamma(ptyb_handle* h, double* num, double* den) {
     a.out = h->gamma_sums + (size_t)s0 * 2;
     if (h->have_offsets) {
       // the probe and its direction, each moved by the frame's offset (engine/ptycho.rs:527-534)
-      check(h, launch_move<kMoveProbe>(h, move_args(h, a.frames, h->wave), n), "probe move");
-      ++h->launches;
-      MoveArgs md = move_args(h, a.frames, h->wave2);
-      md.probe = h->dir_probe;
-      check(h, launch_move<kMoveProbe>(h, md, n), "direction move");
-      ++h->launches;
-      a.probe = h->wave;
+      move_frames(h, a.frames, n, h->spec_d, h->wave2);
+      a.probe = h->wave_all + (size_t)s0 * h->K * h->N * h->N;
       a.d_probe = h->wave2;
       a.probe_stride = h->K * h->N * h->N;
     }
@@ -1639,6 +1678,10 @@ int ptyb_ml(ptyb_handle* h, const ptyb_ml_params* p, int32_t ncycle) {
       h->wave2_slots = h->slots;
     }
     if (refine && !h->ml_pos_sums) h->ml_pos_sums = alloc<double>(h, (size_t)h->P * 4);
+    if (h->have_offsets) {
+      ensure_spec(h);
+      if (!h->wave_all) h->wave_all = alloc<float2>(h, (size_t)h->P * h->K * h->N * h->N);
+    }
     const bool uo = p->update_object != 0, up = p->update_probe != 0;
     const size_t no = (size_t)h->nyo * h->nxo, np = (size_t)h->K * h->N * h->N;
     begin_call(h);
@@ -1648,8 +1691,16 @@ int ptyb_ml(ptyb_handle* h, const ptyb_ml_params* p, int32_t ncycle) {
     bool have_last = false;
     for (int ic = 0; ic < ncycle; ++ic) {
       const bool due = llk_due(p->calc_llk, ic, ncycle);
+      if (h->have_offsets) {
+        // every frame's moved probe for this cycle, from the probe's spectra
+        spectrum_of(h, h->probe, h->spec);
+        const int stack = std::min(h->P, h->stack);
+        for (int s0 = 0; s0 < h->P; s0 += stack)
+          move_frames(h, h->iota + s0, std::min(stack, h->P - s0), h->spec,
+                      h->wave_all + (size_t)s0 * h->K * h->N * h->N);
+      }
       ptyb_llk l = {};
-      if (due) l = llk_pass(h);
+      if (due) l = llk_pass(h, h->have_offsets ? h->wave_all : nullptr);
       if (refine) ml_position_sums(h);
       ml_gradients(h, uo, up);
       double beta = 0.0;
@@ -1945,6 +1996,7 @@ int ptyb_set_timing(ptyb_handle* h, int32_t on) {
     for (int k = 0; k < kNumKinds; ++k) {
       h->kind_ms[k] = 0.0;
       h->kind_n[k] = 0;
+      h->kind_frames[k] = 0;
     }
     return PTYB_OK;
   });
@@ -1962,6 +2014,12 @@ int ptyb_kernel_times(ptyb_handle* h, double* ms, int64_t* launches, int32_t cap
     ms[k] = h->kind_ms[k];
     launches[k] = h->kind_n[k];
   }
+  return PTYB_OK;
+}
+
+int ptyb_kernel_frames(ptyb_handle* h, int64_t* frames, int32_t cap) {
+  if (!h || !frames) return PTYB_INVALID;
+  for (int k = 0; k < std::min<int>(cap, kNumKinds); ++k) frames[k] = h->kind_frames[k];
   return PTYB_OK;
 }
 
@@ -2002,8 +2060,8 @@ void ptyb_destroy(ptyb_handle* h) {
   for (auto& b : h->bufs) cudaFree(b.p);
   for (auto e : h->event_pool) cudaEventDestroy(e);
   for (auto& p : h->pending) {
-    cudaEventDestroy(p.second.first);
-    cudaEventDestroy(p.second.second);
+    cudaEventDestroy(p.a);
+    cudaEventDestroy(p.b);
   }
   for (auto e : h->call_ev)
     if (e) cudaEventDestroy(e);

@@ -8,23 +8,27 @@
 namespace ptyb {
 
 enum MoveMode : int {
-  kMoveProbe = 0,  // planes[slot][m] = conj(q)·T_d(q·P_m)       (probe of frame f moved by d_f)
-  kMoveBack = 1,   // planes[slot][m] = conj(q)·T_{−d}(q·planes)  (the adjoint move, in place)
+  kMoveBack = 1,    // planes[slot][m] = conj(q)·T_{−d}(q·planes)  (the adjoint move, in place)
   kDerivWindow = 2, // planes[slot][a] = ∂_a O_window (periodic Fourier derivative), a = y, x
-  kDerivProbe = 3   // planes[slot][m] = ∂T_d(q·P_m)/∂d[axis]: the moved wave's derivative
+  kSpectrum = 4,    // planes[m] = DFT(q·P_m), unnormalised, [ky][kx] (one slot)
+  kFromSpectrum = 5,// planes[slot][m] = conj(q)·T_d(q·P_m), probe of frame f moved by d_f,
+                    // from the spectrum `spec`
+  kDerivSums = 6    // per frame and axis, the position sums of AP, DM and ML from ∂T_d(q·P)
 };
 
 struct MoveArgs {
-  const float2* probe;    // [K][N][N] shared probe (kMoveProbe)
+  const float2* probe;    // [K][N][N] shared probe (kSpectrum)
   const float2* quad;     // [N][N]
   const float2* tw;       // [N]
-  const float2* object;   // [nyo][nxo] (kDerivWindow)
+  const float2* object;   // [nyo][nxo] (kDerivWindow, kDerivSums)
   const int* frames;
   const int2* corners;
   const double* offsets;  // [nframe][2] (dy, dx) in object pixels
   float2* planes;         // [slot][K][N][N] natural layout
   int nxo, K;
-  int axis;               // kDerivProbe: 0 = dy, 1 = dx
+  const float2* spec;     // [K][N][N] DFT of q·P (kFromSpectrum, kDerivSums)
+  const float2* c;        // [slot][K][N][N] the projection's change of the exit wave (kDerivSums)
+  double* sums;           // [nframe][4] num_y, num_x, den_y, den_x (kDerivSums)
 };
 
 // numpy fftfreq of index k of n points (engine/features.rs:337-344).
@@ -37,86 +41,131 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T) move_kernel(MoveArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int K = MODE == kDerivWindow ? 2 : a.K;
   float2* S = reinterpret_cast<float2*>(smem_raw);
+  double* red = reinterpret_cast<double*>(S + (size_t)K * H * L + N);
   cg::cluster_group cluster = cg::this_cluster();
   const int r = C > 1 ? (int)cluster.block_rank() : 0;
   const int slot = blockIdx.x / C;
-  const int f = a.frames[slot];
-  const int2 corner = a.corners[f];
+  const int f = MODE == kSpectrum ? 0 : a.frames[slot];
+  const int2 corner = MODE == kSpectrum ? make_int2(0, 0) : a.corners[f];
   const int tid = threadIdx.x;
   LineTwiddles<N> ltw;
   ltw.load(a.tw, tid % F::G);
   const size_t plane = (size_t)N * N;
   float2* out = a.planes + (size_t)slot * K * plane;
-
-  // Natural-layout rows r·H .. r·H+H-1 of every plane.
-#pragma unroll 2
-  for (int idx = tid; idx < H * N; idx += T) {
-    const int yl = idx / N, x = idx % N, y = r * H + yl;
-    const float2 q = a.quad[y * N + x];
-    for (int m = 0; m < K; ++m) {
-      float2 v;
-      if (MODE == kMoveProbe || MODE == kDerivProbe)
-        v = cmul(q, a.probe[m * plane + y * N + x]);
-      else if (MODE == kMoveBack)
-        v = cmul(q, out[m * plane + y * N + x]);
-      else
-        v = a.object[(size_t)(corner.x + y) * a.nxo + corner.y + x];
-      const int line = m * H + yl;
-      S[line * L + (x ^ swz(line))] = v;
-    }
-  }
-  __syncthreads();
-  all_lines<N, C, -1>(S, K * H, ltw);
-  transpose<N, C>(S, K, cluster);
-  all_lines<N, C, -1>(S, K * H, ltw);
-
-  // Spectrum: column kx = r·H + c as line (m·H + c), element ky.
   constexpr float inv_n2 = 1.0f / ((float)N * (float)N);
+  constexpr bool from_spec = MODE == kFromSpectrum || MODE == kDerivSums;
+  constexpr bool bare = MODE == kDerivWindow;
+
   float dy = 0.f, dx = 0.f;
-  if (MODE != kDerivWindow) {
+  if (MODE != kDerivWindow && MODE != kSpectrum) {
     const float sgn = MODE == kMoveBack ? -1.f : 1.f;
     dy = sgn * (float)a.offsets[2 * f];
     dx = sgn * (float)a.offsets[2 * f + 1];
   }
+
+  if (!from_spec) {
+    // Natural-layout rows r·H .. r·H+H-1 of every plane.
 #pragma unroll 2
-  for (int idx = tid; idx < H * N; idx += T) {
-    const int c = idx % H, ky = idx / H;
-    const float fy = fft_freq(ky, N), fx = fft_freq(r * H + c, N);
-    float2 e;
-    if (MODE != kDerivWindow) {
-      float sn, cs;
-      sincospif(-2.f * (fy * dy + fx * dx), &sn, &cs);  // exp(−2πi f·d)
-      e = make_float2(cs * inv_n2, sn * inv_n2);
-      if (MODE == kDerivProbe) {
-        // × (−2πi·f_axis): the derivative of the translation phase (engine/features.rs:372-387)
-        const float w = 2.f * 3.14159265358979f * (a.axis == 0 ? fy : fx);
-        e = make_float2(w * e.y, -w * e.x);
+    for (int idx = tid; idx < H * N; idx += T) {
+      const int yl = idx / N, x = idx % N, y = r * H + yl;
+      const float2 q = a.quad[y * N + x];
+      for (int m = 0; m < K; ++m) {
+        float2 v;
+        if (MODE == kSpectrum)
+          v = cmul(q, a.probe[m * plane + y * N + x]);
+        else if (MODE == kMoveBack)
+          v = cmul(q, out[m * plane + y * N + x]);
+        else
+          v = a.object[(size_t)(corner.x + y) * a.nxo + corner.y + x];
+        const int line = m * H + yl;
+        S[line * L + (x ^ swz(line))] = v;
       }
     }
-    for (int m = 0; m < K; ++m) {
-      float2& v = S[(m * H + c) * L + (ky ^ swz(m * H + c))];
-      if (MODE == kDerivWindow) {
-        const float w = 2.f * 3.14159265358979f * (m == 0 ? fy : fx) * inv_n2;
-        v = make_float2(-w * v.y, w * v.x);  // × 2πi·f_axis
-      } else {
-        v = cmul(v, e);
+    __syncthreads();
+    all_lines<N, C, -1>(S, K * H, ltw);
+    transpose<N, C>(S, K, cluster);
+    all_lines<N, C, -1>(S, K * H, ltw);
+    if (MODE == kSpectrum) {
+      // Spectrum columns kx = r·H + c (lines m·H + c, elements ky) to [m][ky][kx].
+#pragma unroll 2
+      for (int idx = tid; idx < H * N; idx += T) {
+        const int c = idx % H, ky = idx / H;
+        for (int m = 0; m < K; ++m)
+          a.planes[((size_t)m * N + ky) * N + r * H + c] = S[(m * H + c) * L + (ky ^ swz(m * H + c))];
       }
+      return;
     }
   }
-  __syncthreads();
-  all_lines<N, C, +1>(S, K * H, ltw);
-  transpose<N, C>(S, K, cluster);
-  all_lines<N, C, +1>(S, K * H, ltw);
 
+  const int naxis = MODE == kDerivSums ? 2 : 1;
+  for (int ax = 0; ax < naxis; ++ax) {
+    const int axis = ax;
+    // Spectrum: column kx = r·H + c as line (m·H + c), element ky.
 #pragma unroll 2
-  for (int idx = tid; idx < H * N; idx += T) {
-    const int yl = idx / N, x = idx % N, y = r * H + yl;
-    constexpr bool bare = MODE == kDerivWindow || MODE == kDerivProbe;
-    const float2 cq = bare ? make_float2(1.f, 0.f) : cconj(a.quad[y * N + x]);
-    for (int m = 0; m < K; ++m) {
-      const int line = m * H + yl;
-      const float2 v = S[line * L + (x ^ swz(line))];
-      out[m * plane + y * N + x] = bare ? v : cmul(cq, v);
+    for (int idx = tid; idx < H * N; idx += T) {
+      const int c = idx % H, ky = idx / H, kx = r * H + c;
+      const float fy = fft_freq(ky, N), fx = fft_freq(kx, N);
+      float2 e;
+      if (MODE != kDerivWindow) {
+        float sn, cs;
+        sincospif(-2.f * (fy * dy + fx * dx), &sn, &cs);  // exp(−2πi f·d)
+        e = make_float2(cs * inv_n2, sn * inv_n2);
+        if (MODE == kDerivSums) {
+          // × (−2πi·f_axis): the derivative of the translation phase (engine/features.rs:372-387)
+          const float w = 2.f * 3.14159265358979f * (axis == 0 ? fy : fx);
+          e = make_float2(w * e.y, -w * e.x);
+        }
+      }
+      for (int m = 0; m < K; ++m) {
+        float2& v = S[(m * H + c) * L + (ky ^ swz(m * H + c))];
+        if (from_spec) {
+          v = cmul(a.spec[((size_t)m * N + ky) * N + kx], e);
+        } else if (MODE == kDerivWindow) {
+          const float w = 2.f * 3.14159265358979f * (m == 0 ? fy : fx) * inv_n2;
+          v = make_float2(-w * v.y, w * v.x);  // × 2πi·f_axis
+        } else {
+          v = cmul(v, e);
+        }
+      }
+    }
+    __syncthreads();
+    all_lines<N, C, +1>(S, K * H, ltw);
+    transpose<N, C>(S, K, cluster);
+    all_lines<N, C, +1>(S, K * H, ltw);
+
+    if (MODE != kDerivSums) {
+#pragma unroll 2
+      for (int idx = tid; idx < H * N; idx += T) {
+        const int yl = idx / N, x = idx % N, y = r * H + yl;
+        const float2 cq = bare ? make_float2(1.f, 0.f) : cconj(a.quad[y * N + x]);
+        for (int m = 0; m < K; ++m) {
+          const int line = m * H + yl;
+          const float2 v = S[line * L + (x ^ swz(line))];
+          out[m * plane + y * N + x] = bare ? v : cmul(cq, v);
+        }
+      }
+    } else {
+      // dψ = O·∂W on natural rows; num = Σ Re(conj(c)·dψ), den = Σ |dψ|² over modes and pixels
+      // (engine/features.rs:992-1025), cluster-summed in rank order.
+      double num = 0.0, den = 0.0;
+      const float2* cf = a.c + (size_t)slot * K * plane;
+#pragma unroll 2
+      for (int idx = tid; idx < H * N; idx += T) {
+        const int yl = idx / N, x = idx % N, y = r * H + yl;
+        const float2 o = a.object[(size_t)(corner.x + y) * a.nxo + corner.y + x];
+        for (int m = 0; m < K; ++m) {
+          const int line = m * H + yl;
+          const float2 d = cmul(o, S[line * L + (x ^ swz(line))]);
+          const float2 v = cf[m * plane + y * N + x];
+          num += (double)v.x * d.x + (double)v.y * d.y;
+          den += (double)d.x * d.x + (double)d.y * d.y;
+        }
+      }
+      cluster_sum2<N, C>(num, den, red, cluster);
+      if (r == 0 && tid == 0) {
+        a.sums[(size_t)f * 4 + axis] = num;
+        a.sums[(size_t)f * 4 + 2 + axis] = den;
+      }
     }
   }
 }
@@ -199,51 +248,6 @@ __global__ void position_step_kernel(const double* sums, int nslot, int nframe, 
       const double dx = 0.3 * (sums[s * 4 + a] / (sums[s * 4 + 2 + a] + mx));
       offsets[2 * frames[s] + a] += fmin(fmax(dx, -limit), limit);
     }
-  }
-}
-
-// Per slot, one axis of the position sums of AP, DM and ML (engine/features.rs:992-1025):
-// with c = x − O·W the magnitude projection's change of the exit wave and dψ = O·∂W/∂d[axis],
-// num = Σ Re(conj(c)·dψ), den = Σ |dψ|² over the frame's modes and pixels, in double, into
-// sums[frame][axis] (num) and sums[frame][2 + axis] (den).
-__global__ void __launch_bounds__(256) ml_position_sums_kernel(const float2* dwave,
-                                                              const float2* c,
-                                                              const float2* object,
-                                                              const int* frames,
-                                                              const int2* corners, int nxo,
-                                                              int K, int N, int axis,
-                                                              double* sums) {
-  __shared__ double sh[16];
-  const int slot = blockIdx.x;
-  const int f = frames[slot];
-  const int2 cn = corners[f];
-  const size_t plane = (size_t)N * N;
-  double num = 0.0, den = 0.0;
-  for (int pix = threadIdx.x; pix < N * N; pix += 256) {
-    const int y = pix / N, x = pix % N;
-    const float2 o = object[(size_t)(cn.x + y) * nxo + cn.y + x];
-    for (int m = 0; m < K; ++m) {
-      const size_t i = ((size_t)slot * K + m) * plane + pix;
-      const float2 d = cmul(o, dwave[i]), v = c[i];
-      num += (double)v.x * d.x + (double)v.y * d.y;
-      den += (double)d.x * d.x + (double)d.y * d.y;
-    }
-  }
-  num = warp_sum(num);
-  den = warp_sum(den);
-  if (threadIdx.x % 32 == 0) {
-    sh[threadIdx.x / 32] = num;
-    sh[8 + threadIdx.x / 32] = den;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double a = 0.0, b = 0.0;
-    for (int w = 0; w < 8; ++w) {
-      a += sh[w];
-      b += sh[8 + w];
-    }
-    sums[(size_t)f * 4 + axis] = a;
-    sums[(size_t)f * 4 + 2 + axis] = b;
   }
 }
 

@@ -267,6 +267,14 @@ class GpuPtycho:
         self._check(self._lib.ptyb_kernel_times(self._h, ms, n, k))
         return {self._lib.ptyb_kernel_name(i).decode(): (ms[i], n[i]) for i in range(k) if n[i]}
 
+    def kernel_frames(self):
+        """`{kernel: frames}` the launches timed since `set_timing` processed (per-frame
+        kernels only)."""
+        k = self._lib.ptyb_kernel_kinds()
+        f = (ctypes.c_int64 * k)()
+        self._check(self._lib.ptyb_kernel_frames(self._h, f, k))
+        return {self._lib.ptyb_kernel_name(i).decode(): f[i] for i in range(k) if f[i]}
+
     def last_call_ms(self):
         """Device time of the last algorithm call (CUDA events on the engine's stream)."""
         return float(self._lib.ptyb_last_call_ms(self._h))

@@ -98,15 +98,54 @@ def far_field_counts(obj, probe, corner, photons, seed, chunk=64):
     return rng.poisson(inten).astype(np.float32)
 
 
+def far_field_counts_gpu(obj, probe, corner, offsets, photons, seed, chunk=128,
+                         device=None):
+    """`far_field_counts` on a CUDA device with torch (data generation only), each frame's
+    probe modes moved by its sub-pixel offset `offsets[f]` (dy, dx px) on the periodic frame
+    grid before the window multiplies them: the Patch model of the position feature. Counts
+    `[P, n, n]` float32, detector order, Poisson-sampled from the seed."""
+    import torch
+    if device is None:
+        device = "cuda" if torch.cuda.is_available() else "cpu"
+    n = probe.shape[-1]
+    P = len(corner)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(int(seed))
+    o = torch.as_tensor(obj[0], dtype=torch.complex64, device=device)
+    pr = torch.as_tensor(probe, dtype=torch.complex64, device=device)
+    spec = torch.fft.fft2(pr)
+    f = torch.fft.fftfreq(n, device=device, dtype=torch.float64)
+    d = torch.as_tensor(offsets, dtype=torch.float64, device=device)
+    iy = torch.arange(n, device=device)
+    inten = torch.empty((P, n, n), dtype=torch.float32, device=device)
+    for s0 in range(0, P, chunk):
+        cs = torch.as_tensor(corner[s0:s0 + chunk], device=device)
+        m = len(cs)
+        rows = (cs[:, 0, None] + iy[None]).reshape(m, n, 1)
+        cols = (cs[:, 1, None] + iy[None]).reshape(m, 1, n)
+        win = o[rows, cols]
+        ph = -2.0 * np.pi * (f[None, :, None] * d[s0:s0 + m, 0, None, None]
+                             + f[None, None, :] * d[s0:s0 + m, 1, None, None])
+        ramp = torch.polar(torch.ones_like(ph), ph).to(torch.complex64)
+        moved = torch.fft.ifft2(spec[None] * ramp[:, None])
+        far = torch.fft.fft2(moved * win[:, None], norm="ortho")
+        inten[s0:s0 + m] = torch.fft.fftshift((far.abs() ** 2).sum(dim=1), dim=(-2, -1))
+    inten *= photons / inten.sum(dim=(1, 2)).mean()
+    counts = torch.poisson(inten, generator=gen)
+    return counts.cpu().numpy()
+
+
 def make_scan(kind, seed=0, scale=1.0):
     """Seeded synthetic inputs of a benchmark configuration: returns a dict with counts
     (float32), y, x (metres), object start, probe start, truth object and sizes.
 
     kind "rpie64": 256² object, 64² aperture probe, 20×20 raster of 8 px ±1 px, 1e5 photons.
     kind "lsqml128": 1024² object, 128² probe with 3 modes (0.8/0.15/0.05), Fermat 4096 at
-    6 px, 1e6 photons. kind "ml256": 2048² object, 256² probe with 2 modes, Fermat 10000 at
-    12 px, 1e7 photons. `scale` < 1 keeps that fraction of the positions (the same first ones)
-    for small cases.
+    6 px, 1e6 photons. kind "ml256": 2048² object, 256² probe with 2 modes (0.8/0.2), Fermat
+    10000 at 12 px, 1e7 photons, the frames taken at true positions off the nominal ones by
+    seeded N(0, 1.5 px) offsets (`true_offsets`; the solver is given the nominal positions),
+    counts generated on the CUDA device. `scale` < 1 keeps that fraction of the positions (the
+    same first ones) for small cases.
     """
     if kind == "rpie64":
         n, side, modes, photons = 64, 256, [1.0], 1e5
@@ -124,9 +163,14 @@ def make_scan(kind, seed=0, scale=1.0):
     truth = smooth_object(side, seed + 2)
     probe = hermite_probe(n, n / 4.0, modes) if len(modes) > 1 else aperture_probe(n, n / 4.0)[None] * 30.0
     c = corners(pos, n, side)
-    counts = far_field_counts(truth, probe, c, photons, seed + 3)
+    true_offsets = np.zeros((len(pos), 2))
+    if kind == "ml256":
+        true_offsets = np.random.default_rng(seed + 4).normal(0.0, 1.5, (len(pos), 2))
+        counts = far_field_counts_gpu(truth, probe, c, true_offsets, photons, seed + 3)
+    else:
+        counts = far_field_counts(truth, probe, c, photons, seed + 3)
     px = object_pixel(n)
     start = np.ones_like(truth)
     return dict(counts=counts, y=pos[:, 0] * px, x=pos[:, 1] * px, object=start, probe=probe,
                 truth=truth, corners=c, n=n, side=side, wavelength=WAVELENGTH,
-                distance=DISTANCE, detector_pixel=DETECTOR_PIXEL)
+                distance=DISTANCE, detector_pixel=DETECTOR_PIXEL, true_offsets=true_offsets)
