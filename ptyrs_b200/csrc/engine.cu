@@ -145,6 +145,7 @@ struct ptyb_handle {
   double* pos_sums = nullptr;    // [slots][4]
   // Multislice (pty-chi's multislice object, LSQML only): slices, gap transfer functions, the
   // incident waves of slices 1.., every slice's χ, a plane of ones (slices without a phase).
+  int C_sums = 1;                // CTAs per frame of the position-sums transform
   int nslice = 1;
   float2* tf = nullptr;          // [nslice-1][N][N]
   float2* incident = nullptr;    // [nslice-1][slots][K][N][N]
@@ -161,6 +162,10 @@ struct ptyb_handle {
   float2* spec = nullptr;        // [K][N][N]
   float2* spec_d = nullptr;      // [K][N][N]
   float2* wave_all = nullptr;    // [P][K][N][N]
+  // ML: every frame's detector field of one cycle's gradient pass, [P][K][kx][ky], and the
+  // probe gradient's summed spectrum under the position model.
+  float2* psi_all = nullptr;
+  float2* g_probe_spec = nullptr; // [K][N][N]
   double* partials = nullptr;    // [kPartialBlocks][2]
   std::vector<Buf> bufs;
   // Per-kernel device timing (CUDA events on the engine's stream), when enabled.
@@ -415,9 +420,10 @@ cudaError_t launch_move(ptyb_handle* h, const MoveArgs& a, int nslot) {
   if (nslot <= 0) return cudaSuccess;
   const int K = MODE == kDerivWindow ? 2 : h->K;
   constexpr int kind = MODE == kDerivSums ? kKDerivSums : MODE == kSpectrum ? kKSpectrum : kKMove;
+  const int C = MODE == kDerivSums ? h->C_sums : h->C;
   cudaError_t e = cudaErrorInvalidValue;
   timed(h, kind, [&] {
-    switch (h->N * 100 + h->C) {
+    switch (h->N * 100 + C) {
       case 6401: e = launch_move_nc<64, 1, MODE>(a, nslot, K, h->stream); break;
       case 12802: e = launch_move_nc<128, 2, MODE>(a, nslot, K, h->stream); break;
       case 12804: e = launch_move_nc<128, 4, MODE>(a, nslot, K, h->stream); break;
@@ -1042,6 +1048,8 @@ void ensure_ml(ptyb_handle* h) {
   h->last_probe = alloc<float2>(h, np);
   h->dir_probe = alloc<float2>(h, np);
   h->gamma_sums = alloc<double>(h, (size_t)h->P * 2);
+  h->psi_all = alloc<float2>(h, (size_t)h->P * np);
+  h->g_probe_spec = alloc<float2>(h, np);
   h->partials = alloc<double>(h, kPartialBlocks * 2);
 }
 
@@ -1068,13 +1076,19 @@ unsigned blocks_for(size_t n) { return (unsigned)((n + 255) / 256); }
 
 // The Poisson gradient numerators of object and probe over every frame, by stacks in frame
 // order (engine/ptycho.rs:497-561).
-void ml_gradients(ptyb_handle* h, bool uo, bool up) {
+// The Poisson gradients of the object and the probe (engine/ptycho.rs:497-569) from one
+// detector field per frame, which is kept for the line search; with `refine`, the position
+// sums of AP, DM and ML from the magnitude projection of the same field (engine/ptycho.rs:
+// 470-480, engine/features.rs:992-1025). Under the position model the probe gradient goes
+// back through the move's adjoint in the spectrum, frame by frame (features.rs:897-957).
+void ml_gradients(ptyb_handle* h, bool uo, bool up, bool refine) {
   const size_t no = (size_t)h->nyo * h->nxo, np = (size_t)h->K * h->N * h->N;
   check(h, cudaMemsetAsync(h->g_obj, 0, no * sizeof(float2), h->stream), "memset");
   check(h, cudaMemsetAsync(h->g_obj_c, 0, no * sizeof(float2), h->stream), "memset");
   check(h, cudaMemsetAsync(h->g_probe, 0, np * sizeof(float2), h->stream), "memset");
   check(h, cudaMemsetAsync(h->g_probe_c, 0, np * sizeof(float2), h->stream), "memset");
-  if (!uo && !up) return;
+  if (h->have_offsets)
+    check(h, cudaMemsetAsync(h->g_probe_spec, 0, np * sizeof(float2), h->stream), "memset");
   const int stack = std::min(h->P, h->stack);
   const int pstride = h->K * h->N * h->N;
   for (int s0 = 0; s0 < h->P; s0 += stack) {
@@ -1087,6 +1101,8 @@ void ml_gradients(ptyb_handle* h, bool uo, bool up) {
       a.probe = waves;
       a.probe_stride = pstride;
     }
+    a.psi_out = h->psi_all + (size_t)s0 * pstride;
+    a.proj_out = refine ? h->field : nullptr;
     check(h, launch_frame<kMlGrad>(h, a, n), "ml gradient pass");
     ++h->launches;
     if (uo) {
@@ -1101,19 +1117,15 @@ void ml_gradients(ptyb_handle* h, bool uo, bool up) {
       launched(h, "object gradient");
     }
     if (up && h->have_offsets) {
-      // conj(q·O_win)·g per frame, moved back by −d, summed in frame order
-      // (engine/features.rs:897-957)
-      timed(h, kKProbePartial, [&] {
-        probe_terms_kernel<<<dim3((h->N * h->N + 255) / 256, n), 256, 0, h->stream>>>(
-            h->object, h->quad, h->upd, frames, h->corners, h->nxo, h->K, h->N, h->field);
-      });
-      launched(h, "probe gradient terms");
-      check(h, launch_move<kMoveBack>(h, move_args(h, frames, h->field), n), "probe move back");
+      // DFT(conj(O_win)·g)·exp(+2πi f·d) per frame, summed in frame order
+      MoveArgs mb = move_args(h, frames, h->wave2);
+      mb.c = h->upd;
+      check(h, launch_move<kBackSpectrum>(h, mb, n), "probe gradient spectra");
       ++h->launches;
       timed(h, kKProbeFinal, [&] {
         probe_finalize_kernel<<<(pstride + 255) / 256, 256, 0, h->stream>>>(
-            h->field, n, pstride, nullptr, h->g_probe, h->g_probe_c, 1.f, 2);
-      });
+            h->wave2, n, pstride, nullptr, h->g_probe_spec, h->g_probe_c, 1.f, 2);
+      }, n);
       launched(h, "probe gradient sum");
     } else if (up) {
       int nchunk = 0;
@@ -1142,29 +1154,22 @@ void ml_gradients(ptyb_handle* h, bool uo, bool up) {
       });
       launched(h, "probe gradient sum");
     }
+    if (refine) {
+      // the moved wave's derivatives from the probe spectra, dotted with the projection's
+      // change of the exit wave on chip
+      MoveArgs md = move_args(h, frames, nullptr);
+      md.spec = h->spec;
+      md.c = h->field;
+      md.sums = h->ml_pos_sums;
+      check(h, launch_move<kDerivSums>(h, md, n), "position sums");
+      ++h->launches;
+    }
   }
-}
-
-// Every frame's position sums from the magnitude projection of the current estimate under
-// the position model (engine/ptycho.rs:470-480, engine/features.rs:992-1025).
-void ml_position_sums(ptyb_handle* h) {
-  const int stack = std::min(h->P, h->stack);
-  const int pstride = h->K * h->N * h->N;
-  for (int s0 = 0; s0 < h->P; s0 += stack) {
-    const int n = std::min(stack, h->P - s0);
-    const int* frames = h->iota + s0;
-    FrameArgs a = frame_args(h, frames);
-    a.probe = h->wave_all + (size_t)s0 * pstride;
-    a.probe_stride = pstride;
-    check(h, launch_frame<kProject>(h, a, n), "magnitude projection");
-    ++h->launches;
-    // the moved wave's derivatives from the probe spectra, dotted with the change of the exit
-    // wave on chip
-    MoveArgs md = move_args(h, frames, nullptr);
-    md.spec = h->spec;
-    md.c = h->upd;
-    md.sums = h->ml_pos_sums;
-    check(h, launch_move<kDerivSums>(h, md, n), "position sums");
+  if (up && h->have_offsets) {
+    // num = conj(q)·IDFT(Σ_f spectra)
+    MoveArgs mi = move_args(h, h->iota, h->g_probe);
+    mi.spec = h->g_probe_spec;
+    check(h, launch_move<kPlainInverse>(h, mi, 1), "probe gradient");
     ++h->launches;
   }
 }
@@ -1190,6 +1195,7 @@ void ml_gamma(ptyb_handle* h, double* num, double* den) {
     const int n = std::min(stack, h->P - s0);
     a.frames = h->iota + s0;
     a.out = h->gamma_sums + (size_t)s0 * 2;
+    a.psi = h->psi_all + (size_t)s0 * h->K * h->N * h->N;
     if (h->have_offsets) {
       // the probe and its direction, each moved by the frame's offset (engine/ptycho.rs:527-534)
       move_frames(h, a.frames, n, h->spec_d, h->wave2);
@@ -1385,7 +1391,12 @@ int create_handle(const ptyb_scan* scan, const double* object, int32_t nobj, int
   h->nyo = nyo;
   h->nxo = nxo;
   h->C = C;
-  h->stack = options && options->stack_size > 0 ? options->stack_size : 64;
+  // The position sums reduce over the whole cluster twice per frame: at side 256 they run on
+  // clusters of 8 (measured faster than 16) when the engine chooses.
+  h->C_sums = C;
+  if (N == 256 && !(options && options->cluster) && frame_smem_bytes<256, 8>(K) <= 227 * 1024)
+    h->C_sums = 8;
+  h->stack = options && options->stack_size > 0 ? options->stack_size : 512;
   h->nslice = nslice;
   h->log_stride = 2 + nslice;
   // Positions: PyNX preprocessing and window corners (base/positions.rs, base/addr.rs).
@@ -1701,8 +1712,7 @@ int ptyb_ml(ptyb_handle* h, const ptyb_ml_params* p, int32_t ncycle) {
       }
       ptyb_llk l = {};
       if (due) l = llk_pass(h, h->have_offsets ? h->wave_all : nullptr);
-      if (refine) ml_position_sums(h);
-      ml_gradients(h, uo, up);
+      ml_gradients(h, uo, up, refine);
       double beta = 0.0;
       if (have_last) {
         double a[2], b[2];

@@ -62,6 +62,12 @@ struct FrameArgs {
   // Elements between consecutive slots' probes: 0 for the shared probe, K·N·N for the
   // per-frame (moved) probes of the position model.
   int probe_stride;
+  // kMlGrad, optional: the detector field Ψ = DFT(P·O·q) of every mode kept for the line
+  // search, [slot][K][kx][ky] (columns contiguous); and the magnitude projection's change of
+  // the exit wave ψ' − ψ, ψ' = IDFT(√I/max(√Ĩ, 1e-12)·Ψ) (masked kept), [slot][K][N][N]
+  // natural, which needs psi_out.
+  float2* psi_out;
+  float2* proj_out;
 };
 
 template <int N, int C>
@@ -257,6 +263,16 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T)
     all_lines<N, C, -1>(S, K * H, ltw);
   }
 
+  if (MODE == kMlGrad && a.psi_out) {
+    // Ψ of this CTA's columns to [slot][m][kx][ky]
+    float2* dst = a.psi_out + (size_t)slot * K * N * N;
+#pragma unroll 8
+    for (int idx = tid; idx < K * H * N; idx += T) {
+      const int line = idx / N, e = idx % N, m = line / H, c = line % H;
+      dst[((size_t)m * N + r * H + c) * N + e] = S[line * L + (e ^ swz(line))];
+    }
+  }
+
   // Detector plane: CTA r holds columns r·H .. r·H+H-1 as lines (m·H + c), elements ky.
   // Unnormalised transforms: Ψ_ortho = S/N, and the inverse of the update takes a 1/N more.
   constexpr float inv_n = 1.0f / N;
@@ -372,29 +388,64 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T)
   transpose<N, C>(S, K, cluster);
   all_lines<N, C, +1>(S, K * H, ltw);
 
-  // Epilogue on shifted rows: out = ψ' − ψ (or ψ'), natural layout; the object window and the
+  // Epilogue on shifted rows: dst = ψ' − ψ (or ψ'), natural layout; the object window and the
   // phase are read once per pixel.
-  float2* out = a.out + (size_t)slot * K * N * N;
+  auto epilogue = [&](float2* base, bool subtract) {
+    float2* dst = base + (size_t)slot * K * N * N;
 #pragma unroll 2
-  for (int idx = tid; idx < H * N; idx += T) {
-    const int yl = idx / N, jx = idx % N;
-    const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
-    float2 q = make_float2(0.f, 0.f);
-    if (MODE != kMlGrad) q = a.quad[ny * N + nx];
-    for (int om = 0; om < a.nobj; ++om) {
-      float2 oq = make_float2(0.f, 0.f);
-      if (MODE != kMlGrad)
-        oq = cmul(a.object[((size_t)om * a.nyo + corner.x + ny) * a.nxo + corner.y + nx], q);
-      for (int pm = 0; pm < a.nprobe; ++pm) {
-        const int m = om * a.nprobe + pm;
-        const int line = m * H + yl;
-        float2 v = S[line * L + (jx ^ swz(line))];
-        if (MODE != kMlGrad)
-          v = csub(v, cmul(a.probe[(size_t)slot * a.probe_stride + ((size_t)pm * N + ny) * N + nx],
-                           oq));
-        out[((size_t)m * N + ny) * N + nx] = v;
+    for (int idx = tid; idx < H * N; idx += T) {
+      const int yl = idx / N, jx = idx % N;
+      const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
+      float2 q = make_float2(0.f, 0.f);
+      if (subtract) q = a.quad[ny * N + nx];
+      for (int om = 0; om < a.nobj; ++om) {
+        float2 oq = make_float2(0.f, 0.f);
+        if (subtract)
+          oq = cmul(a.object[((size_t)om * a.nyo + corner.x + ny) * a.nxo + corner.y + nx], q);
+        for (int pm = 0; pm < a.nprobe; ++pm) {
+          const int m = om * a.nprobe + pm;
+          const int line = m * H + yl;
+          float2 v = S[line * L + (jx ^ swz(line))];
+          if (subtract)
+            v = csub(v, cmul(a.probe[(size_t)slot * a.probe_stride + ((size_t)pm * N + ny) * N + nx],
+                             oq));
+          dst[((size_t)m * N + ny) * N + nx] = v;
+        }
       }
     }
+  };
+  epilogue(a.out, MODE != kMlGrad);
+
+  if (MODE == kMlGrad && a.proj_out) {
+    // The magnitude projection of the same Ψ (ApplyAmplitude, engine/ops.rs:83-107), reloaded
+    // from psi_out: ψ' − ψ to proj_out.
+    __syncthreads();
+    const float2* src = a.psi_out + (size_t)slot * K * N * N;
+#pragma unroll 8
+    for (int idx = tid; idx < K * H * N; idx += T) {
+      const int line = idx / N, e = idx % N, m = line / H, c = line % H;
+      S[line * L + (e ^ swz(line))] = src[((size_t)m * N + r * H + c) * N + e];
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int i = 0; i < kPixPerThread; ++i) {
+      const int idx = tid + i * T;
+      const int c = idx % H, ky = idx / H;
+      const float yo = iobs[ky * N + r * H + c];
+      float ic = 0.f;
+      for (int m = 0; m < K; ++m) ic += cnorm2(S[(m * H + c) * L + (ky ^ swz(m * H + c))]);
+      ic *= inv_n2;
+      const float fac = (yo < 0.f ? 1.f : sqrtf(yo) / fmaxf(sqrtf(ic), 1e-12f)) * inv_n2;
+      for (int m = 0; m < K; ++m) {
+        float2& v = S[(m * H + c) * L + (ky ^ swz(m * H + c))];
+        v = cscale(v, fac);
+      }
+    }
+    __syncthreads();
+    all_lines<N, C, +1>(S, K * H, ltw);
+    transpose<N, C>(S, K, cluster);
+    all_lines<N, C, +1>(S, K * H, ltw);
+    epilogue(a.proj_out, true);
   }
 }
 

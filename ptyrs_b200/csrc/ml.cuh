@@ -26,6 +26,9 @@ struct GammaArgs {
   // Elements between consecutive slots' probe and probe direction: 0 for the shared ones,
   // K·N·N for the per-frame moved ones of the position model.
   int probe_stride;
+  // Optional: po = DFT(P·O·q) of every slot and mode as the gradient pass kept it,
+  // [slot][K][kx][ky]; null computes it here.
+  const float2* psi;
 };
 
 template <int N, int C>
@@ -70,13 +73,27 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T) gamma_kernel(GammaArgs a)
       const float2 p = a.probe[pi], dp = a.d_probe[pi];
       const float2 o = a.object[oi], dob = a.d_obj[oi];
       const float2 q = a.quad[ny * N + nx];
-      S0[yl * L + (jx ^ swz(yl))] = cmul(cmul(p, o), q);
+      if (!a.psi) S0[yl * L + (jx ^ swz(yl))] = cmul(cmul(p, o), q);
       S1[yl * L + (jx ^ swz(yl))] = cmul(cadd(cmul(p, dob), cmul(dp, o)), q);
     }
-    __syncthreads();
-    all_lines<N, C, -1>(S0, 2 * H, ltw);  // both planes: lines 0..2H-1 (S1 follows S0)
-    transpose<N, C>(S0, 2, cluster);
-    all_lines<N, C, -1>(S0, 2 * H, ltw);
+    if (a.psi) {
+      // po of this CTA's columns, kept by the gradient pass
+      const float2* src = a.psi + ((size_t)slot * K + m) * N * N;
+#pragma unroll 4
+      for (int idx = tid; idx < H * N; idx += T) {
+        const int c = idx / N, e = idx % N;
+        S0[c * L + (e ^ swz(c))] = src[(size_t)(r * H + c) * N + e];
+      }
+      __syncthreads();
+      all_lines<N, C, -1>(S1, H, ltw);
+      transpose<N, C>(S1, 1, cluster);
+      all_lines<N, C, -1>(S1, H, ltw);
+    } else {
+      __syncthreads();
+      all_lines<N, C, -1>(S0, 2 * H, ltw);  // both planes: lines 0..2H-1 (S1 follows S0)
+      transpose<N, C>(S0, 2, cluster);
+      all_lines<N, C, -1>(S0, 2 * H, ltw);
+    }
 #pragma unroll 4
     for (int idx = tid; idx < H * N; idx += T) {
       const int c = idx % H, ky = idx / H;

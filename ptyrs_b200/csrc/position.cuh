@@ -8,26 +8,31 @@
 namespace ptyb {
 
 enum MoveMode : int {
-  kMoveBack = 1,    // planes[slot][m] = conj(q)·T_{−d}(q·planes)  (the adjoint move, in place)
-  kDerivWindow = 2, // planes[slot][a] = ∂_a O_window (periodic Fourier derivative), a = y, x
-  kSpectrum = 4,    // planes[m] = DFT(q·P_m), unnormalised, [ky][kx] (one slot)
-  kFromSpectrum = 5,// planes[slot][m] = conj(q)·T_d(q·P_m), probe of frame f moved by d_f,
-                    // from the spectrum `spec`
-  kDerivSums = 6    // per frame and axis, the position sums of AP, DM and ML from ∂T_d(q·P)
+  kMoveBack = 1,      // planes[slot][m] = conj(q)·T_{−d}(q·planes)  (the adjoint move, in place)
+  kDerivWindow = 2,   // planes[slot][a] = ∂_a O_window (periodic Fourier derivative), a = y, x
+  kSpectrum = 4,      // planes[m] = DFT(q·P_m), unnormalised, [ky][kx] (one slot)
+  kFromSpectrum = 5,  // planes[slot][m] = conj(q)·T_d(q·P_m), probe of frame f moved by d_f,
+                      // from the spectrum `spec`
+  kDerivSums = 6,     // per frame and axis, the position sums of AP, DM and ML from ∂T_d(q·P)
+  kBackSpectrum = 7,  // planes[slot][m] = DFT(conj(O_win)·c_m)·exp(+2πi f·d)/N², [ky][kx]: one
+                      // frame's term of the probe back-projection through the move's adjoint
+  kPlainInverse = 8   // planes[m] = conj(q)·IDFT(spec_m), unnormalised (one slot)
 };
 
 struct MoveArgs {
   const float2* probe;    // [K][N][N] shared probe (kSpectrum)
   const float2* quad;     // [N][N]
   const float2* tw;       // [N]
-  const float2* object;   // [nyo][nxo] (kDerivWindow, kDerivSums)
+  const float2* object;   // [nyo][nxo] (kDerivWindow, kDerivSums, kBackSpectrum)
   const int* frames;
   const int2* corners;
   const double* offsets;  // [nframe][2] (dy, dx) in object pixels
-  float2* planes;         // [slot][K][N][N] natural layout
+  float2* planes;         // [slot][K][N][N]
   int nxo, K;
-  const float2* spec;     // [K][N][N] DFT of q·P (kFromSpectrum, kDerivSums)
-  const float2* c;        // [slot][K][N][N] the projection's change of the exit wave (kDerivSums)
+  const float2* spec;     // [K][N][N] a spectrum, [ky][kx] (kFromSpectrum, kDerivSums,
+                          // kPlainInverse)
+  const float2* c;        // [slot][K][N][N] natural: the change of the exit wave (kDerivSums),
+                          // the exit-plane gradient (kBackSpectrum)
   double* sums;           // [nframe][4] num_y, num_x, den_y, den_x (kDerivSums)
 };
 
@@ -45,36 +50,60 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T) move_kernel(MoveArgs a) {
   cg::cluster_group cluster = cg::this_cluster();
   const int r = C > 1 ? (int)cluster.block_rank() : 0;
   const int slot = blockIdx.x / C;
-  const int f = MODE == kSpectrum ? 0 : a.frames[slot];
-  const int2 corner = MODE == kSpectrum ? make_int2(0, 0) : a.corners[f];
+  constexpr bool one = MODE == kSpectrum || MODE == kPlainInverse;  // not per frame
+  const int f = one ? 0 : a.frames[slot];
+  const int2 corner = one ? make_int2(0, 0) : a.corners[f];
   const int tid = threadIdx.x;
   LineTwiddles<N> ltw;
   ltw.load(a.tw, tid % F::G);
   const size_t plane = (size_t)N * N;
   float2* out = a.planes + (size_t)slot * K * plane;
   constexpr float inv_n2 = 1.0f / ((float)N * (float)N);
-  constexpr bool from_spec = MODE == kFromSpectrum || MODE == kDerivSums;
+  constexpr bool from_spec = MODE == kFromSpectrum || MODE == kDerivSums || MODE == kPlainInverse;
+  constexpr bool moves = MODE == kMoveBack || MODE == kFromSpectrum || MODE == kDerivSums ||
+                         MODE == kBackSpectrum;
   constexpr bool bare = MODE == kDerivWindow;
 
   float dy = 0.f, dx = 0.f;
-  if (MODE != kDerivWindow && MODE != kSpectrum) {
-    const float sgn = MODE == kMoveBack ? -1.f : 1.f;
+  if (moves) {
+    const float sgn = MODE == kMoveBack || MODE == kBackSpectrum ? -1.f : 1.f;
     dy = sgn * (float)a.offsets[2 * f];
     dx = sgn * (float)a.offsets[2 * f + 1];
   }
+  // The translation phase exp(−2πi f·d) = exp(−2πi fy·dy)·exp(−2πi fx·dx), over N²: the row
+  // factor for every ky in the free N-entry region after the planes, the column factor of this
+  // thread's one column (T is a multiple of H, so a thread keeps c = tid % H).
+  float2* ey = S + (size_t)K * H * L;
+  float2 ex = make_float2(1.f, 0.f);
+  if (moves) {
+    for (int k = tid; k < N; k += T) {
+      float sn, cs;
+      sincospif(-2.f * fft_freq(k, N) * dy, &sn, &cs);
+      ey[k] = make_float2(cs * inv_n2, sn * inv_n2);
+    }
+    float sn, cs;
+    sincospif(-2.f * fft_freq(r * H + tid % H, N) * dx, &sn, &cs);
+    ex = make_float2(cs, sn);
+  }
 
   if (!from_spec) {
-    // Natural-layout rows r·H .. r·H+H-1 of every plane.
+    // Natural-layout rows r·H .. r·H+H-1 of every plane, then the forward transform.
 #pragma unroll 2
     for (int idx = tid; idx < H * N; idx += T) {
       const int yl = idx / N, x = idx % N, y = r * H + yl;
-      const float2 q = a.quad[y * N + x];
+      float2 w;
+      if (MODE == kSpectrum || MODE == kMoveBack)
+        w = a.quad[y * N + x];
+      else if (MODE == kBackSpectrum)
+        w = cconj(a.object[(size_t)(corner.x + y) * a.nxo + corner.y + x]);
       for (int m = 0; m < K; ++m) {
         float2 v;
         if (MODE == kSpectrum)
-          v = cmul(q, a.probe[m * plane + y * N + x]);
+          v = cmul(w, a.probe[m * plane + y * N + x]);
         else if (MODE == kMoveBack)
-          v = cmul(q, out[m * plane + y * N + x]);
+          v = cmul(w, out[m * plane + y * N + x]);
+        else if (MODE == kBackSpectrum)
+          v = cmul(w, a.c[(size_t)slot * K * plane + m * plane + y * N + x]);
         else
           v = a.object[(size_t)(corner.x + y) * a.nxo + corner.y + x];
         const int line = m * H + yl;
@@ -85,16 +114,20 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T) move_kernel(MoveArgs a) {
     all_lines<N, C, -1>(S, K * H, ltw);
     transpose<N, C>(S, K, cluster);
     all_lines<N, C, -1>(S, K * H, ltw);
-    if (MODE == kSpectrum) {
-      // Spectrum columns kx = r·H + c (lines m·H + c, elements ky) to [m][ky][kx].
+    if (MODE == kSpectrum || MODE == kBackSpectrum) {
+      // Spectrum columns kx = r·H + c (lines m·H + c, elements ky) to [slot][m][ky][kx].
 #pragma unroll 2
       for (int idx = tid; idx < H * N; idx += T) {
         const int c = idx % H, ky = idx / H;
+        const float2 e = MODE == kBackSpectrum ? cmul(ey[ky], ex) : make_float2(1.f, 0.f);
         for (int m = 0; m < K; ++m)
-          a.planes[((size_t)m * N + ky) * N + r * H + c] = S[(m * H + c) * L + (ky ^ swz(m * H + c))];
+          out[((size_t)m * N + ky) * N + r * H + c] =
+              cmul(S[(m * H + c) * L + (ky ^ swz(m * H + c))], e);
       }
       return;
     }
+  } else if (moves) {
+    __syncthreads();  // the row factors
   }
 
   const int naxis = MODE == kDerivSums ? 2 : 1;
@@ -105,11 +138,9 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T) move_kernel(MoveArgs a) {
     for (int idx = tid; idx < H * N; idx += T) {
       const int c = idx % H, ky = idx / H, kx = r * H + c;
       const float fy = fft_freq(ky, N), fx = fft_freq(kx, N);
-      float2 e;
-      if (MODE != kDerivWindow) {
-        float sn, cs;
-        sincospif(-2.f * (fy * dy + fx * dx), &sn, &cs);  // exp(−2πi f·d)
-        e = make_float2(cs * inv_n2, sn * inv_n2);
+      float2 e = make_float2(1.f, 0.f);
+      if (moves) {
+        e = cmul(ey[ky], ex);
         if (MODE == kDerivSums) {
           // × (−2πi·f_axis): the derivative of the translation phase (engine/features.rs:372-387)
           const float w = 2.f * 3.14159265358979f * (axis == 0 ? fy : fx);

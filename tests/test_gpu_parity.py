@@ -18,6 +18,10 @@ RUN_TOL = 1e-4
 # pixels by xi = 1 − I/(Ĩ + 1e-5): at the far-field zeros of a hard-edged aperture Ĩ is set by
 # the FP32 FFT's absolute rounding, so over several epochs a_far holds to 3e-4 of its largest.
 AFAR_RUN_TOL = 3e-4
+# ML's LLK records after its first Newton step: on the two-mode 64² scan a 1e-7 relative change
+# of the start probe moves the float64 record after the first step by 3.3e-5 (an amplification
+# of ~300), so the FP32 path's records hold to 3e-4 of the largest there.
+ML_LLK_TOL = 3e-4
 
 # (frame side, probe modes, frames, object side)
 SHAPES = [(64, 1, 40, 192), (64, 2, 40, 192), (128, 3, 24, 320), (256, 2, 10, 448)]
@@ -178,7 +182,7 @@ def test_ml_cycles(case, update_probe, ramp):
         h = g.history()
         want = np.array([r["poisson"] for r in cpu.history])
         assert list(h["algorithm"]) == ["ml"] * 4
-        assert np.abs(h["poisson"] - want).max() <= RUN_TOL * np.abs(want).max()
+        assert np.abs(h["poisson"] - want).max() <= ML_LLK_TOL * np.abs(want).max()
 
 
 @pytest.mark.parametrize("refine", [False, True])
@@ -248,7 +252,7 @@ def test_ml_with_positions(case, refine):
         assert rel_l2(g.probe(), cpu.probe) < RUN_TOL
         h = g.history()
         want = np.array([r["poisson"] for r in cpu.history])
-        assert np.abs(h["poisson"] - want).max() <= RUN_TOL * np.abs(want).max()
+        assert np.abs(h["poisson"] - want).max() <= ML_LLK_TOL * np.abs(want).max()
         d = g.positions()
         if refine:
             moved = cpu.offsets - d0
