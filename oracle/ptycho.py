@@ -216,6 +216,33 @@ class Ptycho:
         self.probe = self.probe * fp
         self.object = self.object * fo
 
+    def position_grad(self, cost="poisson", offsets=None):
+        """`position_grad` (engine/features.rs:1055-1100): per frame `[∂C/∂dy, ∂C/∂dx]` of the
+        Poisson (or amplitude) cost at `offsets` (the state's when None) under Patch sampling,
+        `Σ_views Σ Re(conj(g)·∂psi/∂d)` with `g = 2·IDFT(slope·DFT(psi))`, `slope` =
+        `1 − I/Ĩ` (Poisson) or `1 − √(I/Ĩ)` (amplitude), Ĩ floored at 1e-12, 0 where masked."""
+        d = self.offsets if offsets is None else np.asarray(offsets, np.float64)
+        s = Shifted(self.addr.views, self.probe, self.optics.quad, d)
+        nframe, nmode = self.addr.nframe, self.addr.nmode
+        psi = ops.fft2(s.to_psi(self.object))
+        ny, nx = psi.shape[-2:]
+        b = psi.reshape(nframe, nmode, ny, nx)
+        icalc = np.maximum((np.abs(b) ** 2).sum(axis=1), 1e-12)
+        iobs, mask = self.obs.iobs[:nframe], self.obs.mask[:nframe]
+        if cost == "poisson":
+            slope = 1.0 - iobs / icalc
+        else:
+            slope = 1.0 - np.sqrt(np.maximum(iobs, 0.0) / icalc)
+        r = np.where(mask, 0.0, 2.0 * slope)
+        g = ops.ifft2((b * r[:, None]).reshape(psi.shape))
+        grad = np.zeros((nframe, 2))
+        for axis in range(2):
+            dpsi = s.derivatives(self.object, axis)
+            per_view = (np.conj(g) * dpsi).real.sum(axis=(1, 2))
+            for k, f in enumerate(s.frames):
+                grad[f, axis] += per_view[k]
+        return grad
+
     def projected_position_sums(self, s):
         """`Shifted::position_sums` of the magnitude projection of the current estimate's
         exit waves (engine/ptycho.rs:470-480)."""

@@ -8,8 +8,12 @@ float64, `refs/f64/lsqml_near.py`), and the PyNX set `pynx_near_*_f64.txt` (PyNX
 to float64, `refs/f64/pynx_near.py`) whose ML run pins the Poisson conjugate gradient, and `lsqml_near_pos_*_f64.txt` (one pty-chi
 LSQML step refining the positions under PATCH, `refs/f64/lsqml_near_pos.py`) and
 `lsqml_multislice_*_f64.txt` (pty-chi LSQML through three slices with angular-spectrum, Fresnel
-and far-field exits, `refs/f64/lsqml_multislice.py`). Each text table becomes one float64 array of the same
-rows and columns under its stem in `rpie_near.npz`, `lsqml_near.npz` and `pynx_near.npz`.
+and far-field exits, `refs/f64/lsqml_multislice.py`); and the far-field results on the seeded
+scenario `dm_scenario(32, 40, nprobe, 2e5, 4.0)` (`tests/common/engine/scenario.rs`), whose
+counts `oracle/scenario.py` redraws: the position gradient (`pos_grad*`), ML with positions
+(`ml_pos_*`), LSQML steps and epochs with and without positions (`lsqml_*`) and rPIE against
+pty-chi (`rpie_ptychi_f64.txt`). Each text table becomes one float64 array of the same rows and
+columns under its stem (`table` for a file without one) in `<group>.npz`.
 
     python tests/golden/make_golden.py [REFERENCE_ROOT]
 """
@@ -30,6 +34,17 @@ GROUPS = {
     "lsqml_multislice": ["cases", "corners", "counts", "obj", "probe", "icalc", "llk",
                          "step_steps", "step_obj", "step_probe", "epochs_steps", "epochs_obj",
                          "epochs_probe"],
+    # The far-field sets on the seeded scenario `dm_scenario(32, 40, nprobe, 2e5, 4.0)`, whose
+    # counts the oracle redraws (oracle/scenario.py): results only, no state.
+    "pos_grad": ["", "values"],
+    "ml_pos": ["obj", "offsets", "probe"],
+    "lsqml_gaussian": ["obj", "probe", "steps"],
+    "lsqml_poisson": ["obj", "probe", "steps"],
+    "lsqml_epochs_gaussian": ["obj", "probe", "steps"],
+    "lsqml_epochs_poisson": ["obj", "probe", "steps"],
+    "lsqml_pos": ["steps", "offsets", "obj", "probe"],
+    "lsqml_pos_epochs": ["steps", "offsets", "obj", "probe"],
+    "rpie_ptychi": [""],
 }
 
 
@@ -39,8 +54,8 @@ def main(root):
     for group, stems in GROUPS.items():
         arrays = {}
         for stem in stems:
-            path = os.path.join(data, f"{group}_{stem}_f64.txt")
-            arrays[stem] = np.loadtxt(path, ndmin=2)
+            name = f"{group}_{stem}_f64.txt" if stem else f"{group}_f64.txt"
+            arrays[stem or "table"] = np.loadtxt(os.path.join(data, name), ndmin=2)
         np.savez_compressed(os.path.join(here, f"{group}.npz"), **arrays)
         print(group, {k: v.shape for k, v in arrays.items()})
 
