@@ -136,6 +136,16 @@ int ptyb_ml(ptyb_handle* h, const ptyb_ml_params* params, int32_t ncycle);
 /* Reference `GpuPtycho::llk` (engine/gpu/mod.rs:871-881): normalised LLK of the estimate. */
 int ptyb_get_llk(ptyb_handle* h, ptyb_llk* out);
 
+/* The hand-written adjoint of the far-field model: the Poisson LLK sum L over the unmasked
+ * pixels of the current estimate (not normalised, reference `llk` engine/ops.rs:119-154) into
+ * *loss, its gradients over the object's and the probe's real and imaginary parts packed as
+ * 2·∂L/∂X* = ∂L/∂Re X + i·∂L/∂Im X (reference `Ptycho::obj_grad` / `probe_grad`,
+ * engine/ptycho.rs:492-515; complex128 [nyo][nxo] and [nprobe][ny][nx]) and over each frame's
+ * sub-pixel offset ∂L/∂d [nframe][2] (reference `position_grad`, engine/features.rs:1055-1100),
+ * all under the position model when offsets are set. Any output may be NULL; d_pos needs
+ * offsets (ptyb_set_positions). The handle's arrays are not changed. */
+int ptyb_gradients(ptyb_handle* h, double* loss, double* d_obj, double* d_probe, double* d_pos);
+
 /* The model intensity Σ_modes |Ψ|² of the current estimate for frames[0..n) into out[n][ny][nx]
  * in the FFT-shifted detector layout (zero frequency at [0, 0]), the far-field forward model of
  * the reference binding's `forward` (ptyrs-py/src/cpu.rs) summed over modes. */

@@ -61,6 +61,8 @@ SIGNATURES = {
     "ptyb_lsqml": (c_int32, [c_void_p, P(LsqmlParams), c_int32, c_int32]),
     "ptyb_ml": (c_int32, [c_void_p, P(MlParams), c_int32]),
     "ptyb_get_llk": (c_int32, [c_void_p, P(Llk)]),
+    "ptyb_gradients": (c_int32, [c_void_p, P(c_double), P(c_double), P(c_double),
+                                 P(c_double)]),
     "ptyb_forward_intensity": (c_int32, [c_void_p, P(c_int32), c_int32, P(ctypes.c_float)]),
     "ptyb_forward_intensity_noalloc": (c_int32, [c_void_p, P(c_int32), c_int32,
                                                  P(ctypes.c_float)]),

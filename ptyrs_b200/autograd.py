@@ -1,0 +1,43 @@
+"""The far-field Poisson model as a torch autograd function, its backward the engine's
+hand-written adjoint (`ptyb_gradients`).
+
+    loss = PoissonLoss.apply(obj, probe, offsets, engine)
+    loss.backward()       # obj.grad, probe.grad, offsets.grad
+
+`obj` is complex `[1, nyo, nxo]`, `probe` complex `[nprobe, ny, nx]`, `offsets` real
+`[nframe, 2]` (sub-pixel (dy, dx) per frame in object pixels under Patch sampling, physwkim/ptyrs
+engine/features.rs:558-1025), `engine` a `GpuPtycho` of the scan. The loss is the Poisson LLK
+sum over the unmasked pixels (engine/ops.rs:119-154); the complex gradients follow torch's
+convention, ∂L/∂Re z + i·∂L/∂Im z, which is the reference's `obj_grad` / `probe_grad`
+(engine/ptycho.rs:492-515), and the offsets' gradient is its `position_grad`
+(engine/features.rs:1055-1100). Forward writes the arrays into the engine's state.
+"""
+import numpy as np
+import torch
+
+
+class PoissonLoss(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, obj, probe, offsets, engine):
+        engine.set_object(obj.detach().cpu().numpy().astype(np.complex128))
+        engine.set_probe(probe.detach().cpu().numpy().astype(np.complex128))
+        engine.set_positions(offsets.detach().cpu().numpy().astype(np.float64), refine=False)
+        g = engine.gradients(obj=ctx.needs_input_grad[0], probe=ctx.needs_input_grad[1],
+                             positions=True)
+        grads = []
+        for x, key in ((obj, "object"), (probe, "probe"), (offsets, "positions")):
+            v = g[key]
+            grads.append(None if v is None else
+                         torch.as_tensor(v, device=x.device).to(x.dtype).reshape(x.shape))
+        ctx.grads = grads
+        return torch.tensor(g["loss"], dtype=torch.float64, device=obj.device)
+
+    @staticmethod
+    def backward(ctx, grad_loss):
+        out = [None if g is None else grad_loss.to(g.real.dtype) * g for g in ctx.grads]
+        return out[0], out[1], out[2], None
+
+
+def poisson_loss(obj, probe, offsets, engine):
+    """`PoissonLoss.apply(obj, probe, offsets, engine)`."""
+    return PoissonLoss.apply(obj, probe, offsets, engine)

@@ -1081,7 +1081,7 @@ unsigned blocks_for(size_t n) { return (unsigned)((n + 255) / 256); }
 // sums of AP, DM and ML from the magnitude projection of the same field (engine/ptycho.rs:
 // 470-480, engine/features.rs:992-1025). Under the position model the probe gradient goes
 // back through the move's adjoint in the spectrum, frame by frame (features.rs:897-957).
-void ml_gradients(ptyb_handle* h, bool uo, bool up, bool refine) {
+void ml_gradients(ptyb_handle* h, bool uo, bool up, bool refine, bool pos_grad = false) {
   const size_t no = (size_t)h->nyo * h->nxo, np = (size_t)h->K * h->N * h->N;
   check(h, cudaMemsetAsync(h->g_obj, 0, no * sizeof(float2), h->stream), "memset");
   check(h, cudaMemsetAsync(h->g_obj_c, 0, no * sizeof(float2), h->stream), "memset");
@@ -1154,12 +1154,13 @@ void ml_gradients(ptyb_handle* h, bool uo, bool up, bool refine) {
       });
       launched(h, "probe gradient sum");
     }
-    if (refine) {
-      // the moved wave's derivatives from the probe spectra, dotted with the projection's
-      // change of the exit wave on chip
+    if (refine || pos_grad) {
+      // the moved wave's derivatives from the probe spectra, dotted on chip with the
+      // projection's change of the exit wave (refine) or with the gradient field g, whose
+      // sums are ∂L/∂d (engine/features.rs:1055-1100)
       MoveArgs md = move_args(h, frames, nullptr);
       md.spec = h->spec;
-      md.c = h->field;
+      md.c = refine ? h->field : h->upd;
       md.sums = h->ml_pos_sums;
       check(h, launch_move<kDerivSums>(h, md, n), "position sums");
       ++h->launches;
@@ -1774,6 +1775,63 @@ int ptyb_get_llk(ptyb_handle* h, ptyb_llk* out) {
   if (!h || !out) return PTYB_INVALID;
   return guarded(h, true, [&]() -> int {
     *out = llk_pass(h);
+    return PTYB_OK;
+  });
+}
+
+int ptyb_gradients(ptyb_handle* h, double* loss, double* d_obj, double* d_probe, double* d_pos) {
+  if (!h) return PTYB_INVALID;
+  if (h->nslice > 1) {
+    h->err = "the gradients run on a single-slice object";
+    return PTYB_INVALID;
+  }
+  if (d_pos && !h->have_offsets) {
+    h->err = "position gradients need position offsets (ptyb_set_positions)";
+    return PTYB_INVALID;
+  }
+  return guarded(h, true, [&]() -> int {
+    ensure_slots(h, std::min(h->P, h->stack));
+    ensure_ml(h);
+    const size_t np = (size_t)h->K * h->N * h->N, no = (size_t)h->nyo * h->nxo;
+    if (h->have_offsets) {
+      ensure_spec(h);
+      if (!h->wave_all) h->wave_all = alloc<float2>(h, (size_t)h->P * np);
+      if (h->wave2_slots < h->slots) {
+        h->wave2 = alloc<float2>(h, (size_t)h->slots * np);
+        h->wave2_slots = h->slots;
+      }
+      if (!h->ml_pos_sums) h->ml_pos_sums = alloc<double>(h, (size_t)h->P * 4);
+      spectrum_of(h, h->probe, h->spec);
+      const int stack = std::min(h->P, h->stack);
+      for (int s0 = 0; s0 < h->P; s0 += stack)
+        move_frames(h, h->iota + s0, std::min(stack, h->P - s0), h->spec,
+                    h->wave_all + (size_t)s0 * np);
+    }
+    ml_gradients(h, d_obj != nullptr, d_probe != nullptr, false, d_pos != nullptr);
+    const ptyb_llk l = llk_pass(h, h->have_offsets ? h->wave_all : nullptr);
+    if (loss) *loss = l.poisson * h->nb_obs;
+    if (d_obj) {
+      std::vector<float2> v(no);
+      check(h, cudaMemcpy(v.data(), h->g_obj, no * sizeof(float2), cudaMemcpyDeviceToHost),
+            "gradient");
+      to_c64(v.data(), d_obj, no);
+    }
+    if (d_probe) {
+      std::vector<float2> v(np);
+      check(h, cudaMemcpy(v.data(), h->g_probe, np * sizeof(float2), cudaMemcpyDeviceToHost),
+            "gradient");
+      to_c64(v.data(), d_probe, np);
+    }
+    if (d_pos) {
+      std::vector<double> v((size_t)h->P * 4);
+      check(h, cudaMemcpy(v.data(), h->ml_pos_sums, v.size() * sizeof(double),
+                          cudaMemcpyDeviceToHost),
+            "gradient");
+      for (int f = 0; f < h->P; ++f) {
+        d_pos[2 * f] = v[(size_t)f * 4];
+        d_pos[2 * f + 1] = v[(size_t)f * 4 + 1];
+      }
+    }
     return PTYB_OK;
   });
 }

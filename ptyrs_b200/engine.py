@@ -140,6 +140,20 @@ class GpuPtycho:
         return dict(poisson=out.poisson, gaussian=out.gaussian, euclidian=out.euclidian,
                     nb_photons_calc=out.nb_photons_calc)
 
+    def gradients(self, obj=True, probe=True, positions=True):
+        """The Poisson LLK sum `loss` of the current estimate and its gradients through the
+        hand-written adjoint: `object` and `probe` as 2·∂L/∂X* (the complex gradient torch
+        uses), `positions` ∂L/∂d `[nframe, 2]` (needs `set_positions`); a dict, None for
+        what is not asked."""
+        loss = ctypes.c_double()
+        go = np.empty(self._obj_shape, np.complex128) if obj else None
+        gp = np.empty(self._probe_shape, np.complex128) if probe else None
+        gd = np.empty((self._nframe, 2), np.float64) if positions else None
+        ptr = lambda a, view=True: None if a is None else _dptr(a.view(np.float64) if view else a)
+        self._check(self._lib.ptyb_gradients(self._h, ctypes.byref(loss), ptr(go), ptr(gp),
+                                             ptr(gd, False)))
+        return dict(loss=loss.value, object=go, probe=gp, positions=gd)
+
     def forward_intensity(self, frames=None):
         """Model intensity `Σ_modes |Ψ|²` `[len(frames), ny, nx]` of the current estimate, in the
         FFT-shifted detector layout (zero frequency at [0, 0])."""
@@ -193,7 +207,8 @@ class GpuPtycho:
 
     def set_positions(self, offsets=None, refine=True):
         """Per-frame sub-pixel offsets `[nframe, 2]` (dy, dx) in object pixels, modelled by
-        moving each frame's probe and refined by LSQML when `refine`; None clears them."""
+        moving each frame's probe and refined by LSQML and ML when `refine`; None clears
+        them."""
         if offsets is None:
             self._check(self._lib.ptyb_set_positions(self._h, None, 0))
             return
