@@ -167,10 +167,10 @@ int ptyb_forward_intensity_noalloc(ptyb_handle* h, const int32_t* frames, int32_
 /* Reference `GpuPtycho::set_features` with `Features::position` (engine/gpu/mod.rs:848-859,
  * engine/features.rs:20-130): per-frame sub-pixel offsets [nframe][2] (dy, dx) in object pixels
  * on top of the views' corners, modelled under Patch sampling (each frame's probe moved by its
- * offset) by LSQML and ML, and refined when `refine` is set: LSQML takes pty-chi's step
- * (engine/lsqml.rs:237-270), ML the step of AP and DM from the magnitude projection
- * (engine/ptycho.rs:775-842, engine/features.rs:1028-1047). rPIE refuses offsets. NULL clears
- * them. Read back with ptyb_get_positions. */
+ * offset) by rPIE, LSQML and ML, and refined when `refine` is set: rPIE and LSQML take
+ * pty-chi's step (engine/ptycho.rs:1037-1085, engine/lsqml.rs:237-270), ML the step of AP and
+ * DM from the magnitude projection (engine/ptycho.rs:775-842, engine/features.rs:1028-1047).
+ * NULL clears them. Read back with ptyb_get_positions. */
 int ptyb_set_positions(ptyb_handle* h, const double* offsets, int32_t refine);
 int ptyb_get_positions(ptyb_handle* h, double* dst);
 

@@ -340,14 +340,21 @@ class Ptycho:
             self.cycle += 1
 
     def rpie_batch(self, frames, obj_step, probe_step, obj_alpha, probe_alpha):
-        """One rPIE batch from the batch-start object and probe (engine/ptycho.rs:904-1085),
-        Patch sampling without offsets."""
+        """One rPIE batch from the batch-start object, probe and offsets
+        (engine/ptycho.rs:904-1085) under Patch sampling: with offsets every view's wave is
+        its frame's moved probe, the probe direction of a frame moves back before it adds in,
+        and refined offsets take pty-chi's step from mode 0."""
         ny, nx = self.probe.shape[-2:]
         nmode = self.addr.nmode
         nbatch = len(frames)
         views = np.concatenate([self.addr.frame_views(f) for f in frames])
         q = self.optics.quad
-        psi = ops.obj_probe_to_psi(views, self.object, self.probe, q)
+        shifted = (None if self.offsets is None else
+                   Shifted(views, self.probe, q, self.offsets))
+        if shifted is not None:
+            psi = shifted.to_psi(self.object)
+        else:
+            psi = ops.obj_probe_to_psi(views, self.object, self.probe, q)
         delta = self.optics.exit_forward(psi)
         sh = (nbatch, nmode, ny, nx)
         d4 = delta.reshape(sh)
@@ -358,8 +365,12 @@ class Ptycho:
         delta = self.optics.exit_adjoint(delta) - psi
 
         pidx = views["probe"].astype(np.int64)
-        wave = fftshift2(self.probe[pidx] * q)            # shifted, per view
-        w2 = fftshift2(np.abs(self.probe[pidx]) ** 2)       # shifted, per view
+        if shifted is not None:
+            wave = fftshift2(shifted.waves)                  # moved W, shifted, per view
+            w2 = fftshift2(np.abs(shifted.waves) ** 2)
+        else:
+            wave = fftshift2(self.probe[pidx] * q)            # shifted, per view
+            w2 = fftshift2(np.abs(self.probe[pidx]) ** 2)       # shifted, per view
         nyo, nxo = self.object.shape[-2:]
         new_obj = new_probe = None
         if obj_step is not None:
@@ -394,13 +405,32 @@ class Ptycho:
                 win = ob[oy:oy + ny, ox:ox + nx]
                 omax = (np.abs(win) ** 2).max()
                 w = np.conj(win * q) / ((1.0 - a) * np.abs(win) ** 2 + a * omax)
+                frame = np.zeros_like(self.probe)
                 for m, v in enumerate(fv):
-                    dp[int(v["probe"])] += w * deltan[b * nmode + m]
+                    frame[int(v["probe"])] += w * deltan[b * nmode + m]
+                if shifted is not None:
+                    # back through the frame's move (engine/ptycho.rs:1027-1035)
+                    frame = ops.move_planes(frame, q, -self.offsets[int(fv[0]["frame"])])
+                dp += frame
             new_probe = dp
+        dirs = None
+        if shifted is not None and self.refine:
+            # pty-chi's gradient position sums from mode 0 (engine/ptycho.rs:1037-1064)
+            sums = []
+            for b in range(nbatch):
+                k = b * nmode
+                v = views[k]
+                oy, ox = int(v["oy"]), int(v["ox"])
+                patch = self.object[int(v["obj"]), oy:oy + ny, ox:ox + nx]
+                sums.append(ops.gradient_sums(patch, fftshift2(shifted.waves[k]), delta[k]))
+            dirs = ops.gradient_directions(
+                sums, ops.EPS_POSITION * self.optics.intensity_scale())
         if obj_step is not None:
             self.object = self.object + new_obj[None] * obj_step
         if probe_step is not None:
             self.probe = self.probe + new_probe * (probe_step / nbatch)
+        if dirs is not None:
+            ops.batch_position_step(self.offsets, frames, dirs)
 
 
 def zero_phase_ramp(obj, probe):

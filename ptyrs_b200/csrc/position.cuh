@@ -206,18 +206,22 @@ __host__ __device__ constexpr size_t move_smem_bytes(int K) {
   return frame_smem_bytes<N, C>(K);
 }
 
-// planes[slot][m] = conj(q·O_window)·χ_m per natural pixel: each frame's probe direction
-// before its adjoint move (engine/lsqml.rs:200-207).
+// planes[slot][m] = w·χ_m per natural pixel: each frame's probe direction before its adjoint
+// move, w = conj(q·O_window) (LSQML, engine/lsqml.rs:200-207) or, with `omax`, rPIE's weight
+// conj(q·O)/((1 − α)|O|² + α·max|O|²) (engine/ptycho.rs:1007-1026).
 __global__ void probe_terms_kernel(const float2* object, const float2* quad, const float2* chi,
                                    const int* frames, const int2* corners, int nxo, int K, int N,
-                                   float2* planes) {
+                                   float2* planes, const float* omax = nullptr,
+                                   float alpha = 0.f) {
   const int slot = blockIdx.y;
   const size_t plane = (size_t)N * N;
   const int2 c = corners[frames[slot]];
   for (int pix = blockIdx.x * blockDim.x + threadIdx.x; pix < N * N;
        pix += gridDim.x * blockDim.x) {
     const int y = pix / N, x = pix % N;
-    const float2 w = cconj(cmul(quad[pix], object[(size_t)(c.x + y) * nxo + c.y + x]));
+    const float2 o = object[(size_t)(c.x + y) * nxo + c.y + x];
+    float2 w = cconj(cmul(quad[pix], o));
+    if (omax) w = cscale(w, 1.f / ((1.f - alpha) * cnorm2(o) + alpha * omax[slot]));
     for (int m = 0; m < K; ++m) {
       const size_t i = ((size_t)slot * K + m) * plane + pix;
       planes[i] = cmul(w, chi[i]);

@@ -260,3 +260,29 @@ def test_ml_with_positions(case, refine):
             assert np.abs((d - d0) - moved).max() <= RUN_TOL * 10 * np.abs(moved).max()
         else:
             assert np.array_equal(d, d0)
+
+
+@pytest.mark.parametrize("refine", [False, True])
+def test_rpie_with_positions(case, refine):
+    """rPIE under per-frame sub-pixel offsets (every frame's probe moved by its offset, each
+    frame's probe direction moved back, with `refine` pty-chi's position step from mode 0)
+    against the oracle, which is pinned to pty-chi's golden run: the arrays and the offset
+    changes after two epochs of batches of 13."""
+    nframe = len(case["counts"])
+    d0 = np.random.default_rng(7).uniform(-0.6, 0.6, (nframe, 2))
+    start = dict(case, object=case["truth"] * 0.9 * np.exp(0.1j))
+    cpu = oracle_state(start)
+    cpu.set_positions(d0, refine=refine)
+    cpu.rpie(2, obj_alpha=0.1, probe_alpha=0.1, batch_size=13, seed=7)
+    with gpu_of(start) as g:
+        g.set_positions(d0, refine=refine)
+        g.rpie(2, obj_alpha=0.1, probe_alpha=0.1, batch_size=13, seed=7)
+        assert rel_l2(g.object() - start["object"], cpu.object - start["object"]) < RUN_TOL
+        assert rel_l2(g.probe(), cpu.probe) < RUN_TOL
+        d = g.positions()
+        if refine:
+            moved = cpu.offsets - d0
+            assert np.abs(moved).max() > 0
+            assert np.abs((d - d0) - moved).max() <= RUN_TOL * 10 * np.abs(moved).max()
+        else:
+            assert np.array_equal(d, d0)

@@ -205,3 +205,23 @@ def test_rpie_llk_trace_matches_ptychi():
         assert rec["cycle"] == row[0]
         for key, want in zip(("poisson", "gaussian", "euclidian", "nb_photons_calc"), row[1:]):
             assert abs(rec[key] - want) < 1e-9 * abs(want), (rec["cycle"], key)
+
+
+@pytest.mark.parametrize("name,params,nepoch", [
+    ("rpie_pos_step", dict(obj_step=0.9, probe_step=0.8, obj_alpha=0.3, probe_alpha=0.2,
+                           batch_size=20), 1),
+    ("rpie_pos_epochs", dict(obj_step=1.0, probe_step=1.0, obj_alpha=0.5, probe_alpha=0.5,
+                             batch_size=4), 3)])
+def test_rpie_with_refined_positions_matches_ptychi(name, params, nepoch):
+    """rPIE refining the offsets under PATCH against pty-chi's `RPIEReconstructor`
+    (engine_rpie_pos.rs:59-150): object and probe changes to 1e-12, offset changes 3e-12."""
+    p = state()
+    g = golden(name)
+    start = frame_offsets(p, g["offsets"], 1)
+    p.set_positions(start, refine=True)
+    o0, p0 = p.object.copy(), p.probe.copy()
+    p.rpie(nepoch, calc_llk=1, seed=7, **params)
+    assert max_rel(re_im(p.object - o0), g["obj"][:, 2:4]) < 1e-12
+    assert max_rel(re_im(p.probe - p0), g["probe"][:, 3:5]) < 1e-12
+    want = frame_offsets(p, g["offsets"], 3) - start
+    assert max_rel(p.offsets - start, want) < 3e-12
