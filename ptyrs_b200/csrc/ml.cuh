@@ -7,10 +7,11 @@
 
 namespace ptyb {
 
-// Per frame: po = F(P·O·q), a = F(P·dO·q + dP·O·q), b = F(dP·dO·q) mode by mode, with
-// per-pixel accumulators calc = Σ|po|², r = Σ Re(p̄o·a), s = Σ |a|² + 2·Re(p̄o·b); then over
-// unmasked pixels, d = 1 − I/max(calc, 1e-32): num = −Σ 2·r·d, den = Σ 2·s·d + I·(2r/calc)².
-// Shared memory: two planes (po, then a / b) of H lines and the three accumulators.
+// Per frame: with po = F(P·O·q) the gradient pass kept, a = F(P·dO·q + dP·O·q) and
+// b = F(dP·dO·q) mode by mode, per-pixel accumulators calc = Σ|po|², r = Σ Re(p̄o·a),
+// s = Σ |a|² + 2·Re(p̄o·b); then over unmasked pixels, d = 1 − I/max(calc, 1e-32):
+// num = −Σ 2·r·d, den = Σ 2·s·d + I·(2r/calc)². Shared memory: one plane of H lines (a, then
+// b) and the three accumulators (rows padded to N + 1), so two CTAs share an SM.
 struct GammaArgs {
   const float2* object;
   const float2* d_obj;
@@ -26,28 +27,25 @@ struct GammaArgs {
   // Elements between consecutive slots' probe and probe direction: 0 for the shared ones,
   // K·N·N for the per-frame moved ones of the position model.
   int probe_stride;
-  // Optional: po = DFT(P·O·q) of every slot and mode as the gradient pass kept it,
-  // [slot][K][kx][ky]; null computes it here.
+  // po = DFT(P·O·q) of every slot and mode as the gradient pass kept it, [slot][K][kx][ky].
   const float2* psi;
 };
 
 template <int N, int C>
 __host__ __device__ constexpr size_t gamma_smem_bytes() {
   using F = FrameShape<N, C>;
-  return 2 * (size_t)F::H * F::L * sizeof(float2) + 3 * (size_t)F::H * N * sizeof(float) +
+  return (size_t)F::H * F::L * sizeof(float2) + 3 * (size_t)F::H * (N + 1) * sizeof(float) +
          N * sizeof(float2) + 160 * sizeof(double);
 }
 
 template <int N, int C>
-__global__ void __launch_bounds__(FrameShape<N, C>::T) gamma_kernel(GammaArgs a) {
+__global__ void __launch_bounds__(FrameShape<N, C>::T, 2) gamma_kernel(GammaArgs a) {
   using F = FrameShape<N, C>;
-  constexpr int H = F::H, T = F::T, L = F::L;
+  constexpr int H = F::H, T = F::T, L = F::L, AS = N + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  float2* S0 = reinterpret_cast<float2*>(smem_raw);  // po
-  float2* S1 = S0 + (size_t)H * L;                   // a, then b
-  float* acc = reinterpret_cast<float*>(S1 + (size_t)H * L);  // [3][H·N]
-  float2* tw = reinterpret_cast<float2*>(acc + 3 * H * N);
-  double* red = reinterpret_cast<double*>(tw + N);
+  float2* S1 = reinterpret_cast<float2*>(smem_raw);           // a, then b
+  float* acc = reinterpret_cast<float*>(S1 + (size_t)H * L);  // [3][H][N + 1]
+  double* red = reinterpret_cast<double*>(acc + 3 * H * AS + 2 * N);
   cg::cluster_group cluster = cg::this_cluster();
   const int r = C > 1 ? (int)cluster.block_rank() : 0;
   const int slot = blockIdx.x / C;
@@ -58,71 +56,44 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T) gamma_kernel(GammaArgs a)
   constexpr float inv_n2 = 1.0f / ((float)N * (float)N);
   LineTwiddles<N> ltw;
   ltw.load(a.tw, tid % F::G);
-  (void)tw;
-  for (int i = tid; i < 3 * H * N; i += T) acc[i] = 0.f;
+  for (int i = tid; i < 3 * H * AS; i += T) acc[i] = 0.f;
 
   for (int m = 0; m < K; ++m) {
     const int pm = m % a.nprobe, om = m / a.nprobe;
-    // Exit-plane rows of po and a.
-#pragma unroll 4
-    for (int idx = tid; idx < H * N; idx += T) {
-      const int yl = idx / N, jx = idx % N;
-      const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
-      const size_t pi = (size_t)slot * a.probe_stride + ((size_t)pm * N + ny) * N + nx;
-      const size_t oi = ((size_t)om * a.nyo + corner.x + ny) * a.nxo + corner.y + nx;
-      const float2 p = a.probe[pi], dp = a.d_probe[pi];
-      const float2 o = a.object[oi], dob = a.d_obj[oi];
-      const float2 q = a.quad[ny * N + nx];
-      if (!a.psi) S0[yl * L + (jx ^ swz(yl))] = cmul(cmul(p, o), q);
-      S1[yl * L + (jx ^ swz(yl))] = cmul(cadd(cmul(p, dob), cmul(dp, o)), q);
-    }
-    if (a.psi) {
-      // po of this CTA's columns, kept by the gradient pass
-      const float2* src = a.psi + ((size_t)slot * K + m) * N * N;
+    const float2* po_m = a.psi + ((size_t)slot * K + m) * N * N + (size_t)r * H * N;
+    for (int pass = 0; pass < 2; ++pass) {
+      // Exit-plane rows of a (pass 0) or b (pass 1).
 #pragma unroll 4
       for (int idx = tid; idx < H * N; idx += T) {
-        const int c = idx / N, e = idx % N;
-        S0[c * L + (e ^ swz(c))] = src[(size_t)(r * H + c) * N + e];
+        const int yl = idx / N, jx = idx % N;
+        const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
+        const size_t pi = (size_t)slot * a.probe_stride + ((size_t)pm * N + ny) * N + nx;
+        const size_t oi = ((size_t)om * a.nyo + corner.x + ny) * a.nxo + corner.y + nx;
+        const float2 dp = a.d_probe[pi], dob = a.d_obj[oi], q = a.quad[ny * N + nx];
+        const float2 v = pass == 0 ? cadd(cmul(a.probe[pi], dob), cmul(dp, a.object[oi]))
+                                   : cmul(dp, dob);
+        S1[yl * L + (jx ^ swz(yl))] = cmul(v, q);
       }
       __syncthreads();
       all_lines<N, C, -1>(S1, H, ltw);
       transpose<N, C>(S1, 1, cluster);
       all_lines<N, C, -1>(S1, H, ltw);
-    } else {
+      // Columns kx = r·H + c, elements ky; po read from the gradient pass's columns.
+#pragma unroll 4
+      for (int idx = tid; idx < H * N; idx += T) {
+        const int c = idx / N, ky = idx % N;
+        const float2 po = po_m[(size_t)c * N + ky], v = S1[c * L + (ky ^ swz(c))];
+        const float pv = (po.x * v.x + po.y * v.y) * inv_n2;
+        if (pass == 0) {
+          acc[c * AS + ky] += cnorm2(po) * inv_n2;
+          acc[(H + c) * AS + ky] += pv;
+          acc[(2 * H + c) * AS + ky] += cnorm2(v) * inv_n2;
+        } else {
+          acc[(2 * H + c) * AS + ky] += 2.f * pv;
+        }
+      }
       __syncthreads();
-      all_lines<N, C, -1>(S0, 2 * H, ltw);  // both planes: lines 0..2H-1 (S1 follows S0)
-      transpose<N, C>(S0, 2, cluster);
-      all_lines<N, C, -1>(S0, 2 * H, ltw);
     }
-#pragma unroll 4
-    for (int idx = tid; idx < H * N; idx += T) {
-      const int c = idx % H, ky = idx / H;
-      const float2 po = S0[c * L + (ky ^ swz(c))], av = S1[c * L + (ky ^ swz(c))];
-      acc[idx] += cnorm2(po) * inv_n2;
-      acc[H * N + idx] += (po.x * av.x + po.y * av.y) * inv_n2;
-      acc[2 * H * N + idx] += cnorm2(av) * inv_n2;
-    }
-    __syncthreads();
-    // b into the second plane, through the same transform; po stays in column layout.
-#pragma unroll 4
-    for (int idx = tid; idx < H * N; idx += T) {
-      const int yl = idx / N, jx = idx % N;
-      const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
-      const size_t pi = (size_t)slot * a.probe_stride + ((size_t)pm * N + ny) * N + nx;
-      const size_t oi = ((size_t)om * a.nyo + corner.x + ny) * a.nxo + corner.y + nx;
-      S1[yl * L + (jx ^ swz(yl))] = cmul(cmul(a.d_probe[pi], a.d_obj[oi]), a.quad[ny * N + nx]);
-    }
-    __syncthreads();
-    all_lines<N, C, -1>(S1, H, ltw);
-    transpose<N, C>(S1, 1, cluster);
-    all_lines<N, C, -1>(S1, H, ltw);
-#pragma unroll 4
-    for (int idx = tid; idx < H * N; idx += T) {
-      const int c = idx % H, ky = idx / H;
-      const float2 po = S0[c * L + (ky ^ swz(c))], bv = S1[c * L + (ky ^ swz(c))];
-      acc[2 * H * N + idx] += 2.f * (po.x * bv.x + po.y * bv.y) * inv_n2;
-    }
-    __syncthreads();
   }
   const float* iobs = a.iobs + (size_t)f * N * N;
   double v[4] = {0.0, 0.0, 0.0, 0.0};
@@ -130,8 +101,8 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T) gamma_kernel(GammaArgs a)
     const int c = idx % H, ky = idx / H;
     const float yo = iobs[ky * N + r * H + c];
     if (yo < 0.f) continue;
-    const double calc = fmax((double)acc[idx], 1e-32);
-    const double rr = acc[H * N + idx], ss = acc[2 * H * N + idx];
+    const double calc = fmax((double)acc[c * AS + ky], 1e-32);
+    const double rr = acc[(H + c) * AS + ky], ss = acc[(2 * H + c) * AS + ky];
     const double d = 1.0 - (double)yo / calc;
     v[0] -= 2.0 * rr * d;
     const double t = 2.0 * rr / calc;
