@@ -381,7 +381,7 @@ cudaError_t launch_frame(ptyb_handle* h, const FrameArgs& a, int nslot) {
                        : MODE == kMlGrad ? kKFrameMl
                        : MODE == kLlk ? kKFrameLlk
                        : MODE == kStore ? kKFrameStore
-                       : MODE == kProject ? kKFrameProject
+                       : MODE == kProject || MODE == kProjectKept ? kKFrameProject
                                         : kKFrameFromStore;
   cudaError_t e = cudaSuccess;
   timed(h, kind, [&] { e = launch_frame_raw<MODE>(h, a, nslot); }, nslot);
@@ -1141,9 +1141,15 @@ void ml_gradients(ptyb_handle* h, bool uo, bool up, bool refine, bool pos_grad =
       a.probe_stride = pstride;
     }
     a.psi_out = h->psi_all + (size_t)s0 * pstride;
-    a.proj_out = refine ? h->field : nullptr;
     check(h, launch_frame<kMlGrad>(h, a, n), "ml gradient pass");
     ++h->launches;
+    if (refine) {
+      // the magnitude projection's change of the exit wave from the kept Ψ
+      FrameArgs ap = a;
+      ap.out = h->field;
+      check(h, launch_frame<kProjectKept>(h, ap, n), "magnitude projection");
+      ++h->launches;
+    }
     if (uo) {
       GatherArgs g = gather_args(h, frames, n);
       g.out = h->g_obj;

@@ -33,6 +33,7 @@ enum FrameMode : int {
   kStore = 4,      // forward only; detector field and Σ_modes |Ψ|² to global
   kFromStore = 5,  // detector field from global; LSQML residual; out = χ
   kProject = 6,    // magnitude projection √I/max(√Ĩ, 1e-12), masked kept; out = ψ' − ψ
+  kProjectKept = 7,// kProject from the detector field a kMlGrad pass kept (psi_out)
 };
 
 enum Cost : int { kCostPoisson = 0, kCostAmplitude = 1 };
@@ -63,11 +64,9 @@ struct FrameArgs {
   // per-frame (moved) probes of the position model.
   int probe_stride;
   // kMlGrad, optional: the detector field Ψ = DFT(P·O·q) of every mode kept for the line
-  // search, [slot][K][kx][ky] (columns contiguous); and the magnitude projection's change of
-  // the exit wave ψ' − ψ, ψ' = IDFT(√I/max(√Ĩ, 1e-12)·Ψ) (masked kept), [slot][K][N][N]
-  // natural, which needs psi_out.
+  // search and the magnitude projection, [slot][K][kx][ky] (columns contiguous); kProjectKept
+  // reads it back.
   float2* psi_out;
-  float2* proj_out;
 };
 
 template <int N, int C>
@@ -215,6 +214,14 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T)
       const int line = idx / N, e = idx % N;
       S[line * L + (e ^ swz(line))] = src[idx];
     }
+  } else if (MODE == kProjectKept) {
+    // this CTA's columns of the kept Ψ, [slot][m][kx][ky]
+    const float2* src = a.psi_out + (size_t)slot * K * N * N;
+#pragma unroll 8
+    for (int idx = tid; idx < K * H * N; idx += T) {
+      const int line = idx / N, e = idx % N, m = line / H, c = line % H;
+      S[line * L + (e ^ swz(line))] = src[((size_t)m * N + r * H + c) * N + e];
+    }
   } else {
     // Exit waves ψ = P·O·q of shifted rows r·H .. r·H+H-1, every mode; the object window and
     // the phase are read once per pixel.
@@ -251,7 +258,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T)
     }
   }
 
-  if (MODE != kFromStore) {
+  if (MODE != kFromStore && MODE != kProjectKept) {
     all_lines<N, C, -1>(S, K * H, ltw);
     transpose<N, C>(S, K, cluster);  // its first cluster barrier publishes red[0]
     if (MODE == kRpie && r == 0 && tid == 0) {
@@ -340,7 +347,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T)
     float fac;
     if (MODE == kRpie) {
       fac = masked ? 1.f : sqrtf(yo + 1e-7f) / (sqrtf(ic) + 1e-7f);
-    } else if (MODE == kProject) {
+    } else if (MODE == kProject || MODE == kProjectKept) {
       // ApplyAmplitude (engine/ops.rs:83-107)
       fac = masked ? 1.f : sqrtf(yo) / fmaxf(sqrtf(ic), 1e-12f);
     } else if (MODE == kMlGrad) {
@@ -415,38 +422,6 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T)
     }
   };
   epilogue(a.out, MODE != kMlGrad);
-
-  if (MODE == kMlGrad && a.proj_out) {
-    // The magnitude projection of the same Ψ (ApplyAmplitude, engine/ops.rs:83-107), reloaded
-    // from psi_out: ψ' − ψ to proj_out.
-    __syncthreads();
-    const float2* src = a.psi_out + (size_t)slot * K * N * N;
-#pragma unroll 8
-    for (int idx = tid; idx < K * H * N; idx += T) {
-      const int line = idx / N, e = idx % N, m = line / H, c = line % H;
-      S[line * L + (e ^ swz(line))] = src[((size_t)m * N + r * H + c) * N + e];
-    }
-    __syncthreads();
-#pragma unroll 4
-    for (int i = 0; i < kPixPerThread; ++i) {
-      const int idx = tid + i * T;
-      const int c = idx % H, ky = idx / H;
-      const float yo = iobs[ky * N + r * H + c];
-      float ic = 0.f;
-      for (int m = 0; m < K; ++m) ic += cnorm2(S[(m * H + c) * L + (ky ^ swz(m * H + c))]);
-      ic *= inv_n2;
-      const float fac = (yo < 0.f ? 1.f : sqrtf(yo) / fmaxf(sqrtf(ic), 1e-12f)) * inv_n2;
-      for (int m = 0; m < K; ++m) {
-        float2& v = S[(m * H + c) * L + (ky ^ swz(m * H + c))];
-        v = cscale(v, fac);
-      }
-    }
-    __syncthreads();
-    all_lines<N, C, +1>(S, K * H, ltw);
-    transpose<N, C>(S, K, cluster);
-    all_lines<N, C, +1>(S, K * H, ltw);
-    epilogue(a.proj_out, true);
-  }
 }
 
 }  // namespace ptyb
