@@ -61,6 +61,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T, 2) gamma_kernel(GammaArgs
   for (int m = 0; m < K; ++m) {
     const int pm = m % a.nprobe, om = m / a.nprobe;
     const float2* po_m = a.psi + ((size_t)slot * K + m) * N * N + (size_t)r * H * N;
+#pragma unroll 1
     for (int pass = 0; pass < 2; ++pass) {
       // Exit-plane rows of a (pass 0) or b (pass 1).
 #pragma unroll 4

@@ -131,6 +131,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T) move_kernel(MoveArgs a) {
   }
 
   const int naxis = MODE == kDerivSums ? 2 : 1;
+#pragma unroll 1
   for (int ax = 0; ax < naxis; ++ax) {
     const int axis = ax;
     // Spectrum: column kx = r·H + c as line (m·H + c), element ky.
