@@ -228,10 +228,36 @@ void check(ptyb_handle* h, cudaError_t e, const char* what) {
   }
 }
 
+// Device memory comes from the device's stream-ordered pool, whose release threshold is set to
+// its maximum once per device: memory a destroyed handle gave back stays with the pool, so the
+// next handle on that device reuses it instead of the driver mapping new pages (as torch's
+// caching allocator does). Each allocation is waited for, so any stream may use it at once.
+std::mutex g_pool_mutex;
+bool g_pool_kept[kMaxDevices] = {};
+
+cudaError_t pool_alloc(ptyb_handle* h, void** p, size_t bytes) {
+  if (h->device < 0 || h->device >= kMaxDevices) return cudaErrorInvalidDevice;
+  {
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    if (!g_pool_kept[h->device]) {
+      cudaMemPool_t pool;
+      cudaError_t e = cudaDeviceGetDefaultMemPool(&pool, h->device);
+      if (e != cudaSuccess) return e;
+      uint64_t keep = UINT64_MAX;
+      e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      if (e != cudaSuccess) return e;
+      g_pool_kept[h->device] = true;
+    }
+  }
+  cudaError_t e = cudaMallocAsync(p, bytes, h->stream);
+  if (e != cudaSuccess) return e;
+  return cudaStreamSynchronize(h->stream);
+}
+
 template <typename T>
 T* alloc(ptyb_handle* h, size_t count) {
   void* p = nullptr;
-  check(h, cudaMalloc(&p, count * sizeof(T) + 16), "cudaMalloc");
+  check(h, pool_alloc(h, &p, count * sizeof(T) + 16), "cudaMallocAsync");
   h->bufs.push_back({p, count * sizeof(T)});
   return static_cast<T*>(p);
 }
@@ -1472,7 +1498,7 @@ int create_handle(const ptyb_scan* scan, const double* object, int32_t nobj, int
                                                                 : 8;
     h->iobs = alloc<float>(h, nval);
     void* raw = nullptr;
-    check(h, cudaMalloc(&raw, nval * esize), "cudaMalloc");
+    check(h, pool_alloc(h, &raw, nval * esize), "cudaMallocAsync");
     double* power = alloc<double>(h, h->P);
     int* nobs = alloc<int>(h, h->P + 1);
     check(h, cudaMemset(nobs, 0, (h->P + 1) * sizeof(int)), "memset");
@@ -1491,7 +1517,7 @@ int create_handle(const ptyb_scan* scan, const double* object, int32_t nobj, int
       ++h->launches;
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-    cudaFree(raw);
+    cudaFreeAsync(raw, h->stream);
     check(h, e, "counts upload");
     std::vector<double> pw(h->P);
     std::vector<int> nb(h->P + 1);
@@ -2166,7 +2192,8 @@ void ptyb_destroy(ptyb_handle* h) {
   if (!h) return;
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
-  for (auto& b : h->bufs) cudaFree(b.p);
+  for (auto& b : h->bufs) cudaFreeAsync(b.p, h->stream);
+  if (h->stream) cudaStreamSynchronize(h->stream);
   for (auto e : h->event_pool) cudaEventDestroy(e);
   for (auto& p : h->pending) {
     cudaEventDestroy(p.a);
