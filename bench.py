@@ -151,10 +151,15 @@ def algorithmic_bytes(kind, s, wl):
         "frame_rpie": 8 * n2 + 4 * n2 + 8 * K * n2,
         "frame_lsqml": 8 * n2 + 4 * n2 + 8 * K * n2,
         "frame_llk": 8 * n2 + 4 * n2 + moved,
-        "frame_ml": 8 * n2 + 4 * n2 + 8 * K * n2 + moved,
-        "frame_project": 8 * n2 + 4 * n2 + 8 * K * n2 + moved,
-        "ml_gamma": 16 * n2 + 4 * n2 + 2 * moved,
+        # gradient pass: object window, counts, (moved probe), Ψ kept and g written
+        "frame_ml_grad": 8 * n2 + 4 * n2 + 16 * K * n2 + moved,
+        # projection from the kept Ψ: Ψ read, object window, counts, (moved probe), change
+        "frame_project": 8 * n2 + 4 * n2 + 16 * K * n2 + moved,
+        # line search: object and direction windows, counts, kept Ψ, (moved probe and direction)
+        "ml_gamma": 16 * n2 + 4 * n2 + 8 * K * n2 + 2 * moved,
         "move": 8 * K * n2,
+        "back_spectrum": 16 * K * n2 + 8 * n2,
+        "deriv_sums": 8 * K * n2 + 8 * n2,
         "position_sums": 16 * K * n2 + 8 * n2,
         "probe_partial": 8 * K * n2 + 8 * n2,
         "lsqml_dots": 8 * K * n2 + 16 * n2,

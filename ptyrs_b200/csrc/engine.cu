@@ -275,7 +275,7 @@ enum Kind : int {
   kKObjRpie, kKObjOverlap, kKObjLsqml, kKObjMl, kKIllum, kKProbePartial, kKProbeFinal,
   kKAfar, kKDots, kKSolve, kKAxpy, kKMax, kKCounts, kKMisc, kKGamma, kKArraySums, kKMove,
   kKPositionSums, kKSliceForward, kKSliceBackward, kKSliceLlk, kKFrameProject, kKSpectrum,
-  kKDerivSums, kNumKinds
+  kKDerivSums, kKBackSpectrum, kNumKinds
 };
 const char* const kKindNames[kNumKinds] = {
     "frame_rpie", "frame_lsqml", "frame_ml_grad", "frame_llk", "frame_store",
@@ -283,7 +283,7 @@ const char* const kKindNames[kNumKinds] = {
     "illumination", "probe_partial", "probe_finalize", "lsqml_afar", "lsqml_dots",
     "lsqml_solve", "axpy", "max", "counts", "misc", "ml_gamma", "array_sums", "move",
     "position_sums", "slice_forward", "slice_backward", "slice_llk", "frame_project", "spectrum",
-    "deriv_sums"};
+    "deriv_sums", "back_spectrum"};
 
 cudaEvent_t take_event(ptyb_handle* h) {
   if (!h->event_pool.empty()) {
@@ -445,7 +445,10 @@ template <int MODE>
 cudaError_t launch_move(ptyb_handle* h, const MoveArgs& a, int nslot) {
   if (nslot <= 0) return cudaSuccess;
   const int K = MODE == kDerivWindow ? 2 : h->K;
-  constexpr int kind = MODE == kDerivSums ? kKDerivSums : MODE == kSpectrum ? kKSpectrum : kKMove;
+  constexpr int kind = MODE == kDerivSums      ? kKDerivSums
+                       : MODE == kSpectrum     ? kKSpectrum
+                       : MODE == kBackSpectrum ? kKBackSpectrum
+                                               : kKMove;
   const int C = MODE == kDerivSums ? h->C_sums : h->C;
   cudaError_t e = cudaErrorInvalidValue;
   timed(h, kind, [&] {

@@ -40,7 +40,9 @@ struct MoveArgs {
 PTYB_D float fft_freq(int k, int n) { return (float)(k < (n + 1) / 2 ? k : k - n) / (float)n; }
 
 template <int N, int C, int MODE>
-__global__ void __launch_bounds__(FrameShape<N, C>::T) move_kernel(MoveArgs a) {
+__global__ void __launch_bounds__(FrameShape<N, C>::T,
+                                  FrameShape<N, C>::T <= 256 && MODE != kDerivSums ? 3 : 1)
+    move_kernel(MoveArgs a) {
   using F = FrameShape<N, C>;
   constexpr int H = F::H, T = F::T, L = F::L;
   extern __shared__ __align__(16) unsigned char smem_raw[];
