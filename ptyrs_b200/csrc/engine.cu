@@ -254,6 +254,22 @@ cudaError_t pool_alloc(ptyb_handle* h, void** p, size_t bytes) {
   return cudaStreamSynchronize(h->stream);
 }
 
+// Host↔device copies and fills on the handle's stream, waited for. The stream is
+// non-blocking, so its kernels do not order after copies or fills on the legacy default
+// stream: every transfer goes through it.
+cudaError_t copy_sync(ptyb_handle* h, void* dst, const void* src, size_t bytes,
+                      cudaMemcpyKind kind) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, h->stream);
+  if (e != cudaSuccess) return e;
+  return cudaStreamSynchronize(h->stream);
+}
+
+cudaError_t fill_sync(ptyb_handle* h, void* dst, int value, size_t bytes) {
+  cudaError_t e = cudaMemsetAsync(dst, value, bytes, h->stream);
+  if (e != cudaSuccess) return e;
+  return cudaStreamSynchronize(h->stream);
+}
+
 template <typename T>
 T* alloc(ptyb_handle* h, size_t count) {
   void* p = nullptr;
@@ -748,7 +764,7 @@ void upload_orders(ptyb_handle* h, int nepoch, int size, uint64_t seed, int64_t 
     h->order_cap = all.size();
   }
   if (!all.empty())
-    check(h, cudaMemcpy(h->order_all, all.data(), all.size() * sizeof(int32_t),
+    check(h, copy_sync(h, h->order_all, all.data(), all.size() * sizeof(int32_t),
                         cudaMemcpyHostToDevice),
           "order upload");
 }
@@ -1504,8 +1520,8 @@ int create_handle(const ptyb_scan* scan, const double* object, int32_t nobj, int
     check(h, pool_alloc(h, &raw, nval * esize), "cudaMallocAsync");
     double* power = alloc<double>(h, h->P);
     int* nobs = alloc<int>(h, h->P + 1);
-    check(h, cudaMemset(nobs, 0, (h->P + 1) * sizeof(int)), "memset");
-    cudaError_t e = cudaMemcpy(raw, scan->counts, nval * esize, cudaMemcpyHostToDevice);
+    check(h, fill_sync(h, nobs, 0, (h->P + 1) * sizeof(int)), "memset");
+    cudaError_t e = copy_sync(h, raw, scan->counts, nval * esize, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) {
       if (scan->counts_kind == PTYB_COUNTS_U16)
         counts_kernel<<<h->P, 256, 0, h->stream>>>(static_cast<const uint16_t*>(raw), 1, h->iobs,
@@ -1524,8 +1540,8 @@ int create_handle(const ptyb_scan* scan, const double* object, int32_t nobj, int
     check(h, e, "counts upload");
     std::vector<double> pw(h->P);
     std::vector<int> nb(h->P + 1);
-    check(h, cudaMemcpy(pw.data(), power, h->P * sizeof(double), cudaMemcpyDeviceToHost), "counts");
-    check(h, cudaMemcpy(nb.data(), nobs, (h->P + 1) * sizeof(int), cudaMemcpyDeviceToHost), "counts");
+    check(h, copy_sync(h, pw.data(), power, h->P * sizeof(double), cudaMemcpyDeviceToHost), "counts");
+    check(h, copy_sync(h, nb.data(), nobs, (h->P + 1) * sizeof(int), cudaMemcpyDeviceToHost), "counts");
     if (nb[h->P]) {
       h->err = "counts must be finite";
       return PTYB_INVALID;
@@ -1536,15 +1552,15 @@ int create_handle(const ptyb_scan* scan, const double* object, int32_t nobj, int
       h->nb_obs += nb[f];
     }
     h->corners = alloc<int2>(h, h->P);
-    check(h, cudaMemcpy(h->corners, h->corners_h.data(), h->P * sizeof(int2), cudaMemcpyHostToDevice),
+    check(h, copy_sync(h, h->corners, h->corners_h.data(), h->P * sizeof(int2), cudaMemcpyHostToDevice),
           "corners upload");
     h->object = alloc<float2>(h, (size_t)nslice * nobj * nyo * nxo);
     auto o = from_c64(object, (size_t)nslice * nobj * nyo * nxo);
-    check(h, cudaMemcpy(h->object, o.data(), o.size() * sizeof(float2), cudaMemcpyHostToDevice),
+    check(h, copy_sync(h, h->object, o.data(), o.size() * sizeof(float2), cudaMemcpyHostToDevice),
           "object upload");
     h->probe = alloc<float2>(h, (size_t)nprobe * plane);
     auto pr = from_c64(probe, (size_t)nprobe * plane);
-    check(h, cudaMemcpy(h->probe, pr.data(), pr.size() * sizeof(float2), cudaMemcpyHostToDevice),
+    check(h, copy_sync(h, h->probe, pr.data(), pr.size() * sizeof(float2), cudaMemcpyHostToDevice),
           "probe upload");
     // Far-field plane phase (engine/ops.rs:17-33) and the FFT twiddles, in double.
     std::vector<float2> q(plane), tw(N);
@@ -1559,13 +1575,13 @@ int create_handle(const ptyb_scan* scan, const double* object, int32_t nobj, int
     for (int t = 0; t < N; ++t)
       tw[t] = make_float2((float)std::cos(2.0 * M_PI * t / N), (float)-std::sin(2.0 * M_PI * t / N));
     h->quad = alloc<float2>(h, plane);
-    check(h, cudaMemcpy(h->quad, q.data(), plane * sizeof(float2), cudaMemcpyHostToDevice), "quad");
+    check(h, copy_sync(h, h->quad, q.data(), plane * sizeof(float2), cudaMemcpyHostToDevice), "quad");
     h->tw = alloc<float2>(h, N);
-    check(h, cudaMemcpy(h->tw, tw.data(), N * sizeof(float2), cudaMemcpyHostToDevice), "tw");
+    check(h, copy_sync(h, h->tw, tw.data(), N * sizeof(float2), cudaMemcpyHostToDevice), "tw");
     std::vector<int> iota(h->P);
     for (int f = 0; f < h->P; ++f) iota[f] = f;
     h->iota = alloc<int>(h, h->P);
-    check(h, cudaMemcpy(h->iota, iota.data(), h->P * sizeof(int), cudaMemcpyHostToDevice), "iota");
+    check(h, copy_sync(h, h->iota, iota.data(), h->P * sizeof(int), cudaMemcpyHostToDevice), "iota");
     h->order = alloc<int>(h, h->P);
     h->afar_all = alloc<float>(h, h->P);
     h->llk = alloc<double>(h, (size_t)h->P * 4);
@@ -1574,7 +1590,7 @@ int create_handle(const ptyb_scan* scan, const double* object, int32_t nobj, int
     h->d_obj = alloc<float2>(h, (size_t)nslice * nyo * nxo);
     h->d_probe = alloc<float2>(h, (size_t)K * plane);
     h->steplog = alloc<double>(h, (size_t)h->P * h->log_stride);
-    check(h, cudaMemset(h->scal, 0, kScalars * sizeof(float)), "memset");
+    check(h, fill_sync(h, h->scal, 0, kScalars * sizeof(float)), "memset");
     if (nslice > 1) {
       // Angular-spectrum transfer functions exp(2πi z √(1 − r)) of the gaps in DFT order, 0 on
       // the evanescent band (engine/propagate.rs:505-531), in double; the plane of ones is the
@@ -1597,9 +1613,9 @@ int create_handle(const ptyb_scan* scan, const double* object, int32_t nobj, int
           }
       }
       h->tf = alloc<float2>(h, t.size());
-      check(h, cudaMemcpy(h->tf, t.data(), t.size() * sizeof(float2), cudaMemcpyHostToDevice), "tf");
+      check(h, copy_sync(h, h->tf, t.data(), t.size() * sizeof(float2), cudaMemcpyHostToDevice), "tf");
       h->ones = alloc<float2>(h, plane);
-      check(h, cudaMemcpy(h->ones, ones.data(), plane * sizeof(float2), cudaMemcpyHostToDevice),
+      check(h, copy_sync(h, h->ones, ones.data(), plane * sizeof(float2), cudaMemcpyHostToDevice),
             "ones");
     }
     return PTYB_OK;
@@ -1717,7 +1733,7 @@ int ptyb_lsqml(ptyb_handle* h, const ptyb_lsqml_params* p, int32_t nepoch, int32
     if (nepoch > 0) {
       const int stride = h->log_stride;
       std::vector<double> log((size_t)h->P * stride);
-      check(h, cudaMemcpy(log.data(), h->steplog, log.size() * sizeof(double),
+      check(h, copy_sync(h, log.data(), h->steplog, log.size() * sizeof(double),
                           cudaMemcpyDeviceToHost),
             "steps");
       int b = 0, o = 0;
@@ -1882,19 +1898,19 @@ int ptyb_gradients(ptyb_handle* h, double* loss, double* d_obj, double* d_probe,
     if (loss) *loss = l.poisson * h->nb_obs;
     if (d_obj) {
       std::vector<float2> v(no);
-      check(h, cudaMemcpy(v.data(), h->g_obj, no * sizeof(float2), cudaMemcpyDeviceToHost),
+      check(h, copy_sync(h, v.data(), h->g_obj, no * sizeof(float2), cudaMemcpyDeviceToHost),
             "gradient");
       to_c64(v.data(), d_obj, no);
     }
     if (d_probe) {
       std::vector<float2> v(np);
-      check(h, cudaMemcpy(v.data(), h->g_probe, np * sizeof(float2), cudaMemcpyDeviceToHost),
+      check(h, copy_sync(h, v.data(), h->g_probe, np * sizeof(float2), cudaMemcpyDeviceToHost),
             "gradient");
       to_c64(v.data(), d_probe, np);
     }
     if (d_pos) {
       std::vector<double> v((size_t)h->P * 4);
-      check(h, cudaMemcpy(v.data(), h->ml_pos_sums, v.size() * sizeof(double),
+      check(h, copy_sync(h, v.data(), h->ml_pos_sums, v.size() * sizeof(double),
                           cudaMemcpyDeviceToHost),
             "gradient");
       for (int f = 0; f < h->P; ++f) {
@@ -2003,7 +2019,7 @@ int ptyb_set_positions(ptyb_handle* h, const double* offsets, int32_t refine) {
       return PTYB_OK;
     }
     if (!h->offsets) h->offsets = alloc<double>(h, (size_t)h->P * 2);
-    check(h, cudaMemcpy(h->offsets, offsets, (size_t)h->P * 2 * sizeof(double),
+    check(h, copy_sync(h, h->offsets, offsets, (size_t)h->P * 2 * sizeof(double),
                         cudaMemcpyHostToDevice),
           "offsets");
     if (!h->have_offsets && h->slots > 0) {
@@ -2025,7 +2041,7 @@ int ptyb_get_positions(ptyb_handle* h, double* dst) {
       std::fill(dst, dst + 2 * h->P, 0.0);
       return PTYB_OK;
     }
-    check(h, cudaMemcpy(dst, h->offsets, (size_t)h->P * 2 * sizeof(double), cudaMemcpyDeviceToHost),
+    check(h, copy_sync(h, dst, h->offsets, (size_t)h->P * 2 * sizeof(double), cudaMemcpyDeviceToHost),
           "offsets");
     return PTYB_OK;
   });
@@ -2037,7 +2053,7 @@ int ptyb_get_object(ptyb_handle* h, double* dst) {
     const size_t n = (size_t)h->nobj * h->nyo * h->nxo;
     std::vector<float2> v(n);
     check(h, cudaStreamSynchronize(h->stream), "sync");
-    check(h, cudaMemcpy(v.data(), h->object, n * sizeof(float2), cudaMemcpyDeviceToHost), "object");
+    check(h, copy_sync(h, v.data(), h->object, n * sizeof(float2), cudaMemcpyDeviceToHost), "object");
     to_c64(v.data(), dst, n);
     return PTYB_OK;
   });
@@ -2049,7 +2065,7 @@ int ptyb_get_objects(ptyb_handle* h, double* dst) {
     const size_t n = (size_t)h->nslice * h->nobj * h->nyo * h->nxo;
     std::vector<float2> v(n);
     check(h, cudaStreamSynchronize(h->stream), "sync");
-    check(h, cudaMemcpy(v.data(), h->object, n * sizeof(float2), cudaMemcpyDeviceToHost), "objects");
+    check(h, copy_sync(h, v.data(), h->object, n * sizeof(float2), cudaMemcpyDeviceToHost), "objects");
     to_c64(v.data(), dst, n);
     return PTYB_OK;
   });
@@ -2061,7 +2077,7 @@ int ptyb_get_probe(ptyb_handle* h, double* dst) {
     const size_t n = (size_t)h->nprobe * h->N * h->N;
     std::vector<float2> v(n);
     check(h, cudaStreamSynchronize(h->stream), "sync");
-    check(h, cudaMemcpy(v.data(), h->probe, n * sizeof(float2), cudaMemcpyDeviceToHost), "probe");
+    check(h, copy_sync(h, v.data(), h->probe, n * sizeof(float2), cudaMemcpyDeviceToHost), "probe");
     to_c64(v.data(), dst, n);
     return PTYB_OK;
   });
@@ -2073,7 +2089,7 @@ int ptyb_set_object(ptyb_handle* h, const double* src) {
     const size_t n = (size_t)h->nobj * h->nyo * h->nxo;
     auto v = from_c64(src, n);
     check(h, cudaStreamSynchronize(h->stream), "sync");
-    check(h, cudaMemcpy(h->object, v.data(), n * sizeof(float2), cudaMemcpyHostToDevice), "object");
+    check(h, copy_sync(h, h->object, v.data(), n * sizeof(float2), cudaMemcpyHostToDevice), "object");
     return PTYB_OK;
   });
 }
@@ -2084,7 +2100,7 @@ int ptyb_set_probe(ptyb_handle* h, const double* src) {
     const size_t n = (size_t)h->nprobe * h->N * h->N;
     auto v = from_c64(src, n);
     check(h, cudaStreamSynchronize(h->stream), "sync");
-    check(h, cudaMemcpy(h->probe, v.data(), n * sizeof(float2), cudaMemcpyHostToDevice), "probe");
+    check(h, copy_sync(h, h->probe, v.data(), n * sizeof(float2), cudaMemcpyHostToDevice), "probe");
     return PTYB_OK;
   });
 }
