@@ -187,7 +187,12 @@ PTYB_D void cluster_sum2(double& x, double& y, double* red, cg::cluster_group& c
 }
 
 template <int N, int C, int MODE>
-__global__ void __launch_bounds__(FrameShape<N, C>::T)
+__global__ void __launch_bounds__(FrameShape<N, C>::T,
+                                  N == 256 && FrameShape<N, C>::T <= 256 &&
+                                          (MODE == kMlGrad || MODE == kProjectKept ||
+                                           MODE == kLlk)
+                                      ? 3
+                                      : 1)
     frame_kernel(FrameArgs a) {
   using F = FrameShape<N, C>;
   constexpr int H = F::H, T = F::T, L = F::L;
