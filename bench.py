@@ -58,8 +58,8 @@ WORKLOADS = {
 
 
 def dist_env():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    return int(os.environ.get("RANK", "0")), ws, int(os.environ.get("LOCAL_RANK", "0"))
+    from ptyrs_b200.replicas import env
+    return env()
 
 
 def peaks():
@@ -305,15 +305,9 @@ def main():
     if args.impl == "reference":
         return reference_arm(args, wl)
 
-    rank, ws, local = dist_env()
-    dist = None
-    if ws > 1:
-        import datetime
-
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from ptyrs_b200.replicas import Replicas, job_value
+    group = Replicas("nccl")
+    rank, ws, local = group.rank, group.world, group.local
     import torch
 
     from ptyrs_b200 import GpuPtycho, Scan, build, sim
@@ -327,9 +321,7 @@ def main():
     run_algorithm(g, wl, args.warmup)
     g.synchronize()
 
-    def barrier():
-        if dist is not None:
-            dist.barrier()
+    barrier = group.barrier
 
     # Timed region: K epochs, device time from events on the engine's stream.
     g.set_timing(True)
@@ -346,11 +338,8 @@ def main():
     times = g.kernel_times()
     kframes = g.kernel_frames()
     g.set_timing(False)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = P * ws * args.steps / (ms / 1e3)
+    ms = group.max(ms)
+    value = job_value(P, ws, args.steps, ms)
 
     # Dominant kernel and its roofline (algorithmic bytes per launch / mean launch time).
     pk, pk_kind = peaks()
@@ -391,10 +380,7 @@ def main():
                 if wl["algorithm"] == "ml":
                     w.positions()
         dt = time.perf_counter() - t0
-        if dist is not None:
-            t = torch.tensor([dt], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            dt = float(t.item())
+        dt = group.max(dt)
         n = s["n"]
         # counts (f32), object and probe (complex64 on the device), positions (y, x and the
         # ML offsets in f64)
@@ -437,9 +423,7 @@ def main():
             "kernels_ms": {k: round(v[0], 3) for k, v in sorted(times.items())},
         }
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    group.close()
 
 
 if __name__ == "__main__":
