@@ -78,6 +78,13 @@ struct FrameShape {
   static constexpr int E = H * N / T;       // = 16
 };
 
+// Resident CTAs per SM the per-frame kernels are compiled for: two at 256 threads or fewer
+// (a cap of 128 registers), one above.
+template <int N, int C>
+__host__ __device__ constexpr int frame_min_blocks() {
+  return FrameShape<N, C>::T <= 256 ? 2 : 1;
+}
+
 template <int N, int C>
 __host__ __device__ constexpr size_t frame_smem_bytes(int K) {
   return (size_t)K * FrameShape<N, C>::H * FrameShape<N, C>::L * sizeof(float2) +
@@ -192,7 +199,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
                                           (MODE == kMlGrad || MODE == kProjectKept ||
                                            MODE == kLlk)
                                       ? 3
-                                      : 1)
+                                      : frame_min_blocks<N, C>())
     frame_kernel(FrameArgs a) {
   using F = FrameShape<N, C>;
   constexpr int H = F::H, T = F::T, L = F::L;

@@ -99,7 +99,8 @@ PTYB_D void rows_io(float2* S, float2* dst, int r, int K, bool store) {
 }
 
 template <int N, int C, int MODE>
-__global__ void __launch_bounds__(FrameShape<N, C>::T) slice_kernel(SliceArgs sa) {
+__global__ void __launch_bounds__(FrameShape<N, C>::T, frame_min_blocks<N, C>())
+    slice_kernel(SliceArgs sa) {
   using F = FrameShape<N, C>;
   constexpr int H = F::H, T = F::T, L = F::L;
   const FrameArgs& a = sa.f;

@@ -41,7 +41,11 @@ PTYB_D float fft_freq(int k, int n) { return (float)(k < (n + 1) / 2 ? k : k - n
 
 template <int N, int C, int MODE>
 __global__ void __launch_bounds__(FrameShape<N, C>::T,
-                                  FrameShape<N, C>::T <= 256 && MODE != kDerivSums ? 3 : 1)
+                                  N == 256 && FrameShape<N, C>::T <= 256 &&
+                                          (MODE == kFromSpectrum || MODE == kBackSpectrum ||
+                                           MODE == kSpectrum || MODE == kPlainInverse)
+                                      ? 3
+                                      : frame_min_blocks<N, C>())
     move_kernel(MoveArgs a) {
   using F = FrameShape<N, C>;
   constexpr int H = F::H, T = F::T, L = F::L;
