@@ -175,6 +175,16 @@ def sample_scan(s, m):
     return dict(s, counts=s["counts"][:m], y=s["y"][:m], x=s["x"][:m])
 
 
+# DRAM bytes per frame of each kernel (ncu dram__bytes_read.sum + dram__bytes_write.sum over
+# its launches' frames) on the 1000-frame cut of the ml256 scan, profiles/ml256_launch_list.md:
+# roofline.traffic scales them to the launch's frames.
+NCU_DRAM_BYTES_PER_FRAME = {
+    "ml256": {"ml_gamma": 3.45e6, "frame_ml_grad": 3.51e6, "frame_project": 3.54e6,
+              "deriv_sums": 1.06e6, "move": 0.97e6, "back_spectrum": 2.06e6,
+              "object_ml": 2.17e6, "frame_llk": 1.34e6},
+}
+
+
 def cpu_baseline(s, wl, seconds=15.0, threads=None, cycles=2):
     """The oracle (numpy float64 restatement of the reference's CPU engine) on a bounded sample
     of the workload. ML: `cycles` cycles (one call, as the GPU step) over the first
@@ -348,11 +358,17 @@ def main():
     per_frame = algorithmic_bytes(kname, s, wl)
     roofline = None
     if per_frame and kframes.get(kname):
-        bytes_launch = per_frame * kframes[kname] / kn
+        frames_launch = kframes[kname] / kn
+        bytes_launch = per_frame * frames_launch
         achieved = bytes_launch / (kms / kn / 1e3) / 1e9
+        measured = NCU_DRAM_BYTES_PER_FRAME.get(args.workload, {}).get(kname)
+        traffic = measured * frames_launch if measured and args.scale == 1.0 else None
         roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved,
                     "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
-                    "peak_source": pk_kind, "traffic": None,
+                    "peak_source": pk_kind, "traffic": traffic,
+                    "traffic_source": None if traffic is None else
+                    "ncu DRAM bytes per frame on a 1000-frame cut of the same scan "
+                    "(profiles/ml256_launch_list.md) times this launch's frames",
                     "bytes_per_launch": bytes_launch, "mean_launch_ms": kms / kn,
                     "share": kms / sum(v[0] for v in times.values())}
 
