@@ -306,6 +306,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cluster", type=int, default=0,
                     help="CTAs per frame of the frame kernel (0: the engine chooses)")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="skip the launch-shape autotuner (cluster and stack from the flags)")
     ap.add_argument("--stack", type=int, default=0,
                     help="frames per launch of the whole-scan passes (0: the engine's default)")
     ap.add_argument("--scale", type=float, default=1.0,
@@ -325,6 +327,17 @@ def main():
     s = make_inputs(args.workload, seed=rank, scale=args.scale)
     P = len(s["counts"])
     scan = Scan(s["counts"], s["y"], s["x"], s["wavelength"], s["distance"], s["detector_pixel"])
+    tuned = None
+    if not args.no_tune and not args.cluster and not args.stack:
+        # launch shapes by measurement, outside the timed region (ptyrs_b200.tune)
+        from ptyrs_b200.tune import autotune
+        best, table = autotune(scan, s["object"], s["probe"],
+                               run=lambda h: run_algorithm(h, wl, 1),
+                               prepare=lambda h: prepare(h, s, wl), device=local)
+        args.cluster, args.stack = best["cluster"], best["stack_size"]
+        tuned = {"chosen": best, "candidates_ms": [
+            {"cluster": o["cluster"], "stack": o["stack_size"],
+             "ms": None if ms is None else round(ms, 3)} for ms, o in table]}
     g = GpuPtycho(scan, s["object"], s["probe"], device=local, cluster=args.cluster,
                   stack_size=args.stack)
     prepare(g, s, wl)
@@ -435,7 +448,7 @@ def main():
                        "l2": "inputs larger than L2 (counts "
                              f"{s['counts'].nbytes / 1e6:.0f} MB)"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "accuracy": acc,
-            "gpu_launches": int(launches), "clocks": clk,
+            "gpu_launches": int(launches), "clocks": clk, "autotune": tuned,
             "kernels_ms": {k: round(v[0], 3) for k, v in sorted(times.items())},
         }
         print(json.dumps(line), flush=True)

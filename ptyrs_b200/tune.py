@@ -1,0 +1,41 @@
+"""The engine's launch shapes picked by measurement: for a scan, each candidate of the cluster
+size (the CTAs that share one frame's FFT tiles, so the rows each CTA transforms) and the stack
+(frames per launch of the whole-scan passes) runs one warm-up and one timed call of the
+algorithm on its own handle, timed on the device; the fastest wins. Candidates the device cannot
+launch (a cluster too large for its shared memory) are skipped.
+"""
+import itertools
+
+from .engine import GpuPtycho, PtybError
+
+
+def clusters_for(n):
+    """The cluster sizes the engine has kernels for at frame side `n` (0 lets it choose)."""
+    return {64: [1], 128: [2, 4], 256: [16, 8]}.get(n, [0])
+
+
+def autotune(scan, obj, probe, run, prepare=None, stacks=(256, 512, 1024), clusters=None,
+             device=0, **kw):
+    """`(best, table)`: `best` the `dict(cluster=..., stack_size=...)` of the fastest timed call
+    of `run(handle)` and `table` every candidate's `(ms, options)` (None if it failed);
+    `prepare(handle)` sets each fresh handle up (positions and the like) before the warm-up."""
+    n = probe.shape[-1]
+    clusters = clusters_for(n) if clusters is None else clusters
+    table = []
+    for c, st in itertools.product(clusters, stacks):
+        opts = dict(cluster=c, stack_size=st)
+        try:
+            with GpuPtycho(scan, obj, probe, device=device, **opts, **kw) as g:
+                if prepare is not None:
+                    prepare(g)
+                run(g)
+                g.synchronize()
+                run(g)
+                g.synchronize()
+                table.append((g.last_call_ms(), opts))
+        except PtybError:
+            table.append((None, opts))
+    timed = [t for t in table if t[0] is not None]
+    if not timed:
+        raise RuntimeError("no candidate launch shape ran")
+    return min(timed, key=lambda t: t[0])[1], table
