@@ -122,6 +122,9 @@ int ptyb_nslice(const ptyb_handle* h);
 
 /* Reference `GpuPtycho::objects` (engine/gpu/mod.rs:772-779): every slice, [nslice][nyo][nxo]. */
 int ptyb_get_objects(ptyb_handle* h, double* dst);
+/* No counterpart in the reference (its `set_object` replaces slice 0 alone): replaces every
+ * slice, [nslice][nyo][nxo], as the torch function of the adjoint needs. */
+int ptyb_set_objects(ptyb_handle* h, const double* src);
 
 /* Reference `GpuPtycho::rpie` (engine/gpu/rpie.rs:31-63). */
 int ptyb_rpie(ptyb_handle* h, const ptyb_rpie_params* params, int32_t nepoch);
@@ -143,7 +146,9 @@ int ptyb_get_llk(ptyb_handle* h, ptyb_llk* out);
  * engine/ptycho.rs:492-515; complex128 [nyo][nxo] and [nprobe][ny][nx]) and over each frame's
  * sub-pixel offset ∂L/∂d [nframe][2] (reference `position_grad`, engine/features.rs:1055-1100),
  * all under the position model when offsets are set. Any output may be NULL; d_pos needs
- * offsets (ptyb_set_positions). The handle's arrays are not changed. */
+ * offsets (ptyb_set_positions). On a multislice handle the model is the walk through every
+ * slice and d_obj is every slice's gradient, [nslice][nyo][nxo] (d_pos must be NULL). The
+ * handle's arrays are not changed. */
 int ptyb_gradients(ptyb_handle* h, double* loss, double* d_obj, double* d_probe, double* d_pos);
 
 /* The model intensity Σ_modes |Ψ|² of the current estimate for frames[0..n) into out[n][ny][nx]

@@ -82,6 +82,22 @@ class SliceWaves:
         return ops.obj_probe_to_psi(self.own, d, self.incident[s], self.shared(s))
 
 
+def multislice_grads(addr, obs, optics, objs, probe):
+    """The Poisson LLK sum through the slices and its gradients 2·∂L/∂O_s* per slice and
+    2·∂L/∂P*: the exit wave's `poisson_grad` back through the exit transform and the slices'
+    adjoints (engine/multislice.rs:266-286, 399-438), each slice's Σ conj(q_s·in_s)·g_s and
+    the probe's Σ conj(O_0)·g_0. Returns `(loss, [d_obj per slice], d_probe)`."""
+    views, nmode, nframe = addr.views, addr.nmode, addr.nframe
+    waves = SliceWaves(optics, views, objs, probe[views["probe"].astype(np.int64)])
+    psi = optics.exit_forward(waves.psi)
+    loss = ops.llk(obs, slice(0, nframe), nmode, psi).poisson
+    g = optics.exit_adjoint(ops.poisson_grad(obs, slice(0, nframe), nmode, psi))
+    chis = waves.back_propagate(g)
+    d_objs = [waves.obj_adjoint(s, chis[s]) for s in range(len(objs))]
+    d_probe = ops.accumulate_probe(views, objs[0], probe.shape, waves.shared(0), chis[0])[0]
+    return loss, d_objs, d_probe
+
+
 class Lsqml:
     """LSQML state across epochs (engine/lsqml.rs:415-430). cost: "poisson" or "amplitude"."""
 

@@ -57,6 +57,7 @@ SIGNATURES = {
                                      c_int32, P(c_double), c_int32, P(Options), P(c_void_p)]),
     "ptyb_nslice": (c_int32, [c_void_p]),
     "ptyb_get_objects": (c_int32, [c_void_p, P(c_double)]),
+    "ptyb_set_objects": (c_int32, [c_void_p, P(c_double)]),
     "ptyb_rpie": (c_int32, [c_void_p, P(RpieParams), c_int32]),
     "ptyb_lsqml": (c_int32, [c_void_p, P(LsqmlParams), c_int32, c_int32]),
     "ptyb_ml": (c_int32, [c_void_p, P(MlParams), c_int32]),

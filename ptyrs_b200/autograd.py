@@ -4,9 +4,10 @@ hand-written adjoint (`ptyb_gradients`).
     loss = PoissonLoss.apply(obj, probe, offsets, engine)
     loss.backward()       # obj.grad, probe.grad, offsets.grad
 
-`obj` is complex `[1, nyo, nxo]`, `probe` complex `[nprobe, ny, nx]`, `offsets` real
-`[nframe, 2]` (sub-pixel (dy, dx) per frame in object pixels under Patch sampling, physwkim/ptyrs
-engine/features.rs:558-1025), `engine` a `GpuPtycho` of the scan. The loss is the Poisson LLK
+`obj` is complex `[1, nyo, nxo]` (every slice, `[nslice, nyo, nxo]`, on a multislice engine),
+`probe` complex `[nprobe, ny, nx]`, `offsets` real `[nframe, 2]` (sub-pixel (dy, dx) per frame in
+object pixels under Patch sampling, physwkim/ptyrs engine/features.rs:558-1025) or None (required
+None on a multislice engine), `engine` a `GpuPtycho` of the scan. The loss is the Poisson LLK
 sum over the unmasked pixels (engine/ops.rs:119-154); the complex gradients follow torch's
 convention, ∂L/∂Re z + i·∂L/∂Im z, which is the reference's `obj_grad` / `probe_grad`
 (engine/ptycho.rs:492-515), and the offsets' gradient is its `position_grad`
@@ -19,13 +20,22 @@ import torch
 class PoissonLoss(torch.autograd.Function):
     @staticmethod
     def forward(ctx, obj, probe, offsets, engine):
-        engine.set_object(obj.detach().cpu().numpy().astype(np.complex128))
+        o = obj.detach().cpu().numpy().astype(np.complex128)
+        if engine.nslice() > 1:
+            engine.set_objects(o)
+        else:
+            engine.set_object(o)
         engine.set_probe(probe.detach().cpu().numpy().astype(np.complex128))
-        engine.set_positions(offsets.detach().cpu().numpy().astype(np.float64), refine=False)
+        if offsets is not None:
+            engine.set_positions(offsets.detach().cpu().numpy().astype(np.float64),
+                                 refine=False)
         g = engine.gradients(obj=ctx.needs_input_grad[0], probe=ctx.needs_input_grad[1],
-                             positions=True)
+                             positions=offsets is not None)
         grads = []
         for x, key in ((obj, "object"), (probe, "probe"), (offsets, "positions")):
+            if x is None:
+                grads.append(None)
+                continue
             v = g[key]
             grads.append(None if v is None else
                          torch.as_tensor(v, device=x.device).to(x.dtype).reshape(x.shape))

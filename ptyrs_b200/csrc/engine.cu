@@ -166,6 +166,9 @@ struct ptyb_handle {
   // probe gradient's summed spectrum under the position model.
   float2* psi_all = nullptr;
   float2* g_probe_spec = nullptr; // [K][N][N]
+  // Multislice gradients: every slice's 2·∂L/∂O_s* and its compensation.
+  float2* g_slices = nullptr;     // [S][nyo][nxo]
+  float2* g_slices_c = nullptr;
   double* partials = nullptr;    // [kPartialBlocks][2]
   std::vector<Buf> bufs;
   // Per-kernel device timing (CUDA events on the engine's stream), when enabled.
@@ -291,7 +294,7 @@ enum Kind : int {
   kKObjRpie, kKObjOverlap, kKObjLsqml, kKObjMl, kKIllum, kKProbePartial, kKProbeFinal,
   kKAfar, kKDots, kKSolve, kKAxpy, kKMax, kKCounts, kKMisc, kKGamma, kKArraySums, kKMove,
   kKPositionSums, kKSliceForward, kKSliceBackward, kKSliceLlk, kKFrameProject, kKSpectrum,
-  kKDerivSums, kKBackSpectrum, kNumKinds
+  kKDerivSums, kKBackSpectrum, kKSliceGrad, kNumKinds
 };
 const char* const kKindNames[kNumKinds] = {
     "frame_rpie", "frame_lsqml", "frame_ml_grad", "frame_llk", "frame_store",
@@ -299,7 +302,7 @@ const char* const kKindNames[kNumKinds] = {
     "illumination", "probe_partial", "probe_finalize", "lsqml_afar", "lsqml_dots",
     "lsqml_solve", "axpy", "max", "counts", "misc", "ml_gamma", "array_sums", "move",
     "position_sums", "slice_forward", "slice_backward", "slice_llk", "frame_project", "spectrum",
-    "deriv_sums", "back_spectrum"};
+    "deriv_sums", "back_spectrum", "slice_grad"};
 
 cudaEvent_t take_event(ptyb_handle* h) {
   if (!h->event_pool.empty()) {
@@ -509,6 +512,7 @@ cudaError_t launch_slice(ptyb_handle* h, const SliceArgs& a, int nslot) {
   if (nslot <= 0) return cudaSuccess;
   constexpr int kind = MODE == kSliceForward ? kKSliceForward
                        : MODE == kSliceBackward ? kKSliceBackward
+                       : MODE == kSliceGrad     ? kKSliceGrad
                                                 : kKSliceLlk;
   cudaError_t e = cudaErrorInvalidValue;
   timed(h, kind, [&] {
@@ -1060,6 +1064,83 @@ void lsqml_batch(ptyb_handle* h, const ptyb_lsqml_params& p, const int* frames, 
                                                     h->offsets);
     });
     launched(h, "position step");
+  }
+}
+
+// Every slice's 2·∂L/∂O_s* and the probe's 2·∂L/∂P* of the Poisson LLK sum through a
+// multislice object (the adjoint of engine/multislice.rs:87-173, 266-286, 399-438): per stack,
+// the exit wave's Poisson gradient back-propagated through the slices on chip, then per slice
+// Σ conj(q_s·in_s)·g_s gathered in frame order, the probe's Σ conj(O_0)·g_0.
+void ensure_ml(ptyb_handle* h);
+
+void slice_gradients(ptyb_handle* h, bool uo, bool up) {
+  const int S = h->nslice, stack = std::min(h->P, h->stack);
+  ensure_slots(h, stack);
+  ensure_ml(h);
+  const size_t plane = (size_t)h->N * h->N, fplanes = (size_t)h->K * plane;
+  const size_t no = (size_t)h->nyo * h->nxo;
+  if (!h->g_slices) {
+    h->g_slices = alloc<float2>(h, (size_t)S * no);
+    h->g_slices_c = alloc<float2>(h, (size_t)S * no);
+  }
+  check(h, cudaMemsetAsync(h->g_slices, 0, (size_t)S * no * sizeof(float2), h->stream), "memset");
+  check(h, cudaMemsetAsync(h->g_slices_c, 0, (size_t)S * no * sizeof(float2), h->stream), "memset");
+  check(h, cudaMemsetAsync(h->g_probe, 0, fplanes * sizeof(float2), h->stream), "memset");
+  check(h, cudaMemsetAsync(h->g_probe_c, 0, fplanes * sizeof(float2), h->stream), "memset");
+  for (int s0 = 0; s0 < h->P; s0 += stack) {
+    const int n = std::min(stack, h->P - s0);
+    const int* frames = h->iota + s0;
+    const size_t slice_stride = (size_t)n * fplanes;
+    SliceArgs sa = {};
+    sa.f = frame_args(h, frames);
+    sa.f.nslot = n;
+    sa.tf = h->tf;
+    sa.incident = h->incident;
+    sa.chi = h->chi_slices;
+    sa.nslice = S;
+    sa.obj_plane = no;
+    check(h, launch_slice<kSliceGrad>(h, sa, n), "multislice gradient");
+    ++h->launches;
+    for (int s = 0; uo && s < S; ++s) {
+      GatherArgs g = gather_args(h, frames, n);
+      g.upd = h->chi_slices + s * slice_stride;
+      g.out = h->g_slices + s * no;
+      g.comp = h->g_slices_c + s * no;
+      g.quad = s + 1 == S ? h->quad : h->ones;
+      if (s > 0) {
+        g.probe = h->incident + (s - 1) * slice_stride;
+        g.probe_stride = (int)fplanes;
+      }
+      timed(h, kKObjMl, [&] { object_tile_kernel<kGatherMl><<<ntiles(h), 1024, 0, h->stream>>>(g); }, n);
+      launched(h, "slice gradient");
+    }
+    if (up) {
+      int nchunk = 0;
+      const int chunk = probe_chunk(h, n, &nchunk);
+      ProbeArgs pa = {};
+      pa.object = h->object;
+      pa.quad = h->ones;
+      pa.upd = h->chi_slices;
+      pa.frames = frames;
+      pa.corners = h->corners;
+      pa.omax = h->omax;
+      pa.partial = h->partial;
+      pa.nslot = n;
+      pa.chunk = chunk;
+      pa.nxo = h->nxo;
+      pa.K = h->K;
+      pa.N = h->N;
+      pa.mode = 1;
+      dim3 grid((h->N * h->N + 255) / 256, nchunk);
+      timed(h, kKProbePartial, [&] { probe_partial_kernel<<<grid, 256, 0, h->stream>>>(pa); }, n);
+      launched(h, "probe gradient");
+      const int count = (int)fplanes;
+      timed(h, kKProbeFinal, [&] {
+        probe_finalize_kernel<<<(count + 255) / 256, 256, 0, h->stream>>>(
+            h->partial, nchunk, count, nullptr, h->g_probe, h->g_probe_c, 1.f, 2);
+      });
+      launched(h, "probe gradient sum");
+    }
   }
 }
 
@@ -1867,10 +1948,31 @@ int ptyb_get_llk(ptyb_handle* h, ptyb_llk* out) {
 
 int ptyb_gradients(ptyb_handle* h, double* loss, double* d_obj, double* d_probe, double* d_pos) {
   if (!h) return PTYB_INVALID;
-  if (h->nslice > 1) {
-    h->err = "the gradients run on a single-slice object";
+  if (h->nslice > 1 && d_pos) {
+    h->err = "position gradients run on a single-slice object";
     return PTYB_INVALID;
   }
+  if (h->nslice > 1)
+    return guarded(h, true, [&]() -> int {
+      slice_gradients(h, d_obj != nullptr, d_probe != nullptr);
+      const ptyb_llk l = llk_pass(h);
+      if (loss) *loss = l.poisson * h->nb_obs;
+      const size_t np = (size_t)h->K * h->N * h->N;
+      const size_t no = (size_t)h->nslice * h->nyo * h->nxo;
+      if (d_obj) {
+        std::vector<float2> v(no);
+        check(h, copy_sync(h, v.data(), h->g_slices, no * sizeof(float2), cudaMemcpyDeviceToHost),
+              "gradient");
+        to_c64(v.data(), d_obj, no);
+      }
+      if (d_probe) {
+        std::vector<float2> v(np);
+        check(h, copy_sync(h, v.data(), h->g_probe, np * sizeof(float2), cudaMemcpyDeviceToHost),
+              "gradient");
+        to_c64(v.data(), d_probe, np);
+      }
+      return PTYB_OK;
+    });
   if (d_pos && !h->have_offsets) {
     h->err = "position gradients need position offsets (ptyb_set_positions)";
     return PTYB_INVALID;
@@ -2067,6 +2169,17 @@ int ptyb_get_objects(ptyb_handle* h, double* dst) {
     check(h, cudaStreamSynchronize(h->stream), "sync");
     check(h, copy_sync(h, v.data(), h->object, n * sizeof(float2), cudaMemcpyDeviceToHost), "objects");
     to_c64(v.data(), dst, n);
+    return PTYB_OK;
+  });
+}
+
+int ptyb_set_objects(ptyb_handle* h, const double* src) {
+  if (!h || !src) return PTYB_INVALID;
+  return guarded(h, true, [&]() -> int {
+    const size_t n = (size_t)h->nslice * h->nobj * h->nyo * h->nxo;
+    auto v = from_c64(src, n);
+    check(h, copy_sync(h, h->object, v.data(), n * sizeof(float2), cudaMemcpyHostToDevice),
+          "objects");
     return PTYB_OK;
   });
 }

@@ -22,7 +22,10 @@ struct SliceArgs {
   size_t obj_plane;      // nyo·nxo: slice s's object at object + s·obj_plane
 };
 
-enum SliceMode : int { kSliceForward = 0, kSliceBackward = 1, kSliceLlk = 2 };
+// kSliceGrad: forward (incident waves stored), the Poisson gradient 2(1 − I/Ĩ) of the exit
+// wave (masked 0) and its back-propagation through the slices into `chi` (no subtraction):
+// every slice's 2·∂L/∂ψ_s*, the adjoint of the multislice model.
+enum SliceMode : int { kSliceForward = 0, kSliceBackward = 1, kSliceLlk = 2, kSliceGrad = 3 };
 
 // Window of slice s times `v` for every plane's rows of this CTA (shifted layout); the last
 // slice also takes q. `conj_mode` multiplies by conj(q·O) instead.
@@ -136,7 +139,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T, frame_min_blocks<N, C>())
     apply_window<N, C>(S, sa, 0, corner, r, K, false);
     for (int s = 0; s + 1 < sa.nslice; ++s) {
       through_gap<N, C>(S, sa.tf + (size_t)s * N * N, K, false, ltw, cluster, r);
-      if (MODE == kSliceForward)
+      if (MODE == kSliceForward || MODE == kSliceGrad)
         rows_io<N, C>(S, sa.incident + s * slice_stride + slot * frame_planes, r, K, true);
       apply_window<N, C>(S, sa, s + 1, corner, r, K, false);
     }
@@ -192,7 +195,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T, frame_min_blocks<N, C>())
     return;
   }
   float afar = 0.5f;
-  if (a.cost == kCostPoisson) {
+  if (MODE != kSliceGrad && a.cost == kCostPoisson) {
     const double prev = MODE == kSliceForward
                             ? batch_mean(a.a_prev, a.frames, a.a_prev_by_frame, a.nslot, red + 7)
                             : batch_mean(a.a_mid, a.frames, 0, a.nslot, red + 7);
@@ -227,11 +230,17 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T, frame_min_blocks<N, C>())
     const int idx = tid + i * T;
     const int c = idx % H, ky = idx / H;
     const float yo = yo_r[i], ic = ic_r[i];
-    float cres = 0.f;
-    if (yo >= 0.f)
-      cres = a.cost == kCostPoisson ? 1.f - yo / (ic + 1e-6f)
-                                    : 2.f * (1.f - sqrtf(fmaxf(yo, 0.f)) / (sqrtf(ic) + 1e-9f));
-    const float fac = (1.f - afar * cres) * inv_n2;
+    float fac;
+    if (MODE == kSliceGrad) {
+      // GradPoissonFourier (engine/ops.rs:161-195)
+      fac = (yo < 0.f ? 0.f : 2.f * (1.f - yo / fmaxf(ic, 1e-12f))) * inv_n2;
+    } else {
+      float cres = 0.f;
+      if (yo >= 0.f)
+        cres = a.cost == kCostPoisson ? 1.f - yo / (ic + 1e-6f)
+                                      : 2.f * (1.f - sqrtf(fmaxf(yo, 0.f)) / (sqrtf(ic) + 1e-9f));
+      fac = (1.f - afar * cres) * inv_n2;
+    }
     for (int m = 0; m < K; ++m) {
       float2& v = S[(m * H + c) * L + (ky ^ swz(m * H + c))];
       v = cscale(v, fac);
@@ -241,12 +250,12 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T, frame_min_blocks<N, C>())
   all_lines<N, C, +1>(S, K * H, ltw);
   transpose<N, C>(S, K, cluster);
   all_lines<N, C, +1>(S, K * H, ltw);
-  // χ of the last slice: ψ' − q·O_last·in_last.
+  // χ of the last slice: ψ' − q·O_last·in_last (the gradient: ψ' itself).
   const int last = sa.nslice - 1;
   const float2* in_last = last == 0 ? nullptr : sa.incident + (last - 1) * slice_stride + slot * frame_planes;
   const float2* obj_last = a.object + (size_t)last * sa.obj_plane;
 #pragma unroll 2
-  for (int idx = tid; idx < H * N; idx += T) {
+  for (int idx = tid; idx < (MODE == kSliceGrad ? 0 : H * N); idx += T) {
     const int yl = idx / N, jx = idx % N;
     const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
     const float2 oq =

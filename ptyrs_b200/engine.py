@@ -143,10 +143,13 @@ class GpuPtycho:
     def gradients(self, obj=True, probe=True, positions=True):
         """The Poisson LLK sum `loss` of the current estimate and its gradients through the
         hand-written adjoint: `object` and `probe` as 2·∂L/∂X* (the complex gradient torch
-        uses), `positions` ∂L/∂d `[nframe, 2]` (needs `set_positions`); a dict, None for
-        what is not asked."""
+        uses; on a multislice handle `object` holds every slice's), `positions` ∂L/∂d
+        `[nframe, 2]` (needs `set_positions`, single slice); a dict, None for what is not
+        asked."""
         loss = ctypes.c_double()
-        go = np.empty(self._obj_shape, np.complex128) if obj else None
+        oshape = ((self._nslice,) + tuple(self._obj_shape[1:]) if self._nslice > 1
+                  else self._obj_shape)
+        go = np.empty(oshape, np.complex128) if obj else None
         gp = np.empty(self._probe_shape, np.complex128) if probe else None
         gd = np.empty((self._nframe, 2), np.float64) if positions else None
         ptr = lambda a, view=True: None if a is None else _dptr(a.view(np.float64) if view else a)
@@ -191,6 +194,12 @@ class GpuPtycho:
         out = np.empty((self._nslice,) + tuple(self._obj_shape[1:]), np.complex128)
         self._check(self._lib.ptyb_get_objects(self._h, _dptr(out.view(np.float64))))
         return out
+
+    def set_objects(self, objs):
+        """Replaces every object slice `[nslice, nyo, nxo]`."""
+        objs = np.ascontiguousarray(objs, dtype=np.complex128).reshape(
+            (self._nslice,) + tuple(self._obj_shape[1:]))
+        self._check(self._lib.ptyb_set_objects(self._h, _dptr(objs.view(np.float64))))
 
     def probe(self):
         out = np.empty(self._probe_shape, np.complex128)

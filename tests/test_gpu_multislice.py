@@ -150,3 +150,31 @@ def test_set_object_replaces_slice_zero(case):
         objs = g.objects()
         assert np.array_equal(objs[0:1], new)
         assert np.array_equal(objs[1:], np.ones((2, side, side)))
+
+
+def test_gradients_through_slices_match_oracle(case):
+    """The adjoint through the slices (`ptyb_gradients` on a multislice handle): the Poisson
+    sum, every slice's gradient and the probe's against the oracle's `multislice_grads`, whose
+    gradients match central differences (test_oracle_multislice_grad.py); and the torch
+    function on it."""
+    import torch
+
+    from oracle.lsqml import multislice_grads
+    from ptyrs_b200.autograd import poisson_loss
+    cpu = oracle_of(case)
+    rng = np.random.default_rng(2)
+    objs = [o * (1 + 0.05 * rng.normal(size=o.shape)) * np.exp(0.05j) for o in case["objects"]]
+    loss, d_objs, d_probe = multislice_grads(cpu.addr, cpu.obs, cpu.optics, objs, cpu.probe)
+    with gpu_of(case) as g:
+        g.set_objects(np.concatenate(objs))
+        got = g.gradients(positions=False)
+        assert abs(got["loss"] - loss) <= ONE_STEP_TOL * abs(loss)
+        for k in range(3):
+            assert rel_l2(got["object"][k], d_objs[k][0]) < RUN_TOL, k
+        assert rel_l2(got["probe"], d_probe) < RUN_TOL
+        o = torch.tensor(np.concatenate(objs), requires_grad=True)
+        p = torch.tensor(case["probe"], requires_grad=True)
+        t = poisson_loss(o, p, None, g)
+        t.backward()
+        assert np.array_equal(o.grad.numpy(), got["object"])
+        assert np.array_equal(p.grad.numpy(), got["probe"])
