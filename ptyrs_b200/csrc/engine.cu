@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -1144,17 +1145,62 @@ void slice_gradients(ptyb_handle* h, bool uo, bool up) {
   }
 }
 
-void to_c64(const float2* src, double* dst, size_t n) {
-  for (size_t i = 0; i < n; ++i) {
-    dst[2 * i] = src[i].x;
-    dst[2 * i + 1] = src[i].y;
+// Runs fn(begin, end) over [0, n) on up to eight host threads (one below a million).
+template <class F>
+void parallel_range(size_t n, F&& fn) {
+  const size_t nt = n < (size_t(1) << 20) ? 1 : std::min<size_t>(8, std::thread::hardware_concurrency());
+  if (nt <= 1) {
+    fn(size_t(0), n);
+    return;
   }
+  std::vector<std::thread> ts;
+  const size_t chunk = (n + nt - 1) / nt;
+  for (size_t t = 0; t < nt; ++t) {
+    const size_t b = t * chunk, e = std::min(n, b + chunk);
+    if (b < e) ts.emplace_back([&fn, b, e] { fn(b, e); });
+  }
+  for (auto& t : ts) t.join();
 }
 
-std::vector<float2> from_c64(const double* src, size_t n) {
-  std::vector<float2> v(n);
-  for (size_t i = 0; i < n; ++i) v[i] = make_float2((float)src[2 * i], (float)src[2 * i + 1]);
-  return v;
+// The process's page-locked host staging buffer of at least n float2, grown on demand and kept
+// (as the device pool keeps device memory), so that a new handle does not pin pages again.
+// Callers hold g_stage_mutex while they use it.
+std::mutex g_stage_mutex;
+float2* g_stage = nullptr;
+size_t g_stage_n = 0;
+
+float2* staging(ptyb_handle* h, size_t n) {
+  if (n > g_stage_n) {
+    if (g_stage) cudaFreeHost(g_stage);
+    g_stage = nullptr;
+    g_stage_n = 0;
+    check(h, cudaMallocHost(&g_stage, n * sizeof(float2)), "cudaMallocHost");
+    g_stage_n = n;
+  }
+  return g_stage;
+}
+
+// Device float2 [n] to host complex128 [n] through the staging buffer.
+void download_c64(ptyb_handle* h, const float2* src, double* dst, size_t n, const char* what) {
+  std::lock_guard<std::mutex> lock(g_stage_mutex);
+  float2* st = staging(h, n);
+  check(h, copy_sync(h, st, src, n * sizeof(float2), cudaMemcpyDeviceToHost), what);
+  parallel_range(n, [&](size_t b, size_t e) {
+    for (size_t i = b; i < e; ++i) {
+      dst[2 * i] = st[i].x;
+      dst[2 * i + 1] = st[i].y;
+    }
+  });
+}
+
+// Host complex128 [n] to device float2 [n] through the staging buffer.
+void upload_c64(ptyb_handle* h, const double* src, float2* dst, size_t n, const char* what) {
+  std::lock_guard<std::mutex> lock(g_stage_mutex);
+  float2* st = staging(h, n);
+  parallel_range(n, [&](size_t b, size_t e) {
+    for (size_t i = b; i < e; ++i) st[i] = make_float2((float)src[2 * i], (float)src[2 * i + 1]);
+  });
+  check(h, copy_sync(h, dst, st, n * sizeof(float2), cudaMemcpyHostToDevice), what);
 }
 
 template <int N, int C>
@@ -1636,13 +1682,9 @@ int create_handle(const ptyb_scan* scan, const double* object, int32_t nobj, int
     check(h, copy_sync(h, h->corners, h->corners_h.data(), h->P * sizeof(int2), cudaMemcpyHostToDevice),
           "corners upload");
     h->object = alloc<float2>(h, (size_t)nslice * nobj * nyo * nxo);
-    auto o = from_c64(object, (size_t)nslice * nobj * nyo * nxo);
-    check(h, copy_sync(h, h->object, o.data(), o.size() * sizeof(float2), cudaMemcpyHostToDevice),
-          "object upload");
+    upload_c64(h, object, h->object, (size_t)nslice * nobj * nyo * nxo, "object upload");
     h->probe = alloc<float2>(h, (size_t)nprobe * plane);
-    auto pr = from_c64(probe, (size_t)nprobe * plane);
-    check(h, copy_sync(h, h->probe, pr.data(), pr.size() * sizeof(float2), cudaMemcpyHostToDevice),
-          "probe upload");
+    upload_c64(h, probe, h->probe, (size_t)nprobe * plane, "probe upload");
     // Far-field plane phase (engine/ops.rs:17-33) and the FFT twiddles, in double.
     std::vector<float2> q(plane), tw(N);
     const double fq = M_PI / (scan->wavelength * scan->distance);
@@ -1960,16 +2002,10 @@ int ptyb_gradients(ptyb_handle* h, double* loss, double* d_obj, double* d_probe,
       const size_t np = (size_t)h->K * h->N * h->N;
       const size_t no = (size_t)h->nslice * h->nyo * h->nxo;
       if (d_obj) {
-        std::vector<float2> v(no);
-        check(h, copy_sync(h, v.data(), h->g_slices, no * sizeof(float2), cudaMemcpyDeviceToHost),
-              "gradient");
-        to_c64(v.data(), d_obj, no);
+        download_c64(h, h->g_slices, d_obj, no, "gradient");
       }
       if (d_probe) {
-        std::vector<float2> v(np);
-        check(h, copy_sync(h, v.data(), h->g_probe, np * sizeof(float2), cudaMemcpyDeviceToHost),
-              "gradient");
-        to_c64(v.data(), d_probe, np);
+        download_c64(h, h->g_probe, d_probe, np, "gradient");
       }
       return PTYB_OK;
     });
@@ -1999,16 +2035,10 @@ int ptyb_gradients(ptyb_handle* h, double* loss, double* d_obj, double* d_probe,
     const ptyb_llk l = llk_pass(h, h->have_offsets ? h->wave_all : nullptr);
     if (loss) *loss = l.poisson * h->nb_obs;
     if (d_obj) {
-      std::vector<float2> v(no);
-      check(h, copy_sync(h, v.data(), h->g_obj, no * sizeof(float2), cudaMemcpyDeviceToHost),
-            "gradient");
-      to_c64(v.data(), d_obj, no);
+      download_c64(h, h->g_obj, d_obj, no, "gradient");
     }
     if (d_probe) {
-      std::vector<float2> v(np);
-      check(h, copy_sync(h, v.data(), h->g_probe, np * sizeof(float2), cudaMemcpyDeviceToHost),
-            "gradient");
-      to_c64(v.data(), d_probe, np);
+      download_c64(h, h->g_probe, d_probe, np, "gradient");
     }
     if (d_pos) {
       std::vector<double> v((size_t)h->P * 4);
@@ -2153,10 +2183,7 @@ int ptyb_get_object(ptyb_handle* h, double* dst) {
   if (!h || !dst) return PTYB_INVALID;
   return guarded(h, false, [&]() -> int {
     const size_t n = (size_t)h->nobj * h->nyo * h->nxo;
-    std::vector<float2> v(n);
-    check(h, cudaStreamSynchronize(h->stream), "sync");
-    check(h, copy_sync(h, v.data(), h->object, n * sizeof(float2), cudaMemcpyDeviceToHost), "object");
-    to_c64(v.data(), dst, n);
+    download_c64(h, h->object, dst, n, "object");
     return PTYB_OK;
   });
 }
@@ -2165,10 +2192,7 @@ int ptyb_get_objects(ptyb_handle* h, double* dst) {
   if (!h || !dst) return PTYB_INVALID;
   return guarded(h, false, [&]() -> int {
     const size_t n = (size_t)h->nslice * h->nobj * h->nyo * h->nxo;
-    std::vector<float2> v(n);
-    check(h, cudaStreamSynchronize(h->stream), "sync");
-    check(h, copy_sync(h, v.data(), h->object, n * sizeof(float2), cudaMemcpyDeviceToHost), "objects");
-    to_c64(v.data(), dst, n);
+    download_c64(h, h->object, dst, n, "objects");
     return PTYB_OK;
   });
 }
@@ -2177,9 +2201,7 @@ int ptyb_set_objects(ptyb_handle* h, const double* src) {
   if (!h || !src) return PTYB_INVALID;
   return guarded(h, true, [&]() -> int {
     const size_t n = (size_t)h->nslice * h->nobj * h->nyo * h->nxo;
-    auto v = from_c64(src, n);
-    check(h, copy_sync(h, h->object, v.data(), n * sizeof(float2), cudaMemcpyHostToDevice),
-          "objects");
+    upload_c64(h, src, h->object, n, "objects");
     return PTYB_OK;
   });
 }
@@ -2188,10 +2210,7 @@ int ptyb_get_probe(ptyb_handle* h, double* dst) {
   if (!h || !dst) return PTYB_INVALID;
   return guarded(h, false, [&]() -> int {
     const size_t n = (size_t)h->nprobe * h->N * h->N;
-    std::vector<float2> v(n);
-    check(h, cudaStreamSynchronize(h->stream), "sync");
-    check(h, copy_sync(h, v.data(), h->probe, n * sizeof(float2), cudaMemcpyDeviceToHost), "probe");
-    to_c64(v.data(), dst, n);
+    download_c64(h, h->probe, dst, n, "probe");
     return PTYB_OK;
   });
 }
@@ -2200,9 +2219,7 @@ int ptyb_set_object(ptyb_handle* h, const double* src) {
   if (!h || !src) return PTYB_INVALID;
   return guarded(h, true, [&]() -> int {
     const size_t n = (size_t)h->nobj * h->nyo * h->nxo;
-    auto v = from_c64(src, n);
-    check(h, cudaStreamSynchronize(h->stream), "sync");
-    check(h, copy_sync(h, h->object, v.data(), n * sizeof(float2), cudaMemcpyHostToDevice), "object");
+    upload_c64(h, src, h->object, n, "object");
     return PTYB_OK;
   });
 }
@@ -2211,9 +2228,7 @@ int ptyb_set_probe(ptyb_handle* h, const double* src) {
   if (!h || !src) return PTYB_INVALID;
   return guarded(h, true, [&]() -> int {
     const size_t n = (size_t)h->nprobe * h->N * h->N;
-    auto v = from_c64(src, n);
-    check(h, cudaStreamSynchronize(h->stream), "sync");
-    check(h, copy_sync(h, h->probe, v.data(), n * sizeof(float2), cudaMemcpyHostToDevice), "probe");
+    upload_c64(h, src, h->probe, n, "probe");
     return PTYB_OK;
   });
 }
