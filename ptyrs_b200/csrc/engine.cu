@@ -1519,8 +1519,9 @@ void zero_phase_ramp(ptyb_handle* h) {
 }
 
 // PyNX ScaleObjProbe(absolute=True) without background (engine/ptycho.rs:577-591).
-void scale_obj_probe(ptyb_handle* h) {
-  const ptyb_llk l = llk_pass(h);
+// `waves` (optional): every frame's moved probe of the current probe, scaled along with it.
+void scale_obj_probe(ptyb_handle* h, float2* waves = nullptr) {
+  const ptyb_llk l = llk_pass(h, waves);
   const double s = std::sqrt(h->obs_total / l.nb_photons_calc);
   const size_t no = (size_t)h->nobj * h->nyo * h->nxo, np = (size_t)h->K * h->N * h->N;
   double so[2], sp[2];
@@ -1531,6 +1532,12 @@ void scale_obj_probe(ptyb_handle* h) {
   launched(h, "scale");
   timed(h, kKAxpy, [&] { scale_kernel<<<blocks_for(no), 256, 0, h->stream>>>(h->object, (float)fo, no); });
   launched(h, "scale");
+  if (waves) {
+    // the moves are linear in the probe: the moved probes scale by the same factor
+    const size_t nw = (size_t)h->P * np;
+    timed(h, kKAxpy, [&] { scale_kernel<<<blocks_for(nw), 256, 0, h->stream>>>(waves, (float)fp, nw); });
+    launched(h, "scale");
+  }
 }
 
 template <typename F>
@@ -1906,19 +1913,27 @@ int ptyb_ml(ptyb_handle* h, const ptyb_ml_params* p, int32_t ncycle) {
     const bool uo = p->update_object != 0, up = p->update_probe != 0;
     const size_t no = (size_t)h->nyo * h->nxo, np = (size_t)h->K * h->N * h->N;
     begin_call(h);
-    scale_obj_probe(h);
+    auto move_all = [&] {
+      // every frame's moved probe of the current probe, from its spectra
+      spectrum_of(h, h->probe, h->spec);
+      const int stack = std::min(h->P, h->stack);
+      for (int s0 = 0; s0 < h->P; s0 += stack)
+        move_frames(h, h->iota + s0, std::min(stack, h->P - s0), h->spec,
+                    h->wave_all + (size_t)s0 * h->K * h->N * h->N);
+    };
+    if (h->have_offsets) move_all();
+    // the opening rescale's LLK reads the moved probes, which it scales with the probe
+    scale_obj_probe(h, h->have_offsets ? h->wave_all : nullptr);
     check(h, cudaMemsetAsync(h->dir_obj, 0, no * sizeof(float2), h->stream), "memset");
     check(h, cudaMemsetAsync(h->dir_probe, 0, np * sizeof(float2), h->stream), "memset");
     bool have_last = false;
     for (int ic = 0; ic < ncycle; ++ic) {
       const bool due = llk_due(p->calc_llk, ic, ncycle);
       if (h->have_offsets) {
-        // every frame's moved probe for this cycle, from the probe's spectra
-        spectrum_of(h, h->probe, h->spec);
-        const int stack = std::min(h->P, h->stack);
-        for (int s0 = 0; s0 < h->P; s0 += stack)
-          move_frames(h, h->iota + s0, std::min(stack, h->P - s0), h->spec,
-                      h->wave_all + (size_t)s0 * h->K * h->N * h->N);
+        if (ic == 0)
+          spectrum_of(h, h->probe, h->spec);  // the moved probes were scaled above
+        else
+          move_all();
       }
       ptyb_llk l = {};
       if (due) l = llk_pass(h, h->have_offsets ? h->wave_all : nullptr);
