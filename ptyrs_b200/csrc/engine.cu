@@ -166,6 +166,7 @@ struct ptyb_handle {
   // ML: every frame's detector field of one cycle's gradient pass, [P][K][kx][ky], and the
   // probe gradient's summed spectrum under the position model.
   float2* psi_all = nullptr;
+  float2* g_all = nullptr;         // [P][K][N][N] the gradient pass's exit-plane field g
   float2* g_probe_spec = nullptr; // [K][N][N]
   // Multislice gradients: every slice's 2·∂L/∂O_s* and its compensation.
   float2* g_slices = nullptr;     // [S][nyo][nxo]
@@ -1260,6 +1261,7 @@ void ensure_ml(ptyb_handle* h) {
   h->dir_probe = alloc<float2>(h, np);
   h->gamma_sums = alloc<double>(h, (size_t)h->P * 2);
   h->psi_all = alloc<float2>(h, (size_t)h->P * np);
+  h->g_all = alloc<float2>(h, (size_t)h->P * np);
   h->g_probe_spec = alloc<float2>(h, np);
   h->partials = alloc<double>(h, kPartialBlocks * 2);
 }
@@ -1306,6 +1308,9 @@ void ml_gradients(ptyb_handle* h, bool uo, bool up, bool refine, bool pos_grad =
     const int n = std::min(stack, h->P - s0);
     const int* frames = h->iota + s0;
     FrameArgs a = frame_args(h, frames);
+    // the gradient field g of these frames, kept for the line search
+    float2* gfield = h->g_all + (size_t)s0 * pstride;
+    a.out = gfield;
     const float2* waves = h->have_offsets ? h->wave_all + (size_t)s0 * pstride : nullptr;
     if (waves) {
       // each frame's moved probe conj(q)·T_d(q·P) in place of P (engine/ptycho.rs:373-450)
@@ -1324,6 +1329,7 @@ void ml_gradients(ptyb_handle* h, bool uo, bool up, bool refine, bool pos_grad =
     }
     if (uo) {
       GatherArgs g = gather_args(h, frames, n);
+      g.upd = gfield;
       g.out = h->g_obj;
       g.comp = h->g_obj_c;
       if (waves) {
@@ -1336,7 +1342,7 @@ void ml_gradients(ptyb_handle* h, bool uo, bool up, bool refine, bool pos_grad =
     if (up && h->have_offsets) {
       // DFT(conj(O_win)·g)·exp(+2πi f·d) per frame, summed in frame order
       MoveArgs mb = move_args(h, frames, h->wave2);
-      mb.c = h->upd;
+      mb.c = gfield;
       check(h, launch_move<kBackSpectrum>(h, mb, n), "probe gradient spectra");
       ++h->launches;
       timed(h, kKProbeFinal, [&] {
@@ -1350,7 +1356,7 @@ void ml_gradients(ptyb_handle* h, bool uo, bool up, bool refine, bool pos_grad =
       ProbeArgs pa = {};
       pa.object = h->object;
       pa.quad = h->quad;
-      pa.upd = h->upd;
+      pa.upd = gfield;
       pa.frames = frames;
       pa.corners = h->corners;
       pa.omax = h->omax;
@@ -1377,7 +1383,7 @@ void ml_gradients(ptyb_handle* h, bool uo, bool up, bool refine, bool pos_grad =
       // sums are ∂L/∂d (engine/features.rs:1055-1100)
       MoveArgs md = move_args(h, frames, nullptr);
       md.spec = h->spec;
-      md.c = refine ? h->field : h->upd;
+      md.c = refine ? h->field : gfield;
       md.sums = h->ml_pos_sums;
       check(h, launch_move<kDerivSums>(h, md, n), "position sums");
       ++h->launches;
@@ -1414,6 +1420,7 @@ void ml_gamma(ptyb_handle* h, double* num, double* den) {
     a.frames = h->iota + s0;
     a.out = h->gamma_sums + (size_t)s0 * 2;
     a.psi = h->psi_all + (size_t)s0 * h->K * h->N * h->N;
+    a.g = h->g_all + (size_t)s0 * h->K * h->N * h->N;
     if (h->have_offsets) {
       // the probe and its direction, each moved by the frame's offset (engine/ptycho.rs:527-534)
       move_frames(h, a.frames, n, h->spec_d, h->wave2);

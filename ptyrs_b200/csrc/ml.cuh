@@ -10,8 +10,10 @@ namespace ptyb {
 // Per frame: with po = F(P·O·q) the gradient pass kept, a = F(P·dO·q + dP·O·q) and
 // b = F(dP·dO·q) mode by mode, per-pixel accumulators calc = Σ|po|², r = Σ Re(p̄o·a),
 // s = Σ |a|² + 2·Re(p̄o·b); then over unmasked pixels, d = 1 − I/max(calc, 1e-32):
-// num = −Σ 2·r·d, den = Σ 2·s·d + I·(2r/calc)². Shared memory: one plane of H lines (a, then
-// b) and the three accumulators (rows padded to N + 1), so two CTAs share an SM.
+// num = −Σ 2·r·d, den = Σ 2·s·d + I·(2r/calc)². The b-term of den is linear in b, so it is
+// taken in the exit plane against the gradient pass's field (no transform of b). Shared
+// memory: one plane of H lines (a) and the three accumulators (rows padded to N + 1), so two
+// CTAs share an SM.
 struct GammaArgs {
   const float2* object;
   const float2* d_obj;
@@ -27,8 +29,10 @@ struct GammaArgs {
   // Elements between consecutive slots' probe and probe direction: 0 for the shared ones,
   // K·N·N for the per-frame moved ones of the position model.
   int probe_stride;
-  // po = DFT(P·O·q) of every slot and mode as the gradient pass kept it, [slot][K][kx][ky].
+  // po = DFT(P·O·q) of every slot and mode as the gradient pass kept it, [slot][K][kx][ky],
+  // and its exit-plane gradient field g = IDFT(2(1 − I/Ĩ)·po)/N² (masked 0), [slot][K][N][N].
   const float2* psi;
+  const float2* g;
 };
 
 template <int N, int C>
@@ -58,43 +62,40 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T, 2) gamma_kernel(GammaArgs
   ltw.load(a.tw, tid % F::G);
   for (int i = tid; i < 3 * H * AS; i += T) acc[i] = 0.f;
 
+  // The b-term of den, Σ_pix 2·d·2·Re(p̄o·B)/N², by Parseval in the exit plane:
+  // 2·Re Σ_x conj(g)·b with g = IDFT(2d·po)/N² the gradient pass's field (0 where masked).
+  double gb = 0.0;
   for (int m = 0; m < K; ++m) {
     const int pm = m % a.nprobe, om = m / a.nprobe;
     const float2* po_m = a.psi + ((size_t)slot * K + m) * N * N + (size_t)r * H * N;
-#pragma unroll 1
-    for (int pass = 0; pass < 2; ++pass) {
-      // Exit-plane rows of a (pass 0) or b (pass 1).
+    const float2* g_m = a.g + ((size_t)slot * K + m) * N * N;
+    // Exit-plane rows of a; b and its product with g on the way.
 #pragma unroll 4
-      for (int idx = tid; idx < H * N; idx += T) {
-        const int yl = idx / N, jx = idx % N;
-        const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
-        const size_t pi = (size_t)slot * a.probe_stride + ((size_t)pm * N + ny) * N + nx;
-        const size_t oi = ((size_t)om * a.nyo + corner.x + ny) * a.nxo + corner.y + nx;
-        const float2 dp = a.d_probe[pi], dob = a.d_obj[oi], q = a.quad[ny * N + nx];
-        const float2 v = pass == 0 ? cadd(cmul(a.probe[pi], dob), cmul(dp, a.object[oi]))
-                                   : cmul(dp, dob);
-        S1[yl * L + (jx ^ swz(yl))] = cmul(v, q);
-      }
-      __syncthreads();
-      all_lines<N, C, -1>(S1, H, ltw);
-      transpose<N, C>(S1, 1, cluster);
-      all_lines<N, C, -1>(S1, H, ltw);
-      // Columns kx = r·H + c, elements ky; po read from the gradient pass's columns.
-#pragma unroll 4
-      for (int idx = tid; idx < H * N; idx += T) {
-        const int c = idx / N, ky = idx % N;
-        const float2 po = po_m[(size_t)c * N + ky], v = S1[c * L + (ky ^ swz(c))];
-        const float pv = (po.x * v.x + po.y * v.y) * inv_n2;
-        if (pass == 0) {
-          acc[c * AS + ky] += cnorm2(po) * inv_n2;
-          acc[(H + c) * AS + ky] += pv;
-          acc[(2 * H + c) * AS + ky] += cnorm2(v) * inv_n2;
-        } else {
-          acc[(2 * H + c) * AS + ky] += 2.f * pv;
-        }
-      }
-      __syncthreads();
+    for (int idx = tid; idx < H * N; idx += T) {
+      const int yl = idx / N, jx = idx % N;
+      const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
+      const size_t pi = (size_t)slot * a.probe_stride + ((size_t)pm * N + ny) * N + nx;
+      const size_t oi = ((size_t)om * a.nyo + corner.x + ny) * a.nxo + corner.y + nx;
+      const float2 dp = a.d_probe[pi], dob = a.d_obj[oi], q = a.quad[ny * N + nx];
+      const float2 v = cadd(cmul(a.probe[pi], dob), cmul(dp, a.object[oi]));
+      S1[yl * L + (jx ^ swz(yl))] = cmul(v, q);
+      const float2 b = cmul(cmul(dp, dob), q), gv = g_m[(size_t)ny * N + nx];
+      gb += (double)gv.x * b.x + (double)gv.y * b.y;
     }
+    __syncthreads();
+    all_lines<N, C, -1>(S1, H, ltw);
+    transpose<N, C>(S1, 1, cluster);
+    all_lines<N, C, -1>(S1, H, ltw);
+    // Columns kx = r·H + c, elements ky; po read from the gradient pass's columns.
+#pragma unroll 4
+    for (int idx = tid; idx < H * N; idx += T) {
+      const int c = idx / N, ky = idx % N;
+      const float2 po = po_m[(size_t)c * N + ky], v = S1[c * L + (ky ^ swz(c))];
+      acc[c * AS + ky] += cnorm2(po) * inv_n2;
+      acc[(H + c) * AS + ky] += (po.x * v.x + po.y * v.y) * inv_n2;
+      acc[(2 * H + c) * AS + ky] += cnorm2(v) * inv_n2;
+    }
+    __syncthreads();
   }
   const float* iobs = a.iobs + (size_t)f * N * N;
   double v[4] = {0.0, 0.0, 0.0, 0.0};
@@ -109,6 +110,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T, 2) gamma_kernel(GammaArgs
     const double t = 2.0 * rr / calc;
     v[1] += 2.0 * ss * d + (double)yo * t * t;
   }
+  v[1] += 2.0 * gb;
   block_sum<T>(v, 2, red);
   csync<C>(cluster);
   if (r == 0 && tid == 0) {
