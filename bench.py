@@ -155,8 +155,9 @@ def algorithmic_bytes(kind, s, wl):
         "frame_ml_grad": 8 * n2 + 4 * n2 + 16 * K * n2 + moved,
         # projection from the kept Ψ: Ψ read, object window, counts, (moved probe), change
         "frame_project": 8 * n2 + 4 * n2 + 16 * K * n2 + moved,
-        # line search: object and direction windows, counts, kept Ψ, (moved probe and direction)
-        "ml_gamma": 16 * n2 + 4 * n2 + 8 * K * n2 + 2 * moved,
+        # line search: object and direction windows, counts, kept Ψ and g, (moved probe and
+        # direction)
+        "ml_gamma": 16 * n2 + 4 * n2 + 16 * K * n2 + 2 * moved,
         "move": 8 * K * n2,
         "back_spectrum": 16 * K * n2 + 8 * n2,
         "deriv_sums": 8 * K * n2 + 8 * n2,
@@ -179,7 +180,7 @@ def sample_scan(s, m):
 # its launches' frames) on the 1000-frame cut of the ml256 scan, profiles/ml256_launch_list.md:
 # roofline.traffic scales them to the launch's frames.
 NCU_DRAM_BYTES_PER_FRAME = {
-    "ml256": {"ml_gamma": 3.45e6, "frame_ml_grad": 3.51e6, "frame_project": 3.54e6,
+    "ml256": {"ml_gamma": 4.51e6, "frame_ml_grad": 3.51e6, "frame_project": 3.54e6,
               "deriv_sums": 1.06e6, "move": 0.97e6, "back_spectrum": 2.06e6,
               "object_ml": 2.17e6, "frame_llk": 1.34e6},
 }
