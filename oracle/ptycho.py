@@ -209,7 +209,11 @@ class Ptycho:
     def scale_obj_probe(self):
         """PyNX ScaleObjProbe(absolute=True) without background (engine/ptycho.rs:577-591)."""
         calc = self.llk().nb_photons_calc
-        s = np.sqrt(self.obs.total() / calc)
+        self.split_scale(np.sqrt(self.obs.total() / calc))
+
+    def split_scale(self, s):
+        """Scale `O·P` by `s` and balance `Σ|O|` and `Σ|P|` (engine/ptycho.rs:593-603); with
+        `s = 1` PyNX ScaleObjProbe(absolute=False)."""
         os_ = float(np.abs(self.object).sum())
         ps = float(np.abs(self.probe).sum())
         fp, fo = np.sqrt(os_ / ps * s), np.sqrt(ps / os_ * s)
@@ -297,7 +301,7 @@ class Ptycho:
         """PyNX ZeroPhaseRamp (engine/ptycho.rs:1134-1170)."""
         self.object, self.probe = zero_phase_ramp(self.object, self.probe)
 
-    # AP (only as the warm-up of the reference's golden ML run) ----------------------------
+    # AP ---------------------------------------------------------------------------------
     def ap(self, ncycle, obj_inertia=0.01, probe_inertia=None, calc_llk=0,
            zero_phase_ramp=True):
         """PyNX AP without features (engine/ptycho.rs:609-641, ops.rs:352-381)."""
@@ -319,6 +323,79 @@ class Ptycho:
                 self.object = _blend(self.object, acc[0], acc[1], obj_inertia)
             if l is not None:
                 self.record("ap", l)
+            self.cycle += 1
+        if zero_phase_ramp:
+            self.zero_phase_ramp()
+
+    # DM and RAAR ------------------------------------------------------------------------
+    def _project(self, psi):
+        """Object-plane magnitude projection `F⁻¹ Π_F F psi` (engine/ptycho.rs:671-674)."""
+        far = self.optics.exit_forward(psi)
+        far = ops.apply_amplitude(self.obs, slice(0, self.addr.nframe), self.addr.nmode, far)
+        return self.optics.exit_adjoint(far)
+
+    def update_obj_probe(self, psi, obj_inertia, probe_inertia, loops):
+        """DM's and RAAR's update (engine/ptycho.rs:732-754) without features: `loops` times an
+        object-only then a probe-only `psi_to_obj_probe`, so the probe update sees the new
+        object (engine/ops.rs:352-369)."""
+        views, q = self.addr.views, self.optics.quad
+        for _ in range(loops):
+            if obj_inertia is not None:
+                num, norm = ops.accumulate_obj(views, self.object.shape, self.probe, q, psi)
+                self.object = _blend(self.object, num, norm, obj_inertia)
+            if probe_inertia is not None:
+                num, norm = ops.accumulate_probe(views, self.object, self.probe.shape, q, psi)
+                self.probe = _blend(self.probe, num, norm, probe_inertia)
+
+    def dm(self, ncycle, obj_inertia=0.01, probe_inertia=0.001, alpha=0.02, loop_obj_probe=1,
+           calc_llk=0, zero_phase_ramp=True):
+        """PyNX DM with `a = alpha` (engine/ptycho.rs:653-691): cycle 0 starts from `psi = PO`,
+        later cycles reflect the carried `psi`, `psi ← (2 − a)·PO − (1 − a)·psi`, project it
+        and add `(1 − a)·(PO − refl)`; the LLK is of the estimate the cycle starts from, and a
+        recorded cycle ends with `split_scale(1)`."""
+        a = alpha
+        psi = None
+        for ic in range(ncycle):
+            l = self.llk() if llk_due(calc_llk, ic, ncycle) else None
+            po = self.calc_psi()
+            if ic == 0:
+                psi = po.copy()
+                refl = None
+            else:
+                psi = po * (2.0 - a) - psi * (1.0 - a)
+                refl = psi.copy()
+            psi = self._project(psi)
+            if refl is not None:
+                psi = psi + (po - refl) * (1.0 - a)
+            self.update_obj_probe(psi, obj_inertia, probe_inertia, loop_obj_probe)
+            if l is not None:
+                self.record("dm", l)
+                self.split_scale(1.0)
+            self.cycle += 1
+        if zero_phase_ramp:
+            self.zero_phase_ramp()
+
+    def raar(self, ncycle, obj_inertia=0.01, probe_inertia=0.001, beta=0.9, loop_obj_probe=1,
+             calc_llk=0, zero_phase_ramp=True):
+        """PyNX RAAR with `b = beta` (engine/ptycho.rs:698-730): cycle 0 starts from
+        `psi = PO`, later cycles mix the carried projection with the carried iterate,
+        `psi ← (1 − b/2)·psi + (b/2)·(2·PO − it)`, which becomes the next iterate, then
+        project; update, LLK record and balance as DM's."""
+        h = 0.5 * beta
+        psi = it = None
+        for ic in range(ncycle):
+            l = self.llk() if llk_due(calc_llk, ic, ncycle) else None
+            po = self.calc_psi()
+            if ic == 0:
+                psi = po.copy()
+            else:
+                psi = psi * (1.0 - h) + (po * 2.0 - it) * h
+            it = psi.copy()
+            psi = self._project(psi)
+            self.update_obj_probe(psi, obj_inertia, probe_inertia, loop_obj_probe)
+            if l is not None:
+                self.record("raar", l)
+                self.split_scale(1.0)
             self.cycle += 1
         if zero_phase_ramp:
             self.zero_phase_ramp()

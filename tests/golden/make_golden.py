@@ -12,7 +12,8 @@ and far-field exits, `refs/f64/lsqml_multislice.py`); and the far-field results 
 scenario `dm_scenario(32, 40, nprobe, 2e5, 4.0)` (`tests/common/engine/scenario.rs`), whose
 counts `oracle/scenario.py` redraws: the position gradient (`pos_grad*`), ML with positions
 (`ml_pos_*`), LSQML steps and epochs with and without positions (`lsqml_*`), rPIE against
-pty-chi (`rpie_ptychi_f64.txt`) and with positions under PATCH (`rpie_pos_*`). Each text table becomes one float64 array of the same rows and
+pty-chi (`rpie_ptychi_f64.txt`) and with positions under PATCH (`rpie_pos_*`), DM and RAAR
+against PyNX (`dm_pynx_f64.txt`, `raar_pynx_f64.txt`). Each text table becomes one float64 array of the same rows and
 columns under its stem (`table` for a file without one) in `<group>.npz`.
 
     python tests/golden/make_golden.py [REFERENCE_ROOT]
@@ -45,6 +46,8 @@ GROUPS = {
     "lsqml_pos": ["steps", "offsets", "obj", "probe"],
     "lsqml_pos_epochs": ["steps", "offsets", "obj", "probe"],
     "rpie_ptychi": [""],
+    "dm_pynx": [""],
+    "raar_pynx": [""],
     "rpie_pos_step": ["obj", "probe", "offsets"],
     "rpie_pos_epochs": ["obj", "probe", "offsets"],
 }

@@ -3,8 +3,9 @@ results: `oracle/scenario.py` redraws `dm_scenario(32, 40, nprobe, 2e5, 4.0)` (C
 counts, tests/common/engine/scenario.rs) and is itself pinned by the scenario's Poisson and
 Euclidian sums; then the position gradient (ptyrs/tests/engine_features.rs:56-103), ML with
 refined positions (engine_ml_pos.rs), LSQML steps and epochs with and without positions
-(engine_lsqml.rs, engine_lsqml_pos.rs) and rPIE's LLK trace against pty-chi
-(engine_reconstruct.rs:222-236), to the reference's own tolerances."""
+(engine_lsqml.rs, engine_lsqml_pos.rs), rPIE's LLK trace against pty-chi
+(engine_reconstruct.rs:222-236) and DM's and RAAR's against PyNX (engine_reconstruct.rs:186-220),
+to the reference's own tolerances."""
 import functools
 import os
 
@@ -204,6 +205,25 @@ def test_rpie_llk_trace_matches_ptychi():
     for rec, row in zip(p.history, rows):
         assert rec["cycle"] == row[0]
         for key, want in zip(("poisson", "gaussian", "euclidian", "nb_photons_calc"), row[1:]):
+            assert abs(rec[key] - want) < 1e-9 * abs(want), (rec["cycle"], key)
+
+
+@pytest.mark.parametrize("algorithm", ["dm", "raar"])
+def test_dm_raar_llk_traces_match_pynx(algorithm):
+    """Twenty-one cycles of DM or RAAR at PyNX's defaults recording every cycle on the scaled
+    one-mode scenario: record 0 is the start, record c + 1 the PyNX record of cycle c (PyNX
+    takes the estimate after the update), every column to 1e-9 (engine_reconstruct.rs:162-220)."""
+    p = state(nprobe=1)
+    start = p.llk().as_dict()
+    getattr(p, algorithm)(21, calc_llk=1)
+    first, rest = p.history[0], p.history[1:]
+    cols = ("poisson", "gaussian", "euclidian", "nb_photons_calc")
+    assert first["cycle"] == 0 and all(first[k] == start[k] for k in cols)
+    rows = golden(f"{algorithm}_pynx")["table"]
+    assert len(rest) == len(rows)
+    for rec, row in zip(rest, rows):
+        assert rec["cycle"] == row[0] + 1 and rec["algorithm"] == algorithm
+        for key, want in zip(cols, row[1:]):
             assert abs(rec[key] - want) < 1e-9 * abs(want), (rec["cycle"], key)
 
 

@@ -158,6 +158,66 @@ def test_lsqml_epochs_match_ptychi():
         assert max_rel(change(probe, probe0), of_run(g["epochs_probe"], k, 4)) < 1e-12
 
 
+def pynx_near_start(g):
+    """engine_pynx_near.rs:51-96: the case's angular-spectrum optics, positions from the golden
+    corners, the counts, the start object and the two-mode probe."""
+    c = g["case"][0]
+    pixel = c[1]
+    corners = g["corners"]
+    ys = (corners[:, 1] - (OBJ[0] - SHAPE[0]) // 2) * pixel
+    xs = (corners[:, 2] - (OBJ[1] - SHAPE[1]) // 2) * pixel
+    counts = counts_from_f64(g["counts"][:, 1:].reshape(len(corners), *SHAPE))
+    optics = ops.Optics.free_space(ops.Wavefield(SHAPE, c[0], [pixel, pixel], c[2]))
+    assert optics.propagator.kind == "angular"
+    obj = stack((1,) + OBJ, g["obj"], 2)
+    probe = stack((NPROBE,) + SHAPE, g["probe"], 3)
+    return Ptycho(counts, ys, xs, optics, obj, probe)
+
+
+def unit(a):
+    """`a / Σ|a|` as re, im pairs: DM and RAAR balance `Σ|O|` and `Σ|P|` after each recorded
+    cycle, PyNX's cpu_operator does not, and the updates commute with that balance
+    (engine_pynx_near.rs:43-49)."""
+    a = np.ravel(a) / np.abs(a).sum()
+    return np.stack([a.real, a.imag], 1)
+
+
+@pytest.mark.parametrize("algorithm", [0, 1, 2], ids=["ap", "dm", "raar"])
+def test_ap_dm_raar_match_pynx_near_field(algorithm):
+    """engine_pynx_near.rs:98-205, the exact-kernel AP, DM and RAAR runs (runs 4-6), 30 cycles
+    recording every one: every LLK column per record (DM and RAAR from their second record on,
+    then the final LLK, as PyNX records after the update) and the final object and probe (DM's
+    and RAAR's over their `Σ|·|`) to the reference's 5e-12."""
+    g = golden("pynx_near")
+    run = g["runs"][4 + algorithm]
+    assert run[1] == 1 and run[2] == algorithm
+    p = pynx_near_start(g)
+    cycles = int(run[3])
+    if algorithm == 0:
+        p.ap(cycles, probe_inertia=0.001, calc_llk=1, zero_phase_ramp=False)
+    elif algorithm == 1:
+        p.dm(cycles, calc_llk=1, zero_phase_ramp=False)
+    else:
+        p.raar(cycles, calc_llk=1, zero_phase_ramp=False)
+    cols = ["poisson", "gaussian", "euclidian", "nb_photons_calc"]
+    got = [[h[k] for k in cols] for h in p.history]
+    if algorithm > 0:
+        got = got[1:] + [[p.llk().as_dict()[k] for k in cols]]
+    got = np.asarray(got)
+    want = g["llk"][g["llk"][:, 0] == run[0]][:, 2:6]
+    assert got.shape == want.shape
+    err = (np.abs(got - want) / np.abs(want)).max()
+    assert err < 5e-12, err
+    for arr, rows, lead in [(p.object, g["run_obj"], 3), (p.probe, g["run_probe"], 4)]:
+        r = rows[rows[:, 0] == run[0]]
+        want = r[:, lead] + 1j * r[:, lead + 1]
+        if algorithm > 0:
+            assert max_rel(unit(arr), unit(want)) < 5e-12
+        else:
+            assert max_rel(np.stack([arr.ravel().real, arr.ravel().imag], 1),
+                           np.stack([want.real, want.imag], 1)) < 5e-12
+
+
 def test_ml_matches_pynx_near_field():
     """engine_pynx_near.rs:107-205, the exact-kernel ML run (run 7): 10 AP cycles with probe
     inertia 0.001, then 30 ML cycles updating object and probe; every LLK column per record
