@@ -76,13 +76,37 @@ typedef struct ptyb_ml_params {
   int32_t update_object, update_probe, calc_llk, zero_phase_ramp;
 } ptyb_ml_params;
 
+/* Reference `ApParams` (engine/ptycho.rs:48-68): an update flag of 0 is the reference's `None`
+ * inertia (that array stays fixed). Defaults: object on at 0.01, probe off (0.001). */
+typedef struct ptyb_ap_params {
+  int32_t update_object, update_probe;
+  double obj_inertia, probe_inertia;
+  int32_t calc_llk, zero_phase_ramp;
+} ptyb_ap_params;
+
+/* Reference `DmParams` (engine/ptycho.rs:71-96): alpha the AP/DM mix (0 plain DM, default
+ * 0.02), loop_obj_probe object-then-probe updates per cycle (default 1). */
+typedef struct ptyb_dm_params {
+  int32_t update_object, update_probe;
+  double obj_inertia, probe_inertia, alpha;
+  int32_t loop_obj_probe, calc_llk, zero_phase_ramp;
+} ptyb_dm_params;
+
+/* Reference `RaarParams` (engine/ptycho.rs:98-123): beta the relaxation (default 0.9). */
+typedef struct ptyb_raar_params {
+  int32_t update_object, update_probe;
+  double obj_inertia, probe_inertia, beta;
+  int32_t loop_obj_probe, calc_llk, zero_phase_ramp;
+} ptyb_raar_params;
+
 /* Reference `Llk` (engine/ops.rs:257-277), normalised by the unmasked pixel count. */
 typedef struct ptyb_llk {
   double poisson, gaussian, euclidian, nb_photons_calc;
 } ptyb_llk;
 
-/* Reference `LlkRecord` (engine/ptycho.rs:36-41); algorithm 3 = rPIE, 4 = ML, 6 = LSQML
- * (the reference's `Algorithm` order Ap, Dm, Raar, Rpie, Ml, Bh, Lsqml). */
+/* Reference `LlkRecord` (engine/ptycho.rs:36-41); algorithm 0 = AP, 1 = DM, 2 = RAAR,
+ * 3 = rPIE, 4 = ML, 6 = LSQML (the reference's `Algorithm` order Ap, Dm, Raar, Rpie, Ml, Bh,
+ * Lsqml). */
 typedef struct ptyb_llk_record {
   int64_t cycle;
   int32_t algorithm;
@@ -135,6 +159,23 @@ int ptyb_lsqml(ptyb_handle* h, const ptyb_lsqml_params* params, int32_t nepoch,
 
 /* Reference `GpuPtycho::ml` (engine/gpu/ml.rs:38-83). */
 int ptyb_ml(ptyb_handle* h, const ptyb_ml_params* params, int32_t ncycle);
+
+/* Reference `GpuPtycho::ap` (engine/gpu/ap.rs:28-44; CPU twin `Ptycho::ap`,
+ * engine/ptycho.rs:609-641): per cycle every frame's exit waves, the magnitude projection (the
+ * LLK record is of the estimate it projects), then both updates from the old arrays. Single
+ * slice, without the position model (PTYB_INVALID otherwise). */
+int ptyb_ap(ptyb_handle* h, const ptyb_ap_params* params, int32_t ncycle);
+
+/* Reference `GpuPtycho::dm` (engine/gpu/dm.rs:32-38; CPU twin `Ptycho::dm`,
+ * engine/ptycho.rs:653-691): cycle 0 of a call starts from the estimate's exit waves, later
+ * cycles reflect the carried waves; the LLK record is of the estimate the cycle starts from,
+ * and a recorded cycle ends by balancing Σ|O| and Σ|P|. Single slice, without the position
+ * model. */
+int ptyb_dm(ptyb_handle* h, const ptyb_dm_params* params, int32_t ncycle);
+
+/* Reference `GpuPtycho::raar` (engine/gpu/raar.rs:17-23; CPU twin `Ptycho::raar`,
+ * engine/ptycho.rs:698-730): DM's cycle with RAAR's mix of the carried projection and iterate. */
+int ptyb_raar(ptyb_handle* h, const ptyb_raar_params* params, int32_t ncycle);
 
 /* Reference `GpuPtycho::llk` (engine/gpu/mod.rs:871-881): normalised LLK of the estimate. */
 int ptyb_get_llk(ptyb_handle* h, ptyb_llk* out);

@@ -30,6 +30,24 @@ class LsqmlParams(ctypes.Structure):
     _fields_ = [("batch_size", c_int32), ("cost", c_int32), ("seed", ctypes.c_uint64)]
 
 
+class ApParams(ctypes.Structure):
+    _fields_ = [("update_object", c_int32), ("update_probe", c_int32),
+                ("obj_inertia", c_double), ("probe_inertia", c_double), ("calc_llk", c_int32),
+                ("zero_phase_ramp", c_int32)]
+
+
+class DmParams(ctypes.Structure):
+    _fields_ = [("update_object", c_int32), ("update_probe", c_int32),
+                ("obj_inertia", c_double), ("probe_inertia", c_double), ("alpha", c_double),
+                ("loop_obj_probe", c_int32), ("calc_llk", c_int32), ("zero_phase_ramp", c_int32)]
+
+
+class RaarParams(ctypes.Structure):
+    _fields_ = [("update_object", c_int32), ("update_probe", c_int32),
+                ("obj_inertia", c_double), ("probe_inertia", c_double), ("beta", c_double),
+                ("loop_obj_probe", c_int32), ("calc_llk", c_int32), ("zero_phase_ramp", c_int32)]
+
+
 class MlParams(ctypes.Structure):
     _fields_ = [("update_object", c_int32), ("update_probe", c_int32), ("calc_llk", c_int32),
                 ("zero_phase_ramp", c_int32)]
@@ -61,6 +79,9 @@ SIGNATURES = {
     "ptyb_rpie": (c_int32, [c_void_p, P(RpieParams), c_int32]),
     "ptyb_lsqml": (c_int32, [c_void_p, P(LsqmlParams), c_int32, c_int32]),
     "ptyb_ml": (c_int32, [c_void_p, P(MlParams), c_int32]),
+    "ptyb_ap": (c_int32, [c_void_p, P(ApParams), c_int32]),
+    "ptyb_dm": (c_int32, [c_void_p, P(DmParams), c_int32]),
+    "ptyb_raar": (c_int32, [c_void_p, P(RaarParams), c_int32]),
     "ptyb_get_llk": (c_int32, [c_void_p, P(Llk)]),
     "ptyb_gradients": (c_int32, [c_void_p, P(c_double), P(c_double), P(c_double),
                                  P(c_double)]),

@@ -83,12 +83,14 @@ constexpr size_t kNoallocScratchBytes = size_t(32) << 20;
 // Object slices of a multislice handle, and the float scalars on the device (maxima, the
 // batch's object and probe steps, one step per further slice).
 constexpr int kMaxSlices = 16;
-constexpr int kScalars = 8 + kMaxSlices;
+constexpr int kScalars = 8 + kMaxSlices + 2;
+// The maxima of the AP / DM / RAAR blends' object and probe norms.
+constexpr int kScalObjNorm = 8 + kMaxSlices, kScalProbeNorm = kScalObjNorm + 1;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];
 
 namespace {
 
-constexpr int kAlgRpie = 3, kAlgMl = 4, kAlgLsqml = 6;
+constexpr int kAlgAp = 0, kAlgDm = 1, kAlgRaar = 2, kAlgRpie = 3, kAlgMl = 4, kAlgLsqml = 6;
 
 // One device allocation, freed with the handle.
 struct Buf {
@@ -171,6 +173,13 @@ struct ptyb_handle {
   // Multislice gradients: every slice's 2·∂L/∂O_s* and its compensation.
   float2* g_slices = nullptr;     // [S][nyo][nxo]
   float2* g_slices_c = nullptr;
+  // AP / DM / RAAR: every frame's carried exit waves and RAAR's iterate, [P][K][N][N]; the
+  // probe blend's per-chunk norms and its norm plane.
+  float2* carry = nullptr;
+  float2* carry_it = nullptr;
+  float* partial_den = nullptr;   // [max_den_chunks][N][N]
+  int max_den_chunks = 0;
+  float* probe_norm = nullptr;    // [N][N]
   double* partials = nullptr;    // [kPartialBlocks][2]
   std::vector<Buf> bufs;
   // Per-kernel device timing (CUDA events on the engine's stream), when enabled.
@@ -296,7 +305,7 @@ enum Kind : int {
   kKObjRpie, kKObjOverlap, kKObjLsqml, kKObjMl, kKIllum, kKProbePartial, kKProbeFinal,
   kKAfar, kKDots, kKSolve, kKAxpy, kKMax, kKCounts, kKMisc, kKGamma, kKArraySums, kKMove,
   kKPositionSums, kKSliceForward, kKSliceBackward, kKSliceLlk, kKFrameProject, kKSpectrum,
-  kKDerivSums, kKBackSpectrum, kKSliceGrad, kNumKinds
+  kKDerivSums, kKBackSpectrum, kKSliceGrad, kKFrameCarry, kKObjBlend, kNumKinds
 };
 const char* const kKindNames[kNumKinds] = {
     "frame_rpie", "frame_lsqml", "frame_ml_grad", "frame_llk", "frame_store",
@@ -304,7 +313,7 @@ const char* const kKindNames[kNumKinds] = {
     "illumination", "probe_partial", "probe_finalize", "lsqml_afar", "lsqml_dots",
     "lsqml_solve", "axpy", "max", "counts", "misc", "ml_gamma", "array_sums", "move",
     "position_sums", "slice_forward", "slice_backward", "slice_llk", "frame_project", "spectrum",
-    "deriv_sums", "back_spectrum", "slice_grad"};
+    "deriv_sums", "back_spectrum", "slice_grad", "frame_carry", "object_blend"};
 
 cudaEvent_t take_event(ptyb_handle* h) {
   if (!h->event_pool.empty()) {
@@ -429,6 +438,7 @@ cudaError_t launch_frame(ptyb_handle* h, const FrameArgs& a, int nslot) {
                        : MODE == kLlk ? kKFrameLlk
                        : MODE == kStore ? kKFrameStore
                        : MODE == kProject || MODE == kProjectKept ? kKFrameProject
+                       : MODE == kCarry ? kKFrameCarry
                                         : kKFrameFromStore;
   cudaError_t e = cudaSuccess;
   timed(h, kind, [&] { e = launch_frame_raw<MODE>(h, a, nslot); }, nslot);
@@ -686,6 +696,8 @@ void probe_pass(ptyb_handle* h, const int* frames, int nslot, int mode, float al
   launched(h, "probe_finalize");
 }
 
+ptyb_llk llk_of_frames(ptyb_handle* h);
+
 // The LLK of the current estimate over every frame: per-frame sums in frame order.
 // `waves` (optional): every frame's moved probe, [P][K][N][N], when the caller has them.
 ptyb_llk llk_pass(ptyb_handle* h, const float2* waves = nullptr) {
@@ -724,6 +736,11 @@ ptyb_llk llk_pass(ptyb_handle* h, const float2* waves = nullptr) {
     check(h, launch_frame<kLlk>(h, a, n), "llk pass");
     ++h->launches;
   }
+  return llk_of_frames(h);
+}
+
+// The normalised LLK from every frame's sums in h->llk, added in frame order on the host.
+ptyb_llk llk_of_frames(ptyb_handle* h) {
   std::vector<double> v((size_t)h->P * 4);
   check(h, cudaMemcpyAsync(v.data(), h->llk, v.size() * sizeof(double), cudaMemcpyDeviceToHost,
                            h->stream),
@@ -1263,12 +1280,14 @@ void ensure_ml(ptyb_handle* h) {
   h->psi_all = alloc<float2>(h, (size_t)h->P * np);
   h->g_all = alloc<float2>(h, (size_t)h->P * np);
   h->g_probe_spec = alloc<float2>(h, np);
-  h->partials = alloc<double>(h, kPartialBlocks * 2);
+  if (!h->partials) h->partials = alloc<double>(h, kPartialBlocks * 2);
 }
 
 // Two double sums of an array (mode 0: Polak–Ribière numerator and |h|²; 1: Σ|g|), the block
 // partials added in block order on the host.
 void array_sums(ptyb_handle* h, const float2* g, const float2* hh, size_t n, int mode, double out[2]) {
+  // the block partials, made on first use (ML's set-up, or DM's and RAAR's balance)
+  if (!h->partials) h->partials = alloc<double>(h, kPartialBlocks * 2);
   timed(h, kKArraySums, [&] {
     array_sums_kernel<<<kPartialBlocks, 256, 0, h->stream>>>(g, hh, n, mode, h->partials);
   });
@@ -1527,9 +1546,16 @@ void zero_phase_ramp(ptyb_handle* h) {
 
 // PyNX ScaleObjProbe(absolute=True) without background (engine/ptycho.rs:577-591).
 // `waves` (optional): every frame's moved probe of the current probe, scaled along with it.
+void split_scale(ptyb_handle* h, double s, float2* waves);
+
 void scale_obj_probe(ptyb_handle* h, float2* waves = nullptr) {
   const ptyb_llk l = llk_pass(h, waves);
-  const double s = std::sqrt(h->obs_total / l.nb_photons_calc);
+  split_scale(h, std::sqrt(h->obs_total / l.nb_photons_calc), waves);
+}
+
+// Scales O·P by s and balances Σ|O| and Σ|P| (engine/ptycho.rs:593-603): P *= √(Σ|O|/Σ|P|·s),
+// O *= √(Σ|P|/Σ|O|·s); `waves`, every frame's moved probe, scale with the probe.
+void split_scale(ptyb_handle* h, double s, float2* waves) {
   const size_t no = (size_t)h->nobj * h->nyo * h->nxo, np = (size_t)h->K * h->N * h->N;
   double so[2], sp[2];
   array_sums(h, h->object, nullptr, no, 1, so);
@@ -1545,6 +1571,121 @@ void scale_obj_probe(ptyb_handle* h, float2* waves = nullptr) {
     timed(h, kKAxpy, [&] { scale_kernel<<<blocks_for(nw), 256, 0, h->stream>>>(waves, (float)fp, nw); });
     launched(h, "scale");
   }
+}
+
+// AP / DM / RAAR (engine/ptycho.rs:609-754) ---------------------------------------------
+
+// Every frame's carried exit waves (and RAAR's iterate), allocated on first use.
+void ensure_carry(ptyb_handle* h, bool iterate) {
+  const size_t n = (size_t)h->P * h->K * h->N * h->N;
+  if (!h->carry) h->carry = alloc<float2>(h, n);
+  if (iterate && !h->carry_it) h->carry_it = alloc<float2>(h, n);
+  if (!h->probe_norm) h->probe_norm = alloc<float>(h, (size_t)h->N * h->N);
+}
+
+// The frame kernel's carry mode over every frame, stack by stack: the carried waves become
+// Π(S) + c_refl·(PO − S) with S = c_po·PO + c_psi·carried + c_it·iterate; with `llk`, each
+// frame's LLK sums of the field it projects go to h->llk.
+void carry_pass(ptyb_handle* h, float c_po, float c_psi, float c_it, float c_refl, bool llk,
+                bool iterate) {
+  const int stack = std::min(h->P, h->stack);
+  const size_t pstride = (size_t)h->K * h->N * h->N;
+  for (int s0 = 0; s0 < h->P; s0 += stack) {
+    const int n = std::min(stack, h->P - s0);
+    FrameArgs a = frame_args(h, h->iota + s0);
+    a.carry = h->carry + s0 * pstride;
+    a.iter = iterate ? h->carry_it + s0 * pstride : nullptr;
+    a.c_po = c_po;
+    a.c_psi = c_psi;
+    a.c_it = c_it;
+    a.c_refl = c_refl;
+    a.llk = llk ? h->llk + (size_t)s0 * 4 : nullptr;
+    check(h, launch_frame<kCarry>(h, a, n), "carry pass");
+    ++h->launches;
+  }
+}
+
+// psi_to_obj_probe's object blend from the carried waves and the current probe
+// (engine/ops.rs:352-381): the norm's maximum over the object, then the blend.
+void object_blend(ptyb_handle* h, double inertia) {
+  GatherArgs g = gather_args(h, h->iota, h->P);
+  g.upd = h->carry;
+  g.pmax = h->scal + kScalObjNorm;
+  g.step = (float)inertia;
+  check(h, cudaMemsetAsync(g.pmax, 0, sizeof(float), h->stream), "memset");
+  timed(h, kKObjOverlap, [&] { object_tile_kernel<kGatherOverlap><<<ntiles(h), 1024, 0, h->stream>>>(g); }, h->P);
+  launched(h, "object norm max");
+  timed(h, kKObjBlend, [&] { object_tile_kernel<kGatherBlend><<<ntiles(h), 1024, 0, h->stream>>>(g); }, h->P);
+  launched(h, "object blend");
+}
+
+// The probe blend's chunk sums Σ conj(q·O)·carried and Σ|O|² from the current object; the
+// blend itself is probe_blend_finish, so AP's probe sums can read the object before its update.
+int probe_blend_sums(ptyb_handle* h) {
+  int nchunk = 0;
+  const int chunk = probe_chunk(h, h->P, &nchunk);
+  const int plane = h->N * h->N;
+  if (nchunk > h->max_den_chunks) {
+    h->partial_den = alloc<float>(h, (size_t)nchunk * plane);
+    h->max_den_chunks = nchunk;
+  }
+  ProbeArgs p = {};
+  p.object = h->object;
+  p.quad = h->quad;
+  p.upd = h->carry;
+  p.frames = h->iota;
+  p.corners = h->corners;
+  p.partial = h->partial;
+  p.partial_den = h->partial_den;
+  p.nslot = h->P;
+  p.chunk = chunk;
+  p.nxo = h->nxo;
+  p.K = h->K;
+  p.N = h->N;
+  p.mode = 2;
+  dim3 grid((plane + 255) / 256, nchunk);
+  timed(h, kKProbePartial, [&] { probe_partial_kernel<<<grid, 256, 0, h->stream>>>(p); }, h->P);
+  launched(h, "probe partial");
+  return nchunk;
+}
+
+void probe_blend_finish(ptyb_handle* h, int nchunk, double inertia) {
+  const int plane = h->N * h->N, count = h->K * plane;
+  float* nmax = h->scal + kScalProbeNorm;
+  check(h, cudaMemsetAsync(nmax, 0, sizeof(float), h->stream), "memset");
+  timed(h, kKProbeFinal, [&] {
+    probe_norm_kernel<<<(plane + 255) / 256, 256, 0, h->stream>>>(h->partial_den, nchunk, plane,
+                                                                  h->probe_norm, nmax);
+  });
+  launched(h, "probe norm");
+  timed(h, kKProbeFinal, [&] {
+    probe_finalize_kernel<<<(count + 255) / 256, 256, 0, h->stream>>>(
+        h->partial, nchunk, count, h->probe, nullptr, nullptr, (float)inertia, 3, h->probe_norm,
+        nmax, plane);
+  });
+  launched(h, "probe blend");
+}
+
+// DM's and RAAR's update (engine/ptycho.rs:732-754): `loops` times an object-only then a
+// probe-only blend, the probe's from the new object.
+void update_obj_probe(ptyb_handle* h, bool uo, double oi, bool up, double pi, int loops) {
+  for (int l = 0; l < loops; ++l) {
+    if (uo) object_blend(h, oi);
+    if (up) probe_blend_finish(h, probe_blend_sums(h), pi);
+  }
+}
+
+// AP, DM and RAAR run on a single-slice object without the position model.
+int carried_refusal(ptyb_handle* h, int32_t ncycle, const char* what) {
+  if (ncycle < 0) {
+    h->err = "ncycle must be >= 0";
+    return PTYB_INVALID;
+  }
+  if (h->nslice > 1 || h->have_offsets) {
+    h->err = std::string(what) + " runs on a single-slice object without the position model";
+    return PTYB_INVALID;
+  }
+  return PTYB_OK;
 }
 
 template <typename F>
@@ -1565,6 +1706,43 @@ int guarded(ptyb_handle* h, bool enqueues, F&& body) {
   } catch (const Fail& f) {
     return f.code;
   }
+}
+
+// DM (RAAR when `raar`) cycles (engine/ptycho.rs:653-730): the LLK of the estimate the cycle
+// starts from when due, the mix and projection of the carried waves, the updates, and after a
+// recorded cycle the balance of Σ|O| and Σ|P|.
+int carried_cycles(ptyb_handle* h, bool raar, double mix, bool uo, double oi, bool up, double pi,
+                   int loops, int calc_llk, bool ramp, int32_t ncycle) {
+  return guarded(h, true, [&]() -> int {
+    ensure_slots(h, std::min(h->P, h->stack));
+    ensure_carry(h, raar);
+    begin_call(h);
+    for (int ic = 0; ic < ncycle; ++ic) {
+      const bool due = llk_due(calc_llk, ic, ncycle);
+      ptyb_llk l = {};
+      if (due) l = llk_pass(h);
+      if (ic == 0) {
+        carry_pass(h, 1.f, 0.f, 0.f, 0.f, false, raar);
+      } else if (raar) {
+        // psi ← (1 − b/2)·psi + (b/2)·(2·PO − it), the next iterate, then Π
+        const double hb = 0.5 * mix;
+        carry_pass(h, (float)(2.0 * hb), (float)(1.0 - hb), (float)(-hb), 0.f, false, true);
+      } else {
+        // refl = (2 − a)·PO − (1 − a)·psi; psi ← Π(refl) + (1 − a)·(PO − refl)
+        carry_pass(h, (float)(2.0 - mix), (float)(-(1.0 - mix)), 0.f, (float)(1.0 - mix), false,
+                   false);
+      }
+      update_obj_probe(h, uo, oi, up, pi, loops);
+      if (due) {
+        record(h, raar ? kAlgRaar : kAlgDm, l);
+        split_scale(h, 1.0, nullptr);
+      }
+      ++h->cycle;
+    }
+    if (ramp) zero_phase_ramp(h);
+    end_call(h, raar ? "raar" : "dm");
+    return PTYB_OK;
+  });
 }
 
 }  // namespace
@@ -2000,6 +2178,57 @@ int ptyb_ml(ptyb_handle* h, const ptyb_ml_params* p, int32_t ncycle) {
     end_call(h, "ml");
     return PTYB_OK;
   });
+}
+
+int ptyb_ap(ptyb_handle* h, const ptyb_ap_params* p, int32_t ncycle) {
+  if (!h || !p) return PTYB_INVALID;
+  if (const int e = carried_refusal(h, ncycle, "AP")) return e;
+  return guarded(h, true, [&]() -> int {
+    ensure_slots(h, std::min(h->P, h->stack));
+    ensure_carry(h, false);
+    const bool uo = p->update_object != 0, up = p->update_probe != 0;
+    begin_call(h);
+    for (int ic = 0; ic < ncycle; ++ic) {
+      // the LLK of the estimate comes from the field the projection reads
+      const bool due = llk_due(p->calc_llk, ic, ncycle);
+      carry_pass(h, 1.f, 0.f, 0.f, 0.f, due, false);
+      ptyb_llk l = {};
+      if (due) l = llk_of_frames(h);
+      // both updates from the old arrays: the probe's sums read the object before its blend
+      const int nchunk = up ? probe_blend_sums(h) : 0;
+      if (uo) object_blend(h, p->obj_inertia);
+      if (up) probe_blend_finish(h, nchunk, p->probe_inertia);
+      if (due) record(h, kAlgAp, l);
+      ++h->cycle;
+    }
+    if (p->zero_phase_ramp) zero_phase_ramp(h);
+    end_call(h, "ap");
+    return PTYB_OK;
+  });
+}
+
+int ptyb_dm(ptyb_handle* h, const ptyb_dm_params* p, int32_t ncycle) {
+  if (!h || !p) return PTYB_INVALID;
+  if (const int e = carried_refusal(h, ncycle, "DM")) return e;
+  if (p->loop_obj_probe < 0) {
+    h->err = "loop_obj_probe must be >= 0";
+    return PTYB_INVALID;
+  }
+  return carried_cycles(h, false, p->alpha, p->update_object != 0, p->obj_inertia,
+                        p->update_probe != 0, p->probe_inertia, p->loop_obj_probe, p->calc_llk,
+                        p->zero_phase_ramp != 0, ncycle);
+}
+
+int ptyb_raar(ptyb_handle* h, const ptyb_raar_params* p, int32_t ncycle) {
+  if (!h || !p) return PTYB_INVALID;
+  if (const int e = carried_refusal(h, ncycle, "RAAR")) return e;
+  if (p->loop_obj_probe < 0) {
+    h->err = "loop_obj_probe must be >= 0";
+    return PTYB_INVALID;
+  }
+  return carried_cycles(h, true, p->beta, p->update_object != 0, p->obj_inertia,
+                        p->update_probe != 0, p->probe_inertia, p->loop_obj_probe, p->calc_llk,
+                        p->zero_phase_ramp != 0, ncycle);
 }
 
 int ptyb_get_llk(ptyb_handle* h, ptyb_llk* out) {

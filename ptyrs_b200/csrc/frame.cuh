@@ -14,7 +14,8 @@
 // Reference operators followed (physwkim/ptyrs): exit wave `obj_probe_to_psi`
 // (engine/ops.rs:47-71), unitary FFT (engine/fft.rs:155-234), the rPIE modulus
 // (engine/ptycho.rs:928-945), the Poisson gradient (engine/ops.rs:161-195), the LSQML residual
-// (engine/lsqml.rs:155-170) and the LLK sums (engine/ops.rs:119-154).
+// (engine/lsqml.rs:155-170), the LLK sums (engine/ops.rs:119-154) and PyNX's AP, DM and RAAR
+// mixes of carried exit waves around the magnitude projection (engine/ptycho.rs:609-730).
 #pragma once
 #include <cooperative_groups.h>
 
@@ -34,6 +35,7 @@ enum FrameMode : int {
   kFromStore = 5,  // detector field from global; LSQML residual; out = χ
   kProject = 6,    // magnitude projection √I/max(√Ĩ, 1e-12), masked kept; out = ψ' − ψ
   kProjectKept = 7,// kProject from the detector field a kMlGrad pass kept (psi_out)
+  kCarry = 8,      // AP / DM / RAAR: projection of a mix of P·O·q and the carried waves
 };
 
 enum Cost : int { kCostPoisson = 0, kCostAmplitude = 1 };
@@ -67,6 +69,14 @@ struct FrameArgs {
   // search and the magnitude projection, [slot][K][kx][ky] (columns contiguous); kProjectKept
   // reads it back.
   float2* psi_out;
+  // kCarry (AP, DM, RAAR; engine/ptycho.rs:609-730): the carried exit waves `carry` and RAAR's
+  // iterate `iter` of the launch's frames, [slot][K][N][N] natural layout. The projection's
+  // input is S = c_po·PO + c_psi·carry + c_it·iter (iter ← S when `iter` is set); the carried
+  // waves become Π(S) + c_refl·(PO − S). Terms whose coefficient is 0 are not read. With `llk`
+  // set, the pass also writes the per-frame LLK sums of the field it projects.
+  float2* carry;
+  float2* iter;
+  float c_po, c_psi, c_it, c_refl;
 };
 
 template <int N, int C>
@@ -193,6 +203,19 @@ PTYB_D void cluster_sum2(double& x, double& y, double* red, cg::cluster_group& c
   y = sy;
 }
 
+// The projection's input S = c_po·po + c_psi·carry + c_it·iter at element `pix` of mode m of
+// `slot` (kCarry); the prologue (`store`) also writes it to RAAR's iterate.
+template <int N>
+PTYB_D float2 carry_mix(const FrameArgs& a, float2 po, int slot, int m, int pix, int K,
+                        bool store) {
+  const size_t gi = ((size_t)slot * K + m) * N * N + pix;
+  float2 v = cscale(po, a.c_po);
+  if (a.c_psi != 0.f) v = cadd(v, cscale(a.carry[gi], a.c_psi));
+  if (a.c_it != 0.f) v = cadd(v, cscale(a.iter[gi], a.c_it));
+  if (store && a.iter) a.iter[gi] = v;
+  return v;
+}
+
 template <int N, int C, int MODE>
 __global__ void __launch_bounds__(FrameShape<N, C>::T,
                                   N == 256 && FrameShape<N, C>::T <= 256 &&
@@ -249,8 +272,11 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
         for (int pm = 0; pm < a.nprobe; ++pm) {
           const int line = (om * a.nprobe + pm) * H + yl;
           // (P·O)·q as P·(O·q): the reference's product up to rounding
-          S[line * L + (jx ^ swz(line))] =
+          float2 v =
               cmul(a.probe[(size_t)slot * a.probe_stride + ((size_t)pm * N + ny) * N + nx], oq);
+          if (MODE == kCarry)
+            v = carry_mix<N>(a, v, slot, om * a.nprobe + pm, ny * N + nx, K, true);
+          S[line * L + (jx ^ swz(line))] = v;
         }
       }
     }
@@ -345,7 +371,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
       a.icalc[((size_t)slot * N + ky) * N + kx] = ic;
       continue;
     }
-    if (MODE == kLlk) {
+    if (MODE == kLlk || (MODE == kCarry && a.llk)) {
       if (!masked) {
         acc[0] += yo > 0.f ? (double)ic - yo + (double)yo * log((double)yo / ic) : (double)ic;
         const double dg = (double)yo - ic;
@@ -354,12 +380,12 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
         acc[2] += 4.0 * de * de;
         acc[3] += ic;
       }
-      continue;
+      if (MODE == kLlk) continue;
     }
     float fac;
     if (MODE == kRpie) {
       fac = masked ? 1.f : sqrtf(yo + 1e-7f) / (sqrtf(ic) + 1e-7f);
-    } else if (MODE == kProject || MODE == kProjectKept) {
+    } else if (MODE == kProject || MODE == kProjectKept || MODE == kCarry) {
       // ApplyAmplitude (engine/ops.rs:83-107)
       fac = masked ? 1.f : sqrtf(yo) / fmaxf(sqrtf(ic), 1e-12f);
     } else if (MODE == kMlGrad) {
@@ -379,7 +405,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
   }
   (void)inv_n;
 
-  if (MODE == kLlk) {
+  if (MODE == kLlk || (MODE == kCarry && a.llk)) {
     block_sum<T>(acc, 4, red);
     csync<C>(cluster);
     if (r == 0 && tid == 0) {
@@ -390,7 +416,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
       }
     }
     csync<C>(cluster);
-    return;
+    if (MODE == kLlk) return;
   }
   if (MODE == kStore) {
     __syncthreads();
@@ -433,6 +459,30 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
       }
     }
   };
+  if (MODE == kCarry) {
+    // carried waves ← Π(S) + c_refl·(PO − S), in place (this thread read these pixels above)
+#pragma unroll 2
+    for (int idx = tid; idx < H * N; idx += T) {
+      const int yl = idx / N, jx = idx % N;
+      const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
+      const int pix = ny * N + nx;
+      float2 oq = make_float2(0.f, 0.f);
+      if (a.c_refl != 0.f)
+        oq = cmul(a.object[(size_t)(corner.x + ny) * a.nxo + corner.y + nx], a.quad[pix]);
+      for (int m = 0; m < K; ++m) {
+        const int line = m * H + yl;
+        float2 v = S[line * L + (jx ^ swz(line))];
+        const size_t gi = ((size_t)slot * K + m) * N * N + pix;
+        if (a.c_refl != 0.f) {
+          const float2 po =
+              cmul(a.probe[(size_t)slot * a.probe_stride + (size_t)m * N * N + pix], oq);
+          v = cadd(v, cscale(csub(po, carry_mix<N>(a, po, slot, m, pix, K, false)), a.c_refl));
+        }
+        a.carry[gi] = v;
+      }
+    }
+    return;
+  }
   epilogue(a.out, MODE != kMlGrad);
 }
 

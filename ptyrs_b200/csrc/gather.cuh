@@ -23,6 +23,7 @@ enum GatherMode : int {
   kGatherMl = 2,     // grad += Σ conj(q·P)·g (compensated across launches)
   kGatherOverlap = 3,  // pmax = max over pixels of Σ_m D_m
   kGatherIllum = 4,    // pre = (pre + I)/2 with I = Σ|P|² over every view
+  kGatherBlend = 5,    // O = (num + reg·O) / max(norm + reg, 1e-12), reg = inertia·max norm
 };
 
 struct GatherArgs {
@@ -37,7 +38,7 @@ struct GatherArgs {
   const float* pre_max;    // LSQML: max of pre (device scalar)
   float2* out;             // LSQML d_obj / ML gradient sum [nyo][nxo]
   float2* comp;            // ML gradient compensation [nyo][nxo]
-  float alpha, step, pre_scale;
+  float alpha, step, pre_scale;  // kGatherBlend: step = inertia, pmax = max of the norm
   int nslot, nyo, nxo, nprobe, N;
   int probe_stride;        // elements between slots' probes (0: the shared probe)
 };
@@ -84,7 +85,7 @@ PTYB_D int tile_list(const GatherArgs& a, int s0, int s1, int ty0, int tx0, int*
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(1024, MODE == kGatherRpie ? 1 : 2) object_tile_kernel(GatherArgs a) {
+__global__ void __launch_bounds__(1024, MODE == kGatherRpie || MODE == kGatherBlend ? 1 : 2) object_tile_kernel(GatherArgs a) {
   constexpr int kChunk = 1024;
   constexpr int kPix = kTile * kTile;  // 256 pixels, kGroups threads each
   // The view list (during the walk), then the groups' partial sums (after it).
@@ -131,15 +132,18 @@ __global__ void __launch_bounds__(1024, MODE == kGatherRpie ? 1 : 2) object_tile
       float2 u[kMaxModes];
 #pragma unroll
       for (int m = 0; m < kMaxModes; ++m)
-        if (m < K && (MODE == kGatherRpie || MODE == kGatherLsqml || MODE == kGatherMl))
+        if (m < K && (MODE == kGatherRpie || MODE == kGatherLsqml || MODE == kGatherMl ||
+                      MODE == kGatherBlend))
           u[m] = a.upd[((size_t)s * K + m) * plane + pix];
 #pragma unroll
       for (int m = 0; m < kMaxModes; ++m) {
         if (m >= K) break;
         const float2 p = a.probe[(size_t)s * a.probe_stride + m * plane + pix];
-        if (MODE == kGatherOverlap || MODE == kGatherIllum || MODE == kGatherRpie)
+        if (MODE == kGatherOverlap || MODE == kGatherIllum || MODE == kGatherRpie ||
+            MODE == kGatherBlend)
           den[m].add(cnorm2(p));
-        if (MODE == kGatherRpie || MODE == kGatherLsqml || MODE == kGatherMl) {
+        if (MODE == kGatherRpie || MODE == kGatherLsqml || MODE == kGatherMl ||
+            MODE == kGatherBlend) {
           const float2 t = cmulc(cmul(p, q), u[m]);  // conj(P·q)·u
           if (MODE == kGatherRpie)
             num[m].add(t);
@@ -213,6 +217,15 @@ __global__ void __launch_bounds__(1024, MODE == kGatherRpie ? 1 : 2) object_tile
     cc = make_float2((tr - g.x) - yr, (ti - g.y) - yi);
     a.out[o] = make_float2(tr, ti);
     a.comp[o] = cc;
+  } else if (MODE == kGatherBlend) {
+    // psi_to_obj_probe's object blend (engine/ops.rs:352-381) over every pixel, covered or not
+    float d = 0.f;
+#pragma unroll
+    for (int m = 0; m < kMaxModes; ++m)
+      if (m < K) d += den[m].s;
+    const float reg = a.step * (*a.pmax);
+    const float2 v = cadd(num[0].value(), cscale(a.object[o], reg));
+    a.object[o] = cscale(v, 1.f / fmaxf(d + reg, 1e-12f));
   } else if (MODE == kGatherIllum) {
     float d = 0.f;
 #pragma unroll
@@ -231,8 +244,9 @@ struct ProbeArgs {
   const int2* corners;
   const float* omax;      // rPIE [slot]
   float2* partial;        // [nchunk][K][N][N]
+  float* partial_den;     // mode 2: [nchunk][N][N] Σ_slots |O|² over the window
   float alpha;
-  int nslot, chunk, nxo, K, N, mode;  // mode 0 rPIE weight, 1 plain conj(q·O)
+  int nslot, chunk, nxo, K, N, mode;  // mode 0 rPIE weight, 1 plain conj(q·O), 2 also Σ|O|²
 };
 
 constexpr int kMaxProbeChunk = 256;
@@ -255,12 +269,15 @@ __global__ void __launch_bounds__(256) probe_partial_kernel(ProbeArgs a) {
   const int yy = pix / N, xx = pix % N;
   const float2 q = a.quad[pix];
   KahanC acc[kMaxModes];
+  Kahan den;
+  den.init();
 #pragma unroll
   for (int m = 0; m < kMaxModes; ++m) acc[m].init();
 #pragma unroll 4
   for (int s = s0; s < s1; ++s) {
     const int2 c = cs[s - s0];
     const float2 o = a.object[(size_t)(c.x + yy) * a.nxo + c.y + xx];
+    if (a.mode == 2) den.add(cnorm2(o));
     float2 w = cconj(cmul(o, q));
     if (a.mode == 0) w = cscale(w, 1.f / ((1.f - a.alpha) * cnorm2(o) + a.alpha * om[s - s0]));
 #pragma unroll
@@ -272,12 +289,40 @@ __global__ void __launch_bounds__(256) probe_partial_kernel(ProbeArgs a) {
 #pragma unroll
   for (int m = 0; m < kMaxModes; ++m)
     if (m < a.K) a.partial[((size_t)blockIdx.y * a.K + m) * plane + pix] = acc[m].value();
+  if (a.mode == 2) a.partial_den[(size_t)blockIdx.y * plane + pix] = den.s - den.c;
 }
 
-// Σ over chunks in order; mode 0: P += coef·Σ; 1: out = coef·Σ; 2: out += Σ compensated.
+// The probe blend's norm Σ_frames |O|² per pixel: the chunks' sums in chunk order into `den`,
+// and its maximum into *dmax (zeroed by the caller).
+__global__ void __launch_bounds__(256) probe_norm_kernel(const float* partial_den, int nchunk,
+                                                         int plane, float* den, float* dmax) {
+  __shared__ float red[8];
+  const int i = blockIdx.x * 256 + threadIdx.x;
+  float v = 0.f;
+  if (i < plane) {
+    Kahan acc;
+    acc.init();
+    for (int ch = 0; ch < nchunk; ++ch) acc.add(partial_den[(size_t)ch * plane + i]);
+    v = acc.s - acc.c;
+    den[i] = v;
+  }
+  v = warp_max(v);
+  if (threadIdx.x % 32 == 0) red[threadIdx.x / 32] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float mx = 0.f;
+    for (int w = 0; w < 8; ++w) mx = fmaxf(mx, red[w]);
+    atomic_max_nonneg(dmax, mx);
+  }
+}
+
+// Σ over chunks in order; mode 0: P += coef·Σ; 1: out = coef·Σ; 2: out += Σ compensated;
+// 3: the blend P = (Σ + reg·P) / max(norm + reg, 1e-12) with reg = coef·max norm
+// (engine/ops.rs:371-381), `norm` one plane shared by the modes.
 __global__ void probe_finalize_kernel(const float2* partial, int nchunk, int count,
                                       float2* probe, float2* out, float2* comp, float coef,
-                                      int mode) {
+                                      int mode, const float* norm = nullptr,
+                                      const float* norm_max = nullptr, int plane = 1) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
   KahanC acc;
@@ -286,6 +331,9 @@ __global__ void probe_finalize_kernel(const float2* partial, int nchunk, int cou
   const float2 v = acc.value();
   if (mode == 0) {
     probe[i] = cadd(probe[i], cscale(v, coef));
+  } else if (mode == 3) {
+    const float reg = coef * (*norm_max);
+    probe[i] = cscale(cadd(v, cscale(probe[i], reg)), 1.f / fmaxf(norm[i % plane] + reg, 1e-12f));
   } else if (mode == 1) {
     out[i] = cscale(v, coef);
   } else {

@@ -133,6 +133,30 @@ class GpuPtycho:
         p = _lib.MlParams(update_object, update_probe, calc_llk, zero_phase_ramp)
         self._check(self._lib.ptyb_ml(self._h, ctypes.byref(p), ncycle))
 
+    @staticmethod
+    def _inertia(x):
+        return (0, 0.0) if x is None else (1, float(x))
+
+    def ap(self, ncycle, obj_inertia=0.01, probe_inertia=None, calc_llk=0, zero_phase_ramp=True):
+        """PyNX AP cycles (reference `ApParams`); an inertia of None leaves that array fixed."""
+        (uo, oi), (up, pi) = self._inertia(obj_inertia), self._inertia(probe_inertia)
+        p = _lib.ApParams(uo, up, oi, pi, calc_llk, zero_phase_ramp)
+        self._check(self._lib.ptyb_ap(self._h, ctypes.byref(p), ncycle))
+
+    def dm(self, ncycle, obj_inertia=0.01, probe_inertia=0.001, alpha=0.02, loop_obj_probe=1,
+           calc_llk=0, zero_phase_ramp=True):
+        """PyNX DM cycles (reference `DmParams`)."""
+        (uo, oi), (up, pi) = self._inertia(obj_inertia), self._inertia(probe_inertia)
+        p = _lib.DmParams(uo, up, oi, pi, alpha, loop_obj_probe, calc_llk, zero_phase_ramp)
+        self._check(self._lib.ptyb_dm(self._h, ctypes.byref(p), ncycle))
+
+    def raar(self, ncycle, obj_inertia=0.01, probe_inertia=0.001, beta=0.9, loop_obj_probe=1,
+             calc_llk=0, zero_phase_ramp=True):
+        """PyNX RAAR cycles (reference `RaarParams`)."""
+        (uo, oi), (up, pi) = self._inertia(obj_inertia), self._inertia(probe_inertia)
+        p = _lib.RaarParams(uo, up, oi, pi, beta, loop_obj_probe, calc_llk, zero_phase_ramp)
+        self._check(self._lib.ptyb_raar(self._h, ctypes.byref(p), ncycle))
+
     # State --------------------------------------------------------------------------------
     def llk(self):
         out = _lib.Llk()
