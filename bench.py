@@ -54,7 +54,23 @@ WORKLOADS = {
     "rpie64": dict(kind="rpie64", algorithm="rpie", batch=100,
                    desc="rPIE, 256^2 object, 64^2 probe, 20x20 raster 8 px +-1 px, "
                         "1e5 photons, batch 100, alpha=beta=0.1"),
+    # the reference's own AP / DM benchmark shape: Fermat 4096 frames, 256^2, 2 modes
+    "dm256": dict(kind="fermat256", algorithm="dm", sample_frames=48,
+                  desc="DM (PyNX defaults: alpha 0.02, object inertia 0.01, probe inertia "
+                       "0.001), 1280^2 object, 256^2 probe x2 modes, Fermat 4096 @ 12 px, "
+                       "1e7 photons"),
+    "raar256": dict(kind="fermat256", algorithm="raar", sample_frames=48,
+                    desc="RAAR (PyNX defaults: beta 0.9, object inertia 0.01, probe inertia "
+                         "0.001), 1280^2 object, 256^2 probe x2 modes, Fermat 4096 @ 12 px, "
+                         "1e7 photons"),
+    "ap256": dict(kind="fermat256", algorithm="ap", sample_frames=48,
+                  desc="AP (object inertia 0.01, probe inertia 0.001), 1280^2 object, 256^2 "
+                       "probe x2 modes, Fermat 4096 @ 12 px, 1e7 photons"),
 }
+
+# Algorithms whose step is one cycle over every frame (the bounded CPU sample runs cycles over
+# the scan's first frames); the others step through seeded batches.
+CYCLES = ("ml", "dm", "raar", "ap")
 
 
 def dist_env():
@@ -131,6 +147,10 @@ def prepare(g, s, wl):
 def run_algorithm(g, wl, nepoch):
     if wl["algorithm"] == "ml":
         g.ml(nepoch, update_object=True, update_probe=True, calc_llk=0, zero_phase_ramp=False)
+    elif wl["algorithm"] in ("dm", "raar"):
+        getattr(g, wl["algorithm"])(nepoch, calc_llk=0, zero_phase_ramp=False)
+    elif wl["algorithm"] == "ap":
+        g.ap(nepoch, probe_inertia=0.001, calc_llk=0, zero_phase_ramp=False)
     elif wl["algorithm"] == "lsqml":
         g.lsqml(nepoch, batch_size=wl["batch"], cost=wl["cost"], seed=7)
     else:
@@ -167,6 +187,10 @@ def algorithmic_bytes(kind, s, wl):
         "object_lsqml": 8 * K * n2,
         "object_rpie": 8 * K * n2,
         "object_ml": 8 * K * n2 + moved,
+        # AP / DM / RAAR: object window, counts, the carried waves read and written (RAAR also
+        # its iterate)
+        "frame_carry": 8 * n2 + 4 * n2 + (32 if wl["algorithm"] == "raar" else 16) * K * n2,
+        "object_blend": 8 * K * n2,
     }
     return table.get(kind)
 
@@ -199,12 +223,19 @@ def cpu_baseline(s, wl, seconds=15.0, threads=None, cycles=2):
     ops.FFT_WORKERS = threads
     n = s["n"]
     optics = ops.Optics.far_field(sim.WAVELENGTH, sim.DISTANCE, sim.DETECTOR_PIXEL, [n, n])
-    if wl["algorithm"] == "ml":
+    if wl["algorithm"] in CYCLES:
         t = sample_scan(s, min(wl["sample_frames"], len(s["counts"])))
         p = Ptycho(t["counts"], t["y"], t["x"], optics, t["object"], t["probe"])
-        p.set_positions(np.zeros((p.addr.nframe, 2)), refine=wl["refine"])
         t0 = time.perf_counter()
-        p.ml(cycles, update_object=True, update_probe=True, calc_llk=0, zero_phase_ramp=False)
+        if wl["algorithm"] == "ml":
+            p.set_positions(np.zeros((p.addr.nframe, 2)), refine=wl["refine"])
+            t0 = time.perf_counter()
+            p.ml(cycles, update_object=True, update_probe=True, calc_llk=0,
+                 zero_phase_ramp=False)
+        elif wl["algorithm"] == "ap":
+            p.ap(cycles, probe_inertia=0.001, calc_llk=0, zero_phase_ramp=False)
+        else:
+            getattr(p, wl["algorithm"])(cycles, calc_llk=0, zero_phase_ramp=False)
         dt = time.perf_counter() - t0
         ops.FFT_WORKERS = None
         return p.addr.nframe * cycles / dt, p.addr.nframe * cycles, dt, p
@@ -239,8 +270,9 @@ def object_nrmse(a, b, weight):
 
 
 def accuracy(s, wl, oracle_state, device, cycles=2):
-    """The FP32 GPU path against the float64 oracle on the bounded ML sample: object NRMSE
-    after the global phase, over the illuminated pixels (illumination ≥ 1e-3 of its max)."""
+    """The FP32 GPU path against the float64 oracle on the bounded sample of cycles: object
+    NRMSE after the global phase, over the illuminated pixels (illumination ≥ 1e-3 of its
+    max), and for ML the largest difference of the refined offsets."""
     from oracle import ops
     from ptyrs_b200 import GpuPtycho, Scan
     t = sample_scan(s, oracle_state.addr.nframe)
@@ -249,15 +281,17 @@ def accuracy(s, wl, oracle_state, device, cycles=2):
         prepare(g, t, wl)
         run_algorithm(g, wl, cycles)
         obj = g.object()
-        d = g.positions()
+        d = g.positions() if wl["algorithm"] == "ml" else None
     illum = ops.illumination(oracle_state.addr.views, oracle_state.object.shape,
                              oracle_state.probe)
     w = (illum >= 1e-3 * illum.max()).astype(float)
-    moved = oracle_state.offsets
-    return {"object_nrmse_vs_f64": object_nrmse(obj, oracle_state.object, w),
-            "offsets_max_abs_diff_px": float(np.abs(d - moved).max()),
-            "sample": f"{cycles} ML cycles over the first {t['counts'].shape[0]} frames, GPU "
-                      "FP32 vs the float64 oracle from the same start"}
+    out = {"object_nrmse_vs_f64": object_nrmse(obj, oracle_state.object, w),
+           "sample": f"{cycles} {wl['algorithm'].upper()} cycles over the first "
+                     f"{t['counts'].shape[0]} frames, GPU FP32 vs the float64 oracle from the "
+                     "same start"}
+    if d is not None:
+        out["offsets_max_abs_diff_px"] = float(np.abs(d - oracle_state.offsets).max())
+    return out
 
 
 def reference_arm(args, wl):
@@ -278,6 +312,8 @@ def reference_arm(args, wl):
     if wl["algorithm"] == "ml":
         what = (f"one ML cycle (with position refinement) over the first "
                 f"{wl['sample_frames']} frames")
+    elif wl["algorithm"] in CYCLES:
+        what = f"one {wl['algorithm'].upper()} cycle over the first {wl['sample_frames']} frames"
     else:
         what = f"one {wl['algorithm']} batch update of {wl['batch']} frames"
     sample = (f"{args.steps} steps of {what} of the {args.workload} scan ({frames} "
@@ -421,15 +457,16 @@ def main():
         e2e = {"value": P * ws * args.e2e_steps / dt, "unit": "patterns*iter/s",
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "what": "per step: create from pinned host counts (and the start offsets), one "
-                       "epoch or ML cycle, the object, probe (and offsets) read back"}
+                       "epoch or cycle, the object, probe (and offsets) read back"}
 
     cpu, acc = None, None
     if rank == 0 and not args.no_cpu:
         threads = os.cpu_count() or 1
         v, done, secs, state = cpu_baseline(s, wl, seconds=15.0, threads=threads)
-        if wl["algorithm"] == "ml":
-            what = (f"2 ML cycles with position refinement over the first "
-                    f"{state.addr.nframe} frames of the scan")
+        if wl["algorithm"] in CYCLES:
+            what = (f"2 {wl['algorithm'].upper()} cycles"
+                    + (" with position refinement" if wl["algorithm"] == "ml" else "")
+                    + f" over the first {state.addr.nframe} frames of the scan")
             acc = accuracy(s, wl, state, local)
         else:
             what = f"{done // wl['batch']} batch updates of {wl['batch']} frames of the scan"

@@ -83,6 +83,8 @@ constexpr size_t kNoallocScratchBytes = size_t(32) << 20;
 // Object slices of a multislice handle, and the float scalars on the device (maxima, the
 // batch's object and probe steps, one step per further slice).
 constexpr int kMaxSlices = 16;
+// Room for the kernel kinds of the per-kernel timing (the Kind enum below fits it).
+constexpr int kMaxKinds = 48;
 constexpr int kScalars = 8 + kMaxSlices + 2;
 // The maxima of the AP / DM / RAAR blends' object and probe norms.
 constexpr int kScalObjNorm = 8 + kMaxSlices, kScalProbeNorm = kScalObjNorm + 1;
@@ -191,9 +193,9 @@ struct ptyb_handle {
     cudaEvent_t a, b;
   };
   std::vector<Pending> pending;
-  double kind_ms[32] = {0};
-  int64_t kind_n[32] = {0};
-  int64_t kind_frames[32] = {0};  // frames the launches of each kind processed
+  double kind_ms[kMaxKinds] = {0};
+  int64_t kind_n[kMaxKinds] = {0};
+  int64_t kind_frames[kMaxKinds] = {0};  // frames the launches of each kind processed
   cudaEvent_t call_ev[2] = {nullptr, nullptr};
   float last_call_ms = 0.f;
   // Host state.
@@ -307,6 +309,7 @@ enum Kind : int {
   kKPositionSums, kKSliceForward, kKSliceBackward, kKSliceLlk, kKFrameProject, kKSpectrum,
   kKDerivSums, kKBackSpectrum, kKSliceGrad, kKFrameCarry, kKObjBlend, kNumKinds
 };
+static_assert(kNumKinds <= kMaxKinds, "the timing arrays hold kMaxKinds kinds");
 const char* const kKindNames[kNumKinds] = {
     "frame_rpie", "frame_lsqml", "frame_ml_grad", "frame_llk", "frame_store",
     "frame_from_store", "object_rpie", "object_overlap", "object_lsqml", "object_ml",

@@ -220,7 +220,7 @@ template <int N, int C, int MODE>
 __global__ void __launch_bounds__(FrameShape<N, C>::T,
                                   N == 256 && FrameShape<N, C>::T <= 256 &&
                                           (MODE == kMlGrad || MODE == kProjectKept ||
-                                           MODE == kLlk)
+                                           MODE == kLlk || MODE == kCarry)
                                       ? 3
                                       : frame_min_blocks<N, C>())
     frame_kernel(FrameArgs a) {

@@ -145,7 +145,9 @@ def make_scan(kind, seed=0, scale=1.0):
     10000 at 12 px, 1e7 photons, the frames taken at true positions off the nominal ones by
     seeded N(0, 1.5 px) offsets (`true_offsets`; the solver is given the nominal positions),
     counts generated on the CUDA device. `scale` < 1 keeps that fraction of the positions (the
-    same first ones) for small cases.
+    same first ones) for small cases. kind "fermat256": 1280² object, 256² probe with 2 modes
+    (0.8/0.2), Fermat 4096 at 12 px, 1e7 photons, counts on the CUDA device (the scan of the
+    AP / DM / RAAR workloads).
     """
     if kind == "rpie64":
         n, side, modes, photons = 64, 256, [1.0], 1e5
@@ -156,6 +158,9 @@ def make_scan(kind, seed=0, scale=1.0):
     elif kind == "ml256":
         n, side, modes, photons = 256, 2048, [0.8, 0.2], 1e7
         pos = fermat_positions(10000, 12.0)
+    elif kind == "fermat256":
+        n, side, modes, photons = 256, 1280, [0.8, 0.2], 1e7
+        pos = fermat_positions(4096, 12.0)
     else:
         raise ValueError(kind)
     if scale < 1.0:
@@ -166,6 +171,8 @@ def make_scan(kind, seed=0, scale=1.0):
     true_offsets = np.zeros((len(pos), 2))
     if kind == "ml256":
         true_offsets = np.random.default_rng(seed + 4).normal(0.0, 1.5, (len(pos), 2))
+        counts = far_field_counts_gpu(truth, probe, c, true_offsets, photons, seed + 3)
+    elif kind == "fermat256":
         counts = far_field_counts_gpu(truth, probe, c, true_offsets, photons, seed + 3)
     else:
         counts = far_field_counts(truth, probe, c, photons, seed + 3)

@@ -33,6 +33,16 @@ def test_every_declared_symbol_is_exported(lib):
     assert set(names) == set(_lib.SIGNATURES)
 
 
+def test_kernel_kinds_are_named(lib):
+    """Every kernel kind of the per-kernel timing has its own name (the names key the bench's
+    kernel table)."""
+    k = lib.ptyb_kernel_kinds()
+    names = [lib.ptyb_kernel_name(i).decode() for i in range(k)]
+    assert all(names) and len(set(names)) == k
+    assert {"frame_carry", "object_blend", "frame_ml_grad"} <= set(names)
+    assert lib.ptyb_kernel_name(k).decode() == ""
+
+
 @pytest.mark.parametrize("nframe,size,seed,epoch", [(0, 3, 7, 0), (1, 1, 7, 0), (30, 4, 7, 0),
                                                     (30, 4, 7, 5), (400, 100, 7, 3),
                                                     (4096, 256, 123456789, 99),
