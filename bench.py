@@ -207,7 +207,11 @@ NCU_DRAM_BYTES_PER_FRAME = {
     "ml256": {"ml_gamma": 4.51e6, "frame_ml_grad": 3.51e6, "frame_project": 3.54e6,
               "deriv_sums": 1.06e6, "move": 0.97e6, "back_spectrum": 2.06e6,
               "object_ml": 2.17e6, "frame_llk": 1.34e6},
+    # the carry pass on the 1024-frame cut of the dm256 scan, profiles/dm256_launch_list.md
+    "dm256": {"frame_carry": 2.33e6},
 }
+NCU_PROFILE = {"ml256": "profiles/ml256_launch_list.md (a 1000-frame cut)",
+               "dm256": "profiles/dm256_launch_list.md (a 1024-frame cut)"}
 
 
 def cpu_baseline(s, wl, seconds=15.0, threads=None, cycles=2):
@@ -417,8 +421,8 @@ def main():
                     "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
                     "peak_source": pk_kind, "traffic": traffic,
                     "traffic_source": None if traffic is None else
-                    "ncu DRAM bytes per frame on a 1000-frame cut of the same scan "
-                    "(profiles/ml256_launch_list.md) times this launch's frames",
+                    "ncu DRAM bytes per frame on a cut of the same scan "
+                    f"({NCU_PROFILE[args.workload]}) times this launch's frames",
                     "bytes_per_launch": bytes_launch, "mean_launch_ms": kms / kn,
                     "share": kms / sum(v[0] for v in times.values())}
 
