@@ -1,9 +1,9 @@
-"""rPIE and ML (Poisson conjugate gradient) in float64 (oracle restatement, test
+"""rPIE, ML (Poisson conjugate gradient), AP, DM and RAAR in float64 (oracle restatement, test
 infrastructure only).
 
 Follows physwkim/ptyrs `ptyrs/src/engine/ptycho.rs` (`Ptycho`) for the far-field and
-planar near-field optics of a single object slice; ML also under `Features::position`'s
-sub-pixel offsets with Patch sampling (`engine/features.rs`, `Shifted`).
+planar near-field optics of a single object slice; rPIE, ML, AP, DM and RAAR also under
+`Features::position`'s sub-pixel offsets with Patch sampling (`engine/features.rs`, `Shifted`).
 """
 import numpy as np
 
@@ -88,6 +88,34 @@ class Shifted:
             e, _ = ops.translation(probe_shape[-2:], self.offsets[f])
             spectrum += ops.fft2(y) * np.conj(e)
         return np.conj(self.quad) * ops.ifft2(spectrum), norm
+
+    def psi_to_obj_probe(self, obj, probe, psi, obj_inertia, probe_inertia):
+        """psi_to_obj_probe under the move (features.rs:653-725), both from the arrays on entry;
+        returns `(object, probe)`. The probe takes the first conjugate-gradient step of
+        `min ‖psi − A·P'‖² + reg·‖P' − P‖²` preconditioned by `D = Σ|O|² + reg` per mode:
+        `s = g / D` with `g = A^H(psi − A·P)`, `P += α·s`, `α = <g, s> / (‖A·s‖² + reg·‖s‖²)`
+        where `<g, s> > 0`; the object takes `blend` of its sums under this (old) probe's
+        waves."""
+        new_obj, new_probe = obj, probe
+        if probe_inertia is not None:
+            residual = psi - self.to_psi(obj)
+            num, norm = self.accumulate_probe(obj, probe.shape, residual)
+            reg = max(0.0, float(norm.max())) * probe_inertia
+            d = np.maximum(norm + reg, 1e-12)
+            slope = (np.abs(num) ** 2 / d).sum(axis=(1, 2))
+            step = num / d
+            curvature = reg * (np.abs(step) ** 2).sum(axis=(1, 2))
+            moved = fftshift2(Shifted(self.views, step, self.quad, self.offsets).to_psi(obj))
+            for k, p in enumerate(self.pidx):
+                curvature[p] += float((np.abs(moved[k]) ** 2).sum())
+            new_probe = probe.copy()
+            for m in range(probe.shape[0]):
+                if slope[m] > 0.0:
+                    new_probe[m] = probe[m] + step[m] * (slope[m] / curvature[m])
+        if obj_inertia is not None:
+            num, norm = self.accumulate_obj(obj.shape, psi)
+            new_obj = _blend(obj, num, norm, obj_inertia)
+        return new_obj, new_probe
 
     def position_sums(self, obj, psi, nframe):
         """Per frame `[num, den]` (features.rs:992-1025): `num[a] = Re Σ conj(x − O·W)·∂psi_a`,
@@ -304,7 +332,8 @@ class Ptycho:
     # AP ---------------------------------------------------------------------------------
     def ap(self, ncycle, obj_inertia=0.01, probe_inertia=None, calc_llk=0,
            zero_phase_ramp=True):
-        """PyNX AP without features (engine/ptycho.rs:609-641, ops.rs:352-381)."""
+        """PyNX AP (engine/ptycho.rs:609-641, ops.rs:352-381), under the position model when
+        offsets are set."""
         nframe, nmode = self.addr.nframe, self.addr.nmode
         views, q = self.addr.views, self.optics.quad
         for ic in range(ncycle):
@@ -314,6 +343,19 @@ class Ptycho:
                 l = ops.llk(self.obs, slice(0, nframe), nmode, psi).normalised(self.obs.nb_obs)
             psi = ops.apply_amplitude(self.obs, slice(0, nframe), nmode, psi)
             psi = self.optics.exit_adjoint(psi)
+            s = self.shifted()
+            if s is not None:
+                # under the move: the position sums against the arrays the projection read,
+                # both updates from them, then the position step (engine/ptycho.rs:627-636)
+                sums = s.position_sums(self.object, psi, nframe) if self.refine else None
+                self.object, self.probe = s.psi_to_obj_probe(self.object, self.probe, psi,
+                                                             obj_inertia, probe_inertia)
+                if sums is not None:
+                    ops.position_step(self.offsets, sums)
+                if l is not None:
+                    self.record("ap", l)
+                self.cycle += 1
+                continue
             acc = (ops.accumulate_obj(views, self.object.shape, self.probe, q, psi)
                    if obj_inertia is not None else None)
             if probe_inertia is not None:
@@ -335,10 +377,25 @@ class Ptycho:
         return self.optics.exit_adjoint(far)
 
     def update_obj_probe(self, psi, obj_inertia, probe_inertia, loops):
-        """DM's and RAAR's update (engine/ptycho.rs:732-754) without features: `loops` times an
-        object-only then a probe-only `psi_to_obj_probe`, so the probe update sees the new
-        object (engine/ops.rs:352-369)."""
+        """DM's and RAAR's update (engine/ptycho.rs:732-754): the position sums of `psi` under
+        the cycle's model while the positions are refined, `loops` times an object-only then a
+        probe-only `psi_to_obj_probe` (engine/ops.rs:352-369; under the move each from the
+        current probe's waves), so the probe update sees the new object, then the position
+        step."""
         views, q = self.addr.views, self.optics.quad
+        s = self.shifted()
+        if s is not None:
+            sums = s.position_sums(self.object, psi, self.addr.nframe) if self.refine else None
+            for _ in range(loops):
+                if obj_inertia is not None:
+                    self.object, _ = self.shifted().psi_to_obj_probe(
+                        self.object, self.probe, psi, obj_inertia, None)
+                if probe_inertia is not None:
+                    _, self.probe = self.shifted().psi_to_obj_probe(
+                        self.object, self.probe, psi, None, probe_inertia)
+            if sums is not None:
+                ops.position_step(self.offsets, sums)
+            return
         for _ in range(loops):
             if obj_inertia is not None:
                 num, norm = ops.accumulate_obj(views, self.object.shape, self.probe, q, psi)

@@ -3,7 +3,10 @@ internal consistency: with zero offsets it is the unshifted model; its back-proj
 the adjoints of its forward map; its gradients and position derivatives match central finite
 differences of the Poisson LLK and of the exit waves; the ML loop with refined offsets moves
 them toward the offsets the data were made with (slowly: AP's step from the magnitude
-projection moves a frame by a few thousandths of a pixel per cycle here)."""
+projection moves a frame by a few thousandths of a pixel per cycle here). The probe update of
+AP, DM and RAAR under the move holds the reference's own checks (engine/ptycho.rs:1495-1596):
+with zero offsets it is the blend, the overlap error never rises, the solution is a fixed
+point; and AP, DM and RAAR refining positions move them toward the drawn ones."""
 import numpy as np
 import pytest
 
@@ -137,3 +140,106 @@ def test_ml_with_refined_positions_lowers_llk_and_recovers_offsets(update_probe)
     assert np.abs(p.offsets - true).mean() < before
     moved = p.offsets.ravel()
     assert np.dot(moved, true.ravel()) > 0.8 * np.linalg.norm(moved) * np.linalg.norm(true)
+
+
+# The probe update of AP, DM and RAAR under the move (engine/features.rs:653-725), checked as the
+# reference checks it (engine/ptycho.rs:1495-1596): five frames of a 3-pixel Fermat spiral, 16²
+# frames, two probe modes, an object of random phase whose modulus is `modulus(u)` of a uniform
+# u, the exit waves those of a truth probe, the probe started 30 % away from it.
+
+def overlap_state(modulus=None, offsets=None, seed=11):
+    n, nframe = 16, 5
+    rng = np.random.default_rng(seed)
+    pos = sim.fermat_positions(nframe, 3.0)
+    side = 40
+    obj = sim.smooth_object(side, seed)
+    if modulus is not None:
+        u = rng.uniform(size=(1, side, side))
+        obj = modulus(u) * np.exp(2j * np.pi * rng.uniform(size=(1, side, side)))
+    truth = sim.hermite_probe(n, n / 4.0, [0.7, 0.3])
+    px = sim.object_pixel(n)
+    optics = ops.Optics.far_field(sim.WAVELENGTH, sim.DISTANCE, sim.DETECTOR_PIXEL, [n, n])
+    p = Ptycho(np.zeros((nframe, n, n), np.float32), pos[:, 0] * px, pos[:, 1] * px, optics,
+               obj, truth)
+    if offsets is not None:
+        p.set_positions(np.array([offsets(f) for f in range(nframe)], np.float64))
+    psi = p.calc_psi()
+    p.probe = truth * (1.0 + 0.3 * rng.normal(size=truth.shape)) * np.exp(0.3j)
+    return p, psi, truth
+
+
+def fractional(f):
+    return [np.sin(1.3 * f + 0.2), -np.cos(0.7 * f)]
+
+
+def whole(f):
+    return [(f % 5) - 2.0, ((2 * f + 1) % 3) - 1.0]
+
+
+def probe_update(p, psi, inertia):
+    s = p.shifted()
+    if s is None:
+        views, q = p.addr.views, p.optics.quad
+        num, norm = ops.accumulate_probe(views, p.object, p.probe.shape, q, psi)
+        from oracle.ptycho import _blend
+        return _blend(p.probe, num, norm, inertia)
+    return s.psi_to_obj_probe(p.object, p.probe, psi, None, inertia)[1]
+
+
+def overlap_error(p, psi):
+    return float((np.abs(p.calc_psi() - psi) ** 2).sum())
+
+
+@pytest.mark.parametrize("inertia", [0.0, 0.001])
+def test_probe_update_under_zero_offsets_is_the_blend(inertia):
+    plain, psi, _ = overlap_state()
+    still, psi2, _ = overlap_state(offsets=lambda f: [0.0, 0.0])
+    a, b = probe_update(still, psi2, inertia), probe_update(plain, psi, inertia)
+    assert np.abs(a - b).max() < 1e-14 * np.abs(b).max()
+
+
+@pytest.mark.parametrize("modulus", [lambda u: 10.0 ** (-3.0 * u),
+                                     lambda u: np.where(u < 0.5, 0.0, 1.0)],
+                         ids=["decades", "binary"])
+@pytest.mark.parametrize("offsets", [whole, fractional], ids=["whole", "fractional"])
+@pytest.mark.parametrize("inertia", [0.0, 0.05])
+def test_overlap_error_never_rises_under_a_moved_probe(modulus, offsets, inertia):
+    p, psi, _ = overlap_state(modulus, offsets)
+    first = before = overlap_error(p, psi)
+    rise = 0.0
+    for _ in range(30):
+        p.probe = probe_update(p, psi, inertia)
+        now = overlap_error(p, psi)
+        if before > 1e-24 * first:
+            rise = max(rise, now / before)
+        before = now
+    assert rise <= 1.0 + 1e-12
+    assert before / first < (1.0 if inertia == 0.0 else 0.2)
+
+
+@pytest.mark.parametrize("inertia", [0.0, 0.001])
+def test_probe_update_under_a_moved_probe_holds_the_solution(inertia):
+    p, psi, truth = overlap_state(lambda u: 0.2 + 0.8 * u, fractional)
+    p.probe = truth.copy()
+    for _ in range(3):
+        p.probe = probe_update(p, psi, inertia)
+    assert np.abs(p.probe - truth).max() < 1e-13 * np.abs(truth).max()
+    p.probe = np.zeros_like(truth)
+    assert not probe_update(p, np.zeros_like(psi), inertia).any()
+
+
+@pytest.mark.parametrize("algorithm", ["ap", "dm", "raar"])
+def test_carried_algorithms_with_refined_positions_recover_offsets(algorithm):
+    """AP, DM and RAAR under the move with the positions refined, from the nominal positions of
+    counts made at sub-pixel offsets: the LLK falls and the offsets move toward the drawn ones."""
+    d0 = np.random.default_rng(8).uniform(-0.8, 0.8, (14, 2))
+    p, truth = small_scan(offsets=d0)
+    p.object = truth * 0.97 * np.exp(0.05j)
+    p.set_positions(np.zeros((p.addr.nframe, 2)), refine=True)
+    start = p.llk().poisson
+    kw = dict(probe_inertia=0.001) if algorithm == "ap" else {}
+    getattr(p, algorithm)(15, calc_llk=0, zero_phase_ramp=False, **kw)
+    err0 = np.abs(d0 - d0.mean(0)).mean()
+    err = np.abs((d0 - d0.mean(0)) - (p.offsets - p.offsets.mean(0))).mean()
+    assert p.llk().poisson < start
+    assert err < err0
