@@ -162,15 +162,19 @@ int ptyb_ml(ptyb_handle* h, const ptyb_ml_params* params, int32_t ncycle);
 
 /* Reference `GpuPtycho::ap` (engine/gpu/ap.rs:28-44; CPU twin `Ptycho::ap`,
  * engine/ptycho.rs:609-641): per cycle every frame's exit waves, the magnitude projection (the
- * LLK record is of the estimate it projects), then both updates from the old arrays. Single
- * slice, without the position model (PTYB_INVALID otherwise). */
+ * LLK record is of the estimate it projects), then both updates from the old arrays. Under
+ * the position model (ptyb_set_positions) every frame's probe is moved by its offset, the
+ * probe takes the reference's line-searched step through the move's adjoint
+ * (engine/features.rs:653-725) and refined offsets take the position step from the projected
+ * waves. Single slice (PTYB_INVALID otherwise). */
 int ptyb_ap(ptyb_handle* h, const ptyb_ap_params* params, int32_t ncycle);
 
 /* Reference `GpuPtycho::dm` (engine/gpu/dm.rs:32-38; CPU twin `Ptycho::dm`,
  * engine/ptycho.rs:653-691): cycle 0 of a call starts from the estimate's exit waves, later
  * cycles reflect the carried waves; the LLK record is of the estimate the cycle starts from,
- * and a recorded cycle ends by balancing Σ|O| and Σ|P|. Single slice, without the position
- * model. */
+ * and a recorded cycle ends by balancing Σ|O| and Σ|P|. Under the position model as ptyb_ap,
+ * each update from the current probe's moves and the position sums from the carried waves.
+ * Single slice. */
 int ptyb_dm(ptyb_handle* h, const ptyb_dm_params* params, int32_t ncycle);
 
 /* Reference `GpuPtycho::raar` (engine/gpu/raar.rs:17-23; CPU twin `Ptycho::raar`,

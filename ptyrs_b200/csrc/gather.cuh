@@ -246,7 +246,8 @@ struct ProbeArgs {
   float2* partial;        // [nchunk][K][N][N]
   float* partial_den;     // mode 2: [nchunk][N][N] Σ_slots |O|² over the window
   float alpha;
-  int nslot, chunk, nxo, K, N, mode;  // mode 0 rPIE weight, 1 plain conj(q·O), 2 also Σ|O|²
+  // mode 0 rPIE weight, 1 plain conj(q·O), 2 also Σ|O|², 3 Σ|O|² alone
+  int nslot, chunk, nxo, K, N, mode;
 };
 
 constexpr int kMaxProbeChunk = 256;
@@ -277,7 +278,8 @@ __global__ void __launch_bounds__(256) probe_partial_kernel(ProbeArgs a) {
   for (int s = s0; s < s1; ++s) {
     const int2 c = cs[s - s0];
     const float2 o = a.object[(size_t)(c.x + yy) * a.nxo + c.y + xx];
-    if (a.mode == 2) den.add(cnorm2(o));
+    if (a.mode >= 2) den.add(cnorm2(o));
+    if (a.mode == 3) continue;
     float2 w = cconj(cmul(o, q));
     if (a.mode == 0) w = cscale(w, 1.f / ((1.f - a.alpha) * cnorm2(o) + a.alpha * om[s - s0]));
 #pragma unroll
@@ -286,10 +288,88 @@ __global__ void __launch_bounds__(256) probe_partial_kernel(ProbeArgs a) {
       acc[m].add(cmul(w, a.upd[((size_t)s * a.K + m) * plane + pix]));
     }
   }
+  if (a.mode != 3) {
 #pragma unroll
-  for (int m = 0; m < kMaxModes; ++m)
-    if (m < a.K) a.partial[((size_t)blockIdx.y * a.K + m) * plane + pix] = acc[m].value();
-  if (a.mode == 2) a.partial_den[(size_t)blockIdx.y * plane + pix] = den.s - den.c;
+    for (int m = 0; m < kMaxModes; ++m)
+      if (m < a.K) a.partial[((size_t)blockIdx.y * a.K + m) * plane + pix] = acc[m].value();
+  }
+  if (a.mode >= 2) a.partial_den[(size_t)blockIdx.y * plane + pix] = den.s - den.c;
+}
+
+// The probe step of AP / DM / RAAR under the move (engine/features.rs:673-712), one block per
+// probe mode m: with D = max(norm + reg, 1e-12) and reg = inertia·max norm, step = g / D,
+// sums[m] = (Σ|g|²/D, reg·Σ|step|²) in double, added in a fixed order.
+__global__ void __launch_bounds__(1024) probe_pcg_step_kernel(const float2* g, const float* norm,
+                                                              const float* norm_max,
+                                                              float inertia, int plane,
+                                                              float2* step, double* sums) {
+  __shared__ double red[2][32];
+  const int m = blockIdx.x;
+  const float reg = inertia * (*norm_max);
+  double slope = 0.0, curv = 0.0;
+  for (int i = threadIdx.x; i < plane; i += 1024) {
+    const float2 v = g[(size_t)m * plane + i];
+    const float d = fmaxf(norm[i] + reg, 1e-12f);
+    const float2 s = cscale(v, 1.f / d);
+    step[(size_t)m * plane + i] = s;
+    slope += ((double)v.x * v.x + (double)v.y * v.y) / d;
+    curv += (double)reg * ((double)s.x * s.x + (double)s.y * s.y);
+  }
+  slope = warp_sum(slope);
+  curv = warp_sum(curv);
+  if (threadIdx.x % 32 == 0) {
+    red[0][threadIdx.x / 32] = slope;
+    red[1][threadIdx.x / 32] = curv;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int w = 0; w < 32; ++w) {
+      a += red[0][w];
+      b += red[1][w];
+    }
+    sums[2 * m] = a;
+    sums[2 * m + 1] = b;
+  }
+}
+
+// Per slot and probe mode, Σ_pixels |O_window|²·|W|² in double (‖A·s‖² of one frame's view of
+// the moved step W), added in a fixed order; grid (slots, K).
+__global__ void __launch_bounds__(256) weighted_norm_kernel(const float2* waves,
+                                                            const float2* object,
+                                                            const int* frames,
+                                                            const int2* corners, int nxo, int N,
+                                                            int K, double* out) {
+  __shared__ double red[8];
+  const int slot = blockIdx.x, m = blockIdx.y;
+  const size_t plane = (size_t)N * N;
+  const int2 c = corners[frames[slot]];
+  const float2* w = waves + ((size_t)slot * K + m) * plane;
+  double acc = 0.0;
+  for (int pix = threadIdx.x; pix < N * N; pix += 256) {
+    const int y = pix / N, x = pix % N;
+    acc += (double)cnorm2(object[(size_t)(c.x + y) * nxo + c.y + x]) * cnorm2(w[pix]);
+  }
+  acc = warp_sum(acc);
+  if (threadIdx.x % 32 == 0) red[threadIdx.x / 32] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int i = 0; i < 8; ++i) s += red[i];
+    out[(size_t)slot * K + m] = s;
+  }
+}
+
+// P_m += alpha_m·step_m over the K probe planes.
+struct ModeCoefs {
+  float c[kMaxModes];
+};
+__global__ void probe_modes_axpy_kernel(float2* probe, const float2* step, ModeCoefs alpha,
+                                        int plane, int count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const float a = alpha.c[i / plane];
+  if (a != 0.f) probe[i] = cadd(probe[i], cscale(step[i], a));
 }
 
 // The probe blend's norm Σ_frames |O|² per pixel: the chunks' sums in chunk order into `den`,

@@ -34,6 +34,10 @@ struct MoveArgs {
   const float2* c;        // [slot][K][N][N] natural: the change of the exit wave (kDerivSums),
                           // the exit-plane gradient (kBackSpectrum)
   double* sums;           // [nframe][4] num_y, num_x, den_y, den_x (kDerivSums)
+  // Optional, [slot][K][N][N] natural: each frame's moved probes W; kDerivSums and
+  // kBackSpectrum then take c − W·O·q, the carried waves' residual against the model
+  // (AP / DM / RAAR, engine/features.rs:653-725, 992-1025).
+  const float2* minus;
 };
 
 // numpy fftfreq of index k of n points (engine/features.rs:337-344).
@@ -108,8 +112,14 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
           v = cmul(w, a.probe[m * plane + y * N + x]);
         else if (MODE == kMoveBack)
           v = cmul(w, out[m * plane + y * N + x]);
-        else if (MODE == kBackSpectrum)
-          v = cmul(w, a.c[(size_t)slot * K * plane + m * plane + y * N + x]);
+        else if (MODE == kBackSpectrum) {
+          float2 cv = a.c[(size_t)slot * K * plane + m * plane + y * N + x];
+          if (a.minus)
+            cv = csub(cv, cmul(cmul(a.minus[(size_t)slot * K * plane + m * plane + y * N + x],
+                                    cconj(w)),
+                               a.quad[y * N + x]));
+          v = cmul(w, cv);
+        }
         else
           v = a.object[(size_t)(corner.x + y) * a.nxo + corner.y + x];
         const int line = m * H + yl;
@@ -194,7 +204,10 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
         for (int m = 0; m < K; ++m) {
           const int line = m * H + yl;
           const float2 d = cmul(o, S[line * L + (x ^ swz(line))]);
-          const float2 v = cf[m * plane + y * N + x];
+          float2 v = cf[m * plane + y * N + x];
+          if (a.minus)
+            v = csub(v, cmul(cmul(a.minus[(size_t)slot * K * plane + m * plane + y * N + x], o),
+                             a.quad[y * N + x]));
           num += (double)v.x * d.x + (double)v.y * d.y;
           den += (double)d.x * d.x + (double)d.y * d.y;
         }

@@ -92,16 +92,44 @@ def test_carried_runs_are_deterministic(case):
 
 
 def test_carried_refusals(case):
-    """The position model and negative counts are refused with the state unchanged."""
-    nframe = len(case["counts"])
+    """Negative counts are refused with the state unchanged."""
     with gpu_of(case) as g:
         before = g.object()
         with pytest.raises(PtybError):
             g.dm(-1)
         with pytest.raises(PtybError):
             g.raar(1, loop_obj_probe=-1)
-        g.set_positions(np.zeros((nframe, 2)))
-        for run in (g.ap, g.dm, g.raar):
-            with pytest.raises(PtybError):
-                run(1)
+        with pytest.raises(PtybError):
+            g.ap(-2)
         assert np.array_equal(g.object(), before)
+
+
+@pytest.mark.parametrize("algorithm", ["ap", "dm", "raar"])
+@pytest.mark.parametrize("refine", [False, True], ids=["held", "refined"])
+def test_carried_with_positions(case, algorithm, refine):
+    """Under per-frame sub-pixel offsets (Patch sampling: every frame's probe moved by its
+    offset), held or refined: the carried waves of the moved model, the object blend under the
+    moved probes, the probe's line-searched step through the move's adjoint and, refining, the
+    position step from the carried waves' sums, against the oracle: the arrays, the LLK records
+    and the offsets' changes. The start object is the perturbed truth (under a flat object the
+    intensities do not depend on the offsets); DM also runs two updates per cycle. The single
+    hard-edged aperture runs one cycle (its moved copies ring over the whole frame)."""
+    nframe = len(case["counts"])
+    ncycle = 1 if case["probe"].shape[0] == 1 else 3
+    d0 = np.random.default_rng(6).uniform(-0.6, 0.6, (nframe, 2))
+    start = dict(case, object=case["truth"] * 0.9 * np.exp(0.1j))
+    kw = dict(calc_llk=1, zero_phase_ramp=False)
+    kw.update(dict(probe_inertia=0.001) if algorithm == "ap" else
+              dict(loop_obj_probe=2) if algorithm == "dm" else {})
+    cpu = oracle_state(start)
+    cpu.set_positions(d0, refine=refine)
+    getattr(cpu, algorithm)(ncycle, **kw)
+    with gpu_of(start) as g:
+        g.set_positions(d0, refine=refine)
+        getattr(g, algorithm)(ncycle, **kw)
+        assert_matches(g, cpu, algorithm)
+        d = g.positions()
+        if refine:
+            assert rel_l2(d - d0, cpu.offsets - d0) < RUN_TOL
+        else:
+            assert np.array_equal(d, d0)
