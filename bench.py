@@ -54,6 +54,11 @@ WORKLOADS = {
     "rpie64": dict(kind="rpie64", algorithm="rpie", batch=100,
                    desc="rPIE, 256^2 object, 64^2 probe, 20x20 raster 8 px +-1 px, "
                         "1e5 photons, batch 100, alpha=beta=0.1"),
+    # pty-chi's multislice object (3 slices) under LSQML, the multislice configuration's shapes
+    "ms128": dict(kind="ms128", algorithm="lsqml", batch=256, cost="poisson",
+                  desc="multislice LSQML, 3 slices of 1536^2 10 um apart (angular spectrum, "
+                       "lambda 0.1 nm, 10 nm pixels), 128^2 probe x2 modes, Fermat 6000 @ "
+                       "12 px, 1e6 photons, batch 256, Poisson"),
     # the reference's own AP / DM benchmark shape: Fermat 4096 frames, 256^2, 2 modes
     "dm256": dict(kind="fermat256", algorithm="dm", sample_frames=48,
                   desc="DM (PyNX defaults: alpha 0.02, object inertia 0.01, probe inertia "
@@ -164,6 +169,7 @@ def algorithmic_bytes(kind, s, wl):
     position model are not."""
     n2 = s["n"] ** 2
     K = s["probe"].shape[0]
+    S = s["object"].shape[0] if s.get("gaps") else 1
     moved = 8 * K * n2 if wl.get("refine") else 0
     table = {
         "frame_store": 8 * n2 + 8 * K * n2 + 4 * n2,
@@ -191,6 +197,10 @@ def algorithmic_bytes(kind, s, wl):
         # its iterate)
         "frame_carry": 8 * n2 + 4 * n2 + (32 if wl["algorithm"] == "raar" else 16) * K * n2,
         "object_blend": 8 * K * n2,
+        # multislice: every slice's window and the counts; forward writes the incident waves
+        # of slices 1.. and the detector field, backward reads them and writes every slice's χ
+        "slice_forward": 8 * n2 * S + 4 * n2 + 8 * K * n2 * S,
+        "slice_backward": 4 * n2 + 8 * n2 * S + 16 * K * n2 * S,
     }
     return table.get(kind)
 
@@ -214,6 +224,25 @@ NCU_PROFILE = {"ml256": "profiles/ml256_launch_list.md (a 1000-frame cut)",
                "dm256": "profiles/dm256_launch_list.md (a 1024-frame cut)"}
 
 
+def oracle_optics(s):
+    """The oracle's optics of the scan: the far field of its geometry, through its slices when
+    it has gaps."""
+    from oracle import ops
+    n = s["n"]
+    optics = ops.Optics.far_field(s["wavelength"], s["distance"], s["detector_pixel"], [n, n])
+    if s.get("gaps"):
+        optics = optics.with_slices([ops.Wavefield([n, n], s["wavelength"], optics.pixel, z)
+                                     for z in s["gaps"]])
+    return optics
+
+
+def oracle_objects(s):
+    """The start object as the oracle takes it: one array, or a list of [1, ny, nx] slices."""
+    if s.get("gaps"):
+        return [s["object"][k:k + 1] for k in range(s["object"].shape[0])]
+    return s["object"]
+
+
 def cpu_baseline(s, wl, seconds=15.0, threads=None, cycles=2):
     """The oracle (numpy float64 restatement of the reference's CPU engine) on a bounded sample
     of the workload. ML: `cycles` cycles (one call, as the GPU step) over the first
@@ -225,8 +254,7 @@ def cpu_baseline(s, wl, seconds=15.0, threads=None, cycles=2):
     from oracle.ptycho import Ptycho
     from ptyrs_b200 import sim
     ops.FFT_WORKERS = threads
-    n = s["n"]
-    optics = ops.Optics.far_field(sim.WAVELENGTH, sim.DISTANCE, sim.DETECTOR_PIXEL, [n, n])
+    optics = oracle_optics(s)
     if wl["algorithm"] in CYCLES:
         t = sample_scan(s, min(wl["sample_frames"], len(s["counts"])))
         p = Ptycho(t["counts"], t["y"], t["x"], optics, t["object"], t["probe"])
@@ -243,14 +271,14 @@ def cpu_baseline(s, wl, seconds=15.0, threads=None, cycles=2):
         dt = time.perf_counter() - t0
         ops.FFT_WORKERS = None
         return p.addr.nframe * cycles / dt, p.addr.nframe * cycles, dt, p
-    p = Ptycho(s["counts"], s["y"], s["x"], optics, s["object"], s["probe"])
+    p = Ptycho(s["counts"], s["y"], s["x"], optics, s["object"][:1], s["probe"])
     from oracle.base import random_batches
     batches = random_batches(p.addr.nframe, wl["batch"], 7, 0)
     done, t0 = 0, time.perf_counter()
-    obj, probe = p.object, p.probe
+    obj, probe = oracle_objects(s), p.probe
     if wl["algorithm"] == "lsqml":
         run = Lsqml(wl["batch"], wl["cost"], 7)
-        run.preconditioner = ops.illumination(p.addr.views, obj.shape, probe)
+        run.preconditioner = ops.illumination(p.addr.views, p.object.shape, probe)
     for frames in batches:
         views = np.concatenate([p.addr.frame_views(f) for f in frames])
         if wl["algorithm"] == "lsqml":
@@ -296,6 +324,38 @@ def accuracy(s, wl, oracle_state, device, cycles=2):
     if d is not None:
         out["offsets_max_abs_diff_px"] = float(np.abs(d - oracle_state.offsets).max())
     return out
+
+
+def accuracy_batches(s, wl, device, nbatch=None):
+    """rPIE and LSQML: one epoch over the first `nbatch` batches' frames of the scan (the same
+    seeded batches) on the GPU in FP32 and in the float64 oracle from the same start; object
+    NRMSE after the global phase over the illuminated pixels."""
+    from oracle import ops
+    from oracle.lsqml import Lsqml
+    from oracle.ptycho import Ptycho
+    from ptyrs_b200 import GpuPtycho, Scan
+    if nbatch is None:
+        nbatch = 1 if s.get("gaps") else 2
+    t = sample_scan(s, min(len(s["counts"]), nbatch * wl["batch"]))
+    optics = oracle_optics(t)
+    p = Ptycho(t["counts"], t["y"], t["x"], optics, t["object"][:1], t["probe"])
+    if wl["algorithm"] == "lsqml":
+        run = Lsqml(wl["batch"], wl["cost"], 7)
+        ref, _, _ = run.epoch(p.addr, p.obs, optics, oracle_objects(t), p.probe)
+    else:
+        p.rpie(1, batch_size=wl["batch"], obj_alpha=0.1, probe_alpha=0.1, seed=7)
+        ref = p.object
+    ref = np.concatenate(ref) if isinstance(ref, list) else ref
+    scan = Scan(t["counts"], t["y"], t["x"], t["wavelength"], t["distance"], t["detector_pixel"])
+    with GpuPtycho(scan, t["object"], t["probe"], device=device, gaps=t.get("gaps")) as g:
+        run_algorithm(g, wl, 1)
+        obj = g.objects()
+    illum = ops.illumination(p.addr.views, p.object.shape, p.probe)
+    w = np.broadcast_to(illum >= 1e-3 * illum.max(), obj.shape).astype(float)
+    return {"object_nrmse_vs_f64": object_nrmse(obj, ref, w),
+            "sample": f"one {wl['algorithm']} epoch over the first {len(t['counts'])} frames "
+                      f"(batches of {wl['batch']}), GPU FP32 vs the float64 oracle from the "
+                      "same start"}
 
 
 def reference_arm(args, wl):
@@ -374,13 +434,14 @@ def main():
         from ptyrs_b200.tune import autotune
         best, table = autotune(scan, s["object"], s["probe"],
                                run=lambda h: run_algorithm(h, wl, 1),
-                               prepare=lambda h: prepare(h, s, wl), device=local)
+                               prepare=lambda h: prepare(h, s, wl), device=local,
+                               gaps=s.get("gaps"))
         args.cluster, args.stack = best["cluster"], best["stack_size"]
         tuned = {"chosen": best, "candidates_ms": [
             {"cluster": o["cluster"], "stack": o["stack_size"],
              "ms": None if ms is None else round(ms, 3)} for ms, o in table]}
     g = GpuPtycho(scan, s["object"], s["probe"], device=local, cluster=args.cluster,
-                  stack_size=args.stack)
+                  stack_size=args.stack, gaps=s.get("gaps"))
     prepare(g, s, wl)
     run_algorithm(g, wl, args.warmup)
     g.synchronize()
@@ -434,7 +495,7 @@ def main():
         pinned.numpy()[...] = s["counts"]
         escan = Scan(pinned.numpy(), s["y"], s["x"], s["wavelength"], s["distance"],
                      s["detector_pixel"])
-        ekw = dict(device=local, cluster=args.cluster, stack_size=args.stack)
+        ekw = dict(device=local, cluster=args.cluster, stack_size=args.stack, gaps=s.get("gaps"))
         with GpuPtycho(escan, s["object"], s["probe"], **ekw) as w:  # warm-up
             prepare(w, s, wl)
             run_algorithm(w, wl, 1)
@@ -445,7 +506,7 @@ def main():
             with GpuPtycho(escan, s["object"], s["probe"], **ekw) as w:
                 prepare(w, s, wl)
                 run_algorithm(w, wl, 1)
-                w.object()
+                w.objects()
                 w.probe()
                 if wl["algorithm"] == "ml":
                     w.positions()
@@ -474,6 +535,7 @@ def main():
             acc = accuracy(s, wl, state, local)
         else:
             what = f"{done // wl['batch']} batch updates of {wl['batch']} frames of the scan"
+            acc = accuracy_batches(s, wl, local)
         cpu = {"value": v, "unit": "patterns*iter/s", "cores": threads, "kind": "port",
                "sample": f"{done} pattern-iterations ({what}) in {secs:.1f} s, numpy float64, "
                          f"FFTs on {threads} threads"}

@@ -135,6 +135,49 @@ def far_field_counts_gpu(obj, probe, corner, offsets, photons, seed, chunk=128,
     return counts.cpu().numpy()
 
 
+def multislice_counts_gpu(slices, probe, corner, gaps, wavelength, pixel, photons, seed,
+                          chunk=64, device=None):
+    """Poisson counts of a multislice object (data generation only, torch): per frame and probe
+    mode the wave crosses the slices, `ψ ← O_s[win]·ψ`, with an angular-spectrum propagation
+    `exp(2πi·z·√(1/λ² − |f|²))` (evanescent frequencies dropped) over each gap `z` between
+    them; the far field of the last product, summed over the modes. Counts `[P, n, n]` float32,
+    detector order, scaled so the mean pattern holds `photons`."""
+    import torch
+    if device is None:
+        device = "cuda" if torch.cuda.is_available() else "cpu"
+    n = probe.shape[-1]
+    P = len(corner)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(int(seed))
+    o = torch.as_tensor(np.concatenate(slices), dtype=torch.complex64, device=device)
+    pr = torch.as_tensor(probe, dtype=torch.complex64, device=device)
+    f = torch.fft.fftfreq(n, d=pixel, device=device, dtype=torch.float64)
+    f2 = f[:, None] ** 2 + f[None, :] ** 2
+    arg = 1.0 / wavelength ** 2 - f2
+    prop = []
+    for z in gaps:
+        ph = 2.0 * np.pi * z * torch.sqrt(torch.clamp(arg, min=0.0))
+        h = torch.polar((arg > 0).to(torch.float64), ph).to(torch.complex64)
+        prop.append(h)
+    iy = torch.arange(n, device=device)
+    inten = torch.empty((P, n, n), dtype=torch.float32, device=device)
+    for s0 in range(0, P, chunk):
+        cs = torch.as_tensor(corner[s0:s0 + chunk], device=device)
+        m = len(cs)
+        rows = (cs[:, 0, None] + iy[None]).reshape(m, n, 1)
+        cols = (cs[:, 1, None] + iy[None]).reshape(m, 1, n)
+        psi = pr[None].expand(m, -1, -1, -1)
+        for s in range(o.shape[0]):
+            psi = psi * o[s][rows, cols][:, None]
+            if s < len(prop):
+                psi = torch.fft.ifft2(torch.fft.fft2(psi) * prop[s])
+        far = torch.fft.fft2(psi, norm="ortho")
+        inten[s0:s0 + m] = torch.fft.fftshift((far.abs() ** 2).sum(dim=1), dim=(-2, -1))
+    inten *= photons / inten.sum(dim=(1, 2)).mean()
+    counts = torch.poisson(inten, generator=gen)
+    return counts.cpu().numpy()
+
+
 def make_scan(kind, seed=0, scale=1.0):
     """Seeded synthetic inputs of a benchmark configuration: returns a dict with counts
     (float32), y, x (metres), object start, probe start, truth object and sizes.
@@ -147,8 +190,28 @@ def make_scan(kind, seed=0, scale=1.0):
     counts generated on the CUDA device. `scale` < 1 keeps that fraction of the positions (the
     same first ones) for small cases. kind "fermat256": 1280² object, 256² probe with 2 modes
     (0.8/0.2), Fermat 4096 at 12 px, 1e7 photons, counts on the CUDA device (the scan of the
-    AP / DM / RAAR workloads).
+    AP / DM / RAAR workloads). kind "ms128": three slices of 1536² (phase scale π/4, independent
+    seeds) 10 µm apart, λ = 0.1 nm at a 10 nm object pixel (detector 0.96 m away, 75 µm
+    pixels), 128² probe with 2 modes (0.8/0.2), Fermat 6000 at 12 px, 1e6 photons; the start
+    is three slices of ones and `gaps` holds the spacings.
     """
+    if kind == "ms128":
+        n, side, photons, wavelength, distance = 128, 1536, 1e6, 1e-10, 0.96
+        pos = fermat_positions(6000, 12.0)
+        if scale < 1.0:
+            pos = pos[:max(2, int(len(pos) * scale))]
+        truth = [smooth_object(side, seed + 2 + k, np.pi / 4) for k in range(3)]
+        probe = hermite_probe(n, n / 4.0, [0.8, 0.2])
+        c = corners(pos, n, side)
+        px = wavelength * distance / (n * DETECTOR_PIXEL)
+        gaps = (1e-5, 1e-5)
+        counts = multislice_counts_gpu(truth, probe, c, gaps, wavelength, px, photons, seed + 3)
+        start = np.ones((3, side, side), np.complex128)
+        return dict(counts=counts, y=pos[:, 0] * px, x=pos[:, 1] * px, object=start,
+                    probe=probe * np.sqrt(photons / (np.abs(probe) ** 2).sum()),
+                    truth=np.concatenate(truth), corners=c, n=n, side=side,
+                    wavelength=wavelength, distance=distance, detector_pixel=DETECTOR_PIXEL,
+                    true_offsets=np.zeros((len(pos), 2)), gaps=gaps)
     if kind == "rpie64":
         n, side, modes, photons = 64, 256, [1.0], 1e5
         pos = raster_positions(20, 20, 8, 1.0, seed + 1)
