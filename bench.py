@@ -59,6 +59,14 @@ WORKLOADS = {
                   desc="multislice LSQML, 3 slices of 1536^2 10 um apart (angular spectrum, "
                        "lambda 0.1 nm, 10 nm pixels), 128^2 probe x2 modes, Fermat 6000 @ "
                        "12 px, 1e6 photons, batch 256, Poisson"),
+    # 32 independent uneven scans at once (ptyb_batch_run), each step one rPIE epoch (batches of
+    # 100) then one LSQML epoch (batches of 256) on every scan
+    "batch32": dict(kind="batch32", algorithm="batch", batch=100, lsqml_batch=256,
+                    desc="32 independent seeded scans at once (one stream each): sides from "
+                         "{64, 128, 256}, objects 4-8x the side, 500-5000 Fermat positions, "
+                         "1e4-1e7 photons (log-uniform), one probe mode; per step one rPIE "
+                         "epoch (batches of 100, alpha 0.1) then one LSQML epoch (batches of "
+                         "256, Poisson) on every scan"),
     # the reference's own AP / DM benchmark shape: Fermat 4096 frames, 256^2, 2 modes
     "dm256": dict(kind="fermat256", algorithm="dm", sample_frames=48,
                   desc="DM (PyNX defaults: alpha 0.02, object inertia 0.01, probe inertia "
@@ -362,7 +370,14 @@ def reference_arm(args, wl):
     rank, ws, _ = dist_env()
     if rank != 0:
         return
-    s = make_inputs(args.workload, 0, scale=args.scale)
+    desc = wl["desc"]
+    if wl["algorithm"] == "batch":
+        # the batch's first scan (make_batch draws the scans in order), rPIE batch updates
+        from ptyrs_b200 import sim
+        s = sim.make_batch(1, seed=0, scale=args.scale)[0]
+        wl = RPIE_OF_BATCH
+    else:
+        s = make_inputs(args.workload, 0, scale=args.scale)
     threads = os.cpu_count() or 1
     for _ in range(args.warmup):
         cpu_baseline(s, wl, seconds=0.0, threads=threads, cycles=1)
@@ -387,13 +402,126 @@ def reference_arm(args, wl):
         "unit": "patterns*iter/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * secs / max(args.steps, 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "description": wl["desc"]},
+        "config": {"workload": args.workload, "description": desc},
         "cpu_baseline": {"value": value, "unit": "patterns*iter/s", "cores": threads,
                          "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "patterns*iter/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+BATCH_RPIE = dict(batch_size=100, obj_alpha=0.1, probe_alpha=0.1, seed=7)
+BATCH_LSQML = dict(batch_size=256, cost="poisson", seed=7)
+RPIE_OF_BATCH = dict(kind="batch32", algorithm="rpie", batch=100)
+
+
+def batch_main(args, wl):
+    """The batched workload: every scan a handle, all run at once by `ptyb_batch_run`; the
+    step's device time is the batch's, from the first launch to the last of any scan."""
+    from ptyrs_b200 import GpuPtycho, Scan, batch_run, build, sim
+    from ptyrs_b200.replicas import Replicas, job_value
+    group = Replicas("nccl")
+    rank, ws, local = group.rank, group.world, group.local
+    import torch
+    build.build()
+    scans = sim.make_batch(32, seed=rank, scale=args.scale)
+    P = sum(len(s["counts"]) for s in scans)
+    scan_of = lambda s, counts=None: Scan(s["counts"] if counts is None else counts, s["y"],
+                                          s["x"], s["wavelength"], s["distance"],
+                                          s["detector_pixel"])
+    handles = [GpuPtycho(scan_of(s), s["object"], s["probe"], device=local) for s in scans]
+    batch_run(handles, args.warmup, args.warmup, rpie=BATCH_RPIE, lsqml=BATCH_LSQML)
+    for h in handles:
+        h.set_timing(True)
+    group.barrier()
+    launches0 = sum(h.launches() for h in handles)
+    clocks = Clocks(local)
+    ms = batch_run(handles, args.steps, args.steps, rpie=BATCH_RPIE, lsqml=BATCH_LSQML)
+    clk = clocks.stop()
+    group.barrier()
+    launches = sum(h.launches() for h in handles) - launches0
+    times, frames, bytes_ = {}, {}, {}
+    for h, s in zip(handles, scans):
+        kf = h.kernel_frames()
+        for k, (kms, kn) in h.kernel_times().items():
+            t = times.setdefault(k, [0.0, 0])
+            t[0] += kms
+            t[1] += kn
+            per = algorithmic_bytes(k, s, RPIE_OF_BATCH) or algorithmic_bytes(
+                k, s, dict(algorithm="lsqml"))
+            if per and kf.get(k):
+                bytes_[k] = bytes_.get(k, 0.0) + per * kf[k]
+                frames[k] = frames.get(k, 0) + kf[k]
+        h.set_timing(False)
+    ms = group.max(ms)
+    value = job_value(2 * P, ws, args.steps, ms)
+    pk, pk_kind = peaks()
+    kname = max(times.items(), key=lambda kv: kv[1][0])[0]
+    # The scans' kernels overlap in time (one stream each), so a kernel's event times do not
+    # add up to wall time: the step's bandwidth is every kernel's algorithmic bytes over the
+    # batch's device time.
+    total = sum(bytes_.values())
+    achieved = total / (ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "whole step (every kernel of every scan)",
+                "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / pk["hbm_gbs"], "peak_source": pk_kind, "traffic": None,
+                "traffic_source": None, "bytes_per_step": total / args.steps,
+                "largest_kernel_by_event_time": kname,
+                "kernels_counted": sorted(bytes_)}
+    e2e = None
+    if args.e2e_steps > 0:
+        pinned = []
+        for s in scans:
+            t = torch.empty(s["counts"].shape, dtype=torch.float32, pin_memory=True)
+            t.numpy()[...] = s["counts"]
+            pinned.append(t)
+        group.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            hs = [GpuPtycho(scan_of(s, c.numpy()), s["object"], s["probe"], device=local)
+                  for s, c in zip(scans, pinned)]
+            batch_run(hs, 1, 1, rpie=BATCH_RPIE, lsqml=BATCH_LSQML)
+            for h in hs:
+                h.object()
+                h.probe()
+                h.close()
+        dt = group.max(time.perf_counter() - t0)
+        h2d = sum(s["counts"].nbytes + 8 * s["object"].size + 8 * s["probe"].size
+                  + 16 * len(s["counts"]) for s in scans)
+        d2h = sum(8 * s["object"].size + 8 * s["probe"].size for s in scans)
+        e2e = {"value": 2 * P * ws * args.e2e_steps / dt, "unit": "patterns*iter/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "what": "per step: create every scan's handle from pinned host counts, one rPIE "
+                       "and one LSQML epoch on all at once, every object and probe read back"}
+    cpu, acc = None, None
+    if rank == 0 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        v, done, secs, _ = cpu_baseline(scans[0], RPIE_OF_BATCH, seconds=15.0, threads=threads)
+        cpu = {"value": v, "unit": "patterns*iter/s", "cores": threads, "kind": "port",
+               "sample": f"{done} pattern-iterations ({done // 100} rPIE batch updates of 100 "
+                         f"frames of the first scan, side {scans[0]['n']}) in {secs:.1f} s, "
+                         f"numpy float64, FFTs on {threads} threads"}
+        acc = accuracy_batches(scans[0], RPIE_OF_BATCH, local)
+    for h in handles:
+        h.close()
+    if rank == 0:
+        sides = {n: sum(1 for s in scans if s["n"] == n) for n in (64, 128, 256)}
+        print(json.dumps({
+            "metric": "diffraction patterns*iter/sec", "value": value,
+            "unit": "patterns*iter/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "description": wl["desc"],
+                       "scale": args.scale, "scans": len(scans), "sides": sides,
+                       "patterns_per_step_per_gpu": 2 * P, "parallelism": f"replicas{ws}",
+                       "l2": "inputs larger than L2 (counts "
+                             f"{sum(s['counts'].nbytes for s in scans) / 1e6:.0f} MB)"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "accuracy": acc,
+            "gpu_launches": int(launches), "clocks": clk,
+            "kernels_ms": {k: round(v[0], 3) for k, v in sorted(times.items())},
+        }), flush=True)
+    group.close()
 
 
 def main():
@@ -417,6 +545,8 @@ def main():
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
         return reference_arm(args, wl)
+    if wl["algorithm"] == "batch":
+        return batch_main(args, wl)
 
     from ptyrs_b200.replicas import Replicas, job_value
     group = Replicas("nccl")

@@ -181,6 +181,18 @@ int ptyb_dm(ptyb_handle* h, const ptyb_dm_params* params, int32_t ncycle);
  * engine/ptycho.rs:698-730): DM's cycle with RAAR's mix of the carried projection and iterate. */
 int ptyb_raar(ptyb_handle* h, const ptyb_raar_params* params, int32_t ncycle);
 
+/* No counterpart in the reference (its engine runs one scan per call; this is the batch of
+ * independent uneven-size scans): `rpie_epochs` rPIE epochs then `lsqml_epochs` LSQML epochs on
+ * every handle at once, one host thread per handle and each handle on its own stream, so the
+ * scans' kernels share the GPU. status[i] (may be NULL) gets handle i's return code; the call
+ * returns PTYB_OK when every handle succeeded, else the first failing handle's code (the
+ * others keep their results). *device_ms (may be NULL) gets the batch's device time from the
+ * first launch to the last of the handles on the first handle's device, -1 if it could not be
+ * taken. The handles must be distinct. */
+int ptyb_batch_run(ptyb_handle* const* handles, int32_t n, const ptyb_rpie_params* rpie,
+                   int32_t rpie_epochs, const ptyb_lsqml_params* lsqml, int32_t lsqml_epochs,
+                   int32_t calc_llk, int32_t* status, float* device_ms);
+
 /* Reference `GpuPtycho::llk` (engine/gpu/mod.rs:871-881): normalised LLK of the estimate. */
 int ptyb_get_llk(ptyb_handle* h, ptyb_llk* out);
 

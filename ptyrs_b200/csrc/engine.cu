@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <set>
 #include <thread>
 #include <string>
 #include <vector>
@@ -2419,6 +2420,69 @@ int ptyb_raar(ptyb_handle* h, const ptyb_raar_params* p, int32_t ncycle) {
   return carried_cycles(h, true, p->beta, p->update_object != 0, p->obj_inertia,
                         p->update_probe != 0, p->probe_inertia, p->loop_obj_probe, p->calc_llk,
                         p->zero_phase_ramp != 0, ncycle);
+}
+
+int ptyb_batch_run(ptyb_handle* const* handles, int32_t n, const ptyb_rpie_params* rpie,
+                   int32_t rpie_epochs, const ptyb_lsqml_params* lsqml, int32_t lsqml_epochs,
+                   int32_t calc_llk, int32_t* status, float* device_ms) {
+  if (device_ms) *device_ms = -1.f;
+  if (!handles || n <= 0 || rpie_epochs < 0 || lsqml_epochs < 0 || (rpie_epochs > 0 && !rpie) ||
+      (lsqml_epochs > 0 && !lsqml))
+    return PTYB_INVALID;
+  std::set<ptyb_handle*> seen;
+  for (int i = 0; i < n; ++i)
+    if (!handles[i] || !seen.insert(handles[i]).second) return PTYB_INVALID;
+  // The batch's device time: every handle's stream waits on a start event recorded on a stream
+  // of the batch's own, and that stream waits on every handle's last work before the end event
+  // (handles on the first handle's device; the others are not timed).
+  const int dev = handles[0]->device;
+  cudaStream_t ts = nullptr;
+  cudaEvent_t start = nullptr, end = nullptr;
+  bool timing = cudaSetDevice(dev) == cudaSuccess &&
+                cudaStreamCreateWithFlags(&ts, cudaStreamNonBlocking) == cudaSuccess &&
+                cudaEventCreate(&start) == cudaSuccess && cudaEventCreate(&end) == cudaSuccess &&
+                cudaEventRecord(start, ts) == cudaSuccess;
+  for (int i = 0; i < n && timing; ++i)
+    if (handles[i]->device == dev && handles[i]->stream)
+      timing = cudaStreamWaitEvent(handles[i]->stream, start, 0) == cudaSuccess;
+  std::vector<int32_t> rc(n, PTYB_OK);
+  {
+    std::vector<std::thread> workers;
+    workers.reserve(n);
+    for (int i = 0; i < n; ++i)
+      workers.emplace_back([&, i] {
+        int r = rpie_epochs > 0 ? ptyb_rpie(handles[i], rpie, rpie_epochs) : PTYB_OK;
+        if (r == PTYB_OK && lsqml_epochs > 0)
+          r = ptyb_lsqml(handles[i], lsqml, lsqml_epochs, calc_llk);
+        rc[i] = r;
+      });
+    for (auto& w : workers) w.join();
+  }
+  if (timing) {
+    cudaSetDevice(dev);
+    for (int i = 0; i < n && timing; ++i) {
+      if (handles[i]->device != dev || !handles[i]->stream) continue;
+      cudaEvent_t e = nullptr;
+      timing = cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess &&
+               cudaEventRecord(e, handles[i]->stream) == cudaSuccess &&
+               cudaStreamWaitEvent(ts, e, 0) == cudaSuccess;
+      if (e) cudaEventDestroy(e);
+    }
+    float ms = -1.f;
+    if (timing && cudaEventRecord(end, ts) == cudaSuccess &&
+        cudaEventSynchronize(end) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, start, end) == cudaSuccess && device_ms)
+      *device_ms = ms;
+  }
+  if (start) cudaEventDestroy(start);
+  if (end) cudaEventDestroy(end);
+  if (ts) cudaStreamDestroy(ts);
+  int first = PTYB_OK;
+  for (int i = 0; i < n; ++i) {
+    if (status) status[i] = rc[i];
+    if (first == PTYB_OK && rc[i] != PTYB_OK) first = rc[i];
+  }
+  return first;
 }
 
 int ptyb_get_llk(ptyb_handle* h, ptyb_llk* out) {

@@ -332,6 +332,38 @@ class GpuPtycho:
         return int(self._lib.ptyb_launches(self._h))
 
 
+def batch_run(handles, rpie_epochs=30, lsqml_epochs=30, calc_llk=0, rpie=None, lsqml=None):
+    """Independent scans at once (`ptyb_batch_run`): `rpie_epochs` rPIE epochs then
+    `lsqml_epochs` LSQML epochs on every `GpuPtycho` of `handles`, each on its own stream from
+    its own host thread. `rpie` / `lsqml` hold the keywords of `GpuPtycho.rpie` / `.lsqml`
+    (steps, alphas, batch size, cost, seed). Returns the batch's device time in ms; raises
+    PtybError with the first failing handle's message (the others keep their results)."""
+    if not handles:
+        raise ValueError("no handles")
+    r = dict(obj_step=1.0, probe_step=1.0, obj_alpha=0.1, probe_alpha=0.1, batch_size=100,
+             seed=7)
+    r.update(rpie or {})
+    q = dict(batch_size=256, cost="poisson", seed=7)
+    q.update(lsqml or {})
+    rp = _lib.RpieParams(r["obj_step"] is not None, r["probe_step"] is not None,
+                         0.0 if r["obj_step"] is None else r["obj_step"],
+                         0.0 if r["probe_step"] is None else r["probe_step"], r["obj_alpha"],
+                         r["probe_alpha"], r["batch_size"], calc_llk, r["seed"])
+    lp = _lib.LsqmlParams(q["batch_size"], COSTS[q["cost"]], q["seed"])
+    n = len(handles)
+    hs = (ctypes.c_void_p * n)(*[h._h for h in handles])
+    status = (ctypes.c_int32 * n)()
+    ms = ctypes.c_float(-1.0)
+    lib = handles[0]._lib
+    rc = lib.ptyb_batch_run(hs, n, ctypes.byref(rp), rpie_epochs, ctypes.byref(lp), lsqml_epochs,
+                            calc_llk, status, ctypes.byref(ms))
+    if rc != 0:
+        bad = next((i for i in range(n) if status[i] != 0), None)
+        msg = lib.ptyb_last_error(hs[bad]).decode() if bad is not None else "invalid batch"
+        raise PtybError(STATUS.get(rc, rc), f"handle {bad}: {msg}")
+    return float(ms.value)
+
+
 def random_batches(nframe, size, seed, epoch):
     """The reference's seeded mini-batches of one epoch from the native host code, as a list of
     sorted frame lists."""

@@ -178,6 +178,37 @@ def multislice_counts_gpu(slices, probe, corner, gaps, wavelength, pixel, photon
     return counts.cpu().numpy()
 
 
+def make_batch(count=32, seed=0, scale=1.0, sides=(64, 128, 256)):
+    """`count` independent seeded scans of uneven sizes (the batched configuration, on the frame
+    sides the engine has kernels for): per scan a side drawn from `sides`, an object 4–8 times
+    the side, 500–5000 Fermat positions (times `scale`) at a step that keeps the scan inside the
+    object (at most a quarter of the side), log-uniform 1e4–1e7 photons, the defocused aperture
+    probe (one mode); counts made on the CUDA device. Returns a list of `make_scan`-style
+    dicts."""
+    rng = np.random.default_rng(seed + 100)
+    out = []
+    for i in range(count):
+        n = int(rng.choice(sides))
+        side = int(n * rng.uniform(4.0, 8.0))
+        npos = max(2, int(rng.uniform(500, 5000) * scale))
+        photons = 10.0 ** rng.uniform(4.0, 7.0)
+        step = min(n / 4.0, (side - n - 8) * np.sqrt(np.pi) / (2.0 * np.sqrt(npos)))
+        pos = fermat_positions(npos, step)
+        truth = smooth_object(side, seed + 1000 + i)
+        probe = aperture_probe(n, n / 4.0)[None]
+        c = corners(pos, n, side)
+        counts = far_field_counts_gpu(truth, probe, c, np.zeros((npos, 2)), photons,
+                                      seed + 2000 + i)
+        px = object_pixel(n)
+        out.append(dict(counts=counts, y=pos[:, 0] * px, x=pos[:, 1] * px,
+                        object=np.ones_like(truth),
+                        probe=probe * np.sqrt(photons / (np.abs(probe) ** 2).sum()),
+                        truth=truth, corners=c, n=n, side=side, wavelength=WAVELENGTH,
+                        distance=DISTANCE, detector_pixel=DETECTOR_PIXEL,
+                        true_offsets=np.zeros((npos, 2)), photons=photons))
+    return out
+
+
 def make_scan(kind, seed=0, scale=1.0):
     """Seeded synthetic inputs of a benchmark configuration: returns a dict with counts
     (float32), y, x (metres), object start, probe start, truth object and sizes.
