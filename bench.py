@@ -213,6 +213,24 @@ def algorithmic_bytes(kind, s, wl):
     return table.get(kind)
 
 
+# 2-D transforms of one K-plane stack per frame each kernel runs (forward and inverse count one
+# each); the FFT's FP32 work is 5·N²·log2(N²) per plane and transform.
+FFT_PASSES = {"frame_rpie": 2, "frame_lsqml": 2, "frame_ml_grad": 2, "frame_project": 1,
+              "frame_llk": 1, "frame_store": 1, "frame_from_store": 1, "frame_carry": 2,
+              "ml_gamma": 1, "move": 1, "back_spectrum": 1, "deriv_sums": 2}
+# FP32 lanes × 2 flops × clock: 148 SMs × 128 × 2 × 1.965 GHz
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
+
+
+def fft_flops(kind, s):
+    """FP32 flops of a kernel's FFTs per frame, None for kernels without per-frame FFTs."""
+    passes = FFT_PASSES.get(kind)
+    if passes is None:
+        return None
+    n2 = s["n"] ** 2
+    return passes * s["probe"].shape[0] * 5.0 * n2 * np.log2(n2)
+
+
 def sample_scan(s, m):
     """The first `m` frames of the scan, its object and probe starts (a bounded sample)."""
     return dict(s, counts=s["counts"][:m], y=s["y"][:m], x=s["x"][:m])
@@ -623,6 +641,14 @@ def main():
                     f"({NCU_PROFILE[args.workload]}) times this launch's frames",
                     "bytes_per_launch": bytes_launch, "mean_launch_ms": kms / kn,
                     "share": kms / sum(v[0] for v in times.values())}
+        flops = fft_flops(kname, s)
+        if flops:
+            tf = flops * frames_launch / (kms / kn / 1e3) / 1e12
+            roofline["secondary"] = {
+                "bound": "fp32", "achieved": tf, "peak": FP32_NOMINAL_TFLOPS,
+                "unit": "TFLOP/s", "frac": tf / FP32_NOMINAL_TFLOPS,
+                "peak_source": "nominal (148 SMs x 128 FP32 lanes x 2 x 1.965 GHz)",
+                "what": "the kernel's FFT flops, 5 N^2 log2(N^2) per plane and transform"}
 
     # End to end through the public API from pinned host buffers: per step, a fresh state
     # (counts, positions, object and probe uploaded), one epoch, the object and probe read back.
