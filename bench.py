@@ -63,7 +63,7 @@ WORKLOADS = {
     # 100) then one LSQML epoch (batches of 256) on every scan
     "batch32": dict(kind="batch32", algorithm="batch", batch=100, lsqml_batch=256,
                     desc="32 independent seeded scans at once (one stream each): sides from "
-                         "{64, 128, 256}, objects 4-8x the side, 500-5000 Fermat positions, "
+                         "{64, 96, 128, 192, 256}, objects 4-8x the side, 500-5000 Fermat positions, "
                          "1e4-1e7 photons (log-uniform), one probe mode; per step one rPIE "
                          "epoch (batches of 100, alpha 0.1) then one LSQML epoch (batches of "
                          "256, Poisson) on every scan"),
@@ -526,7 +526,7 @@ def batch_main(args, wl):
     for h in handles:
         h.close()
     if rank == 0:
-        sides = {n: sum(1 for s in scans if s["n"] == n) for n in (64, 128, 256)}
+        sides = {n: sum(1 for s in scans if s["n"] == n) for n in (64, 96, 128, 192, 256)}
         print(json.dumps({
             "metric": "diffraction patterns*iter/sec", "value": value,
             "unit": "patterns*iter/s", "n_gpus": ws, "steps": args.steps,

@@ -36,7 +36,8 @@ enum ptyb_counts_kind {
 };
 
 /* A far-field scan (reference `Scan` + `Geometry`, ptyrs-py/src/lib.rs:435-463): counts
- * [nframe][ny][nx] in detector order (zero frequency at the centre), positions in metres. */
+ * [nframe][ny][nx] in detector order (zero frequency at the centre), positions in metres;
+ * square frames of side 64, 96, 128, 192 or 256. */
 typedef struct ptyb_scan {
   int32_t nframe, ny, nx;
   int32_t counts_kind;

@@ -390,8 +390,9 @@ int cluster_for(int N, int K, int want) {
     int n, c;
     size_t bytes;
   };
-  const Opt opts[] = {{64, 1, frame_smem_bytes<64, 1>(K)},   {128, 2, frame_smem_bytes<128, 2>(K)},
-                      {128, 4, frame_smem_bytes<128, 4>(K)}, {256, 8, frame_smem_bytes<256, 8>(K)},
+  const Opt opts[] = {{64, 1, frame_smem_bytes<64, 1>(K)},   {96, 2, frame_smem_bytes<96, 2>(K)},
+                      {128, 2, frame_smem_bytes<128, 2>(K)}, {128, 4, frame_smem_bytes<128, 4>(K)},
+                      {192, 8, frame_smem_bytes<192, 8>(K)}, {256, 8, frame_smem_bytes<256, 8>(K)},
                       {256, 16, frame_smem_bytes<256, 16>(K)}};
   for (const Opt& o : opts)
     if (o.n == N && o.c == want && o.bytes <= lim) return o.c;
@@ -434,6 +435,8 @@ cudaError_t launch_frame_raw(ptyb_handle* h, const FrameArgs& a, int nslot) {
     case 6401: return launch_frame_nc<64, 1, MODE>(a, nslot, h->K, h->stream);
     case 12802: return launch_frame_nc<128, 2, MODE>(a, nslot, h->K, h->stream);
     case 12804: return launch_frame_nc<128, 4, MODE>(a, nslot, h->K, h->stream);
+    case 9602: return launch_frame_nc<96, 2, MODE>(a, nslot, h->K, h->stream);
+    case 19208: return launch_frame_nc<192, 8, MODE>(a, nslot, h->K, h->stream);
     case 25608: return launch_frame_nc<256, 8, MODE>(a, nslot, h->K, h->stream);
     case 25616: return launch_frame_nc<256, 16, MODE>(a, nslot, h->K, h->stream);
   }
@@ -497,6 +500,8 @@ cudaError_t launch_move(ptyb_handle* h, const MoveArgs& a, int nslot) {
       case 6401: e = launch_move_nc<64, 1, MODE>(a, nslot, K, h->stream); break;
       case 12802: e = launch_move_nc<128, 2, MODE>(a, nslot, K, h->stream); break;
       case 12804: e = launch_move_nc<128, 4, MODE>(a, nslot, K, h->stream); break;
+      case 9602: e = launch_move_nc<96, 2, MODE>(a, nslot, K, h->stream); break;
+      case 19208: e = launch_move_nc<192, 8, MODE>(a, nslot, K, h->stream); break;
       case 25608: e = launch_move_nc<256, 8, MODE>(a, nslot, K, h->stream); break;
       case 25616: e = launch_move_nc<256, 16, MODE>(a, nslot, K, h->stream); break;
     }
@@ -542,6 +547,8 @@ cudaError_t launch_slice(ptyb_handle* h, const SliceArgs& a, int nslot) {
       case 6401: e = launch_slice_nc<64, 1, MODE>(a, nslot, h->K, h->stream); break;
       case 12802: e = launch_slice_nc<128, 2, MODE>(a, nslot, h->K, h->stream); break;
       case 12804: e = launch_slice_nc<128, 4, MODE>(a, nslot, h->K, h->stream); break;
+      case 9602: e = launch_slice_nc<96, 2, MODE>(a, nslot, h->K, h->stream); break;
+      case 19208: e = launch_slice_nc<192, 8, MODE>(a, nslot, h->K, h->stream); break;
       case 25608: e = launch_slice_nc<256, 8, MODE>(a, nslot, h->K, h->stream); break;
       case 25616: e = launch_slice_nc<256, 16, MODE>(a, nslot, h->K, h->stream); break;
     }
@@ -1268,7 +1275,9 @@ cudaError_t launch_gamma(ptyb_handle* h, const GammaArgs& a, int nslot) {
   timed(h, kKGamma, [&] {
     switch (h->N) {
       case 64: e = launch_gamma_nc<64, 1>(a, nslot, h->stream); break;
+      case 96: e = launch_gamma_nc<96, 2>(a, nslot, h->stream); break;
       case 128: e = launch_gamma_nc<128, 4>(a, nslot, h->stream); break;
+      case 192: e = launch_gamma_nc<192, 8>(a, nslot, h->stream); break;
       case 256: e = launch_gamma_nc<256, 16>(a, nslot, h->stream); break;
     }
   }, nslot);
@@ -1472,8 +1481,29 @@ void ml_gamma(ptyb_handle* h, double* num, double* den) {
   }
 }
 
-// In-place radix-2 FFT of n (a power of 2) complex doubles, forward, unscaled.
+// In-place FFT of n complex doubles, forward, unscaled: radix 2 for a power of 2, else the
+// direct sum (sides 96 and 192, host-only work of the phase-ramp removal).
 void host_fft(std::vector<double>& re, std::vector<double>& im, size_t off, size_t stride, int n) {
+  if (n & (n - 1)) {
+    std::vector<double> r(n), i(n);
+    for (int k = 0; k < n; ++k) {
+      double sr = 0.0, si = 0.0;
+      for (int j = 0; j < n; ++j) {
+        const double a = -2.0 * M_PI * (double)((long long)j * k % n) / n;
+        const double c = std::cos(a), s = std::sin(a);
+        const double xr = re[off + j * stride], xi = im[off + j * stride];
+        sr += xr * c - xi * s;
+        si += xr * s + xi * c;
+      }
+      r[k] = sr;
+      i[k] = si;
+    }
+    for (int k = 0; k < n; ++k) {
+      re[off + k * stride] = r[k];
+      im[off + k * stride] = i[k];
+    }
+    return;
+  }
   std::vector<double> r(n), i(n);
   for (int k = 0; k < n; ++k) {
     r[k] = re[off + k * stride];
@@ -1947,8 +1977,8 @@ int create_handle(const ptyb_scan* scan, const double* object, int32_t nobj, int
       g_create_error = "slice gaps must be finite";
       return PTYB_INVALID;
     }
-  if (scan->nx != N || !(N == 64 || N == 128 || N == 256)) {
-    g_create_error = "frames must be square with a side of 64, 128 or 256";
+  if (scan->nx != N || !(N == 64 || N == 96 || N == 128 || N == 192 || N == 256)) {
+    g_create_error = "frames must be square with a side of 64, 96, 128, 192 or 256";
     return PTYB_INVALID;
   }
   if (scan->nframe <= 0 || nprobe <= 0 || nprobe > kMaxModes || nobj != 1 || nyo < N || nxo < N) {

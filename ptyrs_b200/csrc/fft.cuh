@@ -1,4 +1,4 @@
-// Shared-memory line FFTs of length N = N1·N2 (N1, N2 ∈ {8, 16}) for sm_100a.
+// Shared-memory line FFTs of length N = N1·N2 (N1 ∈ {8, 16, 24}, N2 ∈ {4, 8, 16}) for sm_100a.
 //
 // A line lives in shared memory, N contiguous float2. G = N2 threads of one warp transform it
 // in place: each thread runs an N1-point DFT in registers over a stride-N2 decimation of the
@@ -67,19 +67,80 @@ PTYB_D void dft_stages(float2 (&x)[R]) {
   }
 }
 
-// In-register DFT of R = 2, 4, 8 or 16 points: x[k] ← Σ_n x[n]·e^{DIR·2πi·nk/R}.
+// cos(2π·t/24) for t = 0..23.
+PTYB_HD constexpr float cos24(int t) {
+  switch (((t % 24) + 24) % 24) {
+    case 0: return 1.0f;
+    case 1: case 23: return 0.96592582628906829f;
+    case 2: case 22: return 0.86602540378443865f;
+    case 3: case 21: return 0.70710678118654752f;
+    case 4: case 20: return 0.5f;
+    case 5: case 19: return 0.25881904510252076f;
+    case 6: case 18: return 0.0f;
+    case 7: case 17: return -0.25881904510252076f;
+    case 8: case 16: return -0.5f;
+    case 9: case 15: return -0.70710678118654752f;
+    case 10: case 14: return -0.86602540378443865f;
+    case 11: case 13: return -0.96592582628906829f;
+    default: return -1.0f;
+  }
+}
+
+// x · e^{DIR·2πi·t/24} (t compile-time after unrolling).
+template <int DIR>
+PTYB_D float2 rotate24(float2 x, int t) {
+  if (t % 24 == 0) return x;
+  const float c = cos24(t);
+  const float s = DIR * cos24(t - 6);  // DIR·sin(2πt/24)
+  return make_float2(x.x * c - x.y * s, x.x * s + x.y * c);
+}
+
+template <int R, int DIR>
+PTYB_D void dft(float2 (&x)[R]);
+
+// In-register DFT of 24 points as 3 × 8: with n = 3a + b and k = c + 8d,
+// X[c + 8d] = Σ_b e^{DIR·2πi·bd/3}·(e^{DIR·2πi·bc/24}·Σ_a x[3a + b]·e^{DIR·2πi·ac/8}):
+// three 8-point DFTs, the twiddles, then eight 3-point butterflies.
+template <int DIR>
+PTYB_D void dft24(float2 (&x)[24]) {
+  float2 y[3][8];
+#pragma unroll
+  for (int b = 0; b < 3; ++b) {
+#pragma unroll
+    for (int a = 0; a < 8; ++a) y[b][a] = x[3 * a + b];
+    dft<8, DIR>(y[b]);
+#pragma unroll
+    for (int c = 1; c < 8; ++c) y[b][c] = rotate24<DIR>(y[b][c], b * c);
+  }
+  constexpr float h3 = 0.86602540378443865f;  // sin(2π/3)
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const float2 s = cadd(y[1][c], y[2][c]), d = csub(y[1][c], y[2][c]);
+    const float2 t = make_float2(y[0][c].x - 0.5f * s.x, y[0][c].y - 0.5f * s.y);
+    const float2 u = make_float2(-DIR * h3 * d.y, DIR * h3 * d.x);  // DIR·i·sin(2π/3)·d
+    x[c] = cadd(y[0][c], s);
+    x[c + 8] = cadd(t, u);
+    x[c + 16] = csub(t, u);
+  }
+}
+
+// In-register DFT of R = 2, 4, 8, 16 or 24 points: x[k] ← Σ_n x[n]·e^{DIR·2πi·nk/R}.
 template <int R, int DIR>
 PTYB_D void dft(float2 (&x)[R]) {
+  if constexpr (R == 24) {
+    dft24<DIR>(x);
+  } else {
 #pragma unroll
-  for (int i = 0; i < R; ++i) {
-    const int j = bitrev<R>(i);
-    if (i < j) {
-      float2 t = x[i];
-      x[i] = x[j];
-      x[j] = t;
+    for (int i = 0; i < R; ++i) {
+      const int j = bitrev<R>(i);
+      if (i < j) {
+        float2 t = x[i];
+        x[i] = x[j];
+        x[j] = t;
+      }
     }
+    dft_stages<R, DIR, 1>(x);
   }
-  dft_stages<R, DIR, 1>(x);
 }
 
 template <int N>
@@ -96,6 +157,14 @@ template <>
 struct LineShape<256> {
   static constexpr int N1 = 16, N2 = 16;
 };
+template <>
+struct LineShape<96> {
+  static constexpr int N1 = 24, N2 = 4;
+};
+template <>
+struct LineShape<192> {
+  static constexpr int N1 = 24, N2 = 8;
+};
 
 // Bank swizzle of a shared-memory line: element e of line `l` sits at l·N + (e ^ swz(l)).
 // Consecutive lines differ in bit 3 and any 16 consecutive lines take 16 distinct values, so
@@ -110,7 +179,7 @@ struct LineTwiddles {
   float2 w[LineShape<N>::N1];
   PTYB_D void load(const float2* tw, int t) {
 #pragma unroll
-    for (int k1 = 1; k1 < LineShape<N>::N1; ++k1) w[k1] = tw[(t * k1) & (N - 1)];
+    for (int k1 = 1; k1 < LineShape<N>::N1; ++k1) w[k1] = tw[(t * k1) % N];
   }
 };
 

@@ -88,11 +88,11 @@ struct FrameShape {
   static constexpr int E = H * N / T;       // = 16
 };
 
-// Resident CTAs per SM the per-frame kernels are compiled for: two at 256 threads or fewer
-// (a cap of 128 registers), one above.
+// Resident CTAs per SM the per-frame kernels are compiled for: two at 384 threads or fewer
+// (a cap of 128 registers at 256 threads, 113 at the 288 of sides 96 and 192), one above.
 template <int N, int C>
 __host__ __device__ constexpr int frame_min_blocks() {
-  return FrameShape<N, C>::T <= 256 ? 2 : 1;
+  return FrameShape<N, C>::T <= 384 ? 2 : 1;
 }
 
 template <int N, int C>
@@ -263,7 +263,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
 #pragma unroll 2
     for (int idx = tid; idx < H * N; idx += T) {
       const int yl = idx / N, jx = idx % N;
-      const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
+      const int ny = (r * H + yl + N / 2) % N, nx = (jx + N / 2) % N;
       const float2 q = a.quad[ny * N + nx];
       for (int om = 0; om < a.nobj; ++om) {
         const float2 o = a.object[((size_t)om * a.nyo + corner.x + ny) * a.nxo + corner.y + nx];
@@ -440,7 +440,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
 #pragma unroll 2
     for (int idx = tid; idx < H * N; idx += T) {
       const int yl = idx / N, jx = idx % N;
-      const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
+      const int ny = (r * H + yl + N / 2) % N, nx = (jx + N / 2) % N;
       float2 q = make_float2(0.f, 0.f);
       if (subtract) q = a.quad[ny * N + nx];
       for (int om = 0; om < a.nobj; ++om) {
@@ -464,7 +464,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
 #pragma unroll 2
     for (int idx = tid; idx < H * N; idx += T) {
       const int yl = idx / N, jx = idx % N;
-      const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
+      const int ny = (r * H + yl + N / 2) % N, nx = (jx + N / 2) % N;
       const int pix = ny * N + nx;
       float2 oq = make_float2(0.f, 0.f);
       if (a.c_refl != 0.f)

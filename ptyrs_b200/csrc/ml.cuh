@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T, 2) gamma_kernel(GammaArgs
 #pragma unroll 4
     for (int idx = tid; idx < H * N; idx += T) {
       const int yl = idx / N, jx = idx % N;
-      const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
+      const int ny = (r * H + yl + N / 2) % N, nx = (jx + N / 2) % N;
       const size_t pi = (size_t)slot * a.probe_stride + ((size_t)pm * N + ny) * N + nx;
       const size_t oi = ((size_t)om * a.nyo + corner.x + ny) * a.nxo + corner.y + nx;
       const float2 dp = a.d_probe[pi], dob = a.d_obj[oi], q = a.quad[ny * N + nx];

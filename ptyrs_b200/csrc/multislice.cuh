@@ -39,7 +39,7 @@ PTYB_D void apply_window(float2* S, const SliceArgs& a, int s, int2 corner, int 
 #pragma unroll 2
   for (int idx = threadIdx.x; idx < H * N; idx += T) {
     const int yl = idx / N, jx = idx % N;
-    const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
+    const int ny = (r * H + yl + N / 2) % N, nx = (jx + N / 2) % N;
     float2 w = obj[(size_t)(corner.x + ny) * a.f.nxo + corner.y + nx];
     if (last) w = cmul(w, a.f.quad[ny * N + nx]);
     if (conj_mode) w = cconj(w);
@@ -87,7 +87,7 @@ PTYB_D void rows_io(float2* S, float2* dst, int r, int K, bool store) {
 #pragma unroll 2
   for (int idx = threadIdx.x; idx < H * N; idx += T) {
     const int yl = idx / N, jx = idx % N;
-    const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
+    const int ny = (r * H + yl + N / 2) % N, nx = (jx + N / 2) % N;
     for (int m = 0; m < K; ++m) {
       const int line = m * H + yl;
       float2& v = S[line * L + (jx ^ swz(line))];
@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T, frame_min_blocks<N, C>())
 #pragma unroll 2
     for (int idx = tid; idx < H * N; idx += T) {
       const int yl = idx / N, jx = idx % N;
-      const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
+      const int ny = (r * H + yl + N / 2) % N, nx = (jx + N / 2) % N;
       for (int m = 0; m < K; ++m) {
         const int line = m * H + yl;
         S[line * L + (jx ^ swz(line))] = a.probe[((size_t)m * N + ny) * N + nx];
@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T, frame_min_blocks<N, C>())
 #pragma unroll 2
   for (int idx = tid; idx < (MODE == kSliceGrad ? 0 : H * N); idx += T) {
     const int yl = idx / N, jx = idx % N;
-    const int ny = (r * H + yl + N / 2) & (N - 1), nx = (jx + N / 2) & (N - 1);
+    const int ny = (r * H + yl + N / 2) % N, nx = (jx + N / 2) % N;
     const float2 oq =
         cmul(obj_last[(size_t)(corner.x + ny) * a.nxo + corner.y + nx], a.quad[ny * N + nx]);
     for (int m = 0; m < K; ++m) {

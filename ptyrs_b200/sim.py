@@ -178,7 +178,7 @@ def multislice_counts_gpu(slices, probe, corner, gaps, wavelength, pixel, photon
     return counts.cpu().numpy()
 
 
-def make_batch(count=32, seed=0, scale=1.0, sides=(64, 128, 256)):
+def make_batch(count=32, seed=0, scale=1.0, sides=(64, 96, 128, 192, 256)):
     """`count` independent seeded scans of uneven sizes (the batched configuration, on the frame
     sides the engine has kernels for): per scan a side drawn from `sides`, an object 4–8 times
     the side, 500–5000 Fermat positions (times `scale`) at a step that keeps the scan inside the

@@ -11,7 +11,7 @@ from .engine import GpuPtycho, PtybError
 
 def clusters_for(n):
     """The cluster sizes the engine has kernels for at frame side `n` (0 lets it choose)."""
-    return {64: [1], 128: [2, 4], 256: [16, 8]}.get(n, [0])
+    return {64: [1], 96: [2], 128: [2, 4], 192: [8], 256: [16, 8]}.get(n, [0])
 
 
 def autotune(scan, obj, probe, run, prepare=None, stacks=(256, 512, 1024), clusters=None,
