@@ -8,6 +8,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <exception>
 #include <mutex>
 #include <set>
 #include <thread>
@@ -1897,6 +1898,11 @@ int guarded(ptyb_handle* h, bool enqueues, F&& body) {
     return body();
   } catch (const Fail& f) {
     return f.code;
+  } catch (const std::exception& ex) {
+    // a host failure (out of host memory and the like) must not cross the C ABI
+    h->err = std::string("host: ") + ex.what();
+    if (enqueues) h->aborted = true;
+    return PTYB_GPU;
   }
 }
 
