@@ -2160,13 +2160,26 @@ extern "C" {
 int ptyb_create(const ptyb_scan* scan, const double* object, int32_t nobj, int32_t nyo,
                 int32_t nxo, const double* probe, int32_t nprobe, const ptyb_options* options,
                 ptyb_handle** out) {
-  return create_handle(scan, object, nobj, 1, nullptr, nyo, nxo, probe, nprobe, options, out);
+  try {
+    return create_handle(scan, object, nobj, 1, nullptr, nyo, nxo, probe, nprobe, options, out);
+  } catch (const std::exception& ex) {
+    // host failures (out of host memory and the like) stop here, as a status and message
+    g_create_error = std::string("host: ") + ex.what();
+    if (out) *out = nullptr;
+    return PTYB_GPU;
+  }
 }
 
 int ptyb_create_slices(const ptyb_scan* scan, const double* objects, int32_t nslice,
                        const double* gaps, int32_t nyo, int32_t nxo, const double* probe,
                        int32_t nprobe, const ptyb_options* options, ptyb_handle** out) {
-  return create_handle(scan, objects, 1, nslice, gaps, nyo, nxo, probe, nprobe, options, out);
+  try {
+    return create_handle(scan, objects, 1, nslice, gaps, nyo, nxo, probe, nprobe, options, out);
+  } catch (const std::exception& ex) {
+    g_create_error = std::string("host: ") + ex.what();
+    if (out) *out = nullptr;
+    return PTYB_GPU;
+  }
 }
 
 int ptyb_nslice(const ptyb_handle* h) { return h ? h->nslice : 0; }
@@ -2458,7 +2471,9 @@ int ptyb_raar(ptyb_handle* h, const ptyb_raar_params* p, int32_t ncycle) {
                         p->zero_phase_ramp != 0, ncycle);
 }
 
-int ptyb_batch_run(ptyb_handle* const* handles, int32_t n, const ptyb_rpie_params* rpie,
+namespace {
+
+int batch_run_impl(ptyb_handle* const* handles, int32_t n, const ptyb_rpie_params* rpie,
                    int32_t rpie_epochs, const ptyb_lsqml_params* lsqml, int32_t lsqml_epochs,
                    int32_t calc_llk, int32_t* status, float* device_ms) {
   if (device_ms) *device_ms = -1.f;
@@ -2485,13 +2500,19 @@ int ptyb_batch_run(ptyb_handle* const* handles, int32_t n, const ptyb_rpie_param
   {
     std::vector<std::thread> workers;
     workers.reserve(n);
-    for (int i = 0; i < n; ++i)
-      workers.emplace_back([&, i] {
-        int r = rpie_epochs > 0 ? ptyb_rpie(handles[i], rpie, rpie_epochs) : PTYB_OK;
-        if (r == PTYB_OK && lsqml_epochs > 0)
-          r = ptyb_lsqml(handles[i], lsqml, lsqml_epochs, calc_llk);
-        rc[i] = r;
-      });
+    try {
+      for (int i = 0; i < n; ++i)
+        workers.emplace_back([&, i] {
+          int r = rpie_epochs > 0 ? ptyb_rpie(handles[i], rpie, rpie_epochs) : PTYB_OK;
+          if (r == PTYB_OK && lsqml_epochs > 0)
+            r = ptyb_lsqml(handles[i], lsqml, lsqml_epochs, calc_llk);
+          rc[i] = r;
+        });
+    } catch (...) {
+      // no thread for the rest: the started ones finish before the failure goes up
+      for (auto& w : workers) w.join();
+      throw;
+    }
     for (auto& w : workers) w.join();
   }
   if (timing) {
@@ -2519,6 +2540,20 @@ int ptyb_batch_run(ptyb_handle* const* handles, int32_t n, const ptyb_rpie_param
     if (first == PTYB_OK && rc[i] != PTYB_OK) first = rc[i];
   }
   return first;
+}
+
+}  // namespace
+
+int ptyb_batch_run(ptyb_handle* const* handles, int32_t n, const ptyb_rpie_params* rpie,
+                   int32_t rpie_epochs, const ptyb_lsqml_params* lsqml, int32_t lsqml_epochs,
+                   int32_t calc_llk, int32_t* status, float* device_ms) {
+  try {
+    return batch_run_impl(handles, n, rpie, rpie_epochs, lsqml, lsqml_epochs, calc_llk, status,
+                          device_ms);
+  } catch (const std::exception&) {
+    // a host failure (no thread or host memory for the batch): nothing is reported per handle
+    return PTYB_GPU;
+  }
 }
 
 int ptyb_get_llk(ptyb_handle* h, ptyb_llk* out) {
