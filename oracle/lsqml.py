@@ -1,7 +1,7 @@
 """pty-chi LSQML in float64 (oracle restatement, test infrastructure only).
 
-Follows physwkim/ptyrs `ptyrs/src/engine/lsqml.rs` without probe variation
-(`ProbeVariation::none`), with the position feature under Patch sampling and pty-chi's
+Follows physwkim/ptyrs `ptyrs/src/engine/lsqml.rs`, with or without OPR probe variation
+(`ProbeVariation`, oracle/opr.py), with the position feature under Patch sampling and pty-chi's
 multislice object (`SliceWaves`, engine/multislice.rs:87-438): `LsqmlBatch::new` (lsqml.rs:102-179),
 `obj_directions`, `frame_probe_directions`, `probe_direction` (lsqml.rs:194-229),
 `step_sizes` (lsqml.rs:286-350), `trim_mean` (lsqml.rs:392-398), `Lsqml::step`
@@ -101,7 +101,8 @@ def multislice_grads(addr, obs, optics, objs, probe):
 class Lsqml:
     """LSQML state across epochs (engine/lsqml.rs:415-430). cost: "poisson" or "amplitude"."""
 
-    def __init__(self, batch_size, cost="poisson", seed=7, offsets=None, refine=False):
+    def __init__(self, batch_size, cost="poisson", seed=7, offsets=None, refine=False,
+                 var=None):
         if batch_size == 0:
             raise ValueError("LSQML batch_size must be >= 1")
         self.batch_size, self.cost, self.seed = batch_size, cost, seed
@@ -111,16 +112,20 @@ class Lsqml:
         # Features::position under Patch sampling: per-frame offsets [P, 2] in object pixels
         self.offsets = None if offsets is None else np.array(offsets, np.float64)
         self.refine = refine
+        # ProbeVariation (oracle/opr.py): OPR of probe mode 0, or None for the shared probe
+        self.var = var
 
     def frame_probes(self, frames, probe, quad):
         """`ProbeVariation::unique` planes moved by each frame's offset (engine/lsqml.rs:
         474-499): `[len(frames)·nprobe, ny, nx]`."""
-        planes = np.concatenate([probe] * len(frames))
+        planes = (self.var.planes(frames, probe) if self.var is not None
+                  else np.concatenate([probe] * len(frames)))
         if self.offsets is None:
             return planes
         np_ = probe.shape[0]
         for b, f in enumerate(frames):
-            planes[b * np_:(b + 1) * np_] = ops.move_planes(probe, quad, self.offsets[f])
+            planes[b * np_:(b + 1) * np_] = ops.move_planes(planes[b * np_:(b + 1) * np_], quad,
+                                                            self.offsets[f])
         return planes
 
     @staticmethod
@@ -187,9 +192,10 @@ class Lsqml:
         nb = len(frames)
         d_obj = [waves.obj_adjoint(s, chis[s]) / np.sqrt(pre * pre + floor)
                  for s in range(len(objs))]
-        # frame_probe_directions on slice 0, moved back by −offset
-        d, _ = ops.accumulate_probe(uviews, objs[0], (nb * np_, ny, nx), waves.shared(0),
-                                    chis[0])
+        # frame_probe_directions on slice 0 (and |V_b|²), moved back by −offset
+        d_raw, vv = ops.accumulate_probe(uviews, objs[0], (nb * np_, ny, nx), waves.shared(0),
+                                         chis[0])
+        d = d_raw.copy()
         if self.offsets is not None:
             for b, f in enumerate(frames):
                 d[b * np_:(b + 1) * np_] = ops.move_planes(d[b * np_:(b + 1) * np_],
@@ -207,6 +213,10 @@ class Lsqml:
             d_pos = self.position_directions(frames, nmode, optics, objs, waves, chis, uviews)
         for f, a in zip(frames, a_far):
             self.a_far_all[f] = a
+        if self.var is not None:
+            # the eigenmodes and refined weights from the state on entry (engine/lsqml.rs:
+            # 620-621)
+            self.var.step(frames, probe[0], d, d_raw, vv, np_)
         new_objs = [o + trim_mean(a) * dd for o, a, dd in zip(objs, a_obj, d_obj)]
         sp = sum(a_probe) / len(a_probe)
         new_probe = probe + sp * d_probe

@@ -13,7 +13,8 @@ scenario `dm_scenario(32, 40, nprobe, 2e5, 4.0)` (`tests/common/engine/scenario.
 counts `oracle/scenario.py` redraws: the position gradient (`pos_grad*`), ML with positions
 (`ml_pos_*`), LSQML steps and epochs with and without positions (`lsqml_*`), rPIE against
 pty-chi (`rpie_ptychi_f64.txt`) and with positions under PATCH (`rpie_pos_*`), DM and RAAR
-against PyNX (`dm_pynx_f64.txt`, `raar_pynx_f64.txt`). Each text table becomes one float64 array of the same rows and
+against PyNX (`dm_pynx_f64.txt`, `raar_pynx_f64.txt`), and OPR probe variation alone and inside
+an LSQML step (`opr_*`, `lsqml_opr_*`, `lsqml_opr_int_*`). Each text table becomes one float64 array of the same rows and
 columns under its stem (`table` for a file without one) in `<group>.npz`.
 
     python tests/golden/make_golden.py [REFERENCE_ROOT]
@@ -48,6 +49,9 @@ GROUPS = {
     "rpie_ptychi": [""],
     "dm_pynx": [""],
     "raar_pynx": [""],
+    "opr": ["eigen", "weights", "values"],
+    "lsqml_opr": ["eigen", "weights", "values", "steps", "obj", "probe"],
+    "lsqml_opr_int": ["eigen", "weights", "values", "steps", "obj", "probe"],
     "rpie_pos_step": ["obj", "probe", "offsets"],
     "rpie_pos_epochs": ["obj", "probe", "offsets"],
 }
