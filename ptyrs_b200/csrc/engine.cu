@@ -184,6 +184,7 @@ struct ptyb_handle {
   float* partial_den = nullptr;   // [max_den_chunks][N][N]
   int max_den_chunks = 0;
   float* probe_norm = nullptr;    // [N][N]
+  float* blend_norm = nullptr;    // [nyo][nxo] the object blend's norm
   // Their probe step under the position model: the residual's back-projection g, the step,
   // g's spectrum summed over frames with its compensation, each frame's ‖A·step‖² per mode
   // and the modes' slope and regulariser sums.
@@ -1622,6 +1623,7 @@ void ensure_carry(ptyb_handle* h, bool iterate) {
   if (!h->carry) h->carry = alloc<float2>(h, n);
   if (iterate && !h->carry_it) h->carry_it = alloc<float2>(h, n);
   if (!h->probe_norm) h->probe_norm = alloc<float>(h, (size_t)h->N * h->N);
+  if (!h->blend_norm) h->blend_norm = alloc<float>(h, (size_t)h->nyo * h->nxo);
 }
 
 // The frame kernel's carry mode over every frame, stack by stack: the carried waves become
@@ -1652,7 +1654,8 @@ void carry_pass(ptyb_handle* h, float c_po, float c_psi, float c_it, float c_ref
 }
 
 // psi_to_obj_probe's object blend from the carried waves and the current probe
-// (engine/ops.rs:352-381): the norm's maximum over the object, then the blend.
+// (engine/ops.rs:352-381): one tile-owned pass writes the numerator and the norm and takes the
+// norm's maximum, then the blend runs per pixel.
 void object_blend(ptyb_handle* h, double inertia, const float2* waves = nullptr) {
   GatherArgs g = gather_args(h, h->iota, h->P);
   g.upd = h->carry;
@@ -1662,11 +1665,16 @@ void object_blend(ptyb_handle* h, double inertia, const float2* waves = nullptr)
     g.probe_stride = h->K * h->N * h->N;
   }
   g.pmax = h->scal + kScalObjNorm;
-  g.step = (float)inertia;
+  g.out = h->d_obj;
+  g.pre = h->blend_norm;
   check(h, cudaMemsetAsync(g.pmax, 0, sizeof(float), h->stream), "memset");
-  timed(h, kKObjOverlap, [&] { object_tile_kernel<kGatherOverlap><<<ntiles(h), 1024, 0, h->stream>>>(g); }, h->P);
-  launched(h, "object norm max");
   timed(h, kKObjBlend, [&] { object_tile_kernel<kGatherBlend><<<ntiles(h), 1024, 0, h->stream>>>(g); }, h->P);
+  launched(h, "object blend sums");
+  const size_t no = (size_t)h->nyo * h->nxo;
+  timed(h, kKAxpy, [&] {
+    blend_apply_kernel<<<(unsigned)((no + 255) / 256), 256, 0, h->stream>>>(
+        h->object, h->d_obj, h->blend_norm, g.pmax, (float)inertia, no);
+  });
   launched(h, "object blend");
 }
 

@@ -23,7 +23,7 @@ enum GatherMode : int {
   kGatherMl = 2,     // grad += Σ conj(q·P)·g (compensated across launches)
   kGatherOverlap = 3,  // pmax = max over pixels of Σ_m D_m
   kGatherIllum = 4,    // pre = (pre + I)/2 with I = Σ|P|² over every view
-  kGatherBlend = 5,    // O = (num + reg·O) / max(norm + reg, 1e-12), reg = inertia·max norm
+  kGatherBlend = 5,    // the object blend's sums: out = num, pre = norm, pmax = max norm
 };
 
 struct GatherArgs {
@@ -38,7 +38,7 @@ struct GatherArgs {
   const float* pre_max;    // LSQML: max of pre (device scalar)
   float2* out;             // LSQML d_obj / ML gradient sum [nyo][nxo]
   float2* comp;            // ML gradient compensation [nyo][nxo]
-  float alpha, step, pre_scale;  // kGatherBlend: step = inertia, pmax = max of the norm
+  float alpha, step, pre_scale;
   int nslot, nyo, nxo, nprobe, N;
   int probe_stride;        // elements between slots' probes (0: the shared probe)
 };
@@ -176,11 +176,16 @@ __global__ void __launch_bounds__(1024, MODE == kGatherRpie || MODE == kGatherBl
     }
   }
   const size_t o = (size_t)y * a.nxo + x;
-  if (MODE == kGatherOverlap) {
+  if (MODE == kGatherOverlap || MODE == kGatherBlend) {
     float d = 0.f;
 #pragma unroll
     for (int m = 0; m < kMaxModes; ++m)
       if (m < K) d += den[m].s;
+    if (MODE == kGatherBlend && inside && grp == 0) {
+      // psi_to_obj_probe's object sums (engine/ops.rs:352-369), every pixel, covered or not
+      a.out[o] = num[0].value();
+      a.pre[o] = d;
+    }
     d = warp_max(inside && grp == 0 ? d : 0.f);
     if (threadIdx.x % 32 == 0) red[threadIdx.x / 32] = d;
     __syncthreads();
@@ -217,15 +222,6 @@ __global__ void __launch_bounds__(1024, MODE == kGatherRpie || MODE == kGatherBl
     cc = make_float2((tr - g.x) - yr, (ti - g.y) - yi);
     a.out[o] = make_float2(tr, ti);
     a.comp[o] = cc;
-  } else if (MODE == kGatherBlend) {
-    // psi_to_obj_probe's object blend (engine/ops.rs:352-381) over every pixel, covered or not
-    float d = 0.f;
-#pragma unroll
-    for (int m = 0; m < kMaxModes; ++m)
-      if (m < K) d += den[m].s;
-    const float reg = a.step * (*a.pmax);
-    const float2 v = cadd(num[0].value(), cscale(a.object[o], reg));
-    a.object[o] = cscale(v, 1.f / fmaxf(d + reg, 1e-12f));
   } else if (MODE == kGatherIllum) {
     float d = 0.f;
 #pragma unroll
@@ -294,6 +290,16 @@ __global__ void __launch_bounds__(256) probe_partial_kernel(ProbeArgs a) {
       if (m < a.K) a.partial[((size_t)blockIdx.y * a.K + m) * plane + pix] = acc[m].value();
   }
   if (a.mode >= 2) a.partial_den[(size_t)blockIdx.y * plane + pix] = den.s - den.c;
+}
+
+// The object blend of AP / DM / RAAR (engine/ops.rs:371-381) from the sums kGatherBlend wrote:
+// O = (num + reg·O) / max(norm + reg, 1e-12) with reg = inertia·max norm.
+__global__ void blend_apply_kernel(float2* object, const float2* num, const float* norm,
+                                   const float* norm_max, float inertia, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float reg = inertia * (*norm_max);
+  object[i] = cscale(cadd(num[i], cscale(object[i], reg)), 1.f / fmaxf(norm[i] + reg, 1e-12f));
 }
 
 // The probe step of AP / DM / RAAR under the move (engine/features.rs:673-712), one block per
