@@ -194,6 +194,19 @@ int ptyb_batch_run(ptyb_handle* const* handles, int32_t n, const ptyb_rpie_param
                    int32_t rpie_epochs, const ptyb_lsqml_params* lsqml, int32_t lsqml_epochs,
                    int32_t calc_llk, int32_t* status, float* device_ms);
 
+/* Reference `ProbeVariation` (engine/opr.rs:17-88) for the LSQML calls that follow (the
+ * reference passes it to `GpuPtycho::lsqml`, engine/gpu/lsqml.rs:75-121): pty-chi's OPR of
+ * probe mode 0 with k eigenmodes, complex128 [k][ny][nx], weights [nframe][k] and, when not
+ * NULL, the main mode's weights [nframe]; each moves with the LSQML steps when its refine flag
+ * is set. k = 0 returns to the shared probe. Single slice, without the position model
+ * (PTYB_INVALID otherwise). */
+int ptyb_set_probe_variation(ptyb_handle* h, const double* eigenmodes, int32_t k,
+                             const double* weights, int32_t refine_weights,
+                             const double* intensity, int32_t refine_intensity);
+/* The variation's eigenmodes, weights and main-mode weights (when modelled); NULL skips one. */
+int ptyb_get_probe_variation(ptyb_handle* h, double* eigenmodes, double* weights,
+                             double* intensity);
+
 /* Reference `GpuPtycho::llk` (engine/gpu/mod.rs:871-881): normalised LLK of the estimate. */
 int ptyb_get_llk(ptyb_handle* h, ptyb_llk* out);
 

@@ -82,6 +82,9 @@ SIGNATURES = {
     "ptyb_ap": (c_int32, [c_void_p, P(ApParams), c_int32]),
     "ptyb_dm": (c_int32, [c_void_p, P(DmParams), c_int32]),
     "ptyb_raar": (c_int32, [c_void_p, P(RaarParams), c_int32]),
+    "ptyb_set_probe_variation": (c_int32, [c_void_p, P(c_double), c_int32, P(c_double), c_int32,
+                                           P(c_double), c_int32]),
+    "ptyb_get_probe_variation": (c_int32, [c_void_p, P(c_double), P(c_double), P(c_double)]),
     "ptyb_batch_run": (c_int32, [P(c_void_p), c_int32, P(RpieParams), c_int32, P(LsqmlParams),
                                  c_int32, c_int32, P(c_int32), P(ctypes.c_float)]),
     "ptyb_get_llk": (c_int32, [c_void_p, P(Llk)]),

@@ -22,6 +22,7 @@
 #include "ml.cuh"
 #include "position.cuh"
 #include "multislice.cuh"
+#include "opr.cuh"
 #include "scan.h"
 
 using namespace ptyb;
@@ -185,6 +186,20 @@ struct ptyb_handle {
   int max_den_chunks = 0;
   float* probe_norm = nullptr;    // [N][N]
   float* blend_norm = nullptr;    // [nyo][nxo] the object blend's norm
+  // OPR probe variation of LSQML (engine/opr.rs): k eigenmodes, the weights [P][k] and, when
+  // modelled, the main mode's weights [P]; scratch for a batch's step.
+  int opr_k = 0;
+  int opr_slots = 0;             // slots the batch scratch below holds
+  bool opr_on = false, opr_refine_w = true, opr_has_c = false, opr_refine_c = true;
+  float2* opr_u = nullptr;       // [k][N][N]
+  double* opr_w = nullptr;       // [P][k]
+  double* opr_c = nullptr;       // [P]
+  float* opr_vv = nullptr;       // [slots][N][N]
+  float2* opr_r = nullptr;       // [slots][N][N]
+  float2* opr_e = nullptr;       // [N][N]
+  double* opr_sums = nullptr;    // [slots][3]
+  double* opr_p = nullptr;       // [slots]
+  double* opr_scal = nullptr;    // [4]
   // Their probe step under the position model: the residual's back-projection g, the step,
   // g's spectrum summed over frames with its compensation, each frame's ‖A·step‖² per mode
   // and the modes' slope and regulariser sums.
@@ -742,14 +757,13 @@ ptyb_llk llk_pass(ptyb_handle* h, const float2* waves = nullptr) {
       ++h->launches;
       continue;
     }
-    if (h->have_offsets) {
-      // each frame's own moved probe (engine/lsqml.rs:537-551)
-      if (waves) {
-        a.probe = waves + s0 * pstride;
-      } else {
-        move_frames(h, h->iota + s0, n, h->spec, h->wave);
-        a.probe = h->wave;
-      }
+    if (waves) {
+      // each frame's own (moved or varied) probe (engine/lsqml.rs:537-551)
+      a.probe = waves + s0 * pstride;
+      a.probe_stride = (int)pstride;
+    } else if (h->have_offsets) {
+      move_frames(h, h->iota + s0, n, h->spec, h->wave);
+      a.probe = h->wave;
       a.probe_stride = (int)pstride;
     }
     check(h, launch_frame<kLlk>(h, a, n), "llk pass");
@@ -1002,11 +1016,130 @@ void lsqml_batch_slices(ptyb_handle* h, const ptyb_lsqml_params& p, const int* f
 // One LSQML step on a batch (engine/lsqml.rs:581-643), with the position model when offsets
 // are set: each frame's probe moved by its offset, the probe directions moved back before
 // their frame mean, and with refinement pty-chi's position step after the update.
+// The probe variation's batch scratch for h->slots frames and the planes of every frame.
+void ensure_opr(ptyb_handle* h) {
+  const size_t plane = (size_t)h->N * h->N;
+  if (h->opr_slots < h->slots) {
+    h->opr_vv = alloc<float>(h, (size_t)h->slots * plane);
+    h->opr_r = alloc<float2>(h, (size_t)h->slots * plane);
+    h->opr_sums = alloc<double>(h, (size_t)h->slots * 3);
+    h->opr_p = alloc<double>(h, h->slots);
+    h->wave = alloc<float2>(h, (size_t)h->slots * h->K * plane);
+    h->opr_slots = h->slots;
+  }
+  if (!h->opr_e) {
+    h->opr_e = alloc<float2>(h, plane);
+    h->opr_scal = alloc<double>(h, 4);
+  }
+  if (!h->wave_all) h->wave_all = alloc<float2>(h, (size_t)h->P * h->K * plane);
+}
+
+// Every slot's own probe planes under the probe variation into `out` ([slot][K][N][N]).
+void opr_planes(ptyb_handle* h, const int* frames, int nslot, float2* out) {
+  const int plane = h->N * h->N;
+  timed(h, kKMisc, [&] {
+    opr_planes_kernel<<<dim3((plane + 255) / 256, nslot), 256, 0, h->stream>>>(
+        h->probe, h->opr_u, h->opr_w, h->opr_has_c ? h->opr_c : nullptr, frames, h->K, h->opr_k,
+        plane, out);
+  }, nslot);
+  launched(h, "opr planes");
+}
+
+// The OPR step of the batch (engine/opr.rs:122-224) from its frame probe directions, mode-0
+// plane of each slot of h->field, and the probe's mode 0 on entry.
+void opr_step(ptyb_handle* h, const int* frames, int count) {
+  const int plane = h->N * h->N, k = h->opr_k;
+  const size_t dstride = (size_t)h->K * plane;
+  const unsigned pb = (unsigned)((plane + 255) / 256);
+  timed(h, kKMisc, [&] {
+    window_power_kernel<<<dim3(pb, count), 256, 0, h->stream>>>(h->object, frames, h->corners,
+                                                               h->nxo, h->N, h->opr_vv);
+  }, count);
+  launched(h, "opr window power");
+  if (h->opr_has_c && h->opr_refine_c) {
+    timed(h, kKMisc, [&] {
+      opr_frame_sums_kernel<<<count, 256, 0, h->stream>>>(h->probe, h->field, dstride, h->opr_vv,
+                                                          plane, h->opr_sums);
+    });
+    launched(h, "opr intensity sums");
+    timed(h, kKMisc, [&] {
+      opr_intensity_kernel<<<(count + 255) / 256, 256, 0, h->stream>>>(h->opr_sums, frames, count,
+                                                                        h->opr_c);
+    });
+    launched(h, "opr intensity");
+  }
+  if (k == 0 || count < 2) return;
+  timed(h, kKMisc, [&] {
+    opr_residue_kernel<<<pb, 256, 0, h->stream>>>(h->field, dstride, count, plane, h->opr_r);
+  });
+  launched(h, "opr residues");
+  const double a_u = std::min(0.1, (double)count / h->P);
+  for (int i = 0; i < k; ++i) {
+    float2* u = h->opr_u + (size_t)i * plane;
+    timed(h, kKMisc, [&] {
+      opr_frame_sums_kernel<<<count, 256, 0, h->stream>>>(u, h->opr_r, plane, nullptr, plane,
+                                                          h->opr_sums);
+    });
+    launched(h, "opr dots");
+    timed(h, kKMisc, [&] {
+      opr_coef_kernel<<<1, 256, 0, h->stream>>>(h->opr_sums, h->opr_w, frames, k, i, count,
+                                                (double)plane, h->opr_p);
+    });
+    launched(h, "opr coefficients");
+    timed(h, kKMisc, [&] {
+      opr_e_kernel<<<pb, 256, 0, h->stream>>>(h->opr_r, h->opr_p, count, plane, h->opr_e);
+    });
+    launched(h, "opr e");
+    timed(h, kKMisc, [&] { opr_norm2_kernel<<<1, 1024, 0, h->stream>>>(h->opr_e, plane, h->opr_scal); });
+    launched(h, "opr norm");
+    timed(h, kKMisc, [&] {
+      opr_u_step_kernel<<<pb, 256, 0, h->stream>>>(u, h->opr_e, h->opr_scal, a_u, plane);
+    });
+    launched(h, "opr eigenmode step");
+    timed(h, kKMisc, [&] { opr_norm2_kernel<<<1, 1024, 0, h->stream>>>(u, plane, h->opr_scal + 1); });
+    launched(h, "opr norm");
+    timed(h, kKMisc, [&] { opr_u_scale_kernel<<<pb, 256, 0, h->stream>>>(u, h->opr_scal + 1, plane); });
+    launched(h, "opr eigenmode scale");
+    if (h->opr_refine_w) {
+      timed(h, kKMisc, [&] {
+        opr_frame_sums_kernel<<<count, 256, 0, h->stream>>>(u, h->field, dstride, h->opr_vv,
+                                                            plane, h->opr_sums);
+      });
+      launched(h, "opr weight sums");
+      timed(h, kKMisc, [&] {
+        opr_weights_kernel<<<1, 256, 0, h->stream>>>(h->opr_sums, frames, count, k, i, h->opr_w);
+      });
+      launched(h, "opr weights");
+    }
+    if (i + 1 < k) {
+      timed(h, kKMisc, [&] { opr_norm2_kernel<<<1, 1024, 0, h->stream>>>(u, plane, h->opr_scal + 2); });
+      launched(h, "opr norm");
+      timed(h, kKMisc, [&] {
+        opr_frame_sums_kernel<<<count, 256, 0, h->stream>>>(u, h->opr_r, plane, nullptr, plane,
+                                                            h->opr_sums);
+      });
+      launched(h, "opr projections");
+      timed(h, kKMisc, [&] {
+        opr_gs_kernel<<<pb, 256, 0, h->stream>>>(h->opr_r, u, h->opr_sums, h->opr_scal + 2, count,
+                                                 plane);
+      });
+      launched(h, "opr orthogonalisation");
+    }
+  }
+}
+
 void lsqml_batch(ptyb_handle* h, const ptyb_lsqml_params& p, const int* frames, int nslot,
                  double* log) {
   const int pstride = h->K * h->N * h->N;
   FrameArgs a = frame_args(h, frames);
   a.cost = p.cost;
+  const bool opr = h->opr_on;
+  if (opr) {
+    // every frame's own probe (engine/opr.rs:88-120) in place of the shared one
+    opr_planes(h, frames, nslot, h->wave);
+    a.probe = h->wave;
+    a.probe_stride = pstride;
+  }
   if (h->have_offsets) {
     ensure_spec(h);
     spectrum_of(h, h->probe, h->spec);
@@ -1036,13 +1169,25 @@ void lsqml_batch(ptyb_handle* h, const ptyb_lsqml_params& p, const int* frames, 
     ++h->launches;
   }
   GatherArgs g = gather_args(h, frames, nslot);
-  if (h->have_offsets) {
+  if (h->have_offsets || opr) {
     g.probe = h->wave;
     g.probe_stride = pstride;
   }
   timed(h, kKObjLsqml, [&] { object_tile_kernel<kGatherLsqml><<<ntiles(h), 1024, 0, h->stream>>>(g); }, nslot);
   launched(h, "object direction");
-  if (h->have_offsets) {
+  if (opr) {
+    // each frame's probe direction conj(q·O)·χ (the OPR step reads mode 0), their mean dP
+    timed(h, kKProbePartial, [&] {
+      probe_terms_kernel<<<dim3((h->N * h->N + 255) / 256, nslot), 256, 0, h->stream>>>(
+          h->object, h->quad, h->upd, frames, h->corners, h->nxo, h->K, h->N, h->field);
+    });
+    launched(h, "probe terms");
+    timed(h, kKProbeFinal, [&] {
+      probe_finalize_kernel<<<(pstride + 255) / 256, 256, 0, h->stream>>>(
+          h->field, nslot, pstride, h->probe, h->d_probe, nullptr, 1.0f / nslot, 1);
+    });
+    launched(h, "probe direction");
+  } else if (h->have_offsets) {
     timed(h, kKProbePartial, [&] {
       probe_terms_kernel<<<dim3((h->N * h->N + 255) / 256, nslot), 256, 0, h->stream>>>(
           h->object, h->quad, h->upd, frames, h->corners, h->nxo, h->K, h->N, h->field);
@@ -1059,8 +1204,8 @@ void lsqml_batch(ptyb_handle* h, const ptyb_lsqml_params& p, const int* frames, 
     probe_pass(h, frames, nslot, 1, 0.f, 1.0f / nslot);
   }
   const double lambda0 = 1.2e-7 * ((double)h->N * h->N) / ((double)h->N * h->N);
-  const float2* fprobe = h->have_offsets ? h->wave : h->probe;
-  const int fstride = h->have_offsets ? pstride : 0;
+  const float2* fprobe = h->have_offsets || opr ? h->wave : h->probe;
+  const int fstride = h->have_offsets || opr ? pstride : 0;
   timed(h, kKDots, [&] {
     lsqml_dots_kernel<<<nslot * kDotParts, 512, 0, h->stream>>>(h->object, h->d_obj, fprobe, h->d_probe,
                                                      h->quad, h->upd, frames, h->corners,
@@ -1084,6 +1229,8 @@ void lsqml_batch(ptyb_handle* h, const ptyb_lsqml_params& p, const int* frames, 
                                                    frames, h->afar_all, log, h->scal + 2, 3);
   });
   launched(h, "step solve");
+  // the eigenmodes and the refined weights from the state on entry (engine/lsqml.rs:620-621)
+  if (opr) opr_step(h, frames, nslot);
   const size_t no = (size_t)h->nyo * h->nxo, np = (size_t)h->K * h->N * h->N;
   timed(h, kKAxpy, [&] {
     axpy_scal_kernel<<<(unsigned)((no + 255) / 256), 256, 0, h->stream>>>(h->object, h->d_obj,
@@ -2247,6 +2394,7 @@ int ptyb_lsqml(ptyb_handle* h, const ptyb_lsqml_params* p, int32_t nepoch, int32
   return guarded(h, true, [&]() -> int {
     const int size = std::min(p->batch_size, h->P);
     ensure_slots(h, std::max(size, std::min(h->P, h->stack)));
+    if (h->opr_on) ensure_opr(h);
     std::vector<std::vector<int32_t>> sizes;
     std::vector<int32_t> last;
     // A fresh run: epochs from 0 (engine/gpu/lsqml.rs:97-105).
@@ -2268,7 +2416,18 @@ int ptyb_lsqml(ptyb_handle* h, const ptyb_lsqml_params* p, int32_t nepoch, int32
           lsqml_batch(h, *p, order + off, n, h->steplog + (size_t)off * stride);
         off += n;
       }
-      if (llk_due(calc_llk, ic, nepoch)) record(h, kAlgLsqml, llk_pass(h));
+      if (llk_due(calc_llk, ic, nepoch)) {
+        if (h->opr_on) {
+          // the LLK of every frame's own probe (engine/lsqml.rs:537-551)
+          const int stack = std::min(h->P, h->stack);
+          for (int s0 = 0; s0 < h->P; s0 += stack)
+            opr_planes(h, h->iota + s0, std::min(stack, h->P - s0),
+                       h->wave_all + (size_t)s0 * h->K * h->N * h->N);
+          record(h, kAlgLsqml, llk_pass(h, h->wave_all));
+        } else {
+          record(h, kAlgLsqml, llk_pass(h));
+        }
+      }
       ++h->cycle;
     }
     end_call(h, "lsqml");
@@ -2564,6 +2723,61 @@ int ptyb_batch_run(ptyb_handle* const* handles, int32_t n, const ptyb_rpie_param
   }
 }
 
+int ptyb_set_probe_variation(ptyb_handle* h, const double* eigenmodes, int32_t k,
+                             const double* weights, int32_t refine_weights,
+                             const double* intensity, int32_t refine_intensity) {
+  if (!h) return PTYB_INVALID;
+  if (k < 0 || (k > 0 && (!eigenmodes || !weights))) {
+    h->err = "probe variation: k >= 0 with eigenmodes and weights";
+    return PTYB_INVALID;
+  }
+  if (intensity && k == 0) {
+    h->err = "main-mode weights need an eigenmode";
+    return PTYB_INVALID;
+  }
+  if (h->nslice > 1 || h->have_offsets) {
+    h->err = "the probe variation runs on a single slice without the position model";
+    return PTYB_INVALID;
+  }
+  return guarded(h, true, [&]() -> int {
+    const size_t plane = (size_t)h->N * h->N;
+    h->opr_on = k > 0;
+    h->opr_k = k;
+    h->opr_has_c = intensity != nullptr;
+    h->opr_refine_w = refine_weights != 0;
+    h->opr_refine_c = refine_intensity != 0;
+    if (!h->opr_on) return PTYB_OK;
+    h->opr_u = alloc<float2>(h, (size_t)k * plane);
+    upload_c64(h, eigenmodes, h->opr_u, (size_t)k * plane, "eigenmodes");
+    h->opr_w = alloc<double>(h, (size_t)h->P * k);
+    check(h, copy_sync(h, h->opr_w, weights, (size_t)h->P * k * sizeof(double),
+                       cudaMemcpyHostToDevice), "weights");
+    if (intensity) {
+      h->opr_c = alloc<double>(h, h->P);
+      check(h, copy_sync(h, h->opr_c, intensity, (size_t)h->P * sizeof(double),
+                         cudaMemcpyHostToDevice), "intensity");
+    }
+    return PTYB_OK;
+  });
+}
+
+int ptyb_get_probe_variation(ptyb_handle* h, double* eigenmodes, double* weights,
+                             double* intensity) {
+  if (!h) return PTYB_INVALID;
+  return guarded(h, false, [&]() -> int {
+    const size_t plane = (size_t)h->N * h->N;
+    if (!h->opr_on) return PTYB_OK;
+    if (eigenmodes) download_c64(h, h->opr_u, eigenmodes, (size_t)h->opr_k * plane, "eigenmodes");
+    if (weights)
+      check(h, copy_sync(h, weights, h->opr_w, (size_t)h->P * h->opr_k * sizeof(double),
+                         cudaMemcpyDeviceToHost), "weights");
+    if (intensity && h->opr_has_c)
+      check(h, copy_sync(h, intensity, h->opr_c, (size_t)h->P * sizeof(double),
+                         cudaMemcpyDeviceToHost), "intensity");
+    return PTYB_OK;
+  });
+}
+
 int ptyb_get_llk(ptyb_handle* h, ptyb_llk* out) {
   if (!h || !out) return PTYB_INVALID;
   return guarded(h, true, [&]() -> int {
@@ -2718,6 +2932,10 @@ int ptyb_forward_intensity_noalloc(ptyb_handle* h, const int32_t* frames, int32_
 
 int ptyb_set_positions(ptyb_handle* h, const double* offsets, int32_t refine) {
   if (!h) return PTYB_INVALID;
+  if (h->opr_on && offsets) {
+    h->err = "the position model with a probe variation is not built";
+    return PTYB_INVALID;
+  }
   if (h->nslice > 1 && offsets) {
     h->err = "the position model runs on a single-slice object in this version";
     return PTYB_INVALID;

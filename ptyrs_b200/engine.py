@@ -303,6 +303,36 @@ class GpuPtycho:
     def synchronize(self):
         self._check(self._lib.ptyb_synchronize(self._h))
 
+    def set_probe_variation(self, eigenmodes, weights, refine_weights=True, intensity=None,
+                            refine_intensity=True):
+        """pty-chi's OPR probe variation of mode 0 for the LSQML calls that follow (reference
+        `ProbeVariation`): eigenmodes `[k, ny, nx]`, weights `[nframe, k]`, optional main-mode
+        weights `[nframe]`; `eigenmodes=None` returns to the shared probe."""
+        if eigenmodes is None:
+            self._check(self._lib.ptyb_set_probe_variation(self._h, None, 0, None, 0, None, 0))
+            self._opr = None
+            return
+        u = np.ascontiguousarray(eigenmodes, np.complex128)
+        w = np.ascontiguousarray(weights, np.float64).reshape(self._nframe, len(u))
+        c = None if intensity is None else np.ascontiguousarray(intensity, np.float64)
+        self._check(self._lib.ptyb_set_probe_variation(
+            self._h, _dptr(u.view(np.float64)), len(u), _dptr(w), int(refine_weights),
+            None if c is None else _dptr(c), int(refine_intensity)))
+        self._opr = (u.shape, c is not None)
+
+    def probe_variation(self):
+        """`(eigenmodes, weights, intensity)` of the probe variation (intensity None when not
+        modelled), or None without one."""
+        if getattr(self, "_opr", None) is None:
+            return None
+        shape, has_c = self._opr
+        u = np.empty(shape, np.complex128)
+        w = np.empty((self._nframe, shape[0]), np.float64)
+        c = np.empty(self._nframe, np.float64) if has_c else None
+        self._check(self._lib.ptyb_get_probe_variation(
+            self._h, _dptr(u.view(np.float64)), _dptr(w), None if c is None else _dptr(c)))
+        return u, w, c
+
     def set_timing(self, on=True):
         """Per-kernel device timing of every later launch (resets the totals)."""
         self._check(self._lib.ptyb_set_timing(self._h, int(on)))
