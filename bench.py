@@ -1,7 +1,7 @@
 """Throughput of the reconstruction hot path on B200: diffraction patterns·iterations per second.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload ml256|lsqml128|rpie64]
+                    [--workload ml256|lsqml128|opr128|rpie64|ms128|batch32|dm256|raar256|ap256]
 
 Workload `ml256` (default; the configuration the metric names, a 256² probe): Poisson
 maximum-likelihood conjugate gradient with position refinement — a 2048² smooth-noise object,
@@ -12,7 +12,8 @@ model), Poisson counts at 1e7 photons per pattern, FP32. A step is one ML cycle 
 patterns: the position sums from the magnitude projection, the object and probe gradients,
 the Polak–Ribière direction, the Poisson line search, the update and the position step.
 `lsqml128`: the LSQML configuration (1024² object, 128² probe × 3 modes, Fermat 4096 at 6 px,
-1e6 photons, batches of 256, Poisson cost), a step one epoch. `rpie64`: the rPIE
+1e6 photons, batches of 256, Poisson cost), a step one epoch; `opr128` the same with pty-chi's
+OPR probe variation of mode 0 (2 eigenmodes, their weights and the main mode's refined). `rpie64`: the rPIE
 configuration (256² object, 64² probe, 20×20 raster, batch 100), a step one epoch. Inputs
 live in HBM before the timed region; the counts of `ml256` (2.6 GB) and `lsqml128` (268 MB)
 are larger than the 126 MB L2, so no flush is needed between steps.
@@ -54,6 +55,12 @@ WORKLOADS = {
     "rpie64": dict(kind="rpie64", algorithm="rpie", batch=100,
                    desc="rPIE, 256^2 object, 64^2 probe, 20x20 raster 8 px +-1 px, "
                         "1e5 photons, batch 100, alpha=beta=0.1"),
+    # the LSQML configuration with pty-chi's OPR probe variation of mode 0 (2 eigenmodes, the
+    # per-frame weights and main-mode weights refined)
+    "opr128": dict(kind="lsqml128", algorithm="lsqml", batch=256, cost="poisson", opr=2,
+                   desc="LSQML with OPR probe variation (2 eigenmodes, weights and main-mode "
+                        "weights refined), 1024^2 object, 128^2 probe x3 modes, Fermat 4096 @ "
+                        "6 px, 1e6 photons, batch 256, Poisson"),
     # pty-chi's multislice object (3 slices) under LSQML, the multislice configuration's shapes
     "ms128": dict(kind="ms128", algorithm="lsqml", batch=256, cost="poisson",
                   desc="multislice LSQML, 3 slices of 1536^2 10 um apart (angular spectrum, "
@@ -155,6 +162,23 @@ def prepare(g, s, wl):
     sub-pixel offsets refined."""
     if wl["algorithm"] == "ml":
         g.set_positions(np.zeros((len(s["counts"]), 2)), refine=wl["refine"])
+    if wl.get("opr"):
+        u, w, c = opr_start(s, wl)
+        g.set_probe_variation(u, w, intensity=c)
+
+
+def opr_start(s, wl):
+    from ptyrs_b200 import sim
+    return sim.opr_start(s["probe"], len(s["counts"]), wl["opr"])
+
+
+def oracle_variation(s, wl):
+    """The oracle's copy of the workload's OPR start, or None without one."""
+    if not wl.get("opr"):
+        return None
+    from oracle.opr import ProbeVariation
+    u, w, c = opr_start(s, wl)
+    return ProbeVariation(u, w.ravel(), intensity=c)
 
 
 def run_algorithm(g, wl, nepoch):
@@ -179,11 +203,13 @@ def algorithmic_bytes(kind, s, wl):
     K = s["probe"].shape[0]
     S = s["object"].shape[0] if s.get("gaps") else 1
     moved = 8 * K * n2 if wl.get("refine") else 0
+    # OPR: every frame's own probe planes, written per batch and read by the frame pass
+    planes = 8 * K * n2 if wl.get("opr") else 0
     table = {
         "frame_store": 8 * n2 + 8 * K * n2 + 4 * n2,
         "frame_from_store": 8 * K * n2 + 4 * n2 + 8 * n2 + 8 * K * n2,
         "frame_rpie": 8 * n2 + 4 * n2 + 8 * K * n2,
-        "frame_lsqml": 8 * n2 + 4 * n2 + 8 * K * n2,
+        "frame_lsqml": 8 * n2 + 4 * n2 + 8 * K * n2 + planes,
         "frame_llk": 8 * n2 + 4 * n2 + moved,
         # gradient pass: object window, counts, (moved probe), Ψ kept and g written
         "frame_ml_grad": 8 * n2 + 4 * n2 + 16 * K * n2 + moved,
@@ -205,6 +231,9 @@ def algorithmic_bytes(kind, s, wl):
         # its iterate)
         "frame_carry": 8 * n2 + 4 * n2 + (32 if wl["algorithm"] == "raar" else 16) * K * n2,
         "object_blend": 8 * K * n2,
+        # OPR step per frame of a batch: the frame's object window (|O|² weights) and its
+        # mode-0 probe direction read, its own K probe planes written
+        "opr_step": 8 * n2 + 8 * n2 + 8 * K * n2,
         # multislice: every slice's window and the counts; forward writes the incident waves
         # of slices 1.. and the detector field, backward reads them and writes every slice's χ
         "slice_forward": 8 * n2 * S + 4 * n2 + 8 * K * n2 * S,
@@ -303,7 +332,7 @@ def cpu_baseline(s, wl, seconds=15.0, threads=None, cycles=2):
     done, t0 = 0, time.perf_counter()
     obj, probe = oracle_objects(s), p.probe
     if wl["algorithm"] == "lsqml":
-        run = Lsqml(wl["batch"], wl["cost"], 7)
+        run = Lsqml(wl["batch"], wl["cost"], 7, var=oracle_variation(s, wl))
         run.preconditioner = ops.illumination(p.addr.views, p.object.shape, probe)
     for frames in batches:
         views = np.concatenate([p.addr.frame_views(f) for f in frames])
@@ -366,7 +395,7 @@ def accuracy_batches(s, wl, device, nbatch=None):
     optics = oracle_optics(t)
     p = Ptycho(t["counts"], t["y"], t["x"], optics, t["object"][:1], t["probe"])
     if wl["algorithm"] == "lsqml":
-        run = Lsqml(wl["batch"], wl["cost"], 7)
+        run = Lsqml(wl["batch"], wl["cost"], 7, var=oracle_variation(t, wl))
         ref, _, _ = run.epoch(p.addr, p.obs, optics, oracle_objects(t), p.probe)
     else:
         p.rpie(1, batch_size=wl["batch"], obj_alpha=0.1, probe_alpha=0.1, seed=7)
@@ -374,6 +403,7 @@ def accuracy_batches(s, wl, device, nbatch=None):
     ref = np.concatenate(ref) if isinstance(ref, list) else ref
     scan = Scan(t["counts"], t["y"], t["x"], t["wavelength"], t["distance"], t["detector_pixel"])
     with GpuPtycho(scan, t["object"], t["probe"], device=device, gaps=t.get("gaps")) as g:
+        prepare(g, t, wl)
         run_algorithm(g, wl, 1)
         obj = g.objects()
     illum = ops.illumination(p.addr.views, p.object.shape, p.probe)
@@ -623,7 +653,9 @@ def main():
 
     # Dominant kernel and its roofline (algorithmic bytes per launch / mean launch time).
     pk, pk_kind = peaks()
-    top = max(times.items(), key=lambda kv: kv[1][0])
+    # the top kernel kind with a per-frame byte count (the "misc" kind has none)
+    typed = {k: v for k, v in times.items() if algorithmic_bytes(k, s, wl) and kframes.get(k)}
+    top = max((typed or times).items(), key=lambda kv: kv[1][0])
     kname, (kms, kn) = top
     per_frame = algorithmic_bytes(kname, s, wl)
     roofline = None

@@ -331,7 +331,7 @@ enum Kind : int {
   kKObjRpie, kKObjOverlap, kKObjLsqml, kKObjMl, kKIllum, kKProbePartial, kKProbeFinal,
   kKAfar, kKDots, kKSolve, kKAxpy, kKMax, kKCounts, kKMisc, kKGamma, kKArraySums, kKMove,
   kKPositionSums, kKSliceForward, kKSliceBackward, kKSliceLlk, kKFrameProject, kKSpectrum,
-  kKDerivSums, kKBackSpectrum, kKSliceGrad, kKFrameCarry, kKObjBlend, kNumKinds
+  kKDerivSums, kKBackSpectrum, kKSliceGrad, kKFrameCarry, kKObjBlend, kKOprStep, kNumKinds
 };
 static_assert(kNumKinds <= kMaxKinds, "the timing arrays hold kMaxKinds kinds");
 const char* const kKindNames[kNumKinds] = {
@@ -340,7 +340,7 @@ const char* const kKindNames[kNumKinds] = {
     "illumination", "probe_partial", "probe_finalize", "lsqml_afar", "lsqml_dots",
     "lsqml_solve", "axpy", "max", "counts", "misc", "ml_gamma", "array_sums", "move",
     "position_sums", "slice_forward", "slice_backward", "slice_llk", "frame_project", "spectrum",
-    "deriv_sums", "back_spectrum", "slice_grad", "frame_carry", "object_blend"};
+    "deriv_sums", "back_spectrum", "slice_grad", "frame_carry", "object_blend", "opr_step"};
 
 cudaEvent_t take_event(ptyb_handle* h) {
   if (!h->event_pool.empty()) {
@@ -1037,11 +1037,11 @@ void ensure_opr(ptyb_handle* h) {
 // Every slot's own probe planes under the probe variation into `out` ([slot][K][N][N]).
 void opr_planes(ptyb_handle* h, const int* frames, int nslot, float2* out) {
   const int plane = h->N * h->N;
-  timed(h, kKMisc, [&] {
+  timed(h, kKOprStep, [&] {
     opr_planes_kernel<<<dim3((plane + 255) / 256, nslot), 256, 0, h->stream>>>(
         h->probe, h->opr_u, h->opr_w, h->opr_has_c ? h->opr_c : nullptr, frames, h->K, h->opr_k,
         plane, out);
-  }, nslot);
+  });
   launched(h, "opr planes");
 }
 
@@ -1050,77 +1050,77 @@ void opr_planes(ptyb_handle* h, const int* frames, int nslot, float2* out) {
 void opr_step(ptyb_handle* h, const int* frames, int count) {
   const int plane = h->N * h->N, k = h->opr_k;
   const size_t dstride = (size_t)h->K * plane;
-  const unsigned pb = (unsigned)((plane + 255) / 256);
-  timed(h, kKMisc, [&] {
+  const unsigned pb = (unsigned)((plane + 255) / 256), pb64 = (unsigned)((plane + 63) / 64);
+  timed(h, kKOprStep, [&] {
     window_power_kernel<<<dim3(pb, count), 256, 0, h->stream>>>(h->object, frames, h->corners,
                                                                h->nxo, h->N, h->opr_vv);
   }, count);
   launched(h, "opr window power");
   if (h->opr_has_c && h->opr_refine_c) {
-    timed(h, kKMisc, [&] {
+    timed(h, kKOprStep, [&] {
       opr_frame_sums_kernel<<<count, 256, 0, h->stream>>>(h->probe, h->field, dstride, h->opr_vv,
                                                           plane, h->opr_sums);
     });
     launched(h, "opr intensity sums");
-    timed(h, kKMisc, [&] {
+    timed(h, kKOprStep, [&] {
       opr_intensity_kernel<<<(count + 255) / 256, 256, 0, h->stream>>>(h->opr_sums, frames, count,
                                                                         h->opr_c);
     });
     launched(h, "opr intensity");
   }
   if (k == 0 || count < 2) return;
-  timed(h, kKMisc, [&] {
-    opr_residue_kernel<<<pb, 256, 0, h->stream>>>(h->field, dstride, count, plane, h->opr_r);
+  timed(h, kKOprStep, [&] {
+    opr_residue_kernel<<<pb64, 64, 0, h->stream>>>(h->field, dstride, count, plane, h->opr_r);
   });
   launched(h, "opr residues");
   const double a_u = std::min(0.1, (double)count / h->P);
   for (int i = 0; i < k; ++i) {
     float2* u = h->opr_u + (size_t)i * plane;
-    timed(h, kKMisc, [&] {
+    timed(h, kKOprStep, [&] {
       opr_frame_sums_kernel<<<count, 256, 0, h->stream>>>(u, h->opr_r, plane, nullptr, plane,
                                                           h->opr_sums);
     });
     launched(h, "opr dots");
-    timed(h, kKMisc, [&] {
+    timed(h, kKOprStep, [&] {
       opr_coef_kernel<<<1, 256, 0, h->stream>>>(h->opr_sums, h->opr_w, frames, k, i, count,
                                                 (double)plane, h->opr_p);
     });
     launched(h, "opr coefficients");
-    timed(h, kKMisc, [&] {
-      opr_e_kernel<<<pb, 256, 0, h->stream>>>(h->opr_r, h->opr_p, count, plane, h->opr_e);
+    timed(h, kKOprStep, [&] {
+      opr_e_kernel<<<pb64, 64, 0, h->stream>>>(h->opr_r, h->opr_p, count, plane, h->opr_e);
     });
     launched(h, "opr e");
-    timed(h, kKMisc, [&] { opr_norm2_kernel<<<1, 1024, 0, h->stream>>>(h->opr_e, plane, h->opr_scal); });
+    timed(h, kKOprStep, [&] { opr_norm2_kernel<<<1, 1024, 0, h->stream>>>(h->opr_e, plane, h->opr_scal); });
     launched(h, "opr norm");
-    timed(h, kKMisc, [&] {
+    timed(h, kKOprStep, [&] {
       opr_u_step_kernel<<<pb, 256, 0, h->stream>>>(u, h->opr_e, h->opr_scal, a_u, plane);
     });
     launched(h, "opr eigenmode step");
-    timed(h, kKMisc, [&] { opr_norm2_kernel<<<1, 1024, 0, h->stream>>>(u, plane, h->opr_scal + 1); });
+    timed(h, kKOprStep, [&] { opr_norm2_kernel<<<1, 1024, 0, h->stream>>>(u, plane, h->opr_scal + 1); });
     launched(h, "opr norm");
-    timed(h, kKMisc, [&] { opr_u_scale_kernel<<<pb, 256, 0, h->stream>>>(u, h->opr_scal + 1, plane); });
+    timed(h, kKOprStep, [&] { opr_u_scale_kernel<<<pb, 256, 0, h->stream>>>(u, h->opr_scal + 1, plane); });
     launched(h, "opr eigenmode scale");
     if (h->opr_refine_w) {
-      timed(h, kKMisc, [&] {
+      timed(h, kKOprStep, [&] {
         opr_frame_sums_kernel<<<count, 256, 0, h->stream>>>(u, h->field, dstride, h->opr_vv,
                                                             plane, h->opr_sums);
       });
       launched(h, "opr weight sums");
-      timed(h, kKMisc, [&] {
+      timed(h, kKOprStep, [&] {
         opr_weights_kernel<<<1, 256, 0, h->stream>>>(h->opr_sums, frames, count, k, i, h->opr_w);
       });
       launched(h, "opr weights");
     }
     if (i + 1 < k) {
-      timed(h, kKMisc, [&] { opr_norm2_kernel<<<1, 1024, 0, h->stream>>>(u, plane, h->opr_scal + 2); });
+      timed(h, kKOprStep, [&] { opr_norm2_kernel<<<1, 1024, 0, h->stream>>>(u, plane, h->opr_scal + 2); });
       launched(h, "opr norm");
-      timed(h, kKMisc, [&] {
+      timed(h, kKOprStep, [&] {
         opr_frame_sums_kernel<<<count, 256, 0, h->stream>>>(u, h->opr_r, plane, nullptr, plane,
                                                             h->opr_sums);
       });
       launched(h, "opr projections");
-      timed(h, kKMisc, [&] {
-        opr_gs_kernel<<<pb, 256, 0, h->stream>>>(h->opr_r, u, h->opr_sums, h->opr_scal + 2, count,
+      timed(h, kKOprStep, [&] {
+        opr_gs_kernel<<<dim3(pb, count), 256, 0, h->stream>>>(h->opr_r, u, h->opr_sums, h->opr_scal + 2, count,
                                                  plane);
       });
       launched(h, "opr orthogonalisation");

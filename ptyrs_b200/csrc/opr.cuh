@@ -96,6 +96,7 @@ __global__ void opr_residue_kernel(const float2* d, size_t dstride, int count, i
   const int pix = blockIdx.x * blockDim.x + threadIdx.x;
   if (pix >= plane) return;
   double mr = 0.0, mi = 0.0;
+#pragma unroll 8
   for (int b = 0; b < count; ++b) {
     const float2 v = d[(size_t)b * dstride + pix];
     mr += v.x;
@@ -103,6 +104,7 @@ __global__ void opr_residue_kernel(const float2* d, size_t dstride, int count, i
   }
   mr /= count;
   mi /= count;
+#pragma unroll 8
   for (int b = 0; b < count; ++b) {
     const float2 v = d[(size_t)b * dstride + pix];
     r[(size_t)b * plane + pix] = make_float2((float)(v.x - mr), (float)(v.y - mi));
@@ -110,17 +112,32 @@ __global__ void opr_residue_kernel(const float2* d, size_t dstride, int count, i
 }
 
 // p_b = (Re<r_b, U>/n² + w_b) / Σ_b w_b², one block (engine/opr.rs:186-192).
-__global__ void opr_coef_kernel(const double* sums, const double* w, const int* frames, int k,
-                                int i, int count, double n, double* p) {
-  __shared__ double w2;
-  if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int b = 0; b < count; ++b) {
-      const double wb = w[(size_t)frames[b] * k + i];
-      s += wb * wb;
-    }
-    w2 = s;
+// Σ_b x_b in frame order by one block of 256 threads: each chunk of 256 terms loaded by all
+// threads at once, then added by thread 0 in order (the same bits as a serial loop).
+template <class F>
+__device__ double ordered_frame_sum(int count, F term) {
+  __shared__ double chunk[256];
+  double s = 0.0;
+  for (int b0 = 0; b0 < count; b0 += 256) {
+    const int n = min(256, count - b0);
+    if ((int)threadIdx.x < n) chunk[threadIdx.x] = term(b0 + (int)threadIdx.x);
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int j = 0; j < n; ++j) s += chunk[j];
+    __syncthreads();
   }
+  return s;
+}
+
+__global__ void __launch_bounds__(256) opr_coef_kernel(const double* sums, const double* w,
+                                                       const int* frames, int k, int i,
+                                                       int count, double n, double* p) {
+  __shared__ double w2;
+  const double s = ordered_frame_sum(count, [&](int b) {
+    const double wb = w[(size_t)frames[b] * k + i];
+    return wb * wb;
+  });
+  if (threadIdx.x == 0) w2 = s;
   __syncthreads();
   for (int b = threadIdx.x; b < count; b += blockDim.x)
     p[b] = (sums[b * 3 + 1] / (n * n) + w[(size_t)frames[b] * k + i]) / w2;
@@ -131,6 +148,7 @@ __global__ void opr_e_kernel(const float2* r, const double* p, int count, int pl
   const int pix = blockIdx.x * blockDim.x + threadIdx.x;
   if (pix >= plane) return;
   double er = 0.0, ei = 0.0;
+#pragma unroll 8
   for (int b = 0; b < count; ++b) {
     const float2 v = r[(size_t)b * plane + pix];
     er += v.x * p[b];
@@ -158,14 +176,11 @@ __global__ void opr_u_scale_kernel(float2* u, const double* nu, int n) {
 
 // w_fi = w_bi + Re<U, d_b> / (Σ|U|²·vv_b + 0.1·mean_b Σ|U|²·vv_b), one block
 // (engine/opr.rs:200-212).
-__global__ void opr_weights_kernel(const double* sums, const int* frames, int count, int k,
-                                   int i, double* w) {
+__global__ void __launch_bounds__(256) opr_weights_kernel(const double* sums, const int* frames,
+                                                          int count, int k, int i, double* w) {
   __shared__ double reg;
-  if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int b = 0; b < count; ++b) s += sums[b * 3];
-    reg = 0.1 * s / count;
-  }
+  const double s = ordered_frame_sum(count, [&](int b) { return sums[b * 3]; });
+  if (threadIdx.x == 0) reg = 0.1 * s / count;
   __syncthreads();
   for (int b = threadIdx.x; b < count; b += blockDim.x) {
     double& wb = w[(size_t)frames[b] * k + i];
@@ -173,17 +188,17 @@ __global__ void opr_weights_kernel(const double* sums, const int* frames, int co
   }
 }
 
-// r_b −= (Σ r_b·conj(U) / Σ|U|²)·U (engine/opr.rs:213-219), thread per pixel.
+// r_b −= (Σ r_b·conj(U) / Σ|U|²)·U (engine/opr.rs:213-219), thread per pixel, frame b =
+// blockIdx.y.
 __global__ void opr_gs_kernel(float2* r, const float2* u, const double* sums, const double* uu,
                               int count, int plane) {
   const int pix = blockIdx.x * blockDim.x + threadIdx.x;
-  if (pix >= plane) return;
+  const int b = blockIdx.y;
+  if (pix >= plane || b >= count) return;
   const float2 uv = u[pix];
-  for (int b = 0; b < count; ++b) {
-    const double cr = sums[b * 3 + 1] / *uu, ci = sums[b * 3 + 2] / *uu;
-    float2& v = r[(size_t)b * plane + pix];
-    v = make_float2((float)(v.x - (cr * uv.x - ci * uv.y)), (float)(v.y - (cr * uv.y + ci * uv.x)));
-  }
+  const double cr = sums[b * 3 + 1] / *uu, ci = sums[b * 3 + 2] / *uu;
+  float2& v = r[(size_t)b * plane + pix];
+  v = make_float2((float)(v.x - (cr * uv.x - ci * uv.y)), (float)(v.y - (cr * uv.y + ci * uv.x)));
 }
 
 }  // namespace ptyb

@@ -209,6 +209,20 @@ def make_batch(count=32, seed=0, scale=1.0, sides=(64, 96, 128, 192, 256)):
     return out
 
 
+def opr_start(probe, nframe, k=2, seed=3):
+    """A seeded start of pty-chi's OPR probe variation of mode 0: `k` smooth eigenmodes at the
+    main mode's scale (the mode times smoothed noise), weights uniform in ±0.1 per frame and
+    main-mode weights 1; `(eigenmodes [k, ny, nx], weights [nframe, k], intensity [nframe])`."""
+    rng = np.random.default_rng(seed)
+    p0 = np.asarray(probe)[0]
+    scale = np.sqrt((np.abs(p0) ** 2).mean())
+    u = []
+    for i in range(k):
+        g = smooth_object(p0.shape[-1], seed + i)[0] - 1.0
+        u.append(p0 * g * scale / np.sqrt((np.abs(p0 * g) ** 2).mean()))
+    return np.array(u), rng.uniform(-0.1, 0.1, (nframe, k)), np.ones(nframe)
+
+
 def make_scan(kind, seed=0, scale=1.0):
     """Seeded synthetic inputs of a benchmark configuration: returns a dict with counts
     (float32), y, x (metres), object start, probe start, truth object and sizes.

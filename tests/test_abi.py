@@ -39,7 +39,7 @@ def test_kernel_kinds_are_named(lib):
     k = lib.ptyb_kernel_kinds()
     names = [lib.ptyb_kernel_name(i).decode() for i in range(k)]
     assert all(names) and len(set(names)) == k
-    assert {"frame_carry", "object_blend", "frame_ml_grad"} <= set(names)
+    assert {"frame_carry", "object_blend", "frame_ml_grad", "opr_step"} <= set(names)
     assert lib.ptyb_kernel_name(k).decode() == ""
 
 
