@@ -1050,7 +1050,7 @@ void opr_planes(ptyb_handle* h, const int* frames, int nslot, float2* out) {
 void opr_step(ptyb_handle* h, const int* frames, int count) {
   const int plane = h->N * h->N, k = h->opr_k;
   const size_t dstride = (size_t)h->K * plane;
-  const unsigned pb = (unsigned)((plane + 255) / 256), pb64 = (unsigned)((plane + 63) / 64);
+  const unsigned pb = (unsigned)((plane + 255) / 256), pb32 = (unsigned)((plane + 31) / 32);
   timed(h, kKOprStep, [&] {
     window_power_kernel<<<dim3(pb, count), 256, 0, h->stream>>>(h->object, frames, h->corners,
                                                                h->nxo, h->N, h->opr_vv);
@@ -1070,7 +1070,7 @@ void opr_step(ptyb_handle* h, const int* frames, int count) {
   }
   if (k == 0 || count < 2) return;
   timed(h, kKOprStep, [&] {
-    opr_residue_kernel<<<pb64, 64, 0, h->stream>>>(h->field, dstride, count, plane, h->opr_r);
+    opr_residue_kernel<<<pb32, 256, 0, h->stream>>>(h->field, dstride, count, plane, h->opr_r);
   });
   launched(h, "opr residues");
   const double a_u = std::min(0.1, (double)count / h->P);
@@ -1087,7 +1087,7 @@ void opr_step(ptyb_handle* h, const int* frames, int count) {
     });
     launched(h, "opr coefficients");
     timed(h, kKOprStep, [&] {
-      opr_e_kernel<<<pb64, 64, 0, h->stream>>>(h->opr_r, h->opr_p, count, plane, h->opr_e);
+      opr_e_kernel<<<pb32, 256, 0, h->stream>>>(h->opr_r, h->opr_p, count, plane, h->opr_e);
     });
     launched(h, "opr e");
     timed(h, kKOprStep, [&] { opr_norm2_kernel<<<1, 1024, 0, h->stream>>>(h->opr_e, plane, h->opr_scal); });

@@ -90,22 +90,42 @@ __global__ void opr_intensity_kernel(const double* sums, const int* frames, int 
   if (b < count) c[frames[b]] += 0.1 * sums[b * 3 + 1] / sums[b * 3];
 }
 
-// r_b = d_b − mean_b d_b (the batch's mean in frame order), thread per pixel.
-__global__ void opr_residue_kernel(const float2* d, size_t dstride, int count, int plane,
-                                   float2* r) {
-  const int pix = blockIdx.x * blockDim.x + threadIdx.x;
-  if (pix >= plane) return;
+// The per-pixel sums over a batch's frames run in blocks of 32 pixels × 8 frame groups: group g
+// takes frames [g·chunk, (g+1)·chunk) in order, and the 8 partials are added in group order (a
+// fixed order, so every run gives the same bits).
+constexpr int kOprGroups = 8;
+
+// r_b = d_b − mean_b d_b.
+__global__ void __launch_bounds__(256) opr_residue_kernel(const float2* d, size_t dstride,
+                                                          int count, int plane, float2* r) {
+  __shared__ double part[2][kOprGroups][32];
+  const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;
+  const int pix = blockIdx.x * 32 + tx;
+  const int chunk = (count + kOprGroups - 1) / kOprGroups;
+  const int b0 = ty * chunk, b1 = min(count, b0 + chunk);
   double mr = 0.0, mi = 0.0;
-#pragma unroll 8
-  for (int b = 0; b < count; ++b) {
-    const float2 v = d[(size_t)b * dstride + pix];
-    mr += v.x;
-    mi += v.y;
+  if (pix < plane) {
+#pragma unroll 4
+    for (int b = b0; b < b1; ++b) {
+      const float2 v = d[(size_t)b * dstride + pix];
+      mr += v.x;
+      mi += v.y;
+    }
+  }
+  part[0][ty][tx] = mr;
+  part[1][ty][tx] = mi;
+  __syncthreads();
+  mr = 0.0;
+  mi = 0.0;
+  for (int g = 0; g < kOprGroups; ++g) {
+    mr += part[0][g][tx];
+    mi += part[1][g][tx];
   }
   mr /= count;
   mi /= count;
-#pragma unroll 8
-  for (int b = 0; b < count; ++b) {
+  if (pix >= plane) return;
+#pragma unroll 4
+  for (int b = b0; b < b1; ++b) {
     const float2 v = d[(size_t)b * dstride + pix];
     r[(size_t)b * plane + pix] = make_float2((float)(v.x - mr), (float)(v.y - mi));
   }
@@ -143,18 +163,33 @@ __global__ void __launch_bounds__(256) opr_coef_kernel(const double* sums, const
     p[b] = (sums[b * 3 + 1] / (n * n) + w[(size_t)frames[b] * k + i]) / w2;
 }
 
-// e = Σ_b r_b·p_b / count, thread per pixel, frames in order.
-__global__ void opr_e_kernel(const float2* r, const double* p, int count, int plane, float2* e) {
-  const int pix = blockIdx.x * blockDim.x + threadIdx.x;
-  if (pix >= plane) return;
+// e = Σ_b r_b·p_b / count, in the frame groups above.
+__global__ void __launch_bounds__(256) opr_e_kernel(const float2* r, const double* p, int count,
+                                                    int plane, float2* e) {
+  __shared__ double part[2][kOprGroups][32];
+  const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;
+  const int pix = blockIdx.x * 32 + tx;
+  const int chunk = (count + kOprGroups - 1) / kOprGroups;
+  const int b0 = ty * chunk, b1 = min(count, b0 + chunk);
   double er = 0.0, ei = 0.0;
-#pragma unroll 8
-  for (int b = 0; b < count; ++b) {
-    const float2 v = r[(size_t)b * plane + pix];
-    er += v.x * p[b];
-    ei += v.y * p[b];
+  if (pix < plane) {
+#pragma unroll 4
+    for (int b = b0; b < b1; ++b) {
+      const float2 v = r[(size_t)b * plane + pix];
+      er += v.x * p[b];
+      ei += v.y * p[b];
+    }
   }
-  e[pix] = make_float2((float)(er / count), (float)(ei / count));
+  part[0][ty][tx] = er;
+  part[1][ty][tx] = ei;
+  __syncthreads();
+  if (ty != 0 || pix >= plane) return;
+  double sr = 0.0, si = 0.0;
+  for (int g = 0; g < kOprGroups; ++g) {
+    sr += part[0][g][tx];
+    si += part[1][g][tx];
+  }
+  e[pix] = make_float2((float)(sr / count), (float)(si / count));
 }
 
 // u += (a_u·√n / mnorm(e))·e, mnorm(e) = √(Σ|e|²/n).
