@@ -712,6 +712,9 @@ def main():
         # ML offsets in f64)
         pos_bytes = 16 * P + (16 * P if wl["algorithm"] == "ml" else 0)
         h2d = s["counts"].nbytes + 8 * s["object"].size + 8 * s["probe"].size + pos_bytes
+        if wl.get("opr"):
+            # the OPR start: eigenmodes (complex128), weights and main-mode weights (f64)
+            h2d += 16 * wl["opr"] * n * n + 8 * P * wl["opr"] + 8 * P
         d2h = (8 * s["object"].size + 8 * s["probe"].size
                + (16 * P if wl["algorithm"] == "ml" else 0))
         e2e = {"value": P * ws * args.e2e_steps / dt, "unit": "patterns*iter/s",
