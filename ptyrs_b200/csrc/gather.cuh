@@ -250,7 +250,7 @@ constexpr int kMaxProbeChunk = 256;
 
 // Chunk `blockIdx.y` of slots (at most kMaxProbeChunk), 256 probe pixels per CTA:
 // Σ_slots w·upd in slot order.
-__global__ void __launch_bounds__(256) probe_partial_kernel(ProbeArgs a) {
+static __global__ void __launch_bounds__(256) probe_partial_kernel(ProbeArgs a) {
   __shared__ int2 cs[kMaxProbeChunk];
   __shared__ float om[kMaxProbeChunk];
   const int N = a.N;
@@ -294,7 +294,7 @@ __global__ void __launch_bounds__(256) probe_partial_kernel(ProbeArgs a) {
 
 // The object blend of AP / DM / RAAR (engine/ops.rs:371-381) from the sums kGatherBlend wrote:
 // O = (num + reg·O) / max(norm + reg, 1e-12) with reg = inertia·max norm.
-__global__ void blend_apply_kernel(float2* object, const float2* num, const float* norm,
+static __global__ void blend_apply_kernel(float2* object, const float2* num, const float* norm,
                                    const float* norm_max, float inertia, size_t n) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -305,7 +305,7 @@ __global__ void blend_apply_kernel(float2* object, const float2* num, const floa
 // The probe step of AP / DM / RAAR under the move (engine/features.rs:673-712), one block per
 // probe mode m: with D = max(norm + reg, 1e-12) and reg = inertia·max norm, step = g / D,
 // sums[m] = (Σ|g|²/D, reg·Σ|step|²) in double, added in a fixed order.
-__global__ void __launch_bounds__(1024) probe_pcg_step_kernel(const float2* g, const float* norm,
+static __global__ void __launch_bounds__(1024) probe_pcg_step_kernel(const float2* g, const float* norm,
                                                               const float* norm_max,
                                                               float inertia, int plane,
                                                               float2* step, double* sums) {
@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(1024) probe_pcg_step_kernel(const float2* g, c
 
 // Per slot and probe mode, Σ_pixels |O_window|²·|W|² in double (‖A·s‖² of one frame's view of
 // the moved step W), added in a fixed order; grid (slots, K).
-__global__ void __launch_bounds__(256) weighted_norm_kernel(const float2* waves,
+static __global__ void __launch_bounds__(256) weighted_norm_kernel(const float2* waves,
                                                             const float2* object,
                                                             const int* frames,
                                                             const int2* corners, int nxo, int N,
@@ -370,7 +370,7 @@ __global__ void __launch_bounds__(256) weighted_norm_kernel(const float2* waves,
 struct ModeCoefs {
   float c[kMaxModes];
 };
-__global__ void probe_modes_axpy_kernel(float2* probe, const float2* step, ModeCoefs alpha,
+static __global__ void probe_modes_axpy_kernel(float2* probe, const float2* step, ModeCoefs alpha,
                                         int plane, int count) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
@@ -380,7 +380,7 @@ __global__ void probe_modes_axpy_kernel(float2* probe, const float2* step, ModeC
 
 // The probe blend's norm Σ_frames |O|² per pixel: the chunks' sums in chunk order into `den`,
 // and its maximum into *dmax (zeroed by the caller).
-__global__ void __launch_bounds__(256) probe_norm_kernel(const float* partial_den, int nchunk,
+static __global__ void __launch_bounds__(256) probe_norm_kernel(const float* partial_den, int nchunk,
                                                          int plane, float* den, float* dmax) {
   __shared__ float red[8];
   const int i = blockIdx.x * 256 + threadIdx.x;
@@ -405,7 +405,7 @@ __global__ void __launch_bounds__(256) probe_norm_kernel(const float* partial_de
 // Σ over chunks in order; mode 0: P += coef·Σ; 1: out = coef·Σ; 2: out += Σ compensated;
 // 3: the blend P = (Σ + reg·P) / max(norm + reg, 1e-12) with reg = coef·max norm
 // (engine/ops.rs:371-381), `norm` one plane shared by the modes.
-__global__ void probe_finalize_kernel(const float2* partial, int nchunk, int count,
+static __global__ void probe_finalize_kernel(const float2* partial, int nchunk, int count,
                                       float2* probe, float2* out, float2* comp, float coef,
                                       int mode, const float* norm = nullptr,
                                       const float* norm_max = nullptr, int plane = 1) {

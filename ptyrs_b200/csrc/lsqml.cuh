@@ -24,7 +24,7 @@ PTYB_D double block_sum1(double v, double* sh) {
 // block adds the threads' sums in double; λ0 joins once per pixel and mode.
 constexpr int kDotParts = 4;  // blocks per frame; their sums are added in block order
 
-__global__ void __launch_bounds__(512) lsqml_dots_kernel(
+static __global__ void __launch_bounds__(512) lsqml_dots_kernel(
     const float2* object, const float2* d_obj, const float2* probe, const float2* d_probe,
     const float2* quad, const float2* chi, const int* frames, const int2* corners, int nxo,
     int K, int N, double lambda0, double* sums, int probe_stride) {
@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(512) lsqml_dots_kernel(
 // One block: the per-frame 2×2 solves in double, trimmed mean of a_obj, mean of a_probe;
 // scal[0] = object step, scal[1] = probe step. Records a_far / a_obj / a_probe per slot in
 // `log` ([slot][3]) and the frames' a_far in `a_far_all`.
-__global__ void __launch_bounds__(1024) lsqml_solve_kernel(const double* sums, int nslot,
+static __global__ void __launch_bounds__(1024) lsqml_solve_kernel(const double* sums, int nslot,
                                                            double scale, const float* a_far,
                                                            const int* frames, float* a_far_all,
                                                            double* log, float* scal,
@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(1024) lsqml_solve_kernel(const double* sums, i
 }
 
 // x += scal[which]·d over n values.
-__global__ void axpy_scal_kernel(float2* x, const float2* d, const float* scal, int which,
+static __global__ void axpy_scal_kernel(float2* x, const float2* d, const float* scal, int which,
                                  size_t n) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -128,7 +128,7 @@ __global__ void axpy_scal_kernel(float2* x, const float2* d, const float* scal, 
 }
 
 // Max of a non-negative float array into *out (which starts at 0).
-__global__ void max_kernel(const float* v, size_t n, float* out) {
+static __global__ void max_kernel(const float* v, size_t n, float* out) {
   float m = 0.f;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)

@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T, 2) gamma_kernel(GammaArgs
 
 // Per block, in double: mode 0 Σ Re(conj(g)·(g − h)) and Σ |h|² (Polak–Ribière);
 // mode 1 Σ |g| (the modulus sum of scale_obj_probe). Partial sums [block][2].
-__global__ void __launch_bounds__(256) array_sums_kernel(const float2* g, const float2* h,
+static __global__ void __launch_bounds__(256) array_sums_kernel(const float2* g, const float2* h,
                                                          size_t n, int mode, double* partial) {
   __shared__ double sh[16];
   double s0 = 0.0, s1 = 0.0;
@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(256) array_sums_kernel(const float2* g, const 
 }
 
 // d = beta·d − g.
-__global__ void cg_direction_kernel(float2* d, const float2* g, float beta, size_t n) {
+static __global__ void cg_direction_kernel(float2* d, const float2* g, float beta, size_t n) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float2 a = d[i], b = g[i];
@@ -169,14 +169,14 @@ __global__ void cg_direction_kernel(float2* d, const float2* g, float beta, size
 }
 
 // x += gamma·d (gamma in double, applied in float).
-__global__ void axpy_kernel(float2* x, const float2* d, float gamma, size_t n) {
+static __global__ void axpy_kernel(float2* x, const float2* d, float gamma, size_t n) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   x[i] = cadd(x[i], cscale(d[i], gamma));
 }
 
 // x *= s.
-__global__ void scale_kernel(float2* x, float s, size_t n) {
+static __global__ void scale_kernel(float2* x, float s, size_t n) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   x[i] = cscale(x[i], s);
@@ -184,7 +184,7 @@ __global__ void scale_kernel(float2* x, float s, size_t n) {
 
 // x[k][y][x] *= exp(i·2π·sign·(dy·(y − hy)/sy + dx·(x − hx)/sx)) for every plane k
 // (the ramps of `zero_phase_ramp`, engine/ptycho.rs:1153-1170), phase in double.
-__global__ void ramp_kernel(float2* x, int nplanes, int ny, int nx, double dy, double dx,
+static __global__ void ramp_kernel(float2* x, int nplanes, int ny, int nx, double dy, double dx,
                             double sy, double sx, double sign) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const size_t n = (size_t)nplanes * ny * nx;

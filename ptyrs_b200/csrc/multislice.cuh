@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T, frame_min_blocks<N, C>())
 
 // Per slot, slice s ≥ 1's Eq. 23b sums (engine/lsqml.rs:327-347): with dop = q_s·dO_s·in_s,
 // num = Σ Re(conj(dop)·χ_s), den = Σ |dop|² over modes and pixels; sums [slot][2] in double.
-__global__ void __launch_bounds__(512) slice_dots_kernel(const float2* d_obj,
+static __global__ void __launch_bounds__(512) slice_dots_kernel(const float2* d_obj,
                                                         const float2* incident,
                                                         const float2* quad, const float2* chi,
                                                         const int* frames, const int2* corners,
@@ -317,7 +317,7 @@ __global__ void __launch_bounds__(512) slice_dots_kernel(const float2* d_obj,
 
 // One block: a_obj_s = max(0.5·num/den·0.9/scale, 0) per frame, their trimmed mean into
 // *step (engine/lsqml.rs:327-347, 392-398).
-__global__ void __launch_bounds__(1024) slice_solve_kernel(const double* sums, int nslot,
+static __global__ void __launch_bounds__(1024) slice_solve_kernel(const double* sums, int nslot,
                                                            double scale, double* log,
                                                            int log_stride, float* step) {
   __shared__ double a[1024], sorted[1024];

@@ -8,7 +8,7 @@
 namespace ptyb {
 
 // out[slot][m] = c_f·P_0 + Σ_i w_fi·U_i for m = 0, P_m otherwise (engine/opr.rs:88-120).
-__global__ void opr_planes_kernel(const float2* probe, const float2* u, const double* w,
+static __global__ void opr_planes_kernel(const float2* probe, const float2* u, const double* w,
                                   const double* c, const int* frames, int K, int k, int plane,
                                   float2* out) {
   const int slot = blockIdx.y;
@@ -25,7 +25,7 @@ __global__ void opr_planes_kernel(const float2* probe, const float2* u, const do
 }
 
 // vv[slot] = |O_window|² per pixel.
-__global__ void window_power_kernel(const float2* object, const int* frames, const int2* corners,
+static __global__ void window_power_kernel(const float2* object, const int* frames, const int2* corners,
                                     int nxo, int N, float* vv) {
   const int slot = blockIdx.y;
   const int2 c = corners[frames[slot]];
@@ -38,7 +38,7 @@ __global__ void window_power_kernel(const float2* object, const int* frames, con
 
 // Per slot (one block each): s0 = Σ |a|²·vv, s1 + i·s2 = Σ conj(a)·x, over the plane;
 // `a` a shared plane, `x` the slot's plane at x + slot·xstride.
-__global__ void __launch_bounds__(256) opr_frame_sums_kernel(const float2* a, const float2* x,
+static __global__ void __launch_bounds__(256) opr_frame_sums_kernel(const float2* a, const float2* x,
                                                              size_t xstride, const float* vv,
                                                              int plane, double* out) {
   __shared__ double red[3][8];
@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(256) opr_frame_sums_kernel(const float2* a, co
 }
 
 // Σ |x|² over n elements, one block, fixed order.
-__global__ void __launch_bounds__(1024) opr_norm2_kernel(const float2* x, int n, double* out) {
+static __global__ void __launch_bounds__(1024) opr_norm2_kernel(const float2* x, int n, double* out) {
   __shared__ double red[32];
   double s = 0.0;
   for (int i = threadIdx.x; i < n; i += 1024) s += (double)cnorm2(x[i]);
@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(1024) opr_norm2_kernel(const float2* x, int n,
 }
 
 // The main mode's weights (engine/opr.rs:162-168): c_f += 0.1·Re<P_0, d_b> / Σ|P_0|²·vv_b.
-__global__ void opr_intensity_kernel(const double* sums, const int* frames, int count,
+static __global__ void opr_intensity_kernel(const double* sums, const int* frames, int count,
                                      double* c) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b < count) c[frames[b]] += 0.1 * sums[b * 3 + 1] / sums[b * 3];
@@ -96,7 +96,7 @@ __global__ void opr_intensity_kernel(const double* sums, const int* frames, int 
 constexpr int kOprGroups = 8;
 
 // r_b = d_b − mean_b d_b.
-__global__ void __launch_bounds__(256) opr_residue_kernel(const float2* d, size_t dstride,
+static __global__ void __launch_bounds__(256) opr_residue_kernel(const float2* d, size_t dstride,
                                                           int count, int plane, float2* r) {
   __shared__ double part[2][kOprGroups][32];
   const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;
@@ -149,7 +149,7 @@ __device__ double ordered_frame_sum(int count, F term) {
   return s;
 }
 
-__global__ void __launch_bounds__(256) opr_coef_kernel(const double* sums, const double* w,
+static __global__ void __launch_bounds__(256) opr_coef_kernel(const double* sums, const double* w,
                                                        const int* frames, int k, int i,
                                                        int count, double n, double* p) {
   __shared__ double w2;
@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(256) opr_coef_kernel(const double* sums, const
 }
 
 // e = Σ_b r_b·p_b / count, in the frame groups above.
-__global__ void __launch_bounds__(256) opr_e_kernel(const float2* r, const double* p, int count,
+static __global__ void __launch_bounds__(256) opr_e_kernel(const float2* r, const double* p, int count,
                                                     int plane, float2* e) {
   __shared__ double part[2][kOprGroups][32];
   const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;
@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(256) opr_e_kernel(const float2* r, const doubl
 }
 
 // u += (a_u·√n / mnorm(e))·e, mnorm(e) = √(Σ|e|²/n).
-__global__ void opr_u_step_kernel(float2* u, const float2* e, const double* ne, double a_u,
+static __global__ void opr_u_step_kernel(float2* u, const float2* e, const double* ne, double a_u,
                                   int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -202,7 +202,7 @@ __global__ void opr_u_step_kernel(float2* u, const float2* e, const double* ne, 
 }
 
 // u *= √n / mnorm(u).
-__global__ void opr_u_scale_kernel(float2* u, const double* nu, int n) {
+static __global__ void opr_u_scale_kernel(float2* u, const double* nu, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float s = (float)(sqrt((double)n) / sqrt(*nu / n));
@@ -211,7 +211,7 @@ __global__ void opr_u_scale_kernel(float2* u, const double* nu, int n) {
 
 // w_fi = w_bi + Re<U, d_b> / (Σ|U|²·vv_b + 0.1·mean_b Σ|U|²·vv_b), one block
 // (engine/opr.rs:200-212).
-__global__ void __launch_bounds__(256) opr_weights_kernel(const double* sums, const int* frames,
+static __global__ void __launch_bounds__(256) opr_weights_kernel(const double* sums, const int* frames,
                                                           int count, int k, int i, double* w) {
   __shared__ double reg;
   const double s = ordered_frame_sum(count, [&](int b) { return sums[b * 3]; });
@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(256) opr_weights_kernel(const double* sums, co
 
 // r_b −= (Σ r_b·conj(U) / Σ|U|²)·U (engine/opr.rs:213-219), thread per pixel, frame b =
 // blockIdx.y.
-__global__ void opr_gs_kernel(float2* r, const float2* u, const double* sums, const double* uu,
+static __global__ void opr_gs_kernel(float2* r, const float2* u, const double* sums, const double* uu,
                               int count, int plane) {
   const int pix = blockIdx.x * blockDim.x + threadIdx.x;
   const int b = blockIdx.y;

@@ -229,7 +229,7 @@ __host__ __device__ constexpr size_t move_smem_bytes(int K) {
 // planes[slot][m] = w·χ_m per natural pixel: each frame's probe direction before its adjoint
 // move, w = conj(q·O_window) (LSQML, engine/lsqml.rs:200-207) or, with `omax`, rPIE's weight
 // conj(q·O)/((1 − α)|O|² + α·max|O|²) (engine/ptycho.rs:1007-1026).
-__global__ void probe_terms_kernel(const float2* object, const float2* quad, const float2* chi,
+static __global__ void probe_terms_kernel(const float2* object, const float2* quad, const float2* chi,
                                    const int* frames, const int2* corners, int nxo, int K, int N,
                                    float2* planes, const float* omax = nullptr,
                                    float alpha = 0.f) {
@@ -252,7 +252,7 @@ __global__ void probe_terms_kernel(const float2* object, const float2* quad, con
 // Per slot, pty-chi's position sums on mode 0 (engine/features.rs:459-492): with w the
 // frame's moved probe times q, per axis num = Σ Re(conj(∂O·w)·χ), den = Σ |∂O·w|²;
 // sums[slot] = (num_y, num_x, den_y, den_x) in double.
-__global__ void __launch_bounds__(256) position_sums_kernel(const float2* dwin,
+static __global__ void __launch_bounds__(256) position_sums_kernel(const float2* dwin,
                                                            const float2* wave, int wave_stride,
                                                            const float2* quad,
                                                            const float2* chi, int K, int N,
@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(256) position_sums_kernel(const float2* dwin,
 // pty-chi's gradient position step on the batch (engine/features.rs:496-521), one thread in
 // double: delta = num/(den + max(max_batch den, eps)), dx = 0.3·delta at the batch's frames
 // (0 elsewhere), each axis clipped to min(10·mean|dx − mean dx|, 0.1) over every frame.
-__global__ void position_step_kernel(const double* sums, int nslot, int nframe, double eps,
+static __global__ void position_step_kernel(const double* sums, int nslot, int nframe, double eps,
                                      const int* frames, double* offsets) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   for (int a = 0; a < 2; ++a) {
@@ -321,7 +321,7 @@ PTYB_D double fixed_block_sum(double v, double* sh) {
 // The position step of AP, DM and ML on every frame (engine/features.rs:1028-1047), one block:
 // per axis, with max the largest den, step = clip(0.3·num / (den + max), ±0.1) (0 where that
 // denominator is not positive) and d += step − mean(step) over every frame.
-__global__ void __launch_bounds__(1024) ml_position_step_kernel(const double* sums, int nframe,
+static __global__ void __launch_bounds__(1024) ml_position_step_kernel(const double* sums, int nframe,
                                                                double* offsets) {
   __shared__ double sh[32];
   const int t = threadIdx.x;
