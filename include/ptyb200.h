@@ -234,8 +234,10 @@ int ptyb_forward_intensity(ptyb_handle* h, const int32_t* frames, int32_t n, flo
  * scratch (frame list, detector field, intensities) in one fixed 32 MiB device array that
  * every GPU loading this library holds until exit. Frames are processed in chunks that fit it;
  * PTYB_INVALID when a single frame (K field planes and one intensity plane) does not. The
- * first call on a device looks the array's address up (cudaGetSymbolAddress); make that call
- * before any stream capture. Every call shares the array and leaves its last contents there:
+ * first call on a device looks the array's address up (cudaGetSymbolAddress) and keeps it for
+ * the life of the process, which assumes the device's primary context lives as long (a host
+ * program that calls cudaDeviceReset must not call this entry point afterwards); make that
+ * first call before any stream capture. Every call shares the array and leaves its last contents there:
  * every byte a call reads it writes first, and calls that overlap on the GPU (other handles or
  * threads at the same time) race on it. */
 int ptyb_forward_intensity_noalloc(ptyb_handle* h, const int32_t* frames, int32_t n, float* out);
