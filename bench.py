@@ -298,25 +298,25 @@ def oracle_objects(s):
     return s["object"]
 
 
-def cpu_baseline(s, wl, seconds=15.0, threads=None, cycles=2):
-    """The oracle (numpy float64 restatement of the reference's CPU engine) on a bounded sample
-    of the workload. ML: `cycles` cycles (one call, as the GPU step) over the first
-    `wl["sample_frames"]` frames of the scan. LSQML / rPIE: successive batch updates of
-    `wl["batch"]` frames from the same start until `seconds` pass. Returns patterns·iter/s,
-    the pattern-iterations done, the seconds and the oracle state."""
+def _threads(n):
+    """numpy's FFT workers and the BLAS pools limited to `n` threads (None: all)."""
     from oracle import ops
-    from oracle.lsqml import Lsqml
+    from threadpoolctl import threadpool_limits
+    ops.FFT_WORKERS = n
+    return threadpool_limits(limits=n)
+
+
+def cpu_cycles(s, wl, m, cycles, threads):
+    """`cycles` cycles (one call, as the GPU step) of the oracle over the first `m` frames of
+    the scan with the full object; returns the seconds and the oracle state."""
     from oracle.ptycho import Ptycho
-    from ptyrs_b200 import sim
-    ops.FFT_WORKERS = threads
-    optics = oracle_optics(s)
-    if wl["algorithm"] in CYCLES:
-        t = sample_scan(s, min(wl["sample_frames"], len(s["counts"])))
-        p = Ptycho(t["counts"], t["y"], t["x"], optics, t["object"], t["probe"])
-        t0 = time.perf_counter()
+    t = sample_scan(s, min(m, len(s["counts"])))
+    p = Ptycho(t["counts"], t["y"], t["x"], oracle_optics(s), t["object"], t["probe"])
+    with _threads(threads):
         if wl["algorithm"] == "ml":
             p.set_positions(np.zeros((p.addr.nframe, 2)), refine=wl["refine"])
-            t0 = time.perf_counter()
+        t0 = time.perf_counter()
+        if wl["algorithm"] == "ml":
             p.ml(cycles, update_object=True, update_probe=True, calc_llk=0,
                  zero_phase_ramp=False)
         elif wl["algorithm"] == "ap":
@@ -324,42 +324,103 @@ def cpu_baseline(s, wl, seconds=15.0, threads=None, cycles=2):
         else:
             getattr(p, wl["algorithm"])(cycles, calc_llk=0, zero_phase_ramp=False)
         dt = time.perf_counter() - t0
-        ops.FFT_WORKERS = None
-        return p.addr.nframe * cycles / dt, p.addr.nframe * cycles, dt, p
-    p = Ptycho(s["counts"], s["y"], s["x"], optics, s["object"][:1], s["probe"])
+    from oracle import ops
+    ops.FFT_WORKERS = None
+    return dt, p
+
+
+def cycle_fit(s, wl, threads, cycles=2, reps=1):
+    """The oracle's cycle time over the whole scan, from cycles over its first m/2 and m frames
+    (m = wl["sample_frames"]) with the full object: T(m) = a + b·m separates the object-sized
+    work of a cycle (a: gradients, conjugate directions, line-search sums and updates over
+    every object pixel) from the per-frame work (b), so the sample's few frames do not carry
+    the whole object's work. Returns patterns·iter/s over the scan's P frames, P / (a + b·P),
+    the fit, and the larger sample's oracle state."""
+    m2 = min(wl["sample_frames"], len(s["counts"]))
+    m1 = max(1, m2 // 2)
+    t1 = t2 = 0.0
+    for _ in range(reps):
+        t1 += cpu_cycles(s, wl, m1, cycles, threads)[0] / cycles
+        d, state = cpu_cycles(s, wl, m2, cycles, threads)
+        t2 += d / cycles
+    t1, t2 = t1 / reps, t2 / reps
+    b = max((t2 - t1) / (m2 - m1), 1e-12)
+    a = max(t1 - b * m1, 0.0)
+    P = len(s["counts"])
+    fit = {"object_s_per_cycle": a, "frame_s": b, "samples": [[m1, t1], [m2, t2]],
+           "cycles_per_sample": cycles * reps}
+    return P / (a + b * P), fit, state
+
+
+def cpu_batches(s, wl, seconds, threads):
+    """Successive batch updates (`wl["batch"]` frames, the seeded order of the GPU run) of the
+    oracle from the same start until `seconds` pass (at least one). Returns patterns·iter/s,
+    the pattern-iterations done, the seconds and the oracle state."""
+    from oracle import ops
     from oracle.base import random_batches
+    from oracle.lsqml import Lsqml
+    from oracle.ptycho import Ptycho
+    optics = oracle_optics(s)
+    p = Ptycho(s["counts"], s["y"], s["x"], optics, s["object"][:1], s["probe"])
     batches = random_batches(p.addr.nframe, wl["batch"], 7, 0)
-    done, t0 = 0, time.perf_counter()
+    done = 0
     obj, probe = oracle_objects(s), p.probe
-    if wl["algorithm"] == "lsqml":
-        run = Lsqml(wl["batch"], wl["cost"], 7, var=oracle_variation(s, wl))
-        run.preconditioner = ops.illumination(p.addr.views, p.object.shape, probe)
-    for frames in batches:
-        views = np.concatenate([p.addr.frame_views(f) for f in frames])
+    with _threads(threads):
+        t0 = time.perf_counter()
         if wl["algorithm"] == "lsqml":
-            obj, probe, _ = run.step(views, p.obs, optics, obj, probe)
-        else:
-            p.rpie_batch(frames, 1.0, 1.0, 0.1, 0.1)
-        done += len(frames)
-        if time.perf_counter() - t0 > seconds:
-            break
-    dt = time.perf_counter() - t0
+            run = Lsqml(wl["batch"], wl["cost"], 7, var=oracle_variation(s, wl))
+            run.preconditioner = ops.illumination(p.addr.views, p.object.shape, probe)
+        for frames in batches:
+            views = np.concatenate([p.addr.frame_views(f) for f in frames])
+            if wl["algorithm"] == "lsqml":
+                obj, probe, _ = run.step(views, p.obs, optics, obj, probe)
+            else:
+                p.rpie_batch(frames, 1.0, 1.0, 0.1, 0.1)
+            done += len(frames)
+            if time.perf_counter() - t0 > seconds:
+                break
+        dt = time.perf_counter() - t0
     ops.FFT_WORKERS = None
     return done / dt, done, dt, p
 
 
+def cpu_baseline(s, wl, threads, seconds=15.0):
+    """The oracle (numpy float64 restatement of the reference's CPU engine) on the host cores
+    for `s`'s workload, like for like with the GPU step: for cycle algorithms the whole-scan
+    cycle time from cycle_fit, for batch algorithms batch updates of the run's own size.
+    Returns the cpu_baseline object of the bench line and the oracle state of its sample."""
+    if wl["algorithm"] in CYCLES:
+        v, fit, state = cycle_fit(s, wl, threads)
+        what = (f"{wl['algorithm'].upper()} cycles"
+                + (" with position refinement" if wl["algorithm"] == "ml" else "")
+                + f" over the first {fit['samples'][0][0]} and {fit['samples'][1][0]} frames "
+                  f"({fit['cycles_per_sample']} per sample) with the full object, "
+                  f"{fit['samples'][0][1]:.2f} s and {fit['samples'][1][1]:.2f} s per cycle; "
+                  f"a cycle over all {len(s['counts'])} frames = {fit['object_s_per_cycle']:.2f} "
+                  f"s object-sized work + {1e3 * fit['frame_s']:.1f} ms per frame, extrapolated")
+        out = {"value": v, "unit": "patterns*iter/s", "cores": threads, "kind": "port",
+               "sample": what + f", numpy float64 on {threads} threads", "fit": fit}
+        return out, state
+    v, done, secs, state = cpu_batches(s, wl, seconds, threads)
+    out = {"value": v, "unit": "patterns*iter/s", "cores": threads, "kind": "port",
+           "sample": f"{done} pattern-iterations ({done // wl['batch']} batch updates of "
+                     f"{wl['batch']} frames of the scan) in {secs:.1f} s, numpy float64 on "
+                     f"{threads} threads"}
+    return out, state
+
+
 def object_nrmse(a, b, weight):
-    """‖a − c·b‖/‖c·b‖ over the pixels where `weight` > 0, c the least-squares complex scalar
-    that removes the global phase (and scale) between them."""
-    a, b = a[weight > 0], b[weight > 0]
-    c = np.vdot(b, a) / np.vdot(b, b)
-    return float(np.linalg.norm(a - c * b) / np.linalg.norm(c * b))
+    """Object NRMSE with the global phase and a linear phase ramp removed and the scale kept
+    (ptyrs_b200.metrics)."""
+    from ptyrs_b200.metrics import object_nrmse as nrmse
+    return nrmse(a, b, weight)
 
 
 def accuracy(s, wl, oracle_state, device, cycles=2):
     """The FP32 GPU path against the float64 oracle on the bounded sample of cycles: object
-    NRMSE after the global phase, over the illuminated pixels (illumination ≥ 1e-3 of its
-    max), and for ML the largest difference of the refined offsets."""
+    NRMSE after the global phase and phase ramp, scale kept, over the illuminated pixels
+    (illumination ≥ 1e-3 of its max), and for ML the largest difference of the refined
+    offsets."""
     from oracle import ops
     from ptyrs_b200 import GpuPtycho, Scan
     t = sample_scan(s, oracle_state.addr.nframe)
@@ -384,7 +445,7 @@ def accuracy(s, wl, oracle_state, device, cycles=2):
 def accuracy_batches(s, wl, device, nbatch=None):
     """rPIE and LSQML: one epoch over the first `nbatch` batches' frames of the scan (the same
     seeded batches) on the GPU in FP32 and in the float64 oracle from the same start; object
-    NRMSE after the global phase over the illuminated pixels."""
+    NRMSE after the global phase and phase ramp, scale kept, over the illuminated pixels."""
     from oracle import ops
     from oracle.lsqml import Lsqml
     from oracle.ptycho import Ptycho
@@ -414,45 +475,76 @@ def accuracy_batches(s, wl, device, nbatch=None):
                       "same start"}
 
 
+def line_config(args, wl, s, patterns, ws):
+    """The `config` of both arms' lines (the same keys, so the two lines name one workload)."""
+    counts = sum(x["counts"].nbytes for x in s) if isinstance(s, list) else s["counts"].nbytes
+    out = {"workload": args.workload, "description": wl["desc"], "scale": args.scale,
+           "patterns_per_step_per_gpu": patterns, "parallelism": f"replicas{ws}",
+           "l2": f"inputs larger than L2 (counts {counts / 1e6:.0f} MB)"}
+    if isinstance(s, list):
+        out["scans"] = len(s)
+        out["sides"] = {n: sum(1 for x in s if x["n"] == n) for n in (64, 96, 128, 192, 256)}
+    return out
+
+
 def reference_arm(args, wl):
+    """The reference's CPU path for the same workload on the host cores (its numpy float64
+    restatement, every host thread), a bounded sample per step: cycle algorithms one cycle over
+    the scan's first m/2 and m frames with the full object, extrapolated to the whole scan by
+    the fitted object-sized and per-frame costs (cycle_fit); batch algorithms one batch update
+    of the run's own batch size."""
     rank, ws, _ = dist_env()
     if rank != 0:
         return
-    desc = wl["desc"]
+    full_wl = wl
     if wl["algorithm"] == "batch":
         # the batch's first scan (make_batch draws the scans in order), rPIE batch updates
         from ptyrs_b200 import sim
-        s = sim.make_batch(1, seed=0, scale=args.scale)[0]
+        scans = sim.make_batch(32, seed=0, scale=args.scale)
+        s = scans[0]
+        patterns = 2 * sum(len(x["counts"]) for x in scans)
         wl = RPIE_OF_BATCH
     else:
         s = make_inputs(args.workload, 0, scale=args.scale)
+        scans, patterns = s, len(s["counts"])
     threads = os.cpu_count() or 1
-    for _ in range(args.warmup):
-        cpu_baseline(s, wl, seconds=0.0, threads=threads, cycles=1)
-    vals, frames, secs = [], 0, 0.0
-    for _ in range(args.steps):
-        v, d, t, _ = cpu_baseline(s, wl, seconds=0.0, threads=threads, cycles=1)
-        vals.append(v)
-        frames += d
-        secs += t
-    value = frames / secs
-    if wl["algorithm"] == "ml":
-        what = (f"one ML cycle (with position refinement) over the first "
-                f"{wl['sample_frames']} frames")
-    elif wl["algorithm"] in CYCLES:
-        what = f"one {wl['algorithm'].upper()} cycle over the first {wl['sample_frames']} frames"
+    a = b = 0.0
+    frames, secs = 0, 0.0
+    fits = []
+    for step in range(args.warmup + args.steps):
+        if wl["algorithm"] in CYCLES:
+            _, fit, _ = cycle_fit(s, wl, threads, cycles=1)
+            if step >= args.warmup:
+                fits.append(fit)
+        else:
+            _, d, t, _ = cpu_batches(s, wl, 0.0, threads)
+            if step >= args.warmup:
+                frames += d
+                secs += t
+    if wl["algorithm"] in CYCLES:
+        a = statistics.mean(f["object_s_per_cycle"] for f in fits)
+        b = statistics.mean(f["frame_s"] for f in fits)
+        P = len(s["counts"])
+        value = P / (a + b * P)
+        ms_step = 1e3 * sum(f["samples"][0][1] + f["samples"][1][1] for f in fits) / len(fits)
+        sample = (f"{args.steps} steps of one {wl['algorithm'].upper()} cycle over the first "
+                  f"{fits[0]['samples'][0][0]} and {fits[0]['samples'][1][0]} frames with the "
+                  f"full object; a cycle over all {P} frames = {a:.2f} s object-sized work + "
+                  f"{1e3 * b:.1f} ms per frame, extrapolated")
     else:
-        what = f"one {wl['algorithm']} batch update of {wl['batch']} frames"
-    sample = (f"{args.steps} steps of {what} of the {args.workload} scan ({frames} "
-              f"pattern-iterations in {secs:.1f} s)")
+        value = frames / secs
+        ms_step = 1e3 * secs / max(args.steps, 1)
+        sample = (f"{args.steps} steps of one {wl['algorithm']} batch update of {wl['batch']} "
+                  f"frames ({frames} pattern-iterations in {secs:.1f} s)")
     line = {
         "impl": "reference", "metric": "diffraction patterns*iter/sec", "value": value,
         "unit": "patterns*iter/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * secs / max(args.steps, 1), "higher_is_better": True,
+        "ms_per_step": ms_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "description": desc},
+        "config": line_config(args, full_wl, scans, patterns, ws),
         "cpu_baseline": {"value": value, "unit": "patterns*iter/s", "cores": threads,
-                         "kind": "port", "sample": sample},
+                         "kind": "port", "sample": sample + f", numpy float64 on {threads} "
+                                                            "threads"},
         "e2e": {"value": value, "unit": "patterns*iter/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -547,26 +639,25 @@ def batch_main(args, wl):
     cpu, acc = None, None
     if rank == 0 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        v, done, secs, _ = cpu_baseline(scans[0], RPIE_OF_BATCH, seconds=15.0, threads=threads)
-        cpu = {"value": v, "unit": "patterns*iter/s", "cores": threads, "kind": "port",
-               "sample": f"{done} pattern-iterations ({done // 100} rPIE batch updates of 100 "
-                         f"frames of the first scan, side {scans[0]['n']}) in {secs:.1f} s, "
-                         f"numpy float64, FFTs on {threads} threads"}
-        acc = accuracy_batches(scans[0], RPIE_OF_BATCH, local)
+        cpu, _ = cpu_baseline(scans[0], RPIE_OF_BATCH, threads)
+        cpu["sample"] += f" (rPIE batch updates of the first scan, side {scans[0]['n']})"
+        one, _ = cpu_baseline(scans[0], RPIE_OF_BATCH, 1, seconds=5.0)
+        cpu["single_core"] = {"value": one["value"], "cores": 1, "sample": one["sample"]}
+        # every scan: one rPIE epoch over its first batch, FP32 GPU vs float64 oracle
+        per_scan = [accuracy_batches(x, RPIE_OF_BATCH, local, nbatch=1)["object_nrmse_vs_f64"]
+                    for x in scans]
+        acc = {"object_nrmse_vs_f64_per_scan": per_scan, "max": max(per_scan),
+               "sample": "per scan: one rPIE epoch (batches of 100) over its first 100 frames, "
+                         "GPU FP32 vs the float64 oracle from the same start"}
     for h in handles:
         h.close()
     if rank == 0:
-        sides = {n: sum(1 for s in scans if s["n"] == n) for n in (64, 96, 128, 192, 256)}
         print(json.dumps({
             "metric": "diffraction patterns*iter/sec", "value": value,
             "unit": "patterns*iter/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": args.workload, "description": wl["desc"],
-                       "scale": args.scale, "scans": len(scans), "sides": sides,
-                       "patterns_per_step_per_gpu": 2 * P, "parallelism": f"replicas{ws}",
-                       "l2": "inputs larger than L2 (counts "
-                             f"{sum(s['counts'].nbytes for s in scans) / 1e6:.0f} MB)"},
+            "config": line_config(args, wl, scans, 2 * P, ws),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "accuracy": acc,
             "gpu_launches": int(launches), "clocks": clk,
             "kernels_ms": {k: round(v[0], 3) for k, v in sorted(times.items())},
@@ -725,18 +816,20 @@ def main():
     cpu, acc = None, None
     if rank == 0 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        v, done, secs, state = cpu_baseline(s, wl, seconds=15.0, threads=threads)
+        cpu, state = cpu_baseline(s, wl, threads)
         if wl["algorithm"] in CYCLES:
-            what = (f"2 {wl['algorithm'].upper()} cycles"
-                    + (" with position refinement" if wl["algorithm"] == "ml" else "")
-                    + f" over the first {state.addr.nframe} frames of the scan")
             acc = accuracy(s, wl, state, local)
         else:
-            what = f"{done // wl['batch']} batch updates of {wl['batch']} frames of the scan"
             acc = accuracy_batches(s, wl, local)
-        cpu = {"value": v, "unit": "patterns*iter/s", "cores": threads, "kind": "port",
-               "sample": f"{done} pattern-iterations ({what}) in {secs:.1f} s, numpy float64, "
-                         f"FFTs on {threads} threads"}
+        # the like-for-like figure of a single-threaded CPU engine
+        if wl["algorithm"] in CYCLES:
+            v1, fit1, _ = cycle_fit(s, wl, 1, cycles=1)
+            one = {"value": v1, "cores": 1, "fit": fit1,
+                   "sample": "as above, one cycle per sample, numpy float64 on 1 thread"}
+        else:
+            o, _ = cpu_baseline(s, wl, 1, seconds=8.0)
+            one = {"value": o["value"], "cores": 1, "sample": o["sample"]}
+        cpu["single_core"] = one
     g.close()
     if rank == 0:
         line = {
@@ -744,11 +837,7 @@ def main():
             "unit": "patterns*iter/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": args.workload, "description": wl["desc"],
-                       "scale": args.scale,
-                       "patterns_per_step_per_gpu": P, "parallelism": f"replicas{ws}",
-                       "l2": "inputs larger than L2 (counts "
-                             f"{s['counts'].nbytes / 1e6:.0f} MB)"},
+            "config": line_config(args, wl, s, P, ws),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "accuracy": acc,
             "gpu_launches": int(launches), "clocks": clk, "autotune": tuned,
             "ms_per_step_with_kernel_events": instrumented_ms / args.steps,
