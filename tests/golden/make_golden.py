@@ -70,4 +70,9 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    # the checkout of physwkim/ptyrs whose golden tables are converted: the first argument, or
+    # PTYRS_REFERENCE
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PTYRS_REFERENCE")
+    if not root:
+        sys.exit("usage: make_golden.py PTYRS_CHECKOUT (or set PTYRS_REFERENCE)")
+    main(root)
