@@ -17,7 +17,7 @@ against PyNX (`dm_pynx_f64.txt`, `raar_pynx_f64.txt`), and OPR probe variation a
 an LSQML step (`opr_*`, `lsqml_opr_*`, `lsqml_opr_int_*`). Each text table becomes one float64 array of the same rows and
 columns under its stem (`table` for a file without one) in `<group>.npz`.
 
-    python tests/golden/make_golden.py [REFERENCE_ROOT]
+    python tests/golden/make_golden.py REFERENCE_ROOT [GROUP ...]
 """
 import os
 import sys
@@ -36,6 +36,9 @@ GROUPS = {
     "lsqml_multislice": ["cases", "corners", "counts", "obj", "probe", "icalc", "llk",
                          "step_steps", "step_obj", "step_probe", "epochs_steps", "epochs_obj",
                          "epochs_probe"],
+    # one LSQML step through the three slices refining positions under Patch
+    # (refs/f64/lsqml_multislice_pos.py): the start slices, steps, offsets and changes
+    "lsqml_multislice_pos": ["start", "steps", "offsets", "obj", "probe"],
     # The far-field sets on the seeded scenario `dm_scenario(32, 40, nprobe, 2e5, 4.0)`, whose
     # counts the oracle redraws (oracle/scenario.py): results only, no state.
     "pos_grad": ["", "values"],
@@ -46,6 +49,12 @@ GROUPS = {
     "lsqml_epochs_poisson": ["obj", "probe", "steps"],
     "lsqml_pos": ["steps", "offsets", "obj", "probe"],
     "lsqml_pos_epochs": ["steps", "offsets", "obj", "probe"],
+    # pty-chi BH on the amplitude cost, two epochs with one batch of every frame (conjugate
+    # directions) and with batches of 16 (steepest descent); step rows padded with -1
+    "bh_full": ["obj", "probe", "steps"],
+    "bh_mini": ["obj", "probe", "steps"],
+    # one LSQML step refining the offsets with three eigenmodes of probe mode 0
+    "lsqml_pos_opr": ["eigen", "weights", "steps", "offsets", "obj", "probe"],
     "rpie_ptychi": [""],
     "dm_pynx": [""],
     "raar_pynx": [""],
@@ -57,14 +66,25 @@ GROUPS = {
 }
 
 
-def main(root):
+def load_table(path):
+    """A whitespace table as float64 rows; rows of unequal length (a batch's frames at the end
+    of each step row) are padded with -1."""
+    rows = [[float(v) for v in line.split()] for line in open(path) if line.strip()]
+    width = max(len(r) for r in rows)
+    return np.array([r + [-1.0] * (width - len(r)) for r in rows], np.float64).reshape(
+        len(rows), width)
+
+
+def main(root, only=()):
     data = os.path.join(root, "ptyrs", "tests", "engine", "data")
     here = os.path.dirname(os.path.abspath(__file__))
     for group, stems in GROUPS.items():
+        if only and group not in only:
+            continue
         arrays = {}
         for stem in stems:
             name = f"{group}_{stem}_f64.txt" if stem else f"{group}_f64.txt"
-            arrays[stem or "table"] = np.loadtxt(os.path.join(data, name), ndmin=2)
+            arrays[stem or "table"] = load_table(os.path.join(data, name))
         np.savez_compressed(os.path.join(here, f"{group}.npz"), **arrays)
         print(group, {k: v.shape for k, v in arrays.items()})
 
@@ -75,4 +95,4 @@ if __name__ == "__main__":
     root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PTYRS_REFERENCE")
     if not root:
         sys.exit("usage: make_golden.py PTYRS_CHECKOUT (or set PTYRS_REFERENCE)")
-    main(root)
+    main(root, sys.argv[2:])

@@ -245,3 +245,39 @@ def test_rpie_with_refined_positions_matches_ptychi(name, params, nepoch):
     assert max_rel(re_im(p.probe - p0), g["probe"][:, 3:5]) < 1e-12
     want = frame_offsets(p, g["offsets"], 3) - start
     assert max_rel(p.offsets - start, want) < 3e-12
+
+
+@pytest.mark.parametrize("cost,noise", [("amplitude", 0), ("poisson", 1)])
+def test_lsqml_positions_with_opr_step_matches_golden(cost, noise):
+    """One step refining the offsets with three eigenmodes of probe mode 0 and their weights
+    refined (engine_lsqml_pos.rs:121-200 with `opr`): steps, changes, offsets, eigenmodes and
+    weights after it."""
+    from oracle.opr import ProbeVariation
+    p = state()
+    g = golden("lsqml_pos_opr")
+    rows = g["steps"]
+    frames = [int(v) for v in rows[:, 0]]
+    start = frame_offsets(p, g["offsets"], 1)
+    e, w = g["eigen"], g["weights"]
+    u0 = (e[:, 3] + 1j * e[:, 4]).reshape(3, 32, 32)
+    w0 = w[:, 1:4].ravel()
+    var = ProbeVariation(u0, w0)
+    run = Lsqml(len(frames), cost, 0, offsets=start.copy(), refine=True, var=var)
+    run.preconditioner = ops.illumination(p.addr.views, p.object.shape, p.probe)
+    obj, probe, st = run.step(views_of(p, frames), p.obs, p.optics, p.object, p.probe)
+    col = 1 + 3 * noise
+    assert st["frames"] == frames
+    assert max_rel(st["a_far"], rows[:, col]) < 1e-13
+    assert max_rel(st["a_obj"], rows[:, col + 1]) < 1e-12
+    assert max_rel(st["a_probe"], rows[:, col + 2]) < 1e-12
+    c = 2 + 2 * noise
+    assert max_rel(re_im(obj - p.object), g["obj"][:, c:c + 2]) < 1e-12
+    c = 3 + 2 * noise
+    assert max_rel(re_im(probe - p.probe), g["probe"][:, c:c + 2]) < 1e-12
+    want = frame_offsets(p, g["offsets"], 3 + 2 * noise) - start
+    assert max_rel(run.offsets - start, want) < 1e-12
+    c = 5 + 2 * noise
+    u1 = (e[:, c] + 1j * e[:, c + 1]).reshape(3, 32, 32)
+    assert max_rel(re_im(var.eigenmodes), re_im(u1)) < 1e-13
+    w1 = w[:, 4 + 3 * noise:7 + 3 * noise].ravel()
+    assert max_rel(var.weights - w0, w1 - w0) < 1e-13

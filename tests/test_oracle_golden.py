@@ -369,3 +369,31 @@ def test_multislice_epochs_match_ptychi():
         assert max_rel(llks, want[:, 2]) < 1e-12
         assert max_rel(multislice_changes(objs, objs0), of_case(g["epochs_obj"], k)) < 1e-12
         assert max_rel(change(probe, probe0), of_case(g["epochs_probe"], k)) < 1e-12
+
+
+def test_multislice_step_with_positions_matches_ptychi():
+    """engine_lsqml_multislice.rs:374-458 (`step_with_positions_matches_ptychi`): one LSQML
+    step on frames 0..8 through the three slices from `lsqml_multislice_pos.py`'s start, every
+    frame moved by its offset under Patch and the offsets refined on the middle slice; the
+    case whose exit has no plane phase (the only one the reference checks under Patch): the
+    steps, the object and probe changes and the offset changes."""
+    g, addr, _, probe, cases = multislice_state()
+    p = golden("lsqml_multislice_pos")
+    start = p["start"]
+    objs = [stack((1,) + OBJ, start[start[:, 0] == s], 3) for s in range(NSLICE)]
+    views = addr.views[:8 * addr.nmode]
+    checked = 0
+    for k, (optics, obs, _) in enumerate(cases):
+        if not np.all(optics.quad == 1.0):
+            continue
+        checked += 1
+        rows = p["offsets"][p["offsets"][:, 0] == k]
+        d0, want = rows[:, 2:4], rows[:, 4:6]
+        run = Lsqml(8, "poisson", 0, offsets=d0, refine=True)
+        run.preconditioner = ops.illumination(addr.views, objs[0].shape, probe)
+        o, pr, st = run.step(views, obs, optics, objs, probe)
+        assert_ms_step(st, p["steps"][p["steps"][:, 0] == k], 1)
+        assert max_rel(multislice_changes(o, objs), of_case(p["obj"], k)) < 1e-12
+        assert max_rel(change(pr, probe), of_case(p["probe"], k)) < 1e-12
+        assert max_rel(run.offsets - d0, want - d0) < 1e-11
+    assert checked == 1
