@@ -58,6 +58,17 @@ cudaError_t launch_gamma_side(int N, const GammaArgs& a, int nslot, cudaStream_t
   return cudaErrorInvalidValue;
 }
 
+cudaError_t launch_bh_side(int N, const BhArgs& a, int nslot, cudaStream_t s) {
+  switch (N) {
+    case 64: return SideKernels<64>::bh(a, nslot, s);
+    case 96: return SideKernels<96>::bh(a, nslot, s);
+    case 128: return SideKernels<128>::bh(a, nslot, s);
+    case 192: return SideKernels<192>::bh(a, nslot, s);
+    case 256: return SideKernels<256>::bh(a, nslot, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
 }  // namespace ptyb
 
 namespace ptyb::eng {
@@ -153,6 +164,16 @@ cudaError_t fill_sync(ptyb_handle* h, void* dst, int value, size_t bytes) {
   if (e != cudaSuccess) return e;
   return cudaStreamSynchronize(h->stream);
 }
+bool on_device(ptyb_handle* h, const void* p) {
+  cudaPointerAttributes a = {};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();  // not a pointer the runtime knows: clear the error it left
+    return false;
+  }
+  return (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) &&
+         a.device == h->device;
+}
+
 void launched(ptyb_handle* h, const char* what) {
   ++h->launches;
   check(h, cudaGetLastError(), what);
@@ -164,7 +185,8 @@ const char* const kKindNames[kNumKinds] = {
     "illumination", "probe_partial", "probe_finalize", "lsqml_afar", "lsqml_dots",
     "lsqml_solve", "axpy", "max", "counts", "misc", "ml_gamma", "array_sums", "move",
     "position_sums", "slice_forward", "slice_backward", "slice_llk", "frame_project", "spectrum",
-    "deriv_sums", "back_spectrum", "slice_grad", "frame_carry", "object_blend", "opr_step"};
+    "deriv_sums", "back_spectrum", "slice_grad", "frame_carry", "object_blend", "opr_step",
+    "bh_hessian"};
 
 
 cudaEvent_t take_event(ptyb_handle* h) {
@@ -233,7 +255,9 @@ int cluster_for(int N, int K, int want) {
 MoveArgs move_args(ptyb_handle* h, const int* frames, float2* planes) {
   MoveArgs m = {};
   m.probe = h->probe;
-  m.quad = h->quad;
+  // the phase the probe moves with: the exit's on one slice, none on slice 0 of a multislice
+  // object (engine/lsqml.rs:500-523, `optics.slice_quad(0)`)
+  m.quad = h->nslice > 1 ? h->ones : h->quad;
   m.tw = h->tw;
   m.object = h->object;
   m.frames = frames;
@@ -322,7 +346,9 @@ void ensure_slots(ptyb_handle* h, int n) {
   if (n <= h->slots) return;
   const size_t plane = (size_t)h->N * h->N;
   h->upd = alloc<float2>(h, (size_t)n * h->K * plane);
-  h->field = alloc<float2>(h, (size_t)n * h->K * plane);
+  // the detector field (K planes per slot), also the window derivatives of the position model
+  // (two planes per slot)
+  h->field = alloc<float2>(h, (size_t)n * std::max(h->K, 2) * plane);
   h->icalc = alloc<float>(h, (size_t)n * plane);
   h->omax = alloc<float>(h, n);
   h->afar1 = alloc<float>(h, n);
@@ -395,7 +421,7 @@ ptyb_llk llk_pass(ptyb_handle* h, const float2* waves) {
   const int stack = std::min(h->P, h->stack);
   const size_t pstride = (size_t)h->K * h->N * h->N;
   ensure_slots(h, stack);
-  if (h->have_offsets && !waves && h->nslice == 1) {
+  if (h->have_offsets && !waves) {
     ensure_spec(h);
     spectrum_of(h, h->probe, h->spec);
   }
@@ -410,6 +436,16 @@ ptyb_llk llk_pass(ptyb_handle* h, const float2* waves) {
       sa.tf = h->tf;
       sa.nslice = h->nslice;
       sa.obj_plane = (size_t)h->nyo * h->nxo;
+      if (waves) {
+        // each frame's own (moved or varied) probe enters slice 0
+        sa.f.probe = waves + s0 * pstride;
+        sa.f.probe_stride = (int)pstride;
+      } else if (h->have_offsets) {
+        // each frame's moved probe enters slice 0
+        move_frames(h, h->iota + s0, n, h->spec, h->wave);
+        sa.f.probe = h->wave;
+        sa.f.probe_stride = (int)pstride;
+      }
       check(h, launch_slice<kSliceLlk>(h, sa, n), "llk pass");
       ++h->launches;
       continue;
@@ -936,14 +972,6 @@ int ptyb_get_llk(ptyb_handle* h, ptyb_llk* out) {
 
 int ptyb_set_positions(ptyb_handle* h, const double* offsets, int32_t refine) {
   if (!h) return PTYB_INVALID;
-  if (h->opr_on && offsets) {
-    h->err = "the position model with a probe variation is not built";
-    return PTYB_INVALID;
-  }
-  if (h->nslice > 1 && offsets) {
-    h->err = "the position model runs on a single-slice object in this version";
-    return PTYB_INVALID;
-  }
   if (offsets)
     for (int i = 0; i < 2 * h->P; ++i)
       if (!std::isfinite(offsets[i])) {
@@ -1008,6 +1036,63 @@ int ptyb_set_objects(ptyb_handle* h, const double* src) {
   return guarded(h, true, [&]() -> int {
     const size_t n = (size_t)h->nslice * h->nobj * h->nyo * h->nxo;
     upload_c64(h, src, h->object, n, "objects");
+    return PTYB_OK;
+  });
+}
+
+int ptyb_set_object_device(ptyb_handle* h, int32_t nobj, int32_t nyo, int32_t nxo,
+                           const void* src) {
+  if (!h || !src) return PTYB_INVALID;
+  if (nobj != h->nobj || nyo != h->nyo || nxo != h->nxo) {
+    h->err = "object dims differ from the handle's";
+    return PTYB_INVALID;
+  }
+  if (!on_device(h, src)) {
+    h->err = "the object must be device memory of the handle's device";
+    return PTYB_INVALID;
+  }
+  return guarded(h, true, [&]() -> int {
+    const size_t n = (size_t)h->nobj * h->nyo * h->nxo;
+    check(h, copy_sync(h, h->object, src, n * sizeof(float2), cudaMemcpyDeviceToDevice),
+          "object");
+    return PTYB_OK;
+  });
+}
+
+int ptyb_set_objects_device(ptyb_handle* h, int32_t nslice, int32_t nyo, int32_t nxo,
+                            const void* src) {
+  if (!h || !src) return PTYB_INVALID;
+  if (nslice != h->nslice || nyo != h->nyo || nxo != h->nxo) {
+    h->err = "slice dims differ from the handle's";
+    return PTYB_INVALID;
+  }
+  if (!on_device(h, src)) {
+    h->err = "the slices must be device memory of the handle's device";
+    return PTYB_INVALID;
+  }
+  return guarded(h, true, [&]() -> int {
+    const size_t n = (size_t)h->nslice * h->nobj * h->nyo * h->nxo;
+    check(h, copy_sync(h, h->object, src, n * sizeof(float2), cudaMemcpyDeviceToDevice),
+          "objects");
+    return PTYB_OK;
+  });
+}
+
+int ptyb_set_probe_device(ptyb_handle* h, int32_t nprobe, int32_t ny, int32_t nx,
+                          const void* src) {
+  if (!h || !src) return PTYB_INVALID;
+  if (nprobe != h->nprobe || ny != h->N || nx != h->N) {
+    h->err = "probe dims differ from the handle's";
+    return PTYB_INVALID;
+  }
+  if (!on_device(h, src)) {
+    h->err = "the probe must be device memory of the handle's device";
+    return PTYB_INVALID;
+  }
+  return guarded(h, true, [&]() -> int {
+    const size_t n = (size_t)h->nprobe * h->N * h->N;
+    check(h, copy_sync(h, h->probe, src, n * sizeof(float2), cudaMemcpyDeviceToDevice),
+          "probe");
     return PTYB_OK;
   });
 }

@@ -26,17 +26,67 @@ void lsqml_preconditioner(ptyb_handle* h, bool init) {
   launched(h, "pre max");
 }
 
+// Every slot's own probe planes of the batch into h->wave, or nullptr for the shared probe:
+// the probe variation's planes (engine/opr.rs:88-120), each moved by its frame's offset under
+// the position model (engine/lsqml.rs:500-523), or the shared probe moved.
+const float2* frame_probes(ptyb_handle* h, const int* frames, int nslot);
+
+// The batch's probe direction into h->d_probe (engine/lsqml.rs:200-229): each frame's
+// conj(q·O_0)·χ_0 over its slice-0 window into h->field, moved back through the frame's move
+// under the position model, and their frame mean. Returns the per-frame directions the mean
+// was taken over (the moved-back ones; h->field keeps the raw ones the OPR step also reads).
+const float2* probe_directions(ptyb_handle* h, const int* frames, int nslot,
+                               const float2* quad, const float2* chi) {
+  const int pstride = h->K * h->N * h->N;
+  timed(h, kKProbePartial, [&] {
+    probe_terms_kernel<<<dim3((h->N * h->N + 255) / 256, nslot), 256, 0, h->stream>>>(
+        h->object, quad, chi, frames, h->corners, h->nxo, h->K, h->N, h->field);
+  });
+  launched(h, "probe terms");
+  const float2* dirs = h->field;
+  if (h->have_offsets) {
+    float2* moved = h->field;
+    if (h->opr_on) {
+      // the OPR step reads both the raw and the moved-back directions
+      moved = h->opr_moved;
+      check(h, cudaMemcpyAsync(moved, h->field, (size_t)nslot * pstride * sizeof(float2),
+                               cudaMemcpyDeviceToDevice, h->stream),
+            "directions");
+    }
+    check(h, launch_move<kMoveBack>(h, move_args(h, frames, moved), nslot), "probe move back");
+    ++h->launches;
+    dirs = moved;
+  }
+  timed(h, kKProbeFinal, [&] {
+    probe_finalize_kernel<<<(pstride + 255) / 256, 256, 0, h->stream>>>(
+        dirs, nslot, pstride, h->probe, h->d_probe, nullptr, 1.0f / nslot, 1);
+  });
+  launched(h, "probe direction");
+  return dirs;
+}
+
+void opr_step(ptyb_handle* h, const int* frames, int count, const float2* moved);
+
 // One LSQML step through pty-chi's multislice object (engine/lsqml.rs:581-643 with
 // SliceWaves, engine/multislice.rs): forward through the slices, backward χ per slice, every
 // slice's object direction from its incident wave, the probe direction from χ of slice 0,
-// slice 0's step sizes jointly with the probe and Eq. 23b on the others.
+// slice 0's step sizes jointly with the probe and Eq. 23b on the others. Under the position
+// model every frame's probe enters slice 0 moved by its offset (no phase on slice 0), the
+// probe directions go back through the moves before their frame mean, and refinement takes
+// pty-chi's position step from the middle slice (engine/lsqml.rs:231-270, 500-523).
 void lsqml_batch_slices(ptyb_handle* h, const ptyb_lsqml_params& p, const int* frames, int nslot,
                         double* log, int log_stride) {
   const int S = h->nslice;
   const size_t plane = (size_t)h->N * h->N, fplanes = (size_t)h->K * plane;
   const size_t slice_stride = (size_t)nslot * fplanes, no = (size_t)h->nyo * h->nxo;
+  const bool refine = h->have_offsets && h->refine_offsets;
   SliceArgs sa = {};
   sa.f = frame_args(h, frames);
+  const float2* own = frame_probes(h, frames, nslot);
+  if (own) {
+    sa.f.probe = own;
+    sa.f.probe_stride = (int)fplanes;
+  }
   sa.f.cost = p.cost;
   sa.f.nslot = nslot;
   sa.f.a_prev = h->afar_all;
@@ -61,19 +111,46 @@ void lsqml_batch_slices(ptyb_handle* h, const ptyb_lsqml_params& p, const int* f
     if (s > 0) {
       g.probe = h->incident + (s - 1) * slice_stride;
       g.probe_stride = (int)fplanes;
+    } else if (own) {
+      g.probe = own;
+      g.probe_stride = (int)fplanes;
     }
     timed(h, kKObjLsqml, [&] { object_tile_kernel<kGatherLsqml><<<ntiles(h), 1024, 0, h->stream>>>(g); }, nslot);
     launched(h, "slice object direction");
   }
   // probe direction from χ of slice 0 through slice 0's windows (no phase when S > 1)
-  probe_pass(h, frames, nslot, 1, 0.f, 1.0f / nslot, h->ones, h->chi_slices);
+  const float2* dirs = nullptr;
+  if (own)
+    dirs = probe_directions(h, frames, nslot, h->ones, h->chi_slices);
+  else
+    probe_pass(h, frames, nslot, 1, 0.f, 1.0f / nslot, h->ones, h->chi_slices);
   const double lambda0 = 1.2e-7 * ((double)h->N * h->N) / ((double)h->N * h->N);
   timed(h, kKDots, [&] {
     lsqml_dots_kernel<<<nslot * kDotParts, 512, 0, h->stream>>>(
-        h->object, h->d_obj, h->probe, h->d_probe, h->ones, h->chi_slices, frames, h->corners,
-        h->nxo, h->K, h->N, lambda0, h->sums, 0);
+        h->object, h->d_obj, own ? own : h->probe, h->d_probe, h->ones, h->chi_slices,
+        frames, h->corners, h->nxo, h->K, h->N, lambda0, h->sums, own ? (int)fplanes : 0);
   }, nslot);
   launched(h, "step sums");
+  // the eigenmodes and the refined weights on slice 0 from the state on entry, before the
+  // window derivatives below take h->field, where the frame directions are
+  if (h->opr_on) opr_step(h, frames, nslot, dirs);
+  if (refine) {
+    // pty-chi's position sums on slice S/2 (`slice_for_correction`) from the state on entry:
+    // the wave entering it at mode 0 times its phase, its χ and its window's derivatives
+    const int sc = S / 2;
+    MoveArgs md = move_args(h, frames, h->field);
+    md.object = h->object + sc * no;
+    check(h, launch_move<kDerivWindow>(h, md, nslot), "window derivative");
+    ++h->launches;
+    const float2* in = sc == 0 ? own : h->incident + (sc - 1) * slice_stride;
+    const float2* q = sc + 1 == S ? h->quad : h->ones;
+    timed(h, kKPositionSums, [&] {
+      position_sums_kernel<<<nslot, 256, 0, h->stream>>>(h->field, in, (int)fplanes, q,
+                                                          h->chi_slices + sc * slice_stride,
+                                                          h->K, h->N, h->pos_sums);
+    }, nslot);
+    launched(h, "position sums");
+  }
   const double scale = (double)(S * h->K);
   for (int s = 1; s < S; ++s) {
     timed(h, kKDots, [&] {
@@ -107,6 +184,14 @@ void lsqml_batch_slices(ptyb_handle* h, const ptyb_lsqml_params& p, const int* f
         h->probe, h->d_probe, h->scal + 2, 1, fplanes);
   });
   launched(h, "probe step");
+  if (refine) {
+    const double eps = 1e-6 * ((double)h->N * h->N);
+    timed(h, kKSolve, [&] {
+      position_step_kernel<<<1, 32, 0, h->stream>>>(h->pos_sums, nslot, h->P, eps, frames,
+                                                    h->offsets);
+    });
+    launched(h, "position step");
+  }
 }
 
 // One LSQML step on a batch (engine/lsqml.rs:581-643), with the position model when offsets
@@ -121,6 +206,7 @@ void ensure_opr(ptyb_handle* h) {
     h->opr_sums = alloc<double>(h, (size_t)h->slots * 3);
     h->opr_p = alloc<double>(h, h->slots);
     h->wave = alloc<float2>(h, (size_t)h->slots * h->K * plane);
+    h->opr_moved = alloc<float2>(h, (size_t)h->slots * h->K * plane);
     h->opr_slots = h->slots;
   }
   if (!h->opr_e) {
@@ -141,9 +227,27 @@ void opr_planes(ptyb_handle* h, const int* frames, int nslot, float2* out) {
   launched(h, "opr planes");
 }
 
+const float2* frame_probes(ptyb_handle* h, const int* frames, int nslot) {
+  if (h->opr_on) {
+    opr_planes(h, frames, nslot, h->wave);
+    if (h->have_offsets) {
+      check(h, launch_move<kMoveOwn>(h, move_args(h, frames, h->wave), nslot), "planes move");
+      ++h->launches;
+    }
+    return h->wave;
+  }
+  if (!h->have_offsets) return nullptr;
+  ensure_spec(h);
+  spectrum_of(h, h->probe, h->spec);
+  move_frames(h, frames, nslot, h->spec, h->wave);
+  return h->wave;
+}
+
 // The OPR step of the batch (engine/opr.rs:122-224) from its frame probe directions, mode-0
-// plane of each slot of h->field, and the probe's mode 0 on entry.
-void opr_step(ptyb_handle* h, const int* frames, int count) {
+// plane of each slot of h->field (the main-mode weights and the weights) and of `moved` (the
+// same taken back through the frames' moves, h->field without offsets: the residues), and the
+// probe's mode 0 on entry.
+void opr_step(ptyb_handle* h, const int* frames, int count, const float2* moved) {
   const int plane = h->N * h->N, k = h->opr_k;
   const size_t dstride = (size_t)h->K * plane;
   const unsigned pb = (unsigned)((plane + 255) / 256), pb32 = (unsigned)((plane + 31) / 32);
@@ -166,7 +270,7 @@ void opr_step(ptyb_handle* h, const int* frames, int count) {
   }
   if (k == 0 || count < 2) return;
   timed(h, kKOprStep, [&] {
-    opr_residue_kernel<<<pb32, 256, 0, h->stream>>>(h->field, dstride, count, plane, h->opr_r);
+    opr_residue_kernel<<<pb32, 256, 0, h->stream>>>(moved, dstride, count, plane, h->opr_r);
   });
   launched(h, "opr residues");
   const double a_u = std::min(0.1, (double)count / h->P);
@@ -230,17 +334,9 @@ void lsqml_batch(ptyb_handle* h, const ptyb_lsqml_params& p, const int* frames, 
   FrameArgs a = frame_args(h, frames);
   a.cost = p.cost;
   const bool opr = h->opr_on;
-  if (opr) {
-    // every frame's own probe (engine/opr.rs:88-120) in place of the shared one
-    opr_planes(h, frames, nslot, h->wave);
-    a.probe = h->wave;
-    a.probe_stride = pstride;
-  }
-  if (h->have_offsets) {
-    ensure_spec(h);
-    spectrum_of(h, h->probe, h->spec);
-    move_frames(h, frames, nslot, h->spec, h->wave);
-    a.probe = h->wave;
+  const float2* own = frame_probes(h, frames, nslot);
+  if (own) {
+    a.probe = own;
     a.probe_stride = pstride;
   }
   if (p.cost == PTYB_COST_POISSON) {
@@ -265,43 +361,20 @@ void lsqml_batch(ptyb_handle* h, const ptyb_lsqml_params& p, const int* frames, 
     ++h->launches;
   }
   GatherArgs g = gather_args(h, frames, nslot);
-  if (h->have_offsets || opr) {
-    g.probe = h->wave;
+  if (own) {
+    g.probe = own;
     g.probe_stride = pstride;
   }
   timed(h, kKObjLsqml, [&] { object_tile_kernel<kGatherLsqml><<<ntiles(h), 1024, 0, h->stream>>>(g); }, nslot);
   launched(h, "object direction");
-  if (opr) {
-    // each frame's probe direction conj(q·O)·χ (the OPR step reads mode 0), their mean dP
-    timed(h, kKProbePartial, [&] {
-      probe_terms_kernel<<<dim3((h->N * h->N + 255) / 256, nslot), 256, 0, h->stream>>>(
-          h->object, h->quad, h->upd, frames, h->corners, h->nxo, h->K, h->N, h->field);
-    });
-    launched(h, "probe terms");
-    timed(h, kKProbeFinal, [&] {
-      probe_finalize_kernel<<<(pstride + 255) / 256, 256, 0, h->stream>>>(
-          h->field, nslot, pstride, h->probe, h->d_probe, nullptr, 1.0f / nslot, 1);
-    });
-    launched(h, "probe direction");
-  } else if (h->have_offsets) {
-    timed(h, kKProbePartial, [&] {
-      probe_terms_kernel<<<dim3((h->N * h->N + 255) / 256, nslot), 256, 0, h->stream>>>(
-          h->object, h->quad, h->upd, frames, h->corners, h->nxo, h->K, h->N, h->field);
-    });
-    launched(h, "probe terms");
-    check(h, launch_move<kMoveBack>(h, move_args(h, frames, h->field), nslot), "probe move back");
-    ++h->launches;
-    timed(h, kKProbeFinal, [&] {
-      probe_finalize_kernel<<<(pstride + 255) / 256, 256, 0, h->stream>>>(
-          h->field, nslot, pstride, h->probe, h->d_probe, nullptr, 1.0f / nslot, 1);
-    });
-    launched(h, "probe direction");
-  } else {
+  const float2* dirs = nullptr;
+  if (own)
+    dirs = probe_directions(h, frames, nslot, h->quad, h->upd);
+  else
     probe_pass(h, frames, nslot, 1, 0.f, 1.0f / nslot);
-  }
   const double lambda0 = 1.2e-7 * ((double)h->N * h->N) / ((double)h->N * h->N);
-  const float2* fprobe = h->have_offsets || opr ? h->wave : h->probe;
-  const int fstride = h->have_offsets || opr ? pstride : 0;
+  const float2* fprobe = own ? own : h->probe;
+  const int fstride = own ? pstride : 0;
   timed(h, kKDots, [&] {
     lsqml_dots_kernel<<<nslot * kDotParts, 512, 0, h->stream>>>(h->object, h->d_obj, fprobe, h->d_probe,
                                                      h->quad, h->upd, frames, h->corners,
@@ -309,6 +382,9 @@ void lsqml_batch(ptyb_handle* h, const ptyb_lsqml_params& p, const int* frames, 
                                                      fstride);
   }, nslot);
   launched(h, "step sums");
+  // the eigenmodes and the refined weights from the state on entry (engine/lsqml.rs:620-621),
+  // before the window derivatives below take h->field, where the frame directions are
+  if (opr) opr_step(h, frames, nslot, dirs);
   const bool refine = h->have_offsets && h->refine_offsets;
   if (refine) {
     // position directions from the state on entry (engine/lsqml.rs:237-270)
@@ -325,8 +401,6 @@ void lsqml_batch(ptyb_handle* h, const ptyb_lsqml_params& p, const int* frames, 
                                                    frames, h->afar_all, log, h->scal + 2, 3);
   });
   launched(h, "step solve");
-  // the eigenmodes and the refined weights from the state on entry (engine/lsqml.rs:620-621)
-  if (opr) opr_step(h, frames, nslot);
   const size_t no = (size_t)h->nyo * h->nxo, np = (size_t)h->K * h->N * h->N;
   timed(h, kKAxpy, [&] {
     axpy_scal_kernel<<<(unsigned)((no + 255) / 256), 256, 0, h->stream>>>(h->object, h->d_obj,
@@ -401,9 +475,16 @@ int ptyb_lsqml(ptyb_handle* h, const ptyb_lsqml_params* p, int32_t nepoch, int32
         if (h->opr_on) {
           // the LLK of every frame's own probe (engine/lsqml.rs:537-551)
           const int stack = std::min(h->P, h->stack);
-          for (int s0 = 0; s0 < h->P; s0 += stack)
-            opr_planes(h, h->iota + s0, std::min(stack, h->P - s0),
-                       h->wave_all + (size_t)s0 * h->K * h->N * h->N);
+          for (int s0 = 0; s0 < h->P; s0 += stack) {
+            const int n = std::min(stack, h->P - s0);
+            float2* planes = h->wave_all + (size_t)s0 * h->K * h->N * h->N;
+            opr_planes(h, h->iota + s0, n, planes);
+            if (h->have_offsets) {
+              check(h, launch_move<kMoveOwn>(h, move_args(h, h->iota + s0, planes), n),
+                    "planes move");
+              ++h->launches;
+            }
+          }
           record(h, kAlgLsqml, llk_pass(h, h->wave_all));
         } else {
           record(h, kAlgLsqml, llk_pass(h));
@@ -452,10 +533,6 @@ int ptyb_set_probe_variation(ptyb_handle* h, const double* eigenmodes, int32_t k
   }
   if (intensity && k == 0) {
     h->err = "main-mode weights need an eigenmode";
-    return PTYB_INVALID;
-  }
-  if (h->nslice > 1 || h->have_offsets) {
-    h->err = "the probe variation runs on a single slice without the position model";
     return PTYB_INVALID;
   }
   return guarded(h, true, [&]() -> int {

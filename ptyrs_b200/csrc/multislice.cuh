@@ -132,7 +132,8 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T, frame_min_blocks<N, C>())
       const int ny = (r * H + yl + N / 2) % N, nx = (jx + N / 2) % N;
       for (int m = 0; m < K; ++m) {
         const int line = m * H + yl;
-        S[line * L + (jx ^ swz(line))] = a.probe[((size_t)m * N + ny) * N + nx];
+        S[line * L + (jx ^ swz(line))] =
+            a.probe[(size_t)slot * a.probe_stride + ((size_t)m * N + ny) * N + nx];
       }
     }
     __syncthreads();
@@ -263,7 +264,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T, frame_min_blocks<N, C>())
     for (int m = 0; m < K; ++m) {
       const int line = m * H + yl;
       const size_t pi = ((size_t)m * N + ny) * N + nx;
-      const float2 in = in_last ? in_last[pi] : a.probe[pi];
+      const float2 in = in_last ? in_last[pi] : a.probe[(size_t)slot * a.probe_stride + pi];
       float2& v = S[line * L + (jx ^ swz(line))];
       v = csub(v, cmul(in, oq));
     }

@@ -16,7 +16,9 @@ enum MoveMode : int {
   kDerivSums = 6,     // per frame and axis, the position sums of AP, DM and ML from ∂T_d(q·P)
   kBackSpectrum = 7,  // planes[slot][m] = DFT(conj(O_win)·c_m)·exp(+2πi f·d)/N², [ky][kx]: one
                       // frame's term of the probe back-projection through the move's adjoint
-  kPlainInverse = 8   // planes[m] = conj(q)·IDFT(spec_m), unnormalised (one slot)
+  kPlainInverse = 8,  // planes[m] = conj(q)·IDFT(spec_m), unnormalised (one slot)
+  kMoveOwn = 9        // planes[slot][m] = conj(q)·T_d(q·planes), in place: each frame's own
+                      // probe planes (the probe variation's) moved by its offset
 };
 
 struct MoveArgs {
@@ -70,7 +72,8 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
   float2* out = a.planes + (size_t)slot * K * plane;
   constexpr float inv_n2 = 1.0f / ((float)N * (float)N);
   constexpr bool from_spec = MODE == kFromSpectrum || MODE == kDerivSums || MODE == kPlainInverse;
-  constexpr bool moves = MODE == kMoveBack || MODE == kFromSpectrum || MODE == kDerivSums ||
+  constexpr bool in_place = MODE == kMoveBack || MODE == kMoveOwn;
+  constexpr bool moves = in_place || MODE == kFromSpectrum || MODE == kDerivSums ||
                          MODE == kBackSpectrum;
   constexpr bool bare = MODE == kDerivWindow;
 
@@ -102,7 +105,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
     for (int idx = tid; idx < H * N; idx += T) {
       const int yl = idx / N, x = idx % N, y = r * H + yl;
       float2 w;
-      if (MODE == kSpectrum || MODE == kMoveBack)
+      if (MODE == kSpectrum || in_place)
         w = a.quad[y * N + x];
       else if (MODE == kBackSpectrum)
         w = cconj(a.object[(size_t)(corner.x + y) * a.nxo + corner.y + x]);
@@ -110,7 +113,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
         float2 v;
         if (MODE == kSpectrum)
           v = cmul(w, a.probe[m * plane + y * N + x]);
-        else if (MODE == kMoveBack)
+        else if (in_place)
           v = cmul(w, out[m * plane + y * N + x]);
         else if (MODE == kBackSpectrum) {
           float2 cv = a.c[(size_t)slot * K * plane + m * plane + y * N + x];

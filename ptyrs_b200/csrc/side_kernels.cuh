@@ -74,6 +74,7 @@ cudaError_t move_modes(int mode, const MoveArgs& a, int nslot, int K, cudaStream
       return launch_clusters<N, C>(move_kernel<N, C, kBackSpectrum>, a, nslot, smem, s);
     case kPlainInverse:
       return launch_clusters<N, C>(move_kernel<N, C, kPlainInverse>, a, nslot, smem, s);
+    case kMoveOwn: return launch_clusters<N, C>(move_kernel<N, C, kMoveOwn>, a, nslot, smem, s);
   }
   return cudaErrorInvalidValue;
 }
@@ -136,6 +137,13 @@ template <int N>
 cudaError_t SideKernels<N>::gamma(const GammaArgs& a, int nslot, cudaStream_t s) {
   constexpr int C = gamma_cluster(N);
   return launch_clusters<N, C>(gamma_kernel<N, C>, a, nslot, gamma_smem_bytes<N, C>(), s, true);
+}
+
+template <int N>
+cudaError_t SideKernels<N>::bh(const BhArgs& a, int nslot, cudaStream_t s) {
+  constexpr int C = gamma_cluster(N);
+  return launch_clusters<N, C>(bh_hessian_kernel<N, C>, a, nslot, bh_smem_bytes<N, C>(), s,
+                               true);
 }
 
 }  // namespace ptyb

@@ -1,7 +1,7 @@
 """pty-chi's multislice object on the CUDA path against the f64 oracle (oracle.lsqml with a list
 of slices, itself pinned to the reference's golden multislice runs): the LLK through the slices,
-LSQML epochs with every slice's step sizes, every slice and the probe, on the far field of
-three slices with two unequal angular-spectrum gaps. Frame sides 64, 128 and 256 run the
+LSQML epochs with every slice's step sizes, every slice and the probe, with and without the
+position model, on the far field of three slices with two unequal angular-spectrum gaps. Frame sides 64, 128 and 256 run the
 cluster sizes 1, 2 and 16."""
 import numpy as np
 import pytest
@@ -135,8 +135,9 @@ def test_multislice_refuses_other_algorithms(case):
             g.ml(1)
         with pytest.raises(PtybError):
             g.forward_intensity([0])
+        g.set_positions(np.zeros((len(case["counts"]), 2)))
         with pytest.raises(PtybError):
-            g.set_positions(np.zeros((len(case["counts"]), 2)))
+            g.gradients(positions=False)  # not built through slices under the position model
         # the handle still runs LSQML after the refusals
         g.lsqml(1, batch_size=8)
         assert np.isfinite(g.objects()).all()
@@ -178,3 +179,41 @@ def test_gradients_through_slices_match_oracle(case):
         t.backward()
         assert np.array_equal(o.grad.numpy(), got["object"])
         assert np.array_equal(p.grad.numpy(), got["probe"])
+
+
+@pytest.mark.parametrize("refine", [False, True], ids=["held", "refined"])
+def test_lsqml_epochs_through_slices_with_positions(case, refine):
+    """Two epochs of batches of 8 under the position model (Patch): every frame's probe moved
+    by its sub-pixel offset before slice 0, the probe directions moved back, and with
+    refinement pty-chi's position step on the middle slice (oracle pinned to the reference's
+    `lsqml_multislice_pos` set): steps, slices, probe, offsets and the LLK."""
+    nframe = len(case["counts"])
+    d0 = np.random.default_rng(5).uniform(-0.5, 0.5, (nframe, 2))
+    cpu = oracle_of(case)
+    run = Lsqml(8, "poisson", 7, offsets=d0.copy(), refine=refine)
+    objs, probe, steps = list(case["objects"]), cpu.probe, None
+    for _ in range(2):
+        objs, probe, steps = run.epoch(cpu.addr, cpu.obs, cpu.optics, objs, probe)
+    with gpu_of(case) as g:
+        g.set_positions(d0, refine=refine)
+        g.lsqml(2, batch_size=8, cost="poisson", seed=7)
+        got = g.lsqml_steps()
+        assert [s["frames"] for s in got] == [s["frames"] for s in steps]
+        for gs, cs in zip(got, steps):
+            a, b = np.array(gs["a_probe"]), np.array(cs["a_probe"])
+            assert np.abs(a - b).max() <= RUN_TOL * np.abs(b).max() + 1e-30
+            for k in range(3):
+                a, b = np.array(gs["a_obj"][k]), np.array(cs["a_obj"][k])
+                assert np.abs(a - b).max() <= RUN_TOL * np.abs(b).max() + 1e-30, ("a_obj", k)
+        got_objs = g.objects()
+        for k in range(3):
+            assert rel_l2(got_objs[k] - 1.0, objs[k][0] - 1.0) < RUN_TOL, k
+        assert rel_l2(g.probe(), probe) < RUN_TOL
+        d = g.positions()
+        if refine:
+            assert rel_l2(d - d0, run.offsets - d0) < RUN_TOL
+            assert np.abs(d - d0).max() > 0
+        else:
+            assert np.array_equal(d, d0)
+        ref = run.llk(cpu.addr, cpu.obs, cpu.optics, objs, probe)
+        assert abs(g.llk()["poisson"] - ref.poisson) <= RUN_TOL * abs(ref.poisson)

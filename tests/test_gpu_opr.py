@@ -3,13 +3,13 @@ every frame's own probe c_f·P_0 + Σ_i w_fi·U_i, and each batch's step of the 
 refined weights) through the C ABI against the f64 oracle (`Lsqml(var=...)`, pinned to the
 reference's golden OPR sets): two epochs, the object, the probe, the eigenmodes, the weights,
 the main mode's weights and the LLK of every frame's own probe, to the reference's GPU-vs-CPU
-1e-4."""
+1e-4; with the position model (held and refined offsets) and through a multislice object."""
 import numpy as np
 import pytest
 
 from oracle.lsqml import Lsqml
 from oracle.opr import ProbeVariation
-from ptyrs_b200 import GpuPtycho, PtybError, Scan, sim
+from ptyrs_b200 import GpuPtycho, Scan, sim
 from scenarios import far_field, oracle_state, rel_l2
 
 pytestmark = pytest.mark.gpu
@@ -75,13 +75,64 @@ def test_lsqml_with_opr(case, cost, intensity, refine_w):
         assert abs(got - ref.poisson) <= RUN_TOL * abs(ref.poisson)
 
 
-def test_opr_refuses_the_position_model(case):
-    u, w = start_variation(case, 1)
+@pytest.mark.parametrize("refine", [False, True], ids=["held", "refined"])
+def test_lsqml_with_opr_and_positions(case, refine):
+    """The probe variation under the position model (reference GPU engine/gpu/lsqml.rs:63-121,
+    oracle pinned to the reference's `lsqml_pos_opr` set): every frame's own planes moved by
+    its offset, the OPR step from the raw and the moved-back frame directions; two epochs, the
+    object, probe, eigenmodes, weights, main-mode weights, offsets and the LLK."""
+    nframe = len(case["counts"])
+    u, w = start_variation(case, 2)
+    c = np.linspace(0.9, 1.1, nframe)
+    d0 = np.random.default_rng(7).uniform(-0.5, 0.5, (nframe, 2))
+    var = ProbeVariation(u, w.ravel(), intensity=c)
+    cpu = oracle_state(case)
+    run = Lsqml(8, "poisson", 7, offsets=d0.copy(), refine=refine, var=var)
+    obj, probe = cpu.object, cpu.probe
+    for _ in range(2):
+        obj, probe, _ = run.epoch(cpu.addr, cpu.obs, cpu.optics, obj, probe)
+    ref = run.llk(cpu.addr, cpu.obs, cpu.optics, obj, probe)
     with gpu_of(case) as g:
+        g.set_probe_variation(u, w, intensity=c)
+        g.set_positions(d0, refine=refine)
+        g.lsqml(2, batch_size=8, cost="poisson", seed=7, calc_llk=1)
+        assert rel_l2(g.object(), obj) < RUN_TOL
+        assert rel_l2(g.probe(), probe) < RUN_TOL
+        gu, gw, gc = g.probe_variation()
+        assert rel_l2(gu, var.eigenmodes) < RUN_TOL
+        want_w = var.weights.reshape(nframe, 2)
+        assert np.abs(gw - want_w).max() <= RUN_TOL * np.abs(want_w - w).max() + 1e-12
+        assert np.abs(gc - var.intensity).max() <= RUN_TOL * np.abs(var.intensity - c).max() + 1e-12
+        d = g.positions()
+        if refine:
+            assert rel_l2(d - d0, run.offsets - d0) < RUN_TOL
+        else:
+            assert np.array_equal(d, d0)
+        got = g.history()["poisson"][-1]
+        assert abs(got - ref.poisson) <= RUN_TOL * abs(ref.poisson)
+
+
+def test_lsqml_with_opr_through_slices():
+    """The probe variation on a multislice object: every frame's own planes enter slice 0, the
+    OPR step on slice 0 (engine/lsqml.rs:571-643), against the oracle over two epochs."""
+    from test_gpu_multislice import gpu_of as ms_gpu_of, multislice_scan, oracle_of
+    s = multislice_scan(64, 2, 30, 192, (2e-6, 3e-6), seed=9)
+    nframe = len(s["counts"])
+    u, w = start_variation(dict(probe=s["probe"], counts=s["counts"]), 2)
+    var = ProbeVariation(u, w.ravel())
+    cpu = oracle_of(s)
+    run = Lsqml(8, "poisson", 7, var=var)
+    objs, probe = list(s["objects"]), cpu.probe
+    for _ in range(2):
+        objs, probe, _ = run.epoch(cpu.addr, cpu.obs, cpu.optics, objs, probe)
+    with ms_gpu_of(s) as g:
         g.set_probe_variation(u, w)
-        with pytest.raises(PtybError):
-            g.set_positions(np.zeros((len(case["counts"]), 2)))
-        g.set_probe_variation(None, None)
-        g.set_positions(np.zeros((len(case["counts"]), 2)))
-        with pytest.raises(PtybError):
-            g.set_probe_variation(u, w)
+        g.lsqml(2, batch_size=8, cost="poisson", seed=7)
+        got = g.objects()
+        for k in range(3):
+            assert rel_l2(got[k] - 1.0, objs[k][0] - 1.0) < RUN_TOL, k
+        assert rel_l2(g.probe(), probe) < RUN_TOL
+        gu, gw, _ = g.probe_variation()
+        assert rel_l2(gu, var.eigenmodes) < RUN_TOL
+        want_w = var.weights.reshape(nframe, 2)
+        assert np.abs(gw - want_w).max() <= RUN_TOL * np.abs(want_w - w).max() + 1e-12
