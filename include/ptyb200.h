@@ -106,8 +106,8 @@ typedef struct ptyb_llk {
 } ptyb_llk;
 
 /* Reference `LlkRecord` (engine/ptycho.rs:36-41); algorithm 0 = AP, 1 = DM, 2 = RAAR,
- * 3 = rPIE, 4 = ML, 6 = LSQML (the reference's `Algorithm` order Ap, Dm, Raar, Rpie, Ml, Bh,
- * Lsqml). */
+ * 3 = rPIE, 4 = ML, 5 = BH, 6 = LSQML (the reference's `Algorithm` order Ap, Dm, Raar, Rpie,
+ * Ml, Bh, Lsqml). */
 typedef struct ptyb_llk_record {
   int64_t cycle;
   int32_t algorithm;
@@ -120,6 +120,23 @@ typedef struct ptyb_lsqml_step {
   int32_t batch, frame;
   double a_far, a_obj, a_probe;
 } ptyb_lsqml_step;
+
+/* Reference `BhParams` (engine/bh.rs:29-49): frames per batch (one batch of every frame runs
+ * conjugate directions across epochs, smaller batches steepest descent), pty-chi's probe
+ * `rho` (the probe variable is the probe over rho·√k), the offsets' rho (the reference's
+ * layout; BH here runs without the position model) and the batches' seed. */
+typedef struct ptyb_bh_params {
+  int32_t batch_size, pad_;
+  double probe_rho, position_rho;
+  uint64_t seed;
+} ptyb_bh_params;
+
+/* One batch's BH step (reference `BhStep`, engine/bh.rs:58-70): its place in the epoch, its
+ * frame count, the conjugate weight beta, the step alpha, −⟨g, D⟩ and H(D, D). */
+typedef struct ptyb_bh_step {
+  int32_t batch, count;
+  double beta, alpha, top, bottom;
+} ptyb_bh_step;
 
 typedef struct ptyb_handle ptyb_handle;
 
@@ -221,6 +238,12 @@ int ptyb_get_llk(ptyb_handle* h, ptyb_llk* out);
  * slice and d_obj is every slice's gradient, [nslice][nyo][nxo] (d_pos must be NULL). The
  * handle's arrays are not changed. */
 int ptyb_gradients(ptyb_handle* h, double* loss, double* d_obj, double* d_probe, double* d_pos);
+/* ptyb_gradients with the object and probe gradients written as complex64 (interleaved float
+ * re, im) to device memory of the handle's device, d_obj [nslice][nyo][nxo] and d_probe
+ * [nprobe][ny][nx] (either NULL to skip), the torch function's path; loss and d_pos on the
+ * host as there. No counterpart in the reference. */
+int ptyb_gradients_device(ptyb_handle* h, double* loss, void* d_obj, void* d_probe,
+                          double* d_pos);
 
 /* The model intensity Σ_modes |Ψ|² of the current estimate for frames[0..n) into out[n][ny][nx]
  * in the FFT-shifted detector layout (zero frequency at [0, 0]), the far-field forward model of
@@ -252,11 +275,35 @@ int ptyb_forward_intensity_noalloc(ptyb_handle* h, const int32_t* frames, int32_
 int ptyb_set_positions(ptyb_handle* h, const double* offsets, int32_t refine);
 int ptyb_get_positions(ptyb_handle* h, double* dst);
 
+/* Reference `GpuPtycho::bh` (engine/gpu/bh.rs:29-66; CPU twin `Bh::epoch`, engine/bh.rs:
+ * 645-760): pty-chi's bilinear-Hessian method on the amplitude cost, `nepoch` epochs from a
+ * fresh run (epoch e's batches `random_batches(nframe, batch_size, seed, e)`), every batch
+ * moving object and probe by α·D; an LLK record after every due epoch (calc_llk as
+ * ptyb_lsqml's). One object slice without the position model (PTYB_INVALID otherwise). */
+int ptyb_bh(ptyb_handle* h, const ptyb_bh_params* p, int32_t nepoch, int32_t calc_llk);
+/* Reference `GpuPtycho::bh_steps` (engine/gpu/bh.rs:68-72): the last epoch's steps. */
+int ptyb_bh_steps_len(ptyb_handle* h);
+int ptyb_bh_steps(ptyb_handle* h, ptyb_bh_step* dst, int32_t cap);
+
 /* Reference `GpuPtycho::{object, probe, set_object}` (engine/gpu/mod.rs:763-817). */
 int ptyb_get_object(ptyb_handle* h, double* dst);
 int ptyb_get_probe(ptyb_handle* h, double* dst);
 int ptyb_set_object(ptyb_handle* h, const double* src);
 int ptyb_set_probe(ptyb_handle* h, const double* src);
+
+/* Reference `GpuPtycho::set_object_device` (engine/gpu/mod.rs:795-805): the object (of a
+ * multislice object its first slice) from `src`, complex64 [nobj][nyo][nxo] (interleaved
+ * float re, im) in device memory of the handle's device whose writes have finished; the copy
+ * is waited for, so `src` may be released or rewritten on return. PTYB_INVALID, changing
+ * nothing, when the dims differ from the handle's or `src` is not memory of that device. */
+int ptyb_set_object_device(ptyb_handle* h, int32_t nobj, int32_t nyo, int32_t nxo,
+                           const void* src);
+/* No counterpart in the reference: as ptyb_set_object_device for every slice
+ * ([nslice][nyo][nxo]) and for the probe ([nprobe][ny][nx]). */
+int ptyb_set_objects_device(ptyb_handle* h, int32_t nslice, int32_t nyo, int32_t nxo,
+                            const void* src);
+int ptyb_set_probe_device(ptyb_handle* h, int32_t nprobe, int32_t ny, int32_t nx,
+                          const void* src);
 
 /* Window corners [nframe][2] (oy, ox) of the address table (reference `AddrTable`,
  * base/addr.rs:35-81). */

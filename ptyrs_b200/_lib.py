@@ -67,6 +67,16 @@ class LsqmlStep(ctypes.Structure):
                 ("a_probe", c_double)]
 
 
+class BhParams(ctypes.Structure):
+    _fields_ = [("batch_size", c_int32), ("pad_", c_int32), ("probe_rho", c_double),
+                ("position_rho", c_double), ("seed", ctypes.c_uint64)]
+
+
+class BhStep(ctypes.Structure):
+    _fields_ = [("batch", c_int32), ("count", c_int32), ("beta", c_double), ("alpha", c_double),
+                ("top", c_double), ("bottom", c_double)]
+
+
 # Every symbol include/ptyb200.h declares, with (restype, argtypes).
 SIGNATURES = {
     "ptyb_create": (c_int32, [P(Scan), P(c_double), c_int32, c_int32, c_int32, P(c_double),
@@ -80,6 +90,9 @@ SIGNATURES = {
     "ptyb_lsqml": (c_int32, [c_void_p, P(LsqmlParams), c_int32, c_int32]),
     "ptyb_ml": (c_int32, [c_void_p, P(MlParams), c_int32]),
     "ptyb_ap": (c_int32, [c_void_p, P(ApParams), c_int32]),
+    "ptyb_bh": (c_int32, [c_void_p, P(BhParams), c_int32, c_int32]),
+    "ptyb_bh_steps_len": (c_int32, [c_void_p]),
+    "ptyb_bh_steps": (c_int32, [c_void_p, P(BhStep), c_int32]),
     "ptyb_dm": (c_int32, [c_void_p, P(DmParams), c_int32]),
     "ptyb_raar": (c_int32, [c_void_p, P(RaarParams), c_int32]),
     "ptyb_set_probe_variation": (c_int32, [c_void_p, P(c_double), c_int32, P(c_double), c_int32,
@@ -99,6 +112,11 @@ SIGNATURES = {
     "ptyb_get_probe": (c_int32, [c_void_p, P(c_double)]),
     "ptyb_set_object": (c_int32, [c_void_p, P(c_double)]),
     "ptyb_set_probe": (c_int32, [c_void_p, P(c_double)]),
+    "ptyb_set_object_device": (c_int32, [c_void_p, c_int32, c_int32, c_int32, c_void_p]),
+    "ptyb_set_objects_device": (c_int32, [c_void_p, c_int32, c_int32, c_int32, c_void_p]),
+    "ptyb_set_probe_device": (c_int32, [c_void_p, c_int32, c_int32, c_int32, c_void_p]),
+    "ptyb_gradients_device": (c_int32, [c_void_p, P(c_double), c_void_p, c_void_p,
+                                        P(c_double)]),
     "ptyb_corners": (c_int32, [c_void_p, P(c_int32)]),
     "ptyb_history_len": (c_int32, [c_void_p]),
     "ptyb_history": (c_int32, [c_void_p, P(LlkRecord), c_int32]),

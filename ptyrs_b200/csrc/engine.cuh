@@ -42,7 +42,8 @@ namespace ptyb::eng {
 // Devices a process may use (per-device tables of the pool and the no-alloc scratch).
 constexpr int kMaxDevices = 64;
 
-constexpr int kAlgAp = 0, kAlgDm = 1, kAlgRaar = 2, kAlgRpie = 3, kAlgMl = 4, kAlgLsqml = 6;
+constexpr int kAlgAp = 0, kAlgDm = 1, kAlgRaar = 2, kAlgRpie = 3, kAlgMl = 4, kAlgLsqml = 6,
+              kAlgBh = 5;
 
 // One device allocation, freed with the handle.
 struct Buf {
@@ -143,6 +144,7 @@ struct ptyb_handle {
   double* opr_c = nullptr;       // [P]
   float* opr_vv = nullptr;       // [slots][N][N]
   float2* opr_r = nullptr;       // [slots][N][N]
+  float2* opr_moved = nullptr;   // [slots][K][N][N] frame probe directions moved back
   float2* opr_e = nullptr;       // [N][N]
   double* opr_sums = nullptr;    // [slots][3]
   double* opr_p = nullptr;       // [slots]
@@ -175,6 +177,7 @@ struct ptyb_handle {
   std::vector<ptyb_llk_record> history;
   std::vector<ptyb_lsqml_step> steps;
   std::vector<double> slice_steps;  // [frame of the last epoch][slice 1..]: a_obj
+  std::vector<ptyb_bh_step> bh_steps;  // the last BH epoch's steps
   int log_stride = 3;
   bool aborted = false;
   std::string err;
@@ -196,6 +199,8 @@ cudaError_t copy_sync(ptyb_handle* h, void* dst, const void* src, size_t bytes,
                       cudaMemcpyKind kind);
 cudaError_t fill_sync(ptyb_handle* h, void* dst, int value, size_t bytes);
 void launched(ptyb_handle* h, const char* what);
+// Whether `p` is device (or managed) memory of the handle's device.
+bool on_device(ptyb_handle* h, const void* p);
 
 // `count` elements of T from the device pool, freed with the handle.
 template <typename T>
@@ -214,7 +219,8 @@ enum Kind : int {
   kKObjRpie, kKObjOverlap, kKObjLsqml, kKObjMl, kKIllum, kKProbePartial, kKProbeFinal,
   kKAfar, kKDots, kKSolve, kKAxpy, kKMax, kKCounts, kKMisc, kKGamma, kKArraySums, kKMove,
   kKPositionSums, kKSliceForward, kKSliceBackward, kKSliceLlk, kKFrameProject, kKSpectrum,
-  kKDerivSums, kKBackSpectrum, kKSliceGrad, kKFrameCarry, kKObjBlend, kKOprStep, kNumKinds
+  kKDerivSums, kKBackSpectrum, kKSliceGrad, kKFrameCarry, kKObjBlend, kKOprStep, kKBhHessian,
+  kNumKinds
 };
 static_assert(kNumKinds <= kMaxKinds, "the timing arrays hold kMaxKinds kinds");
 extern const char* const kKindNames[kNumKinds];

@@ -29,7 +29,8 @@ namespace ptyb {
 enum FrameMode : int {
   kRpie = 0,       // rPIE modulus; out = Δ = ψ' − ψ
   kLsqmlFused = 1, // LSQML residual from a per-frame a_far; out = χ = ψ' − ψ
-  kMlGrad = 2,     // Poisson gradient 2(1 − I/Ĩ), masked 0; out = ψ'
+  kMlGrad = 2,     // Poisson gradient 2(1 − I/Ĩ) (BH's amplitude one with cost amplitude),
+                   // masked 0; out = ψ'
   kLlk = 3,        // forward only; per-frame LLK sums
   kStore = 4,      // forward only; detector field and Σ_modes |Ψ|² to global
   kFromStore = 5,  // detector field from global; LSQML residual; out = χ
@@ -389,7 +390,12 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
       // ApplyAmplitude (engine/ops.rs:83-107)
       fac = masked ? 1.f : sqrtf(yo) / fmaxf(sqrtf(ic), 1e-12f);
     } else if (MODE == kMlGrad) {
-      fac = masked ? 0.f : 2.f * (1.f - yo / fmaxf(ic, 1e-12f));
+      // Poisson: GradPoissonFourier (engine/ops.rs:161-195); amplitude: BH's 2·(1 − √I/A)
+      // with A = √Ĩ + 1e-8 (engine/bh.rs:255-265)
+      if (a.cost == kCostAmplitude)
+        fac = masked ? 0.f : 2.f * (1.f - sqrtf(yo) / (sqrtf(ic) + 1e-8f));
+      else
+        fac = masked ? 0.f : 2.f * (1.f - yo / fmaxf(ic, 1e-12f));
     } else {
       float cres = 0.f;
       if (!masked)

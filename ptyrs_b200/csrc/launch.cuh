@@ -3,6 +3,7 @@
 // sequencing compiles none of these kernels. Each function launches `nslot` frames, C CTAs per
 // frame, on stream `s`; cudaErrorInvalidValue for a side, cluster size or mode not built.
 #pragma once
+#include "bh.cuh"
 #include "frame.cuh"
 #include "ml.cuh"
 #include "multislice.cuh"
@@ -18,6 +19,8 @@ cudaError_t launch_slice_side(int N, int C, int mode, const SliceArgs& a, int ns
                               cudaStream_t s);
 // The line search's kernel at its one cluster size per side (gamma_cluster).
 cudaError_t launch_gamma_side(int N, const GammaArgs& a, int nslot, cudaStream_t s);
+// BH's bilinear Hessian at the line search's cluster size.
+cudaError_t launch_bh_side(int N, const BhArgs& a, int nslot, cudaStream_t s);
 constexpr int gamma_cluster(int N) {
   return N == 64 ? 1 : N == 96 ? 2 : N == 128 ? 4 : N == 192 ? 8 : 16;
 }
@@ -29,6 +32,7 @@ struct SideKernels {
   static cudaError_t move(int C, int mode, const MoveArgs& a, int nslot, int K, cudaStream_t s);
   static cudaError_t slice(int C, int mode, const SliceArgs& a, int nslot, int K, cudaStream_t s);
   static cudaError_t gamma(const GammaArgs& a, int nslot, cudaStream_t s);
+  static cudaError_t bh(const BhArgs& a, int nslot, cudaStream_t s);
 };
 extern template struct SideKernels<64>;
 extern template struct SideKernels<96>;

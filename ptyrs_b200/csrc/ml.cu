@@ -240,6 +240,67 @@ void ml_gamma(ptyb_handle* h, double* num, double* den) {
   }
 }
 
+// The Poisson sum and its gradients of the handle's state (ptyb_gradients): object and probe
+// gradients handed to `sink(g_obj, g_probe, object elements, probe elements)` on the device,
+// the position gradient to host d_pos.
+template <typename Sink>
+int gradients_to(ptyb_handle* h, double* loss, bool want_obj, bool want_probe, double* d_pos,
+                 Sink&& sink) {
+  if (!h) return PTYB_INVALID;
+  if (h->nslice > 1 && (d_pos || h->have_offsets)) {
+    h->err = "gradients through slices run without the position model";
+    return PTYB_INVALID;
+  }
+  if (h->nslice > 1)
+    return guarded(h, true, [&]() -> int {
+      slice_gradients(h, want_obj, want_probe);
+      const ptyb_llk l = llk_pass(h);
+      if (loss) *loss = l.poisson * h->nb_obs;
+      const size_t np = (size_t)h->K * h->N * h->N;
+      const size_t no = (size_t)h->nslice * h->nyo * h->nxo;
+      sink(h->g_slices, h->g_probe, no, np);
+      return PTYB_OK;
+    });
+  if (d_pos && !h->have_offsets) {
+    h->err = "position gradients need position offsets (ptyb_set_positions)";
+    return PTYB_INVALID;
+  }
+  return guarded(h, true, [&]() -> int {
+    ensure_slots(h, std::min(h->P, h->stack));
+    ensure_ml(h);
+    const size_t np = (size_t)h->K * h->N * h->N, no = (size_t)h->nyo * h->nxo;
+    if (h->have_offsets) {
+      ensure_spec(h);
+      if (!h->wave_all) h->wave_all = alloc<float2>(h, (size_t)h->P * np);
+      if (h->wave2_slots < h->slots) {
+        h->wave2 = alloc<float2>(h, (size_t)h->slots * np);
+        h->wave2_slots = h->slots;
+      }
+      if (!h->ml_pos_sums) h->ml_pos_sums = alloc<double>(h, (size_t)h->P * 4);
+      spectrum_of(h, h->probe, h->spec);
+      const int stack = std::min(h->P, h->stack);
+      for (int s0 = 0; s0 < h->P; s0 += stack)
+        move_frames(h, h->iota + s0, std::min(stack, h->P - s0), h->spec,
+                    h->wave_all + (size_t)s0 * np);
+    }
+    ml_gradients(h, want_obj, want_probe, false, d_pos != nullptr);
+    const ptyb_llk l = llk_pass(h, h->have_offsets ? h->wave_all : nullptr);
+    if (loss) *loss = l.poisson * h->nb_obs;
+    sink(h->g_obj, h->g_probe, no, np);
+    if (d_pos) {
+      std::vector<double> v((size_t)h->P * 4);
+      check(h, copy_sync(h, v.data(), h->ml_pos_sums, v.size() * sizeof(double),
+                          cudaMemcpyDeviceToHost),
+            "gradient");
+      for (int f = 0; f < h->P; ++f) {
+        d_pos[2 * f] = v[(size_t)f * 4];
+        d_pos[2 * f + 1] = v[(size_t)f * 4 + 1];
+      }
+    }
+    return PTYB_OK;
+  });
+}
+
 }  // namespace
 }  // namespace ptyb::eng
 
@@ -356,69 +417,31 @@ int ptyb_ml(ptyb_handle* h, const ptyb_ml_params* p, int32_t ncycle) {
 }
 
 int ptyb_gradients(ptyb_handle* h, double* loss, double* d_obj, double* d_probe, double* d_pos) {
+  return gradients_to(h, loss, d_obj != nullptr, d_probe != nullptr, d_pos,
+                      [&](const float2* g_obj, const float2* g_probe, size_t no, size_t np) {
+                        if (d_obj) download_c64(h, g_obj, d_obj, no, "gradient");
+                        if (d_probe) download_c64(h, g_probe, d_probe, np, "gradient");
+                      });
+}
+
+int ptyb_gradients_device(ptyb_handle* h, double* loss, void* d_obj, void* d_probe,
+                          double* d_pos) {
   if (!h) return PTYB_INVALID;
-  if (h->nslice > 1 && d_pos) {
-    h->err = "position gradients run on a single-slice object";
+  if ((d_obj && !on_device(h, d_obj)) || (d_probe && !on_device(h, d_probe))) {
+    h->err = "gradient outputs must be device memory of the handle's device";
     return PTYB_INVALID;
   }
-  if (h->nslice > 1)
-    return guarded(h, true, [&]() -> int {
-      slice_gradients(h, d_obj != nullptr, d_probe != nullptr);
-      const ptyb_llk l = llk_pass(h);
-      if (loss) *loss = l.poisson * h->nb_obs;
-      const size_t np = (size_t)h->K * h->N * h->N;
-      const size_t no = (size_t)h->nslice * h->nyo * h->nxo;
-      if (d_obj) {
-        download_c64(h, h->g_slices, d_obj, no, "gradient");
-      }
-      if (d_probe) {
-        download_c64(h, h->g_probe, d_probe, np, "gradient");
-      }
-      return PTYB_OK;
-    });
-  if (d_pos && !h->have_offsets) {
-    h->err = "position gradients need position offsets (ptyb_set_positions)";
-    return PTYB_INVALID;
-  }
-  return guarded(h, true, [&]() -> int {
-    ensure_slots(h, std::min(h->P, h->stack));
-    ensure_ml(h);
-    const size_t np = (size_t)h->K * h->N * h->N, no = (size_t)h->nyo * h->nxo;
-    if (h->have_offsets) {
-      ensure_spec(h);
-      if (!h->wave_all) h->wave_all = alloc<float2>(h, (size_t)h->P * np);
-      if (h->wave2_slots < h->slots) {
-        h->wave2 = alloc<float2>(h, (size_t)h->slots * np);
-        h->wave2_slots = h->slots;
-      }
-      if (!h->ml_pos_sums) h->ml_pos_sums = alloc<double>(h, (size_t)h->P * 4);
-      spectrum_of(h, h->probe, h->spec);
-      const int stack = std::min(h->P, h->stack);
-      for (int s0 = 0; s0 < h->P; s0 += stack)
-        move_frames(h, h->iota + s0, std::min(stack, h->P - s0), h->spec,
-                    h->wave_all + (size_t)s0 * np);
-    }
-    ml_gradients(h, d_obj != nullptr, d_probe != nullptr, false, d_pos != nullptr);
-    const ptyb_llk l = llk_pass(h, h->have_offsets ? h->wave_all : nullptr);
-    if (loss) *loss = l.poisson * h->nb_obs;
-    if (d_obj) {
-      download_c64(h, h->g_obj, d_obj, no, "gradient");
-    }
-    if (d_probe) {
-      download_c64(h, h->g_probe, d_probe, np, "gradient");
-    }
-    if (d_pos) {
-      std::vector<double> v((size_t)h->P * 4);
-      check(h, copy_sync(h, v.data(), h->ml_pos_sums, v.size() * sizeof(double),
-                          cudaMemcpyDeviceToHost),
-            "gradient");
-      for (int f = 0; f < h->P; ++f) {
-        d_pos[2 * f] = v[(size_t)f * 4];
-        d_pos[2 * f + 1] = v[(size_t)f * 4 + 1];
-      }
-    }
-    return PTYB_OK;
-  });
+  return gradients_to(h, loss, d_obj != nullptr, d_probe != nullptr, d_pos,
+                      [&](const float2* g_obj, const float2* g_probe, size_t no, size_t np) {
+                        if (d_obj)
+                          check(h, copy_sync(h, d_obj, g_obj, no * sizeof(float2),
+                                             cudaMemcpyDeviceToDevice),
+                                "gradient");
+                        if (d_probe)
+                          check(h, copy_sync(h, d_probe, g_probe, np * sizeof(float2),
+                                             cudaMemcpyDeviceToDevice),
+                                "gradient");
+                      });
 }
 
 }  // extern "C"

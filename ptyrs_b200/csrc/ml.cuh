@@ -127,7 +127,8 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T, 2) gamma_kernel(GammaArgs
 }
 
 // Per block, in double: mode 0 Σ Re(conj(g)·(g − h)) and Σ |h|² (Polak–Ribière);
-// mode 1 Σ |g| (the modulus sum of scale_obj_probe). Partial sums [block][2].
+// mode 1 Σ |g| (the modulus sum of scale_obj_probe); mode 2 Σ Re(conj(g)·h) (BH's ⟨g, D⟩).
+// Partial sums [block][2].
 static __global__ void __launch_bounds__(256) array_sums_kernel(const float2* g, const float2* h,
                                                          size_t n, int mode, double* partial) {
   __shared__ double sh[16];
@@ -138,6 +139,9 @@ static __global__ void __launch_bounds__(256) array_sums_kernel(const float2* g,
       const float2 b = h[i];
       s0 += (double)a.x * ((double)a.x - b.x) + (double)a.y * ((double)a.y - b.y);
       s1 += (double)b.x * b.x + (double)b.y * b.y;
+    } else if (mode == 2) {
+      const float2 b = h[i];
+      s0 += (double)a.x * b.x + (double)a.y * b.y;
     } else {
       s0 += sqrt((double)a.x * a.x + (double)a.y * a.y);
     }

@@ -133,6 +133,20 @@ class GpuPtycho:
         p = _lib.MlParams(update_object, update_probe, calc_llk, zero_phase_ramp)
         self._check(self._lib.ptyb_ml(self._h, ctypes.byref(p), ncycle))
 
+    def bh(self, nepoch, batch_size, probe_rho=0.01, seed=7, calc_llk=0):
+        """pty-chi's BH on the amplitude cost (reference `GpuPtycho::bh`): `nepoch` epochs from
+        a fresh run; one batch of every frame runs conjugate directions across epochs."""
+        p = _lib.BhParams(batch_size, 0, probe_rho, 0.1, seed)
+        self._check(self._lib.ptyb_bh(self._h, ctypes.byref(p), nepoch, calc_llk))
+
+    def bh_steps(self):
+        """The last BH epoch's steps: dicts of batch, count, beta, alpha, top, bottom."""
+        n = self._lib.ptyb_bh_steps_len(self._h)
+        out = (_lib.BhStep * max(n, 1))()
+        self._check(self._lib.ptyb_bh_steps(self._h, out, n))
+        return [dict(batch=s.batch, count=s.count, beta=s.beta, alpha=s.alpha, top=s.top,
+                     bottom=s.bottom) for s in out[:n]]
+
     @staticmethod
     def _inertia(x):
         return (0, 0.0) if x is None else (1, float(x))
@@ -180,6 +194,29 @@ class GpuPtycho:
         self._check(self._lib.ptyb_gradients(self._h, ctypes.byref(loss), ptr(go), ptr(gp),
                                              ptr(gd, False)))
         return dict(loss=loss.value, object=go, probe=gp, positions=gd)
+
+    def gradients_device(self, d_obj, d_probe, positions=False):
+        """`gradients` with the object and probe gradients written as complex64 into device
+        buffers (`data_ptr()` of contiguous complex64 CUDA tensors of the handle's device, or
+        None to skip): returns `(loss, positions gradient or None)`."""
+        loss = ctypes.c_double()
+        gd = np.empty((self._nframe, 2), np.float64) if positions else None
+        self._check(self._lib.ptyb_gradients_device(
+            self._h, ctypes.byref(loss), d_obj, d_probe, None if gd is None else _dptr(gd)))
+        return loss.value, gd
+
+    def set_object_device(self, ptr, nobj, nyo, nxo):
+        """The object (slice 0) from complex64 device memory `ptr` of the handle's device,
+        `[nobj, nyo, nxo]` (reference `GpuPtycho::set_object_device`)."""
+        self._check(self._lib.ptyb_set_object_device(self._h, nobj, nyo, nxo, ptr))
+
+    def set_objects_device(self, ptr, nslice, nyo, nxo):
+        """Every slice from complex64 device memory `ptr`, `[nslice, nyo, nxo]`."""
+        self._check(self._lib.ptyb_set_objects_device(self._h, nslice, nyo, nxo, ptr))
+
+    def set_probe_device(self, ptr, nprobe, ny, nx):
+        """The probe from complex64 device memory `ptr`, `[nprobe, ny, nx]`."""
+        self._check(self._lib.ptyb_set_probe_device(self._h, nprobe, ny, nx, ptr))
 
     def forward_intensity(self, frames=None):
         """Model intensity `Σ_modes |Ψ|²` `[len(frames), ny, nx]` of the current estimate, in the
