@@ -475,6 +475,153 @@ def accuracy_batches(s, wl, device, nbatch=None):
                       "same start"}
 
 
+# Time to target (the reference's method, refs/py/time_to_target_ptychi.py): long runs fix an
+# LLK target, then timed runs of each algorithm to it from the same start.
+TTT_ALGOS = ("rpie", "lsqml", "ml")
+TTT_LABELS = {"rpie": "rPIE (alpha = beta = 0.1, batches of 100)",
+              "lsqml": "LSQML (Poisson, batches of 100)",
+              "ml": "ML (Poisson conjugate gradient, object and probe)"}
+
+
+def ttt_call(g, algo, n, calc_llk=0):
+    """`n` iterations of `algo` in one call from the handle's current state."""
+    if algo == "rpie":
+        g.rpie(n, batch_size=100, obj_alpha=0.1, probe_alpha=0.1, calc_llk=calc_llk, seed=7)
+    elif algo == "lsqml":
+        g.lsqml(n, calc_llk=calc_llk, batch_size=100, cost="poisson", seed=7)
+    else:
+        g.ml(n, update_object=True, update_probe=True, calc_llk=calc_llk, zero_phase_ramp=False)
+
+
+def llk_after(algo, trace):
+    """The Poisson LLK after 1, 2, … iterations from a call's LLK records (rPIE and LSQML record
+    the state after each epoch; ML the state a cycle starts from, so its first record is the
+    start and the last cycle's result is not recorded): entry i is the LLK after i + 1
+    iterations."""
+    trace = list(trace)
+    return trace[1:] if algo == "ml" else trace
+
+
+def ttt_targets(traces, margin=1.01):
+    """The targets of the long runs' LLK traces (`llk_after` form) and each algorithm's
+    iterations to them: the first target is `margin` times the lowest final LLK; when some
+    algorithm never reaches it, a second target is `margin` times the highest final among
+    those (the reference's rule), which every algorithm then reaches. An algorithm whose long
+    run diverged (a non-finite final LLK) sets no target and reaches none. Returns a list of
+    (target, {algo: iterations or None})."""
+    finals = {a: float(t[-1]) for a, t in traces.items() if np.isfinite(t[-1])}
+
+    def reach(target):
+        out = {}
+        for a, t in traces.items():
+            hit = [i for i, v in enumerate(t) if v <= target]
+            out[a] = hit[0] + 1 if hit else None
+        return out
+
+    first = margin * min(finals.values())
+    targets = [(first, reach(first))]
+    missed = [a for a, c in targets[0][1].items() if c is None and a in finals]
+    if missed:
+        second = margin * max(finals[a] for a in missed)
+        targets.append((second, reach(second)))
+    return targets
+
+
+def time_to_target(device, kind="rpie64", long_iters=500, reps=5, check=True, scale=1.0):
+    """Each algorithm's time to an LLK target on the scan `kind` (config 0's rPIE scan by
+    default), the reference's time-to-target method on this GPU: the long runs (`long_iters`
+    iterations, the Poisson LLK recorded after each) fix the targets (ttt_targets); then each
+    algorithm runs the iterations it needs in one call on a fresh handle from the common start,
+    `reps` times in ABBA order, with no LLK; device time from the engine's events and host wall
+    time of the call (handle creation apart). At the headline target (the last: the one every
+    algorithm reaches) the FP32 object is checked against the float64 oracle run for the same
+    iterations from the same start (object NRMSE, global phase and phase ramp removed, scale
+    kept, over the illuminated pixels)."""
+    from ptyrs_b200 import GpuPtycho, Scan, sim
+    s = sim.make_scan(kind, seed=0, scale=scale)
+    scan = Scan(s["counts"], s["y"], s["x"], s["wavelength"], s["distance"], s["detector_pixel"])
+    traces, long_ms = {}, {}
+    for algo in TTT_ALGOS:
+        with GpuPtycho(scan, s["object"], s["probe"], device=device) as g:
+            ttt_call(g, algo, long_iters, calc_llk=1)
+            traces[algo] = llk_after(algo, g.history()["poisson"])
+            long_ms[algo] = g.last_call_ms()
+    targets = ttt_targets(traces)
+    target, iters = targets[-1]
+    timed = {a: {"device_ms": [], "wall_ms": []} for a in TTT_ALGOS}
+    objects = {}
+    reached = tuple(a for a in TTT_ALGOS if iters[a] is not None)
+    for rep in range(reps):
+        for algo in (reached if rep % 2 == 0 else reached[::-1]):
+            with GpuPtycho(scan, s["object"], s["probe"], device=device) as g:
+                g.synchronize()
+                t0 = time.perf_counter()
+                ttt_call(g, algo, iters[algo])
+                g.synchronize()
+                timed[algo]["wall_ms"].append(1e3 * (time.perf_counter() - t0))
+                timed[algo]["device_ms"].append(g.last_call_ms())
+                if rep == 0:
+                    objects[algo] = g.object()
+    out = {"scan": kind, "scale": scale, "frames": len(s["counts"]),
+           "long_iterations": long_iters, "reps": reps,
+           "llk": "Poisson, normalised by the unmasked pixels",
+           "long_final_llk": {a: float(t[-1]) for a, t in traces.items()},
+           "diverged": [a for a, t in traces.items() if not np.isfinite(t[-1])],
+           "long_llk_every_10": {a: [float(v) for v in t[9::10]] for a, t in traces.items()},
+           "long_call_ms": long_ms,
+           "targets": [{"llk": t, "iterations": c} for t, c in targets],
+           "target_llk": target, "algorithms": TTT_LABELS, "per_algorithm": {}}
+    for algo in TTT_ALGOS:
+        if iters[algo] is None:
+            out["per_algorithm"][algo] = {"iterations": None, "time_to_target_s": None}
+            continue
+        out["per_algorithm"][algo] = {
+            "iterations": iters[algo],
+            "time_to_target_s": statistics.median(timed[algo]["wall_ms"]) / 1e3,
+            "device_s": statistics.median(timed[algo]["device_ms"]) / 1e3,
+            "wall_ms_runs": [round(v, 3) for v in timed[algo]["wall_ms"]]}
+    r = out["per_algorithm"]
+    if r["rpie"]["time_to_target_s"]:
+        out["rpie_over"] = {a: r["rpie"]["time_to_target_s"] / r[a]["time_to_target_s"]
+                            for a in ("lsqml", "ml") if r[a]["time_to_target_s"]}
+    if check:
+        out["nrmse_vs_f64_at_target"] = ttt_precision(
+            s, {a: n for a, n in iters.items() if n is not None}, objects)
+    return out
+
+
+def ttt_precision(s, iters, objects):
+    """Object NRMSE of each algorithm's FP32 GPU object after its iterations to the target
+    against the float64 oracle run of the same iterations from the same start."""
+    from oracle import ops
+    from oracle.lsqml import Lsqml
+    from oracle.ptycho import Ptycho
+    optics = oracle_optics(s)
+    out = {}
+    with _threads(os.cpu_count() or 1):
+        for algo, n in iters.items():
+            p = Ptycho(s["counts"], s["y"], s["x"], optics, s["object"], s["probe"])
+            if algo == "rpie":
+                p.rpie(n, batch_size=100, obj_alpha=0.1, probe_alpha=0.1, seed=7)
+                ref = p.object
+            elif algo == "lsqml":
+                run = Lsqml(100, "poisson", 7)
+                obj, probe = p.object, p.probe
+                for _ in range(n):
+                    obj, probe, _ = run.epoch(p.addr, p.obs, optics, obj, probe)
+                ref = obj
+            else:
+                p.ml(n, update_object=True, update_probe=True, calc_llk=0,
+                     zero_phase_ramp=False)
+                ref = p.object
+            illum = ops.illumination(p.addr.views, p.object.shape, p.probe)
+            w = (illum >= 1e-3 * illum.max()).astype(float)
+            out[algo] = object_nrmse(objects[algo], ref, w)
+    from oracle import ops as _ops
+    _ops.FFT_WORKERS = None
+    return out
+
+
 def line_config(args, wl, s, patterns, ws):
     """The `config` of both arms' lines (the same keys, so the two lines name one workload)."""
     counts = sum(x["counts"].nbytes for x in s) if isinstance(s, list) else s["counts"].nbytes
@@ -682,6 +829,13 @@ def main():
                     help="frames per launch of the whole-scan passes (0: the engine's default)")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="keep this fraction of the scan's positions (small profiling cases)")
+    ap.add_argument("--no-ttt", action="store_true", help="skip the time-to-target leg")
+    ap.add_argument("--ttt-scan", default="rpie64",
+                    help="scan of the time-to-target leg (rpie64: the rPIE configuration)")
+    ap.add_argument("--ttt-iters", type=int, default=500,
+                    help="iterations of the time-to-target leg's long runs")
+    ap.add_argument("--ttt-scale", type=float, default=1.0,
+                    help="fraction of the time-to-target scan's positions (a cut)")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
@@ -831,6 +985,10 @@ def main():
             one = {"value": o["value"], "cores": 1, "sample": o["sample"]}
         cpu["single_core"] = one
     g.close()
+    ttt = None
+    if rank == 0 and not args.no_ttt:
+        ttt = time_to_target(local, kind=args.ttt_scan, long_iters=args.ttt_iters,
+                             check=not args.no_cpu, scale=args.ttt_scale)
     if rank == 0:
         line = {
             "metric": "diffraction patterns*iter/sec", "value": value,
@@ -839,6 +997,7 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": line_config(args, wl, s, P, ws),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "accuracy": acc,
+            "time_to_target": ttt,
             "gpu_launches": int(launches), "clocks": clk, "autotune": tuned,
             "ms_per_step_with_kernel_events": instrumented_ms / args.steps,
             "kernels_ms": {k: round(v[0], 3) for k, v in sorted(times.items())},

@@ -10,7 +10,7 @@ import pytest
 import torch
 
 from oracle import ops
-from ptyrs_b200 import GpuPtycho, Scan, sim
+from ptyrs_b200 import GpuPtycho, PtybError, Scan, sim
 from ptyrs_b200.autograd import poisson_loss
 from scenarios import far_field, oracle_state, rel_l2
 
@@ -116,3 +116,33 @@ def test_autograd_function(case):
             t = 1e-3 * obj.abs().max() / obj.grad.abs().max()
             obj2 = obj - t * obj.grad
         assert poisson_loss(obj2, probe, d, g).item() < loss.item()
+
+
+def test_autograd_function_on_cuda_tensors(case):
+    """CUDA tensors stay on the device (`ptyb_set_object_device`, `ptyb_set_probe_device`,
+    `ptyb_gradients_device`): the same loss and, in complex64, the same gradients as the host
+    path's, on CUDA tensors; a host pointer is refused and changes nothing."""
+    dev = torch.device("cuda:0")
+    with gpu_of(case) as g:
+        g.set_positions(case["offsets"], refine=False)
+        want = g.gradients()
+        obj = torch.tensor(case["object"], dtype=torch.complex64, device=dev, requires_grad=True)
+        probe = torch.tensor(case["probe"], dtype=torch.complex64, device=dev, requires_grad=True)
+        d = torch.tensor(case["offsets"], device=dev, requires_grad=True)
+        loss = poisson_loss(obj, probe, d, g)
+        assert loss.device.type == "cuda"
+        # the state went in as complex64 either way, so the loss and gradients are the same
+        assert abs(loss.item() - want["loss"]) <= 1e-12 * abs(want["loss"])
+        loss.backward()
+        assert obj.grad.is_cuda and probe.grad.is_cuda
+        go, gp = obj.grad.cpu().numpy(), probe.grad.cpu().numpy()
+        assert np.abs(go - want["object"]).max() <= 1e-6 * np.abs(want["object"]).max()
+        assert np.abs(gp - want["probe"]).max() <= 1e-6 * np.abs(want["probe"]).max()
+        assert np.allclose(d.grad.cpu().numpy(), want["positions"], rtol=0, atol=0)
+        before = g.object()
+        host = np.ascontiguousarray(case["object"], np.complex64)
+        with pytest.raises(PtybError):
+            g.set_object_device(host.ctypes.data, *host.shape)
+        with pytest.raises(PtybError):
+            g.set_object_device(obj.detach().data_ptr(), 1, 1, 1)  # wrong dims
+        assert np.array_equal(g.object(), before)
