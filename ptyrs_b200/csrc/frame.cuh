@@ -35,7 +35,8 @@ enum FrameMode : int {
   kStore = 4,      // forward only; detector field and Σ_modes |Ψ|² to global
   kFromStore = 5,  // detector field from global; LSQML residual; out = χ
   kProject = 6,    // magnitude projection √I/max(√Ĩ, 1e-12), masked kept; out = ψ' − ψ
-  kProjectKept = 7,// kProject from the detector field a kMlGrad pass kept (psi_out)
+  kProjectKept = 7,// from the detector field a kMlGrad pass kept (psi_out): out = ψ' − ψ as
+                   // the inverse of Ψ' − Ψ
   kCarry = 8,      // AP / DM / RAAR: projection of a mix of P·O·q and the carried waves
 };
 
@@ -386,7 +387,11 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
     float fac;
     if (MODE == kRpie) {
       fac = masked ? 1.f : sqrtf(yo + 1e-7f) / (sqrtf(ic) + 1e-7f);
-    } else if (MODE == kProject || MODE == kProjectKept || MODE == kCarry) {
+    } else if (MODE == kProjectKept) {
+      // ApplyAmplitude (engine/ops.rs:83-107) minus the identity: the kept field Ψ = DFT(ψ)
+      // goes to ΔΨ = Ψ' − Ψ, whose inverse is the change ψ' − ψ itself (no model re-read)
+      fac = masked ? 0.f : sqrtf(yo) / fmaxf(sqrtf(ic), 1e-12f) - 1.f;
+    } else if (MODE == kProject || MODE == kCarry) {
       // ApplyAmplitude (engine/ops.rs:83-107)
       fac = masked ? 1.f : sqrtf(yo) / fmaxf(sqrtf(ic), 1e-12f);
     } else if (MODE == kMlGrad) {
@@ -489,7 +494,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
     }
     return;
   }
-  epilogue(a.out, MODE != kMlGrad);
+  epilogue(a.out, MODE != kMlGrad && MODE != kProjectKept);
 }
 
 }  // namespace ptyb

@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
       // (engine/features.rs:992-1025), cluster-summed in rank order.
       double num = 0.0, den = 0.0;
       const float2* cf = a.c + (size_t)slot * K * plane;
-#pragma unroll 2
+#pragma unroll 4
       for (int idx = tid; idx < H * N; idx += T) {
         const int yl = idx / N, x = idx % N, y = r * H + yl;
         const float2 o = a.object[(size_t)(corner.x + y) * a.nxo + corner.y + x];
