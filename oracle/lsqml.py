@@ -319,3 +319,87 @@ class Lsqml:
 
 def fftshift_planes(a):
     return fftshift2(a)
+
+
+def slice_jet(optics, views, objs, probe, d_objs, d_probe):
+    """The exit waves through the slices and their first and second Taylor coefficients along
+    the displacement (d_objs, d_probe): with every slice O_s + γ·dO_s and the probe P + γ·dP,
+    the wave entering slice s is w_s + γ·w′_s + γ²·w″_s + O(γ³), w_0 = P, w′_0 = dP, w″_0 = 0,
+    and through slice s and its gap G_s: w_{s+1} = G_s(O_s·w_s),
+    w′_{s+1} = G_s(O_s·w′_s + dO_s·w_s), w″_{s+1} = G_s(O_s·w″_s + dO_s·w′_s); the exit
+    multiplies by q·(O_last + γ·dO_last) the same way. Returns (ψ, ψ′, ψ″) in the detector
+    plane (the exit transform applied), shifted, one plane per view. One slice gives PyNX's
+    (po, a, b) of `cg_gamma` (engine/ptycho.rs:517-545)."""
+    own = views.copy()
+    own["probe"] = np.arange(len(views))
+    pk = views["probe"].astype(np.int64)
+    w, w1, w2 = probe[pk], d_probe[pk], np.zeros_like(probe[pk])
+    ny, nx = w.shape[-2:]
+    one = _unit((ny, nx))
+    n = len(objs)
+    for s in range(n):
+        q = optics.slice_quad(s)
+        q = one if q is None else q
+        t0 = ops.obj_probe_to_psi(own, objs[s], w, q)
+        t1 = ops.obj_probe_to_psi(own, objs[s], w1, q) + ops.obj_probe_to_psi(own, d_objs[s], w, q)
+        t2 = ops.obj_probe_to_psi(own, objs[s], w2, q) + ops.obj_probe_to_psi(own, d_objs[s], w1, q)
+        if s + 1 == n:
+            return tuple(optics.exit_forward(t) for t in (t0, t1, t2))
+        gap = optics.gaps[s]
+        w, w1, w2 = (fftshift2(gap.forward(t)) for t in (t0, t1, t2))
+
+
+def multislice_ml(addr, obs, optics, objs, probe, ncycle, update_object=True,
+                  update_probe=True, calc_llk=0):
+    """Poisson ML conjugate gradient through pty-chi's multislice object (this build's
+    definition; the reference runs ML on one slice, engine/ptycho.rs:775-842): the opening
+    rescale of the probe to the data's photons, per cycle the gradients through the slices
+    (`multislice_grads`), the Polak–Ribière β over every slice and the probe, and PyNX's
+    Poisson line search `cg_poisson_gamma` on the second-order expansion of the exit waves
+    along the direction (`slice_jet`). Returns (objs, probe, llk records)."""
+    objs, probe = [o.copy() for o in objs], probe.copy()
+    nframe, nmode = addr.nframe, addr.nmode
+    views = addr.views
+    frames = slice(0, nframe)
+
+    def llk_now():
+        waves = SliceWaves(optics, views, objs, probe[views["probe"].astype(np.int64)])
+        return ops.llk(obs, frames, nmode, optics.exit_forward(waves.psi))
+
+    calc = llk_now().nb_photons_calc
+    probe = probe * np.sqrt(obs.total() / calc)
+    last = None
+    d_objs = [np.zeros_like(o) for o in objs]
+    d_probe = np.zeros_like(probe)
+    records = []
+    for ic in range(ncycle):
+        if calc_llk > 0 and (ic % calc_llk == 0 or ic + 1 == ncycle):
+            records.append(llk_now().normalised(obs.nb_obs))
+        _, go, gp = multislice_grads(addr, obs, optics, objs, probe)
+        if not update_object:
+            go = [np.zeros_like(o) for o in objs]
+        if not update_probe:
+            gp = np.zeros_like(probe)
+        if last is None:
+            beta = 0.0
+        else:
+            num = sum((np.conj(g) * (g - l)).real.sum() for g, l in zip(go, last[0]))
+            num += (np.conj(gp) * (gp - last[1])).real.sum()
+            den = sum((np.abs(l) ** 2).sum() for l in last[0]) + (np.abs(last[1]) ** 2).sum()
+            with np.errstate(divide="ignore", invalid="ignore"):
+                beta = num / den
+            if not (np.isfinite(beta) and beta >= 0.0):
+                beta = 0.0
+        d_objs = [d * beta - g for d, g in zip(d_objs, go)]
+        d_probe = d_probe * beta - gp
+        po, a, b = slice_jet(optics, views, objs, probe, d_objs, d_probe)
+        num, den = ops.cg_poisson_gamma(obs, frames, nmode, po, a, b)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            gamma = np.float64(num) / np.float64(den)
+        if np.isfinite(gamma):
+            objs = [o + d * gamma for o, d in zip(objs, d_objs)]
+            probe = probe + d_probe * gamma
+        else:
+            d_objs, d_probe = [-g for g in go], -gp
+        last = (go, gp)
+    return objs, probe, records

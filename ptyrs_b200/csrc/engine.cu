@@ -69,6 +69,18 @@ cudaError_t launch_bh_side(int N, const BhArgs& a, int nslot, cudaStream_t s) {
   return cudaErrorInvalidValue;
 }
 
+cudaError_t launch_slice_gamma_side(int N, const SliceGammaArgs& a, int nslot, int K,
+                                    cudaStream_t s) {
+  switch (N) {
+    case 64: return SideKernels<64>::slice_gamma(a, nslot, K, s);
+    case 96: return SideKernels<96>::slice_gamma(a, nslot, K, s);
+    case 128: return SideKernels<128>::slice_gamma(a, nslot, K, s);
+    case 192: return SideKernels<192>::slice_gamma(a, nslot, K, s);
+    case 256: return SideKernels<256>::slice_gamma(a, nslot, K, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
 }  // namespace ptyb
 
 namespace ptyb::eng {

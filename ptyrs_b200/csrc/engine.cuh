@@ -126,6 +126,9 @@ struct ptyb_handle {
   // Multislice gradients: every slice's 2·∂L/∂O_s* and its compensation.
   float2* g_slices = nullptr;     // [S][nyo][nxo]
   float2* g_slices_c = nullptr;
+  // ML through the slices: the previous gradients and the directions of every slice.
+  float2* last_slices = nullptr;  // [S][nyo][nxo]
+  float2* dir_slices = nullptr;   // [S][nyo][nxo]
   // AP / DM / RAAR: every frame's carried exit waves and RAAR's iterate, [P][K][N][N]; the
   // probe blend's per-chunk norms and its norm plane.
   float2* carry = nullptr;
@@ -258,7 +261,7 @@ template <int MODE>
 cudaError_t launch_frame(ptyb_handle* h, const FrameArgs& a, int nslot) {
   constexpr int kind = MODE == kRpie ? kKFrameRpie
                        : MODE == kLsqmlFused ? kKFrameLsqml
-                       : MODE == kMlGrad ? kKFrameMl
+                       : MODE == kMlGrad || MODE == kBhGrad ? kKFrameMl
                        : MODE == kLlk ? kKFrameLlk
                        : MODE == kStore ? kKFrameStore
                        : MODE == kProject || MODE == kProjectKept ? kKFrameProject

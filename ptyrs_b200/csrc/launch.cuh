@@ -21,6 +21,9 @@ cudaError_t launch_slice_side(int N, int C, int mode, const SliceArgs& a, int ns
 cudaError_t launch_gamma_side(int N, const GammaArgs& a, int nslot, cudaStream_t s);
 // BH's bilinear Hessian at the line search's cluster size.
 cudaError_t launch_bh_side(int N, const BhArgs& a, int nslot, cudaStream_t s);
+// ML's line search through a multislice object at the line search's cluster size; K modes.
+cudaError_t launch_slice_gamma_side(int N, const SliceGammaArgs& a, int nslot, int K,
+                                    cudaStream_t s);
 constexpr int gamma_cluster(int N) {
   return N == 64 ? 1 : N == 96 ? 2 : N == 128 ? 4 : N == 192 ? 8 : 16;
 }
@@ -33,6 +36,7 @@ struct SideKernels {
   static cudaError_t slice(int C, int mode, const SliceArgs& a, int nslot, int K, cudaStream_t s);
   static cudaError_t gamma(const GammaArgs& a, int nslot, cudaStream_t s);
   static cudaError_t bh(const BhArgs& a, int nslot, cudaStream_t s);
+  static cudaError_t slice_gamma(const SliceGammaArgs& a, int nslot, int K, cudaStream_t s);
 };
 extern template struct SideKernels<64>;
 extern template struct SideKernels<96>;

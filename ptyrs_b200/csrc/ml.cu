@@ -240,6 +240,135 @@ void ml_gamma(ptyb_handle* h, double* num, double* den) {
   }
 }
 
+// Shared memory of the multislice line search for frames of side N with K modes.
+size_t slice_gamma_bytes(int N, int K) {
+  switch (N) {
+    case 64: return slice_gamma_smem_bytes<64, gamma_cluster(64)>(K);
+    case 96: return slice_gamma_smem_bytes<96, gamma_cluster(96)>(K);
+    case 128: return slice_gamma_smem_bytes<128, gamma_cluster(128)>(K);
+    case 192: return slice_gamma_smem_bytes<192, gamma_cluster(192)>(K);
+    case 256: return slice_gamma_smem_bytes<256, gamma_cluster(256)>(K);
+  }
+  return ~size_t(0);
+}
+
+// num and den of the Poisson line search along (dir_slices, dir_probe) through the slices
+// (multislice.cuh `slice_gamma_kernel`), frames summed in order.
+void slice_gamma(ptyb_handle* h, double* num, double* den) {
+  const int stack = std::min(h->P, h->stack);
+  SliceGammaArgs g = {};
+  g.d_obj = h->dir_slices;
+  g.d_probe = h->dir_probe;
+  for (int s0 = 0; s0 < h->P; s0 += stack) {
+    const int n = std::min(stack, h->P - s0);
+    g.sa.f = frame_args(h, h->iota + s0);
+    g.sa.f.nslot = n;
+    g.sa.tf = h->tf;
+    g.sa.nslice = h->nslice;
+    g.sa.obj_plane = (size_t)h->nyo * h->nxo;
+    g.out = h->gamma_sums + (size_t)s0 * 2;
+    cudaError_t e = cudaSuccess;
+    timed(h, kKGamma, [&] { e = launch_slice_gamma_side(h->N, g, n, h->K, h->stream); }, n);
+    check(h, e, "multislice line search");
+    ++h->launches;
+  }
+  std::vector<double> v((size_t)h->P * 2);
+  check(h, copy_sync(h, v.data(), h->gamma_sums, v.size() * sizeof(double),
+                     cudaMemcpyDeviceToHost),
+        "gamma");
+  *num = *den = 0.0;
+  for (int f = 0; f < h->P; ++f) {
+    *num += v[(size_t)f * 2];
+    *den += v[(size_t)f * 2 + 1];
+  }
+}
+
+// ML conjugate gradient through the slices (this build's definition; the reference runs ML
+// on one slice): the opening rescale of the probe to the data's photons, per cycle the
+// gradients through the slices (slice_gradients), the Polak–Ribière β over every slice and the
+// probe, the line search on the second-order expansion (slice_gamma) and the step.
+int ml_slices(ptyb_handle* h, const ptyb_ml_params* p, int32_t ncycle) {
+  return guarded(h, true, [&]() -> int {
+    const int S = h->nslice;
+    ensure_slots(h, std::min(h->P, h->stack));
+    ensure_ml(h);
+    const size_t no = (size_t)S * h->nyo * h->nxo, np = (size_t)h->K * h->N * h->N;
+    if (!h->last_slices) {
+      h->last_slices = alloc<float2>(h, no);
+      h->dir_slices = alloc<float2>(h, no);
+    }
+    const bool uo = p->update_object != 0, up = p->update_probe != 0;
+    begin_call(h);
+    // the probe rescaled so the model's photons are the data's
+    const ptyb_llk l0 = llk_pass(h);
+    const double fp = std::sqrt(h->obs_total / l0.nb_photons_calc);
+    timed(h, kKAxpy, [&] {
+      scale_kernel<<<blocks_for(np), 256, 0, h->stream>>>(h->probe, (float)fp, np);
+    });
+    launched(h, "scale");
+    check(h, cudaMemsetAsync(h->dir_slices, 0, no * sizeof(float2), h->stream), "memset");
+    check(h, cudaMemsetAsync(h->dir_probe, 0, np * sizeof(float2), h->stream), "memset");
+    bool have_last = false;
+    for (int ic = 0; ic < ncycle; ++ic) {
+      const bool due = llk_due(p->calc_llk, ic, ncycle);
+      ptyb_llk l = {};
+      if (due) l = llk_pass(h);
+      slice_gradients(h, uo, up);
+      double beta = 0.0;
+      if (have_last) {
+        double a[2], b[2];
+        array_sums(h, h->g_slices, h->last_slices, no, 0, a);
+        array_sums(h, h->g_probe, h->last_probe, np, 0, b);
+        beta = (a[0] + b[0]) / (a[1] + b[1]);
+        if (!(std::isfinite(beta) && beta >= 0.0)) beta = 0.0;
+      }
+      timed(h, kKAxpy, [&] {
+        cg_direction_kernel<<<blocks_for(no), 256, 0, h->stream>>>(h->dir_slices, h->g_slices,
+                                                                   (float)beta, no);
+      });
+      launched(h, "direction");
+      timed(h, kKAxpy, [&] {
+        cg_direction_kernel<<<blocks_for(np), 256, 0, h->stream>>>(h->dir_probe, h->g_probe,
+                                                                   (float)beta, np);
+      });
+      launched(h, "direction");
+      double num = 0.0, den = 0.0;
+      slice_gamma(h, &num, &den);
+      const double gamma = num / den;
+      if (std::isfinite(gamma)) {
+        timed(h, kKAxpy, [&] {
+          axpy_kernel<<<blocks_for(no), 256, 0, h->stream>>>(h->object, h->dir_slices,
+                                                             (float)gamma, no);
+        });
+        launched(h, "step");
+        timed(h, kKAxpy, [&] {
+          axpy_kernel<<<blocks_for(np), 256, 0, h->stream>>>(h->probe, h->dir_probe,
+                                                             (float)gamma, np);
+        });
+        launched(h, "step");
+      } else {
+        timed(h, kKAxpy, [&] {
+          cg_direction_kernel<<<blocks_for(no), 256, 0, h->stream>>>(h->dir_slices,
+                                                                     h->g_slices, 0.f, no);
+        });
+        launched(h, "direction");
+        timed(h, kKAxpy, [&] {
+          cg_direction_kernel<<<blocks_for(np), 256, 0, h->stream>>>(h->dir_probe, h->g_probe,
+                                                                     0.f, np);
+        });
+        launched(h, "direction");
+      }
+      std::swap(h->g_slices, h->last_slices);
+      std::swap(h->g_probe, h->last_probe);
+      have_last = true;
+      if (due) record(h, kAlgMl, l);
+      ++h->cycle;
+    }
+    end_call(h, "ml");
+    return PTYB_OK;
+  });
+}
+
 // The Poisson sum and its gradients of the handle's state (ptyb_gradients): object and probe
 // gradients handed to `sink(g_obj, g_probe, object elements, probe elements)` on the device,
 // the position gradient to host d_pos.
@@ -315,8 +444,15 @@ int ptyb_ml(ptyb_handle* h, const ptyb_ml_params* p, int32_t ncycle) {
     return PTYB_INVALID;
   }
   if (h->nslice > 1) {
-    h->err = "ML runs on a single-slice object";
-    return PTYB_INVALID;
+    if (h->have_offsets || p->zero_phase_ramp) {
+      h->err = "ML through slices runs without the position model and phase-ramp removal";
+      return PTYB_INVALID;
+    }
+    if (slice_gamma_bytes(h->N, h->K) > 227 * 1024) {
+      h->err = "ML through slices: the frame's modes do not fit one cluster's shared memory";
+      return PTYB_INVALID;
+    }
+    return ml_slices(h, p, ncycle);
   }
   return guarded(h, true, [&]() -> int {
     ensure_slots(h, std::min(h->P, h->stack));

@@ -344,4 +344,126 @@ static __global__ void __launch_bounds__(1024) slice_solve_kernel(const double* 
   }
 }
 
+// ML through the slices (this build's definition; the reference runs ML on one slice): the
+// Poisson line search along the direction (dO_s, dP) on the second-order expansion of the
+// exit waves, one frame per cluster. The wave entering slice s and its first and second Taylor
+// coefficients along the direction, w, w′, w″ (w_0 = P, w′_0 = dP, w″_0 = 0), go through the
+// slices together: w″ ← O_s·w″ + dO_s·w′, w′ ← O_s·w′ + dO_s·w, w ← O_s·w, then the gap (the
+// last slice with the exit phase q, then the far-field transform). With po, a, b the three
+// detector fields, per unmasked pixel calc = Σ_m |po|², r = Σ_m Re(p̄o·a),
+// s = Σ_m |a|² + 2·Re(p̄o·b), d = 1 − I/max(calc, 1e-32): num = −Σ 2·r·d,
+// den = Σ 2·s·d + I·(2r/calc)² (PyNX CG_Poisson_Gamma, engine/ops.rs:206-253). Shared memory
+// holds the three sets of K planes.
+struct SliceGammaArgs {
+  SliceArgs sa;
+  const float2* d_obj;    // [nslice][nyo][nxo]
+  const float2* d_probe;  // [K][N][N]
+  double* out;            // [slot][2]: num, den
+};
+
+template <int N, int C>
+__host__ __device__ constexpr size_t slice_gamma_smem_bytes(int K) {
+  return 3 * frame_smem_bytes<N, C>(K) - 2 * (N * sizeof(float2) + 160 * sizeof(double));
+}
+
+template <int N, int C>
+__global__ void __launch_bounds__(FrameShape<N, C>::T, 1) slice_gamma_kernel(SliceGammaArgs g) {
+  using F = FrameShape<N, C>;
+  constexpr int H = F::H, T = F::T, L = F::L;
+  const SliceArgs& sa = g.sa;
+  const FrameArgs& a = sa.f;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int K = a.nprobe;
+  float2* S = reinterpret_cast<float2*>(smem_raw);  // lines: w (K·H), w′ (K·H), w″ (K·H)
+  double* red = reinterpret_cast<double*>(S + 3 * (size_t)K * H * L + N);
+  cg::cluster_group cluster = cg::this_cluster();
+  const int r = C > 1 ? (int)cluster.block_rank() : 0;
+  const int slot = blockIdx.x / C;
+  const int f = a.frames[slot];
+  const int2 corner = a.corners[f];
+  const int tid = threadIdx.x;
+  LineTwiddles<N> ltw;
+  ltw.load(a.tw, tid % F::G);
+  auto at = [&](int set, int m, int yl, int jx) -> float2& {
+    const int line = (set * K + m) * H + yl;
+    return S[line * L + (jx ^ swz(line))];
+  };
+#pragma unroll 2
+  for (int idx = tid; idx < H * N; idx += T) {
+    const int yl = idx / N, jx = idx % N;
+    const int ny = (r * H + yl + N / 2) % N, nx = (jx + N / 2) % N;
+    for (int m = 0; m < K; ++m) {
+      const size_t pi = ((size_t)m * N + ny) * N + nx;
+      at(0, m, yl, jx) = a.probe[pi];
+      at(1, m, yl, jx) = g.d_probe[pi];
+      at(2, m, yl, jx) = make_float2(0.f, 0.f);
+    }
+  }
+  __syncthreads();
+  for (int s = 0; s < sa.nslice; ++s) {
+    const bool last = s + 1 == sa.nslice;
+    const float2* obj = a.object + (size_t)s * sa.obj_plane;
+    const float2* dob = g.d_obj + (size_t)s * sa.obj_plane;
+#pragma unroll 2
+    for (int idx = tid; idx < H * N; idx += T) {
+      const int yl = idx / N, jx = idx % N;
+      const int ny = (r * H + yl + N / 2) % N, nx = (jx + N / 2) % N;
+      const size_t oi = (size_t)(corner.x + ny) * a.nxo + corner.y + nx;
+      float2 o = obj[oi], d = dob[oi];
+      if (last) {
+        const float2 q = a.quad[ny * N + nx];
+        o = cmul(o, q);
+        d = cmul(d, q);
+      }
+      for (int m = 0; m < K; ++m) {
+        float2 &w = at(0, m, yl, jx), &w1 = at(1, m, yl, jx), &w2 = at(2, m, yl, jx);
+        w2 = cadd(cmul(o, w2), cmul(d, w1));
+        w1 = cadd(cmul(o, w1), cmul(d, w));
+        w = cmul(o, w);
+      }
+    }
+    __syncthreads();
+    if (!last) through_gap<N, C>(S, sa.tf + (size_t)s * N * N, 3 * K, false, ltw, cluster, r);
+  }
+  all_lines<N, C, -1>(S, 3 * K * H, ltw);
+  transpose<N, C>(S, 3 * K, cluster);
+  all_lines<N, C, -1>(S, 3 * K * H, ltw);
+  // Columns kx = r·H + c (lines set·K·H + m·H + c), elements ky.
+  constexpr float inv_n2 = 1.0f / ((float)N * (float)N);
+  const float* iobs = a.iobs + (size_t)f * N * N;
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int idx = tid; idx < H * N; idx += T) {
+    const int c = idx % H, ky = idx / H;
+    const float yo = iobs[ky * N + r * H + c];
+    if (yo < 0.f) continue;
+    double calc = 0.0, rr = 0.0, ss = 0.0;
+    for (int m = 0; m < K; ++m) {
+      const int l0 = m * H + c, l1 = (K + m) * H + c, l2 = (2 * K + m) * H + c;
+      const float2 po = S[l0 * L + (ky ^ swz(l0))], av = S[l1 * L + (ky ^ swz(l1))],
+                   bv = S[l2 * L + (ky ^ swz(l2))];
+      calc += (double)cnorm2(po) * inv_n2;
+      rr += ((double)po.x * av.x + (double)po.y * av.y) * inv_n2;
+      ss += ((double)cnorm2(av) + 2.0 * ((double)po.x * bv.x + (double)po.y * bv.y)) * inv_n2;
+    }
+    calc = fmax(calc, 1e-32);
+    const double d = 1.0 - (double)yo / calc;
+    v[0] -= 2.0 * rr * d;
+    const double t = 2.0 * rr / calc;
+    v[1] += 2.0 * ss * d + (double)yo * t * t;
+  }
+  block_sum<T>(v, 2, red);
+  csync<C>(cluster);
+  if (r == 0 && tid == 0) {
+    double num = 0.0, den = 0.0;
+    for (int q = 0; q < C; ++q) {
+      const double* rq = C > 1 ? cluster.map_shared_rank(red, q) : red;
+      num += rq[0];
+      den += rq[1];
+    }
+    g.out[slot * 2] = num;
+    g.out[slot * 2 + 1] = den;
+  }
+  csync<C>(cluster);
+}
+
 }  // namespace ptyb

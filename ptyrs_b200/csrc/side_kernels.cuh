@@ -47,6 +47,7 @@ cudaError_t frame_modes(int mode, const FrameArgs& a, int nslot, int K, cudaStre
     case kLsqmlFused:
       return launch_clusters<N, C>(frame_kernel<N, C, kLsqmlFused>, a, nslot, smem, s);
     case kMlGrad: return launch_clusters<N, C>(frame_kernel<N, C, kMlGrad>, a, nslot, smem, s);
+    case kBhGrad: return launch_clusters<N, C>(frame_kernel<N, C, kBhGrad>, a, nslot, smem, s);
     case kLlk: return launch_clusters<N, C>(frame_kernel<N, C, kLlk>, a, nslot, smem, s);
     case kStore: return launch_clusters<N, C>(frame_kernel<N, C, kStore>, a, nslot, smem, s);
     case kFromStore:
@@ -137,6 +138,14 @@ template <int N>
 cudaError_t SideKernels<N>::gamma(const GammaArgs& a, int nslot, cudaStream_t s) {
   constexpr int C = gamma_cluster(N);
   return launch_clusters<N, C>(gamma_kernel<N, C>, a, nslot, gamma_smem_bytes<N, C>(), s, true);
+}
+
+template <int N>
+cudaError_t SideKernels<N>::slice_gamma(const SliceGammaArgs& a, int nslot, int K,
+                                        cudaStream_t s) {
+  constexpr int C = gamma_cluster(N);
+  return launch_clusters<N, C>(slice_gamma_kernel<N, C>, a, nslot,
+                               slice_gamma_smem_bytes<N, C>(K), s, true);
 }
 
 template <int N>

@@ -132,8 +132,6 @@ def test_multislice_refuses_other_algorithms(case):
         with pytest.raises(PtybError):
             g.rpie(1, batch_size=8)
         with pytest.raises(PtybError):
-            g.ml(1)
-        with pytest.raises(PtybError):
             g.forward_intensity([0])
         g.set_positions(np.zeros((len(case["counts"]), 2)))
         with pytest.raises(PtybError):
@@ -217,3 +215,27 @@ def test_lsqml_epochs_through_slices_with_positions(case, refine):
             assert np.array_equal(d, d0)
         ref = run.llk(cpu.addr, cpu.obs, cpu.optics, objs, probe)
         assert abs(g.llk()["poisson"] - ref.poisson) <= RUN_TOL * abs(ref.poisson)
+
+
+@pytest.mark.parametrize("probe_too", [True, False], ids=["object_probe", "object"])
+def test_ml_through_slices(case, probe_too):
+    """ML conjugate gradient through the slices (`ptyb_ml` on a multislice handle): the
+    gradients through the slices, the Polak–Ribière direction over every slice and the probe
+    and the Poisson line search on the second-order expansion through the slices, against the
+    oracle's `multislice_ml` (its line-search terms checked by central differences) over three
+    cycles: every slice, the probe and the LLK records."""
+    from oracle.lsqml import multislice_ml
+    cpu = oracle_of(case)
+    objs, probe, recs = multislice_ml(cpu.addr, cpu.obs, cpu.optics, case["objects"], cpu.probe,
+                                      3, update_probe=probe_too, calc_llk=1)
+    with gpu_of(case) as g:
+        g.ml(3, update_object=True, update_probe=probe_too, calc_llk=1, zero_phase_ramp=False)
+        got = g.objects()
+        for k in range(3):
+            assert rel_l2(got[k] - 1.0, objs[k][0] - 1.0) < RUN_TOL, k
+        assert rel_l2(g.probe(), probe) < RUN_TOL
+        hist = g.history()
+        want = [r.poisson for r in recs]
+        assert np.abs(hist["poisson"] - want).max() <= RUN_TOL * max(want)
+        with pytest.raises(PtybError):
+            g.ml(1, zero_phase_ramp=True)
