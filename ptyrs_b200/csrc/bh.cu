@@ -25,10 +25,9 @@ void bh_grads(ptyb_handle* h, const int* frames, int n) {
     const int* fr = frames + s0;
     float2* gfield = h->g_all + (size_t)s0 * np;
     FrameArgs a = frame_args(h, fr);
-    a.cost = kCostAmplitude;
     a.out = gfield;
     a.psi_out = h->psi_all + (size_t)s0 * np;
-    check(h, launch_frame<kMlGrad>(h, a, m), "bh gradient pass");
+    check(h, launch_frame<kBhGrad>(h, a, m), "bh gradient pass");
     ++h->launches;
     GatherArgs g = gather_args(h, fr, m);
     g.upd = gfield;

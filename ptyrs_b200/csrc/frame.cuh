@@ -29,8 +29,7 @@ namespace ptyb {
 enum FrameMode : int {
   kRpie = 0,       // rPIE modulus; out = Δ = ψ' − ψ
   kLsqmlFused = 1, // LSQML residual from a per-frame a_far; out = χ = ψ' − ψ
-  kMlGrad = 2,     // Poisson gradient 2(1 − I/Ĩ) (BH's amplitude one with cost amplitude),
-                   // masked 0; out = ψ'
+  kMlGrad = 2,     // Poisson gradient 2(1 − I/Ĩ), masked 0; out = ψ'
   kLlk = 3,        // forward only; per-frame LLK sums
   kStore = 4,      // forward only; detector field and Σ_modes |Ψ|² to global
   kFromStore = 5,  // detector field from global; LSQML residual; out = χ
@@ -38,6 +37,8 @@ enum FrameMode : int {
   kProjectKept = 7,// from the detector field a kMlGrad pass kept (psi_out): out = ψ' − ψ as
                    // the inverse of Ψ' − Ψ
   kCarry = 8,      // AP / DM / RAAR: projection of a mix of P·O·q and the carried waves
+  kBhGrad = 9,     // BH's amplitude gradient 2(1 − √I/A), A = √Ĩ + 1e-8, masked 0; out = ψ'
+                   // (kMlGrad's pass otherwise: the detector field kept in psi_out)
 };
 
 enum Cost : int { kCostPoisson = 0, kCostAmplitude = 1 };
@@ -221,7 +222,8 @@ PTYB_D float2 carry_mix(const FrameArgs& a, float2 po, int slot, int m, int pix,
 template <int N, int C, int MODE>
 __global__ void __launch_bounds__(FrameShape<N, C>::T,
                                   N == 256 && FrameShape<N, C>::T <= 256 &&
-                                          (MODE == kMlGrad || MODE == kProjectKept ||
+                                          (MODE == kMlGrad || MODE == kBhGrad ||
+                                           MODE == kProjectKept ||
                                            MODE == kLlk || MODE == kCarry)
                                       ? 3
                                       : frame_min_blocks<N, C>())
@@ -310,7 +312,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
     all_lines<N, C, -1>(S, K * H, ltw);
   }
 
-  if (MODE == kMlGrad && a.psi_out) {
+  if ((MODE == kMlGrad || MODE == kBhGrad) && a.psi_out) {
     // Ψ of this CTA's columns to [slot][m][kx][ky]
     float2* dst = a.psi_out + (size_t)slot * K * N * N;
 #pragma unroll 8
@@ -395,12 +397,10 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
       // ApplyAmplitude (engine/ops.rs:83-107)
       fac = masked ? 1.f : sqrtf(yo) / fmaxf(sqrtf(ic), 1e-12f);
     } else if (MODE == kMlGrad) {
-      // Poisson: GradPoissonFourier (engine/ops.rs:161-195); amplitude: BH's 2·(1 − √I/A)
-      // with A = √Ĩ + 1e-8 (engine/bh.rs:255-265)
-      if (a.cost == kCostAmplitude)
-        fac = masked ? 0.f : 2.f * (1.f - sqrtf(yo) / (sqrtf(ic) + 1e-8f));
-      else
-        fac = masked ? 0.f : 2.f * (1.f - yo / fmaxf(ic, 1e-12f));
+      fac = masked ? 0.f : 2.f * (1.f - yo / fmaxf(ic, 1e-12f));
+    } else if (MODE == kBhGrad) {
+      // BH's residual (engine/bh.rs:255-265)
+      fac = masked ? 0.f : 2.f * (1.f - sqrtf(yo) / (sqrtf(ic) + 1e-8f));
     } else {
       float cres = 0.f;
       if (!masked)
@@ -494,7 +494,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
     }
     return;
   }
-  epilogue(a.out, MODE != kMlGrad && MODE != kProjectKept);
+  epilogue(a.out, MODE != kMlGrad && MODE != kBhGrad && MODE != kProjectKept);
 }
 
 }  // namespace ptyb
