@@ -717,7 +717,20 @@ def batch_main(args, wl):
     scan_of = lambda s, counts=None: Scan(s["counts"] if counts is None else counts, s["y"],
                                           s["x"], s["wavelength"], s["distance"],
                                           s["detector_pixel"])
-    handles = [GpuPtycho(scan_of(s), s["object"], s["probe"], device=local) for s in scans]
+    # launch shapes per frame side by measurement, outside the timed region (ptyrs_b200.tune)
+    opts = [dict() for _ in scans]
+    tuned = None
+    if not args.no_tune:
+        from ptyrs_b200.tune import autotune_batch
+        opts, chosen = autotune_batch(
+            scans, run=lambda h: batch_run([h], 1, 1, rpie=BATCH_RPIE, lsqml=BATCH_LSQML),
+            device=local, make=lambda s: (scan_of(s), s["object"], s["probe"]))
+        tuned = {str(n): {"chosen": best, "candidates_ms": [
+            {"cluster": o["cluster"], "stack": o["stack_size"],
+             "ms": None if ms is None else round(ms, 3)} for ms, o in table]}
+            for n, (best, table) in sorted(chosen.items())}
+    handles = [GpuPtycho(scan_of(s), s["object"], s["probe"], device=local, **o)
+               for s, o in zip(scans, opts)]
     batch_run(handles, args.warmup, args.warmup, rpie=BATCH_RPIE, lsqml=BATCH_LSQML)
     group.barrier()
     launches0 = sum(h.launches() for h in handles)
@@ -768,8 +781,8 @@ def batch_main(args, wl):
         group.barrier()
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
-            hs = [GpuPtycho(scan_of(s, c.numpy()), s["object"], s["probe"], device=local)
-                  for s, c in zip(scans, pinned)]
+            hs = [GpuPtycho(scan_of(s, c.numpy()), s["object"], s["probe"], device=local, **o)
+                  for s, c, o in zip(scans, pinned, opts)]
             batch_run(hs, 1, 1, rpie=BATCH_RPIE, lsqml=BATCH_LSQML)
             for h in hs:
                 h.object()
@@ -806,7 +819,7 @@ def batch_main(args, wl):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": line_config(args, wl, scans, 2 * P, ws),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "accuracy": acc,
-            "gpu_launches": int(launches), "clocks": clk,
+            "gpu_launches": int(launches), "clocks": clk, "autotune": tuned,
             "kernels_ms": {k: round(v[0], 3) for k, v in sorted(times.items())},
         }), flush=True)
     group.close()

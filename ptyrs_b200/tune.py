@@ -17,7 +17,8 @@ def clusters_for(n):
 def autotune(scan, obj, probe, run, prepare=None, stacks=(256, 512, 1024), clusters=None,
              device=0, **kw):
     """`(best, table)`: `best` the `dict(cluster=..., stack_size=...)` of the fastest timed call
-    of `run(handle)` and `table` every candidate's `(ms, options)` (None if it failed);
+    of `run(handle)` (its device time: the float `run` returns, else the handle's last call's)
+    and `table` every candidate's `(ms, options)` (None if it failed);
     `prepare(handle)` sets each fresh handle up (positions and the like) before the warm-up."""
     n = probe.shape[-1]
     clusters = clusters_for(n) if clusters is None else clusters
@@ -30,12 +31,26 @@ def autotune(scan, obj, probe, run, prepare=None, stacks=(256, 512, 1024), clust
                     prepare(g)
                 run(g)
                 g.synchronize()
-                run(g)
+                ms = run(g)
                 g.synchronize()
-                table.append((g.last_call_ms(), opts))
+                table.append((ms if isinstance(ms, float) else g.last_call_ms(), opts))
         except PtybError:
             table.append((None, opts))
     timed = [t for t in table if t[0] is not None]
     if not timed:
         raise RuntimeError("no candidate launch shape ran")
     return min(timed, key=lambda t: t[0])[1], table
+
+
+def autotune_batch(scans, run, device=0, stacks=(256, 512, 1024), make=None):
+    """Launch shapes for many uneven scans: per frame side, `autotune` on the side's first scan
+    (the shapes depend on the side and the frame count per launch, not on the object), applied
+    to every scan of that side. `scans` are dicts with `n` (the side) and what `make(scan)`
+    turns into `(Scan, object, probe)`; returns `(options per scan, {side: (best, table)})`."""
+    chosen = {}
+    for s in scans:
+        if s["n"] in chosen:
+            continue
+        scan, obj, probe = make(s)
+        chosen[s["n"]] = autotune(scan, obj, probe, run=run, stacks=stacks, device=device)
+    return [chosen[s["n"]][0] for s in scans], chosen
