@@ -265,17 +265,16 @@ def sample_scan(s, m):
     return dict(s, counts=s["counts"][:m], y=s["y"][:m], x=s["x"][:m])
 
 
-# DRAM bytes per frame of each kernel (ncu dram__bytes_read.sum + dram__bytes_write.sum over
-# its launches' frames) on the 1000-frame cut of the ml256 scan, profiles/ml256_launch_list.md:
-# roofline.traffic scales them to the launch's frames.
+# DRAM bytes per frame of a kernel (ncu dram__bytes_read.sum + dram__bytes_write.sum of one
+# launch over its frames) on a cut of the workload's scan: roofline.traffic scales them to the
+# launch's frames.
 NCU_DRAM_BYTES_PER_FRAME = {
-    "ml256": {"ml_gamma": 4.51e6, "frame_ml_grad": 3.51e6, "frame_project": 3.54e6,
-              "deriv_sums": 1.06e6, "move": 0.97e6, "back_spectrum": 2.06e6,
-              "object_ml": 2.17e6, "frame_llk": 1.34e6},
-    # the carry pass on the 1024-frame cut of the dm256 scan, profiles/dm256_launch_list.md
+    # the 1000-frame cut of the ml256 scan, one 488-frame launch of each
+    "ml256": {"frame_ml_grad": 3.35e6, "deriv_sums": 1.07e6},
+    # the carry pass on the 1024-frame cut of the dm256 scan
     "dm256": {"frame_carry": 2.33e6},
 }
-NCU_PROFILE = {"ml256": "profiles/ml256_launch_list.md (a 1000-frame cut)",
+NCU_PROFILE = {"ml256": "profiles/ml_gradient_and_position_sums_ml256.md (a 1000-frame cut)",
                "dm256": "profiles/dm256_launch_list.md (a 1024-frame cut)"}
 
 

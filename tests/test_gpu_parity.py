@@ -14,10 +14,12 @@ pytestmark = pytest.mark.gpu
 
 ONE_STEP_TOL = 1e-5
 RUN_TOL = 1e-4
-# LSQML's Poisson far-field step (PtychoShelves' xi solver, engine/lsqml.rs:133-150) weighs
-# pixels by xi = 1 − I/(Ĩ + 1e-5): at the far-field zeros of a hard-edged aperture Ĩ is set by
-# the FP32 FFT's absolute rounding, so over several epochs a_far holds to 3e-4 of its largest.
-AFAR_RUN_TOL = 3e-4
+# One LSQML batch under the Poisson cost on the 64² hard-edged apertures: the residual
+# 1 − I/(Ĩ + 1e-6) and the far-field step's xi = 1 − I/(Ĩ + 1e-5) weigh the pixels at the
+# aperture's far-field zeros, where Ĩ is the FP32 FFT's absolute rounding (~1e-7 of the field's
+# largest value): measured there 3.6e-5 (a_far), 3.7e-5 (a_obj) and 1.8e-5 (probe) of the
+# float64 step, against 1e-6 or less for the amplitude cost and the 128² and 256² probes.
+POISSON_64_ONE_STEP_TOL = 1e-4
 # ML's LLK records after its first Newton step: on the two-mode 64² scan a 1e-7 relative change
 # of the start probe moves the float64 record after the first step by 3.3e-5 (an amplification
 # of ~300), so the FP32 path's records hold to 3e-4 of the largest there.
@@ -113,19 +115,20 @@ def test_lsqml_one_batch(case, cost):
         g.lsqml(1, batch_size=nframe, cost=cost, seed=7)
         got = g.lsqml_steps()
         assert len(got) == 1 and got[0]["frames"] == steps[0]["frames"]
+        tol = POISSON_64_ONE_STEP_TOL if cost == "poisson" and case["n"] == 64 else ONE_STEP_TOL
         for key in ("a_far", "a_obj", "a_probe"):
             a, b = np.array(got[0][key]), np.array(steps[0][key])
-            assert np.abs(a - b).max() <= ONE_STEP_TOL * 10 * np.abs(b).max(), key
-        assert rel_l2(g.object() - case["object"], obj - case["object"]) < ONE_STEP_TOL * 10
-        assert rel_l2(g.probe() - case["probe"], probe - case["probe"]) < ONE_STEP_TOL * 10
+            assert np.abs(a - b).max() <= tol * np.abs(b).max(), key
+        assert rel_l2(g.object() - case["object"], obj - case["object"]) < tol
+        assert rel_l2(g.probe() - case["probe"], probe - case["probe"]) < tol
 
 
 @pytest.mark.parametrize("cost", ["poisson", "amplitude"])
 def test_lsqml_epochs(case, cost):
-    """Three epochs of batches of 8; on the single hard-edged aperture under the Poisson cost,
-    whose residual 1 − I/(Ĩ + 1e-6) is led by the pixels at the aperture's far-field zeros,
-    where Ĩ is FP32 FFT rounding, one epoch (its step sizes drift to 4e-4 in three)."""
-    nepoch = 1 if (cost == "poisson" and case["probe"].shape[0] == 1) else 3
+    """Three epochs of batches of 8: every step's a_far, a_obj and a_probe, the object and the
+    probe to 1e-4 (the worst measured, a_far on the single 64² aperture under the Poisson cost,
+    6e-5)."""
+    nepoch = 3
     obj, probe, steps = lsqml_cpu(case, nepoch, 8, cost)
     with gpu_of(case) as g:
         g.lsqml(nepoch, batch_size=8, cost=cost, seed=7)
@@ -134,8 +137,7 @@ def test_lsqml_epochs(case, cost):
         for gs, cs in zip(got, steps):
             for key in ("a_far", "a_obj", "a_probe"):
                 a, b = np.array(gs[key]), np.array(cs[key])
-                tol = AFAR_RUN_TOL if key == "a_far" else RUN_TOL
-                assert np.abs(a - b).max() <= tol * np.abs(b).max() + 1e-30, key
+                assert np.abs(a - b).max() <= RUN_TOL * np.abs(b).max() + 1e-30, key
         assert rel_l2(g.object(), obj) < RUN_TOL
         assert rel_l2(g.probe(), probe) < RUN_TOL
 
@@ -211,8 +213,7 @@ def test_lsqml_with_positions(case, refine):
         for gs, cs in zip(got, steps):
             for key in ("a_far", "a_obj", "a_probe"):
                 a, b = np.array(gs[key]), np.array(cs[key])
-                tol = AFAR_RUN_TOL if key == "a_far" else RUN_TOL
-                assert np.abs(a - b).max() <= tol * np.abs(b).max(), key
+                assert np.abs(a - b).max() <= RUN_TOL * np.abs(b).max(), key
         assert rel_l2(g.object(), obj) < RUN_TOL
         assert rel_l2(g.probe(), probe) < RUN_TOL
         d = g.positions()
