@@ -61,6 +61,12 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T, 2) gamma_kernel(GammaArgs
   LineTwiddles<N> ltw;
   ltw.load(a.tw, tid % F::G);
   for (int i = tid; i < 3 * H * AS; i += T) acc[i] = 0.f;
+  // the kept detector columns the column phase reads, fetched into L2 now
+  for (int i = tid; i < K * H * (N / 16); i += T) {
+    const int row = i / (N / 16), m = row / H, c = row % H;
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(a.psi + ((size_t)slot * K + m) * N * N +
+                                                  (size_t)(r * H + c) * N + (i % (N / 16)) * 16));
+  }
 
   // The b-term of den, Σ_pix 2·d·2·Re(p̄o·B)/N², by Parseval in the exit plane:
   // 2·Re Σ_x conj(g)·b with g = IDFT(2d·po)/N² the gradient pass's field (0 where masked).
