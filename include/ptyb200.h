@@ -285,6 +285,62 @@ int ptyb_bh(ptyb_handle* h, const ptyb_bh_params* p, int32_t nepoch, int32_t cal
 int ptyb_bh_steps_len(ptyb_handle* h);
 int ptyb_bh_steps(ptyb_handle* h, ptyb_bh_step* dst, int32_t cap);
 
+/* Live ingestion: the reference's pinned host ring of frames and the thread that streams it
+ * into the device store (live/ring.rs:1-31), with the position table the uploader joins each
+ * frame with (live/pos.rs). Workers reserve a slot (ptyb_live_reserve, which blocks while the
+ * ring is full), write the frame's counts into its pinned host memory and commit it with the
+ * frame's uid; positions arrive by uid on their own (ptyb_live_position). The uploader takes
+ * committed frames in sequence order: a frame lands once its position is in (the next place of
+ * the device store, in landing order, converted on the device as ptyb_create converts counts);
+ * one whose position is not valid (a coordinate not finite or |pos| > 1e10) is dropped at once;
+ * one still without its position is dropped pos_wait_ns after its commit, or sooner as soon as
+ * a worker waits for its slot. A slot is released only after its copy to the device has
+ * completed. The uploader copies runs of landed frames that sit in consecutive ring slots (at most
+ * `batch` frames, 0 for 32) in one copy and one conversion launch, as soon as they are joined.
+ * ptyb_live_handle makes a reconstruction handle over the frames landed so far. */
+typedef struct ptyb_live ptyb_live;
+
+typedef struct ptyb_live_params {
+  int32_t device, n, counts_kind; /* frame side; PTYB_COUNTS_U16 or PTYB_COUNTS_F32 */
+  int32_t slots, capacity;        /* ring slots; device store places (frames that can land) */
+  int32_t batch;                  /* most frames in one copy to the device (0: 32) */
+  double wavelength, distance, detector_pixel;
+  int64_t pos_wait_ns;
+} ptyb_live_params;
+
+/* Frames committed, landed (given a store place) and ready (copied and converted); dropped
+ * without a position (pos_wait_ns passed, or, dropped_crowded of them, a worker needed the
+ * slot first), with an invalid position, or with the device store full; reservations that
+ * waited for a slot; frames that reached the head of the ring before their position; copy
+ * batches queued (reference live/ring.rs:570-600, UploadReport). */
+typedef struct ptyb_live_stats {
+  int64_t committed, landed, ready, dropped_no_position, dropped_crowded, dropped_invalid,
+      dropped_full, stalls, pos_waits, batches;
+} ptyb_live_stats;
+
+int ptyb_live_create(const ptyb_live_params* p, ptyb_live** out);
+/* A slot for the next frame (sequence number *seq) and its pinned host frame to fill. */
+int ptyb_live_reserve(ptyb_live* l, int64_t* seq, void** frame);
+int ptyb_live_commit(ptyb_live* l, int64_t seq, int64_t uid);
+/* The position (metres) of frame `uid`. */
+int ptyb_live_position(ptyb_live* l, int64_t uid, double y, double x);
+/* Waits (at most timeout_ms) until every committed frame has landed or dropped and every
+ * landed frame's copy and conversion has completed; PTYB_GPU on a device failure, PTYB_INVALID
+ * on the timeout. */
+int ptyb_live_flush(ptyb_live* l, int32_t timeout_ms);
+int ptyb_live_get_stats(ptyb_live* l, ptyb_live_stats* out);
+/* The uids and positions of the landed frames in landing order (at most cap; any of the three
+ * arrays may be NULL); returns how many were written. */
+int ptyb_live_landed(ptyb_live* l, int64_t* uids, double* y, double* x, int32_t cap);
+/* A handle (as ptyb_create, on the ring's device: options->device is not read) over the frames
+ * landed and converted so far, in landing order, with their positions; the counts are copied on
+ * the device. *nframe (if not NULL) receives the handle's frame count. */
+int ptyb_live_handle(ptyb_live* l, const double* object, int32_t nyo, int32_t nxo,
+                     const double* probe, int32_t nprobe, const ptyb_options* options,
+                     ptyb_handle** out, int32_t* nframe);
+const char* ptyb_live_last_error(ptyb_live* l);
+void ptyb_live_destroy(ptyb_live* l);
+
 /* Reference `GpuPtycho::{object, probe, set_object}` (engine/gpu/mod.rs:763-817). */
 int ptyb_get_object(ptyb_handle* h, double* dst);
 int ptyb_get_probe(ptyb_handle* h, double* dst);

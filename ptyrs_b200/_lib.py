@@ -77,6 +77,18 @@ class BhStep(ctypes.Structure):
                 ("top", c_double), ("bottom", c_double)]
 
 
+class LiveParams(ctypes.Structure):
+    _fields_ = [("device", c_int32), ("n", c_int32), ("counts_kind", c_int32), ("slots", c_int32),
+                ("capacity", c_int32), ("batch", c_int32), ("wavelength", c_double),
+                ("distance", c_double), ("detector_pixel", c_double), ("pos_wait_ns", c_int64)]
+
+
+class LiveStats(ctypes.Structure):
+    _fields_ = [(k, c_int64) for k in ("committed", "landed", "ready", "dropped_no_position",
+                                       "dropped_crowded", "dropped_invalid", "dropped_full",
+                                       "stalls", "pos_waits", "batches")]
+
+
 # Every symbol include/ptyb200.h declares, with (restype, argtypes).
 SIGNATURES = {
     "ptyb_create": (c_int32, [P(Scan), P(c_double), c_int32, c_int32, c_int32, P(c_double),
@@ -108,6 +120,17 @@ SIGNATURES = {
                                                  P(ctypes.c_float)]),
     "ptyb_set_positions": (c_int32, [c_void_p, P(c_double), c_int32]),
     "ptyb_get_positions": (c_int32, [c_void_p, P(c_double)]),
+    "ptyb_live_create": (c_int32, [P(LiveParams), P(c_void_p)]),
+    "ptyb_live_reserve": (c_int32, [c_void_p, P(c_int64), P(c_void_p)]),
+    "ptyb_live_commit": (c_int32, [c_void_p, c_int64, c_int64]),
+    "ptyb_live_position": (c_int32, [c_void_p, c_int64, c_double, c_double]),
+    "ptyb_live_flush": (c_int32, [c_void_p, c_int32]),
+    "ptyb_live_get_stats": (c_int32, [c_void_p, P(LiveStats)]),
+    "ptyb_live_landed": (c_int32, [c_void_p, P(c_int64), P(c_double), P(c_double), c_int32]),
+    "ptyb_live_handle": (c_int32, [c_void_p, P(c_double), c_int32, c_int32, P(c_double),
+                                   c_int32, P(Options), P(c_void_p), P(c_int32)]),
+    "ptyb_live_last_error": (ctypes.c_char_p, [c_void_p]),
+    "ptyb_live_destroy": (None, [c_void_p]),
     "ptyb_get_object": (c_int32, [c_void_p, P(c_double)]),
     "ptyb_get_probe": (c_int32, [c_void_p, P(c_double)]),
     "ptyb_set_object": (c_int32, [c_void_p, P(c_double)]),

@@ -15,7 +15,7 @@ OUT = os.path.join(HERE, "libptyb200.so")
 # the per-side kernel units first: they take longest
 SOURCES = ["kernels_256.cu", "kernels_192.cu", "kernels_128.cu", "kernels_96.cu",
            "kernels_64.cu", "engine.cu", "rpie.cu", "lsqml.cu", "ml.cu", "carried.cu",
-           "bh.cu", "batch.cu", "forward.cu", "scan.cpp"]
+           "bh.cu", "batch.cu", "forward.cu", "live.cu", "scan.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC"]
 

@@ -741,6 +741,95 @@ void split_scale(ptyb_handle* h, double s, float2* waves) {
   }
 }
 
+// The state every handle holds past its counts (h->iobs, h->obs_total, h->max_power,
+// h->nb_obs) and its corners (h->corners_h): the corners, object and probe on the device, the
+// far-field phase, the twiddles, the angular-spectrum gaps of a multislice object and the
+// per-frame scratch. The handle's stream exists; the caller runs this inside `guarded`.
+void finish_state(ptyb_handle* h, const double* object, const double* probe, double wavelength,
+                  double distance, const double* gaps) {
+  const int N = h->N, nslice = h->nslice, nobj = h->nobj, nprobe = h->nprobe, K = h->K;
+  const int nyo = h->nyo, nxo = h->nxo;
+  const size_t plane = (size_t)N * N;
+  h->corners = alloc<int2>(h, h->P);
+  check(h, copy_sync(h, h->corners, h->corners_h.data(), h->P * sizeof(int2), cudaMemcpyHostToDevice),
+        "corners upload");
+  h->object = alloc<float2>(h, (size_t)nslice * nobj * nyo * nxo);
+  upload_c64(h, object, h->object, (size_t)nslice * nobj * nyo * nxo, "object upload");
+  h->probe = alloc<float2>(h, (size_t)nprobe * plane);
+  upload_c64(h, probe, h->probe, (size_t)nprobe * plane, "probe upload");
+  // Far-field plane phase (engine/ops.rs:17-33) and the FFT twiddles, in double.
+  std::vector<float2> q(plane), tw(N);
+  const double fq = M_PI / (wavelength * distance);
+  for (int yy = 0; yy < N; ++yy)
+    for (int xx = 0; xx < N; ++xx) {
+      const double dy = (double)yy - (double)(N / 2), dx = (double)xx - (double)(N / 2);
+      const double ph =
+          fq * (dx * dx * h->pixel[1] * h->pixel[1] + dy * dy * h->pixel[0] * h->pixel[0]);
+      q[(size_t)yy * N + xx] = make_float2((float)std::cos(ph), (float)std::sin(ph));
+    }
+  for (int t = 0; t < N; ++t)
+    tw[t] = make_float2((float)std::cos(2.0 * M_PI * t / N), (float)-std::sin(2.0 * M_PI * t / N));
+  h->quad = alloc<float2>(h, plane);
+  check(h, copy_sync(h, h->quad, q.data(), plane * sizeof(float2), cudaMemcpyHostToDevice), "quad");
+  h->tw = alloc<float2>(h, N);
+  check(h, copy_sync(h, h->tw, tw.data(), N * sizeof(float2), cudaMemcpyHostToDevice), "tw");
+  std::vector<int> iota(h->P);
+  for (int f = 0; f < h->P; ++f) iota[f] = f;
+  h->iota = alloc<int>(h, h->P);
+  check(h, copy_sync(h, h->iota, iota.data(), h->P * sizeof(int), cudaMemcpyHostToDevice), "iota");
+  h->order = alloc<int>(h, h->P);
+  h->afar_all = alloc<float>(h, h->P);
+  h->llk = alloc<double>(h, (size_t)h->P * 4);
+  h->scal = alloc<float>(h, kScalars);
+  h->pre = alloc<float>(h, (size_t)nyo * nxo);
+  h->d_obj = alloc<float2>(h, (size_t)nslice * nyo * nxo);
+  h->d_probe = alloc<float2>(h, (size_t)K * plane);
+  h->steplog = alloc<double>(h, (size_t)h->P * h->log_stride);
+  check(h, fill_sync(h, h->scal, 0, kScalars * sizeof(float)), "memset");
+  if (nslice > 1) {
+    // Angular-spectrum transfer functions exp(2πi z √(1 − r)) of the gaps in DFT order, 0 on
+    // the evanescent band (engine/propagate.rs:505-531), in double; the plane of ones is the
+    // phase of every slice but the last.
+    const double width = h->pixel[1] / wavelength, ar = h->pixel[1] / h->pixel[0];
+    std::vector<float2> t((size_t)(nslice - 1) * plane), ones(plane, make_float2(1.f, 0.f));
+    for (int g = 0; g + 1 < nslice; ++g) {
+      const double i2piz = 2.0 * M_PI * (gaps[g] / wavelength);
+      for (int yy = 0; yy < N; ++yy)
+        for (int xx = 0; xx < N; ++xx) {
+          const double fy = (double)(yy < N / 2 ? yy : yy - N) / N;
+          const double fx = (double)(xx < N / 2 ? xx : xx - N) / N;
+          const double ratio = (fx * fx + (ar * fy) * (ar * fy)) / (width * width);
+          float2 v = make_float2(0.f, 0.f);
+          if (ratio < 1.0) {
+            const double ph = i2piz * std::sqrt(1.0 - ratio);
+            v = make_float2((float)std::cos(ph), (float)std::sin(ph));
+          }
+          t[(size_t)g * plane + (size_t)yy * N + xx] = v;
+        }
+    }
+    h->tf = alloc<float2>(h, t.size());
+    check(h, copy_sync(h, h->tf, t.data(), t.size() * sizeof(float2), cudaMemcpyHostToDevice), "tf");
+    h->ones = alloc<float2>(h, plane);
+    check(h, copy_sync(h, h->ones, ones.data(), plane * sizeof(float2), cudaMemcpyHostToDevice),
+          "ones");
+  }
+}
+
+cudaError_t convert_counts(const void* raw, int kind, float* iobs, double* power, int* nobs,
+                           int* bad, int nframe, int N, cudaStream_t s) {
+  if (nframe <= 0) return cudaSuccess;
+  if (kind == PTYB_COUNTS_U16)
+    counts_kernel<<<nframe, 256, 0, s>>>(static_cast<const uint16_t*>(raw), 1, iobs, power, nobs,
+                                         bad, N);
+  else if (kind == PTYB_COUNTS_F32)
+    counts_kernel<<<nframe, 256, 0, s>>>(static_cast<const float*>(raw), 0, iobs, power, nobs,
+                                         bad, N);
+  else
+    counts_kernel<<<nframe, 256, 0, s>>>(static_cast<const double*>(raw), 0, iobs, power, nobs,
+                                         bad, N);
+  return cudaGetLastError();
+}
+
 thread_local std::string g_create_error;
 
 // A handle over `nslice` object slices (each one object mode) with the angular-spectrum gaps
@@ -831,16 +920,8 @@ int create_handle(const ptyb_scan* scan, const double* object, int32_t nobj, int
     check(h, fill_sync(h, nobs, 0, (h->P + 1) * sizeof(int)), "memset");
     cudaError_t e = copy_sync(h, raw, scan->counts, nval * esize, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) {
-      if (scan->counts_kind == PTYB_COUNTS_U16)
-        counts_kernel<<<h->P, 256, 0, h->stream>>>(static_cast<const uint16_t*>(raw), 1, h->iobs,
-                                                   power, nobs, nobs + h->P, N);
-      else if (scan->counts_kind == PTYB_COUNTS_F32)
-        counts_kernel<<<h->P, 256, 0, h->stream>>>(static_cast<const float*>(raw), 0, h->iobs,
-                                                   power, nobs, nobs + h->P, N);
-      else
-        counts_kernel<<<h->P, 256, 0, h->stream>>>(static_cast<const double*>(raw), 0, h->iobs,
-                                                   power, nobs, nobs + h->P, N);
-      e = cudaGetLastError();
+      e = convert_counts(raw, scan->counts_kind, h->iobs, power, nobs, nobs + h->P, h->P, N,
+                         h->stream);
       ++h->launches;
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
@@ -859,69 +940,7 @@ int create_handle(const ptyb_scan* scan, const double* object, int32_t nobj, int
       h->max_power = std::max(h->max_power, pw[f]);
       h->nb_obs += nb[f];
     }
-    h->corners = alloc<int2>(h, h->P);
-    check(h, copy_sync(h, h->corners, h->corners_h.data(), h->P * sizeof(int2), cudaMemcpyHostToDevice),
-          "corners upload");
-    h->object = alloc<float2>(h, (size_t)nslice * nobj * nyo * nxo);
-    upload_c64(h, object, h->object, (size_t)nslice * nobj * nyo * nxo, "object upload");
-    h->probe = alloc<float2>(h, (size_t)nprobe * plane);
-    upload_c64(h, probe, h->probe, (size_t)nprobe * plane, "probe upload");
-    // Far-field plane phase (engine/ops.rs:17-33) and the FFT twiddles, in double.
-    std::vector<float2> q(plane), tw(N);
-    const double fq = M_PI / (scan->wavelength * scan->distance);
-    for (int yy = 0; yy < N; ++yy)
-      for (int xx = 0; xx < N; ++xx) {
-        const double dy = (double)yy - (double)(N / 2), dx = (double)xx - (double)(N / 2);
-        const double ph =
-            fq * (dx * dx * h->pixel[1] * h->pixel[1] + dy * dy * h->pixel[0] * h->pixel[0]);
-        q[(size_t)yy * N + xx] = make_float2((float)std::cos(ph), (float)std::sin(ph));
-      }
-    for (int t = 0; t < N; ++t)
-      tw[t] = make_float2((float)std::cos(2.0 * M_PI * t / N), (float)-std::sin(2.0 * M_PI * t / N));
-    h->quad = alloc<float2>(h, plane);
-    check(h, copy_sync(h, h->quad, q.data(), plane * sizeof(float2), cudaMemcpyHostToDevice), "quad");
-    h->tw = alloc<float2>(h, N);
-    check(h, copy_sync(h, h->tw, tw.data(), N * sizeof(float2), cudaMemcpyHostToDevice), "tw");
-    std::vector<int> iota(h->P);
-    for (int f = 0; f < h->P; ++f) iota[f] = f;
-    h->iota = alloc<int>(h, h->P);
-    check(h, copy_sync(h, h->iota, iota.data(), h->P * sizeof(int), cudaMemcpyHostToDevice), "iota");
-    h->order = alloc<int>(h, h->P);
-    h->afar_all = alloc<float>(h, h->P);
-    h->llk = alloc<double>(h, (size_t)h->P * 4);
-    h->scal = alloc<float>(h, kScalars);
-    h->pre = alloc<float>(h, (size_t)nyo * nxo);
-    h->d_obj = alloc<float2>(h, (size_t)nslice * nyo * nxo);
-    h->d_probe = alloc<float2>(h, (size_t)K * plane);
-    h->steplog = alloc<double>(h, (size_t)h->P * h->log_stride);
-    check(h, fill_sync(h, h->scal, 0, kScalars * sizeof(float)), "memset");
-    if (nslice > 1) {
-      // Angular-spectrum transfer functions exp(2πi z √(1 − r)) of the gaps in DFT order, 0 on
-      // the evanescent band (engine/propagate.rs:505-531), in double; the plane of ones is the
-      // phase of every slice but the last.
-      const double width = h->pixel[1] / scan->wavelength, ar = h->pixel[1] / h->pixel[0];
-      std::vector<float2> t((size_t)(nslice - 1) * plane), ones(plane, make_float2(1.f, 0.f));
-      for (int g = 0; g + 1 < nslice; ++g) {
-        const double i2piz = 2.0 * M_PI * (gaps[g] / scan->wavelength);
-        for (int yy = 0; yy < N; ++yy)
-          for (int xx = 0; xx < N; ++xx) {
-            const double fy = (double)(yy < N / 2 ? yy : yy - N) / N;
-            const double fx = (double)(xx < N / 2 ? xx : xx - N) / N;
-            const double ratio = (fx * fx + (ar * fy) * (ar * fy)) / (width * width);
-            float2 v = make_float2(0.f, 0.f);
-            if (ratio < 1.0) {
-              const double ph = i2piz * std::sqrt(1.0 - ratio);
-              v = make_float2((float)std::cos(ph), (float)std::sin(ph));
-            }
-            t[(size_t)g * plane + (size_t)yy * N + xx] = v;
-          }
-      }
-      h->tf = alloc<float2>(h, t.size());
-      check(h, copy_sync(h, h->tf, t.data(), t.size() * sizeof(float2), cudaMemcpyHostToDevice), "tf");
-      h->ones = alloc<float2>(h, plane);
-      check(h, copy_sync(h, h->ones, ones.data(), plane * sizeof(float2), cudaMemcpyHostToDevice),
-            "ones");
-    }
+    finish_state(h, object, probe, scan->wavelength, scan->distance, gaps);
     return PTYB_OK;
   });
   if (rc != PTYB_OK) {

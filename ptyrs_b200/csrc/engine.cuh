@@ -345,6 +345,13 @@ void ensure_ml(ptyb_handle* h);
 void array_sums(ptyb_handle* h, const float2* g, const float2* hh, size_t n, int mode,
                 double out[2]);
 unsigned blocks_for(size_t n);
+void finish_state(ptyb_handle* h, const double* object, const double* probe, double wavelength,
+                  double distance, const double* gaps);
+// Raw counts of `nframe` frames (PTYB_COUNTS_*, detector order) to the FFT-shifted float layout
+// with masked pixels −1, each frame's photon sum and unmasked count; `*bad` set by a non-finite
+// unmasked value (engine/obs.rs:61-76).
+cudaError_t convert_counts(const void* raw, int kind, float* iobs, double* power, int* nobs,
+                           int* bad, int nframe, int N, cudaStream_t s);
 void zero_phase_ramp(ptyb_handle* h);
 void scale_obj_probe(ptyb_handle* h, float2* waves = nullptr);
 void split_scale(ptyb_handle* h, double s, float2* waves);

@@ -94,6 +94,19 @@ class GpuPtycho:
             raise PtybError(STATUS.get(rc, rc), self._lib.ptyb_last_error(None).decode())
         self._h = h
 
+    @classmethod
+    def _adopt(cls, h, obj_shape, probe_shape, nframe):
+        """A GpuPtycho that owns the single-slice handle `h` made by another entry point (the
+        live ring's ptyb_live_handle)."""
+        self = cls.__new__(cls)
+        self._lib = _lib.load()
+        self._nslice = 1
+        self._obj_shape = tuple(obj_shape)
+        self._probe_shape = tuple(probe_shape)
+        self._nframe = nframe
+        self._h = h
+        return self
+
     def _check(self, rc):
         if rc != 0:
             raise PtybError(STATUS.get(rc, rc), self._lib.ptyb_last_error(self._h).decode())

@@ -88,3 +88,15 @@ def test_view_corners_rejects_a_window_outside(lib):
     y = np.array([0.0, 200.0]) * px
     with pytest.raises(PtybError):
         view_corners(y, y, [px, px], [64, 64], [128, 128])
+
+
+def test_live_ring_refuses_bad_parameters_before_any_device_call():
+    from ptyrs_b200.live import LiveRing
+    from ptyrs_b200 import PtybError
+    for kw in (dict(n=100), dict(n=64, slots=0), dict(n=64, capacity=0), dict(n=64, batch=-1),
+               dict(n=64, pos_wait_s=-1.0)):
+        n = kw.pop("n")
+        with pytest.raises(PtybError, match="invalid: live"):
+            LiveRing(n, 1.5e-10, 1.0, 75e-6, **kw)
+    with pytest.raises(PtybError, match="invalid: live"):
+        LiveRing(64, 0.0, 1.0, 75e-6)
