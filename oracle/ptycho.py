@@ -285,9 +285,11 @@ class Ptycho:
         return s.position_sums(self.object, psi, nframe)
 
     def ml(self, ncycle, update_object=True, update_probe=False, calc_llk=0,
-           zero_phase_ramp=True):
+           zero_phase_ramp=True, after_cycle=None):
         """PyNX ML Poisson CG (engine/ptycho.rs:775-842); refined offsets take AP's and DM's
-        position step from the estimate each cycle starts from, after the update."""
+        position step from the estimate each cycle starts from, after the update.
+        `after_cycle(ic)`, if given, runs after cycle ic (a checkpoint hook; the run is the
+        same without it)."""
         self.scale_obj_probe()
         last = None
         d_obj = np.zeros_like(self.object)
@@ -322,6 +324,8 @@ class Ptycho:
             if l is not None:
                 self.record("ml", l)
             self.cycle += 1
+            if after_cycle is not None:
+                after_cycle(ic)
         if zero_phase_ramp:
             self.zero_phase_ramp()
 

@@ -223,7 +223,7 @@ def opr_start(probe, nframe, k=2, seed=3):
     return np.array(u), rng.uniform(-0.1, 0.1, (nframe, k)), np.ones(nframe)
 
 
-def make_scan(kind, seed=0, scale=1.0):
+def make_scan(kind, seed=0, scale=1.0, device=None):
     """Seeded synthetic inputs of a benchmark configuration: returns a dict with counts
     (float32), y, x (metres), object start, probe start, truth object and sizes.
 
@@ -232,8 +232,9 @@ def make_scan(kind, seed=0, scale=1.0):
     6 px, 1e6 photons. kind "ml256": 2048² object, 256² probe with 2 modes (0.8/0.2), Fermat
     10000 at 12 px, 1e7 photons, the frames taken at true positions off the nominal ones by
     seeded N(0, 1.5 px) offsets (`true_offsets`; the solver is given the nominal positions),
-    counts generated on the CUDA device. `scale` < 1 keeps that fraction of the positions (the
-    same first ones) for small cases. kind "fermat256": 1280² object, 256² probe with 2 modes
+    counts generated on the CUDA device (`device`: "cpu" makes them with torch on the host,
+    the same counts on every machine of this image). `scale` < 1 keeps that fraction of the
+    positions (the same first ones) for small cases. kind "fermat256": 1280² object, 256² probe with 2 modes
     (0.8/0.2), Fermat 4096 at 12 px, 1e7 photons, counts on the CUDA device (the scan of the
     AP / DM / RAAR workloads). kind "ms128": three slices of 1536² (phase scale π/4, independent
     seeds) 10 µm apart, λ = 0.1 nm at a 10 nm object pixel (detector 0.96 m away, 75 µm
@@ -279,9 +280,11 @@ def make_scan(kind, seed=0, scale=1.0):
     true_offsets = np.zeros((len(pos), 2))
     if kind == "ml256":
         true_offsets = np.random.default_rng(seed + 4).normal(0.0, 1.5, (len(pos), 2))
-        counts = far_field_counts_gpu(truth, probe, c, true_offsets, photons, seed + 3)
+        counts = far_field_counts_gpu(truth, probe, c, true_offsets, photons, seed + 3,
+                                      device=device)
     elif kind == "fermat256":
-        counts = far_field_counts_gpu(truth, probe, c, true_offsets, photons, seed + 3)
+        counts = far_field_counts_gpu(truth, probe, c, true_offsets, photons, seed + 3,
+                                      device=device)
     else:
         counts = far_field_counts(truth, probe, c, photons, seed + 3)
     px = object_pixel(n)

@@ -14,14 +14,17 @@ def clusters_for(n):
     return {64: [1], 96: [2], 128: [2, 4], 192: [8], 256: [16, 8]}.get(n, [0])
 
 
-def autotune(scan, obj, probe, run, prepare=None, stacks=(256, 512, 1024), clusters=None,
-             device=0, **kw):
+def autotune(scan, obj, probe, run, prepare=None, stacks=None, clusters=None, device=0, **kw):
     """`(best, table)`: `best` the `dict(cluster=..., stack_size=...)` of the fastest timed call
     of `run(handle)` (its device time: the float `run` returns, else the handle's last call's)
     and `table` every candidate's `(ms, options)` (None if it failed);
-    `prepare(handle)` sets each fresh handle up (positions and the like) before the warm-up."""
+    `prepare(handle)` sets each fresh handle up (positions and the like) before the warm-up.
+    The default stacks run 512, 1024 and 4096 frames per launch and the whole scan in one."""
     n = probe.shape[-1]
     clusters = clusters_for(n) if clusters is None else clusters
+    if stacks is None:
+        nframe = scan.counts.shape[0]
+        stacks = sorted({min(st, nframe) for st in (512, 1024, 4096, nframe)})
     table = []
     for c, st in itertools.product(clusters, stacks):
         opts = dict(cluster=c, stack_size=st)

@@ -1,0 +1,149 @@
+"""Parity at the benchmark configurations' full size: the FP32 CUDA path against the float64
+oracle over whole scans, at checkpoints of one run (test infrastructure, not the product).
+
+    python tests/at_size.py oracle CONFIG DIR   # host only: the oracle's run and checkpoints
+    python tests/at_size.py gpu CONFIG DIR OUT  # the CUDA path from the same inputs, compared
+
+CONFIG is one of CONFIGS: rpie64 (400 frames of 64², rPIE with α = β = 0.1 in batches of 100),
+lsqml128 (4096 frames of 128² × 3 modes, Poisson LSQML in batches of 256) and ml256 (10000
+frames of 256² × 2 modes, Poisson ML conjugate gradient refining the positions). The inputs
+are the benchmark's seeded scans (`sim.make_scan`; ml256's counts made with torch on the host,
+so both phases read the same counts, checked by a digest). The oracle phase runs one call of
+the longest run and keeps a snapshot after each checkpoint's iteration; the GPU phase runs
+each checkpoint as one call of that many iterations on a fresh state (the calls are the
+reference's: a k-iteration call is the first k iterations of a longer one) and writes, per
+checkpoint, the object's and probe's relative L2 error against the oracle's, the object NRMSE
+with the global phase and a phase ramp removed (scale kept) over the illuminated pixels, and
+for ml256 the largest difference of the refined offsets.
+"""
+import hashlib
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    "rpie64": dict(kind="rpie64", algorithm="rpie", batch=100, checkpoints=[1, 2, 5, 10, 20, 50]),
+    "lsqml128": dict(kind="lsqml128", algorithm="lsqml", batch=256, checkpoints=[1, 2, 5, 10]),
+    "ml256": dict(kind="ml256", algorithm="ml", checkpoints=[1, 2]),
+}
+
+
+def inputs(cfg):
+    from ptyrs_b200 import sim
+    s = sim.make_scan(cfg["kind"], seed=0, device="cpu")
+    digest = hashlib.sha256(np.ascontiguousarray(s["counts"]).tobytes()).hexdigest()
+    return s, digest
+
+
+def optics_of(s):
+    from oracle import ops
+    return ops.Optics.far_field(s["wavelength"], s["distance"], s["detector_pixel"],
+                                [s["n"], s["n"]])
+
+
+def run_oracle(name, out):
+    """The oracle's run of the longest checkpoint, a snapshot at each checkpoint."""
+    from oracle import ops
+    from oracle.lsqml import Lsqml
+    from oracle.ptycho import Ptycho
+    cfg = CONFIGS[name]
+    os.makedirs(out, exist_ok=True)
+    t0 = time.perf_counter()
+    s, digest = inputs(cfg)
+    optics = optics_of(s)
+    p = Ptycho(s["counts"], s["y"], s["x"], optics, s["object"], s["probe"])
+    illum = ops.illumination(p.addr.views, p.object.shape, p.probe)
+    mask = illum >= 1e-3 * illum.max()
+    last = max(cfg["checkpoints"])
+    times = {}
+
+    def save(k, obj, probe, offsets=None):
+        times[k] = time.perf_counter() - t0
+        np.savez(os.path.join(out, f"{name}_{k}.npz"), object=obj.astype(np.complex64),
+                 probe=probe, offsets=np.zeros(0) if offsets is None else offsets)
+        print(f"{name}: checkpoint {k} at {times[k]:.0f} s", flush=True)
+
+    if cfg["algorithm"] == "rpie":
+        for k in range(1, last + 1):
+            p.rpie(1, batch_size=cfg["batch"], obj_alpha=0.1, probe_alpha=0.1, seed=7)
+            if k in cfg["checkpoints"]:
+                save(k, p.object, p.probe)
+    elif cfg["algorithm"] == "lsqml":
+        run = Lsqml(cfg["batch"], "poisson", 7)
+        obj, probe = p.object, p.probe
+        for k in range(1, last + 1):
+            obj, probe, _ = run.epoch(p.addr, p.obs, optics, obj, probe)
+            if k in cfg["checkpoints"]:
+                save(k, obj, probe)
+    else:
+        p.set_positions(np.zeros((p.addr.nframe, 2)), refine=True)
+
+        def after(ic):
+            if ic + 1 in cfg["checkpoints"]:
+                save(ic + 1, p.object, p.probe, p.offsets.copy())
+
+        p.ml(last, update_object=True, update_probe=True, calc_llk=0, zero_phase_ramp=False,
+             after_cycle=after)
+    np.savez(os.path.join(out, f"{name}_mask.npz"), mask=np.packbits(mask), shape=mask.shape)
+    with open(os.path.join(out, f"{name}_meta.json"), "w") as f:
+        json.dump({"config": name, "digest": digest, "seconds": times,
+                   "threads": os.cpu_count()}, f)
+
+
+def run_gpu(name, ref, out):
+    """Each checkpoint on the CUDA path, compared with the oracle's snapshot."""
+    from ptyrs_b200 import GpuPtycho, Scan
+    from ptyrs_b200.metrics import object_nrmse
+    cfg = CONFIGS[name]
+    meta = json.load(open(os.path.join(ref, f"{name}_meta.json")))
+    s, digest = inputs(cfg)
+    if digest != meta["digest"]:
+        raise RuntimeError("the inputs differ from the oracle run's")
+    m = np.load(os.path.join(ref, f"{name}_mask.npz"))
+    mask = np.unpackbits(m["mask"])[:int(np.prod(m["shape"]))].reshape(m["shape"])
+    scan = Scan(s["counts"], s["y"], s["x"], s["wavelength"], s["distance"], s["detector_pixel"])
+    rows = []
+    for k in cfg["checkpoints"]:
+        r = np.load(os.path.join(ref, f"{name}_{k}.npz"))
+        with GpuPtycho(scan, s["object"], s["probe"]) as g:
+            if cfg["algorithm"] == "rpie":
+                g.rpie(k, batch_size=cfg["batch"], obj_alpha=0.1, probe_alpha=0.1, seed=7)
+            elif cfg["algorithm"] == "lsqml":
+                g.lsqml(k, batch_size=cfg["batch"], cost="poisson", seed=7)
+            else:
+                g.set_positions(np.zeros((len(s["counts"]), 2)), refine=True)
+                g.ml(k, update_object=True, update_probe=True, calc_llk=0,
+                     zero_phase_ramp=False)
+            obj, probe = g.object(), g.probe()
+            d = g.positions() if cfg["algorithm"] == "ml" else None
+        ro, rp = r["object"].astype(np.complex128), r["probe"]
+        row = {"iterations": k,
+               "object_rel_l2": float(np.linalg.norm(obj - ro) / np.linalg.norm(ro)),
+               "object_rel_l2_illuminated": float(np.linalg.norm((obj - ro)[0][mask])
+                                                  / np.linalg.norm(ro[0][mask])),
+               "probe_rel_l2": float(np.linalg.norm(probe - rp) / np.linalg.norm(rp)),
+               "object_nrmse": object_nrmse(obj, ro, mask.astype(float)[None])}
+        if d is not None:
+            row["offsets_max_abs_diff_px"] = float(np.abs(d - r["offsets"]).max())
+        rows.append(row)
+        print(json.dumps(row), flush=True)
+    with open(out, "w") as f:
+        json.dump({"config": name, "frames": len(s["counts"]), "n": s["n"],
+                   "object": list(s["object"].shape), "modes": s["probe"].shape[0],
+                   "oracle_seconds": meta["seconds"], "oracle_threads": meta["threads"],
+                   "rows": rows}, f, indent=1)
+
+
+if __name__ == "__main__":
+    if len(sys.argv) < 4 or sys.argv[1] not in ("oracle", "gpu") or sys.argv[2] not in CONFIGS:
+        raise SystemExit(__doc__)
+    if sys.argv[1] == "oracle":
+        run_oracle(sys.argv[2], sys.argv[3])
+    else:
+        run_gpu(sys.argv[2], sys.argv[3], sys.argv[4])
