@@ -3,6 +3,8 @@ oracle over whole scans, at checkpoints of one run (test infrastructure, not the
 
     python tests/at_size.py oracle CONFIG DIR   # host only: the oracle's run and checkpoints
     python tests/at_size.py gpu CONFIG DIR OUT  # the CUDA path from the same inputs, compared
+    python tests/at_size.py sensitivity CONFIG DIR OUT [EPS]  # the oracle from a start
+                                                # perturbed by EPS (1e-7), compared the same way
 
 CONFIG is one of CONFIGS: rpie64 (400 frames of 64², rPIE with α = β = 0.1 in batches of 100),
 lsqml128 (4096 frames of 128² × 3 modes, Poisson LSQML in batches of 256) and ml256 (10000
@@ -14,7 +16,9 @@ each checkpoint as one call of that many iterations on a fresh state (the calls 
 reference's: a k-iteration call is the first k iterations of a longer one) and writes, per
 checkpoint, the object's and probe's relative L2 error against the oracle's, the object NRMSE
 with the global phase and a phase ramp removed (scale kept) over the illuminated pixels, and
-for ml256 the largest difference of the refined offsets.
+for ml256 the largest difference of the refined offsets. The sensitivity phase measures how far
+the float64 run itself moves when its start object is multiplied by (1 + EPS·ξ), ξ seeded
+complex normal: the scale of difference that rounding alone leaves after k iterations.
 """
 import hashlib
 import json
@@ -29,7 +33,8 @@ sys.path.insert(0, ROOT)
 
 CONFIGS = {
     "rpie64": dict(kind="rpie64", algorithm="rpie", batch=100, checkpoints=[1, 2, 5, 10, 20, 50]),
-    "lsqml128": dict(kind="lsqml128", algorithm="lsqml", batch=256, checkpoints=[1, 2, 5, 10]),
+    "lsqml128": dict(kind="lsqml128", algorithm="lsqml", batch=256,
+                     checkpoints=[1, 2, 5, 10, 20, 50, 100]),
     "ml256": dict(kind="ml256", algorithm="ml", checkpoints=[1, 2]),
 }
 
@@ -47,8 +52,10 @@ def optics_of(s):
                                 [s["n"], s["n"]])
 
 
-def run_oracle(name, out):
-    """The oracle's run of the longest checkpoint, a snapshot at each checkpoint."""
+def run_oracle(name, out, eps=0.0, save_as=None):
+    """The oracle's run of the longest checkpoint, a snapshot at each checkpoint (`save_as(k,
+    obj, probe, offsets)` instead of the files when given); the start object perturbed by
+    `eps` when it is not 0."""
     from oracle import ops
     from oracle.lsqml import Lsqml
     from oracle.ptycho import Ptycho
@@ -57,7 +64,12 @@ def run_oracle(name, out):
     t0 = time.perf_counter()
     s, digest = inputs(cfg)
     optics = optics_of(s)
-    p = Ptycho(s["counts"], s["y"], s["x"], optics, s["object"], s["probe"])
+    start = s["object"]
+    if eps:
+        rng = np.random.default_rng(11)
+        xi = (rng.standard_normal(start.shape) + 1j * rng.standard_normal(start.shape)) / np.sqrt(2)
+        start = start * (1.0 + eps * xi)
+    p = Ptycho(s["counts"], s["y"], s["x"], optics, start, s["probe"])
     illum = ops.illumination(p.addr.views, p.object.shape, p.probe)
     mask = illum >= 1e-3 * illum.max()
     last = max(cfg["checkpoints"])
@@ -65,6 +77,9 @@ def run_oracle(name, out):
 
     def save(k, obj, probe, offsets=None):
         times[k] = time.perf_counter() - t0
+        if save_as is not None:
+            save_as(k, obj, probe, offsets)
+            return
         np.savez(os.path.join(out, f"{name}_{k}.npz"), object=obj.astype(np.complex64),
                  probe=probe, offsets=np.zeros(0) if offsets is None else offsets)
         print(f"{name}: checkpoint {k} at {times[k]:.0f} s", flush=True)
@@ -90,27 +105,53 @@ def run_oracle(name, out):
 
         p.ml(last, update_object=True, update_probe=True, calc_llk=0, zero_phase_ramp=False,
              after_cycle=after)
+    if save_as is not None:
+        return
     np.savez(os.path.join(out, f"{name}_mask.npz"), mask=np.packbits(mask), shape=mask.shape)
     with open(os.path.join(out, f"{name}_meta.json"), "w") as f:
         json.dump({"config": name, "digest": digest, "seconds": times,
                    "threads": os.cpu_count()}, f)
 
 
+def compare(name, ref, k, obj, probe, offsets):
+    """One checkpoint's row against the oracle's snapshot in `ref`."""
+    from ptyrs_b200.metrics import object_nrmse
+    m = np.load(os.path.join(ref, f"{name}_mask.npz"))
+    mask = np.unpackbits(m["mask"])[:int(np.prod(m["shape"]))].reshape(m["shape"])
+    mask = mask.reshape(mask.shape[-2:]).astype(bool)  # one object mode
+    r = np.load(os.path.join(ref, f"{name}_{k}.npz"))
+    ro, rp = r["object"].astype(np.complex128), r["probe"]
+    row = {"iterations": k,
+           "object_rel_l2": float(np.linalg.norm(obj - ro) / np.linalg.norm(ro)),
+           "object_rel_l2_illuminated": float(np.linalg.norm((obj - ro)[0][mask])
+                                              / np.linalg.norm(ro[0][mask])),
+           "probe_rel_l2": float(np.linalg.norm(probe - rp) / np.linalg.norm(rp)),
+           "object_nrmse": object_nrmse(obj, ro, mask.astype(float)[None])}
+    if offsets is not None and len(r["offsets"]):
+        row["offsets_max_abs_diff_px"] = float(np.abs(offsets - r["offsets"]).max())
+    print(json.dumps(row), flush=True)
+    return row
+
+
+def report(name, ref, out, rows, **extra):
+    cfg = CONFIGS[name]
+    meta = json.load(open(os.path.join(ref, f"{name}_meta.json")))
+    with open(out, "w") as f:
+        json.dump({"config": name, "kind": cfg["kind"], "oracle_seconds": meta["seconds"],
+                   "oracle_threads": meta["threads"], "rows": rows, **extra}, f, indent=1)
+
+
 def run_gpu(name, ref, out):
     """Each checkpoint on the CUDA path, compared with the oracle's snapshot."""
     from ptyrs_b200 import GpuPtycho, Scan
-    from ptyrs_b200.metrics import object_nrmse
     cfg = CONFIGS[name]
     meta = json.load(open(os.path.join(ref, f"{name}_meta.json")))
     s, digest = inputs(cfg)
     if digest != meta["digest"]:
         raise RuntimeError("the inputs differ from the oracle run's")
-    m = np.load(os.path.join(ref, f"{name}_mask.npz"))
-    mask = np.unpackbits(m["mask"])[:int(np.prod(m["shape"]))].reshape(m["shape"])
     scan = Scan(s["counts"], s["y"], s["x"], s["wavelength"], s["distance"], s["detector_pixel"])
     rows = []
     for k in cfg["checkpoints"]:
-        r = np.load(os.path.join(ref, f"{name}_{k}.npz"))
         with GpuPtycho(scan, s["object"], s["probe"]) as g:
             if cfg["algorithm"] == "rpie":
                 g.rpie(k, batch_size=cfg["batch"], obj_alpha=0.1, probe_alpha=0.1, seed=7)
@@ -122,28 +163,26 @@ def run_gpu(name, ref, out):
                      zero_phase_ramp=False)
             obj, probe = g.object(), g.probe()
             d = g.positions() if cfg["algorithm"] == "ml" else None
-        ro, rp = r["object"].astype(np.complex128), r["probe"]
-        row = {"iterations": k,
-               "object_rel_l2": float(np.linalg.norm(obj - ro) / np.linalg.norm(ro)),
-               "object_rel_l2_illuminated": float(np.linalg.norm((obj - ro)[0][mask])
-                                                  / np.linalg.norm(ro[0][mask])),
-               "probe_rel_l2": float(np.linalg.norm(probe - rp) / np.linalg.norm(rp)),
-               "object_nrmse": object_nrmse(obj, ro, mask.astype(float)[None])}
-        if d is not None:
-            row["offsets_max_abs_diff_px"] = float(np.abs(d - r["offsets"]).max())
-        rows.append(row)
-        print(json.dumps(row), flush=True)
-    with open(out, "w") as f:
-        json.dump({"config": name, "frames": len(s["counts"]), "n": s["n"],
-                   "object": list(s["object"].shape), "modes": s["probe"].shape[0],
-                   "oracle_seconds": meta["seconds"], "oracle_threads": meta["threads"],
-                   "rows": rows}, f, indent=1)
+        rows.append(compare(name, ref, k, obj, probe, d))
+    report(name, ref, out, rows, path="CUDA FP32")
+
+
+def run_sensitivity(name, ref, out, eps):
+    """The float64 oracle from the perturbed start, compared with its own unperturbed run."""
+    rows = []
+    run_oracle(name, ref, eps=eps,
+               save_as=lambda k, o, p, d: rows.append(compare(name, ref, k, o, p, d)))
+    report(name, ref, out, rows, path=f"float64 oracle, start perturbed by {eps:g}")
 
 
 if __name__ == "__main__":
-    if len(sys.argv) < 4 or sys.argv[1] not in ("oracle", "gpu") or sys.argv[2] not in CONFIGS:
+    if (len(sys.argv) < 4 or sys.argv[1] not in ("oracle", "gpu", "sensitivity")
+            or sys.argv[2] not in CONFIGS):
         raise SystemExit(__doc__)
     if sys.argv[1] == "oracle":
         run_oracle(sys.argv[2], sys.argv[3])
-    else:
+    elif sys.argv[1] == "gpu":
         run_gpu(sys.argv[2], sys.argv[3], sys.argv[4])
+    else:
+        run_sensitivity(sys.argv[2], sys.argv[3], sys.argv[4],
+                        float(sys.argv[5]) if len(sys.argv) > 5 else 1e-7)
