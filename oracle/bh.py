@@ -1,5 +1,6 @@
 """pty-chi BH (bilinear-Hessian) on the amplitude cost in float64 (oracle restatement, test
-infrastructure only), on one object slice without the position model.
+infrastructure only), on one object slice, with or without the position model under Patch
+sampling.
 
 Follows physwkim/ptyrs `ptyrs/src/engine/bh.rs`: `BhBatch::with_sampling` (bh.rs:168-275: the
 exit waves `U psi`, `A = √Σ_m |U psi_m|² + EPS`, `td = U psi·(1 − √iobs / A)`, zero where
@@ -12,6 +13,19 @@ directions across epochs with one batch of every frame, steepest descent with sm
 The cost is F = Σ_frames Σ_unmasked (A − √iobs)² over the batch's views; the displacement
 `(u_O, u_P)` of object and probe changes the exit wave by `J u = (u_P·O + P·u_O)·q` and to
 second order by `J″(u, v) = (u_P·v_O + v_P·u_O)·q`.
+
+Under the position model (the reference's `Features::position` with Patch sampling, bh.rs:
+92-275 and 630-760, and its float64 model `refs/f64/bh_pos.py`) frame b reads the probe moved by
+its offset d_b, `M_b(P) = conj(q)·T_d(q·P)` (ops.move_planes). Held offsets only move the probe
+and its displacements (`J u = (M_b(u_P)·O + M_b(P)·u_O)·q`). Refined offsets are variables too:
+a displacement carries `u_d` per batch frame, `g_d = Σ_m Re⟨Uᴴ(2·td), ∂_a M_b(P)·O·q⟩` per axis,
+and with `dW_u = M_b(u_P) + Σ_a u_da·∂_a M_b(P)`,
+`J u = (dW_u·O + M_b(P)·u_O)·q` and
+`J″(u, v) = ((Σ_a v_da·∂_a M_b(u_P) + u_da·∂_a M_b(v_P) + Σ_ab u_da·v_db·∂_a∂_b M_b(P))·O
++ dW_u·v_O + dW_v·u_O)·q`.
+The epoch takes the offsets' part of the gradient times `position_rho²`, keeps the direction's
+offsets part per frame for CG and moves the batch's offsets by `0.3·α·D_d` (pty-chi's position
+step size, unclipped).
 """
 import numpy as np
 
@@ -19,6 +33,7 @@ from . import ops
 from .base import fftshift2, random_batches
 
 EPS = 1e-8
+POSITION_STEP = 0.3  # bh.rs POSITION_STEP, pty-chi's ProbePositionOptions step size
 
 
 def _dot(a, b):
@@ -28,9 +43,11 @@ def _dot(a, b):
 
 class BhBatch:
     """The amplitude cost of `views` (whole frames, in order) at `(obj, probe)` and its
-    gradient and Hessian (engine/bh.rs:122-575, one slice, no offsets)."""
+    gradient and Hessian (engine/bh.rs:122-575, one slice); `offsets` `[nb, 2]` (dy, dx in
+    object pixels, one per batch frame in order) move each frame's probe, and with `refine` they
+    are variables of the cost."""
 
-    def __init__(self, views, obs, optics, obj, probe):
+    def __init__(self, views, obs, optics, obj, probe, offsets=None, refine=False):
         self.views, self.optics, self.obj, self.probe = views, optics, obj, probe
         nmode = 1
         while nmode < len(views) and views[nmode]["frame"] == views[0]["frame"]:
@@ -38,7 +55,22 @@ class BhBatch:
         self.nmode = nmode
         self.frames = [int(views[b * nmode]["frame"]) for b in range(len(views) // nmode)]
         ny, nx = probe.shape[-2:]
-        self.psi = optics.exit_forward(ops.obj_probe_to_psi(views, obj, probe, optics.quad))
+        self.offsets = None if offsets is None else np.asarray(offsets, np.float64)
+        self.refine = bool(refine) and self.offsets is not None
+        if self.offsets is not None:
+            # each frame's own probe planes: view probe index b·nprobe + mode
+            np_ = probe.shape[0]
+            self.pviews = views.copy()
+            self.pviews["probe"] = (np.repeat(np.arange(len(self.frames)) * np_, nmode)
+                                    + views["probe"])
+            self.w = self._moved(probe)
+            if self.refine:
+                self.dw = [self._moved(probe, (a,)) for a in range(2)]
+                self.d2w = [[self._moved(probe, (a, b)) for b in range(2)] for a in range(2)]
+        else:
+            self.pviews, self.w = views, probe
+        self.psi = optics.exit_forward(ops.obj_probe_to_psi(self.pviews, obj, self.w,
+                                                            optics.quad))
         sh = (len(self.frames), nmode, ny, nx)
         self.amp = np.sqrt((np.abs(self.psi.reshape(sh)) ** 2).sum(axis=1)) + EPS
         iobs, self.mask = obs.iobs[self.frames], obs.mask[self.frames]
@@ -46,35 +78,81 @@ class BhBatch:
         w = np.where(self.mask, 0.0, 1.0 - self.root / self.amp)
         self.td = (self.psi.reshape(sh) * w[:, None]).reshape(self.psi.shape)
 
-    def _adjoint(self, y):
-        """`Jᴴ Uᴴ y`: the object's and the probe's back-projections (engine/ops.rs:282-345)."""
-        e = self.optics.exit_adjoint(y)
-        g_obj = ops.accumulate_obj(self.views, self.obj.shape, self.probe, self.optics.quad, e)[0]
-        g_probe = ops.accumulate_probe(self.views, self.obj, self.probe.shape, self.optics.quad,
-                                       e)[0]
-        return g_obj, g_probe
+    def _moved(self, x, axes=()):
+        """Every batch frame's `M_b(x)` (or its derivative over the listed offset axes),
+        `[nb·nprobe, ny, nx]` frame-major."""
+        q = self.optics.quad
+        return np.concatenate([ops.move_planes(x, q, d, axes) for d in self.offsets])
+
+    def _per_frame(self, planes, d):
+        """`Σ_a d[b, a]·planes[a]` with one coefficient pair per batch frame."""
+        np_ = self.probe.shape[0]
+        c = np.repeat(np.asarray(d, np.float64), np_, axis=0)
+        return c[:, 0, None, None] * planes[0] + c[:, 1, None, None] * planes[1]
 
     def grads(self):
-        """`2·∂F/∂x*` over the object and the probe (engine/bh.rs:320-380)."""
-        return self._adjoint(2.0 * self.td)
-
-    def _tangent(self, u_obj, u_probe):
-        """`U·J u` per view: the exit waves' first-order change along `(u_O, u_P)`."""
+        """`2·∂F/∂x*` over the object and the probe (engine/bh.rs:320-380), and with refined
+        offsets ∂F/∂d `[nb, 2]` (None otherwise)."""
         q = self.optics.quad
-        t = (ops.obj_probe_to_psi(self.views, self.obj, u_probe, q)
-             + ops.obj_probe_to_psi(self.views, u_obj, self.probe, q))
+        e = self.optics.exit_adjoint(2.0 * self.td)
+        g_obj = ops.accumulate_obj(self.pviews, self.obj.shape, self.w, q, e)[0]
+        if self.offsets is None:
+            g_probe = ops.accumulate_probe(self.views, self.obj, self.probe.shape, q, e)[0]
+            return g_obj, g_probe, None
+        # each frame's probe-plane gradient, back through its move M_bᴴ = conj(q)·T_−d(q·)
+        np_ = self.probe.shape[0]
+        per = ops.accumulate_probe(self.pviews, self.obj, self.w.shape, q, e)[0]
+        g_probe = sum(ops.move_planes(per[b * np_:(b + 1) * np_], q, -d)
+                      for b, d in enumerate(self.offsets))
+        if not self.refine:
+            return g_obj, g_probe, None
+        # Σ_m Re⟨e, shift(∂_a M_b(P)·O·q)⟩ per frame and axis
+        nb = len(self.frames)
+        g_d = np.zeros((nb, 2))
+        for a in range(2):
+            t = ops.obj_probe_to_psi(self.pviews, self.obj, self.dw[a], q)
+            g_d[:, a] = (np.conj(e) * t).real.reshape(nb, -1).sum(axis=1)
+        return g_obj, g_probe, g_d
+
+    def _dw(self, up, ud):
+        """`dW_u`: the frames' probe-plane change along the displacement."""
+        if self.offsets is None:
+            return up
+        t = self._moved(up)
+        if self.refine and ud is not None:
+            t = t + self._per_frame(self.dw, ud)
+        return t
+
+    def _tangent(self, u_obj, dw_u):
+        """`U·J u` per view: the exit waves' first-order change."""
+        q = self.optics.quad
+        t = (ops.obj_probe_to_psi(self.pviews, self.obj, dw_u, q)
+             + ops.obj_probe_to_psi(self.pviews, u_obj, self.w, q))
         return self.optics.exit_forward(t)
 
     def hessian(self, u, v):
-        """pty-chi's bilinear Hessian (engine/bh.rs:500-575) along `u = (u_O, u_P)` and
-        `v = (v_O, v_P)`: Σ 2·Re(conj(td)·L_uv) + 2·Σ_unmasked [(1 − d/a)·Σ_m Re(conj(L_u)·L_v)
+        """pty-chi's bilinear Hessian (engine/bh.rs:500-575) along `u = (u_O, u_P[, u_d])` and
+        `v`: Σ 2·Re(conj(td)·L_uv) + 2·Σ_unmasked [(1 − d/a)·Σ_m Re(conj(L_u)·L_v)
         + d·c_u·c_v/a³], `L_u = U·J u`, `L_uv = U·J″(u, v)`, `c_u = Σ_m Re(conj(U psi)·L_u)`,
         `d = √iobs`, `a` the modelled amplitude plus EPS."""
-        (uo, up), (vo, vp) = u, v
+        uo, up, ud = (tuple(u) + (None,))[:3]
+        vo, vp, vd = (tuple(v) + (None,))[:3]
         q = self.optics.quad
-        lu, lv = self._tangent(uo, up), self._tangent(vo, vp)
-        luv = self.optics.exit_forward(ops.obj_probe_to_psi(self.views, vo, up, q)
-                                       + ops.obj_probe_to_psi(self.views, uo, vp, q))
+        dwu, dwv = self._dw(up, ud), self._dw(vp, vd)
+        lu, lv = self._tangent(uo, dwu), self._tangent(vo, dwv)
+        t2 = (ops.obj_probe_to_psi(self.pviews, vo, dwu, q)
+              + ops.obj_probe_to_psi(self.pviews, uo, dwv, q))
+        if self.refine and ud is not None and vd is not None:
+            d2 = (self._per_frame([self._moved(up, (a,)) for a in range(2)], vd)
+                  + self._per_frame([self._moved(vp, (a,)) for a in range(2)], ud))
+            np_ = self.probe.shape[0]
+            cu = np.repeat(np.asarray(ud, np.float64), np_, axis=0)
+            cv = np.repeat(np.asarray(vd, np.float64), np_, axis=0)
+            for a in range(2):
+                for b in range(2):
+                    d2 = d2 + (cu[:, a] * cv[:, b])[:, None, None] * self.d2w[a][b]
+            t2 = t2 + ops.obj_probe_to_psi(self.pviews, self.obj, d2, q)
+        luv = self.optics.exit_forward(t2)
         h = 2.0 * _dot(self.td, luv)
         ny, nx = self.probe.shape[-2:]
         sh = (len(self.frames), self.nmode, ny, nx)
@@ -89,12 +167,17 @@ class BhBatch:
 
 class Bh:
     """BH state across epochs (engine/bh.rs:580-760): the parameters, the epoch count and, with
-    one batch per epoch, the last direction."""
+    one batch per epoch, the last direction; under the position model `offsets` `[nframe, 2]`
+    (held, or refined with `refine`, in which case `self.offsets` moves)."""
 
-    def __init__(self, batch_size, probe_rho=0.01, seed=7):
+    def __init__(self, batch_size, probe_rho=0.01, seed=7, position_rho=0.1, offsets=None,
+                 refine=False):
         if batch_size < 1:
             raise ValueError("BH batch_size must be >= 1")
         self.batch_size, self.probe_rho, self.seed = batch_size, probe_rho, seed
+        self.position_rho = position_rho
+        self.offsets = None if offsets is None else np.array(offsets, np.float64)
+        self.refine = bool(refine) and self.offsets is not None
         self.epochs = 0
         self.prev = None
 
@@ -108,42 +191,54 @@ class Bh:
         size = min(self.batch_size, nframe)
         full = size == nframe
         rho2 = self.probe_rho ** 2 * optics.intensity_scale()
+        pos_rho2 = self.position_rho ** 2
         epoch = self.epochs
         self.epochs += 1
         steps = []
         for frames in random_batches(nframe, size, self.seed, epoch):
             views = np.concatenate([addr.frame_views(f) for f in frames])
-            b = BhBatch(views, obs, optics, obj, probe)
-            g_obj, g_probe = b.grads()
-            pg = (g_obj, g_probe * rho2)
+            d_b = None if self.offsets is None else self.offsets[list(frames)]
+            b = BhBatch(views, obs, optics, obj, probe, d_b, self.refine)
+            g_obj, g_probe, g_d = b.grads()
+            pg = (g_obj, g_probe * rho2, None if g_d is None else g_d * pos_rho2)
             if full and self.prev is not None:
-                d_obj, d_probe = self.prev
-                beta = b.hessian(pg, (d_obj, d_probe)) / b.hessian((d_obj, d_probe),
-                                                                    (d_obj, d_probe))
-                direction = (beta * d_obj - pg[0], beta * d_probe - pg[1])
+                d_obj, d_probe, by_frame = self.prev
+                prev = (d_obj, d_probe, None if g_d is None else by_frame[list(frames)])
+                beta = b.hessian(pg, prev) / b.hessian(prev, prev)
+                direction = (beta * d_obj - pg[0], beta * d_probe - pg[1],
+                             None if g_d is None else beta * prev[2] - pg[2])
             else:
                 beta = 0.0
-                direction = (-pg[0], -pg[1])
+                direction = (-pg[0], -pg[1], None if g_d is None else -pg[2])
             top = -(_dot(g_obj, direction[0]) + _dot(g_probe, direction[1]))
+            if g_d is not None:
+                top -= float((g_d * direction[2]).sum())
             bottom = b.hessian(direction, direction)
             alpha = top / bottom * len(frames) / size
             obj = obj + alpha * direction[0]
             probe = probe + alpha * direction[1]
+            by_frame = None
+            if g_d is not None:
+                by_frame = np.zeros((nframe, 2))
+                by_frame[list(frames)] = direction[2]
+                self.offsets[list(frames)] += POSITION_STEP * alpha * direction[2]
             if full:
-                self.prev = direction
+                self.prev = (direction[0], direction[1], by_frame)
             steps.append(dict(frames=list(frames), beta=beta, alpha=alpha, top=top,
                               bottom=bottom))
         return obj, probe, steps
 
 
-def amplitude_cost(views, obs, optics, obj, probe):
+def amplitude_cost(views, obs, optics, obj, probe, offsets=None):
     """F without the amplitude offset: Σ_unmasked (|U psi| − √iobs)², a quarter of PyNX's
-    Euclidian sum (the reference test's `cost`)."""
+    Euclidian sum (the reference test's `cost`); `offsets` move each batch frame's probe."""
     nmode = 1
     while nmode < len(views) and views[nmode]["frame"] == views[0]["frame"]:
         nmode += 1
     frames = slice(int(views[0]["frame"]), int(views[-1]["frame"]) + 1)
-    psi = optics.exit_forward(ops.obj_probe_to_psi(views, obj, probe, optics.quad))
+    b = BhBatch(views, obs, optics, obj, probe, offsets) if offsets is not None else None
+    pviews, w = (views, probe) if b is None else (b.pviews, b.w)
+    psi = optics.exit_forward(ops.obj_probe_to_psi(pviews, obj, w, optics.quad))
     return ops.llk(obs, frames, nmode, psi).euclidian / 4.0
 
 

@@ -53,6 +53,10 @@ GROUPS = {
     # directions) and with batches of 16 (steepest descent); step rows padded with -1
     "bh_full": ["obj", "probe", "steps"],
     "bh_mini": ["obj", "probe", "steps"],
+    # the same with the offsets refined under Patch (refs/f64/bh_pos.py; position_rho 2):
+    # every frame's offsets before and after, the object and probe changes of both epochs
+    "bh_pos_full": ["obj", "probe", "offsets", "steps"],
+    "bh_pos_mini": ["obj", "probe", "offsets", "steps"],
     # one LSQML step refining the offsets with three eigenmodes of probe mode 0
     "lsqml_pos_opr": ["eigen", "weights", "steps", "offsets", "obj", "probe"],
     "rpie_ptychi": [""],

@@ -2,7 +2,10 @@
 (`dm_scenario(32, 40, 2, 2e5, 4.0)` after `scale_obj_probe`, redrawn by oracle/scenario.py):
 its gradient and Hessian against central differences, and two epochs with one batch of every
 frame and with batches of 16 against the reference's float64 BH runs
-(ptyrs/tests/engine_bh.rs:85-243, `bh_{full,mini}_*_f64.txt`)."""
+(ptyrs/tests/engine_bh.rs:85-243, `bh_{full,mini}_*_f64.txt`); with the offsets refined under
+Patch the same against central differences over object, probe and offsets and two epochs
+against the reference's float64 model (ptyrs/tests/engine_bh_pos.rs:62-170,
+`bh_pos_{full,mini}_*_f64.txt`, position_rho 2)."""
 import numpy as np
 import pytest
 
@@ -32,7 +35,7 @@ def test_grads_match_central_differences():
     p = state()
     views = batch_views(p)
     b = BhBatch(views, p.obs, p.optics, p.object, p.probe)
-    g_obj, g_probe = b.grads()
+    g_obj, g_probe, _ = b.grads()
     rng = np.random.default_rng(1)
     d_obj, d_probe = direction(p.object, rng), direction(p.probe, rng)
     h = 1e-5
@@ -57,7 +60,7 @@ def test_hessian_matches_central_differences():
     assert rel(h_vu, h_uv) < 1e-13
 
     def du(t):
-        g = BhBatch(views, p.obs, p.optics, p.object + t * v[0], p.probe + t * v[1]).grads()
+        g = BhBatch(views, p.obs, p.optics, p.object + t * v[0], p.probe + t * v[1]).grads()[:2]
         return float(np.sum((np.conj(g[0]) * u[0]).real) + np.sum((np.conj(g[1]) * u[1]).real))
 
     h = 1e-6
@@ -97,3 +100,93 @@ def test_epochs_match_reference(name, batch):
                        np.stack([o.real, o.imag], 1)) < 1e-12
         assert max_rel(np.stack([d_probe.ravel().real, d_probe.ravel().imag], 1),
                        np.stack([pr.real, pr.imag], 1)) < 5e-12
+
+
+def start_offsets(name="bh_pos_full"):
+    """The reference run's start offsets, `[dy, dx]` per frame (columns 1-2 of its table)."""
+    return golden(name)["offsets"][:, 1:3].copy()
+
+
+def test_grads_with_offsets_match_central_differences():
+    """⟨g, d⟩ over object, probe and the refined offsets against central differences of F
+    (bh_pos.py's check)."""
+    p = state()
+    views = batch_views(p)
+    d0 = start_offsets()[list(FRAMES)]
+    b = BhBatch(views, p.obs, p.optics, p.object, p.probe, d0, refine=True)
+    g_obj, g_probe, g_d = b.grads()
+    rng = np.random.default_rng(3)
+    u_obj, u_probe = direction(p.object, rng), direction(p.probe, rng)
+    u_d = rng.uniform(-1, 1, d0.shape)
+    f = lambda o, pr, d: amplitude_cost(views, p.obs, p.optics, o, pr, d)
+    h = 1e-5
+    for an, plus, minus in (
+            (float(np.sum((np.conj(g_obj) * u_obj).real)),
+             (p.object + h * u_obj, p.probe, d0), (p.object - h * u_obj, p.probe, d0)),
+            (float(np.sum((np.conj(g_probe) * u_probe).real)),
+             (p.object, p.probe + h * u_probe, d0), (p.object, p.probe - h * u_probe, d0)),
+            (float((g_d * u_d).sum()),
+             (p.object, p.probe, d0 + h * u_d), (p.object, p.probe, d0 - h * u_d))):
+        assert rel(an, (f(*plus) - f(*minus)) / (2 * h)) < 1e-6
+
+
+@pytest.mark.parametrize("refine", [True, False])
+def test_hessian_with_offsets_matches_central_differences(refine):
+    """H(u, v) = H(v, u) and against the central difference of ⟨g(x + h·v), u⟩ over object,
+    probe and (refined) offsets; held offsets move the probe only."""
+    p = state()
+    views = batch_views(p)
+    d0 = start_offsets()[list(FRAMES)]
+    rng = np.random.default_rng(4)
+    nd = lambda: rng.uniform(-1, 1, d0.shape) if refine else None
+    u = (direction(p.object, rng), direction(p.probe, rng), nd())
+    v = (direction(p.object, rng), direction(p.probe, rng), nd())
+    b = BhBatch(views, p.obs, p.optics, p.object, p.probe, d0, refine=refine)
+    h_uv, h_vu = b.hessian(u, v), b.hessian(v, u)
+    assert rel(h_vu, h_uv) < 1e-12
+
+    def du(t):
+        d = d0 + t * v[2] if refine else d0
+        g = BhBatch(views, p.obs, p.optics, p.object + t * v[0], p.probe + t * v[1], d,
+                    refine=refine).grads()
+        s = float(np.sum((np.conj(g[0]) * u[0]).real) + np.sum((np.conj(g[1]) * u[1]).real))
+        return s + (float((g[2] * u[2]).sum()) if refine else 0.0)
+
+    h = 1e-6
+    assert rel(h_uv, (du(h) - du(-h)) / (2 * h)) < 1e-6
+
+
+@pytest.mark.parametrize("name,batch", [("bh_pos_full", 40), ("bh_pos_mini", 16)])
+def test_epochs_with_refined_offsets_match_reference(name, batch):
+    """engine_bh_pos.rs:62-170: two epochs (seed 7, probe_rho 0.01, position_rho 2) from the
+    reference run's offsets: every step's frames, β, α, −⟨g, D⟩ and H(D, D) to 3e-12, the
+    object and probe changes relative to the largest start value and the offsets' changes
+    relative to the largest of them, to 3e-12."""
+    p = state()
+    g = golden(name)
+    start = g["offsets"][:, 1:3]
+    run = Bh(batch, probe_rho=0.01, seed=7, position_rho=2.0, offsets=start, refine=True)
+    obj, probe = p.object, p.probe
+    got = []
+    for e in range(2):
+        obj, probe, steps = run.epoch(p.addr, p.obs, p.optics, obj, probe)
+        got += [(e, s) for s in steps]
+    rows = g["steps"]
+    assert len(got) == len(rows)
+    for k, ((e, s), r) in enumerate(zip(got, rows)):
+        count = int(r[2])
+        assert [k, e, count] == [int(r[0]), int(r[1]), len(s["frames"])]
+        assert s["frames"] == [int(f) for f in r[7:7 + count]]
+        if r[3] == 0.0:
+            assert s["beta"] == 0.0
+        for key, want in (("beta", r[3]), ("alpha", r[4]), ("top", r[5]), ("bottom", r[6])):
+            if want != 0.0:
+                assert rel(s[key], want) < 3e-12, (k, key)
+    d_obj, d_probe = obj - p.object, probe - p.probe
+    want_o = g["obj"][:, 2] + 1j * g["obj"][:, 3]
+    want_p = g["probe"][:, 3] + 1j * g["probe"][:, 4]
+    ri = lambda z: np.stack([np.ravel(z).real, np.ravel(z).imag], 1)
+    assert max_rel(ri(d_obj), ri(want_o), np.abs(ri(p.object)).max()) < 3e-12
+    assert max_rel(ri(d_probe), ri(want_p), np.abs(ri(p.probe)).max()) < 3e-12
+    want_d = g["offsets"][:, 3:5] - start
+    assert max_rel(run.offsets - start, want_d) < 3e-12
