@@ -123,8 +123,8 @@ typedef struct ptyb_lsqml_step {
 
 /* Reference `BhParams` (engine/bh.rs:29-49): frames per batch (one batch of every frame runs
  * conjugate directions across epochs, smaller batches steepest descent), pty-chi's probe
- * `rho` (the probe variable is the probe over rho·√k), the offsets' rho (the reference's
- * layout; BH here runs without the position model) and the batches' seed. */
+ * `rho` (the probe variable is the probe over rho·√k), the offsets' rho (under refined
+ * offsets the offsets' gradient is scaled by position_rho²) and the batches' seed. */
 typedef struct ptyb_bh_params {
   int32_t batch_size, pad_;
   double probe_rho, position_rho;
@@ -279,7 +279,10 @@ int ptyb_get_positions(ptyb_handle* h, double* dst);
  * 645-760): pty-chi's bilinear-Hessian method on the amplitude cost, `nepoch` epochs from a
  * fresh run (epoch e's batches `random_batches(nframe, batch_size, seed, e)`), every batch
  * moving object and probe by α·D; an LLK record after every due epoch (calc_llk as
- * ptyb_lsqml's). One object slice without the position model (PTYB_INVALID otherwise). */
+ * ptyb_lsqml's). One object slice (PTYB_INVALID otherwise). With ptyb_set_positions every
+ * frame's probe is moved by its offset (Patch sampling, engine/bh.rs:92-275); refined offsets
+ * are BH variables (their part of the gradient and the directions, 0.3·α·D_d added to them,
+ * engine/bh.rs:725-745), held ones only move the probe. */
 int ptyb_bh(ptyb_handle* h, const ptyb_bh_params* p, int32_t nepoch, int32_t calc_llk);
 /* Reference `GpuPtycho::bh_steps` (engine/gpu/bh.rs:68-72): the last epoch's steps. */
 int ptyb_bh_steps_len(ptyb_handle* h);

@@ -7,6 +7,10 @@
 // with g = Uᴴ(2·td) the gradient pass's exit-plane field (the term 2·Re⟨td, U·J″⟩ taken by
 // Parseval in the exit plane, no transform), c_u = Σ_m Re(conj(U psi)·L_u) against the
 // detector field the gradient pass kept, a = √Σ_m |U psi|² + 1e-8 and d = √I.
+// Under the position model (engine/bh.rs:92-275, Patch sampling) each frame reads its moved
+// planes M(P), M(u_P), M(v_P) in place of P, u_P, v_P; with refined offsets the displacements'
+// offsets parts u_d, v_d add dW_u = M(u_P) + Σ_a u_da·∂_a M(P) in place of M(u_P) and to J″
+// the term (Σ_a v_da·∂_a M(u_P) + u_da·∂_a M(v_P) + Σ_ab u_da·v_db·∂_a∂_b M(P))·O·q.
 #pragma once
 #include "frame.cuh"
 
@@ -31,6 +35,12 @@ struct BhArgs {
   // kernel's unnormalised transform), and its exit-plane field g = Uᴴ(2·td), [slot][K][N][N].
   const float2* psi;
   const float2* g;
+  // Position model (null without): every slot's moved planes [slot][K][N][N], M(P), M(u_P),
+  // M(v_P); with refined offsets their offset derivatives (∂y, ∂x of each; ∂y∂y, ∂y∂x, ∂x∂x of
+  // M(P)) and the displacements' offsets parts [slot][2] (dy, dx).
+  const float2 *w, *tu, *tv;
+  const float2 *dwy, *dwx, *dtuy, *dtux, *dtvy, *dtvx, *dwyy, *dwyx, *dwxx;
+  const double *ud, *vd;
 };
 
 template <int N, int C>
@@ -63,6 +73,14 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T, 1) bh_hessian_kernel(BhAr
   ltw.load(a.tw, tid % F::G);
   for (int i = tid; i < 4 * H * AS; i += T) acc[i] = 0.f;
 
+  const bool moved = a.w != nullptr, pos = a.dwy != nullptr;
+  float uy = 0.f, ux = 0.f, vy = 0.f, vx = 0.f;
+  if (pos) {
+    uy = (float)a.ud[2 * slot];
+    ux = (float)a.ud[2 * slot + 1];
+    vy = (float)a.vd[2 * slot];
+    vx = (float)a.vd[2 * slot + 1];
+  }
   double gterm = 0.0;
   for (int m = 0; m < K; ++m) {
     const int pm = m % a.nprobe, om = m / a.nprobe;
@@ -74,19 +92,36 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T, 1) bh_hessian_kernel(BhAr
       const int yl = idx / N, jx = idx % N;
       const int ny = (r * H + yl + N / 2) % N, nx = (jx + N / 2) % N;
       const size_t pi = ((size_t)pm * N + ny) * N + nx;
+      const size_t si = ((size_t)slot * K + m) * N * N + (size_t)ny * N + nx;
       const size_t oi = ((size_t)om * a.nyo + corner.x + ny) * a.nxo + corner.y + nx;
-      const float2 p = a.probe[pi], o = a.object[oi], q = a.quad[ny * N + nx];
-      const float2 up = a.u_probe[pi], uo = a.u_obj[oi];
+      const float2 o = a.object[oi], q = a.quad[ny * N + nx];
+      const float2 p = moved ? a.w[si] : a.probe[pi];
+      float2 up = moved ? a.tu[si] : a.u_probe[pi];
+      float2 vp = a.same ? up : moved ? a.tv[si] : a.v_probe[pi];
+      const float2 uo = a.u_obj[oi];
+      const float2 vo = a.same ? uo : a.v_obj[oi];
+      float2 second = make_float2(0.f, 0.f);  // J″'s offsets terms, before ·O·q
+      if (pos) {
+        const float2 wy = a.dwy[si], wx = a.dwx[si];
+        const float2 sy = a.dtuy[si], sx = a.dtux[si];
+        const float2 ty = a.same ? sy : a.dtvy[si], tx = a.same ? sx : a.dtvx[si];
+        second = cadd(cadd(cscale(sy, vy), cscale(sx, vx)), cadd(cscale(ty, uy), cscale(tx, ux)));
+        second = cadd(second, cadd(cscale(a.dwyy[si], uy * vy),
+                                   cadd(cscale(a.dwyx[si], uy * vx + ux * vy),
+                                        cscale(a.dwxx[si], ux * vx))));
+        up = cadd(up, cadd(cscale(wy, uy), cscale(wx, ux)));
+        vp = a.same ? up : cadd(vp, cadd(cscale(wy, vy), cscale(wx, vx)));
+      }
       S1[yl * L + (jx ^ swz(yl))] = cmul(cadd(cmul(up, o), cmul(p, uo)), q);
       float2 xuv;
       if (a.same) {
         xuv = cscale(cmul(cmul(up, uo), q), 2.f);
       } else {
-        const float2 vp = a.v_probe[pi], vo = a.v_obj[oi];
         const int l2 = H + yl;
         S1[l2 * L + (jx ^ swz(l2))] = cmul(cadd(cmul(vp, o), cmul(p, vo)), q);
         xuv = cmul(cadd(cmul(up, vo), cmul(vp, uo)), q);
       }
+      if (pos) xuv = cadd(xuv, cmul(cmul(second, o), q));
       const float2 gv = g_m[(size_t)ny * N + nx];
       gterm += (double)gv.x * xuv.x + (double)gv.y * xuv.y;
     }

@@ -181,6 +181,13 @@ struct ptyb_handle {
   std::vector<ptyb_lsqml_step> steps;
   std::vector<double> slice_steps;  // [frame of the last epoch][slice 1..]: a_obj
   std::vector<ptyb_bh_step> bh_steps;  // the last BH epoch's steps
+  // BH under the position model: per stack slot the planes its Hessian reads, [bh_slots][K][N][N]
+  // each (M(P), M(u_P), M(v_P), then with refined offsets ∂y, ∂x of each and ∂y∂y, ∂y∂x, ∂x∂x of
+  // M(P)), the spectra of u_P and v_P, and the displacements' offsets parts [bh_slots][2]
+  float2* bh_planes[12] = {};
+  int bh_slots = 0;
+  float2 *bh_spec_u = nullptr, *bh_spec_v = nullptr;
+  double *bh_ud = nullptr, *bh_vd = nullptr;
   int log_stride = 3;
   bool aborted = false;
   std::string err;

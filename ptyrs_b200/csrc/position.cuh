@@ -17,8 +17,11 @@ enum MoveMode : int {
   kBackSpectrum = 7,  // planes[slot][m] = DFT(conj(O_win)·c_m)·exp(+2πi f·d)/N², [ky][kx]: one
                       // frame's term of the probe back-projection through the move's adjoint
   kPlainInverse = 8,  // planes[m] = conj(q)·IDFT(spec_m), unnormalised (one slot)
-  kMoveOwn = 9        // planes[slot][m] = conj(q)·T_d(q·planes), in place: each frame's own
+  kMoveOwn = 9,       // planes[slot][m] = conj(q)·T_d(q·planes), in place: each frame's own
                       // probe planes (the probe variation's) moved by its offset
+  kDerivMove = 10     // planes[slot][m] = conj(q)·∂T_d(q·P_m) from the spectrum `spec`: the
+                      // first (deriv 1 y, 2 x) or second (3 yy, 4 yx, 5 xx) derivative over
+                      // the offset of kFromSpectrum's moved probe (BH's position terms)
 };
 
 struct MoveArgs {
@@ -36,6 +39,7 @@ struct MoveArgs {
   const float2* c;        // [slot][K][N][N] natural: the change of the exit wave (kDerivSums),
                           // the exit-plane gradient (kBackSpectrum)
   double* sums;           // [nframe][4] num_y, num_x, den_y, den_x (kDerivSums)
+  int deriv;              // kDerivMove: 1 ∂y, 2 ∂x, 3 ∂y∂y, 4 ∂y∂x, 5 ∂x∂x
   // Optional, [slot][K][N][N] natural: each frame's moved probes W; kDerivSums and
   // kBackSpectrum then take c − W·O·q, the carried waves' residual against the model
   // (AP / DM / RAAR, engine/features.rs:653-725, 992-1025).
@@ -71,9 +75,11 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
   const size_t plane = (size_t)N * N;
   float2* out = a.planes + (size_t)slot * K * plane;
   constexpr float inv_n2 = 1.0f / ((float)N * (float)N);
-  constexpr bool from_spec = MODE == kFromSpectrum || MODE == kDerivSums || MODE == kPlainInverse;
+  constexpr bool from_spec = MODE == kFromSpectrum || MODE == kDerivSums ||
+                              MODE == kPlainInverse || MODE == kDerivMove;
   constexpr bool in_place = MODE == kMoveBack || MODE == kMoveOwn;
   constexpr bool moves = in_place || MODE == kFromSpectrum || MODE == kDerivSums ||
+                         MODE == kDerivMove ||
                          MODE == kBackSpectrum;
   constexpr bool bare = MODE == kDerivWindow;
 
@@ -165,6 +171,16 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
           // × (−2πi·f_axis): the derivative of the translation phase (engine/features.rs:372-387)
           const float w = 2.f * 3.14159265358979f * (axis == 0 ? fy : fx);
           e = make_float2(w * e.y, -w * e.x);
+        } else if (MODE == kDerivMove) {
+          // × (−2πi·f_a) or × (−2πi·f_a)(−2πi·f_b) = −4π²·f_a·f_b
+          const float wy = 2.f * 3.14159265358979f * fy, wx = 2.f * 3.14159265358979f * fx;
+          if (a.deriv <= 2) {
+            const float w = a.deriv == 1 ? wy : wx;
+            e = make_float2(w * e.y, -w * e.x);
+          } else {
+            const float w = a.deriv == 3 ? -wy * wy : a.deriv == 4 ? -wy * wx : -wx * wx;
+            e = make_float2(w * e.x, w * e.y);
+          }
         }
       }
       for (int m = 0; m < K; ++m) {

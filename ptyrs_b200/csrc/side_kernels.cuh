@@ -76,6 +76,8 @@ cudaError_t move_modes(int mode, const MoveArgs& a, int nslot, int K, cudaStream
     case kPlainInverse:
       return launch_clusters<N, C>(move_kernel<N, C, kPlainInverse>, a, nslot, smem, s);
     case kMoveOwn: return launch_clusters<N, C>(move_kernel<N, C, kMoveOwn>, a, nslot, smem, s);
+    case kDerivMove:
+      return launch_clusters<N, C>(move_kernel<N, C, kDerivMove>, a, nslot, smem, s);
   }
   return cudaErrorInvalidValue;
 }

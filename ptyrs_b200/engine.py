@@ -146,10 +146,12 @@ class GpuPtycho:
         p = _lib.MlParams(update_object, update_probe, calc_llk, zero_phase_ramp)
         self._check(self._lib.ptyb_ml(self._h, ctypes.byref(p), ncycle))
 
-    def bh(self, nepoch, batch_size, probe_rho=0.01, seed=7, calc_llk=0):
+    def bh(self, nepoch, batch_size, probe_rho=0.01, seed=7, calc_llk=0, position_rho=0.1):
         """pty-chi's BH on the amplitude cost (reference `GpuPtycho::bh`): `nepoch` epochs from
-        a fresh run; one batch of every frame runs conjugate directions across epochs."""
-        p = _lib.BhParams(batch_size, 0, probe_rho, 0.1, seed)
+        a fresh run; one batch of every frame runs conjugate directions across epochs. With
+        `set_positions` every frame's probe is moved by its offset; refined offsets are BH
+        variables too (their gradient scaled by `position_rho²`, stepped by 0.3·α·D_d)."""
+        p = _lib.BhParams(batch_size, 0, probe_rho, position_rho, seed)
         self._check(self._lib.ptyb_bh(self._h, ctypes.byref(p), nepoch, calc_llk))
 
     def bh_steps(self):
