@@ -344,6 +344,41 @@ int ptyb_live_handle(ptyb_live* l, const double* object, int32_t nyo, int32_t nx
 const char* ptyb_live_last_error(ptyb_live* l);
 void ptyb_live_destroy(ptyb_live* l);
 
+/* Scan files (reference ptyrs/src/io/cxi.rs:130-200 `read_cxi`): the CXI layout PyNX's
+ * `save_ptycho_data_cxi` writes, read by the library's own HDF5 reader (libhdf5's default
+ * layouts: superblocks 0-3, symbol-table and compact groups, soft links, contiguous, compact and
+ * chunked datasets with deflate and shuffle). Counts are `u16 [nframe][ny][nx]` in detector
+ * order with 65535 masked: raw u16 data with the detector mask applied, or float data under the
+ * reference's `Counts::from_f64` rule (masked or negative → 65535, a non-integer or a value past
+ * 65534 refused). Positions come from the f32 translation rows (x, y), the wavelength from the
+ * energy by PyNX's 12.3984 keV·Å and 1.60218e-16 J/keV. The arrays are the library's; free the
+ * scan with ptyb_free_cxi. A handle takes counts, y and x as they are (counts_kind
+ * PTYB_COUNTS_U16). */
+typedef struct ptyb_cxi_scan {
+  int32_t nframe, ny, nx, pad_;
+  uint16_t* counts;
+  double* y; /* [nframe] metres */
+  double* x;
+  double wavelength, distance, detector_pixel;
+} ptyb_cxi_scan;
+int ptyb_read_cxi(const char* path, ptyb_cxi_scan* out);
+void ptyb_free_cxi(ptyb_cxi_scan* s);
+
+/* Reference `read_ptyr` (ptyrs/src/io/ptyr.rs): the object and probe of a PtyPy `.ptyr`
+ * reconstruction (the one storage under content/obj and content/probe, complex64 or
+ * complex128), as complex128 interleaved `[obj_shape]` and `[probe_shape]`, with the object
+ * storage's pixel size and origin ([y, x]). Free with ptyb_free_ptyr. */
+typedef struct ptyb_ptyr {
+  int32_t obj_shape[3], probe_shape[3];
+  double* object;
+  double* probe;
+  double psize[2], origin[2];
+} ptyb_ptyr;
+int ptyb_read_ptyr(const char* path, ptyb_ptyr* out);
+void ptyb_free_ptyr(ptyb_ptyr* r);
+/* The reason the last ptyb_read_* call of this thread failed. */
+const char* ptyb_io_last_error(void);
+
 /* Reference `GpuPtycho::{object, probe, set_object}` (engine/gpu/mod.rs:763-817). */
 int ptyb_get_object(ptyb_handle* h, double* dst);
 int ptyb_get_probe(ptyb_handle* h, double* dst);

@@ -89,6 +89,18 @@ class LiveStats(ctypes.Structure):
                                        "stalls", "pos_waits", "batches")]
 
 
+class CxiScan(ctypes.Structure):
+    _fields_ = [("nframe", c_int32), ("ny", c_int32), ("nx", c_int32), ("pad_", c_int32),
+                ("counts", P(ctypes.c_uint16)), ("y", P(c_double)), ("x", P(c_double)),
+                ("wavelength", c_double), ("distance", c_double), ("detector_pixel", c_double)]
+
+
+class Ptyr(ctypes.Structure):
+    _fields_ = [("obj_shape", c_int32 * 3), ("probe_shape", c_int32 * 3),
+                ("object", P(c_double)), ("probe", P(c_double)), ("psize", c_double * 2),
+                ("origin", c_double * 2)]
+
+
 # Every symbol include/ptyb200.h declares, with (restype, argtypes).
 SIGNATURES = {
     "ptyb_create": (c_int32, [P(Scan), P(c_double), c_int32, c_int32, c_int32, P(c_double),
@@ -131,6 +143,11 @@ SIGNATURES = {
                                    c_int32, P(Options), P(c_void_p), P(c_int32)]),
     "ptyb_live_last_error": (ctypes.c_char_p, [c_void_p]),
     "ptyb_live_destroy": (None, [c_void_p]),
+    "ptyb_read_cxi": (c_int32, [ctypes.c_char_p, P(CxiScan)]),
+    "ptyb_free_cxi": (None, [P(CxiScan)]),
+    "ptyb_read_ptyr": (c_int32, [ctypes.c_char_p, P(Ptyr)]),
+    "ptyb_free_ptyr": (None, [P(Ptyr)]),
+    "ptyb_io_last_error": (ctypes.c_char_p, []),
     "ptyb_get_object": (c_int32, [c_void_p, P(c_double)]),
     "ptyb_get_probe": (c_int32, [c_void_p, P(c_double)]),
     "ptyb_set_object": (c_int32, [c_void_p, P(c_double)]),

@@ -15,7 +15,7 @@ OUT = os.path.join(HERE, "libptyb200.so")
 # the per-side kernel units first: they take longest
 SOURCES = ["kernels_256.cu", "kernels_192.cu", "kernels_128.cu", "kernels_96.cu",
            "kernels_64.cu", "engine.cu", "rpie.cu", "lsqml.cu", "ml.cu", "carried.cu",
-           "bh.cu", "batch.cu", "forward.cu", "live.cu", "scan.cpp"]
+           "bh.cu", "batch.cu", "forward.cu", "live.cu", "scan.cpp", "h5.cpp", "io.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC"]
 
@@ -65,8 +65,9 @@ def build(force=False, verbose=False, jobs=None):
         objs = list(pool.map(lambda s: _compile(nvcc, s, verbose, force), SOURCES))
     # only the C ABI (ptyb_*) is exported
     exports = "--version-script=" + os.path.join(CSRC, "exports.map")
+    # zlib inflates the deflate-compressed chunks of HDF5 files (io.cpp)
     cmd = [nvcc] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-Xlinker", exports] + objs + [
-        "-o", OUT + ".tmp"]
+        "-lz", "-o", OUT + ".tmp"]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError("nvcc link failed:\n" + res.stderr[-4000:])

@@ -17,6 +17,11 @@ against PyNX (`dm_pynx_f64.txt`, `raar_pynx_f64.txt`), and OPR probe variation a
 an LSQML step (`opr_*`, `lsqml_opr_*`, `lsqml_opr_int_*`). Each text table becomes one float64 array of the same rows and
 columns under its stem (`table` for a file without one) in `<group>.npz`.
 
+The I/O fixtures (`ptyrs/tests/io/data/`) are copied as they are: `pynx_small.cxi` (written by
+PyNX's `save_ptycho_data_cxi` through libhdf5, `make_pynx_small.py` there) and
+`ptypy_small_{single,double}.ptyr` (PtyPy `Ptycho.save_run`, `make_ptypy_small.py` there), the
+files the library's HDF5 reader is checked on.
+
     python tests/golden/make_golden.py REFERENCE_ROOT [GROUP ...]
 """
 import os
@@ -70,6 +75,9 @@ GROUPS = {
 }
 
 
+IO_FILES = ["pynx_small.cxi", "ptypy_small_single.ptyr", "ptypy_small_double.ptyr"]
+
+
 def load_table(path):
     """A whitespace table as float64 rows; rows of unequal length (a batch's frames at the end
     of each step row) are padded with -1."""
@@ -91,6 +99,14 @@ def main(root, only=()):
             arrays[stem or "table"] = load_table(os.path.join(data, name))
         np.savez_compressed(os.path.join(here, f"{group}.npz"), **arrays)
         print(group, {k: v.shape for k, v in arrays.items()})
+    if not only or "io" in only:
+        io = os.path.join(root, "ptyrs", "tests", "io", "data")
+        for name in IO_FILES:
+            with open(os.path.join(io, name), "rb") as src:
+                blob = src.read()
+            with open(os.path.join(here, name), "wb") as dst:
+                dst.write(blob)
+            print(name, len(blob), "bytes")
 
 
 if __name__ == "__main__":
