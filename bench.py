@@ -1,7 +1,7 @@
 """Throughput of the reconstruction hot path on B200: diffraction patterns·iterations per second.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload ml256|lsqml128|opr128|rpie64|ms128|batch32|dm256|raar256|ap256]
+                    [--workload ml256|lsqml128|opr128|rpie64|ms128|msml128|batch32|dm256|raar256|ap256]
 
 Workload `ml256` (default; the configuration the metric names, a 256² probe): Poisson
 maximum-likelihood conjugate gradient with position refinement — a 2048² smooth-noise object,
@@ -66,6 +66,12 @@ WORKLOADS = {
                   desc="multislice LSQML, 3 slices of 1536^2 10 um apart (angular spectrum, "
                        "lambda 0.1 nm, 10 nm pixels), 128^2 probe x2 modes, Fermat 6000 @ "
                        "12 px, 1e6 photons, batch 256, Poisson"),
+    # the multislice configuration's ML: Poisson CG through the three slices
+    "msml128": dict(kind="ms128", algorithm="ml", sample_frames=48,
+                    desc="multislice ML (Poisson conjugate gradient through the slices, object "
+                         "and probe), 3 slices of 1536^2 10 um apart (angular spectrum, lambda "
+                         "0.1 nm, 10 nm pixels), 128^2 probe x2 modes, Fermat 6000 @ 12 px, 1e6 "
+                         "photons"),
     # 32 independent uneven scans at once (ptyb_batch_run), each step one whole reconstruction:
     # 30 rPIE epochs (batches of 100) then 30 LSQML epochs (batches of 256) on every scan
     "batch32": dict(kind="batch32", algorithm="batch", batch=100, lsqml_batch=256,
@@ -161,7 +167,7 @@ def make_inputs(workload, seed, scale=1.0):
 def prepare(g, s, wl):
     """The workload's features on a fresh state: ML starts at the nominal positions with the
     sub-pixel offsets refined."""
-    if wl["algorithm"] == "ml":
+    if wl["algorithm"] == "ml" and "refine" in wl:
         g.set_positions(np.zeros((len(s["counts"]), 2)), refine=wl["refine"])
     if wl.get("opr"):
         u, w, c = opr_start(s, wl)
@@ -217,8 +223,9 @@ def algorithmic_bytes(kind, s, wl):
         # projection from the kept Ψ: Ψ read, object window, counts, (moved probe), change
         "frame_project": 8 * n2 + 4 * n2 + 16 * K * n2 + moved,
         # line search: object and direction windows, counts, kept Ψ and g, (moved probe and
-        # direction)
-        "ml_gamma": 16 * n2 + 4 * n2 + 16 * K * n2 + 2 * moved,
+        # direction); through slices every slice's object and direction windows and the counts
+        "ml_gamma": (16 * n2 * S + 4 * n2 if S > 1
+                     else 16 * n2 + 4 * n2 + 16 * K * n2 + 2 * moved),
         "move": 8 * K * n2,
         "back_spectrum": 16 * K * n2 + 8 * n2,
         "deriv_sums": 8 * K * n2 + 8 * n2,
@@ -239,6 +246,9 @@ def algorithmic_bytes(kind, s, wl):
         # of slices 1.. and the detector field, backward reads them and writes every slice's χ
         "slice_forward": 8 * n2 * S + 4 * n2 + 8 * K * n2 * S,
         "slice_backward": 4 * n2 + 8 * n2 * S + 16 * K * n2 * S,
+        # ML's gradient through the slices: every slice's window and the counts read, the
+        # incident waves of slices 1.. and every slice's gradient field written
+        "slice_grad": 8 * n2 * S + 4 * n2 + 8 * K * n2 * (S - 1) + 8 * K * n2 * S,
     }
     return table.get(kind)
 
@@ -311,9 +321,23 @@ def cpu_cycles(s, wl, m, cycles, threads):
     the scan with the full object; returns the seconds and the oracle state."""
     from oracle.ptycho import Ptycho
     t = sample_scan(s, min(m, len(s["counts"])))
+    if s.get("gaps"):
+        # ML through the slices (oracle.lsqml.multislice_ml); the state keeps every slice
+        from oracle.lsqml import multislice_ml
+        optics = oracle_optics(s)
+        p = Ptycho(t["counts"], t["y"], t["x"], optics, t["object"][:1], t["probe"])
+        with _threads(threads):
+            t0 = time.perf_counter()
+            objs, probe, _ = multislice_ml(p.addr, p.obs, optics, oracle_objects(t), p.probe,
+                                           cycles)
+            dt = time.perf_counter() - t0
+        from oracle import ops
+        ops.FFT_WORKERS = None
+        p.object, p.probe = np.concatenate(objs), probe
+        return dt, p
     p = Ptycho(t["counts"], t["y"], t["x"], oracle_optics(s), t["object"], t["probe"])
     with _threads(threads):
-        if wl["algorithm"] == "ml":
+        if wl["algorithm"] == "ml" and "refine" in wl:
             p.set_positions(np.zeros((p.addr.nframe, 2)), refine=wl["refine"])
         t0 = time.perf_counter()
         if wl["algorithm"] == "ml":
@@ -425,14 +449,15 @@ def accuracy(s, wl, oracle_state, device, cycles=2):
     from ptyrs_b200 import GpuPtycho, Scan
     t = sample_scan(s, oracle_state.addr.nframe)
     scan = Scan(t["counts"], t["y"], t["x"], t["wavelength"], t["distance"], t["detector_pixel"])
-    with GpuPtycho(scan, t["object"], t["probe"], device=device) as g:
+    gaps = s.get("gaps")
+    with GpuPtycho(scan, t["object"], t["probe"], device=device, gaps=gaps) as g:
         prepare(g, t, wl)
         run_algorithm(g, wl, cycles)
-        obj = g.object()
-        d = g.positions() if wl["algorithm"] == "ml" else None
-    illum = ops.illumination(oracle_state.addr.views, oracle_state.object.shape,
+        obj = g.objects() if gaps else g.object()
+        d = g.positions() if wl["algorithm"] == "ml" and "refine" in wl else None
+    illum = ops.illumination(oracle_state.addr.views, oracle_state.object[:1].shape,
                              oracle_state.probe)
-    w = (illum >= 1e-3 * illum.max()).astype(float)
+    w = np.broadcast_to(illum >= 1e-3 * illum.max(), obj.shape).astype(float)
     out = {"object_nrmse_vs_f64": object_nrmse(obj, oracle_state.object, w),
            "sample": f"{cycles} {wl['algorithm'].upper()} cycles over the first "
                      f"{t['counts'].shape[0]} frames, GPU FP32 vs the float64 oracle from the "
