@@ -31,6 +31,7 @@ import numpy as np
 
 from . import ops
 from .base import fftshift2, random_batches
+from .lsqml import SliceWaves, slice_jet
 
 EPS = 1e-8
 POSITION_STEP = 0.3  # bh.rs POSITION_STEP, pty-chi's ProbePositionOptions step size
@@ -165,6 +166,63 @@ class BhBatch:
         return float(h + terms[~self.mask].sum())
 
 
+class BhSlices:
+    """BhBatch through pty-chi's multislice object (engine/bh.rs with several slices, no
+    position model): the exit waves through the slices (`SliceWaves`), 2·∂F/∂x* over every
+    slice and the probe back through the slices' adjoints, and H(u, v) from the quadratic form
+    Q(w) = H(w, w) of the second-order expansion of the exit waves along w (`slice_jet`:
+    L_w = U ψ′, U J″(w, w) = 2·U ψ″) by polarization, H(u, v) = (Q(u + v) − Q(u − v))/4,
+    exact for the symmetric bilinear H."""
+
+    def __init__(self, views, obs, optics, objs, probe):
+        self.views, self.optics, self.objs, self.probe = views, optics, list(objs), probe
+        nmode = 1
+        while nmode < len(views) and views[nmode]["frame"] == views[0]["frame"]:
+            nmode += 1
+        self.nmode = nmode
+        self.frames = [int(views[b * nmode]["frame"]) for b in range(len(views) // nmode)]
+        ny, nx = probe.shape[-2:]
+        self.waves = SliceWaves(optics, views, self.objs, probe[views["probe"].astype(np.int64)])
+        self.psi = optics.exit_forward(self.waves.psi)
+        self.sh = (len(self.frames), nmode, ny, nx)
+        self.amp = np.sqrt((np.abs(self.psi.reshape(self.sh)) ** 2).sum(axis=1)) + EPS
+        iobs, self.mask = obs.iobs[self.frames], obs.mask[self.frames]
+        self.root = np.sqrt(iobs)
+        w = np.where(self.mask, 0.0, 1.0 - self.root / self.amp)
+        self.td = (self.psi.reshape(self.sh) * w[:, None]).reshape(self.psi.shape)
+
+    def grads(self):
+        """2·∂F/∂x* over every slice (a list) and the probe (engine/multislice.rs:266-286,
+        399-438 on the amplitude cost's exit-plane field)."""
+        e = self.optics.exit_adjoint(2.0 * self.td)
+        chis = self.waves.back_propagate(e)
+        g_objs = [self.waves.obj_adjoint(s, chis[s]) for s in range(len(self.objs))]
+        g_probe = ops.accumulate_probe(self.views, self.objs[0], self.probe.shape,
+                                       self.waves.shared(0), chis[0])[0]
+        return g_objs, g_probe, None
+
+    def quad(self, w_objs, w_probe):
+        """Q(w) = H(w, w): 2·Re⟨td, 2·U ψ″⟩ + 2·Σ_unmasked [(1 − d/a)·Σ_m |U ψ′|²
+        + d·c²/a³], c = Σ_m Re(conj(U psi)·U ψ′)."""
+        _, p1, p2 = slice_jet(self.optics, self.views, self.objs, self.probe, list(w_objs),
+                              w_probe)
+        h = 2.0 * _dot(self.td, 2.0 * p2)
+        p1 = p1.reshape(self.sh)
+        uu = (np.abs(p1) ** 2).sum(axis=1)
+        c = (np.conj(self.psi.reshape(self.sh)) * p1).real.sum(axis=1)
+        a, d = self.amp, self.root
+        terms = 2.0 * ((1.0 - d / a) * uu + d * c * c / (a * a * a))
+        return float(h + terms[~self.mask].sum())
+
+    def hessian(self, u, v):
+        (uo, up), (vo, vp) = tuple(u)[:2], tuple(v)[:2]
+        if uo is vo and up is vp:
+            return self.quad(uo, up)
+        plus = self.quad([a + b for a, b in zip(uo, vo)], up + vp)
+        minus = self.quad([a - b for a, b in zip(uo, vo)], up - vp)
+        return (plus - minus) / 4.0
+
+
 class Bh:
     """BH state across epochs (engine/bh.rs:580-760): the parameters, the epoch count and, with
     one batch per epoch, the last direction; under the position model `offsets` `[nframe, 2]`
@@ -187,6 +245,8 @@ class Bh:
         D = −Pg + β·D′ with β = H(Pg, D′)/H(D′, D′); α = −⟨g, D⟩/H(D, D)·count/size;
         object and probe += α·D. Returns `(obj, probe, steps)`, a step
         `dict(frames, beta, alpha, top, bottom)`."""
+        if isinstance(obj, (list, tuple)):
+            return self._epoch_slices(addr, obs, optics, list(obj), probe)
         nframe = addr.nframe
         size = min(self.batch_size, nframe)
         full = size == nframe
@@ -228,6 +288,43 @@ class Bh:
                               bottom=bottom))
         return obj, probe, steps
 
+    def _epoch_slices(self, addr, obs, optics, objs, probe):
+        """`epoch` through a multislice object (`objs` a list of slices; no position model):
+        every slice and the probe are the variables, the probe's part preconditioned by ρ²."""
+        if self.offsets is not None:
+            raise ValueError("BH through slices runs without the position model")
+        nframe = addr.nframe
+        size = min(self.batch_size, nframe)
+        full = size == nframe
+        rho2 = self.probe_rho ** 2 * optics.intensity_scale()
+        epoch = self.epochs
+        self.epochs += 1
+        steps = []
+        for frames in random_batches(nframe, size, self.seed, epoch):
+            views = np.concatenate([addr.frame_views(f) for f in frames])
+            b = BhSlices(views, obs, optics, objs, probe)
+            g_objs, g_probe, _ = b.grads()
+            pg = (g_objs, g_probe * rho2)
+            if full and self.prev is not None:
+                prev = self.prev
+                beta = b.hessian(pg, prev) / b.hessian(prev, prev)
+                direction = ([beta * d - g for d, g in zip(prev[0], pg[0])],
+                             beta * prev[1] - pg[1])
+            else:
+                beta = 0.0
+                direction = ([-g for g in pg[0]], -pg[1])
+            top = -(sum(_dot(g, d) for g, d in zip(g_objs, direction[0]))
+                    + _dot(g_probe, direction[1]))
+            bottom = b.hessian(direction, direction)
+            alpha = top / bottom * len(frames) / size
+            objs = [o + alpha * d for o, d in zip(objs, direction[0])]
+            probe = probe + alpha * direction[1]
+            if full:
+                self.prev = direction
+            steps.append(dict(frames=list(frames), beta=beta, alpha=alpha, top=top,
+                              bottom=bottom))
+        return objs, probe, steps
+
 
 def amplitude_cost(views, obs, optics, obj, probe, offsets=None):
     """F without the amplitude offset: Σ_unmasked (|U psi| − √iobs)², a quarter of PyNX's
@@ -242,4 +339,4 @@ def amplitude_cost(views, obs, optics, obj, probe, offsets=None):
     return ops.llk(obs, frames, nmode, psi).euclidian / 4.0
 
 
-__all__ = ["BhBatch", "Bh", "amplitude_cost", "fftshift2"]
+__all__ = ["BhBatch", "BhSlices", "Bh", "amplitude_cost", "fftshift2"]

@@ -62,6 +62,9 @@ GROUPS = {
     # every frame's offsets before and after, the object and probe changes of both epochs
     "bh_pos_full": ["obj", "probe", "offsets", "steps"],
     "bh_pos_mini": ["obj", "probe", "offsets", "steps"],
+    # through three slices (refs/f64/bh_multislice.py, on lsqml_multislice's state and counts;
+    # probe_rho 1): per case and method the steps, the slices' and the probe's changes
+    "bh_multislice": ["steps", "obj", "probe"],
     # one LSQML step refining the offsets with three eigenmodes of probe mode 0
     "lsqml_pos_opr": ["eigen", "weights", "steps", "offsets", "obj", "probe"],
     "rpie_ptychi": [""],

@@ -190,3 +190,40 @@ def test_epochs_with_refined_offsets_match_reference(name, batch):
     assert max_rel(ri(d_probe), ri(want_p), np.abs(ri(p.probe)).max()) < 3e-12
     want_d = g["offsets"][:, 3:5] - start
     assert max_rel(run.offsets - start, want_d) < 3e-12
+
+
+def test_epochs_through_slices_match_reference():
+    """engine_bh_multislice.rs:116-190: BH through three slices (the multislice LSQML state and
+    counts; angular-spectrum, Fresnel and far-field exits), CG over one batch of all 16 frames
+    and steepest descent over batches of 6, three epochs (seed 7, probe_rho 1): every step's
+    frames, β, α, top and bottom to 2e-13 and the slices' and the probe's changes to 2e-12, the
+    reference's own bounds (measured here 2e-14 and 2.4e-13 with the Hessian's bilinear form by
+    polarization)."""
+    from test_oracle_golden import multislice_state
+    g = golden("bh_multislice")
+    _, addr, objs0, probe0, cases = multislice_state()
+    ri = lambda z: np.stack([np.ravel(z).real, np.ravel(z).imag], 1).ravel()
+    for case, (optics, obs, _) in enumerate(cases):
+        for method, batch in enumerate((16, 6)):
+            run = Bh(batch, probe_rho=1.0, seed=7)
+            objs, probe = list(objs0), probe0.copy()
+            got = []
+            for e in range(3):
+                objs, probe, steps = run.epoch(addr, obs, optics, objs, probe)
+                got += [(e, s) for s in steps]
+            sel = lambda t: t[(t[:, 0] == case) & (t[:, 1] == method)]
+            rows = sel(g["steps"])
+            assert len(got) == len(rows)
+            for k, ((e, s), r) in enumerate(zip(got, rows)):
+                count = int(r[4])
+                assert [k, e, count] == [int(r[2]), int(r[3]), len(s["frames"])]
+                assert s["frames"] == [int(f) for f in r[10:10 + count]]
+                if r[5] == 0.0:
+                    assert s["beta"] == 0.0
+                for key, want in (("beta", r[5]), ("alpha", r[6]), ("top", r[7]),
+                                  ("bottom", r[8])):
+                    if want != 0.0:
+                        assert rel(s[key], want) < 2e-13, (case, method, k, key)
+            d_objs = np.concatenate([ri(o - o0) for o, o0 in zip(objs, objs0)])
+            assert max_rel(d_objs, sel(g["obj"])[:, 5:7].ravel()) < 2e-12
+            assert max_rel(ri(probe - probe0), sel(g["probe"])[:, 5:7].ravel()) < 2e-12
