@@ -279,7 +279,8 @@ int ptyb_get_positions(ptyb_handle* h, double* dst);
  * 645-760): pty-chi's bilinear-Hessian method on the amplitude cost, `nepoch` epochs from a
  * fresh run (epoch e's batches `random_batches(nframe, batch_size, seed, e)`), every batch
  * moving object and probe by α·D; an LLK record after every due epoch (calc_llk as
- * ptyb_lsqml's). One object slice (PTYB_INVALID otherwise). With ptyb_set_positions every
+ * ptyb_lsqml's). On a multislice handle every slice and the probe are the variables (no position
+ * model there: PTYB_INVALID). With ptyb_set_positions every
  * frame's probe is moved by its offset (Patch sampling, engine/bh.rs:92-275); refined offsets
  * are BH variables (their part of the gradient and the directions, 0.3·α·D_d added to them,
  * engine/bh.rs:725-745), held ones only move the probe. */

@@ -247,6 +247,128 @@ double dot_of(ptyb_handle* h, const float2* x, const float2* y, size_t n) {
   return out[0];
 }
 
+// BH through a multislice object (no position model): Q(w) = H(w, w) over the batch from the
+// second-order expansion of the exit waves along w through the slices (multislice.cuh
+// `slice_gamma_kernel` in its BH mode), per frame on the device, added in batch order.
+double bh_slice_quad(ptyb_handle* h, const int* frames, int n, const float2* w_obj,
+                     const float2* w_probe) {
+  SliceGammaArgs g = {};
+  g.d_obj = w_obj;
+  g.d_probe = w_probe;
+  g.bh = 1;
+  const int stack = std::min(n, h->slots);
+  for (int s0 = 0; s0 < n; s0 += stack) {
+    const int m = std::min(stack, n - s0);
+    g.sa.f = frame_args(h, frames + s0);
+    g.sa.f.nslot = m;
+    g.sa.tf = h->tf;
+    g.sa.nslice = h->nslice;
+    g.sa.obj_plane = (size_t)h->nyo * h->nxo;
+    g.out = h->gamma_sums + (size_t)s0 * 2;
+    cudaError_t e = cudaSuccess;
+    timed(h, kKBhHessian, [&] { e = launch_slice_gamma_side(h->N, g, m, h->K, h->stream); }, m);
+    check(h, e, "bh quadratic form through slices");
+    ++h->launches;
+  }
+  std::vector<double> out((size_t)n * 2);
+  check(h, copy_sync(h, out.data(), h->gamma_sums, out.size() * sizeof(double),
+                     cudaMemcpyDeviceToHost),
+        "bh quadratic form");
+  double s = 0.0;
+  for (int k = 0; k < n; ++k) s += out[2 * (size_t)k];
+  return s;
+}
+
+// H(u, v) through the slices by polarization, (Q(u + v) − Q(u − v))/4, exact for the
+// symmetric bilinear H; Q(u) when v is u.
+double bh_slice_hessian(ptyb_handle* h, const int* frames, int n, const BhVec& u,
+                        const BhVec& v) {
+  if (u.obj == v.obj && u.probe == v.probe) return bh_slice_quad(h, frames, n, u.obj, u.probe);
+  const size_t no = (size_t)h->nslice * h->nyo * h->nxo, np = (size_t)h->K * h->N * h->N;
+  float2 *to = h->bh_tmp, *tp = h->bh_tmp + no;
+  double q[2];
+  for (int k = 0; k < 2; ++k) {
+    const float sgn = k == 0 ? 1.f : -1.f;
+    check(h, cudaMemcpyAsync(to, u.obj, no * sizeof(float2), cudaMemcpyDeviceToDevice,
+                             h->stream),
+          "bh polarization");
+    check(h, cudaMemcpyAsync(tp, u.probe, np * sizeof(float2), cudaMemcpyDeviceToDevice,
+                             h->stream),
+          "bh polarization");
+    timed(h, kKAxpy, [&] {
+      axpy_kernel<<<blocks_for(no), 256, 0, h->stream>>>(to, v.obj, sgn, no);
+    });
+    launched(h, "bh polarization");
+    timed(h, kKAxpy, [&] {
+      axpy_kernel<<<blocks_for(np), 256, 0, h->stream>>>(tp, v.probe, sgn, np);
+    });
+    launched(h, "bh polarization");
+    q[k] = bh_slice_quad(h, frames, n, to, tp);
+  }
+  return (q[0] - q[1]) / 4.0;
+}
+
+// One BH epoch through the slices (the multislice counterpart of bh_epoch): the gradients
+// through the slices on BH's amplitude cost, the probe part preconditioned by ρ², β from the
+// polarized Hessian, α·D on every slice and the probe.
+void bh_epoch_slices(ptyb_handle* h, const ptyb_bh_params& p, const int* order,
+                     const std::vector<int32_t>& sizes, bool cg) {
+  const size_t no = (size_t)h->nslice * h->nyo * h->nxo, np = (size_t)h->K * h->N * h->N;
+  const int size = std::min(p.batch_size, h->P);
+  const double rho2 = p.probe_rho * p.probe_rho * ((double)h->N * h->N);
+  h->bh_steps.clear();
+  int off = 0;
+  for (size_t b = 0; b < sizes.size(); ++b) {
+    const int n = sizes[b];
+    const int* frames = order + off;
+    slice_gradients(h, true, true, frames, n, kCostBh);
+    check(h, cudaMemcpyAsync(h->last_probe, h->g_probe, np * sizeof(float2),
+                             cudaMemcpyDeviceToDevice, h->stream),
+          "preconditioned gradient");
+    timed(h, kKAxpy, [&] {
+      scale_kernel<<<blocks_for(np), 256, 0, h->stream>>>(h->last_probe, (float)rho2, np);
+    });
+    launched(h, "preconditioned gradient");
+    const BhVec pg = {h->g_slices, h->last_probe, nullptr};
+    const BhVec dir = {h->dir_slices, h->dir_probe, nullptr};
+    double beta = 0.0;
+    if (cg) beta = bh_slice_hessian(h, frames, n, pg, dir) / bh_slice_hessian(h, frames, n, dir, dir);
+    timed(h, kKAxpy, [&] {
+      cg_direction_kernel<<<blocks_for(no), 256, 0, h->stream>>>(h->dir_slices, h->g_slices,
+                                                                 (float)beta, no);
+    });
+    launched(h, "direction");
+    timed(h, kKAxpy, [&] {
+      cg_direction_kernel<<<blocks_for(np), 256, 0, h->stream>>>(h->dir_probe, h->last_probe,
+                                                                 (float)beta, np);
+    });
+    launched(h, "direction");
+    const double top =
+        -(dot_of(h, h->g_slices, h->dir_slices, no) + dot_of(h, h->g_probe, h->dir_probe, np));
+    const double bottom = bh_slice_hessian(h, frames, n, dir, dir);
+    const double alpha = top / bottom * n / size;
+    timed(h, kKAxpy, [&] {
+      axpy_kernel<<<blocks_for(no), 256, 0, h->stream>>>(h->object, h->dir_slices, (float)alpha,
+                                                         no);
+    });
+    launched(h, "step");
+    timed(h, kKAxpy, [&] {
+      axpy_kernel<<<blocks_for(np), 256, 0, h->stream>>>(h->probe, h->dir_probe, (float)alpha,
+                                                         np);
+    });
+    launched(h, "step");
+    ptyb_bh_step s;
+    s.batch = (int32_t)b;
+    s.count = n;
+    s.beta = beta;
+    s.alpha = alpha;
+    s.top = top;
+    s.bottom = bottom;
+    h->bh_steps.push_back(s);
+    off += n;
+  }
+}
+
 // The run's state on the host: the offsets and, for CG, the direction's offsets part by frame.
 struct BhHost {
   std::vector<double> offsets;  // [P][2]
@@ -374,8 +496,12 @@ int ptyb_bh(ptyb_handle* h, const ptyb_bh_params* p, int32_t nepoch, int32_t cal
     h->err = "BH batch_size must be >= 1";
     return PTYB_INVALID;
   }
-  if (h->nslice > 1) {
-    h->err = "BH runs on a single-slice object";
+  if (h->nslice > 1 && h->have_offsets) {
+    h->err = "BH through slices runs without the position model";
+    return PTYB_INVALID;
+  }
+  if (h->nslice > 1 && slice_gamma_bytes(h->N, h->K) > 227 * 1024) {
+    h->err = "BH through slices: the frame's modes do not fit one cluster's shared memory";
     return PTYB_INVALID;
   }
   if (!std::isfinite(p->position_rho) || !std::isfinite(p->probe_rho)) {
@@ -386,7 +512,15 @@ int ptyb_bh(ptyb_handle* h, const ptyb_bh_params* p, int32_t nepoch, int32_t cal
     const int size = std::min(p->batch_size, h->P);
     ensure_slots(h, std::min(h->P, h->stack));
     ensure_ml(h);
-    const bool pos = h->have_offsets;
+    const bool pos = h->have_offsets, slices = h->nslice > 1;
+    if (slices) {
+      const size_t no = (size_t)h->nslice * h->nyo * h->nxo;
+      if (!h->last_slices) {
+        h->last_slices = alloc<float2>(h, no);
+        h->dir_slices = alloc<float2>(h, no);
+      }
+      if (!h->bh_tmp) h->bh_tmp = alloc<float2>(h, no + (size_t)h->K * h->N * h->N);
+    }
     BhHost st;
     if (pos) {
       ensure_spec(h);
@@ -412,8 +546,12 @@ int ptyb_bh(ptyb_handle* h, const ptyb_bh_params* p, int32_t nepoch, int32_t cal
     }
     begin_call(h);
     for (int ic = 0; ic < nepoch; ++ic) {
-      bh_epoch(h, *p, h->order_all + (size_t)ic * h->P, order_h.data() + (size_t)ic * h->P,
-               sizes[ic], size == h->P && ic > 0, st);
+      if (slices)
+        bh_epoch_slices(h, *p, h->order_all + (size_t)ic * h->P, sizes[ic],
+                        size == h->P && ic > 0);
+      else
+        bh_epoch(h, *p, h->order_all + (size_t)ic * h->P, order_h.data() + (size_t)ic * h->P,
+                 sizes[ic], size == h->P && ic > 0, st);
       if (llk_due(calc_llk, ic, nepoch)) {
         if (pos) {
           // every frame's moved probe at the epoch's end, for the LLK

@@ -129,6 +129,7 @@ struct ptyb_handle {
   // ML through the slices: the previous gradients and the directions of every slice.
   float2* last_slices = nullptr;  // [S][nyo][nxo]
   float2* dir_slices = nullptr;   // [S][nyo][nxo]
+  float2* bh_tmp = nullptr;       // [S][nyo][nxo] then [K][N][N]: BH's u ± v through slices
   // AP / DM / RAAR: every frame's carried exit waves and RAAR's iterate, [P][K][N][N]; the
   // probe blend's per-chunk norms and its norm plane.
   float2* carry = nullptr;
@@ -349,6 +350,12 @@ void parallel_range(size_t n, F&& fn) {
 void download_c64(ptyb_handle* h, const float2* src, double* dst, size_t n, const char* what);
 void upload_c64(ptyb_handle* h, const double* src, float2* dst, size_t n, const char* what);
 void ensure_ml(ptyb_handle* h);
+// 2·∂F/∂x* over every slice (h->g_slices) and the probe (h->g_probe) through a multislice
+// object, over `n` frames (every frame when null), Poisson or with kCostBh BH's amplitude cost.
+void slice_gradients(ptyb_handle* h, bool uo, bool up, const int* frames = nullptr, int n = 0,
+                     int cost = kCostPoisson);
+// Shared memory of the multislice line search (and BH's quadratic form) at side N, K modes.
+size_t slice_gamma_bytes(int N, int K);
 void array_sums(ptyb_handle* h, const float2* g, const float2* hh, size_t n, int mode,
                 double out[2]);
 unsigned blocks_for(size_t n);

@@ -41,7 +41,8 @@ enum FrameMode : int {
                    // (kMlGrad's pass otherwise: the detector field kept in psi_out)
 };
 
-enum Cost : int { kCostPoisson = 0, kCostAmplitude = 1 };
+// kCostBh: BH's amplitude gradient 2(1 − √I/A), A = √Ĩ + 1e-8 (the multislice gradient pass)
+enum Cost : int { kCostPoisson = 0, kCostAmplitude = 1, kCostBh = 2 };
 
 struct FrameArgs {
   const float2* object;  // [nobj][nyo][nxo]

@@ -6,15 +6,19 @@
 using namespace ptyb;
 
 namespace ptyb::eng {
-namespace {
 
-// Every slice's 2·∂L/∂O_s* and the probe's 2·∂L/∂P* of the Poisson LLK sum through a
-// multislice object (the adjoint of engine/multislice.rs:87-173, 266-286, 399-438): per stack,
-// the exit wave's Poisson gradient back-propagated through the slices on chip, then per slice
+// Every slice's 2·∂L/∂O_s* and the probe's 2·∂L/∂P* of the Poisson LLK sum (or with cost
+// kCostBh BH's amplitude cost) through a multislice object over `n` frames (every frame when
+// null) (the adjoint of engine/multislice.rs:87-173, 266-286, 399-438): per stack, the exit
+// wave's gradient back-propagated through the slices on chip, then per slice
 // Σ conj(q_s·in_s)·g_s gathered in frame order, the probe's Σ conj(O_0)·g_0.
-
-void slice_gradients(ptyb_handle* h, bool uo, bool up) {
-  const int S = h->nslice, stack = std::min(h->P, h->stack);
+void slice_gradients(ptyb_handle* h, bool uo, bool up, const int* frames_in, int nframes,
+                     int cost) {
+  if (!frames_in) {
+    frames_in = h->iota;
+    nframes = h->P;
+  }
+  const int S = h->nslice, stack = std::min(nframes, h->stack);
   ensure_slots(h, stack);
   ensure_ml(h);
   const size_t plane = (size_t)h->N * h->N, fplanes = (size_t)h->K * plane;
@@ -27,13 +31,14 @@ void slice_gradients(ptyb_handle* h, bool uo, bool up) {
   check(h, cudaMemsetAsync(h->g_slices_c, 0, (size_t)S * no * sizeof(float2), h->stream), "memset");
   check(h, cudaMemsetAsync(h->g_probe, 0, fplanes * sizeof(float2), h->stream), "memset");
   check(h, cudaMemsetAsync(h->g_probe_c, 0, fplanes * sizeof(float2), h->stream), "memset");
-  for (int s0 = 0; s0 < h->P; s0 += stack) {
-    const int n = std::min(stack, h->P - s0);
-    const int* frames = h->iota + s0;
+  for (int s0 = 0; s0 < nframes; s0 += stack) {
+    const int n = std::min(stack, nframes - s0);
+    const int* frames = frames_in + s0;
     const size_t slice_stride = (size_t)n * fplanes;
     SliceArgs sa = {};
     sa.f = frame_args(h, frames);
     sa.f.nslot = n;
+    sa.f.cost = cost;
     sa.tf = h->tf;
     sa.incident = h->incident;
     sa.chi = h->chi_slices;
@@ -83,6 +88,20 @@ void slice_gradients(ptyb_handle* h, bool uo, bool up) {
     }
   }
 }
+
+// Shared memory of the multislice line search for frames of side N with K modes.
+size_t slice_gamma_bytes(int N, int K) {
+  switch (N) {
+    case 64: return slice_gamma_smem_bytes<64, gamma_cluster(64)>(K);
+    case 96: return slice_gamma_smem_bytes<96, gamma_cluster(96)>(K);
+    case 128: return slice_gamma_smem_bytes<128, gamma_cluster(128)>(K);
+    case 192: return slice_gamma_smem_bytes<192, gamma_cluster(192)>(K);
+    case 256: return slice_gamma_smem_bytes<256, gamma_cluster(256)>(K);
+  }
+  return ~size_t(0);
+}
+
+namespace {
 
 // The Poisson gradient numerators of object and probe over every frame, by stacks in frame
 // order (engine/ptycho.rs:497-561).
@@ -238,18 +257,6 @@ void ml_gamma(ptyb_handle* h, double* num, double* den) {
     *num += v[(size_t)f * 2];
     *den += v[(size_t)f * 2 + 1];
   }
-}
-
-// Shared memory of the multislice line search for frames of side N with K modes.
-size_t slice_gamma_bytes(int N, int K) {
-  switch (N) {
-    case 64: return slice_gamma_smem_bytes<64, gamma_cluster(64)>(K);
-    case 96: return slice_gamma_smem_bytes<96, gamma_cluster(96)>(K);
-    case 128: return slice_gamma_smem_bytes<128, gamma_cluster(128)>(K);
-    case 192: return slice_gamma_smem_bytes<192, gamma_cluster(192)>(K);
-    case 256: return slice_gamma_smem_bytes<256, gamma_cluster(256)>(K);
-  }
-  return ~size_t(0);
 }
 
 // num and den of the Poisson line search along (dir_slices, dir_probe) through the slices

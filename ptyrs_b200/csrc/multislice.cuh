@@ -23,8 +23,9 @@ struct SliceArgs {
 };
 
 // kSliceGrad: forward (incident waves stored), the Poisson gradient 2(1 − I/Ĩ) of the exit
-// wave (masked 0) and its back-propagation through the slices into `chi` (no subtraction):
-// every slice's 2·∂L/∂ψ_s*, the adjoint of the multislice model.
+// wave (masked 0; with cost kCostBh BH's amplitude gradient 2(1 − √I/(√Ĩ + 1e-8))) and its
+// back-propagation through the slices into `chi` (no subtraction): every slice's 2·∂L/∂ψ_s*,
+// the adjoint of the multislice model.
 enum SliceMode : int { kSliceForward = 0, kSliceBackward = 1, kSliceLlk = 2, kSliceGrad = 3 };
 
 // Window of slice s times `v` for every plane's rows of this CTA (shifted layout); the last
@@ -233,8 +234,11 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T, frame_min_blocks<N, C>())
     const float yo = yo_r[i], ic = ic_r[i];
     float fac;
     if (MODE == kSliceGrad) {
-      // GradPoissonFourier (engine/ops.rs:161-195)
-      fac = (yo < 0.f ? 0.f : 2.f * (1.f - yo / fmaxf(ic, 1e-12f))) * inv_n2;
+      // GradPoissonFourier (engine/ops.rs:161-195), or BH's (engine/bh.rs:168-275)
+      fac = yo < 0.f                ? 0.f
+            : a.cost == kCostBh     ? 2.f * (1.f - sqrtf(yo) / (sqrtf(ic) + 1e-8f))
+                                    : 2.f * (1.f - yo / fmaxf(ic, 1e-12f));
+      fac *= inv_n2;
     } else {
       float cres = 0.f;
       if (yo >= 0.f)
@@ -354,11 +358,16 @@ static __global__ void __launch_bounds__(1024) slice_solve_kernel(const double* 
 // s = Σ_m |a|² + 2·Re(p̄o·b), d = 1 − I/max(calc, 1e-32): num = −Σ 2·r·d,
 // den = Σ 2·s·d + I·(2r/calc)² (PyNX CG_Poisson_Gamma, engine/ops.rs:206-253). Shared memory
 // holds the three sets of K planes.
+// With `bh` the kernel takes BH's quadratic form Q(w) = H(w, w) of the amplitude cost along
+// the displacement instead (engine/bh.rs:500-575): per unmasked pixel with A = √Σ_m |po|² +
+// 1e-8, d = √I and c = Σ_m Re(p̄o·a): 4·(1 − d/A)·Σ_m Re(p̄o·b) + 2·(1 − d/A)·Σ_m |a|² +
+// 2·d·c²/A³ (U J″(w, w) = 2·b), into out[slot][0].
 struct SliceGammaArgs {
   SliceArgs sa;
   const float2* d_obj;    // [nslice][nyo][nxo]
   const float2* d_probe;  // [K][N][N]
   double* out;            // [slot][2]: num, den
+  int bh;
 };
 
 template <int N, int C>
@@ -436,15 +445,22 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T, 1) slice_gamma_kernel(Sli
     const int c = idx % H, ky = idx / H;
     const float yo = iobs[ky * N + r * H + c];
     if (yo < 0.f) continue;
-    double calc = 0.0, rr = 0.0, ss = 0.0;
+    double calc = 0.0, rr = 0.0, ss = 0.0, pb = 0.0, aa = 0.0;
     for (int m = 0; m < K; ++m) {
       const int l0 = m * H + c, l1 = (K + m) * H + c, l2 = (2 * K + m) * H + c;
       const float2 po = S[l0 * L + (ky ^ swz(l0))], av = S[l1 * L + (ky ^ swz(l1))],
                    bv = S[l2 * L + (ky ^ swz(l2))];
       calc += (double)cnorm2(po) * inv_n2;
       rr += ((double)po.x * av.x + (double)po.y * av.y) * inv_n2;
-      ss += ((double)cnorm2(av) + 2.0 * ((double)po.x * bv.x + (double)po.y * bv.y)) * inv_n2;
+      pb += ((double)po.x * bv.x + (double)po.y * bv.y) * inv_n2;
+      aa += (double)cnorm2(av) * inv_n2;
     }
+    if (g.bh) {
+      const double amp = sqrt(calc) + 1e-8, d = sqrt((double)yo), w = 1.0 - d / amp;
+      v[0] += 4.0 * w * pb + 2.0 * w * aa + 2.0 * d * rr * rr / (amp * amp * amp);
+      continue;
+    }
+    ss = aa + 2.0 * pb;
     calc = fmax(calc, 1e-32);
     const double d = 1.0 - (double)yo / calc;
     v[0] -= 2.0 * rr * d;

@@ -239,3 +239,39 @@ def test_ml_through_slices(case, probe_too):
         assert np.abs(hist["poisson"] - want).max() <= RUN_TOL * max(want)
         with pytest.raises(PtybError):
             g.ml(1, zero_phase_ramp=True)
+
+
+@pytest.mark.parametrize("full", [True, False], ids=["cg", "mini"])
+def test_bh_through_slices(case, full):
+    """pty-chi's BH through the slices (`ptyb_bh` on a multislice handle): the amplitude cost's
+    gradients through the slices, β from H(u, v) by polarization of the quadratic form on the
+    second-order expansion through the slices, α·D on every slice and the probe, against the
+    oracle (pinned to the reference's bh_multislice runs) over two epochs with one batch of every
+    frame (conjugate directions) and with smaller batches: every step, every slice, the probe."""
+    from oracle.bh import Bh
+    cpu = oracle_of(case)
+    nframe = len(case["counts"])
+    batch = nframe if full else max(2, nframe // 3)
+    run = Bh(batch, probe_rho=0.01, seed=7)
+    objs, probe = list(case["objects"]), cpu.probe
+    for _ in range(2):
+        objs, probe, steps = run.epoch(cpu.addr, cpu.obs, cpu.optics, objs, probe)
+    with gpu_of(case) as g:
+        g.bh(2, batch_size=batch, probe_rho=0.01, seed=7, calc_llk=1)
+        got = g.bh_steps()
+        assert [s["count"] for s in got] == [len(s["frames"]) for s in steps]
+        for gs, cs in zip(got, steps):
+            for key in ("alpha", "top", "bottom"):
+                assert abs(gs[key] - cs[key]) <= RUN_TOL * abs(cs[key]), key
+            if cs["beta"] == 0.0:
+                assert gs["beta"] == 0.0
+            else:
+                assert abs(gs["beta"] - cs["beta"]) <= 10 * RUN_TOL * abs(cs["beta"])
+        got_objs = g.objects()
+        for k in range(3):
+            assert rel_l2(got_objs[k] - 1.0, objs[k][0] - 1.0) < RUN_TOL, k
+        assert rel_l2(g.probe(), probe) < RUN_TOL
+        assert list(g.history()["algorithm"]) == ["bh"] * 2
+        g.set_positions(np.zeros((nframe, 2)))
+        with pytest.raises(PtybError):
+            g.bh(1, batch_size=batch)
