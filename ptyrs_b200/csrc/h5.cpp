@@ -6,6 +6,7 @@
 
 #include <zlib.h>
 
+#include <algorithm>
 #include <cstring>
 #include <fstream>
 #include <iterator>
@@ -17,6 +18,16 @@ namespace {
 [[noreturn]] void fail(const std::string& what) { throw std::runtime_error("HDF5: " + what); }
 
 constexpr int kMaxDepth = 64;
+constexpr uint64_t kMaxNodes = 1u << 22;       // B-tree nodes one read may visit
+constexpr uint64_t kMaxBytes = 1ull << 42;     // the largest dataset read (4 TiB)
+constexpr uint64_t kMaxWork = 1ull << 24;      // work units one public call may spend
+// A dataset is at most what its file can hold: deflate expands at most ~1032:1.
+constexpr uint64_t kMaxExpansion = 1100;
+
+// Fails unless [o, o + k) lies within a field of n bytes.
+inline void need(size_t o, size_t k, size_t n, const char* what) {
+  if (o > n || k > n - o) fail(std::string("truncated ") + what);
+}
 
 uint64_t le(const uint8_t* p, int n) {
   uint64_t v = 0;
@@ -30,7 +41,7 @@ bool undefined(uint64_t addr, int so) {
 
 // Parses a datatype message at p (at most n bytes); *used receives its length.
 Type parse_type(const uint8_t* p, size_t n, size_t* used, int depth = 0) {
-  if (n < 8) fail("truncated datatype");
+  need(0, 8, n, "datatype");
   if (depth > 8) fail("datatype nested too deeply");
   Type t;
   const int cls = p[0] & 15, version = p[0] >> 4;
@@ -42,11 +53,13 @@ Type parse_type(const uint8_t* p, size_t n, size_t* used, int depth = 0) {
       t.cls = Type::kFixed;
       t.big_endian = bits & 1;
       t.is_signed = (bits >> 3) & 1;
+      need(o, 4, n, "fixed-point datatype");
       o += 4;
       break;
     case Type::kFloat:
       t.cls = Type::kFloat;
       t.big_endian = bits & 1;
+      need(o, 12, n, "floating-point datatype");
       o += 12;
       break;
     case Type::kString:
@@ -56,13 +69,14 @@ Type parse_type(const uint8_t* p, size_t n, size_t* used, int depth = 0) {
       t.cls = Type::kCompound;
       const int nmem = (int)(bits & 0xffff);
       for (int k = 0; k < nmem; ++k) {
-        if (o >= n) fail("truncated compound datatype");
+        need(o, 1, n, "compound datatype");
         const char* name = reinterpret_cast<const char*>(p + o);
         const size_t len = strnlen(name, n - o);
         Type::Member m;
         m.name.assign(name, len);
         if (version < 3) {
           o += (len + 8) / 8 * 8;  // name with its terminator, padded to 8 bytes
+          need(o, 4, n, "compound member");
           m.offset = (uint32_t)le(p + o, 4);
           o += 4;
           if (version == 1) o += 1 + 3 + 4 + 4 + 16;  // dimensionality, permutation, sizes
@@ -70,9 +84,11 @@ Type parse_type(const uint8_t* p, size_t n, size_t* used, int depth = 0) {
           o += len + 1;
           int ob = 1;
           while (ob < 4 && (t.size >> (8 * ob))) ++ob;
+          need(o, ob, n, "compound member");
           m.offset = (uint32_t)le(p + o, ob);
           o += ob;
         }
+        need(o, 8, n, "compound member type");
         size_t u = 0;
         m.type = std::make_shared<Type>(parse_type(p + o, n - o, &u, depth + 1));
         o += u;
@@ -84,13 +100,16 @@ Type parse_type(const uint8_t* p, size_t n, size_t* used, int depth = 0) {
       t.cls = Type::kEnum;
       const int nmem = (int)(bits & 0xffff);
       size_t u = 0;
+      need(o, 8, n, "enumeration base type");
       t.base = std::make_shared<Type>(parse_type(p + o, n - o, &u, depth + 1));
       o += u;
       for (int k = 0; k < nmem; ++k) {  // the names
+        need(o, 1, n, "enumeration names");
         const size_t len = strnlen(reinterpret_cast<const char*>(p + o), n - o);
         o += version < 3 ? (len + 8) / 8 * 8 : len + 1;
       }
       o += (size_t)nmem * t.base->size;  // the values
+      need(0, o, n, "enumeration values");
       break;
     }
     default:
@@ -103,9 +122,9 @@ Type parse_type(const uint8_t* p, size_t n, size_t* used, int depth = 0) {
 
 // Undoes HDF5's shuffle filter: byte b of element i was stored at b·n + i.
 std::vector<uint8_t> unshuffle(const std::vector<uint8_t>& in, size_t es) {
-  if (es <= 1) return in;
+  const size_t n = es > 1 ? in.size() / es : 0;
+  if (n == 0) return in;
   std::vector<uint8_t> out(in.size());
-  const size_t n = in.size() / es;
   for (size_t b = 0; b < es; ++b)
     for (size_t i = 0; i < n; ++i) out[i * es + b] = in[b * n + i];
   std::copy(in.begin() + n * es, in.end(), out.begin() + n * es);
@@ -135,11 +154,11 @@ struct Filter {
 
 std::vector<Filter> parse_filters(const uint8_t* p, size_t n) {
   std::vector<Filter> out;
-  if (n < 2) fail("truncated filter pipeline");
+  need(0, 2, n, "filter pipeline");
   const int version = p[0], nf = p[1];
   size_t o = version == 1 ? 8 : 2;
   for (int k = 0; k < nf; ++k) {
-    if (o + 8 > n) fail("truncated filter description");
+    need(o, 8, n, "filter description");
     Filter f;
     f.id = (int)le(p + o, 2);
     o += 2;
@@ -148,10 +167,12 @@ std::vector<Filter> parse_filters(const uint8_t* p, size_t n) {
       namelen = le(p + o, 2);
       o += 2;
     }
+    need(o, 4, n, "filter description");
     f.flags = (int)le(p + o, 2);
     const int nv = (int)le(p + o + 2, 2);
     o += 4;
     o += version == 1 ? (namelen + 7) / 8 * 8 : namelen;
+    need(o, 4 * (size_t)nv, n, "filter client data");
     for (int v = 0; v < nv; ++v, o += 4) f.values.push_back((uint32_t)le(p + o, 4));
     if (version == 1 && (nv & 1)) o += 4;
     out.push_back(f);
@@ -174,23 +195,29 @@ File::File(const std::string& path) {
     }
   if (sb == ~0ull) fail(path + " is not an HDF5 file");
   const uint8_t* p = &buf_[sb + 8];
+  const size_t room = buf_.size() - (sb + 8);
   const int version = p[0];
   if (version <= 1) {
     so_ = p[5];
     sl_ = p[6];
-    size_t o = version == 1 ? 20 : 16;
-    base_ = le(p + o, so_);
-    o += 4 * (size_t)so_;  // base, free-space, end-of-file and driver addresses
-    root_ = le(p + o + so_, so_);  // the root entry's object header address
   } else if (version == 2 || version == 3) {
     so_ = p[1];
     sl_ = p[2];
-    base_ = le(p + 4, so_);
-    root_ = le(p + 4 + 3 * (size_t)so_, so_);
   } else {
     fail("superblock version " + std::to_string(version));
   }
   if ((so_ != 4 && so_ != 8) || (sl_ != 4 && sl_ != 8)) fail("unsupported offset size");
+  if (version <= 1) {
+    size_t o = version == 1 ? 20 : 16;
+    need(o, 6 * (size_t)so_, room, "superblock");
+    base_ = le(p + o, so_);
+    o += 4 * (size_t)so_;  // base, free-space, end-of-file and driver addresses
+    root_ = le(p + o + so_, so_);  // the root entry's object header address
+  } else {
+    need(4, 4 * (size_t)so_, room, "superblock");
+    base_ = le(p + 4, so_);
+    root_ = le(p + 4 + 3 * (size_t)so_, so_);
+  }
 }
 
 const uint8_t* File::ptr(uint64_t addr, uint64_t n) const {
@@ -201,10 +228,16 @@ const uint8_t* File::ptr(uint64_t addr, uint64_t n) const {
 
 uint64_t File::uint_at(uint64_t at, int n) const { return le(ptr(at, n), n); }
 
+void File::spend(uint64_t units) const {
+  work_ += units;
+  if (work_ > kMaxWork) fail("the file's structure does not end (a cycle)");
+}
+
 void File::collect(uint64_t at, uint64_t len, int version, std::vector<Message>* out,
                    int depth) const {
   if (depth > kMaxDepth) fail("object header continuations nested too deeply");
   const uint8_t* p = ptr(at, len);
+  spend(1 + len / 64);
   size_t o = 0;
   // version 2 headers carry their flags in the first byte of `version` (>> 8)
   const int v = version & 0xff, flags = version >> 8;
@@ -222,6 +255,7 @@ void File::collect(uint64_t at, uint64_t len, int version, std::vector<Message>*
     o += head;
     if (o + size > len) fail("a header message overruns its block");
     if (type == 0x10) {  // continuation: more messages elsewhere
+      need(0, (size_t)so_ + sl_, size, "continuation message");
       const uint64_t addr = le(p + o, so_), clen = le(p + o + so_, sl_);
       if (v == 1) {
         collect(addr, clen, version, out, depth + 1);
@@ -246,6 +280,7 @@ std::vector<File::Message> File::messages(uint64_t h) const {
     if (flags & 0x20) o += 16;  // the four times
     if (flags & 0x10) o += 4;   // attribute storage thresholds
     const int sz = 1 << (flags & 3);
+    ptr(h, o + sz);
     const uint64_t len = uint_at(h + o, sz);
     o += sz;
     collect(h + o, len, 2 | (flags << 8), &out, 0);
@@ -265,12 +300,14 @@ void File::group_btree(uint64_t btree, uint64_t heap, std::map<std::string, Link
   const uint8_t* data = ptr(hdata, hsize);
   auto heap_str = [&](uint64_t off) {
     if (off >= hsize) fail("local heap offset out of range");
+    spend(1 + (hsize - off) / 256);
     return std::string(reinterpret_cast<const char*>(data + off), strnlen(
         reinterpret_cast<const char*>(data + off), hsize - off));
   };
   const uint8_t* t = ptr(btree, 8 + 2 * (size_t)so_);
   if (memcmp(t, "TREE", 4) || t[4] != 0) fail("bad group B-tree node");
   const int level = t[5], used = (int)le(t + 6, 2);
+  spend(1 + used);
   const size_t entry = (size_t)sl_ + so_;
   const uint8_t* k = ptr(btree + 8 + 2 * (size_t)so_, entry * used + sl_);
   for (int i = 0; i < used; ++i) {
@@ -282,6 +319,7 @@ void File::group_btree(uint64_t btree, uint64_t heap, std::map<std::string, Link
     const uint8_t* sn = ptr(child, 8);
     if (memcmp(sn, "SNOD", 4)) fail("bad symbol-table node");
     const int nsym = (int)le(sn + 6, 2);
+    spend(1 + nsym);
     const size_t es = 2 * (size_t)so_ + 24;
     const uint8_t* e = ptr(child + 8, es * nsym);
     for (int s = 0; s < nsym; ++s, e += es) {
@@ -303,27 +341,33 @@ std::map<std::string, File::Link> File::links(uint64_t header) const {
   std::vector<std::string> order;
   for (const Message& m : messages(header)) {
     if (m.type == 0x11) {  // symbol table
+      need(0, 2 * (size_t)so_, m.size, "symbol table message");
       group_btree(le(m.p, so_), le(m.p + so_, so_), &out, &order, 0);
     } else if (m.type == 0x06) {  // link
       const uint8_t* p = m.p;
+      need(0, 2, m.size, "link message");
       const int flags = p[1];
       size_t o = 2;
       int ltype = 0;
+      need(o, 1 + 8 + 1 + 8, m.size, "link message");
       if (flags & 8) ltype = p[o++];
       if (flags & 4) o += 8;
       if (flags & 16) o += 1;
       const int nb = 1 << (flags & 3);
       const size_t len = le(p + o, nb);
       o += nb;
-      if (o + len > m.size) fail("bad link message");
+      need(o, len, m.size, "link name");
       const std::string name(reinterpret_cast<const char*>(p + o), len);
       o += len;
       Link l;
       if (ltype == 0) {
+        need(o, so_, m.size, "hard link");
         l.addr = le(p + o, so_);
       } else if (ltype == 1) {
         l.soft = true;
+        need(o, 2, m.size, "soft link");
         const size_t tl = le(p + o, 2);
+        need(o + 2, tl, m.size, "soft link value");
         l.target.assign(reinterpret_cast<const char*>(p + o + 2), tl);
       } else {
         continue;  // external links are not followed
@@ -331,6 +375,7 @@ std::map<std::string, File::Link> File::links(uint64_t header) const {
       if (!out.count(name)) order.push_back(name);
       out[name] = l;
     } else if (m.type == 0x02) {  // link info: a fractal heap means dense link storage
+      need(0, 2 + 8 + (size_t)so_, m.size, "link info message");
       const int flags = m.p[1];
       const uint64_t heap = le(m.p + 2 + ((flags & 1) ? 8 : 0), so_);
       if (!undefined(heap, so_)) fail("groups in dense link storage are not read");
@@ -343,7 +388,10 @@ std::vector<std::string> File::member_order(uint64_t header) const {
   std::map<std::string, Link> out;
   std::vector<std::string> order;
   for (const Message& m : messages(header)) {
-    if (m.type == 0x11) group_btree(le(m.p, so_), le(m.p + so_, so_), &out, &order, 0);
+    if (m.type == 0x11) {
+      need(0, 2 * (size_t)so_, m.size, "symbol table message");
+      group_btree(le(m.p, so_), le(m.p + so_, so_), &out, &order, 0);
+    }
   }
   if (order.empty())
     for (auto& kv : links(header)) order.push_back(kv.first);
@@ -376,6 +424,7 @@ uint64_t File::resolve(const std::string& path, int depth) const {
 }
 
 bool File::exists(const std::string& path) const {
+  work_ = 0;
   try {
     resolve(path);
     return true;
@@ -385,10 +434,12 @@ bool File::exists(const std::string& path) const {
 }
 
 std::vector<std::string> File::members(const std::string& path) const {
+  work_ = 0;
   return member_order(resolve(path));
 }
 
 Dataset File::dataset(const std::string& path) const {
+  work_ = 0;
   const uint64_t h = resolve(path);
   Dataset d;
   bool have_space = false, have_type = false, have_layout = false;
@@ -401,10 +452,11 @@ Dataset File::dataset(const std::string& path) const {
   for (const Message& m : messages(h)) {
     const uint8_t* p = m.p;
     if (m.type == 0x01) {  // dataspace
-      const int version = p[0], rank = p[1], flags = p[2];
+      need(0, 4, m.size, "dataspace");
+      const int version = p[0], rank = p[1];
       size_t o = version == 1 ? 8 : 4;
       if (version == 2 && p[3] == 2) fail(path + " has a null dataspace");
-      (void)flags;
+      need(o, (size_t)rank * sl_, m.size, "dataspace");
       d.shape.clear();
       for (int k = 0; k < rank; ++k, o += sl_) d.shape.push_back(le(p + o, sl_));
       have_space = true;
@@ -415,17 +467,22 @@ Dataset File::dataset(const std::string& path) const {
     } else if (m.type == 0x0B) {
       filters = parse_filters(p, m.size);
     } else if (m.type == 0x08) {
+      need(0, 3, m.size, "data layout");
       const int version = p[0];
       if (version == 3) {
         layout = p[1];
         if (layout == 0) {
+          need(2, 2, m.size, "compact layout");
           compact_n = le(p + 2, 2);
           compact = p + 4;
+          need(4, compact_n, m.size, "compact data");
         } else if (layout == 1) {
+          need(2, (size_t)so_ + sl_, m.size, "contiguous layout");
           addr = le(p + 2, so_);
           csize = le(p + 2 + so_, sl_);
         } else if (layout == 2) {
           const int nd = p[2];
+          need(3, (size_t)so_ + 4 * (size_t)nd, m.size, "chunked layout");
           addr = le(p + 3, so_);
           for (int k = 0; k < nd; ++k) chunk.push_back(le(p + 3 + so_ + 4 * k, 4));
         }
@@ -433,6 +490,8 @@ Dataset File::dataset(const std::string& path) const {
         const int nd = p[1];
         layout = p[2];
         size_t o = 8;
+        need(o, (layout != 0 ? so_ : 0) + 4 * (size_t)nd + (layout == 0 ? 4 : 0), m.size,
+             "data layout");
         if (layout != 0) {
           addr = le(p + o, so_);
           o += so_;
@@ -441,6 +500,7 @@ Dataset File::dataset(const std::string& path) const {
         if (layout == 0) {
           compact_n = le(p + o, 4);
           compact = p + o + 4;
+          need(o + 4, compact_n, m.size, "compact data");
         } else if (layout == 1) {
           csize = 1;
           for (uint64_t c : chunk) csize *= c;
@@ -454,33 +514,47 @@ Dataset File::dataset(const std::string& path) const {
   }
   if (!have_space || !have_type || !have_layout) fail(path + " is not a dataset");
   const size_t es = d.type.size;
-  const uint64_t total = d.count() * es;
+  uint64_t total = es;
+  for (uint64_t dim : d.shape) {
+    if (dim != 0 && total > kMaxBytes / dim) fail(path + " is too large to read");
+    total *= dim;
+  }
+  const uint64_t room = std::max<uint64_t>(buf_.size() * kMaxExpansion, 1u << 20);
+  if (total > room) fail(path + " is larger than its file can hold");
+  if (layout == 1 && !undefined(addr, so_)) ptr(addr, total);  // before any allocation
   d.bytes.assign(total, 0);
   if (layout == 0) {
     if (compact_n < total) fail(path + ": short compact data");
-    std::memcpy(d.bytes.data(), compact, total);
+    if (total) std::memcpy(d.bytes.data(), compact, total);
   } else if (layout == 1) {
-    if (!undefined(addr, so_)) {
+    if (!undefined(addr, so_) && total) {
       if (csize < total) fail(path + ": short contiguous data");
       std::memcpy(d.bytes.data(), ptr(addr, total), total);
     }
   } else if (layout == 2) {
     const size_t rank = d.shape.size();
-    if (chunk.size() != rank + 1) fail(path + ": chunk rank");
+    if (rank == 0 || chunk.size() != rank + 1) fail(path + ": chunk rank");
     uint64_t celems = 1;
-    for (size_t k = 0; k < rank; ++k) celems *= chunk[k];
+    for (size_t k = 0; k < rank; ++k) {
+      if (chunk[k] != 0 && celems > kMaxBytes / chunk[k]) fail(path + ": chunk too large");
+      celems *= chunk[k];
+    }
+    if (celems != 0 && es > room / celems) fail(path + ": chunk larger than its file can hold");
     const uint64_t cbytes = celems * es;
     // Walk the chunk B-tree; decode and place every chunk.
     std::vector<std::pair<uint64_t, int>> stack;  // (node, depth)
     if (!undefined(addr, so_)) stack.push_back({addr, 0});
     const size_t key = 8 + 8 * (rank + 1);
+    uint64_t visited = 0;
     while (!stack.empty()) {
+      if (++visited > kMaxNodes) fail(path + ": chunk B-tree too large");
       const auto [node, depth] = stack.back();
       stack.pop_back();
       if (depth > kMaxDepth) fail(path + ": chunk B-tree too deep");
       const uint8_t* t = ptr(node, 8 + 2 * (size_t)so_);
       if (memcmp(t, "TREE", 4) || t[4] != 1) fail(path + ": bad chunk B-tree node");
       const int level = t[5], used = (int)le(t + 6, 2);
+      spend(1 + used);
       const uint8_t* k = ptr(node + 8 + 2 * (size_t)so_, (key + so_) * used + key);
       for (int i = 0; i < used; ++i) {
         const uint8_t* kk = k + i * (key + so_);
@@ -493,6 +567,7 @@ Dataset File::dataset(const std::string& path) const {
         std::vector<uint64_t> off(rank);
         for (size_t r = 0; r < rank; ++r) off[r] = le(kk + 8 + 8 * r, 8);
         const uint8_t* src = ptr(child, stored);
+        spend(1 + (cbytes + stored) / 65536);
         std::vector<uint8_t> c(src, src + stored);
         for (int fi = (int)filters.size() - 1; fi >= 0; --fi) {
           if (mask & (1u << fi)) continue;
@@ -500,7 +575,10 @@ Dataset File::dataset(const std::string& path) const {
           if (f.id == 1) {
             c = inflate_all(c, cbytes);
           } else if (f.id == 2) {
-            c = unshuffle(c, f.values.empty() ? es : f.values[0]);
+            // the shuffle's element size is the datatype's (HDF5 stores it as client data)
+            if (!f.values.empty() && f.values[0] != es)
+              fail(path + ": shuffle element size differs from the datatype's");
+            c = unshuffle(c, es);
           } else if (f.id == 3) {
             if (c.size() < 4) fail(path + ": short Fletcher-32 chunk");
             c.resize(c.size() - 4);

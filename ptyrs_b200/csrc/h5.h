@@ -61,6 +61,10 @@ class File {
   std::vector<uint8_t> buf_;
   int so_ = 8, sl_ = 8;  // sizes of offsets and lengths
   uint64_t base_ = 0, root_ = 0;
+  // Work done by the current public call (header blocks, B-tree entries, decoded chunk
+  // kilobytes), bounded so that a damaged file's cycles end with an error.
+  mutable uint64_t work_ = 0;
+  void spend(uint64_t units) const;
 
   struct Message {
     uint16_t type;

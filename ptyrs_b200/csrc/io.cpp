@@ -41,9 +41,18 @@ uint64_t le(const uint8_t* p, int n, bool big) {
   return v;
 }
 
-// Element i of a dataset of scalars as double (integers, floats, one-byte enumerations).
+// Element i of a dataset of scalars as double (integers of 1, 2, 4 or 8 bytes, floats of 4 or 8,
+// enumerations over such integers); any other element size is refused.
 double scalar_at(const Type& t, const uint8_t* p) {
-  if (t.cls == Type::kEnum) return scalar_at(*t.base, p);
+  if (t.cls == Type::kEnum) {
+    if (!t.base || t.base->cls != Type::kFixed || t.base->size > t.size)
+      throw std::runtime_error("an enumeration of an unsupported base type");
+    return scalar_at(*t.base, p);
+  }
+  const bool sized = t.size == 1 || t.size == 2 || t.size == 4 || t.size == 8;
+  if (!sized || (t.cls == Type::kFloat && t.size < 4))
+    throw std::runtime_error("a dataset of an unsupported element size " +
+                             std::to_string(t.size));
   if (t.cls == Type::kFixed) {
     const uint64_t u = le(p, (int)t.size, t.big_endian);
     if (!t.is_signed) return (double)u;
@@ -87,6 +96,9 @@ std::vector<double> as_c128(const Dataset& d, const std::string& path) {
   if (t.cls != Type::kCompound || t.members.size() != 2 ||
       t.members[0].type->cls != Type::kFloat || t.members[1].type->cls != Type::kFloat)
     throw std::runtime_error(path + " is not complex64 or complex128");
+  for (const auto& m : t.members)
+    if ((uint64_t)m.offset + m.type->size > t.size)
+      throw std::runtime_error(path + ": a member lies outside its element");
   std::vector<double> out(2 * d.count());
   for (size_t i = 0; i < d.count(); ++i)
     for (int k = 0; k < 2; ++k)

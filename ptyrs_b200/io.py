@@ -10,7 +10,8 @@ from .engine import STATUS, PtybError, Scan
 
 
 def _error(rc, lib):
-    return PtybError(STATUS.get(rc, rc), lib.ptyb_io_last_error().decode())
+    # the reason may quote names out of a damaged file: undecodable bytes are replaced
+    return PtybError(STATUS.get(rc, rc), lib.ptyb_io_last_error().decode(errors="replace"))
 
 
 def read_cxi(path):

@@ -57,3 +57,40 @@ def test_refuses_what_it_cannot_read(tmp_path):
     cut.write_bytes(open(os.path.join(GOLDEN, "pynx_small.cxi"), "rb").read()[:4096])
     with pytest.raises(PtybError):
         read_cxi(cut)
+
+
+FUZZ = r"""
+import sys
+import numpy as np
+from ptyrs_b200 import PtybError
+from ptyrs_b200.io import read_cxi, read_ptyr
+src, out, seed, n = sys.argv[1], sys.argv[2], int(sys.argv[3]), int(sys.argv[4])
+reader = read_ptyr if src.endswith(".ptyr") else read_cxi
+blob = open(src, "rb").read()
+rng = np.random.default_rng(seed)
+for it in range(n):
+    b = bytearray(blob)
+    if it % 3 == 0:
+        b = b[: rng.integers(8, len(b))]
+    for _ in range(rng.integers(1, 12)):
+        b[rng.integers(0, len(b))] = rng.integers(0, 256)
+    open(out, "wb").write(bytes(b))
+    try:
+        reader(out)
+    except PtybError:
+        pass
+"""
+
+
+@pytest.mark.parametrize("name", ["pynx_small.cxi", "ptypy_small_double.ptyr"])
+def test_damaged_files_are_refused_not_crashed(tmp_path, name):
+    """Seeded truncations and byte flips of the fixtures, read in a child process: each read
+    returns its scan or raises PtybError, and the process ends normally within the time limit
+    (a fault, an unbounded allocation or a cycle in the file's structure would fail here)."""
+    import subprocess
+    import sys
+    env = dict(os.environ, PYTHONPATH=os.path.dirname(GOLDEN.rstrip("/")).rsplit("/", 1)[0])
+    r = subprocess.run([sys.executable, "-c", FUZZ, os.path.join(GOLDEN, name),
+                        str(tmp_path / "damaged"), "7", "400"], env=env, timeout=300,
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
