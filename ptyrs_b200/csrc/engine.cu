@@ -716,9 +716,61 @@ void zero_phase_ramp(ptyb_handle* h) {
 }
 
 // PyNX ScaleObjProbe(absolute=True) without background (engine/ptycho.rs:577-591).
+// Per frame, Σ_pixels Σ_modes |P_m·O_window|² in double (one block per frame, the modes'
+// probes shared or, with `waves`, the frame's own moved planes): by Parseval the photons of the
+// model's detector fields, Σ|Ψ|² under the unitary transform (|q| = 1).
+__global__ void __launch_bounds__(256) exit_power_kernel(const float2* object,
+                                                         const float2* probe, size_t stride,
+                                                         const int2* corners, int nxo, int K,
+                                                         int N, double* out) {
+  __shared__ double part[8];
+  const int f = blockIdx.x;
+  const int2 c = corners[f];
+  const float2* p = probe + (size_t)f * stride;
+  double s = 0.0;
+  for (int pix = threadIdx.x; pix < N * N; pix += 256) {
+    const int y = pix / N, x = pix % N;
+    const float2 o = object[(size_t)(c.x + y) * nxo + c.y + x];
+    const float o2 = o.x * o.x + o.y * o.y;
+    float p2 = 0.f;
+    for (int m = 0; m < K; ++m) {
+      const float2 v = p[(size_t)m * N * N + pix];
+      p2 += v.x * v.x + v.y * v.y;
+    }
+    s += (double)p2 * o2;
+  }
+  s = warp_sum(s);
+  if (threadIdx.x % 32 == 0) part[threadIdx.x / 32] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < 8; ++w) t += part[w];
+    out[f] = t;
+  }
+}
+
+// The opening rescale of ML (engine/ptycho.rs:577-591): object and probe scaled so that the
+// model holds the data's photons, from the LLK pass's Σ over the unmasked pixels of |Ψ|². With
+// no pixel masked anywhere that sum is every pixel's, which Parseval gives in the exit plane
+// without a transform (exit_power_kernel); otherwise the LLK pass takes it.
 void scale_obj_probe(ptyb_handle* h, float2* waves) {
-  const ptyb_llk l = llk_pass(h, waves);
-  split_scale(h, std::sqrt(h->obs_total / l.nb_photons_calc), waves);
+  double calc = 0.0;
+  if (h->nslice == 1 && h->nobj == 1 && h->nb_obs == (double)h->P * h->N * h->N) {
+    const size_t np = (size_t)h->K * h->N * h->N;
+    timed(h, kKMisc, [&] {
+      exit_power_kernel<<<h->P, 256, 0, h->stream>>>(h->object, waves ? waves : h->probe,
+                                                     waves ? np : 0, h->corners, h->nxo, h->K,
+                                                     h->N, h->llk);
+    }, h->P);
+    launched(h, "exit power");
+    std::vector<double> v(h->P);
+    check(h, copy_sync(h, v.data(), h->llk, h->P * sizeof(double), cudaMemcpyDeviceToHost),
+          "exit power");
+    for (double x : v) calc += x;
+  } else {
+    calc = llk_pass(h, waves).nb_photons_calc;
+  }
+  split_scale(h, std::sqrt(h->obs_total / calc), waves);
 }
 
 // Scales O·P by s and balances Σ|O| and Σ|P| (engine/ptycho.rs:593-603): P *= √(Σ|O|/Σ|P|·s),

@@ -287,3 +287,33 @@ def test_rpie_with_positions(case, refine):
             assert np.abs((d - d0) - moved).max() <= RUN_TOL * 10 * np.abs(moved).max()
         else:
             assert np.array_equal(d, d0)
+
+
+@pytest.mark.parametrize("offsets", [False, True], ids=["shared", "moved"])
+def test_ml_opening_rescale_without_masked_pixels(offsets):
+    """With no pixel masked, ML's opening rescale takes the model's photons in the exit plane
+    (Parseval: Σ|P·O|² over each window, no transform) instead of from an LLK pass: against the
+    oracle, whose rescale sums |Ψ|² in the detector plane, the arrays, the LLK records and (with
+    moved probes) the offsets after four cycles."""
+    s = far_field(128, 2, 24, 320, seed=9)
+    assert (s["counts"] >= 0).all()
+    nframe = len(s["counts"])
+    d0 = np.random.default_rng(8).uniform(-0.6, 0.6, (nframe, 2))
+    start = dict(s, object=s["truth"] * 0.9 * np.exp(0.1j))
+    cpu = oracle_state(start)
+    if offsets:
+        cpu.set_positions(d0, refine=True)
+    cpu.ml(4, update_probe=True, calc_llk=1, zero_phase_ramp=False)
+    with gpu_of(start) as g:
+        if offsets:
+            g.set_positions(d0, refine=True)
+        g.ml(4, update_probe=True, calc_llk=1, zero_phase_ramp=False)
+        assert rel_l2(g.object(), cpu.object) < RUN_TOL
+        assert rel_l2(g.probe(), cpu.probe) < RUN_TOL
+        h = g.history()
+        want = np.array([r["poisson"] for r in cpu.history])
+        assert np.abs(h["poisson"] - want).max() <= ML_LLK_TOL * np.abs(want).max()
+        if offsets:
+            moved = cpu.offsets - d0
+            assert np.abs(moved).max() > 0
+            assert np.abs((g.positions() - d0) - moved).max() <= RUN_TOL * 10 * np.abs(moved).max()
