@@ -2,6 +2,7 @@
 oracle over whole scans, at checkpoints of one run (test infrastructure, not the product).
 
     python tests/at_size.py oracle CONFIG DIR   # host only: the oracle's run and checkpoints
+    python tests/at_size.py meta CONFIG DIR     # host only: the inputs' digest and the mask alone
     python tests/at_size.py gpu CONFIG DIR OUT  # the CUDA path from the same inputs, compared
     python tests/at_size.py sensitivity CONFIG DIR OUT [EPS]  # the oracle from a start
                                                 # perturbed by EPS (1e-7), compared the same way
@@ -15,8 +16,8 @@ are the benchmark's seeded scans (`sim.make_scan`; ml256's counts made with torc
 so both phases read the same counts, checked by a digest). The oracle phase runs one call of
 the longest run and keeps a snapshot after each checkpoint's iteration; the GPU phase runs
 each checkpoint as one call of that many iterations on a fresh state (the calls are the
-reference's: a k-iteration call is the first k iterations of a longer one) and writes, per
-checkpoint, the object's and probe's relative L2 error against the oracle's, the object NRMSE
+reference's: a k-iteration call is the first k iterations of a longer one) and writes, for
+each checkpoint the oracle's run has reached, the object's and probe's relative L2 error against the oracle's, the object NRMSE
 with the global phase and a phase ramp removed (scale kept) over the illuminated pixels, and
 for ml256 the largest difference of the refined offsets. The sensitivity phase measures how far
 the float64 run itself moves when its start object is multiplied by (1 + EPS·ξ), ξ seeded
@@ -54,6 +55,24 @@ def optics_of(s):
                                 [s["n"], s["n"]])
 
 
+def write_meta(name, out, s, digest, mask, times):
+    os.makedirs(out, exist_ok=True)
+    np.savez(os.path.join(out, f"{name}_mask.npz"), mask=np.packbits(mask), shape=mask.shape)
+    with open(os.path.join(out, f"{name}_meta.json"), "w") as f:
+        json.dump({"config": name, "digest": digest, "seconds": times,
+                   "threads": os.cpu_count()}, f)
+
+
+def run_meta(name, out):
+    """The digest and the illuminated-pixel mask of a configuration's inputs, without the run."""
+    from oracle import ops
+    from oracle.ptycho import Ptycho
+    s, digest = inputs(CONFIGS[name])
+    p = Ptycho(s["counts"], s["y"], s["x"], optics_of(s), s["object"], s["probe"])
+    illum = ops.illumination(p.addr.views, p.object.shape, p.probe)
+    write_meta(name, out, s, digest, illum >= 1e-3 * illum.max(), {})
+
+
 def run_oracle(name, out, eps=0.0, save_as=None):
     """The oracle's run of the longest checkpoint, a snapshot at each checkpoint (`save_as(k,
     obj, probe, offsets)` instead of the files when given); the start object perturbed by
@@ -76,6 +95,8 @@ def run_oracle(name, out, eps=0.0, save_as=None):
     mask = illum >= 1e-3 * illum.max()
     last = max(cfg["checkpoints"])
     times = {}
+    if save_as is None:
+        write_meta(name, out, s, digest, mask, times)
 
     def save(k, obj, probe, offsets=None):
         times[k] = time.perf_counter() - t0
@@ -84,6 +105,7 @@ def run_oracle(name, out, eps=0.0, save_as=None):
             return
         np.savez(os.path.join(out, f"{name}_{k}.npz"), object=obj.astype(np.complex64),
                  probe=probe, offsets=np.zeros(0) if offsets is None else offsets)
+        write_meta(name, out, s, digest, mask, times)
         print(f"{name}: checkpoint {k} at {times[k]:.0f} s", flush=True)
 
     if cfg["algorithm"] == "rpie":
@@ -107,12 +129,6 @@ def run_oracle(name, out, eps=0.0, save_as=None):
 
         p.ml(last, update_object=True, update_probe=True, calc_llk=0, zero_phase_ramp=False,
              after_cycle=after)
-    if save_as is not None:
-        return
-    np.savez(os.path.join(out, f"{name}_mask.npz"), mask=np.packbits(mask), shape=mask.shape)
-    with open(os.path.join(out, f"{name}_meta.json"), "w") as f:
-        json.dump({"config": name, "digest": digest, "seconds": times,
-                   "threads": os.cpu_count()}, f)
 
 
 def compare(name, ref, k, obj, probe, offsets):
@@ -153,7 +169,8 @@ def run_gpu(name, ref, out):
         raise RuntimeError("the inputs differ from the oracle run's")
     scan = Scan(s["counts"], s["y"], s["x"], s["wavelength"], s["distance"], s["detector_pixel"])
     rows = []
-    for k in cfg["checkpoints"]:
+    reached = [k for k in cfg["checkpoints"] if os.path.exists(os.path.join(ref, f"{name}_{k}.npz"))]
+    for k in reached:
         with GpuPtycho(scan, s["object"], s["probe"]) as g:
             if cfg["algorithm"] == "rpie":
                 g.rpie(k, batch_size=cfg["batch"], obj_alpha=0.1, probe_alpha=0.1, seed=7)
@@ -172,17 +189,23 @@ def run_gpu(name, ref, out):
 def run_sensitivity(name, ref, out, eps):
     """The float64 oracle from the perturbed start, compared with its own unperturbed run."""
     rows = []
-    run_oracle(name, ref, eps=eps,
-               save_as=lambda k, o, p, d: rows.append(compare(name, ref, k, o, p, d)))
-    report(name, ref, out, rows, path=f"float64 oracle, start perturbed by {eps:g}")
+    path = f"float64 oracle, start perturbed by {eps:g}"
+
+    def save_as(k, o, p, d):
+        rows.append(compare(name, ref, k, o, p, d))
+        report(name, ref, out, rows, path=path)  # kept current, so a run cut short still reports
+
+    run_oracle(name, ref, eps=eps, save_as=save_as)
 
 
 if __name__ == "__main__":
-    if (len(sys.argv) < 4 or sys.argv[1] not in ("oracle", "gpu", "sensitivity")
+    if (len(sys.argv) < 4 or sys.argv[1] not in ("oracle", "meta", "gpu", "sensitivity")
             or sys.argv[2] not in CONFIGS):
         raise SystemExit(__doc__)
     if sys.argv[1] == "oracle":
         run_oracle(sys.argv[2], sys.argv[3])
+    elif sys.argv[1] == "meta":
+        run_meta(sys.argv[2], sys.argv[3])
     elif sys.argv[1] == "gpu":
         run_gpu(sys.argv[2], sys.argv[3], sys.argv[4])
     else:
