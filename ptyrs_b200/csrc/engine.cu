@@ -727,10 +727,13 @@ __global__ void __launch_bounds__(256) exit_power_kernel(const float2* object,
   const int f = blockIdx.x;
   const int2 c = corners[f];
   const float2* p = probe + (size_t)f * stride;
+  const float2* ow = object + (size_t)c.x * nxo + c.y;
   double s = 0.0;
+  // rows and columns carried along the 256-pixel strides, no division per pixel
+  int y = threadIdx.x / N, x = threadIdx.x % N;
+#pragma unroll 4
   for (int pix = threadIdx.x; pix < N * N; pix += 256) {
-    const int y = pix / N, x = pix % N;
-    const float2 o = object[(size_t)(c.x + y) * nxo + c.y + x];
+    const float2 o = ow[(size_t)y * nxo + x];
     const float o2 = o.x * o.x + o.y * o.y;
     float p2 = 0.f;
     for (int m = 0; m < K; ++m) {
@@ -738,6 +741,12 @@ __global__ void __launch_bounds__(256) exit_power_kernel(const float2* object,
       p2 += v.x * v.x + v.y * v.y;
     }
     s += (double)p2 * o2;
+    y += 256 / N;
+    x += 256 % N;
+    if (x >= N) {
+      x -= N;
+      ++y;
+    }
   }
   s = warp_sum(s);
   if (threadIdx.x % 32 == 0) part[threadIdx.x / 32] = s;

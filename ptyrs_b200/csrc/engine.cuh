@@ -146,13 +146,14 @@ struct ptyb_handle {
   float2* opr_u = nullptr;       // [k][N][N]
   double* opr_w = nullptr;       // [P][k]
   double* opr_c = nullptr;       // [P]
-  float* opr_vv = nullptr;       // [slots][N][N]
   float2* opr_r = nullptr;       // [slots][N][N]
   float2* opr_moved = nullptr;   // [slots][K][N][N] frame probe directions moved back
   float2* opr_e = nullptr;       // [N][N]
-  double* opr_sums = nullptr;    // [slots][3]
+  double* opr_sums = nullptr;    // [slots][parts][≤ 4] per-frame partials, then [slots][2]
+                                 // the Gram–Schmidt sums
   double* opr_p = nullptr;       // [slots]
   double* opr_scal = nullptr;    // [4]
+  unsigned* opr_count = nullptr; // the per-frame passes' count of finished blocks
   // Their probe step under the position model: the residual's back-projection g, the step,
   // g's spectrum summed over frames with its compensation, each frame's ‖A·step‖² per mode
   // and the modes' slope and regulariser sums.

@@ -2,6 +2,8 @@
 // per batch the frame passes with the far-field step, the object and probe directions, the
 // FP64 step sizes and the updates; pty-chi's multislice object; the OPR probe variation
 // (engine/opr.rs) and pty-chi's position step.
+#include <utility>
+
 #include "engine.cuh"
 
 using namespace ptyb;
@@ -201,9 +203,8 @@ void lsqml_batch_slices(ptyb_handle* h, const ptyb_lsqml_params& p, const int* f
 void ensure_opr(ptyb_handle* h) {
   const size_t plane = (size_t)h->N * h->N;
   if (h->opr_slots < h->slots) {
-    h->opr_vv = alloc<float>(h, (size_t)h->slots * plane);
     h->opr_r = alloc<float2>(h, (size_t)h->slots * plane);
-    h->opr_sums = alloc<double>(h, (size_t)h->slots * 3);
+    h->opr_sums = alloc<double>(h, (size_t)h->slots * (4 * kOprParts + 2));
     h->opr_p = alloc<double>(h, h->slots);
     h->wave = alloc<float2>(h, (size_t)h->slots * h->K * plane);
     h->opr_moved = alloc<float2>(h, (size_t)h->slots * h->K * plane);
@@ -212,6 +213,8 @@ void ensure_opr(ptyb_handle* h) {
   if (!h->opr_e) {
     h->opr_e = alloc<float2>(h, plane);
     h->opr_scal = alloc<double>(h, 4);
+    h->opr_count = alloc<unsigned>(h, 1);
+    check(h, cudaMemsetAsync(h->opr_count, 0, sizeof(unsigned), h->stream), "memset");
   }
   if (!h->wave_all) h->wave_all = alloc<float2>(h, (size_t)h->P * h->K * plane);
 }
@@ -246,84 +249,62 @@ const float2* frame_probes(ptyb_handle* h, const int* frames, int nslot) {
 // The OPR step of the batch (engine/opr.rs:122-224) from its frame probe directions, mode-0
 // plane of each slot of h->field (the main-mode weights and the weights) and of `moved` (the
 // same taken back through the frames' moves, h->field without offsets: the residues), and the
-// probe's mode 0 on entry.
+// probe's mode 0 on entry. Two launches for the batch and four per eigenmode: each per-frame
+// pass (kOprParts blocks per frame) finishes its batch-wide step (coefficients, weights) in its
+// last block, and the Gram–Schmidt step of the residues against an eigenmode runs inside the
+// next eigenmode's dots.
 void opr_step(ptyb_handle* h, const int* frames, int count, const float2* moved) {
   const int plane = h->N * h->N, k = h->opr_k;
   const size_t dstride = (size_t)h->K * plane;
-  const unsigned pb = (unsigned)((plane + 255) / 256), pb32 = (unsigned)((plane + 31) / 32);
-  timed(h, kKOprStep, [&] {
-    window_power_kernel<<<dim3(pb, count), 256, 0, h->stream>>>(h->object, frames, h->corners,
-                                                               h->nxo, h->N, h->opr_vv);
-  }, count);
-  launched(h, "opr window power");
+  const unsigned pb32 = (unsigned)((plane + 31) / 32);
+  double* part = h->opr_sums;                                  // [count][parts][≤ 4]
+  double* proj = h->opr_sums + (size_t)count * 4 * kOprParts;  // [count][2]
+  double* uu = h->opr_scal;
+  const dim3 per_frame(count, kOprParts);
+  // the batch's frames counted once, on its first launch
+  int64_t frames_left = count;
+  auto units = [&] { return std::exchange(frames_left, 0); };
   if (h->opr_has_c && h->opr_refine_c) {
     timed(h, kKOprStep, [&] {
-      opr_frame_sums_kernel<<<count, 256, 0, h->stream>>>(h->probe, h->field, dstride, h->opr_vv,
-                                                          plane, h->opr_sums);
-    });
-    launched(h, "opr intensity sums");
-    timed(h, kKOprStep, [&] {
-      opr_intensity_kernel<<<(count + 255) / 256, 256, 0, h->stream>>>(h->opr_sums, frames, count,
-                                                                        h->opr_c);
-    });
+      opr_intensity_kernel<<<per_frame, 256, 0, h->stream>>>(h->probe, h->field, dstride,
+                                                             h->object, frames, h->corners,
+                                                             h->nxo, h->N, h->opr_count, part,
+                                                             h->opr_c);
+    }, units());
     launched(h, "opr intensity");
   }
   if (k == 0 || count < 2) return;
   timed(h, kKOprStep, [&] {
     opr_residue_kernel<<<pb32, 256, 0, h->stream>>>(moved, dstride, count, plane, h->opr_r);
-  });
+  }, units());
   launched(h, "opr residues");
   const double a_u = std::min(0.1, (double)count / h->P);
   for (int i = 0; i < k; ++i) {
     float2* u = h->opr_u + (size_t)i * plane;
+    const float2* prev = i ? u - plane : nullptr;
     timed(h, kKOprStep, [&] {
-      opr_frame_sums_kernel<<<count, 256, 0, h->stream>>>(u, h->opr_r, plane, nullptr, plane,
-                                                          h->opr_sums);
+      opr_dots_kernel<<<per_frame, 256, 0, h->stream>>>(u, h->opr_r, h->N, prev, proj, uu,
+                                                        h->opr_w, frames, k, i, h->opr_count,
+                                                        part, h->opr_p);
     });
-    launched(h, "opr dots");
-    timed(h, kKOprStep, [&] {
-      opr_coef_kernel<<<1, 256, 0, h->stream>>>(h->opr_sums, h->opr_w, frames, k, i, count,
-                                                (double)plane, h->opr_p);
-    });
-    launched(h, "opr coefficients");
+    launched(h, i ? "opr orthogonalisation and dots" : "opr dots");
     timed(h, kKOprStep, [&] {
       opr_e_kernel<<<pb32, 256, 0, h->stream>>>(h->opr_r, h->opr_p, count, plane, h->opr_e);
     });
     launched(h, "opr e");
-    timed(h, kKOprStep, [&] { opr_norm2_kernel<<<1, 1024, 0, h->stream>>>(h->opr_e, plane, h->opr_scal); });
-    launched(h, "opr norm");
     timed(h, kKOprStep, [&] {
-      opr_u_step_kernel<<<pb, 256, 0, h->stream>>>(u, h->opr_e, h->opr_scal, a_u, plane);
+      opr_u_kernel<<<1, 1024, 0, h->stream>>>(u, h->opr_e, a_u, plane, uu);
     });
     launched(h, "opr eigenmode step");
-    timed(h, kKOprStep, [&] { opr_norm2_kernel<<<1, 1024, 0, h->stream>>>(u, plane, h->opr_scal + 1); });
-    launched(h, "opr norm");
-    timed(h, kKOprStep, [&] { opr_u_scale_kernel<<<pb, 256, 0, h->stream>>>(u, h->opr_scal + 1, plane); });
-    launched(h, "opr eigenmode scale");
-    if (h->opr_refine_w) {
+    const bool next = i + 1 < k;
+    if (h->opr_refine_w || next) {
       timed(h, kKOprStep, [&] {
-        opr_frame_sums_kernel<<<count, 256, 0, h->stream>>>(u, h->field, dstride, h->opr_vv,
-                                                            plane, h->opr_sums);
+        opr_weight_proj_kernel<<<per_frame, 256, 0, h->stream>>>(
+            u, h->opr_refine_w ? h->field : nullptr, dstride, next ? h->opr_r : nullptr,
+            h->object, frames, h->corners, h->nxo, h->N, k, i, h->opr_count, part, proj,
+            h->opr_w);
       });
-      launched(h, "opr weight sums");
-      timed(h, kKOprStep, [&] {
-        opr_weights_kernel<<<1, 256, 0, h->stream>>>(h->opr_sums, frames, count, k, i, h->opr_w);
-      });
-      launched(h, "opr weights");
-    }
-    if (i + 1 < k) {
-      timed(h, kKOprStep, [&] { opr_norm2_kernel<<<1, 1024, 0, h->stream>>>(u, plane, h->opr_scal + 2); });
-      launched(h, "opr norm");
-      timed(h, kKOprStep, [&] {
-        opr_frame_sums_kernel<<<count, 256, 0, h->stream>>>(u, h->opr_r, plane, nullptr, plane,
-                                                            h->opr_sums);
-      });
-      launched(h, "opr projections");
-      timed(h, kKOprStep, [&] {
-        opr_gs_kernel<<<dim3(pb, count), 256, 0, h->stream>>>(h->opr_r, u, h->opr_sums, h->opr_scal + 2, count,
-                                                 plane);
-      });
-      launched(h, "opr orthogonalisation");
+      launched(h, h->opr_refine_w ? "opr weights" : "opr projections");
     }
   }
 }

@@ -24,70 +24,99 @@ static __global__ void opr_planes_kernel(const float2* probe, const float2* u, c
   }
 }
 
-// vv[slot] = |O_window|² per pixel.
-static __global__ void window_power_kernel(const float2* object, const int* frames, const int2* corners,
-                                    int nxo, int N, float* vv) {
-  const int slot = blockIdx.y;
-  const int2 c = corners[frames[slot]];
-  for (int pix = blockIdx.x * blockDim.x + threadIdx.x; pix < N * N;
-       pix += gridDim.x * blockDim.x) {
-    const int y = pix / N, x = pix % N;
-    vv[(size_t)slot * N * N + pix] = cnorm2(object[(size_t)(c.x + y) * nxo + c.y + x]);
-  }
-}
-
-// Per slot (one block each): s0 = Σ |a|²·vv, s1 + i·s2 = Σ conj(a)·x, over the plane;
-// `a` a shared plane, `x` the slot's plane at x + slot·xstride.
-static __global__ void __launch_bounds__(256) opr_frame_sums_kernel(const float2* a, const float2* x,
-                                                             size_t xstride, const float* vv,
-                                                             int plane, double* out) {
-  __shared__ double red[3][8];
-  const int slot = blockIdx.x;
-  const float2* xs = x + (size_t)slot * xstride;
-  const float* vs = vv ? vv + (size_t)slot * plane : nullptr;
-  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-  for (int pix = threadIdx.x; pix < plane; pix += 256) {
-    const float2 av = a[pix], xv = xs[pix];
-    if (vs) s0 += (double)cnorm2(av) * vs[pix];
-    s1 += (double)av.x * xv.x + (double)av.y * xv.y;
-    s2 += (double)av.x * xv.y - (double)av.y * xv.x;
-  }
-  s0 = warp_sum(s0);
-  s1 = warp_sum(s1);
-  s2 = warp_sum(s2);
-  if (threadIdx.x % 32 == 0) {
-    red[0][threadIdx.x / 32] = s0;
-    red[1][threadIdx.x / 32] = s1;
-    red[2][threadIdx.x / 32] = s2;
-  }
+// Sums of up to four doubles over a block of 256 threads in a fixed order (the lanes' tree,
+// then the eight warps in order); every thread gets the totals.
+template <int M>
+PTYB_D void block_sums256(double (&v)[M]) {
+  __shared__ double red[M][8];
+#pragma unroll
+  for (int j = 0; j < M; ++j) v[j] = warp_sum(v[j]);
   __syncthreads();
-  if (threadIdx.x < 3) {
+  if (threadIdx.x % 32 == 0)
+#pragma unroll
+    for (int j = 0; j < M; ++j) red[j][threadIdx.x / 32] = v[j];
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
     double t = 0.0;
-    for (int w = 0; w < 8; ++w) t += red[threadIdx.x][w];
-    out[(size_t)slot * 3 + threadIdx.x] = t;
+    for (int w = 0; w < 8; ++w) t += red[j][w];
+    v[j] = t;
   }
 }
 
-// Σ |x|² over n elements, one block, fixed order.
-static __global__ void __launch_bounds__(1024) opr_norm2_kernel(const float2* x, int n, double* out) {
-  __shared__ double red[32];
-  double s = 0.0;
-  for (int i = threadIdx.x; i < n; i += 1024) s += (double)cnorm2(x[i]);
-  s = warp_sum(s);
-  if (threadIdx.x % 32 == 0) red[threadIdx.x / 32] = s;
-  __syncthreads();
+// Whether this block is the grid's last to finish: each block's thread 0 has written its
+// results, fences them and counts the block; the block that counts last sees every result and
+// resets the counter for the next launch. Nothing waits, so no block depends on another's
+// progress.
+PTYB_D bool last_block(unsigned* counter) {
+  __shared__ bool last;
   if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (int w = 0; w < 32; ++w) t += red[w];
-    *out = t;
+    __threadfence();
+    last = atomicAdd(counter, 1u) == gridDim.x * gridDim.y - 1;
+    if (last) *counter = 0;
   }
+  __syncthreads();
+  if (last) __threadfence();
+  return last;
 }
 
-// The main mode's weights (engine/opr.rs:162-168): c_f += 0.1·Re<P_0, d_b> / Σ|P_0|²·vv_b.
-static __global__ void opr_intensity_kernel(const double* sums, const int* frames, int count,
-                                     double* c) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b < count) c[frames[b]] += 0.1 * sums[b * 3 + 1] / sums[b * 3];
+// The per-frame sums run in kOprParts blocks per slot b (blockIdx.x = b, blockIdx.y = part),
+// each over one contiguous span of the plane; the parts' partials are added in part order by
+// the grid's last block, which also takes the batch-wide step.
+constexpr int kOprParts = 4;
+
+// The pixels of a block's span, in strides of 256, with their row and column carried along.
+struct OprSpan {
+  int pix, end, y, x;
+  PTYB_D OprSpan(int plane, int N) {
+    const int span = (plane + kOprParts - 1) / kOprParts;
+    pix = (int)blockIdx.y * span + (int)threadIdx.x;
+    end = min(plane, ((int)blockIdx.y + 1) * span);
+    y = pix / N;
+    x = pix % N;
+  }
+  PTYB_D void next(int N) {
+    pix += 256;
+    y += 256 / N;
+    x += 256 % N;
+    if (x >= N) {
+      x -= N;
+      ++y;
+    }
+  }
+};
+
+// A slot's total of sum m over its parts, in part order.
+PTYB_D double opr_total(const double* part, int M, int b, int m) {
+  double t = 0.0;
+  for (int q = 0; q < kOprParts; ++q) t += __ldcg(part + ((size_t)b * kOprParts + q) * M + m);
+  return t;
+}
+
+// The main mode's weights (engine/opr.rs:162-168): per slot b,
+// c_f += 0.1·Re<P_0, d_b> / Σ|P_0|²·|O_b|², with |O_b|² taken from the frame's object window.
+static __global__ void __launch_bounds__(256) opr_intensity_kernel(
+    const float2* p0, const float2* d, size_t dstride, const float2* object, const int* frames,
+    const int2* corners, int nxo, int N, unsigned* counter, double* part, double* c) {
+  const int b = blockIdx.x, count = gridDim.x;
+  const int2 cr = corners[frames[b]];
+  const float2* db = d + (size_t)b * dstride;
+  const float2* ob = object + (size_t)cr.x * nxo + cr.y;
+  double s[2] = {0.0, 0.0};
+#pragma unroll 4
+  for (OprSpan it(N * N, N); it.pix < it.end; it.next(N)) {
+    const float2 pv = p0[it.pix], dv = db[it.pix];
+    s[0] += (double)cnorm2(pv) * cnorm2(ob[(size_t)it.y * nxo + it.x]);
+    s[1] += (double)pv.x * dv.x + (double)pv.y * dv.y;
+  }
+  block_sums256(s);
+  if (threadIdx.x == 0) {
+    part[((size_t)b * kOprParts + blockIdx.y) * 2] = s[0];
+    part[((size_t)b * kOprParts + blockIdx.y) * 2 + 1] = s[1];
+  }
+  if (!last_block(counter)) return;
+  for (int j = threadIdx.x; j < count; j += 256)
+    c[frames[j]] += 0.1 * opr_total(part, 2, j, 1) / opr_total(part, 2, j, 0);
 }
 
 // The per-pixel sums over a batch's frames run in blocks of 32 pixels × 8 frame groups: group g
@@ -131,7 +160,6 @@ static __global__ void __launch_bounds__(256) opr_residue_kernel(const float2* d
   }
 }
 
-// p_b = (Re<r_b, U>/n² + w_b) / Σ_b w_b², one block (engine/opr.rs:186-192).
 // Σ_b x_b in frame order by one block of 256 threads: each chunk of 256 terms loaded by all
 // threads at once, then added by thread 0 in order (the same bits as a serial loop).
 template <class F>
@@ -149,18 +177,47 @@ __device__ double ordered_frame_sum(int count, F term) {
   return s;
 }
 
-static __global__ void __launch_bounds__(256) opr_coef_kernel(const double* sums, const double* w,
-                                                       const int* frames, int k, int i,
-                                                       int count, double n, double* p) {
+// Per slot b for eigenmode U: with `prev` (the eigenmode before it) first the Gram–Schmidt
+// step of the residues against that one, r_b −= (Σ r_b·conj(U') / Σ|U'|²)·U'
+// (engine/opr.rs:213-219; `proj` [slot][2] the sums, `uu` Σ|U'|²), then Re Σ conj(U)·r_b; the
+// last block turns these dots into the coefficients p_b = (Re<r_b, U>/n² + w_b) / Σ_b w_b²
+// (engine/opr.rs:186-192), the sum over the batch in frame order.
+static __global__ void __launch_bounds__(256) opr_dots_kernel(
+    const float2* u, float2* r, int N, const float2* prev, const double* proj,
+    const double* uu, const double* w, const int* frames, int k, int i, unsigned* counter,
+    double* part, double* p) {
+  const int b = blockIdx.x, count = gridDim.x, plane = N * N;
+  float2* rb = r + (size_t)b * plane;
+  double cr = 0.0, ci = 0.0;
+  if (prev) {
+    cr = proj[b * 2] / *uu;
+    ci = proj[b * 2 + 1] / *uu;
+  }
+  double s[1] = {0.0};
+#pragma unroll 4
+  for (OprSpan it(plane, N); it.pix < it.end; it.next(N)) {
+    float2 v = rb[it.pix];
+    if (prev) {
+      const float2 q = prev[it.pix];
+      v = make_float2((float)(v.x - (cr * q.x - ci * q.y)), (float)(v.y - (cr * q.y + ci * q.x)));
+      rb[it.pix] = v;
+    }
+    const float2 uv = u[it.pix];
+    s[0] += (double)uv.x * v.x + (double)uv.y * v.y;
+  }
+  block_sums256(s);
+  if (threadIdx.x == 0) part[(size_t)b * kOprParts + blockIdx.y] = s[0];
+  if (!last_block(counter)) return;
   __shared__ double w2;
-  const double s = ordered_frame_sum(count, [&](int b) {
-    const double wb = w[(size_t)frames[b] * k + i];
-    return wb * wb;
+  const double t = ordered_frame_sum(count, [&](int j) {
+    const double wj = w[(size_t)frames[j] * k + i];
+    return wj * wj;
   });
-  if (threadIdx.x == 0) w2 = s;
+  if (threadIdx.x == 0) w2 = t;
   __syncthreads();
-  for (int b = threadIdx.x; b < count; b += blockDim.x)
-    p[b] = (sums[b * 3 + 1] / (n * n) + w[(size_t)frames[b] * k + i]) / w2;
+  const double n2 = (double)plane * plane;
+  for (int j = threadIdx.x; j < count; j += blockDim.x)
+    p[j] = (opr_total(part, 1, j, 0) / n2 + w[(size_t)frames[j] * k + i]) / w2;
 }
 
 // e = Σ_b r_b·p_b / count, in the frame groups above.
@@ -192,48 +249,91 @@ static __global__ void __launch_bounds__(256) opr_e_kernel(const float2* r, cons
   e[pix] = make_float2((float)(sr / count), (float)(si / count));
 }
 
-// u += (a_u·√n / mnorm(e))·e, mnorm(e) = √(Σ|e|²/n).
-static __global__ void opr_u_step_kernel(float2* u, const float2* e, const double* ne, double a_u,
-                                  int n) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double s = a_u * sqrt((double)n) / sqrt(*ne / n);
-  u[i] = make_float2((float)(u[i].x + s * e[i].x), (float)(u[i].y + s * e[i].y));
-}
-
-// u *= √n / mnorm(u).
-static __global__ void opr_u_scale_kernel(float2* u, const double* nu, int n) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const float s = (float)(sqrt((double)n) / sqrt(*nu / n));
-  u[i] = cscale(u[i], s);
-}
-
-// w_fi = w_bi + Re<U, d_b> / (Σ|U|²·vv_b + 0.1·mean_b Σ|U|²·vv_b), one block
-// (engine/opr.rs:200-212).
-static __global__ void __launch_bounds__(256) opr_weights_kernel(const double* sums, const int* frames,
-                                                          int count, int k, int i, double* w) {
-  __shared__ double reg;
-  const double s = ordered_frame_sum(count, [&](int b) { return sums[b * 3]; });
-  if (threadIdx.x == 0) reg = 0.1 * s / count;
+// Σ |x|² over n elements by one block of 1024 threads in a fixed order; every thread gets it.
+PTYB_D double norm2_1024(const float2* x, int n) {
+  __shared__ double red[32];
+  __shared__ double total;
+  double s = 0.0;
+  for (int j = threadIdx.x; j < n; j += 1024) s += (double)cnorm2(x[j]);
+  s = warp_sum(s);
   __syncthreads();
-  for (int b = threadIdx.x; b < count; b += blockDim.x) {
-    double& wb = w[(size_t)frames[b] * k + i];
-    wb = wb + sums[b * 3 + 1] / (sums[b * 3] + reg);
+  if (threadIdx.x % 32 == 0) red[threadIdx.x / 32] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < 32; ++w) t += red[w];
+    total = t;
   }
+  __syncthreads();
+  return total;
 }
 
-// r_b −= (Σ r_b·conj(U) / Σ|U|²)·U (engine/opr.rs:213-219), thread per pixel, frame b =
-// blockIdx.y.
-static __global__ void opr_gs_kernel(float2* r, const float2* u, const double* sums, const double* uu,
-                              int count, int plane) {
-  const int pix = blockIdx.x * blockDim.x + threadIdx.x;
-  const int b = blockIdx.y;
-  if (pix >= plane || b >= count) return;
-  const float2 uv = u[pix];
-  const double cr = sums[b * 3 + 1] / *uu, ci = sums[b * 3 + 2] / *uu;
-  float2& v = r[(size_t)b * plane + pix];
-  v = make_float2((float)(v.x - (cr * uv.x - ci * uv.y)), (float)(v.y - (cr * uv.y + ci * uv.x)));
+// The eigenmode's step, one block (engine/opr.rs:193-199): U += (a_u·√n / mnorm(e))·e, then
+// U *= √n / mnorm(U), mnorm(x) = √(Σ|x|²/n); Σ|U|² of the result into *uu for the
+// Gram–Schmidt step.
+static __global__ void __launch_bounds__(1024) opr_u_kernel(float2* u, const float2* e,
+                                                            double a_u, int n, double* uu) {
+  const double ne = norm2_1024(e, n);
+  const double s = a_u * sqrt((double)n) / sqrt(ne / n);
+  for (int j = threadIdx.x; j < n; j += 1024)
+    u[j] = make_float2((float)(u[j].x + s * e[j].x), (float)(u[j].y + s * e[j].y));
+  __syncthreads();
+  const double nu = norm2_1024(u, n);
+  const float su = (float)(sqrt((double)n) / sqrt(nu / n));
+  for (int j = threadIdx.x; j < n; j += 1024) u[j] = cscale(u[j], su);
+  __syncthreads();
+  const double t = norm2_1024(u, n);
+  if (threadIdx.x == 0) *uu = t;
+}
+
+// Per slot b, after the eigenmode's step: with `d` the weights' sums s0 = Σ|U|²·|O_b|² and
+// s1 = Re Σ conj(U)·d_b (|O_b|² from the frame's object window) and the last block's weight
+// step w_fi += s1_b / (s0_b + 0.1·mean_b s0_b) (engine/opr.rs:200-212, the mean over the batch
+// in frame order); with `r` the Gram–Schmidt sums Σ conj(U)·r_b into proj[b] for the next
+// eigenmode's residues.
+static __global__ void __launch_bounds__(256) opr_weight_proj_kernel(
+    const float2* u, const float2* d, size_t dstride, const float2* r, const float2* object,
+    const int* frames, const int2* corners, int nxo, int N, int k, int i, unsigned* counter,
+    double* part, double* proj, double* w) {
+  const int b = blockIdx.x, count = gridDim.x, plane = N * N;
+  const int2 cr = corners[frames[b]];
+  const float2* db = d ? d + (size_t)b * dstride : nullptr;
+  const float2* rb = r ? r + (size_t)b * plane : nullptr;
+  const float2* ob = object + (size_t)cr.x * nxo + cr.y;
+  double s[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 4
+  for (OprSpan it(plane, N); it.pix < it.end; it.next(N)) {
+    const float2 uv = u[it.pix];
+    if (db) {
+      const float2 dv = db[it.pix];
+      s[0] += (double)cnorm2(uv) * cnorm2(ob[(size_t)it.y * nxo + it.x]);
+      s[1] += (double)uv.x * dv.x + (double)uv.y * dv.y;
+    }
+    if (rb) {
+      const float2 rv = rb[it.pix];
+      s[2] += (double)uv.x * rv.x + (double)uv.y * rv.y;
+      s[3] += (double)uv.x * rv.y - (double)uv.y * rv.x;
+    }
+  }
+  block_sums256(s);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int m = 0; m < 4; ++m) part[((size_t)b * kOprParts + blockIdx.y) * 4 + m] = s[m];
+  if (!last_block(counter)) return;
+  if (r)
+    for (int j = threadIdx.x; j < count; j += blockDim.x) {
+      proj[j * 2] = opr_total(part, 4, j, 2);
+      proj[j * 2 + 1] = opr_total(part, 4, j, 3);
+    }
+  if (!d) return;
+  __shared__ double reg;
+  const double t = ordered_frame_sum(count, [&](int j) { return opr_total(part, 4, j, 0); });
+  if (threadIdx.x == 0) reg = 0.1 * t / count;
+  __syncthreads();
+  for (int j = threadIdx.x; j < count; j += blockDim.x) {
+    double& wj = w[(size_t)frames[j] * k + i];
+    wj = wj + opr_total(part, 4, j, 1) / (opr_total(part, 4, j, 0) + reg);
+  }
 }
 
 }  // namespace ptyb
