@@ -941,10 +941,10 @@ int create_handle(const ptyb_scan* scan, const double* object, int32_t nobj, int
   h->nyo = nyo;
   h->nxo = nxo;
   h->C = C;
-  // The position sums reduce over the whole cluster twice per frame: at side 256 they run on
+  // The position sums reduce over the whole cluster once per frame: at side 256 they run on
   // clusters of 8 (measured faster than 16), whatever cluster the frame kernels take.
   h->C_sums = C;
-  if (N == 256 && frame_smem_bytes<256, 8>(K) <= 227 * 1024) h->C_sums = 8;
+  if (N == 256 && frame_smem_bytes<256, 8>(std::max(K, 2)) <= 227 * 1024) h->C_sums = 8;
   h->stack = options && options->stack_size > 0 ? options->stack_size : 512;
   h->nslice = nslice;
   h->log_stride = 2 + nslice;

@@ -282,11 +282,11 @@ cudaError_t launch_frame(ptyb_handle* h, const FrameArgs& a, int nslot) {
 }
 
 // Plane transforms of the position model over `nslot` frames (the frame kernel's cluster
-// shape; window derivatives carry two planes).
+// shape; window derivatives carry two planes, the position sums at least two).
 template <int MODE>
 cudaError_t launch_move(ptyb_handle* h, const MoveArgs& a, int nslot) {
   if (nslot <= 0) return cudaSuccess;
-  const int K = MODE == kDerivWindow ? 2 : h->K;
+  const int K = MODE == kDerivWindow ? 2 : MODE == kDerivSums ? std::max(h->K, 2) : h->K;
   constexpr int kind = MODE == kDerivSums      ? kKDerivSums
                        : MODE == kSpectrum     ? kKSpectrum
                        : MODE == kBackSpectrum ? kKBackSpectrum

@@ -207,6 +207,23 @@ PTYB_D void cluster_sum2(double& x, double& y, double* red, cg::cluster_group& c
   y = sy;
 }
 
+// Cluster-wide sums of four doubles, every thread getting them (rank order, as cluster_sum2).
+template <int N, int C>
+PTYB_D void cluster_sum4(double (&v)[4], double* red, cg::cluster_group& cluster) {
+  using F = FrameShape<N, C>;
+  block_sum<F::T>(v, 4, red);
+  csync<C>(cluster);
+  double t[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int q = 0; q < C; ++q) {
+    const double* rq = C > 1 ? cluster.map_shared_rank(red, q) : red;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) t[k] += rq[k];
+  }
+  csync<C>(cluster);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) v[k] = t[k];
+}
+
 // The projection's input S = c_po·po + c_psi·carry + c_it·iter at element `pix` of mode m of
 // `slot` (kCarry); the prologue (`store`) also writes it to RAAR's iterate.
 template <int N>

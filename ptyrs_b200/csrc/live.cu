@@ -399,7 +399,7 @@ int ptyb_live_handle(ptyb_live* l, const double* object, int32_t nyo, int32_t nx
   h->nxo = nxo;
   h->C = C;
   h->C_sums = C;
-  if (N == 256 && frame_smem_bytes<256, 8>(nprobe) <= 227 * 1024) h->C_sums = 8;
+  if (N == 256 && frame_smem_bytes<256, 8>(std::max(nprobe, 2)) <= 227 * 1024) h->C_sums = 8;
   h->stack = options && options->stack_size > 0 ? options->stack_size : 512;
   h->nslice = 1;
   h->log_stride = 3;

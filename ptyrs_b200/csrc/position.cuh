@@ -61,8 +61,10 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
   constexpr int H = F::H, T = F::T, L = F::L;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int K = MODE == kDerivWindow ? 2 : a.K;
+  // planes held in shared memory: the position sums hold the two axes of one mode at a time
+  const int KP = MODE == kDerivSums ? max(K, 2) : K;
   float2* S = reinterpret_cast<float2*>(smem_raw);
-  double* red = reinterpret_cast<double*>(S + (size_t)K * H * L + N);
+  double* red = reinterpret_cast<double*>(S + (size_t)KP * H * L + N);
   cg::cluster_group cluster = cg::this_cluster();
   const int r = C > 1 ? (int)cluster.block_rank() : 0;
   const int slot = blockIdx.x / C;
@@ -92,7 +94,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
   // The translation phase exp(−2πi f·d) = exp(−2πi fy·dy)·exp(−2πi fx·dx), over N²: the row
   // factor for every ky in the free N-entry region after the planes, the column factor of this
   // thread's one column (T is a multiple of H, so a thread keeps c = tid % H).
-  float2* ey = S + (size_t)K * H * L;
+  float2* ey = S + (size_t)KP * H * L;
   float2 ex = make_float2(1.f, 0.f);
   if (moves) {
     for (int k = tid; k < N; k += T) {
@@ -155,10 +157,58 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
     __syncthreads();  // the row factors
   }
 
-  const int naxis = MODE == kDerivSums ? 2 : 1;
+  if (MODE == kDerivSums) {
+    // Both axes of one mode at a time, the planes holding ∂_y and ∂_x of mode m's moved probe:
+    // each mode's spectrum, field plane and window are read once for both axes.
+    constexpr float two_pi = 2.f * 3.14159265358979f;
+    const float2* cf = a.c + (size_t)slot * K * plane;
+    double v4[4] = {0.0, 0.0, 0.0, 0.0};  // num_y, num_x, den_y, den_x
 #pragma unroll 1
-  for (int ax = 0; ax < naxis; ++ax) {
-    const int axis = ax;
+    for (int m = 0; m < K; ++m) {
+#pragma unroll 2
+      for (int idx = tid; idx < H * N; idx += T) {
+        const int c = idx % H, ky = idx / H, kx = r * H + c;
+        const float2 v = cmul(a.spec[((size_t)m * N + ky) * N + kx], cmul(ey[ky], ex));
+        // × (−2πi·f_axis): the derivative of the translation phase (engine/features.rs:372-387)
+        const float wy = two_pi * fft_freq(ky, N), wx = two_pi * fft_freq(kx, N);
+        S[c * L + (ky ^ swz(c))] = make_float2(wy * v.y, -wy * v.x);
+        S[(H + c) * L + (ky ^ swz(H + c))] = make_float2(wx * v.y, -wx * v.x);
+      }
+      __syncthreads();
+      // two planes, as a value the compiler does not unroll the transforms' plane loops over
+      int two = 2;
+      asm volatile("" : "+r"(two));
+      all_lines<N, C, +1>(S, two * H, ltw);
+      transpose<N, C>(S, two, cluster);
+      all_lines<N, C, +1>(S, two * H, ltw);
+      // dψ = O·∂W on natural rows; num = Σ Re(conj(c)·dψ), den = Σ |dψ|² over modes and
+      // pixels (engine/features.rs:992-1025)
+#pragma unroll 2
+      for (int idx = tid; idx < H * N; idx += T) {
+        const int yl = idx / N, x = idx % N, y = r * H + yl;
+        const float2 o = a.object[(size_t)(corner.x + y) * a.nxo + corner.y + x];
+        float2 v = cf[m * plane + y * N + x];
+        if (a.minus)
+          v = csub(v, cmul(cmul(a.minus[(size_t)slot * K * plane + m * plane + y * N + x], o),
+                           a.quad[y * N + x]));
+#pragma unroll
+        for (int ax = 0; ax < 2; ++ax) {
+          const int line = ax * H + yl;
+          const float2 d = cmul(o, S[line * L + (x ^ swz(line))]);
+          v4[ax] += (double)v.x * d.x + (double)v.y * d.y;
+          v4[2 + ax] += (double)d.x * d.x + (double)d.y * d.y;
+        }
+      }
+      __syncthreads();  // the next mode's spectrum overwrites the planes read above
+    }
+    cluster_sum4<N, C>(v4, red, cluster);
+    if (r == 0 && tid == 0)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) a.sums[(size_t)f * 4 + k] = v4[k];
+    return;
+  }
+
+  {
     // Spectrum: column kx = r·H + c as line (m·H + c), element ky.
 #pragma unroll 2
     for (int idx = tid; idx < H * N; idx += T) {
@@ -167,11 +217,7 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
       float2 e = make_float2(1.f, 0.f);
       if (moves) {
         e = cmul(ey[ky], ex);
-        if (MODE == kDerivSums) {
-          // × (−2πi·f_axis): the derivative of the translation phase (engine/features.rs:372-387)
-          const float w = 2.f * 3.14159265358979f * (axis == 0 ? fy : fx);
-          e = make_float2(w * e.y, -w * e.x);
-        } else if (MODE == kDerivMove) {
+        if (MODE == kDerivMove) {
           // × (−2πi·f_a) or × (−2πi·f_a)(−2πi·f_b) = −4π²·f_a·f_b
           const float wy = 2.f * 3.14159265358979f * fy, wx = 2.f * 3.14159265358979f * fx;
           if (a.deriv <= 2) {
@@ -200,41 +246,14 @@ __global__ void __launch_bounds__(FrameShape<N, C>::T,
     transpose<N, C>(S, K, cluster);
     all_lines<N, C, +1>(S, K * H, ltw);
 
-    if (MODE != kDerivSums) {
 #pragma unroll 2
-      for (int idx = tid; idx < H * N; idx += T) {
-        const int yl = idx / N, x = idx % N, y = r * H + yl;
-        const float2 cq = bare ? make_float2(1.f, 0.f) : cconj(a.quad[y * N + x]);
-        for (int m = 0; m < K; ++m) {
-          const int line = m * H + yl;
-          const float2 v = S[line * L + (x ^ swz(line))];
-          out[m * plane + y * N + x] = bare ? v : cmul(cq, v);
-        }
-      }
-    } else {
-      // dψ = O·∂W on natural rows; num = Σ Re(conj(c)·dψ), den = Σ |dψ|² over modes and pixels
-      // (engine/features.rs:992-1025), cluster-summed in rank order.
-      double num = 0.0, den = 0.0;
-      const float2* cf = a.c + (size_t)slot * K * plane;
-#pragma unroll 4
-      for (int idx = tid; idx < H * N; idx += T) {
-        const int yl = idx / N, x = idx % N, y = r * H + yl;
-        const float2 o = a.object[(size_t)(corner.x + y) * a.nxo + corner.y + x];
-        for (int m = 0; m < K; ++m) {
-          const int line = m * H + yl;
-          const float2 d = cmul(o, S[line * L + (x ^ swz(line))]);
-          float2 v = cf[m * plane + y * N + x];
-          if (a.minus)
-            v = csub(v, cmul(cmul(a.minus[(size_t)slot * K * plane + m * plane + y * N + x], o),
-                             a.quad[y * N + x]));
-          num += (double)v.x * d.x + (double)v.y * d.y;
-          den += (double)d.x * d.x + (double)d.y * d.y;
-        }
-      }
-      cluster_sum2<N, C>(num, den, red, cluster);
-      if (r == 0 && tid == 0) {
-        a.sums[(size_t)f * 4 + axis] = num;
-        a.sums[(size_t)f * 4 + 2 + axis] = den;
+    for (int idx = tid; idx < H * N; idx += T) {
+      const int yl = idx / N, x = idx % N, y = r * H + yl;
+      const float2 cq = bare ? make_float2(1.f, 0.f) : cconj(a.quad[y * N + x]);
+      for (int m = 0; m < K; ++m) {
+        const int line = m * H + yl;
+        const float2 v = S[line * L + (x ^ swz(line))];
+        out[m * plane + y * N + x] = bare ? v : cmul(cq, v);
       }
     }
   }
