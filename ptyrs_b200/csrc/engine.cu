@@ -729,20 +729,22 @@ __global__ void __launch_bounds__(256) exit_power_kernel(const float2* object,
   const float2* p = probe + (size_t)f * stride;
   const float2* ow = object + (size_t)c.x * nxo + c.y;
   double s = 0.0;
-  // rows and columns carried along the 256-pixel strides, no division per pixel
-  int y = threadIdx.x / N, x = threadIdx.x % N;
+  // Two neighbouring pixels of a row per thread and step (N is even), the probe planes read as
+  // 16-byte pairs; rows and columns carried along the 512-pixel strides.
+  int y = 2 * threadIdx.x / N, x = 2 * threadIdx.x % N;
 #pragma unroll 4
-  for (int pix = threadIdx.x; pix < N * N; pix += 256) {
-    const float2 o = ow[(size_t)y * nxo + x];
-    const float o2 = o.x * o.x + o.y * o.y;
-    float p2 = 0.f;
+  for (int pp = threadIdx.x; pp < N * N / 2; pp += 256) {
+    const float2* orow = ow + (size_t)y * nxo + x;
+    const float2 o0 = orow[0], o1 = orow[1];
+    float p0 = 0.f, p1 = 0.f;
     for (int m = 0; m < K; ++m) {
-      const float2 v = p[(size_t)m * N * N + pix];
-      p2 += v.x * v.x + v.y * v.y;
+      const float4 v = reinterpret_cast<const float4*>(p + (size_t)m * N * N)[pp];
+      p0 += v.x * v.x + v.y * v.y;
+      p1 += v.z * v.z + v.w * v.w;
     }
-    s += (double)p2 * o2;
-    y += 256 / N;
-    x += 256 % N;
+    s += (double)p0 * (o0.x * o0.x + o0.y * o0.y) + (double)p1 * (o1.x * o1.x + o1.y * o1.y);
+    y += 512 / N;
+    x += 512 % N;
     if (x >= N) {
       x -= N;
       ++y;

@@ -35,10 +35,13 @@ static __global__ void __launch_bounds__(512) lsqml_dots_kernel(
   const int span = (K * N * N + kDotParts - 1) / kDotParts;
   const int i0 = part * span, i1 = min(K * N * N, i0 + span);
   float s[6] = {0, 0, 0, 0, 0, 0};
+  // mode, pixel, row and column of idx carried along the 512-element strides (no division per
+  // element; N² > 512 at every side)
+  const int nn = N * N;
+  int m = (i0 + (int)threadIdx.x) / nn, pix = (i0 + (int)threadIdx.x) - m * nn;
+  int yy = pix / N, xx = pix - yy * N;
 #pragma unroll 4
   for (int idx = i0 + threadIdx.x; idx < i1; idx += 512) {
-    const int m = idx / (N * N), pix = idx % (N * N);
-    const int yy = pix / N, xx = pix % N;
     const size_t o = (size_t)(c.x + yy) * nxo + c.y + xx;
     const float2 q = quad[pix];
     const float2 u = cmul(cmul(probe[(size_t)slot * probe_stride + m * plane + pix], d_obj[o]), q);
@@ -50,6 +53,18 @@ static __global__ void __launch_bounds__(512) lsqml_dots_kernel(
     s[3] += u.y * v.x - u.x * v.y;
     s[4] += u.x * x.x + u.y * x.y;
     s[5] += v.x * x.x + v.y * x.y;
+    pix += 512;
+    xx += 512 % N;
+    yy += 512 / N;
+    if (xx >= N) {
+      xx -= N;
+      ++yy;
+    }
+    if (pix >= nn) {
+      pix -= nn;
+      yy -= N;
+      ++m;
+    }
   }
   const double reg = part == 0 ? lambda0 * (double)K * (double)plane : 0.0;
   for (int k = 0; k < 6; ++k) {

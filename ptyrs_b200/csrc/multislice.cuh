@@ -294,15 +294,28 @@ static __global__ void __launch_bounds__(512) slice_dots_kernel(const float2* d_
   const int2 c = corners[frames[slot]];
   const size_t plane = (size_t)N * N;
   float s0 = 0.f, s1 = 0.f;
-  for (int idx = threadIdx.x; idx < K * N * N; idx += 512) {
-    const int m = idx / (N * N), pix = idx % (N * N);
-    const int yy = pix / N, xx = pix % N;
+  // mode, pixel, row and column carried along the 512-element strides (N² > 512 at every side)
+  const int nn = N * N;
+  int m = 0, pix = threadIdx.x, yy = pix / N, xx = pix - yy * N;
+  for (int idx = threadIdx.x; idx < K * nn; idx += 512) {
     float2 u = cmul(incident[((size_t)slot * K + m) * plane + pix],
                     d_obj[(size_t)(c.x + yy) * nxo + c.y + xx]);
     if (quad) u = cmul(u, quad[pix]);
     const float2 x = chi[((size_t)slot * K + m) * plane + pix];
     s0 += u.x * x.x + u.y * x.y;
     s1 += cnorm2(u);
+    pix += 512;
+    xx += 512 % N;
+    yy += 512 / N;
+    if (xx >= N) {
+      xx -= N;
+      ++yy;
+    }
+    if (pix >= nn) {
+      pix -= nn;
+      yy -= N;
+      ++m;
+    }
   }
   auto bsum = [&](float v) {
     double d = warp_sum((double)v);
