@@ -281,7 +281,7 @@ def sample_scan(s, m):
 # launch's frames.
 NCU_DRAM_BYTES_PER_FRAME = {
     # the 1000-frame cut of the ml256 scan, one 488-frame launch of each
-    "ml256": {"frame_ml_grad": 3.35e6, "deriv_sums": 1.07e6},
+    "ml256": {"frame_ml_grad": 3.35e6, "deriv_sums": 1.06e6},
     # the carry pass on the 1024-frame cut of the dm256 scan
     "dm256": {"frame_carry": 2.33e6},
 }
