@@ -11,7 +11,10 @@ CONFIG is one of CONFIGS: rpie64 (400 frames of 64², rPIE with α = β = 0.1 in
 lsqml128 (4096 frames of 128² × 3 modes, Poisson LSQML in batches of 256) and ml256 (the first
 2500 of the 10000 frames of 256² × 2 modes with the whole 2048² object, Poisson ML conjugate
 gradient refining the positions: the float64 oracle holds every view's exit wave at once, about
-21 GB per array for all 10000 frames, more host memory than a run here has). The inputs
+21 GB per array for all 10000 frames, more host memory than a run here has) and msml128 (6000
+frames of 128² × 2 modes through three 1536² slices, Poisson ML through the slices; the oracle
+runs one call of k cycles per checkpoint, since the opening rescale and the conjugate
+directions belong to a call). The inputs
 are the benchmark's seeded scans (`sim.make_scan`; ml256's counts made with torch on the host,
 so both phases read the same counts, checked by a digest). The oracle phase runs one call of
 the longest run and keeps a snapshot after each checkpoint's iteration; the GPU phase runs
@@ -39,6 +42,7 @@ CONFIGS = {
     "lsqml128": dict(kind="lsqml128", algorithm="lsqml", batch=256,
                      checkpoints=[1, 2, 5, 10, 20, 50, 100]),
     "ml256": dict(kind="ml256", algorithm="ml", checkpoints=[1, 2], scale=0.25),
+    "msml128": dict(kind="ms128", algorithm="ml_slices", checkpoints=[1, 2, 5]),
 }
 
 
@@ -50,9 +54,14 @@ def inputs(cfg):
 
 
 def optics_of(s):
+    """The far field of the scan's geometry, through its slices when it has gaps."""
     from oracle import ops
-    return ops.Optics.far_field(s["wavelength"], s["distance"], s["detector_pixel"],
-                                [s["n"], s["n"]])
+    optics = ops.Optics.far_field(s["wavelength"], s["distance"], s["detector_pixel"],
+                                  [s["n"], s["n"]])
+    if s.get("gaps"):
+        optics = optics.with_slices([ops.Wavefield([s["n"], s["n"]], s["wavelength"],
+                                                   optics.pixel, z) for z in s["gaps"]])
+    return optics
 
 
 def write_meta(name, out, s, digest, mask, times):
@@ -68,7 +77,7 @@ def run_meta(name, out):
     from oracle import ops
     from oracle.ptycho import Ptycho
     s, digest = inputs(CONFIGS[name])
-    p = Ptycho(s["counts"], s["y"], s["x"], optics_of(s), s["object"], s["probe"])
+    p = Ptycho(s["counts"], s["y"], s["x"], optics_of(s), s["object"][:1], s["probe"])
     illum = ops.illumination(p.addr.views, p.object.shape, p.probe)
     write_meta(name, out, s, digest, illum >= 1e-3 * illum.max(), {})
 
@@ -82,6 +91,7 @@ def run_oracle(name, out, eps=0.0, save_as=None):
     from oracle.ptycho import Ptycho
     cfg = CONFIGS[name]
     os.makedirs(out, exist_ok=True)
+    ops.FFT_WORKERS = os.cpu_count()  # the oracle's transforms on every host core
     t0 = time.perf_counter()
     s, digest = inputs(cfg)
     optics = optics_of(s)
@@ -90,7 +100,7 @@ def run_oracle(name, out, eps=0.0, save_as=None):
         rng = np.random.default_rng(11)
         xi = (rng.standard_normal(start.shape) + 1j * rng.standard_normal(start.shape)) / np.sqrt(2)
         start = start * (1.0 + eps * xi)
-    p = Ptycho(s["counts"], s["y"], s["x"], optics, start, s["probe"])
+    p = Ptycho(s["counts"], s["y"], s["x"], optics, start[:1], s["probe"])
     illum = ops.illumination(p.addr.views, p.object.shape, p.probe)
     mask = illum >= 1e-3 * illum.max()
     last = max(cfg["checkpoints"])
@@ -113,6 +123,14 @@ def run_oracle(name, out, eps=0.0, save_as=None):
             p.rpie(1, batch_size=cfg["batch"], obj_alpha=0.1, probe_alpha=0.1, seed=7)
             if k in cfg["checkpoints"]:
                 save(k, p.object, p.probe)
+    elif cfg["algorithm"] == "ml_slices":
+        # ML through the slices (one call of k cycles per checkpoint: the opening rescale and
+        # the conjugate directions are a call's)
+        from oracle.lsqml import multislice_ml
+        slices = [start[k:k + 1] for k in range(start.shape[0])]
+        for k in cfg["checkpoints"]:
+            objs, probe, _ = multislice_ml(p.addr, p.obs, optics, slices, p.probe, k)
+            save(k, np.concatenate(objs), probe)
     elif cfg["algorithm"] == "lsqml":
         run = Lsqml(cfg["batch"], "poisson", 7)
         obj, probe = p.object, p.probe
@@ -136,15 +154,16 @@ def compare(name, ref, k, obj, probe, offsets):
     from ptyrs_b200.metrics import object_nrmse
     m = np.load(os.path.join(ref, f"{name}_mask.npz"))
     mask = np.unpackbits(m["mask"])[:int(np.prod(m["shape"]))].reshape(m["shape"])
-    mask = mask.reshape(mask.shape[-2:]).astype(bool)  # one object mode
+    mask = mask.reshape(mask.shape[-2:]).astype(bool)  # one object mode (or every slice)
     r = np.load(os.path.join(ref, f"{name}_{k}.npz"))
     ro, rp = r["object"].astype(np.complex128), r["probe"]
+    full = np.broadcast_to(mask, obj.shape)
     row = {"iterations": k,
            "object_rel_l2": float(np.linalg.norm(obj - ro) / np.linalg.norm(ro)),
-           "object_rel_l2_illuminated": float(np.linalg.norm((obj - ro)[0][mask])
-                                              / np.linalg.norm(ro[0][mask])),
+           "object_rel_l2_illuminated": float(np.linalg.norm((obj - ro)[full])
+                                              / np.linalg.norm(ro[full])),
            "probe_rel_l2": float(np.linalg.norm(probe - rp) / np.linalg.norm(rp)),
-           "object_nrmse": object_nrmse(obj, ro, mask.astype(float)[None])}
+           "object_nrmse": object_nrmse(obj, ro, full.astype(float))}
     if offsets is not None and len(r["offsets"]):
         row["offsets_max_abs_diff_px"] = float(np.abs(offsets - r["offsets"]).max())
     print(json.dumps(row), flush=True)
@@ -171,16 +190,20 @@ def run_gpu(name, ref, out):
     rows = []
     reached = [k for k in cfg["checkpoints"] if os.path.exists(os.path.join(ref, f"{name}_{k}.npz"))]
     for k in reached:
-        with GpuPtycho(scan, s["object"], s["probe"]) as g:
+        with GpuPtycho(scan, s["object"], s["probe"], gaps=s.get("gaps")) as g:
             if cfg["algorithm"] == "rpie":
                 g.rpie(k, batch_size=cfg["batch"], obj_alpha=0.1, probe_alpha=0.1, seed=7)
             elif cfg["algorithm"] == "lsqml":
                 g.lsqml(k, batch_size=cfg["batch"], cost="poisson", seed=7)
+            elif cfg["algorithm"] == "ml_slices":
+                g.ml(k, update_object=True, update_probe=True, calc_llk=0,
+                     zero_phase_ramp=False)
             else:
                 g.set_positions(np.zeros((len(s["counts"]), 2)), refine=True)
                 g.ml(k, update_object=True, update_probe=True, calc_llk=0,
                      zero_phase_ramp=False)
-            obj, probe = g.object(), g.probe()
+            obj = g.objects() if s.get("gaps") else g.object()
+            probe = g.probe()
             d = g.positions() if cfg["algorithm"] == "ml" else None
         rows.append(compare(name, ref, k, obj, probe, d))
     report(name, ref, out, rows, path="CUDA FP32")
