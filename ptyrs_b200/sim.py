@@ -251,7 +251,8 @@ def make_scan(kind, seed=0, scale=1.0, device=None):
         c = corners(pos, n, side)
         px = wavelength * distance / (n * DETECTOR_PIXEL)
         gaps = (1e-5, 1e-5)
-        counts = multislice_counts_gpu(truth, probe, c, gaps, wavelength, px, photons, seed + 3)
+        counts = multislice_counts_gpu(truth, probe, c, gaps, wavelength, px, photons, seed + 3,
+                                       device=device)
         start = np.ones((3, side, side), np.complex128)
         return dict(counts=counts, y=pos[:, 0] * px, x=pos[:, 1] * px, object=start,
                     probe=probe * np.sqrt(photons / (np.abs(probe) ** 2).sum()),
