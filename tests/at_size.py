@@ -42,7 +42,7 @@ CONFIGS = {
     "lsqml128": dict(kind="lsqml128", algorithm="lsqml", batch=256,
                      checkpoints=[1, 2, 5, 10, 20, 50, 100]),
     "ml256": dict(kind="ml256", algorithm="ml", checkpoints=[1, 2], scale=0.25),
-    "msml128": dict(kind="ms128", algorithm="ml_slices", checkpoints=[1, 2, 5]),
+    "msml128": dict(kind="ms128", algorithm="ml_slices", checkpoints=[1, 2]),
 }
 
 
